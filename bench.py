@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the CUDA forward path tracer (Mpaths/s on one B200).
+
+A step renders one full frame of the mesh-heavy workload: a seeded 1024x1024-vertex fBm
+terrain (2,093,058 triangles) with 32 tessellated spheres of 20,480 triangles each
+(40 % Lambert, 30 % Beckmann metal, 30 % glass IOR 1.5), lit by a 2048x1024 float32 sky
+map plus a 0.53 degree sun, 1920x1080 pixels at 64 samples per pixel, max depth 16.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank renders the full frame with its own sample streams
+(weak scaling) and the linear framebuffers are summed with one NCCL all-reduce per step.
+The reference arm (--impl reference) times the CPU restatement of the reference tracer
+(oracle/) on this machine's host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mpaths/s at 1 B200"
+UNIT = "Mpaths/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def workload(args):
+    from naivetrace_b200 import scenes
+    if args.small:
+        return scenes.terrain_spheres(xres=480, yres=270, terrain_n=256, sphere_level=4, num_spheres=32,
+                                      env_w=512, env_h=256), 16, 16, "terrain_spheres_small"
+    return scenes.terrain_spheres(), args.spp, 16, "terrain_spheres"
+
+
+def workload_config(scene, spp, depth, name):
+    cam = scene.camera
+    return {
+        "workload": f"{name}: fBm terrain + 32 spheres, {scene.num_triangles} triangles, sky map + sun, "
+                    f"{cam.xres}x{cam.yres} at {spp} spp, max depth {depth}",
+        "triangles": scene.num_triangles,
+        "resolution": [cam.xres, cam.yres],
+        "spp": spp,
+        "max_depth": depth,
+        "paths_per_step": cam.xres * cam.yres * spp,
+        "l2_policy": "inputs larger than L2: BVH + triangles ~0.2 GB and path state ~0.8 GB per wave stream",
+    }
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.dev)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for name, val in zip(names[1:], parts[5:9]):
+                if val.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "power_w_max": max(power),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        peaks = json.loads(PEAKS_FILE.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        return world, rank, local, dist
+    return 1, 0, local, None
+
+
+def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=4096, seed=1):
+    """Times the oracle (CPU restatement of the reference pt) on all host cores over a
+    bounded sample: consecutive pixel chunks of the frame at 1 sample each, until about
+    budget_s of CPU time.  Returns (Mpaths/s, cores, description)."""
+    from oracle.oracle import OracleScene
+    from naivetrace_b200.scene import make_params
+    cores = os.cpu_count() or 1
+    o = OracleScene(scene, make_params(max_ray_depth=depth))
+    npix = o.npix
+    acc = np.zeros(3 * npix)
+    light = np.zeros(3 * npix)
+    done_paths = 0
+    start = npix // 2 - chunk_pixels * 4
+    t0 = time.perf_counter()
+    k = 0
+    while True:
+        pb = (start + k * chunk_pixels) % (npix - chunk_pixels)
+        o.render(1, seed=seed, sample_offset=0, pixel_begin=pb, pixel_end=pb + chunk_pixels, nthreads=cores,
+                 accum=acc, light_accum=light)
+        done_paths += chunk_pixels
+        k += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or k >= 200:
+            break
+    mpaths = done_paths / el / 1e6
+    desc = (f"{k} chunks of {chunk_pixels} consecutive pixels from the frame centre at 1 sample each "
+            f"({done_paths} paths, {el:.1f} s, depth {depth}) on {cores} threads")
+    return mpaths, cores, desc
+
+
+def run_reference_arm(args):
+    world, rank, local, dist = dist_setup(args)
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    scene, spp, depth, name = workload(args)
+    vals = []
+    desc = ""
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference(scene, spp, depth, budget_s=2.0)
+    for _ in range(args.steps):
+        v, cores, desc = cpu_reference(scene, spp, depth, budget_s=args.cpu_budget)
+        vals.append(v)
+    value = float(np.mean(vals))
+    paths = scene.camera.xres * scene.camera.yres * spp
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": paths / (value * 1e6) * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded procedural scene)",
+        "config": workload_config(scene, spp, depth, name),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": desc + "; the reference itself cannot be built here (Embree, Eigen, TBB, "
+                                          "Boost, yaml-cpp, pcg32 are absent), so this is the CPU restatement"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def scene_bytes(scene):
+    v, n, t, m = scene.arrays()
+    b = v.nbytes + (n.nbytes if n is not None else 0) + t.nbytes + m.nbytes
+    for e in scene.env_lights:
+        if e.texture is not None:
+            b += e.texture.nbytes
+    return int(b)
+
+
+def run_ours(args):
+    import torch
+
+    from naivetrace_b200 import abi
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+
+    world, rank, local, dist = dist_setup(args)
+    device = local if torch.cuda.is_available() else 0
+    torch.cuda.set_device(device)
+    scene, spp, depth, name = workload(args)
+    params = make_params(max_ray_depth=depth, wave_paths=args.wave, device=device)
+    seed = 1 + rank
+    g = GpuContext(scene, params)
+    npix = g.npix
+    paths_per_step = npix * spp
+
+    # Bytes-per-ray model: a counting pass (1 spp, seed 1) records BVH nodes visited and
+    # triangles tested by the closest-hit kernel.
+    g.set_profiling(2)
+    g.render(1, seed=1)
+    cst = g.stats()
+    ext_rays = max(cst["extension_rays"], 1)
+    nodes_per_ray = cst["node_visits"] / ext_rays
+    tris_per_ray = cst["tri_tests"] / ext_rays
+    bytes_per_ray = 48.0 + cst["bvh_node_bytes"] * nodes_per_ray + cst["tri_bytes"] * tris_per_ray
+    g.set_profiling(0)
+    g.clear()
+    g.reset_stats()
+
+    fb_tensors = None
+    if dist is not None:
+        fb_tensors = (torch.zeros(3 * npix, dtype=torch.float64, device="cuda"),
+                      torch.zeros(3 * npix, dtype=torch.float64, device="cuda"))
+
+    def step():
+        g.render(spp, seed)
+        if dist is not None:
+            s = torch.cuda.current_stream().cuda_stream
+            st = g.lib.tt_read_accumulators_device(g.h, C.c_void_p(fb_tensors[0].data_ptr()),
+                                                   C.c_void_p(fb_tensors[1].data_ptr()), C.c_void_p(s))
+            abi.check(g.lib, g.h, st, "tt_read_accumulators_device")
+            dist.all_reduce(fb_tensors[0])
+            dist.all_reduce(fb_tensors[1])
+
+    for _ in range(args.warmup):
+        step()
+    g.clear()
+    g.reset_stats()
+    g.set_profiling(1)
+    clocks = ClockSampler(device)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    elapsed_ms = ev0.elapsed_time(ev1)
+    st = g.stats()
+    g.set_profiling(0)
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = world * paths_per_step / (ms_per_step * 1e-3) / 1e6
+    mrays = world * (st["extension_rays"] + st["shadow_rays"]) / args.steps / (ms_per_step * 1e-3) / 1e6
+    # Roofline of the dominant kernel (closest-hit traversal).
+    ext_launch_ms = st["extend_ms"] / max(st["extend_launches"], 1)
+    achieved_gbs = st["extension_rays"] * bytes_per_ray / (st["extend_ms"] * 1e-3) / 1e9 if st["extend_ms"] > 0 else 0.0
+    peak, peak_kind = hbm_peak()
+    rays_per_launch = st["extension_rays"] / max(st["extend_launches"], 1)
+    traffic = None
+    tfile = ROOT / "profiles" / "extend_traffic.json"
+    if tfile.exists():
+        try:
+            td = json.loads(tfile.read_text())
+            traffic = td.get("bytes_per_ray", 0) * rays_per_launch
+        except Exception:
+            traffic = None
+
+    # End to end through the C ABI from host buffers: create + upload (BVH build and the
+    # scene's host-to-device copies) + render + framebuffer read-back + destroy.
+    e2e_ms = []
+    d2h = 3 * npix * 4
+    h2d = scene_bytes(scene)
+    rgb = np.zeros(3 * npix, np.float32)
+    for _ in range(args.e2e_steps):
+        if dist is not None:
+            dist.barrier()
+        t0 = time.perf_counter()
+        ge = GpuContext(scene, params)
+        ge.render(spp, seed)
+        ge.lib.tt_read_framebuffer(ge.h, rgb.ctypes.data_as(C.POINTER(C.c_float)), None)
+        ge.close()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_step = float(np.median(e2e_ms))
+    if dist is not None:
+        t = torch.tensor([e2e_step], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+    e2e_value = world * paths_per_step / (e2e_step * 1e-3) / 1e6
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, cores, desc = cpu_reference(scene, spp, depth, budget_s=args.cpu_budget)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded procedural scene, no dataset)",
+            "config": dict(workload_config(scene, spp, depth, name), parallelism=f"replicas{world}, framebuffer all-reduce"),
+            "mrays_per_s": mrays,
+            "roofline": {
+                "kernel": "k_extend (closest-hit BVH traversal)",
+                "bound": "hbm",
+                "achieved": achieved_gbs,
+                "peak": peak,
+                "peak_source": peak_kind,
+                "unit": "GB/s",
+                "frac": achieved_gbs / peak if peak else None,
+                "traffic": traffic,
+                "bytes_per_ray": bytes_per_ray,
+                "nodes_per_ray": nodes_per_ray,
+                "tris_per_ray": tris_per_ray,
+                "avg_launch_ms": ext_launch_ms,
+                "rays_per_launch": rays_per_launch,
+            },
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": e2e_step,
+                    "what": "tt_create + tt_upload_scene (host BVH build, scene H2D) + tt_render_pass + "
+                            "tt_read_framebuffer + tt_destroy"},
+            "gpu_launches": int(st["kernel_launches"]),
+            "clocks": clk,
+            "stats": {k: st[k] for k in ("extension_rays", "shadow_rays", "extend_launches", "extend_ms",
+                                         "shadow_launches", "shadow_ms", "pass_ms", "bvh_nodes", "bvh_depth",
+                                         "error_flags")},
+        }
+        print(json.dumps(line))
+    g.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--spp", type=int, default=64)
+    ap.add_argument("--wave", type=int, default=0, help="paths per wavefront wave (0 = library default)")
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
+    args = ap.parse_args(argv)
+    if args.warmup < 3 and not args.small:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,252 @@
+/*
+ * toytrace_gpu.h -- C ABI of the B200 forward path tracer with next-event estimation.
+ *
+ * This is the drop-in boundary for ToyTrace's `--algo pt` rendering algorithm.  The
+ * reference runs that algorithm as `ForwardPathTracer`, a `RenderingAlgo` subclass
+ * (src/renderingalgorithms_pathtracing.cxx:59-75; interface in
+ * src/renderingalgorithms_interface.hxx:13-30).  A host adapter (toytrace_gpu_algo.hpp)
+ * implements that interface on top of the entry points below, so toytrace can select the
+ * GPU tracer as one more algorithm name.
+ *
+ * Conventions
+ *  - Every entry point returns a tt_status; nothing throws across the ABI.
+ *  - All pointers in tt_scene_desc and in the batch calls are HOST pointers unless the
+ *    function name ends in `_device`.
+ *  - Spectra are binned: TT_NBINS bins of 10 nm between 370 and 730 nm, bin i centred at
+ *    375 + 10 i nm (src/spectral.hxx:24-44).
+ *  - Pixel ("unit") index = y * xres + x with y = 0 the BOTTOM row of the image, as in
+ *    Camera::UnitToPixel (src/camera.hxx:22-29).  tt_generate_image flips rows the way
+ *    framebuffer::ToImage does (src/renderbuffer.hxx:99-125).
+ */
+#ifndef TOYTRACE_GPU_H
+#define TOYTRACE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TT_NBINS 36
+#define TT_ABI_VERSION 1
+
+typedef int32_t tt_status;
+enum {
+  TT_OK = 0,
+  TT_ERR_CUDA = 1,          /* a CUDA runtime call failed (message via tt_last_error) */
+  TT_ERR_INVALID = 2,       /* bad argument or malformed scene */
+  TT_ERR_CAPACITY = 3,      /* a fixed-size device structure overflowed */
+  TT_ERR_LOOP_CAP = 4,      /* a bounded device loop (BVH stack, tracking) hit its cap */
+  TT_ERR_INTERRUPTED = 5,   /* the pass was stopped by tt_request_stop */
+  TT_ERR_NOT_READY = 6      /* tt_upload_scene has not run yet */
+};
+
+/* Shader kinds: the surface scatterers of src/shader.cxx. */
+enum {
+  TT_SHADER_DIFFUSE = 0,             /* DiffuseShader            shader.cxx:251-318 */
+  TT_SHADER_SPECULAR_REFLECTIVE = 1, /* SpecularReflectiveShader shader.cxx:322-366 */
+  TT_SHADER_SPECULAR_DIELECTRIC = 2, /* SpecularTransmissiveDielectricShader shader.cxx:378-630 */
+  TT_SHADER_MICROFACET = 3           /* MicrofacetShader (Beckmann, VNDF) shader.cxx:634-707 */
+};
+
+/* A material = shader + optional area emitter (struct Material, src/scene.hxx:45-54). */
+typedef struct tt_material {
+  int32_t shader;                  /* TT_SHADER_* */
+  float reflectance[TT_NBINS];     /* kr_d / kr_s per bin (diffuse, mirror, microfacet) */
+  float alpha;                     /* Beckmann roughness (microfacet) */
+  float ior_ratio;                 /* inside / outside IOR (dielectric) */
+  int32_t emissive;                /* nonzero: UniformAreaLight on every triangle */
+  float emission[TT_NBINS];        /* UniformAreaLight spectrum (area power density;
+                                      radiance = spectrum / 2pi, light.hxx:72-108) */
+} tt_material;
+
+/* Environmental lights: the members of TotalEnvironmentalRadianceField (light.hxx:292-304). */
+enum {
+  TT_ENV_DOME = 0,        /* DistantDomeLight   light.hxx:180-219: spectrum, dir = up     */
+  TT_ENV_SUN = 1,         /* Sun                light.hxx:238-288: scalar = total power,
+                             dir = direction the light travels, scalar2 = opening angle deg */
+  TT_ENV_MAP = 2,         /* EnvMapLight        light.cxx:88-189: texture, dir = up      */
+  TT_ENV_DIRECTIONAL = 3  /* DistantDirectionalLight light.hxx:146-177: spectrum, dir       */
+};
+
+typedef struct tt_env_light {
+  int32_t kind;
+  float spectrum[TT_NBINS];
+  float dir[3];
+  float scalar;
+  float scalar2;
+  int32_t tex_width;       /* TT_ENV_MAP: float RGB texture, row 0 = top row of the image */
+  int32_t tex_height;
+  const float* tex_rgb;    /* tex_width * tex_height * 3 floats (linear RGB) */
+} tt_env_light;
+
+/* PointLight (light.hxx:13-42): spectrum = total power, radiated uniformly. */
+typedef struct tt_point_light {
+  float spectrum[TT_NBINS];
+  float pos[3];
+} tt_point_light;
+
+enum { TT_CAMERA_PINHOLE = 0, TT_CAMERA_FISHEYE = 1 };
+
+/* PerspectiveCamera (camera.hxx:62-156): fov_deg is the HORIZONTAL full angle.
+ * FisheyeHemisphereCamera (camera.hxx:159-232) ignores fov_deg. */
+typedef struct tt_camera {
+  int32_t kind;
+  float pos[3];
+  float dir[3];
+  float up[3];
+  float fov_deg;
+  int32_t xres;
+  int32_t yres;
+} tt_camera;
+
+/* Flat scene.  Triangles are numbered in the order given; tt_intersect_batch reports
+ * these global indices.  normals may be NULL (flat shading: smooth normal = geometry
+ * normal, like Mesh::MakeFlatNormals, primitive.cxx:18-46). */
+typedef struct tt_scene_desc {
+  uint32_t num_vertices;
+  const float* vertices;        /* num_vertices * 3 */
+  const float* normals;         /* num_vertices * 3 or NULL */
+  uint32_t num_triangles;
+  const uint32_t* indices;      /* num_triangles * 3 */
+  const uint32_t* material_ids; /* num_triangles */
+  uint32_t num_materials;
+  const tt_material* materials;
+  uint32_t num_env_lights;
+  const tt_env_light* env_lights;
+  uint32_t num_point_lights;
+  const tt_point_light* point_lights;
+  tt_camera camera;
+} tt_scene_desc;
+
+enum { TT_SAMPLE_BOTH = 0, TT_SAMPLE_BSDF = 1, TT_SAMPLE_LIGHTS = 2 }; /* --pt-sample-mode */
+
+/* RenderingParameters subset used by the path (src/scene.hxx:24-43). */
+typedef struct tt_params {
+  int32_t max_ray_depth;        /* --rd (reference default 25) */
+  int32_t pt_sample_mode;       /* TT_SAMPLE_* */
+  int32_t max_samples_per_pixel;/* --spp; <= 0 means unbounded (Run loops until stopped) */
+  int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default */
+  int32_t device;               /* CUDA device ordinal */
+} tt_params;
+
+typedef struct tt_ctx tt_ctx;
+
+/* Per-context counters, accumulated since tt_reset_stats. */
+typedef struct tt_stats {
+  uint64_t paths;               /* camera samples started */
+  uint64_t extension_rays;      /* closest-hit queries */
+  uint64_t shadow_rays;         /* occlusion queries */
+  uint64_t extend_launches;     /* closest-hit kernel launches */
+  double extend_ms;             /* summed CUDA-event time of those launches (if profiling) */
+  uint64_t shadow_launches;
+  double shadow_ms;
+  double pass_ms;               /* summed CUDA-event time of whole passes */
+  uint64_t kernel_launches;     /* all kernels launched by render passes */
+  uint64_t node_visits;         /* closest-hit traversal: BVH nodes visited (counting mode) */
+  uint64_t tri_tests;           /* closest-hit traversal: triangles tested (counting mode) */
+  uint64_t shadow_node_visits;  /* occlusion traversal, counting mode */
+  uint64_t shadow_tri_tests;
+  uint64_t counted_rays;
+  uint32_t bvh_nodes;
+  uint32_t bvh_node_bytes;
+  uint32_t tri_bytes;
+  uint32_t bvh_depth;
+  uint64_t error_flags;         /* device error word (TT_ERR_* bits) */
+} tt_stats;
+
+/* Library/ABI version; lets a loader check it bound the right library. */
+int32_t tt_abi_version(void);
+
+/* RenderAlgorithmFactory + constructor (renderingalgorithms.cxx:27-42): validates and deep
+ * copies the scene description; allocates nothing on the GPU yet. */
+tt_status tt_create(const tt_scene_desc* scene, const tt_params* params, tt_ctx** out_ctx);
+
+/* RenderingAlgo::InitializeScene + Scene::BuildAccelStructure (scene.cxx:116-141): builds
+ * the BVH and uploads geometry, materials, lights and the framebuffer. */
+tt_status tt_upload_scene(tt_ctx* ctx);
+
+/* One pass of the SamplesPerPixelSchedule loop (renderingalgorithms_simplebase.hxx:125-157):
+ * renders spp samples for every pixel into the accumulators.  seed selects the PCG32
+ * stream family; samples are numbered consecutively across passes. */
+tt_status tt_render_pass(tt_ctx* ctx, int32_t spp, uint64_t seed);
+
+/* Same as tt_render_pass restricted to pixels [pixel_begin, pixel_end). */
+tt_status tt_render_pass_range(tt_ctx* ctx, int32_t spp, uint64_t seed,
+                               int32_t pixel_begin, int32_t pixel_end);
+
+/* RenderingAlgo::RequestInterrupt / RequestFullStop: lock-free flag writes, callable from
+ * any thread, also before the first pass.  A stop makes the running and all later
+ * passes return TT_ERR_INTERRUPTED at the next wave boundary. */
+tt_status tt_request_interrupt(tt_ctx* ctx);
+tt_status tt_request_stop(tt_ctx* ctx);
+/* Returns 1 and clears the flag if an interrupt was requested since the last poll. */
+int32_t tt_poll_interrupt(tt_ctx* ctx);
+int32_t tt_stop_requested(tt_ctx* ctx);
+
+/* Linear RGB per pixel = accum / samples_per_pixel + light_accum * npix / splat_count,
+ * exactly Spectral3ImageBuffer::ToImage before the clamp (renderbuffer.hxx:172-200).
+ * rgb: npix*3 floats.  sample_counts (nullable): npix entries of samples per pixel. */
+tt_status tt_read_framebuffer(tt_ctx* ctx, float* rgb_linear, uint64_t* sample_counts);
+
+/* Raw accumulators for parity tests: accum and light_accum, npix*3 doubles each. */
+tt_status tt_read_accumulators(tt_ctx* ctx, double* accum, double* light_accum,
+                               uint64_t* samples_per_pixel, uint64_t* splat_count);
+
+/* GenerateImage: 8-bit RGB, clamp to [0,1], sRGB unless linear, rows flipped
+ * (framebuffer::ToImage, renderbuffer.hxx:99-125).  out: xres*yres*3 bytes. */
+tt_status tt_generate_image(tt_ctx* ctx, int32_t linear_output, uint8_t* out_rgb8);
+
+/* Clears accumulators and sample counters. */
+tt_status tt_clear_framebuffer(tt_ctx* ctx);
+
+/* Closest-hit queries (EmbreeAccelerator::FirstIntersection, embreeaccelerator.cxx:87-131).
+ * rays: n * 8 floats (org xyz, tnear, dir xyz, tfar).  Outputs (n each): prim id or -1,
+ * hit distance, barycentric u, v (hit = (1-u-v) v0 + u v1 + v v2). */
+tt_status tt_intersect_batch(tt_ctx* ctx, const float* rays, int32_t n,
+                             int32_t* prim_ids, float* t, float* u, float* v);
+/* Occlusion queries (EmbreeAccelerator::IsOccluded, embreeaccelerator.cxx:284-304). */
+tt_status tt_occluded_batch(tt_ctx* ctx, const float* rays, int32_t n, uint8_t* occluded);
+/* Device-pointer variants; stream is a cudaStream_t (NULL = legacy default stream). */
+tt_status tt_intersect_batch_device(tt_ctx* ctx, const float* d_rays, int32_t n,
+                                    int32_t* d_prim_ids, float* d_t, float* d_u, float* d_v,
+                                    void* stream);
+
+/* Counting traversal over a ray batch: adds nodes visited and triangles tested to the
+ * stats (for the algorithmic-bytes model of the closest-hit kernel). */
+tt_status tt_count_traversal(tt_ctx* ctx, const float* rays, int32_t n);
+
+/* BSDF sampling/evaluation on the device for the sampling tests
+ * (ShaderScatterer fixture, tests_sampling.cxx:932-1046).  The surface lies in the
+ * z = 0 plane with geometry and shading normal +z; wi: reverse incident direction
+ * (pointing away from the surface).  lambda_idx: 3 bin indices.
+ *   sample: out_dir n*3, out_value n*3, out_pdf n (negative = from a delta distribution).
+ *   eval:   dirs n*3 in, out_value n*3, out_pdf n. */
+tt_status tt_sample_bsdf_batch(tt_ctx* ctx, int32_t material, const float* wi,
+                               const int32_t* lambda_idx, int32_t n, uint64_t seed,
+                               float* out_dir, float* out_value, float* out_pdf);
+tt_status tt_eval_bsdf_batch(tt_ctx* ctx, int32_t material, const float* wi,
+                             const int32_t* lambda_idx, const float* dirs, int32_t n,
+                             float* out_value, float* out_pdf);
+
+/* Device-side copy of the raw accumulators into caller-owned device buffers (npix*3
+ * doubles each), ordered on `stream` (a cudaStream_t; NULL = legacy default stream).
+ * Lets a multi-GPU caller reduce framebuffers with NCCL without a host round trip. */
+tt_status tt_read_accumulators_device(tt_ctx* ctx, double* d_accum, double* d_light_accum, void* stream);
+
+/* Profiling level: 0 off; 1 render passes time each closest-hit and shadow launch with
+ * CUDA events on the launching stream and add the durations to the stats; 2 additionally
+ * counts BVH nodes visited and triangles tested (slower; for the bytes-per-ray model). */
+tt_status tt_set_profiling(tt_ctx* ctx, int32_t on);
+tt_status tt_get_stats(tt_ctx* ctx, tt_stats* out);
+tt_status tt_reset_stats(tt_ctx* ctx);
+
+/* Last error message of this context (or of the last failed tt_create when ctx is NULL). */
+tt_status tt_last_error(tt_ctx* ctx, char* buf, int32_t n);
+void tt_destroy(tt_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOYTRACE_GPU_H */

@@ -1,0 +1,248 @@
+"""ctypes mirror of include/toytrace_gpu.h and the loader of the CUDA library.
+
+The structures below must match the C declarations field for field; tests/test_abi.py
+checks their sizes against the compiled library's expectations.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+NBINS = 36
+
+TT_OK = 0
+TT_ERR_CUDA = 1
+TT_ERR_INVALID = 2
+TT_ERR_CAPACITY = 3
+TT_ERR_LOOP_CAP = 4
+TT_ERR_INTERRUPTED = 5
+TT_ERR_NOT_READY = 6
+
+STATUS_NAMES = {
+    TT_OK: "TT_OK",
+    TT_ERR_CUDA: "TT_ERR_CUDA",
+    TT_ERR_INVALID: "TT_ERR_INVALID",
+    TT_ERR_CAPACITY: "TT_ERR_CAPACITY",
+    TT_ERR_LOOP_CAP: "TT_ERR_LOOP_CAP",
+    TT_ERR_INTERRUPTED: "TT_ERR_INTERRUPTED",
+    TT_ERR_NOT_READY: "TT_ERR_NOT_READY",
+}
+
+SHADER_DIFFUSE = 0
+SHADER_SPECULAR_REFLECTIVE = 1
+SHADER_SPECULAR_DIELECTRIC = 2
+SHADER_MICROFACET = 3
+
+ENV_DOME = 0
+ENV_SUN = 1
+ENV_MAP = 2
+ENV_DIRECTIONAL = 3
+
+CAMERA_PINHOLE = 0
+CAMERA_FISHEYE = 1
+
+SAMPLE_BOTH = 0
+SAMPLE_BSDF = 1
+SAMPLE_LIGHTS = 2
+
+
+class Material(C.Structure):
+    _fields_ = [
+        ("shader", C.c_int32),
+        ("reflectance", C.c_float * NBINS),
+        ("alpha", C.c_float),
+        ("ior_ratio", C.c_float),
+        ("emissive", C.c_int32),
+        ("emission", C.c_float * NBINS),
+    ]
+
+
+class EnvLight(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("spectrum", C.c_float * NBINS),
+        ("dir", C.c_float * 3),
+        ("scalar", C.c_float),
+        ("scalar2", C.c_float),
+        ("tex_width", C.c_int32),
+        ("tex_height", C.c_int32),
+        ("tex_rgb", C.POINTER(C.c_float)),
+    ]
+
+
+class PointLight(C.Structure):
+    _fields_ = [("spectrum", C.c_float * NBINS), ("pos", C.c_float * 3)]
+
+
+class Camera(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("pos", C.c_float * 3),
+        ("dir", C.c_float * 3),
+        ("up", C.c_float * 3),
+        ("fov_deg", C.c_float),
+        ("xres", C.c_int32),
+        ("yres", C.c_int32),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("num_vertices", C.c_uint32),
+        ("vertices", C.POINTER(C.c_float)),
+        ("normals", C.POINTER(C.c_float)),
+        ("num_triangles", C.c_uint32),
+        ("indices", C.POINTER(C.c_uint32)),
+        ("material_ids", C.POINTER(C.c_uint32)),
+        ("num_materials", C.c_uint32),
+        ("materials", C.POINTER(Material)),
+        ("num_env_lights", C.c_uint32),
+        ("env_lights", C.POINTER(EnvLight)),
+        ("num_point_lights", C.c_uint32),
+        ("point_lights", C.POINTER(PointLight)),
+        ("camera", Camera),
+    ]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("max_ray_depth", C.c_int32),
+        ("pt_sample_mode", C.c_int32),
+        ("max_samples_per_pixel", C.c_int32),
+        ("wave_paths", C.c_int32),
+        ("device", C.c_int32),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("paths", C.c_uint64),
+        ("extension_rays", C.c_uint64),
+        ("shadow_rays", C.c_uint64),
+        ("extend_launches", C.c_uint64),
+        ("extend_ms", C.c_double),
+        ("shadow_launches", C.c_uint64),
+        ("shadow_ms", C.c_double),
+        ("pass_ms", C.c_double),
+        ("kernel_launches", C.c_uint64),
+        ("node_visits", C.c_uint64),
+        ("tri_tests", C.c_uint64),
+        ("shadow_node_visits", C.c_uint64),
+        ("shadow_tri_tests", C.c_uint64),
+        ("counted_rays", C.c_uint64),
+        ("bvh_nodes", C.c_uint32),
+        ("bvh_node_bytes", C.c_uint32),
+        ("tri_bytes", C.c_uint32),
+        ("bvh_depth", C.c_uint32),
+        ("error_flags", C.c_uint64),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+PKG_DIR = Path(__file__).resolve().parent
+LIB_DIR = PKG_DIR / "_build"
+LIB_NAME = "libtoytrace_gpu.so"
+
+# Every symbol declared in include/toytrace_gpu.h.
+EXPORTED_SYMBOLS = [
+    "tt_abi_version",
+    "tt_create",
+    "tt_upload_scene",
+    "tt_render_pass",
+    "tt_render_pass_range",
+    "tt_request_interrupt",
+    "tt_request_stop",
+    "tt_poll_interrupt",
+    "tt_stop_requested",
+    "tt_read_framebuffer",
+    "tt_read_accumulators",
+    "tt_generate_image",
+    "tt_clear_framebuffer",
+    "tt_intersect_batch",
+    "tt_occluded_batch",
+    "tt_intersect_batch_device",
+    "tt_count_traversal",
+    "tt_sample_bsdf_batch",
+    "tt_eval_bsdf_batch",
+    "tt_read_accumulators_device",
+    "tt_set_profiling",
+    "tt_get_stats",
+    "tt_reset_stats",
+    "tt_last_error",
+    "tt_destroy",
+]
+
+_lib = None
+
+
+class TTError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def lib_path() -> Path:
+    return Path(os.environ.get("TT_GPU_LIB", LIB_DIR / LIB_NAME))
+
+
+def load_library() -> C.CDLL:
+    """Loads the CUDA library.  Raises if it is missing: there is no CPU fallback."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = lib_path()
+    if not path.exists():
+        raise RuntimeError(
+            f"CUDA path-tracer library not found at {path}; build it with "
+            "`python -m naivetrace_b200.build` (there is no CPU fallback)"
+        )
+    lib = C.CDLL(str(path))
+    P = C.POINTER
+    vp = C.c_void_p
+    sig = {
+        "tt_abi_version": ([], C.c_int32),
+        "tt_create": ([P(SceneDesc), P(Params), P(vp)], C.c_int32),
+        "tt_upload_scene": ([vp], C.c_int32),
+        "tt_render_pass": ([vp, C.c_int32, C.c_uint64], C.c_int32),
+        "tt_render_pass_range": ([vp, C.c_int32, C.c_uint64, C.c_int32, C.c_int32], C.c_int32),
+        "tt_request_interrupt": ([vp], C.c_int32),
+        "tt_request_stop": ([vp], C.c_int32),
+        "tt_poll_interrupt": ([vp], C.c_int32),
+        "tt_stop_requested": ([vp], C.c_int32),
+        "tt_read_framebuffer": ([vp, P(C.c_float), P(C.c_uint64)], C.c_int32),
+        "tt_read_accumulators": ([vp, P(C.c_double), P(C.c_double), P(C.c_uint64), P(C.c_uint64)], C.c_int32),
+        "tt_generate_image": ([vp, C.c_int32, P(C.c_uint8)], C.c_int32),
+        "tt_clear_framebuffer": ([vp], C.c_int32),
+        "tt_intersect_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_int32), P(C.c_float), P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_occluded_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_uint8)], C.c_int32),
+        "tt_intersect_batch_device": ([vp, vp, C.c_int32, vp, vp, vp, vp, vp], C.c_int32),
+        "tt_count_traversal": ([vp, P(C.c_float), C.c_int32], C.c_int32),
+        "tt_sample_bsdf_batch": ([vp, C.c_int32, P(C.c_float), P(C.c_int32), C.c_int32, C.c_uint64, P(C.c_float), P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_eval_bsdf_batch": ([vp, C.c_int32, P(C.c_float), P(C.c_int32), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_read_accumulators_device": ([vp, vp, vp, vp], C.c_int32),
+        "tt_set_profiling": ([vp, C.c_int32], C.c_int32),
+        "tt_get_stats": ([vp, P(Stats)], C.c_int32),
+        "tt_reset_stats": ([vp], C.c_int32),
+        "tt_last_error": ([vp, C.c_char_p, C.c_int32], C.c_int32),
+        "tt_destroy": ([vp], None),
+    }
+    for name, (argtypes, restype) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = restype
+    _lib = lib
+    return lib
+
+
+def last_error(lib, ctx) -> str:
+    buf = C.create_string_buffer(1024)
+    lib.tt_last_error(ctx, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(lib, ctx, status: int, what: str) -> None:
+    if status != TT_OK:
+        raise TTError(status, f"{what}: {last_error(lib, ctx)}")

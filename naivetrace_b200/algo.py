@@ -1,0 +1,233 @@
+"""Python host mirror of ToyTrace's RenderingAlgo interface over the CUDA C ABI.
+
+RenderingAlgo (src/renderingalgorithms_interface.hxx:13-30):
+    SetInterruptCallback(cb)  InitializeScene(scene)  Run()  RequestInterrupt()
+    RequestFullStop()  GenerateImage()
+GpuPathTracer implements it with the SamplesPerPixelSchedule of the reference's
+SimplePixelByPixelRenderingAlgo (renderingalgorithms_simplebase.hxx:34-157): the samples
+per pass double from 1 up to 1024, capped by max_samples_per_pixel; the callback runs on
+the Run thread after every pass with is_complete_pass=True; RequestInterrupt makes Run
+call the callback with is_complete_pass=False at the next pass boundary; RequestFullStop
+ends Run at the next wave boundary.  Both may be called from any thread, also before Run.
+
+GpuContext is the thin object wrapper of the C ABI used by the tests and the benchmark.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Callable, Optional
+
+import numpy as np
+
+from . import abi
+from .image import to_image
+from .scene import Scene, make_params
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class GpuContext:
+    """One tt_ctx: a scene uploaded to one GPU plus its accumulators."""
+
+    def __init__(self, scene: Scene, params: Optional[abi.Params] = None, upload: bool = True):
+        self.lib = abi.load_library()
+        self.scene = scene
+        self.params = params if params is not None else make_params()
+        desc, keep = scene.to_desc()
+        self._keep = keep
+        h = C.c_void_p()
+        st = self.lib.tt_create(C.byref(desc), C.byref(self.params), C.byref(h))
+        if st != abi.TT_OK:
+            raise abi.TTError(st, "tt_create: " + abi.last_error(self.lib, None))
+        self.h = h
+        self.npix = scene.camera.xres * scene.camera.yres
+        if upload:
+            self.upload()
+
+    def _check(self, st, what):
+        abi.check(self.lib, self.h, st, what)
+
+    def upload(self):
+        self._check(self.lib.tt_upload_scene(self.h), "tt_upload_scene")
+
+    def render_pass(self, spp: int, seed: int = 1, pixel_begin: int = 0, pixel_end: Optional[int] = None) -> int:
+        if pixel_end is None and pixel_begin == 0:
+            return self.lib.tt_render_pass(self.h, spp, seed)
+        pe = self.npix if pixel_end is None else pixel_end
+        return self.lib.tt_render_pass_range(self.h, spp, seed, pixel_begin, pe)
+
+    def render(self, spp: int, seed: int = 1, pixel_begin: int = 0, pixel_end: Optional[int] = None) -> None:
+        self._check(self.render_pass(spp, seed, pixel_begin, pixel_end), "tt_render_pass")
+
+    def framebuffer(self) -> np.ndarray:
+        rgb = np.zeros(3 * self.npix, np.float32)
+        self._check(self.lib.tt_read_framebuffer(self.h, _fp(rgb), None), "tt_read_framebuffer")
+        return rgb
+
+    def accumulators(self):
+        acc = np.zeros(3 * self.npix)
+        light = np.zeros(3 * self.npix)
+        spp = np.zeros(self.npix, np.uint64)
+        splat = C.c_uint64(0)
+        dp = C.POINTER(C.c_double)
+        self._check(self.lib.tt_read_accumulators(self.h, acc.ctypes.data_as(dp), light.ctypes.data_as(dp),
+                                                  spp.ctypes.data_as(C.POINTER(C.c_uint64)), C.byref(splat)),
+                    "tt_read_accumulators")
+        return acc, light, spp, splat.value
+
+    def image(self, linear_output: bool = False) -> np.ndarray:
+        out = np.zeros((self.scene.camera.yres, self.scene.camera.xres, 3), np.uint8)
+        self._check(self.lib.tt_generate_image(self.h, int(linear_output), out.ctypes.data_as(C.POINTER(C.c_uint8))),
+                    "tt_generate_image")
+        return out
+
+    def clear(self):
+        self._check(self.lib.tt_clear_framebuffer(self.h), "tt_clear_framebuffer")
+
+    def intersect(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        prim = np.zeros(n, np.int32)
+        t = np.zeros(n, np.float32)
+        u = np.zeros(n, np.float32)
+        v = np.zeros(n, np.float32)
+        self._check(self.lib.tt_intersect_batch(self.h, _fp(rays), n, prim.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                _fp(t), _fp(u), _fp(v)), "tt_intersect_batch")
+        return prim, t, u, v
+
+    def occluded(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        out = np.zeros(len(rays), np.uint8)
+        self._check(self.lib.tt_occluded_batch(self.h, _fp(rays), len(rays), out.ctypes.data_as(C.POINTER(C.c_uint8))),
+                    "tt_occluded_batch")
+        return out.astype(bool)
+
+    def count_traversal(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        self._check(self.lib.tt_count_traversal(self.h, _fp(rays), len(rays)), "tt_count_traversal")
+
+    def sample_bsdf(self, material: int, wi, lambda_idx, n: int, seed: int):
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        d = np.zeros((n, 3), np.float32)
+        val = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        self._check(self.lib.tt_sample_bsdf_batch(self.h, material, _fp(wi), li.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                  n, seed, _fp(d), _fp(val), _fp(pdf)), "tt_sample_bsdf_batch")
+        return d, val, pdf
+
+    def eval_bsdf(self, material: int, wi, lambda_idx, dirs):
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+        n = len(dirs)
+        val = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        self._check(self.lib.tt_eval_bsdf_batch(self.h, material, _fp(wi), li.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                _fp(dirs), n, _fp(val), _fp(pdf)), "tt_eval_bsdf_batch")
+        return val, pdf
+
+    def set_profiling(self, level: int):
+        self._check(self.lib.tt_set_profiling(self.h, level), "tt_set_profiling")
+
+    def stats(self) -> dict:
+        s = abi.Stats()
+        self._check(self.lib.tt_get_stats(self.h, C.byref(s)), "tt_get_stats")
+        return s.as_dict()
+
+    def reset_stats(self):
+        self._check(self.lib.tt_reset_stats(self.h), "tt_reset_stats")
+
+    def request_interrupt(self):
+        self.lib.tt_request_interrupt(self.h)
+
+    def request_stop(self):
+        self.lib.tt_request_stop(self.h)
+
+    def poll_interrupt(self) -> bool:
+        return bool(self.lib.tt_poll_interrupt(self.h))
+
+    def stop_requested(self) -> bool:
+        return bool(self.lib.tt_stop_requested(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.tt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SamplesPerPixelSchedule:
+    """renderingalgorithms_simplebase.hxx:34-62."""
+
+    MAX_SPP_PER_ITERATION = 1024
+
+    def __init__(self, max_spp: int):
+        self.spp = 1
+        self.total = 0
+        self.max_spp = max_spp
+
+    def update_for_next_pass(self):
+        self.total += self.spp
+        if self.spp < self.MAX_SPP_PER_ITERATION:
+            self.spp *= 2
+        if self.max_spp > 0 and self.total + self.spp > self.max_spp:
+            self.spp = self.max_spp - self.total
+
+
+class GpuPathTracer:
+    """RenderingAlgo for the CUDA tracer (`--algo gpu`)."""
+
+    def __init__(self, scene: Scene, params: Optional[abi.Params] = None, seed: int = 1, linear_output: bool = False):
+        self.scene = scene
+        self.params = params if params is not None else make_params()
+        self.seed = seed
+        self.linear_output = linear_output
+        self._cb: Optional[Callable[[bool], None]] = None
+        self.ctx = GpuContext(scene, self.params, upload=False)
+        self.schedule = SamplesPerPixelSchedule(self.params.max_samples_per_pixel)
+        self.last_status = abi.TT_OK
+
+    def set_interrupt_callback(self, cb: Callable[[bool], None]):
+        self._cb = cb
+
+    def initialize_scene(self, scene: Optional[Scene] = None):
+        self.ctx.upload()
+
+    def run(self):
+        self.initialize_scene()
+        while not self.ctx.stop_requested() and self.schedule.spp > 0:
+            st = self.ctx.render_pass(self.schedule.spp, self.seed)
+            self.last_status = st
+            if st == abi.TT_ERR_INTERRUPTED:
+                break
+            self.ctx._check(st, "tt_render_pass")
+            if self.ctx.poll_interrupt() and self._cb:
+                self._cb(False)
+            if self._cb:
+                self._cb(True)
+            self.schedule.update_for_next_pass()
+
+    def request_interrupt(self):
+        self.ctx.request_interrupt()
+
+    def request_full_stop(self):
+        self.ctx.request_stop()
+
+    def generate_image(self) -> np.ndarray:
+        """8-bit RGB, row 0 at the top (framebuffer::ToImage)."""
+        return self.ctx.image(self.linear_output)
+
+    def linear_framebuffer(self) -> np.ndarray:
+        return self.ctx.framebuffer()
+
+
+def to_image_host(rgb, xres, yres, linear_output=False):
+    return to_image(rgb, xres, yres, linear_output)

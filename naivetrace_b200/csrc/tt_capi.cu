@@ -1,0 +1,847 @@
+// C ABI of the CUDA forward path tracer (include/toytrace_gpu.h): context lifetime, scene
+// upload, the pass loop over wavefront waves, framebuffer readback and the batch queries.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/toytrace_gpu.h"
+#include "tt_bvh.h"
+#include "tt_internal.h"
+#include "tt_tables.h"
+
+using namespace tt;
+
+namespace {
+
+constexpr int kDefaultWave = 1 << 22;
+
+std::mutex g_err_mutex;
+std::string g_create_error;
+
+struct HostEnv {
+  tt_env_light desc;
+  std::vector<float> tex;
+};
+
+struct DeviceBuffers {
+  std::vector<void*> allocs;
+  void* alloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    allocs.push_back(p);
+    return p;
+  }
+  void free_all() {
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+  }
+};
+
+__global__ void k_tally(const int* counters, int rounds, unsigned long long* stats) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    unsigned long long e = 0, s = 0;
+    for (int b = 0; b <= rounds; ++b) {
+      e += (unsigned long long)counters[3 * b];
+      s += (unsigned long long)counters[3 * b + 1];
+    }
+    stats[4] += e;
+    stats[5] += s;
+  }
+}
+
+}  // namespace
+
+struct tt_ctx {
+  // Host copy of the scene.
+  std::vector<float> verts, normals;
+  std::vector<uint32_t> idx, mats;
+  std::vector<tt_material> materials;
+  std::vector<HostEnv> envs;
+  std::vector<tt_point_light> points;
+  tt_camera camera{};
+  tt_params params{};
+  int npix = 0;
+  bool uploaded = false;
+  // Device state.
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DeviceBuffers scene_mem, path_mem;
+  DevScene dev{};
+  PathState ps{};
+  Framebuffer fb{};
+  double* d_acc = nullptr;
+  double* d_light = nullptr;
+  unsigned long long* d_stats = nullptr;  // 0..3 traversal counts, 4 ext rays, 5 shadow rays
+  unsigned int* d_err = nullptr;
+  int grid = 0;
+  int wave_cap = 0;
+  int rounds = 0;
+  // Accumulation bookkeeping.
+  std::vector<uint64_t> spp_count;
+  uint64_t splat_count = 0;
+  uint64_t next_sample = 0;
+  // Control.
+  std::atomic<int> stop{0};
+  std::atomic<int> interrupt{0};
+  int profiling = 0;
+  tt_stats stats{};
+  std::string err;
+  uint32_t bvh_nodes = 0, bvh_depth = 0;
+};
+
+static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
+  if (c) c->err = msg;
+  else {
+    std::lock_guard<std::mutex> g(g_err_mutex);
+    g_create_error = msg;
+  }
+  return s;
+}
+
+#define TT_CUDA(ctx, call)                                                                   \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      return fail(ctx, TT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+// OrthogonalSystemZAligned in double (vec3f.hxx:240-258); writes columns X, Y, Z.
+static void frame_z_d(const double z[3], float X[3], float Y[3], float Z[3]) {
+  const double sign = std::copysign(1.0, z[2]);
+  const double a = -1.0 / (sign + z[2]);
+  const double b = z[0] * z[1] * a;
+  const double x[3] = {1.0 + sign * z[0] * z[0] * a, sign * b, -sign * z[0]};
+  const double y[3] = {b, sign + z[1] * z[1] * a, -z[1]};
+  for (int k = 0; k < 3; ++k) { X[k] = (float)x[k]; Y[k] = (float)y[k]; Z[k] = (float)z[k]; }
+}
+
+static void normalize_d(double v[3]) {
+  const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  for (int k = 0; k < 3; ++k) v[k] /= l;
+}
+
+extern "C" {
+
+int32_t tt_abi_version(void) { return TT_ABI_VERSION; }
+
+tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
+  if (!out) return fail(nullptr, TT_ERR_INVALID, "tt_create: out_ctx is NULL");
+  *out = nullptr;
+  if (!d || !p) return fail(nullptr, TT_ERR_INVALID, "tt_create: scene or params is NULL");
+  if (d->num_triangles > (1u << 28)) return fail(nullptr, TT_ERR_CAPACITY, "more than 2^28 triangles");
+  if (d->num_triangles > 0 && (!d->vertices || !d->indices || !d->material_ids))
+    return fail(nullptr, TT_ERR_INVALID, "triangle arrays missing");
+  if (d->num_materials > 0 && !d->materials) return fail(nullptr, TT_ERR_INVALID, "materials missing");
+  if (d->camera.xres <= 0 || d->camera.yres <= 0) return fail(nullptr, TT_ERR_INVALID, "bad camera resolution");
+  if ((int64_t)d->camera.xres * d->camera.yres > (1ll << 30)) return fail(nullptr, TT_ERR_CAPACITY, "too many pixels");
+  if (d->num_env_lights > (uint32_t)MAX_ENV_LIGHTS) return fail(nullptr, TT_ERR_CAPACITY, "too many env lights");
+  if (p->pt_sample_mode < 0 || p->pt_sample_mode > 2) return fail(nullptr, TT_ERR_INVALID, "bad pt_sample_mode");
+  if (p->max_ray_depth > 1000) return fail(nullptr, TT_ERR_INVALID, "max_ray_depth above 1000");
+  for (uint32_t t = 0; t < d->num_triangles; ++t) {
+    for (int k = 0; k < 3; ++k)
+      if (d->indices[3 * (size_t)t + k] >= d->num_vertices)
+        return fail(nullptr, TT_ERR_INVALID, "vertex index out of range in triangle " + std::to_string(t));
+    if (d->material_ids[t] >= d->num_materials)
+      return fail(nullptr, TT_ERR_INVALID, "material index out of range in triangle " + std::to_string(t));
+  }
+  for (uint32_t i = 0; i < d->num_materials; ++i) {
+    const tt_material& m = d->materials[i];
+    if (m.shader < TT_SHADER_DIFFUSE || m.shader > TT_SHADER_MICROFACET)
+      return fail(nullptr, TT_ERR_INVALID, "unknown shader kind in material " + std::to_string(i));
+    if (m.shader == TT_SHADER_MICROFACET && !(m.alpha > 0.f))
+      return fail(nullptr, TT_ERR_INVALID, "microfacet roughness must be positive");
+    if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && !(m.ior_ratio > 0.f))
+      return fail(nullptr, TT_ERR_INVALID, "dielectric ior_ratio must be positive");
+  }
+  auto* c = new tt_ctx;
+  c->verts.assign(d->vertices, d->vertices + 3 * (size_t)d->num_vertices);
+  if (d->normals) c->normals.assign(d->normals, d->normals + 3 * (size_t)d->num_vertices);
+  c->idx.assign(d->indices, d->indices + 3 * (size_t)d->num_triangles);
+  c->mats.assign(d->material_ids, d->material_ids + d->num_triangles);
+  c->materials.assign(d->materials, d->materials + d->num_materials);
+  for (uint32_t i = 0; i < d->num_env_lights; ++i) {
+    HostEnv e;
+    e.desc = d->env_lights[i];
+    if (e.desc.kind < TT_ENV_DOME || e.desc.kind > TT_ENV_DIRECTIONAL) {
+      delete c;
+      return fail(nullptr, TT_ERR_INVALID, "unknown env light kind");
+    }
+    if (e.desc.kind == TT_ENV_MAP) {
+      if (!e.desc.tex_rgb || e.desc.tex_width <= 0 || e.desc.tex_height <= 0) {
+        delete c;
+        return fail(nullptr, TT_ERR_INVALID, "env map without texture");
+      }
+      e.tex.assign(e.desc.tex_rgb, e.desc.tex_rgb + 3 * (size_t)e.desc.tex_width * e.desc.tex_height);
+      e.desc.tex_rgb = nullptr;
+    }
+    c->envs.push_back(std::move(e));
+  }
+  if (d->num_point_lights > 0) c->points.assign(d->point_lights, d->point_lights + d->num_point_lights);
+  c->camera = d->camera;
+  c->params = *p;
+  if (c->params.max_ray_depth <= 0) c->params.max_ray_depth = 25;
+  c->npix = d->camera.xres * d->camera.yres;
+  c->device = p->device;
+  c->spp_count.assign(c->npix, 0);
+  *out = c;
+  return TT_OK;
+}
+
+tt_status tt_upload_scene(tt_ctx* c) {
+  if (!c) return TT_ERR_INVALID;
+  TT_CUDA(c, cudaSetDevice(c->device));
+  if (c->uploaded) return TT_OK;
+  TT_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  upload_constant_tables();
+  TT_CUDA(c, cudaGetLastError());
+  const uint32_t ntri = (uint32_t)c->mats.size();
+  // BVH.
+  BvhInput bi{c->verts.data(), c->idx.data(), c->mats.data(), ntri};
+  BvhOutput bo;
+  if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
+  c->bvh_nodes = bo.num_nodes;
+  c->bvh_depth = bo.max_depth;
+  if (bo.max_depth + 2 >= (uint32_t)BVH_STACK)
+    return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
+  auto upload = [&](const void* src, size_t bytes) -> void* {
+    void* p = c->scene_mem.alloc(bytes);
+    if (p && bytes) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    return p;
+  };
+  DevScene& s = c->dev;
+  s.nodes = (const float4*)upload(bo.nodes.data(), bo.nodes.size() * sizeof(float));
+  s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
+  std::vector<uint32_t> ti(4 * (size_t)ntri);
+  for (uint32_t t = 0; t < ntri; ++t) {
+    ti[4 * t] = c->idx[3 * t];
+    ti[4 * t + 1] = c->idx[3 * t + 1];
+    ti[4 * t + 2] = c->idx[3 * t + 2];
+    ti[4 * t + 3] = c->mats[t];
+  }
+  s.tri_idx = (const uint4*)upload(ti.data(), ti.size() * sizeof(uint32_t));
+  s.normals = c->normals.empty() ? nullptr : (const float*)upload(c->normals.data(), c->normals.size() * sizeof(float));
+  s.num_tris = (int)ntri;
+  // Materials.
+  std::vector<DevMaterial> dm(c->materials.size());
+  for (size_t i = 0; i < dm.size(); ++i) {
+    const tt_material& m = c->materials[i];
+    dm[i].shader = m.shader;
+    dm[i].emissive = m.emissive ? 1 : 0;
+    dm[i].alpha = m.alpha;
+    dm[i].ior_ratio = m.ior_ratio;
+    std::memcpy(dm[i].reflectance, m.reflectance, sizeof(m.reflectance));
+    std::memcpy(dm[i].emission, m.emission, sizeof(m.emission));
+  }
+  s.materials = (const DevMaterial*)upload(dm.data(), dm.size() * sizeof(DevMaterial));
+  // Area lights: every triangle of an emissive material, in triangle order
+  // (Scene::UpdateEmissiveIndexOffset numbers emissive primitives consecutively).
+  std::vector<int> al;
+  std::vector<float> av;
+  for (uint32_t t = 0; t < ntri; ++t) {
+    if (!c->materials[c->mats[t]].emissive) continue;
+    al.push_back((int)t);
+    for (int j = 0; j < 3; ++j) {
+      const float* v = &c->verts[3 * (size_t)c->idx[3 * t + j]];
+      av.push_back(v[0]);
+      av.push_back(v[1]);
+      av.push_back(v[2]);
+      av.push_back(0.f);
+    }
+  }
+  s.area_lights = (const int*)upload(al.data(), al.size() * sizeof(int));
+  s.area_verts = (const float4*)upload(av.data(), av.size() * sizeof(float));
+  s.num_area_lights = (int)al.size();
+  std::vector<float> pl;
+  for (auto& p : c->points) {
+    pl.insert(pl.end(), p.spectrum, p.spectrum + NBINS);
+    pl.insert(pl.end(), p.pos, p.pos + 3);
+  }
+  s.point_lights = (const float*)upload(pl.data(), pl.size() * sizeof(float));
+  s.num_point_lights = (int)c->points.size();
+  // Environmental lights.
+  s.num_env = (int)c->envs.size();
+  for (size_t i = 0; i < c->envs.size(); ++i) {
+    const tt_env_light& e = c->envs[i].desc;
+    DevEnvLight& L = s.env[i];
+    std::memset(&L, 0, sizeof(L));
+    L.kind = e.kind;
+    double dir[3] = {e.dir[0], e.dir[1], e.dir[2]};
+    if (e.kind == TT_ENV_SUN) {
+      // Sun::Sun (light.hxx:253-263).
+      const double cos_open = std::cos(M_PI / 180. * e.scalar2);
+      const double pdf_val = 1. / (2. * M_PI * (1. - cos_open));
+      L.cos_opening = (float)cos_open;
+      L.pdf_val = (float)pdf_val;
+      normalize_d(dir);
+      frame_z_d(dir, L.X, L.Y, L.Z);
+      for (int b = 0; b < NBINS; ++b) L.spectrum[b] = (float)(kSunSpectrum[b] * e.scalar * pdf_val);
+    } else if (e.kind == TT_ENV_DOME) {
+      normalize_d(dir);
+      double down[3] = {-dir[0], -dir[1], -dir[2]};
+      frame_z_d(down, L.X, L.Y, L.Z);
+      std::memcpy(L.spectrum, e.spectrum, sizeof(e.spectrum));
+    } else if (e.kind == TT_ENV_DIRECTIONAL) {
+      normalize_d(dir);
+      for (int k = 0; k < 3; ++k) L.dir[k] = (float)dir[k];
+      std::memcpy(L.spectrum, e.spectrum, sizeof(e.spectrum));
+    } else {
+      // EnvMapLight (light.cxx:88-115): float frame from the (unnormalized) up vector,
+      // row CMFs weighted by sin(theta) * mean(rgb).
+      const float up[3] = {e.dir[0], e.dir[1], e.dir[2]};
+      const float sign = std::copysign(1.0f, up[2]);
+      const float a = -1.0f / (sign + up[2]);
+      const float b = up[0] * up[1] * a;
+      const float X[3] = {1.0f + sign * up[0] * up[0] * a, sign * b, -sign * up[0]};
+      const float Y[3] = {b, sign + up[1] * up[1] * a, -up[1]};
+      for (int k = 0; k < 3; ++k) { L.X[k] = X[k]; L.Y[k] = Y[k]; L.Z[k] = up[k]; }
+      const int w = e.tex_width, h = e.tex_height;
+      const std::vector<float>& tex = c->envs[i].tex;
+      std::vector<float> rows(h), cols((size_t)w * h);
+      for (int y = 0; y < h; ++y) {
+        double row_weight = 0.;
+        for (int x = 0; x < w; ++x) {
+          const float* px = &tex[3 * ((size_t)y * w + x)];
+          const double mean = ((double)px[0] + px[1] + px[2]) / 3.;
+          const float v = ((float)(h - 1 - y) + 0.5f) / h;
+          const float theta = v * (float)M_PI;
+          row_weight += std::sin(theta) * mean;
+          cols[(size_t)y * w + x] = (float)row_weight;
+        }
+        if (!(row_weight > 0.)) return fail(c, TT_ERR_INVALID, "env map row with zero weight");
+        for (int x = 0; x < w; ++x) cols[(size_t)y * w + x] /= (float)row_weight;
+        rows[y] = (float)row_weight;
+      }
+      for (int y = 1; y < h; ++y) rows[y] += rows[y - 1];
+      const float inv = 1.f / rows[h - 1];
+      for (int y = 0; y < h; ++y) rows[y] *= inv;
+      L.w = w;
+      L.h = h;
+      L.tex = (const float*)upload(tex.data(), tex.size() * sizeof(float));
+      L.cmf_rows = (const float*)upload(rows.data(), rows.size() * sizeof(float));
+      L.cmf_cols = (const float*)upload(cols.data(), cols.size() * sizeof(float));
+    }
+  }
+  // Camera (camera.hxx:38-108, 159-175), computed in double.
+  {
+    const tt_camera& cm = c->camera;
+    DevCamera& cam = s.cam;
+    cam.kind = cm.kind;
+    cam.xres = cm.xres;
+    cam.yres = cm.yres;
+    double up[3] = {cm.up[0], cm.up[1], cm.up[2]}, dir[3] = {cm.dir[0], cm.dir[1], cm.dir[2]};
+    normalize_d(up);
+    normalize_d(dir);
+    const double r = up[0] * dir[0] + up[1] * dir[1] + up[2] * dir[2];
+    if (!(std::fabs(r) > 1.0 - 2.220446049250313e-16)) {
+      for (int k = 0; k < 3; ++k) up[k] -= r * dir[k];
+      normalize_d(up);
+    }
+    const double right[3] = {up[1] * dir[2] - up[2] * dir[1], up[2] * dir[0] - up[0] * dir[2],
+                             up[0] * dir[1] - up[1] * dir[0]};
+    for (int k = 0; k < 3; ++k) {
+      cam.pos[k] = cm.pos[k];
+      cam.up[k] = (float)up[k];
+      cam.dir[k] = (float)dir[k];
+      cam.right[k] = (float)right[k];
+    }
+    const double fov = cm.fov_deg * M_PI / 180.;
+    const double aspect = (double)cm.yres / cm.xres;
+    const double a = std::tan(fov * 0.5), b = a * aspect;
+    cam.xmin = (float)-a;
+    cam.ymin = (float)-b;
+    cam.xperpixel = (float)(2. * a / cm.xres);
+    cam.yperpixel = (float)(2. * b / cm.yres);
+    cam.per_pixel_delta = (float)(2. / std::min(cm.xres, cm.yres));
+  }
+  // Light picker (TrivialLightPicker, lightpicker_trivial.cxx:11-31) and scene bounds.
+  const double nl = (double)c->points.size(), ne = c->envs.empty() ? 0. : 1., na = (double)al.size();
+  const double tot = nl + ne + na;
+  const double norm = tot > 0 ? 1. / tot : 0.;
+  s.type_probs[0] = (float)(ne * norm);
+  s.type_probs[1] = (float)(na * norm);
+  s.type_probs[2] = (float)(nl * norm);
+  s.type_probs[3] = 0.f;
+  s.in_class_area = na > 0 ? (float)(1. / na) : 0.f;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (size_t v = 0; v < c->verts.size() / 3; ++v)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], (double)c->verts[3 * v + k]);
+      hi[k] = std::max(hi[k], (double)c->verts[3 * v + k]);
+    }
+  if (c->verts.empty()) for (int k = 0; k < 3; ++k) { lo[k] = hi[k] = 0; }
+  const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                                (hi[2] - lo[2]) * (hi[2] - lo[2]));
+  s.long_distance = (float)(10. * diag);
+  s.max_path_nodes = c->params.max_ray_depth + 1;
+  s.sample_lights = c->params.pt_sample_mode != TT_SAMPLE_BSDF;
+  s.sample_bsdf = c->params.pt_sample_mode != TT_SAMPLE_LIGHTS;
+  if (tot == 0. && s.sample_lights) s.sample_lights = 0;  // no light to sample
+  for (void* p : c->scene_mem.allocs)
+    if (!p) return fail(c, TT_ERR_CUDA, "device allocation failed");
+  // Framebuffers and counters.
+  const size_t n3 = 3 * (size_t)c->npix;
+  c->fb.accum = (float*)c->scene_mem.alloc(n3 * sizeof(float));
+  c->fb.light = (float*)c->scene_mem.alloc(n3 * sizeof(float));
+  c->d_acc = (double*)c->scene_mem.alloc(n3 * sizeof(double));
+  c->d_light = (double*)c->scene_mem.alloc(n3 * sizeof(double));
+  c->d_stats = (unsigned long long*)c->scene_mem.alloc(8 * sizeof(unsigned long long));
+  c->d_err = (unsigned int*)c->scene_mem.alloc(sizeof(unsigned int));
+  if (!c->fb.accum || !c->fb.light || !c->d_acc || !c->d_light || !c->d_stats || !c->d_err)
+    return fail(c, TT_ERR_CUDA, "device allocation failed");
+  TT_CUDA(c, cudaMemset(c->fb.accum, 0, n3 * sizeof(float)));
+  TT_CUDA(c, cudaMemset(c->fb.light, 0, n3 * sizeof(float)));
+  TT_CUDA(c, cudaMemset(c->d_acc, 0, n3 * sizeof(double)));
+  TT_CUDA(c, cudaMemset(c->d_light, 0, n3 * sizeof(double)));
+  TT_CUDA(c, cudaMemset(c->d_stats, 0, 8 * sizeof(unsigned long long)));
+  TT_CUDA(c, cudaMemset(c->d_err, 0, sizeof(unsigned int)));
+  int sms = 0;
+  TT_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  c->grid = sms * kernel_blocks_per_sm();
+  c->rounds = c->params.max_ray_depth;
+  TT_CUDA(c, cudaDeviceSynchronize());
+  c->uploaded = true;
+  return TT_OK;
+}
+
+}  // extern "C"
+
+static tt_status ensure_path_state(tt_ctx* c, int cap) {
+  if (c->ps.cap >= cap) return TT_OK;
+  cudaStreamSynchronize(c->stream);
+  c->path_mem.free_all();
+  PathState& p = c->ps;
+  p = PathState{};
+  DeviceBuffers& m = c->path_mem;
+  const size_t n = (size_t)cap;
+  p.ray_o = (float4*)m.alloc(n * sizeof(float4));
+  p.ray_d = (float4*)m.alloc(n * sizeof(float4));
+  p.hit = (float4*)m.alloc(n * sizeof(float4));
+  p.beta = (float4*)m.alloc(n * sizeof(float4));
+  p.accum = (float4*)m.alloc(n * sizeof(float4));
+  p.rng_state = (unsigned long long*)m.alloc(n * 8);
+  p.rng_inc = (unsigned long long*)m.alloc(n * 8);
+  p.meta = (uint4*)m.alloc(n * sizeof(uint4));
+  p.sh_o = (float4*)m.alloc(n * sizeof(float4));
+  p.sh_d = (float4*)m.alloc(n * sizeof(float4));
+  p.sh_c = (float4*)m.alloc(n * sizeof(float4));
+  p.ext_q[0] = (int*)m.alloc(n * sizeof(int));
+  p.ext_q[1] = (int*)m.alloc(n * sizeof(int));
+  p.sh_q = (int*)m.alloc(n * sizeof(int));
+  p.done_q = (int*)m.alloc(n * sizeof(int));
+  p.counters = (int*)m.alloc(3 * (size_t)(c->rounds + 3) * sizeof(int));
+  p.err = c->d_err;
+  for (void* a : m.allocs)
+    if (!a) {
+      m.free_all();
+      p = PathState{};
+      return fail(c, TT_ERR_CUDA, "path state allocation failed (capacity " + std::to_string(cap) + ")");
+    }
+  p.cap = cap;
+  return TT_OK;
+}
+
+static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb, int32_t pe) {
+  if (!c) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  if (spp <= 0) return fail(c, TT_ERR_INVALID, "spp must be positive");
+  if (pb < 0 || pe > c->npix || pb >= pe) return fail(c, TT_ERR_INVALID, "bad pixel range");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  const int npix_range = pe - pb;
+  const long long total = (long long)spp * npix_range;
+  const int wave_limit = c->params.wave_paths > 0 ? c->params.wave_paths : kDefaultWave;
+  const int cap = (int)std::min<long long>(total, wave_limit);
+  tt_status st = ensure_path_state(c, cap);
+  if (st != TT_OK) return st;
+  const bool counting = c->profiling >= 2;
+  const bool timing = c->profiling >= 1;
+  std::vector<cudaEvent_t> ev;   // begin/end pairs of timed launches
+  std::vector<int> ev_kind;      // 0 closest hit, 1 shadow
+  auto timed = [&](int kind, auto&& launch) {
+    if (!timing) { launch(); return; }
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, c->stream);
+    launch();
+    cudaEventRecord(b, c->stream);
+    ev.push_back(a);
+    ev.push_back(b);
+    ev_kind.push_back(kind);
+  };
+  cudaEvent_t pass_begin, pass_end, wave_ev[2];
+  TT_CUDA(c, cudaEventCreate(&pass_begin));
+  TT_CUDA(c, cudaEventCreate(&pass_end));
+  TT_CUDA(c, cudaEventCreateWithFlags(&wave_ev[0], cudaEventDisableTiming));
+  TT_CUDA(c, cudaEventCreateWithFlags(&wave_ev[1], cudaEventDisableTiming));
+  TT_CUDA(c, cudaEventRecord(pass_begin, c->stream));
+  const int grid = c->grid;
+  const int rounds = c->rounds;
+  uint64_t launches = 0;
+  bool stopped = false;
+  int wave_index = 0;
+  for (long long ws = 0; ws < total; ws += cap, ++wave_index) {
+    if (c->stop.load()) { stopped = true; break; }
+    if (wave_index >= 2) cudaEventSynchronize(wave_ev[wave_index & 1]);
+    WaveArgs w;
+    w.wave_start = ws;
+    w.wave_paths = (int)std::min<long long>(cap, total - ws);
+    w.pixel_begin = pb;
+    w.npix_range = npix_range;
+    w.npix_total = c->npix;
+    w.sample_offset = c->next_sample;
+    w.seed = seed;
+    cudaMemsetAsync(c->ps.counters, 0, 3 * (size_t)(rounds + 3) * sizeof(int), c->stream);
+    launch_generate(c->dev, c->ps, c->fb, w, grid, c->stream);
+    launches++;
+    for (int b = 0; b < rounds; ++b) {
+      timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, b, counting, c->d_stats + 2, grid, c->stream); });
+      launch_flush(c->ps, c->fb, b, grid, c->stream);
+      timed(0, [&] { launch_extend(c->dev, c->ps, b, counting, c->d_stats, grid, c->stream); });
+      launch_shade(c->dev, c->ps, b, grid, c->stream);
+      launches += 4;
+    }
+    timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, rounds, counting, c->d_stats + 2, grid, c->stream); });
+    launch_flush(c->ps, c->fb, rounds, grid, c->stream);
+    k_tally<<<1, 32, 0, c->stream>>>(c->ps.counters, rounds, c->d_stats);
+    launches += 3;
+    cudaEventRecord(wave_ev[wave_index & 1], c->stream);
+  }
+  launch_accumulate(c->fb, c->d_acc, c->d_light, 3 * c->npix, c->stream);
+  launches++;
+  TT_CUDA(c, cudaEventRecord(pass_end, c->stream));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  TT_CUDA(c, cudaGetLastError());
+  float pass_ms = 0.f;
+  cudaEventElapsedTime(&pass_ms, pass_begin, pass_end);
+  c->stats.pass_ms += pass_ms;
+  for (size_t k = 0; k < ev_kind.size(); ++k) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]);
+    if (ev_kind[k] == 0) { c->stats.extend_ms += ms; c->stats.extend_launches++; }
+    else { c->stats.shadow_ms += ms; c->stats.shadow_launches++; }
+    cudaEventDestroy(ev[2 * k]);
+    cudaEventDestroy(ev[2 * k + 1]);
+  }
+  if (!timing) {
+    c->stats.extend_launches += (uint64_t)rounds * wave_index;
+    c->stats.shadow_launches += (uint64_t)(rounds + 1) * wave_index;
+  }
+  cudaEventDestroy(pass_begin);
+  cudaEventDestroy(pass_end);
+  cudaEventDestroy(wave_ev[0]);
+  cudaEventDestroy(wave_ev[1]);
+  c->stats.kernel_launches += launches;
+  c->stats.paths += (uint64_t)std::min<long long>(total, (long long)wave_index * cap);
+  // Bookkeeping as in SimplePixelByPixelRenderingAlgo: the sample count of the pass is
+  // added whether or not the pass completed.
+  for (int px = pb; px < pe; ++px) c->spp_count[px] += (uint64_t)spp;
+  c->splat_count += (uint64_t)spp * (uint64_t)npix_range;
+  c->next_sample += (uint64_t)spp;
+  unsigned int errw = 0;
+  TT_CUDA(c, cudaMemcpy(&errw, c->d_err, sizeof(errw), cudaMemcpyDeviceToHost));
+  if (errw) {
+    c->stats.error_flags |= errw;
+    return fail(c, TT_ERR_LOOP_CAP, "a device loop hit its cap (error word " + std::to_string(errw) + ")");
+  }
+  if (stopped) return fail(c, TT_ERR_INTERRUPTED, "stopped by tt_request_stop");
+  return TT_OK;
+}
+
+extern "C" {
+
+tt_status tt_render_pass(tt_ctx* c, int32_t spp, uint64_t seed) {
+  if (!c) return TT_ERR_INVALID;
+  return render_range(c, spp, seed, 0, c->npix);
+}
+
+tt_status tt_render_pass_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb, int32_t pe) {
+  return render_range(c, spp, seed, pb, pe);
+}
+
+tt_status tt_request_interrupt(tt_ctx* c) {
+  if (!c) return TT_ERR_INVALID;
+  c->interrupt.store(1);
+  return TT_OK;
+}
+
+tt_status tt_request_stop(tt_ctx* c) {
+  if (!c) return TT_ERR_INVALID;
+  c->stop.store(1);
+  return TT_OK;
+}
+
+int32_t tt_poll_interrupt(tt_ctx* c) { return c ? c->interrupt.exchange(0) : 0; }
+int32_t tt_stop_requested(tt_ctx* c) { return c ? c->stop.load() : 0; }
+
+tt_status tt_read_accumulators(tt_ctx* c, double* accum, double* light, uint64_t* spp, uint64_t* splat) {
+  if (!c) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  const size_t n3 = 3 * (size_t)c->npix;
+  if (accum) TT_CUDA(c, cudaMemcpy(accum, c->d_acc, n3 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (light) TT_CUDA(c, cudaMemcpy(light, c->d_light, n3 * sizeof(double), cudaMemcpyDeviceToHost));
+  if (spp) std::memcpy(spp, c->spp_count.data(), c->npix * sizeof(uint64_t));
+  if (splat) *splat = c->splat_count;
+  return TT_OK;
+}
+
+tt_status tt_read_framebuffer(tt_ctx* c, float* rgb, uint64_t* counts) {
+  if (!c || !rgb) return TT_ERR_INVALID;
+  std::vector<double> acc(3 * (size_t)c->npix), light(3 * (size_t)c->npix);
+  tt_status st = tt_read_accumulators(c, acc.data(), light.data(), nullptr, nullptr);
+  if (st != TT_OK) return st;
+  const double sw = c->splat_count > 0 ? (double)c->npix / (double)c->splat_count : 0.;
+  for (int p = 0; p < c->npix; ++p) {
+    const double n = (double)c->spp_count[p];
+    for (int k = 0; k < 3; ++k) {
+      const double avg = n > 0 ? acc[3 * (size_t)p + k] / n : 0.;
+      rgb[3 * (size_t)p + k] = (float)(avg + sw * light[3 * (size_t)p + k]);
+    }
+  }
+  if (counts) std::memcpy(counts, c->spp_count.data(), c->npix * sizeof(uint64_t));
+  return TT_OK;
+}
+
+tt_status tt_generate_image(tt_ctx* c, int32_t linear_output, uint8_t* out) {
+  if (!c || !out) return TT_ERR_INVALID;
+  std::vector<float> rgb(3 * (size_t)c->npix);
+  tt_status st = tt_read_framebuffer(c, rgb.data(), nullptr);
+  if (st != TT_OK) return st;
+  const int xres = c->camera.xres, yres = c->camera.yres;
+  for (int y = 0; y < yres; ++y)
+    for (int x = 0; x < xres; ++x) {
+      const size_t src = 3 * ((size_t)y * xres + x);
+      const size_t dst = 3 * ((size_t)(yres - 1 - y) * xres + x);
+      for (int k = 0; k < 3; ++k) {
+        double v = std::min(1.0, std::max(0.0, (double)rgb[src + k]));
+        if (!linear_output) v = v <= 0.0031308 ? 12.92 * v : 1.055 * std::pow(v, 1.0 / 2.4) - 0.055;
+        out[dst + k] = (uint8_t)(v * 255.999);
+      }
+    }
+  return TT_OK;
+}
+
+tt_status tt_clear_framebuffer(tt_ctx* c) {
+  if (!c) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  const size_t n3 = 3 * (size_t)c->npix;
+  TT_CUDA(c, cudaMemset(c->d_acc, 0, n3 * sizeof(double)));
+  TT_CUDA(c, cudaMemset(c->d_light, 0, n3 * sizeof(double)));
+  std::fill(c->spp_count.begin(), c->spp_count.end(), 0);
+  c->splat_count = 0;
+  c->next_sample = 0;
+  return TT_OK;
+}
+
+static tt_status batch_prep(tt_ctx* c, const void* rays, int32_t n) {
+  if (!c || n < 0 || (n > 0 && !rays)) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  return TT_OK;
+}
+
+tt_status tt_intersect_batch(tt_ctx* c, const float* rays, int32_t n, int32_t* prim, float* t, float* u, float* v) {
+  tt_status st = batch_prep(c, rays, n);
+  if (st != TT_OK || n == 0) return st;
+  float *dr = nullptr, *dt = nullptr, *du = nullptr, *dv = nullptr;
+  int* dp = nullptr;
+  TT_CUDA(c, cudaMalloc(&dr, 8 * (size_t)n * sizeof(float)));
+  cudaMalloc(&dt, n * sizeof(float));
+  cudaMalloc(&du, n * sizeof(float));
+  cudaMalloc(&dv, n * sizeof(float));
+  cudaMalloc(&dp, n * sizeof(int));
+  cudaMemcpy(dr, rays, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  launch_intersect_rays(c->dev, dr, n, dp, dt, du, dv, c->d_err, c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaMemcpy(prim, dp, n * sizeof(int), cudaMemcpyDeviceToHost);
+  cudaMemcpy(t, dt, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (u) cudaMemcpy(u, du, n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (v) cudaMemcpy(v, dv, n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dr); cudaFree(dt); cudaFree(du); cudaFree(dv); cudaFree(dp);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+tt_status tt_occluded_batch(tt_ctx* c, const float* rays, int32_t n, uint8_t* occ) {
+  tt_status st = batch_prep(c, rays, n);
+  if (st != TT_OK || n == 0) return st;
+  float* dr = nullptr;
+  unsigned char* docc = nullptr;
+  TT_CUDA(c, cudaMalloc(&dr, 8 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&docc, n));
+  cudaMemcpy(dr, rays, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  launch_occluded_rays(c->dev, dr, n, docc, c->d_err, c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaMemcpy(occ, docc, n, cudaMemcpyDeviceToHost);
+  cudaFree(dr);
+  cudaFree(docc);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+tt_status tt_intersect_batch_device(tt_ctx* c, const float* d_rays, int32_t n, int32_t* d_prim, float* d_t,
+                                    float* d_u, float* d_v, void* stream) {
+  tt_status st = batch_prep(c, d_rays, n);
+  if (st != TT_OK || n == 0) return st;
+  if (!d_prim || !d_t || !d_u || !d_v) return fail(c, TT_ERR_INVALID, "output pointer is NULL");
+  launch_intersect_rays(c->dev, d_rays, n, d_prim, d_t, d_u, d_v, c->d_err, (cudaStream_t)stream);
+  TT_CUDA(c, cudaGetLastError());
+  return TT_OK;
+}
+
+tt_status tt_count_traversal(tt_ctx* c, const float* rays, int32_t n) {
+  tt_status st = batch_prep(c, rays, n);
+  if (st != TT_OK || n == 0) return st;
+  float* dr = nullptr;
+  TT_CUDA(c, cudaMalloc(&dr, 8 * (size_t)n * sizeof(float)));
+  cudaMemcpy(dr, rays, 8 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  launch_count_rays(c->dev, dr, n, c->d_stats, c->d_err, c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaFree(dr);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  c->stats.counted_rays += (uint64_t)n;
+  return TT_OK;
+}
+
+static tt_status bsdf_prep(tt_ctx* c, int32_t material, const float* wi, const int32_t* li, int32_t n) {
+  if (!c || !wi || !li || n < 0) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  if (material < 0 || material >= (int)c->materials.size()) return fail(c, TT_ERR_INVALID, "bad material index");
+  for (int k = 0; k < 3; ++k)
+    if (li[k] < 0 || li[k] >= NBINS) return fail(c, TT_ERR_INVALID, "bad wavelength bin");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  return TT_OK;
+}
+
+tt_status tt_sample_bsdf_batch(tt_ctx* c, int32_t material, const float* wi, const int32_t* li, int32_t n,
+                               uint64_t seed, float* out_dir, float* out_val, float* out_pdf) {
+  tt_status st = bsdf_prep(c, material, wi, li, n);
+  if (st != TT_OK || n == 0) return st;
+  float *dd = nullptr, *dv = nullptr, *dp = nullptr;
+  TT_CUDA(c, cudaMalloc(&dd, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dv, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dp, (size_t)n * sizeof(float)));
+  launch_sample_bsdf(c->dev, material, make_float3(wi[0], wi[1], wi[2]), make_int3(li[0], li[1], li[2]), n, seed, dd,
+                     dv, dp, c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaMemcpy(out_dir, dd, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_val, dv, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_pdf, dp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dd); cudaFree(dv); cudaFree(dp);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+tt_status tt_eval_bsdf_batch(tt_ctx* c, int32_t material, const float* wi, const int32_t* li, const float* dirs,
+                             int32_t n, float* out_val, float* out_pdf) {
+  tt_status st = bsdf_prep(c, material, wi, li, n);
+  if (st != TT_OK || n == 0) return st;
+  if (!dirs) return TT_ERR_INVALID;
+  float *di = nullptr, *dv = nullptr, *dp = nullptr;
+  TT_CUDA(c, cudaMalloc(&di, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dv, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dp, (size_t)n * sizeof(float)));
+  cudaMemcpy(di, dirs, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  launch_eval_bsdf(c->dev, material, make_float3(wi[0], wi[1], wi[2]), make_int3(li[0], li[1], li[2]), di, n, dv, dp,
+                   c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaMemcpy(out_val, dv, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_pdf, dp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(di); cudaFree(dv); cudaFree(dp);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+tt_status tt_read_accumulators_device(tt_ctx* c, double* d_accum, double* d_light, void* stream) {
+  if (!c || !d_accum || !d_light) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  const size_t bytes = 3 * (size_t)c->npix * sizeof(double);
+  // Order after the last pass on the context's stream, then copy on the caller's stream.
+  cudaEvent_t ev;
+  TT_CUDA(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaEventRecord(ev, c->stream);
+  cudaStreamWaitEvent((cudaStream_t)stream, ev, 0);
+  cudaEventDestroy(ev);
+  TT_CUDA(c, cudaMemcpyAsync(d_accum, c->d_acc, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  TT_CUDA(c, cudaMemcpyAsync(d_light, c->d_light, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return TT_OK;
+}
+
+tt_status tt_set_profiling(tt_ctx* c, int32_t on) {
+  if (!c) return TT_ERR_INVALID;
+  c->profiling = on;
+  return TT_OK;
+}
+
+tt_status tt_get_stats(tt_ctx* c, tt_stats* out) {
+  if (!c || !out) return TT_ERR_INVALID;
+  *out = c->stats;
+  if (c->uploaded) {
+    TT_CUDA(c, cudaSetDevice(c->device));
+    unsigned long long s[8];
+    TT_CUDA(c, cudaMemcpy(s, c->d_stats, sizeof(s), cudaMemcpyDeviceToHost));
+    out->node_visits = s[0];
+    out->tri_tests = s[1];
+    out->shadow_node_visits = s[2];
+    out->shadow_tri_tests = s[3];
+    out->extension_rays = s[4];
+    out->shadow_rays = s[5];
+    unsigned int errw = 0;
+    TT_CUDA(c, cudaMemcpy(&errw, c->d_err, sizeof(errw), cudaMemcpyDeviceToHost));
+    out->error_flags |= errw;
+  }
+  out->bvh_nodes = c->bvh_nodes;
+  out->bvh_node_bytes = 64;
+  out->tri_bytes = 48;
+  out->bvh_depth = c->bvh_depth;
+  return TT_OK;
+}
+
+tt_status tt_reset_stats(tt_ctx* c) {
+  if (!c) return TT_ERR_INVALID;
+  c->stats = tt_stats{};
+  if (c->uploaded) {
+    TT_CUDA(c, cudaSetDevice(c->device));
+    TT_CUDA(c, cudaMemset(c->d_stats, 0, 8 * sizeof(unsigned long long)));
+  }
+  return TT_OK;
+}
+
+tt_status tt_last_error(tt_ctx* c, char* buf, int32_t n) {
+  if (!buf || n <= 0) return TT_ERR_INVALID;
+  std::string msg;
+  if (c) msg = c->err;
+  else {
+    std::lock_guard<std::mutex> g(g_err_mutex);
+    msg = g_create_error;
+  }
+  std::snprintf(buf, (size_t)n, "%s", msg.c_str());
+  return TT_OK;
+}
+
+void tt_destroy(tt_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->path_mem.free_all();
+  c->scene_mem.free_all();
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // extern "C"

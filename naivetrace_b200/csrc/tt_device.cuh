@@ -1,0 +1,643 @@
+// Device-side building blocks of the path tracer: vector math, the PCG32 stream, the
+// sampling warps, spectral conversions, shaders, lights and cameras.  Single precision;
+// each function names the reference code whose semantics it reproduces.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+#include <stdint.h>
+
+#include "tt_internal.h"
+
+namespace tt {
+
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kEps = 2.220446049250313e-16f;   // double epsilon, as added in denominators
+constexpr float kEpsF = 1.1920928955078125e-07f; // float epsilon
+constexpr float kLargeNumber = 3.4028234663852886e+38f / 16.f;
+
+// Spectrum -> RGB matrix and Smits basis, uploaded by upload_constant_tables().  This
+// header is compiled into exactly one translation unit (tt_kernels.cu), which owns them.
+__constant__ float c_spec_to_rgb[3][NBINS];
+__constant__ float c_smits[7][NBINS];
+
+// ----------------------------------------------------------------------------------------
+__device__ __forceinline__ float3 f3(float a, float b, float c) { return make_float3(a, b, c); }
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator-(float3 a) { return f3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ float3 operator*(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 mul(float3 a, float3 b) { return f3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return f3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float len3(float3 a) { return sqrtf(dot3(a, a)); }
+__device__ __forceinline__ float3 normalize3(float3 a) { return a * (1.f / len3(a)); }
+__device__ __forceinline__ float3 abs3(float3 a) { return f3(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+__device__ __forceinline__ float3 xyz(float4 a) { return f3(a.x, a.y, a.z); }
+__device__ __forceinline__ float comp(float3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+__device__ __forceinline__ bool is_zero(float3 a) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
+__device__ __forceinline__ float max3(float3 a) { return fmaxf(a.x, fmaxf(a.y, a.z)); }
+
+// OrthogonalSystemZAligned (vec3f.hxx:240-258): Duff et al. 2017, listing 3.
+struct Frame {
+  float3 X, Y, Z;
+  __device__ __forceinline__ float3 to_world(float3 v) const { return X * v.x + Y * v.y + Z * v.z; }
+  __device__ __forceinline__ float3 to_local(float3 w) const { return f3(dot3(X, w), dot3(Y, w), dot3(Z, w)); }
+};
+__device__ __forceinline__ Frame frame_z(float3 z) {
+  Frame f;
+  f.Z = z;
+  const float sign = copysignf(1.f, z.z);
+  const float a = -1.f / (sign + z.z);
+  const float b = z.x * z.y * a;
+  f.X = f3(1.f + sign * z.x * z.x * a, sign * b, -sign * z.x);
+  f.Y = f3(b, sign + z.y * z.y * a, -z.y);
+  return f;
+}
+
+// ----------------------------------------------------------------------------------------
+// PCG32 (O'Neill 2014) with the pcg32 interface used by RandGen (sampler.cxx:366-393).
+struct Rng {
+  unsigned long long state, inc;
+  __device__ __forceinline__ uint32_t next() {
+    unsigned long long old = state;
+    state = old * 6364136223846793005ULL + inc;
+    uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xorshifted >> rot) | (xorshifted << ((~rot + 1u) & 31));
+  }
+  __device__ __forceinline__ void seed(unsigned long long initstate, unsigned long long initseq) {
+    state = 0ull;
+    inc = (initseq << 1u) | 1u;
+    next();
+    state += initstate;
+    next();
+  }
+  // 23 random mantissa bits (pcg32::nextFloat): the single-precision twin of nextDouble.
+  __device__ __forceinline__ float uniform() { return __uint_as_float((next() >> 9) | 0x3f800000u) - 1.0f; }
+  __device__ __forceinline__ void square(float r[2]) { r[0] = uniform(); r[1] = uniform(); }
+  // RandGen::UniformInt via pcg32::nextUInt(bound); the rejection loop is bounded.
+  __device__ __forceinline__ int uniform_int(int a, int b_inclusive) {
+    const uint32_t bound = (uint32_t)(b_inclusive + 1 - a);
+    const uint32_t threshold = (~bound + 1u) % bound;
+    uint32_t r = next();
+    for (int k = 0; k < 64 && r < threshold; ++k) r = next();
+    return a + (int)(r % bound);
+  }
+};
+
+// ----------------------------------------------------------------------------------------
+// Warps, sampler.cxx:6-124.
+__device__ __forceinline__ float3 to_uniform_sphere(const float r[2]) {
+  float z = 1.f - 2.f * r[1];
+  float s = sqrtf(r[1] * (1.f - r[1]));
+  float sn, cs;
+  sincosf(2.f * kPi * r[0], &sn, &cs);
+  return f3(2.f * cs * s, 2.f * sn * s, z);
+}
+__device__ __forceinline__ float3 to_uniform_hemisphere(const float r[2]) {
+  float3 v = to_uniform_sphere(r);
+  v.z = v.z >= 0.f ? v.z : -v.z;
+  return v;
+}
+__device__ __forceinline__ float3 to_sphere_section(float cos_open, const float r[2]) {
+  float z = 1.f - r[1] * (1.f - cos_open);
+  float s = sqrtf(fmaxf(0.f, 1.f - z * z));
+  float sn, cs;
+  sincosf(2.f * kPi * r[0], &sn, &cs);
+  return f3(cs * s, sn * s, z);
+}
+__device__ __forceinline__ float3 to_sphere_section(const float r[2], float phi0, float z0, float phi1, float z1) {
+  const float z = z0 + r[1] * (z1 - z0);
+  float s = sqrtf(1.f - z * z);
+  s = isnan(s) ? 0.f : s;
+  float sn, cs;
+  sincosf(phi0 + (phi1 - phi0) * r[0], &sn, &cs);
+  return f3(cs * s, sn * s, z);
+}
+__device__ __forceinline__ float3 to_cos_hemisphere(const float r[2]) {
+  float rho = sqrtf(1.f - r[0]);
+  float z = sqrtf(r[0]);
+  float sn, cs;
+  sincosf(2.f * kPi * r[1], &sn, &cs);
+  return f3(cs * rho, sn * rho, z);
+}
+__device__ __forceinline__ float3 to_triangle_barycentric(const float r[2]) {
+  float s = sqrtf(r[0]);
+  return f3(1.f - s, (1.f - r[1]) * s, r[1] * s);
+}
+__device__ __forceinline__ float power_heuristic(float p, float o) {
+  float pp = p * p;
+  return pp / (pp + o * o + kEps);
+}
+__device__ __forceinline__ int tower_sampling4(const float* probs, float r) {
+  int n = 3;
+  while (r >= probs[n] && n > 0) { r -= probs[n]; --n; }
+  return n;
+}
+__device__ __forceinline__ int tower_bisection(const float* cmf, int size, float r) {
+  int upper;
+  if (r < cmf[0]) upper = 0;
+  else if (r >= cmf[size - 1]) upper = size;
+  else {
+    int first = 0, last = size - 1;
+    while (last > first + 1) {
+      int center = (first + last) / 2;
+      if (r < cmf[center]) last = center; else first = center;
+    }
+    upper = last;
+  }
+  return upper >= size ? size - 1 : upper;
+}
+__device__ __forceinline__ float prob_from_cmf(const float* cmf, int idx) {
+  return cmf[idx] - (idx > 0 ? cmf[idx - 1] : 0.f);
+}
+
+// ----------------------------------------------------------------------------------------
+// Spectral selections (spectral.cxx:81-140, shader_util.hxx:47-92).
+struct Lambda {
+  int i0, i1, i2;
+};
+__device__ __forceinline__ unsigned pack_lambda(Lambda l) { return (unsigned)l.i0 | ((unsigned)l.i1 << 8) | ((unsigned)l.i2 << 16); }
+__device__ __forceinline__ Lambda unpack_lambda(unsigned p) {
+  return Lambda{(int)(p & 255u), (int)((p >> 8) & 255u), (int)((p >> 16) & 255u)};
+}
+__device__ __forceinline__ float3 take(const float* spec, Lambda l) { return f3(spec[l.i0], spec[l.i1], spec[l.i2]); }
+__device__ __forceinline__ float3 selection_to_rgb(float3 v, Lambda l) {
+  float3 rgb;
+  rgb.x = v.x * c_spec_to_rgb[0][l.i0] + v.y * c_spec_to_rgb[0][l.i1] + v.z * c_spec_to_rgb[0][l.i2];
+  rgb.y = v.x * c_spec_to_rgb[1][l.i0] + v.y * c_spec_to_rgb[1][l.i1] + v.z * c_spec_to_rgb[1][l.i2];
+  rgb.z = v.x * c_spec_to_rgb[2][l.i0] + v.y * c_spec_to_rgb[2][l.i1] + v.z * c_spec_to_rgb[2][l.i2];
+  return rgb;
+}
+__device__ __forceinline__ float3 lincomb_sel(float a, int ia, float b, int ib, float c, int ic, Lambda l) {
+  return f3(a * c_smits[ia][l.i0] + b * c_smits[ib][l.i0] + c * c_smits[ic][l.i0],
+            a * c_smits[ia][l.i1] + b * c_smits[ib][l.i1] + c * c_smits[ic][l.i1],
+            a * c_smits[ia][l.i2] + b * c_smits[ib][l.i2] + c * c_smits[ic][l.i2]);
+}
+// RGBToSpectralSelection (spectral.cxx:142-174); basis order white, red, green, blue,
+// yellow, cyan, magenta.
+__device__ __forceinline__ float3 rgb_to_selection(float r, float g, float b, Lambda l) {
+  if (r <= g && r <= b) {
+    if (g <= b) return lincomb_sel(r, 0, g - r, 5, b - g, 3, l);
+    return lincomb_sel(r, 0, b - r, 5, g - b, 2, l);
+  } else if (g <= r && g <= b) {
+    if (r <= b) return lincomb_sel(g, 0, r - g, 6, b - r, 3, l);
+    return lincomb_sel(g, 0, b - g, 6, r - b, 1, l);
+  } else {
+    if (r <= g) return lincomb_sel(b, 0, r - b, 4, g - r, 2, l);
+    return lincomb_sel(b, 0, g - b, 4, r - g, 1, l);
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Physics helpers, shader_physics.hxx:10-148, normaldistributionfunction.hxx:8-127.
+__device__ __forceinline__ float3 reflected(float3 wi, float3 n) { return 2.f * dot3(wi, n) * n - wi; }
+__device__ __forceinline__ bool refracted(float3 wi, float3 m, float eta, float3* out) {
+  const float c = dot3(m, wi);
+  const float t2 = 1.f - eta * eta * (1.f - c * c);
+  if (t2 < 0.f) return false;
+  const float s = c >= 0.f ? 1.f : -1.f;
+  *out = (eta * c - s * sqrtf(t2)) * m - eta * wi;
+  return true;
+}
+__device__ __forceinline__ float fresnel_reflectivity(float cs_i, float cs_t, float eta) {
+  float rs = (eta * cs_i - cs_t) / (eta * cs_i + cs_t);
+  float rp = (eta * cs_t - cs_i) / (eta * cs_t + cs_i);
+  return 0.5f * (rs * rs + rp * rp);
+}
+__device__ __forceinline__ float beckmann_d(float alpha, float cs) {
+  if (cs <= 0.f) return 0.f;
+  const float t1 = (cs * cs - 1.f) / (cs * cs * alpha * alpha);
+  const float t2 = alpha * alpha * cs * cs * cs * cs * kPi;
+  return expf(t1) / t2;
+}
+__device__ __forceinline__ float3 beckmann_sample_wh(float alpha, const float r[2]) {
+  const float t1 = -alpha * alpha * logf(r[0]);
+  const float t = 1.f / (t1 + 1.f);
+  const float z = sqrtf(t);
+  const float rho = sqrtf(1.f - t);
+  float sn, cs;
+  sincosf(2.f * kPi * r[1], &sn, &cs);
+  return f3(cs * rho, sn * rho, z);
+}
+__device__ __forceinline__ float g1_vcavity(float cos_v_m, float cos_v_n, float cos_n_m) {
+  if (cos_v_m * cos_v_n < 0.f) return 0.f;
+  return fminf(1.f, 2.f * fabsf(cos_n_m * cos_v_n) / (fabsf(cos_v_m) + kEps));
+}
+__device__ __forceinline__ float g2_vcavity(float wh_in, float wh_out, float ns_in, float ns_out, float ns_wh) {
+  return fminf(g1_vcavity(wh_in, ns_in, ns_wh), g1_vcavity(wh_out, ns_out, ns_wh));
+}
+__device__ __forceinline__ float clamp_dot(float3 a, float3 b) { return fmaxf(0.f, dot3(a, b)); }
+constexpr float kWiBelowHorizonFix = 1.e-6f;
+__device__ __forceinline__ float vndf_pdf(float d, float3 wh, float3 wi) {
+  float3 whp = f3(-wh.x, -wh.y, wh.z);
+  const float a = clamp_dot(wi, whp), b = clamp_dot(wh, wi);
+  return d * fabsf(wh.z) * ((2.f * b + kWiBelowHorizonFix) / (b + a + kWiBelowHorizonFix));
+}
+
+// ----------------------------------------------------------------------------------------
+// Surface interaction (scene.hxx:77-95).
+struct Surf {
+  int prim;
+  int material;
+  float3 pos;
+  float3 ng;        // geometry_normal (winding)
+  float3 ns_raw;    // smooth_normal
+  float3 n;         // oriented geometry normal
+  float3 ns;        // oriented shading normal
+  float3 bounds;    // pos_bounds
+};
+
+// util::Gamma<float>(7) (util.hxx:124-127) with the full float epsilon.
+__device__ __forceinline__ float gamma7() { return (7.f * kEpsF) / (1.f - 7.f * kEpsF); }
+
+// AntiSelfIntersectionOffset (scene.cxx:256-261).
+__device__ __forceinline__ float3 offset_at(const Surf& s, float3 exitant) {
+  const float delta = dot3(s.bounds, abs3(s.ng));
+  return (delta * (dot3(exitant, s.ng) > 0.f ? 1.f : -1.f)) * s.ng;
+}
+
+// Builds the interaction for barycentrics (w0, w1, w2) of the triangle at leaf slot `slot`.
+// FirstIntersectionTriangle (embreeaccelerator.cxx:216-244) passes (u, v, 1-u-v) as the
+// HitId barycentrics to FillPosBoundsTriangle while interpolating with (1-u-v, u, v);
+// `bw` carries the weights used for the bound.
+__device__ __forceinline__ Surf make_surface(const DevScene& sc, int slot, float w0, float w1, float w2, float3 bw) {
+  const float4 a = __ldg(&sc.tris[3 * slot]);
+  const float4 b = __ldg(&sc.tris[3 * slot + 1]);
+  const float4 c = __ldg(&sc.tris[3 * slot + 2]);
+  Surf s;
+  s.prim = __float_as_int(a.w);
+  s.material = __float_as_int(b.w);
+  const float3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(c);
+  s.pos = p0 * w0 + p1 * w1 + p2 * w2;
+  s.ng = normalize3(cross3(p1 - p0, p2 - p0));
+  if (sc.normals) {
+    const uint4 ti = __ldg(&sc.tri_idx[s.prim]);
+    const float* N = sc.normals;
+    float3 na = f3(N[3 * ti.x], N[3 * ti.x + 1], N[3 * ti.x + 2]);
+    float3 nb = f3(N[3 * ti.y], N[3 * ti.y + 1], N[3 * ti.y + 2]);
+    float3 nc = f3(N[3 * ti.z], N[3 * ti.z + 1], N[3 * ti.z + 2]);
+    s.ns_raw = normalize3(na * w0 + nb * w1 + nc * w2);
+  } else {
+    s.ns_raw = s.ng;
+  }
+  s.bounds = (abs3(p0 * bw.x) + abs3(p1 * bw.y) + abs3(p2 * bw.z)) * gamma7();
+  s.n = s.ng;
+  s.ns = s.ns_raw;
+  return s;
+}
+
+__device__ __forceinline__ void orient(Surf& s, float3 incident) {
+  const float sign = -copysignf(1.f, dot3(incident, s.ng));
+  s.n = sign * s.ng;
+  s.ns = sign * s.ns_raw;
+}
+
+// ----------------------------------------------------------------------------------------
+// Shaders (shader.cxx).
+struct ScatterSample {
+  float3 dir;
+  float3 value;
+  float pdf;
+  bool delta;
+};
+
+// EvaluateBSDF of DiffuseShader (shader.cxx:280-297), the delta shaders, and
+// MicrofacetShader (shader.cxx:676-689 with MicrofacetShaderWrapper::Evaluate :74-113).
+__device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, const Surf& s, float3 wo, Lambda l,
+                                            float* pdf) {
+  if (m.shader == TT_SHADER_DIFFUSE) {
+    float3 ret = f3(0.f, 0.f, 0.f);
+    if (dot3(s.n, wo) > 0.f) ret = take(m.reflectance, l) * (1.f / kPi);
+    if (pdf) *pdf = fmaxf(0.f, dot3(s.ns, wo)) / kPi;
+    return ret;
+  }
+  if (m.shader == TT_SHADER_MICROFACET) {
+    const Frame fr = frame_z(s.ns);
+    const float3 ng = fr.to_local(s.n);
+    const float3 lwi = fr.to_local(wi), lwo = fr.to_local(wo);
+    const float3 wh = normalize3(lwi + lwo);
+    const float ns_out = lwo.z, ns_in = lwi.z, ns_wh = wh.z;
+    const float wh_out = dot3(lwo, wh), wh_in = dot3(lwi, wh);
+    const float d = beckmann_d(m.alpha, fabsf(ns_wh));
+    const float g = g2_vcavity(wh_in, wh_out, ns_in, ns_out, ns_wh);
+    if (pdf) {
+      const float3 whf = wh.z < 0.f ? -wh : wh;
+      *pdf = vndf_pdf(d, whf, lwi) * 0.25f / (fabsf(dot3(whf, lwi)) + kEps);
+    }
+    if (dot3(ng, lwo) <= 0.f) return f3(0.f, 0.f, 0.f);
+    const float3 kr = take(m.reflectance, l);
+    const float x = 1.f - fabsf(wh_in);
+    const float f5 = x * x * x * x * x;
+    const float mono = g * d * 0.25f / (fabsf(ns_in * ns_out) + kEps);
+    return f3(kr.x + (1.f - kr.x) * f5, kr.y + (1.f - kr.y) * f5, kr.z + (1.f - kr.z) * f5) * mono;
+  }
+  if (pdf) *pdf = 0.f;
+  return f3(0.f, 0.f, 0.f);
+}
+
+// SampleBSDF: DiffuseShader (shader.cxx:300-318), SpecularReflectiveShader (:345-366),
+// SpecularTransmissiveDielectricShader::SampleBsdfRegular (:401-473), MicrofacetShader
+// (:692-707).  Draw order matches the reference: square, then single uniforms.
+__device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float3 wi, const Surf& s, Rng& rng,
+                                                     Lambda l) {
+  ScatterSample out;
+  out.delta = false;
+  if (m.shader == TT_SHADER_DIFFUSE) {
+    const Frame fr = frame_z(s.ns);
+    float r[2];
+    rng.square(r);
+    const float3 v = to_cos_hemisphere(r);
+    out.pdf = v.z / kPi;
+    out.dir = fr.to_world(v);
+    out.value = dot3(s.n, out.dir) > 0.f ? take(m.reflectance, l) * (1.f / kPi) : f3(0.f, 0.f, 0.f);
+    return out;
+  }
+  if (m.shader == TT_SHADER_SPECULAR_REFLECTIVE) {
+    const float3 r = reflected(wi, s.ns);
+    out.dir = r;
+    out.pdf = 1.f;
+    out.delta = true;
+    out.value = dot3(s.n, r) < 0.f ? f3(0.f, 0.f, 0.f) : take(m.reflectance, l) * (1.f / dot3(s.ns, r));
+    return out;
+  }
+  if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC) {
+    const float abs_i = fabsf(dot3(s.ns, wi));
+    const bool entering = dot3(s.ng, wi) > 0.f;
+    const float eta = entering ? 1.f / m.ior_ratio : m.ior_ratio;
+    float fr = 1.f;
+    float3 wt;
+    const bool has_wt = refracted(wi, s.ns, eta, &wt);
+    if (has_wt) fr = fresnel_reflectivity(abs_i, fabsf(dot3(wt, s.ns)), eta);
+    const float prob_reflection = has_wt ? fmaxf(0.1f, fminf(0.9f, fr)) : 1.f;
+    const bool do_reflect = has_wt ? rng.uniform() < prob_reflection : true;
+    float value;
+    out.delta = true;
+    if (do_reflect) {
+      out.dir = reflected(wi, s.ns);
+      out.pdf = prob_reflection;
+      value = fr;
+    } else {
+      out.dir = wt;
+      out.pdf = 1.f - prob_reflection;
+      value = 1.f - fr;
+    }
+    value /= fabsf(dot3(out.dir, s.ns));
+    if (dot3(out.dir, s.n) < 0.f) value *= eta * eta;  // radiance transport
+    out.value = f3(value, value, value);
+    return out;
+  }
+  // TT_SHADER_MICROFACET
+  const Frame fr = frame_z(s.ns);
+  const float3 lwi = fr.to_local(wi);
+  float r[2];
+  rng.square(r);
+  float3 wh = beckmann_sample_wh(m.alpha, r);
+  {
+    // VisibleNdfVCavity::Sample
+    const float3 whp = f3(-wh.x, -wh.y, wh.z);
+    const float prob = clamp_dot(lwi, whp) / (clamp_dot(lwi, wh) + clamp_dot(lwi, whp) + kWiBelowHorizonFix);
+    if (rng.uniform() < prob) wh = whp;
+  }
+  const float3 lwo = reflected(lwi, wh);
+  const float3 ng = fr.to_local(s.n);
+  const float ns_out = lwo.z, ns_in = lwi.z, ns_wh = wh.z;
+  const float wh_out = dot3(lwo, wh), wh_in = dot3(lwi, wh);
+  const float d = beckmann_d(m.alpha, fabsf(ns_wh));
+  const float g = g2_vcavity(wh_in, wh_out, ns_in, ns_out, ns_wh);
+  const float3 whf = wh.z < 0.f ? -wh : wh;
+  out.pdf = vndf_pdf(d, whf, lwi) * 0.25f / (fabsf(dot3(whf, lwi)) + kEps);
+  out.dir = fr.to_world(lwo);
+  if (dot3(ng, lwo) <= 0.f) {
+    out.value = f3(0.f, 0.f, 0.f);
+    return out;
+  }
+  const float3 kr = take(m.reflectance, l);
+  const float x = 1.f - fabsf(wh_in);
+  const float f5 = x * x * x * x * x;
+  const float mono = g * d * 0.25f / (fabsf(ns_in * ns_out) + kEps);
+  out.value = f3(kr.x + (1.f - kr.x) * f5, kr.y + (1.f - kr.y) * f5, kr.z + (1.f - kr.z) * f5) * mono;
+  return out;
+}
+
+// BsdfCorrectionFactor (rendering_randomwalk_impl.hxx:616-622), radiance transport.
+__device__ __forceinline__ float bsdf_correction(const Surf& s, float3 exitant) {
+  return fabsf(dot3(s.ns, exitant)) / (fabsf(dot3(s.n, exitant)) + kEps);
+}
+
+// ----------------------------------------------------------------------------------------
+// Environmental lights (light.hxx:146-304, light.cxx:10-189).
+__device__ __forceinline__ float3 env_local(const DevEnvLight& L, float3 d) {
+  return f3(L.X[0] * d.x + L.X[1] * d.y + L.X[2] * d.z, L.Y[0] * d.x + L.Y[1] * d.y + L.Y[2] * d.z,
+            L.Z[0] * d.x + L.Z[1] * d.y + L.Z[2] * d.z);
+}
+__device__ __forceinline__ float3 env_world(const DevEnvLight& L, float3 v) {
+  return f3(L.X[0] * v.x + L.Y[0] * v.y + L.Z[0] * v.z, L.X[1] * v.x + L.Y[1] * v.y + L.Z[1] * v.z,
+            L.X[2] * v.x + L.Y[2] * v.y + L.Z[2] * v.z);
+}
+
+// EnvMapLight::MapToImage: KartesianToSpherical (third component up, vec3f.hxx:298-321),
+// SphericalToUv, UvToPixel (texture.hxx:37-55).
+__device__ __forceinline__ void envmap_pixel(const DevEnvLight& L, float3 dir_out, int* px, int* py) {
+  const float3 loc = env_local(L, dir_out);
+  const float x = loc.x, z = loc.y, y = loc.z;
+  const float ax = fabsf(x), az = fabsf(z);
+  const float r = sqrtf(loc.x * loc.x + loc.y * loc.y + loc.z * loc.z);
+  const float theta = acosf(y / r);
+  float phi;
+  if (ax > az) {
+    phi = atan2f(z, ax);
+    phi = (x > 0.f) ? phi : kPi - phi;
+  } else {
+    phi = atan2f(x, az);
+    phi = (z > 0.f) ? (kPi / 2.f) - phi : (3.f / 2.f * kPi) + phi;
+  }
+  float u = phi / (2.f * kPi), v = theta / kPi;
+  float dummy;
+  u = modff(u, &dummy);
+  v = modff(v, &dummy);
+  if (u < 0.f) u = 1.f + u;
+  if (v < 0.f) v = 1.f + v;
+  if (u > 1.f - kEpsF) u -= kEpsF;
+  if (v > 1.f - kEpsF) v -= kEpsF;
+  int ix = (int)(u * L.w);
+  int iy = (int)(v * L.h);
+  iy = L.h - iy - 1;
+  *px = min(max(ix, 0), L.w - 1);
+  *py = min(max(iy, 0), L.h - 1);
+}
+__device__ __forceinline__ void envmap_pixel_angles(const DevEnvLight& L, int x, int y, float* phi0, float* z0,
+                                                    float* phi1, float* z1) {
+  float ul = (float)x / L.w, vl = (float)y / L.h;
+  float uu = ul + 1.f / L.w, vu = vl + 1.f / L.h;
+  vl = 1.f - vl;
+  vu = 1.f - vu;
+  *phi0 = ul * (2.f * kPi);
+  *phi1 = uu * (2.f * kPi);
+  *z0 = cosf(vl * kPi);
+  *z1 = cosf(vu * kPi);
+}
+__device__ __forceinline__ float3 envmap_value(const DevEnvLight& L, int x, int y, Lambda l) {
+  const float* p = L.tex + 3 * ((size_t)y * L.w + x);
+  return rgb_to_selection(__ldg(p), __ldg(p + 1), __ldg(p + 2), l);
+}
+__device__ __forceinline__ float envmap_pdf_of_pixel(const DevEnvLight& L, int x, int y) {
+  const float proby = prob_from_cmf(L.cmf_rows, y);
+  const float probx = prob_from_cmf(L.cmf_cols + (size_t)y * L.w, x);
+  float phi0, z0, phi1, z1;
+  envmap_pixel_angles(L, x, y, &phi0, &z0, &phi1, &z1);
+  return proby * probx / ((z1 - z0) * (phi1 - phi0));
+}
+
+__device__ __forceinline__ float3 env_eval_one(const DevEnvLight& L, float3 dir_out, Lambda l) {
+  switch (L.kind) {
+    // Dome frame Z = down direction: light reaches directions pointing down.
+    case TT_ENV_DOME: return dot3(dir_out, f3(L.Z[0], L.Z[1], L.Z[2])) > 0.f ? take(L.spectrum, l) : f3(0.f, 0.f, 0.f);
+    case TT_ENV_SUN: return dot3(dir_out, f3(L.Z[0], L.Z[1], L.Z[2])) > L.cos_opening ? take(L.spectrum, l) : f3(0.f, 0.f, 0.f);
+    case TT_ENV_MAP: {
+      int x, y;
+      envmap_pixel(L, dir_out, &x, &y);
+      return envmap_value(L, x, y, l);
+    }
+    default: return f3(0.f, 0.f, 0.f);
+  }
+}
+__device__ __forceinline__ float env_pdf_one(const DevEnvLight& L, float3 dir_out) {
+  switch (L.kind) {
+    case TT_ENV_DOME: return dot3(dir_out, f3(L.Z[0], L.Z[1], L.Z[2])) > 0.f ? 1.f / (2.f * kPi) : 0.f;
+    case TT_ENV_SUN: return dot3(dir_out, f3(L.Z[0], L.Z[1], L.Z[2])) > L.cos_opening ? L.pdf_val : 0.f;
+    case TT_ENV_MAP: {
+      int x, y;
+      envmap_pixel(L, dir_out, &x, &y);
+      return envmap_pdf_of_pixel(L, x, y);
+    }
+    default: return 0.f;
+  }
+}
+
+struct DirSample {
+  float3 dir;
+  float3 value;
+  float pdf;
+  bool delta;
+};
+
+__device__ __forceinline__ DirSample env_sample_one(const DevEnvLight& L, Rng& rng, Lambda l) {
+  DirSample s;
+  s.delta = false;
+  float r[2];
+  switch (L.kind) {
+    case TT_ENV_DOME:
+      rng.square(r);
+      s.dir = env_world(L, to_uniform_hemisphere(r));
+      s.value = take(L.spectrum, l);
+      s.pdf = 1.f / (2.f * kPi);
+      return s;
+    case TT_ENV_SUN:
+      rng.square(r);
+      s.dir = env_world(L, to_sphere_section(L.cos_opening, r));
+      s.value = take(L.spectrum, l);
+      s.pdf = L.pdf_val;
+      return s;
+    case TT_ENV_DIRECTIONAL:
+      s.dir = f3(L.dir[0], L.dir[1], L.dir[2]);
+      s.value = take(L.spectrum, l);
+      s.pdf = 1.f;
+      s.delta = true;
+      return s;
+    default: {  // TT_ENV_MAP
+      rng.square(r);
+      const int y = tower_bisection(L.cmf_rows, L.h, r[1]);
+      const float proby = prob_from_cmf(L.cmf_rows, y);
+      const float* row = L.cmf_cols + (size_t)y * L.w;
+      const int x = tower_bisection(row, L.w, r[0]);
+      const float probx = prob_from_cmf(row, x);
+      float phi0, z0, phi1, z1;
+      envmap_pixel_angles(L, x, y, &phi0, &z0, &phi1, &z1);
+      float r2[2];
+      rng.square(r2);
+      s.dir = env_world(L, to_sphere_section(r2, phi0, z0, phi1, z1));
+      s.pdf = proby * probx / ((z1 - z0) * (phi1 - phi0));
+      s.value = envmap_value(L, x, y, l);
+      return s;
+    }
+  }
+}
+
+// TotalEnvironmentalRadianceField::Evaluate / EvaluatePdf (light.cxx:60-85).
+__device__ __forceinline__ float3 env_eval_total(const DevScene& sc, float3 dir_out, Lambda l) {
+  float3 acc = f3(0.f, 0.f, 0.f);
+  for (int i = 0; i < sc.num_env; ++i) acc = acc + env_eval_one(sc.env[i], dir_out, l);
+  return acc;
+}
+__device__ __forceinline__ float env_pdf_total(const DevScene& sc, float3 dir_out) {
+  float sum = 0.f;
+  for (int i = 0; i < sc.num_env; ++i) sum += env_pdf_one(sc.env[i], dir_out);
+  return sum * (sc.num_env > 0 ? 1.f / sc.num_env : 1.f);
+}
+
+// ----------------------------------------------------------------------------------------
+// Camera (camera.hxx:62-232).
+__device__ __forceinline__ float pixel_pdf_wrt_solid_angle(const DevCamera& c, float x, float y) {
+  const float area = c.xperpixel * c.yperpixel;
+  const float l = sqrtf(x * x + y * y + 1.f);
+  const float vz = 1.f / l;
+  return 1.f / area * (l * l / fabsf(vz + kEps));
+}
+
+__device__ __forceinline__ DirSample camera_sample(const DevCamera& c, int unit, Rng& rng) {
+  DirSample s;
+  const int py = unit / c.xres, px = unit - py * c.xres;
+  float r[2];
+  rng.square(r);
+  const float3 right = f3(c.right[0], c.right[1], c.right[2]), up = f3(c.up[0], c.up[1], c.up[2]),
+               dir = f3(c.dir[0], c.dir[1], c.dir[2]);
+  if (c.kind == TT_CAMERA_PINHOLE) {
+    float3 v = f3(c.xmin + (r[0] + px) * c.xperpixel, c.ymin + (r[1] + py) * c.yperpixel, 1.f);
+    v = normalize3(v);
+    s.dir = right * v.x + up * v.y + dir * v.z;
+    const float pdf = pixel_pdf_wrt_solid_angle(c, v.x, v.y);  // normalized components, as the reference
+    s.value = f3(pdf, pdf, pdf);
+    s.pdf = pdf;
+    s.delta = false;
+  } else {
+    const float u = (r[0] + px) * c.per_pixel_delta - 1.f;
+    const float v = (r[1] + py) * c.per_pixel_delta - 1.f;
+    const float rho = u * u + v * v;
+    float3 w = f3(2.f * u, 2.f * v, rho - 1.f) * (1.f / (1.f + rho));
+    w.z = -w.z;
+    if (rho <= 1.f) {
+      s.dir = right * w.x + up * w.y + dir * w.z;
+      s.value = f3(1.f, 1.f, 1.f);
+    } else {
+      s.dir = dir;
+      s.value = f3(0.f, 0.f, 0.f);
+    }
+    s.pdf = 1.f;
+    s.delta = true;
+  }
+  return s;
+}
+
+// PerspectiveCamera::Evaluate (camera.hxx:126-155): unit index and pdf, or unit -1.
+__device__ __forceinline__ int camera_evaluate(const DevCamera& c, float3 dir_out, float* pdf) {
+  *pdf = 0.f;
+  if (c.kind != TT_CAMERA_PINHOLE) return -1;
+  float z = dir_out.x * c.dir[0] + dir_out.y * c.dir[1] + dir_out.z * c.dir[2];
+  float x = dir_out.x * c.right[0] + dir_out.y * c.right[1] + dir_out.z * c.right[2];
+  float y = dir_out.x * c.up[0] + dir_out.y * c.up[1] + dir_out.z * c.up[2];
+  if (z <= 0.f) return -1;
+  x /= z;
+  y /= z;
+  const int px = (int)((x - c.xmin) / c.xperpixel);
+  const int py = (int)((y - c.ymin) / c.yperpixel);
+  if (px < 0 || px >= c.xres || py < 0 || py >= c.yres) return -1;
+  *pdf = pixel_pdf_wrt_solid_angle(c, x, y);
+  return py * c.xres + px;
+}
+
+}  // namespace tt

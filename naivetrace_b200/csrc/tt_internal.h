@@ -1,0 +1,132 @@
+// Shared host/device declarations of the CUDA path tracer: the device scene record, the
+// wavefront path-state layout and the kernel entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/toytrace_gpu.h"
+
+namespace tt {
+
+constexpr int NBINS = TT_NBINS;
+constexpr int MAX_ENV_LIGHTS = 4;
+constexpr int BVH_STACK = 64;        // per-thread traversal stack (entries)
+constexpr uint32_t ERR_STACK = 1u;   // error-word bits written by kernels
+constexpr uint32_t ERR_QUEUE = 2u;
+
+// Surface material as stored on the device.
+struct DevMaterial {
+  int shader;
+  int emissive;
+  float alpha;
+  float ior_ratio;
+  float reflectance[NBINS];
+  float emission[NBINS];
+};
+
+struct DevEnvLight {
+  int kind;
+  int w, h;
+  float pdf_val, cos_opening;            // sun
+  float X[3], Y[3], Z[3];                // frame columns (sun, dome, env map)
+  float dir[3];                          // directional light
+  float spectrum[NBINS];                 // dome / directional / sun emission (pre-scaled)
+  const float* tex;                      // env map RGB, row 0 = top
+  const float* cmf_rows;                 // h
+  const float* cmf_cols;                 // w * h
+};
+
+struct DevCamera {
+  int kind;
+  int xres, yres;
+  float pos[3], up[3], dir[3], right[3];
+  float xmin, ymin, xperpixel, yperpixel, per_pixel_delta;
+};
+
+// Everything a kernel needs to know about the scene; passed by value (constant bank).
+struct DevScene {
+  const float4* nodes;        // BVH2, 4 float4 per node
+  const float4* tris;         // 3 float4 per triangle in leaf order: v0 (w=prim), v1 (w=material), v2
+  const uint4* tri_idx;       // per prim: vertex indices a, b, c and material
+  const float* normals;       // per vertex xyz, or nullptr
+  const DevMaterial* materials;
+  const int* area_lights;     // prim of each area light
+  const float4* area_verts;   // 3 float4 (v0, v1, v2) per area light
+  const float* point_lights;  // per light: spectrum[36], pos[3]
+  int num_area_lights;
+  int num_point_lights;
+  int num_env;
+  int num_tris;
+  DevEnvLight env[MAX_ENV_LIGHTS];
+  DevCamera cam;
+  float type_probs[4];        // ENV, AREA, POINT, VOLUME
+  float in_class_area;
+  float long_distance;        // 10 x bounding-box diagonal
+  int max_path_nodes;         // max_ray_depth + 1
+  int sample_lights;
+  int sample_bsdf;
+};
+
+// Wavefront path state, structure of arrays, capacity `cap` paths.
+struct PathState {
+  int cap;
+  float4* ray_o;       // origin
+  float4* ray_d;       // direction, w = tfar
+  float4* hit;         // t, u, v, triangle slot (int bits, -1 = miss)
+  float4* beta;        // path throughput (3), w = pdf of the last scatter (negative: delta)
+  float4* accum;       // spectral path sum (3)
+  unsigned long long* rng_state;
+  unsigned long long* rng_inc;
+  uint4* meta;         // x pixel, y lambda idx (3 x 8 bits), z node count, w unused
+  float4* sh_o;        // shadow ray origin, w = tfar
+  float4* sh_d;        // direction, w = splat target pixel (int bits) or -1
+  float4* sh_c;        // spectral contribution
+  int* ext_q[2];
+  int* sh_q;
+  int* done_q;
+  int* counters;       // per bounce: [ext, shadow, done] x (max bounces + 2)
+  unsigned int* err;
+};
+
+struct Framebuffer {
+  float* accum;        // npix * 3, this pass
+  float* light;        // npix * 3, this pass
+};
+
+struct WaveArgs {
+  long long wave_start;      // first path of this wave within the pass
+  int wave_paths;
+  int pixel_begin;
+  int npix_range;
+  int npix_total;
+  unsigned long long sample_offset;
+  unsigned long long seed;
+};
+
+// Kernel launchers (tt_kernels.cu).  `stats` (device, 4 x u64) receives node visits and
+// triangle tests of extension and shadow rays when counting is on.
+void upload_constant_tables();
+void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
+                     cudaStream_t st);
+void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats,
+                   int grid, cudaStream_t st);
+void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);
+void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
+                   unsigned long long* stats, int grid, cudaStream_t st);
+void launch_flush(const PathState& p, const Framebuffer& fb, int bounce, int grid, cudaStream_t st);
+void launch_accumulate(const Framebuffer& fb, double* acc, double* light, int n3, cudaStream_t st);
+void launch_intersect_rays(const DevScene& s, const float* rays, int n, int* prim, float* t, float* u, float* v,
+                           unsigned int* err, cudaStream_t st);
+void launch_occluded_rays(const DevScene& s, const float* rays, int n, unsigned char* occ, unsigned int* err,
+                          cudaStream_t st);
+void launch_count_rays(const DevScene& s, const float* rays, int n, unsigned long long* counters,
+                       unsigned int* err, cudaStream_t st);
+void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, int n, unsigned long long seed,
+                        float* dir, float* val, float* pdf, cudaStream_t st);
+void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, const float* dirs, int n, float* val,
+                      float* pdf, cudaStream_t st);
+// Blocks per SM that the shading kernel sustains (for grid sizing).
+int kernel_blocks_per_sm();
+
+}  // namespace tt

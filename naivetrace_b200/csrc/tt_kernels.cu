@@ -1,0 +1,737 @@
+// Wavefront kernels of the forward path tracer with next-event estimation.
+//
+// The per-sample loop of PathTracingWorker::RenderPixel
+// (renderingalgorithms_pathtracing.hxx:731-817) is split into stages that each process a
+// queue of path slots:
+//   generate  - wavelength selection, next-event estimation at the camera vertex
+//               (splatted to the pixel the light sample projects to), camera ray.
+//   extend    - closest hit of the queued extension rays (BVH traversal).
+//   shade     - MIS-weighted emission at the hit, Russian roulette, next-event estimation
+//               (emits a shadow ray), BSDF sampling (emits the next extension ray).
+//   shadow    - occlusion test; adds the NEE contribution of unoccluded rays.
+//   flush     - converts finished paths to RGB and adds them to the framebuffer.
+// Queues are appended with warp-aggregated atomics.  All kernels loop grid-stride over a
+// device-side count, so launch shapes are fixed (a multiple of the SM count).
+#include <cuda_runtime.h>
+
+#include "tt_device.cuh"
+#include "tt_internal.h"
+#include "tt_tables.h"
+
+namespace tt {
+
+// ----------------------------------------------------------------------------------------
+__device__ __forceinline__ int warp_append(int* counter) {
+  const unsigned mask = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  const int rank = __popc(mask & ((1u << lane) - 1u));
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(mask));
+  base = __shfl_sync(mask, base, leader);
+  return base + rank;
+}
+
+__device__ __forceinline__ int* ext_count(const PathState& p, int b) { return &p.counters[3 * b]; }
+__device__ __forceinline__ int* sh_count(const PathState& p, int b) { return &p.counters[3 * b + 1]; }
+__device__ __forceinline__ int* done_count(const PathState& p, int b) { return &p.counters[3 * b + 2]; }
+
+// ----------------------------------------------------------------------------------------
+// BVH traversal (layout in tt_bvh.h) with the watertight ray/triangle test of Woop,
+// Benthin and Wald (2013), replacing rtcIntersect1 / rtcOccluded1
+// (embreeaccelerator.cxx:111, :302).  Hits count for tnear < t <= tfar.
+struct RayPre {
+  float3 o, d, id, ood;
+  int kx, ky, kz;
+  float Sx, Sy, Sz;
+};
+
+__device__ __forceinline__ float safe_inv(float x) {
+  const float ax = fabsf(x) < 1e-20f ? copysignf(1e-20f, x) : x;
+  return 1.f / ax;
+}
+
+__device__ __forceinline__ RayPre prepare_ray(float3 o, float3 d) {
+  RayPre r;
+  r.o = o;
+  r.d = d;
+  r.id = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+  r.ood = f3(o.x * r.id.x, o.y * r.id.y, o.z * r.id.z);
+  const float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  int kz = 0;
+  if (ay > ax) kz = 1;
+  if (az > fmaxf(ax, ay)) kz = 2;
+  int kx = kz + 1 == 3 ? 0 : kz + 1;
+  int ky = kx + 1 == 3 ? 0 : kx + 1;
+  if (comp(d, kz) < 0.f) { int t = kx; kx = ky; ky = t; }
+  r.kx = kx; r.ky = ky; r.kz = kz;
+  const float dz = comp(d, kz);
+  r.Sx = comp(d, kx) / dz;
+  r.Sy = comp(d, ky) / dz;
+  r.Sz = 1.f / dz;
+  return r;
+}
+
+// Returns true with t, and barycentric weights (b0, b1, b2) for (v0, v1, v2).
+__device__ __forceinline__ bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float tnear,
+                                              float tfar, float* tout, float* b1out, float* b2out) {
+  const float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+  const float Az_ = comp(A, r.kz), Bz_ = comp(B, r.kz), Cz_ = comp(C, r.kz);
+  const float Ax = comp(A, r.kx) - r.Sx * Az_, Ay = comp(A, r.ky) - r.Sy * Az_;
+  const float Bx = comp(B, r.kx) - r.Sx * Bz_, By = comp(B, r.ky) - r.Sy * Bz_;
+  const float Cx = comp(C, r.kx) - r.Sx * Cz_, Cy = comp(C, r.ky) - r.Sy * Cz_;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.f || V == 0.f || W == 0.f) {
+    // Edge case: recompute the edge functions in double precision (Woop et al., sec. 4).
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+  const float det = U + V + W;
+  if (det == 0.f) return false;
+  const float T = U * (r.Sz * Az_) + V * (r.Sz * Bz_) + W * (r.Sz * Cz_);
+  const float inv = 1.f / det;
+  const float t = T * inv;
+  if (!(t > tnear && t <= tfar)) return false;
+  *tout = t;
+  *b1out = V * inv;
+  *b2out = W * inv;
+  return true;
+}
+
+struct TraceCounters {
+  unsigned int nodes;
+  unsigned int tris;
+};
+
+// Closest hit (ANY = false) or any hit (ANY = true).  Returns the triangle slot or -1.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float tnear, float tfar, float* t_out,
+                                     float* b1_out, float* b2_out, unsigned int* err, TraceCounters* cnt) {
+  int stack[BVH_STACK];
+  int sp = 0;
+  int cur = 0;  // root is always an inner node
+  int best = -1;
+  float best_t = tfar, bb1 = 0.f, bb2 = 0.f;
+  const float box_tmax_scale = 1.0000004f;  // 1 + 2 gamma(3): conservative slabs
+  for (;;) {
+    if (cur >= 0) {
+      const float4* np = sc.nodes + 4 * (size_t)cur;
+      const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+      const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+      if (COUNT) cnt->nodes++;
+      const float lim = best_t * box_tmax_scale;
+      // Child 0
+      float tx0 = fmaf(n0.x, r.id.x, -r.ood.x), tx1 = fmaf(n0.y, r.id.x, -r.ood.x);
+      float ty0 = fmaf(n0.z, r.id.y, -r.ood.y), ty1 = fmaf(n0.w, r.id.y, -r.ood.y);
+      float tz0 = fmaf(n2.x, r.id.z, -r.ood.z), tz1 = fmaf(n2.y, r.id.z, -r.ood.z);
+      const float c0min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tnear));
+      const float c0max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+      // Child 1
+      tx0 = fmaf(n1.x, r.id.x, -r.ood.x); tx1 = fmaf(n1.y, r.id.x, -r.ood.x);
+      ty0 = fmaf(n1.z, r.id.y, -r.ood.y); ty1 = fmaf(n1.w, r.id.y, -r.ood.y);
+      tz0 = fmaf(n2.z, r.id.z, -r.ood.z); tz1 = fmaf(n2.w, r.id.z, -r.ood.z);
+      const float c1min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tnear));
+      const float c1max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+      const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
+      if (h0 && h1) {
+        int near = n3.x, far = n3.y;
+        if (c1min < c0min) { near = n3.y; far = n3.x; }
+        if (sp >= BVH_STACK) { atomicOr(err, ERR_STACK); return -1; }
+        stack[sp++] = far;
+        cur = near;
+        continue;
+      } else if (h0) {
+        cur = n3.x;
+        continue;
+      } else if (h1) {
+        cur = n3.y;
+        continue;
+      }
+    } else {
+      const unsigned v = ~(unsigned)cur;
+      const int start = (int)(v >> 3), count = (int)(v & 7u) + 1;
+      for (int i = start; i < start + count; ++i) {
+        const float4 a = __ldg(&sc.tris[3 * i]);
+        const float4 b = __ldg(&sc.tris[3 * i + 1]);
+        const float4 c = __ldg(&sc.tris[3 * i + 2]);
+        if (COUNT) cnt->tris++;
+        float t, b1, b2;
+        if (intersect_tri(r, xyz(a), xyz(b), xyz(c), tnear, best_t, &t, &b1, &b2)) {
+          best = i;
+          best_t = t;
+          bb1 = b1;
+          bb2 = b2;
+          if (ANY) { *t_out = t; return i; }
+        }
+      }
+    }
+    if (sp == 0) break;
+    cur = stack[--sp];
+  }
+  if (best >= 0) {
+    *t_out = best_t;
+    *b1_out = bb1;
+    *b2_out = bb2;
+  }
+  return best;
+}
+
+// ----------------------------------------------------------------------------------------
+// Light sampling and connection (TrivialLightPicker::PickLight, EmitterSampleVisitor,
+// CalculateConnection, PdfConversionFactor; rendering_randomwalk_impl.hxx:192-250,
+// 373-409, 493-513).
+enum { LIGHT_NONE = -1, LIGHT_ENV = 0, LIGHT_AREA = 1, LIGHT_POINT = 2 };
+
+struct LightNode {
+  int type;
+  float3 coord;      // area: position; env: direction of travel; point: position
+  float3 ng;         // area: raw winding normal
+  float3 bounds;     // area: position error bound
+  float3 radiance;   // env radiance / point spectrum
+  int prim;
+  float pdf;
+  bool delta;
+};
+
+__device__ __forceinline__ float tri_area(float3 p0, float3 p1, float3 p2) {
+  return 0.5f * len3(cross3(p1 - p0, p2 - p0));
+}
+
+struct Connection {
+  float3 org, dir;
+  float len;
+  float3 weight;    // scatter * target * DFactors * r2 (transmittance excluded)
+  float pdf_due;    // pdf of sampling the light vertex by scattering, light's measure
+  bool valid;       // nonzero weight: a shadow ray is needed
+  int unit;         // camera eye: pixel the connection lands in
+};
+
+struct Eye {
+  bool is_camera;
+  float3 pos;       // camera position or surface position
+  Surf surf;        // surface eye
+  float3 wi;        // reverse incident direction (surface eye)
+  const DevMaterial* mat;
+};
+
+__device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye, const LightNode& L, Lambda l) {
+  Connection c;
+  c.valid = false;
+  c.unit = -1;
+  c.pdf_due = 0.f;
+  c.weight = f3(0.f, 0.f, 0.f);
+  const bool light_env = L.type == LIGHT_ENV;
+  float3 cs = eye.is_camera ? eye.pos : eye.surf.pos;
+  float3 ct = L.coord;
+  // CalculateSegmentToTarget: direction, offsets on surface nodes, recompute.
+  float3 d;
+  float len;
+  if (!light_env) {
+    const float3 dd = ct - cs;
+    len = len3(dd);
+    d = dd * (1.f / len);
+  } else {
+    d = -ct;
+    len = sc.long_distance;
+  }
+  if (!eye.is_camera) cs = cs + offset_at(eye.surf, d);
+  if (L.type == LIGHT_AREA) {
+    const float delta = dot3(L.bounds, abs3(L.ng));
+    ct = ct + (delta * (dot3(-d, L.ng) > 0.f ? 1.f : -1.f)) * L.ng;
+  }
+  if (!light_env) {
+    const float3 dd = ct - cs;
+    len = len3(dd);
+    d = dd * (1.f / len);
+  }
+  c.org = cs;
+  c.dir = d;
+  c.len = len;
+  // Eye factor.
+  float3 sf;
+  float pdf_eye = 0.f;
+  if (eye.is_camera) {
+    const int unit = camera_evaluate(sc.cam, d, &pdf_eye);
+    c.unit = unit;
+    sf = unit >= 0 ? f3(pdf_eye, pdf_eye, pdf_eye) : f3(0.f, 0.f, 0.f);
+  } else {
+    sf = eval_bsdf(*eye.mat, eye.wi, eye.surf, d, l, &pdf_eye) * bsdf_correction(eye.surf, d);
+  }
+  // Light factor and DFactor of the light vertex.
+  float3 tf;
+  float dfac_light = 1.f;
+  if (L.type == LIGHT_AREA) {
+    const DevMaterial& lm = sc.materials[__ldg(&sc.tri_idx[L.prim]).w];
+    const float vis = dot3(L.ng, -d) > 0.f ? 1.f : 0.f;
+    tf = take(lm.emission, l) * (vis / (2.f * kPi));
+    dfac_light = fabsf(dot3(L.ng, d));
+  } else {
+    tf = L.radiance;
+  }
+  // PdfConversionFactor(eye, light): DFactor(light) / (len^2 + eps) unless the light is at
+  // infinity.
+  c.pdf_due = light_env ? pdf_eye * dfac_light : pdf_eye * dfac_light / (len * len + kEps);
+  if (is_zero(sf) || is_zero(tf)) return c;
+  const float dfac_eye = eye.is_camera ? 1.f : fabsf(dot3(eye.surf.ng, d));
+  const float r2 = light_env ? 1.f : 1.f / (len * len);
+  c.weight = mul(sf * dfac_eye, tf * dfac_light) * r2;
+  c.valid = true;
+  return c;
+}
+
+// Completes an area light sample: position, winding normal, error bound and pdf.  The
+// vertices come from the per-light table (area light order), not from the leaf slots.
+__device__ __forceinline__ void resolve_area(const DevScene& sc, int light_index, LightNode& L) {
+  const float4 a = __ldg(&sc.area_verts[3 * light_index]);
+  const float4 b = __ldg(&sc.area_verts[3 * light_index + 1]);
+  const float4 c = __ldg(&sc.area_verts[3 * light_index + 2]);
+  const float3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(c);
+  const float3 w = L.coord;
+  L.coord = p0 * w.x + p1 * w.y + p2 * w.z;
+  L.ng = normalize3(cross3(p1 - p0, p2 - p0));
+  L.bounds = (abs3(p0 * w.x) + abs3(p1 * w.y) + abs3(p2 * w.z)) * gamma7();
+  const float area = tri_area(p0, p1, p2);
+  L.pdf = (sc.type_probs[1] / sc.num_area_lights) * (1.f / area);
+}
+
+// ----------------------------------------------------------------------------------------
+__device__ __forceinline__ float mis_weight(const DevScene& sc, float pdf_taken, bool delta, float pdf_other) {
+  if (!delta && sc.sample_bsdf && sc.sample_lights) return power_heuristic(pdf_taken, pdf_other);
+  return 1.f;
+}
+
+__device__ __forceinline__ LightNode pick_light(const DevScene& sc, Rng& rng, Lambda l) {
+  LightNode L;
+  L.type = LIGHT_NONE;
+  L.delta = false;
+  L.pdf = 0.f;
+  const int which = tower_sampling4(sc.type_probs, rng.uniform());
+  if (which == LIGHT_ENV) {
+    const int i = rng.uniform_int(0, sc.num_env - 1);
+    DirSample s = env_sample_one(sc.env[i], rng, l);
+    L.type = LIGHT_ENV;
+    L.coord = s.dir;
+    L.radiance = s.value;
+    L.pdf = sc.type_probs[0] * (s.pdf * (1.f / sc.num_env));
+    L.delta = s.delta;
+  } else if (which == LIGHT_POINT) {
+    const int n = sc.num_point_lights;
+    const int i = rng.uniform_int(0, n - 1);
+    const float* pl = sc.point_lights + (size_t)i * (NBINS + 3);
+    L.type = LIGHT_POINT;
+    L.coord = f3(pl[NBINS], pl[NBINS + 1], pl[NBINS + 2]);
+    L.radiance = take(pl, l) * (1.f / (4.f * kPi));
+    L.pdf = sc.type_probs[2] / n;
+    L.delta = true;
+  } else if (which == LIGHT_AREA) {
+    const int n = sc.num_area_lights;
+    const int i = rng.uniform_int(0, n - 1);
+    float r[2];
+    rng.square(r);
+    L.type = LIGHT_AREA;
+    L.prim = __ldg(&sc.area_lights[i]);
+    L.coord = to_triangle_barycentric(r);
+    resolve_area(sc, i, L);
+  }
+  return L;
+}
+
+// ----------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Framebuffer fb, WaveArgs w) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.wave_paths; i += gridDim.x * blockDim.x) {
+    const long long g = w.wave_start + i;
+    const int pix_local = (int)(g % w.npix_range);
+    const unsigned long long sample = w.sample_offset + (unsigned long long)(g / w.npix_range);
+    const int pixel = w.pixel_begin + pix_local;
+    Rng rng;
+    rng.seed(w.seed, sample * (unsigned long long)w.npix_total + (unsigned long long)pixel);
+    // LambdaSelectionStrategy::WithWeights (shader_util.hxx:83-91).
+    const int main_idx = rng.uniform_int(0, 11);
+    int idx[3] = {main_idx, main_idx + 12, main_idx + 24};
+    const int rot = rng.uniform_int(0, 2);
+    { const int t = idx[0]; idx[0] = idx[rot]; idx[rot] = t; }
+    rng.uniform(); rng.uniform(); rng.uniform();  // SampleWavelengthStrata
+    const Lambda l{idx[0], idx[1], idx[2]};
+    const float3 beta = f3(12.f, 12.f, 12.f);
+    const float3 cam_pos = f3(sc.cam.pos[0], sc.cam.pos[1], sc.cam.pos[2]);
+    p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    // Next-event estimation at the camera vertex: a light sample seen directly by the
+    // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
+    if (sc.sample_lights) {
+      LightNode L = pick_light(sc, rng, l);
+      if (L.type != LIGHT_NONE) {
+        Eye eye;
+        eye.is_camera = true;
+        eye.pos = cam_pos;
+        Connection c = connect(sc, eye, L, l);
+        if (c.valid && c.unit >= 0) {
+          const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
+          const float3 contrib = mul(c.weight, beta) * (mis / L.pdf / (float)w.npix_total);
+          const int q = warp_append(sh_count(p, 0));
+          p.sh_q[q] = i;
+          p.sh_o[i] = make_float4(c.org.x, c.org.y, c.org.z, c.len * 0.9999f);
+          p.sh_d[i] = make_float4(c.dir.x, c.dir.y, c.dir.z, __int_as_float(c.unit));
+          p.sh_c[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+        }
+      }
+    }
+    // Camera ray (TakeRandomWalkStep from the camera node).
+    DirSample s = camera_sample(sc.cam, pixel, rng);
+    const float3 bf = s.value * (1.f / s.pdf);
+    p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), 1u, s.delta ? 1u : 0u);
+    p.rng_state[i] = rng.state;
+    p.rng_inc[i] = rng.inc;
+    if (is_zero(bf)) {
+      const int q = warp_append(done_count(p, 0));
+      p.done_q[q] = i;
+      continue;
+    }
+    const float3 nb = mul(beta, bf);
+    p.beta[i] = make_float4(nb.x, nb.y, nb.z, s.pdf);
+    p.ray_o[i] = make_float4(cam_pos.x, cam_pos.y, cam_pos.z, 0.f);
+    p.ray_d[i] = make_float4(s.dir.x, s.dir.y, s.dir.z, kLargeNumber);
+    const int q = warp_append(ext_count(p, 0));
+    p.ext_q[0][q] = i;
+  }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bounce,
+                                                unsigned long long* counters) {
+  const int n = *ext_count(p, bounce);
+  const int* q = p.ext_q[bounce & 1];
+  TraceCounters cnt{0u, 0u};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int slot = q[i];
+    const float4 o = p.ray_o[slot], d = p.ray_d[slot];
+    const RayPre r = prepare_ray(xyz(o), xyz(d));
+    float t = 0.f, b1 = 0.f, b2 = 0.f;
+    const int hit = trace<false, COUNT>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
+    p.hit[slot] = make_float4(t, b1, b2, __int_as_float(hit));
+  }
+  if (COUNT) {
+    atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
+    atomicAdd(&counters[1], (unsigned long long)cnt.tris);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bounce) {
+    const int n = *ext_count(p, bounce);
+  const int* q = p.ext_q[bounce & 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int slot = q[i];
+    const float4 h = p.hit[slot];
+    const float4 d4 = p.ray_d[slot];
+    const float3 dir = xyz(d4);
+    uint4 meta = p.meta[slot];
+    const Lambda l = unpack_lambda(meta.y);
+    float4 b4 = p.beta[slot];
+    float3 beta = xyz(b4);
+    const float prev_pdf = b4.w;
+    const bool prev_delta = meta.w & 1u;
+    float4 acc4 = p.accum[slot];
+    float3 acc = xyz(acc4);
+    Rng rng{p.rng_state[slot], p.rng_inc[slot]};
+    const int count = (int)meta.z + 1;
+    const int tri = __float_as_int(h.w);
+    bool done = false;
+    Surf s;
+    if (tri >= 0) {
+      const float u = h.y, v = h.z;
+      s = make_surface(sc, tri, 1.f - u - v, u, v, f3(u, v, 1.f - u - v));
+      orient(s, dir);
+      const DevMaterial& m = sc.materials[s.material];
+      if (sc.sample_bsdf && m.emissive) {
+        // Emission at an emitter hit, MIS against area-light sampling.
+        const float vis = dot3(s.ng, -dir) > 0.f ? 1.f : 0.f;
+        const float3 end_weight = take(m.emission, l) * (vis / (2.f * kPi));
+        const float4 a = __ldg(&sc.tris[3 * tri]), b = __ldg(&sc.tris[3 * tri + 1]), c = __ldg(&sc.tris[3 * tri + 2]);
+        const float area = tri_area(xyz(a), xyz(b), xyz(c));
+        const float pdf_direct = (1.f / area) * sc.type_probs[1] * sc.in_class_area;
+        const float dfac = fabsf(dot3(s.ng, dir));
+        const float pdf_due = prev_delta ? dfac * prev_pdf : dfac / (h.x * h.x + kEps) * prev_pdf;
+        const float mis = mis_weight(sc, pdf_due, prev_delta, pdf_direct);
+        acc = acc + mul(end_weight, beta) * mis;
+      }
+    } else {
+      // Escaped: environment emission with MIS, then the walk ends.
+      if (sc.sample_bsdf && sc.num_env > 0) {
+        const float3 end_weight = env_eval_total(sc, -dir, l);
+        const float pdf_direct = env_pdf_total(sc, -dir) * sc.type_probs[0];
+        const float mis = mis_weight(sc, prev_pdf, prev_delta, pdf_direct);
+        acc = acc + mul(end_weight, beta) * mis;
+      }
+      done = true;
+    }
+    // Russian roulette (SurvivalAtNthScatterNode, rendering_randomwalk_impl.hxx:736-755).
+    if (!done) {
+      if (count < sc.max_path_nodes) {
+        if (count > 5) {
+          const float pr = fminf(0.9f, max3(beta));
+          if (rng.uniform() > pr) done = true;
+          else beta = beta * (1.f / pr);
+        }
+      } else {
+        done = true;
+      }
+    }
+    if (!done) {
+      const DevMaterial& m = sc.materials[s.material];
+      const float3 wi = -dir;
+      if (sc.sample_lights) {
+        LightNode L = pick_light(sc, rng, l);
+        if (L.type != LIGHT_NONE) {
+          Eye eye;
+          eye.is_camera = false;
+          eye.surf = s;
+          eye.wi = wi;
+          eye.mat = &m;
+          Connection c = connect(sc, eye, L, l);
+          if (c.valid) {
+            const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
+            const float3 contrib = mul(c.weight, beta) * (mis / L.pdf);
+            const int qs = warp_append(sh_count(p, bounce + 1));
+            p.sh_q[qs] = slot;
+            p.sh_o[slot] = make_float4(c.org.x, c.org.y, c.org.z, c.len * 0.9999f);
+            p.sh_d[slot] = make_float4(c.dir.x, c.dir.y, c.dir.z, __int_as_float(-1));
+            p.sh_c[slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+          }
+        }
+      }
+      // BSDF sample (TakeRandomWalkStep from a surface scatter node).
+      ScatterSample ss = sample_bsdf(m, wi, s, rng, l);
+      const float3 val = ss.value * (bsdf_correction(s, ss.dir) * fabsf(dot3(s.ng, ss.dir)));
+      const float3 bf = val * (1.f / ss.pdf);
+      if (is_zero(bf) || !(ss.pdf > 0.f)) {
+        done = true;
+      } else {
+        beta = mul(beta, bf);
+        const float3 org = s.pos + offset_at(s, ss.dir);
+        p.ray_o[slot] = make_float4(org.x, org.y, org.z, 0.f);
+        p.ray_d[slot] = make_float4(ss.dir.x, ss.dir.y, ss.dir.z, kLargeNumber);
+        p.beta[slot] = make_float4(beta.x, beta.y, beta.z, ss.pdf);
+        meta.z = (unsigned)count;
+        meta.w = ss.delta ? 1u : 0u;
+        p.meta[slot] = meta;
+        const int qe = warp_append(ext_count(p, bounce + 1));
+        p.ext_q[(bounce + 1) & 1][qe] = slot;
+      }
+    }
+    p.accum[slot] = make_float4(acc.x, acc.y, acc.z, 0.f);
+    p.rng_state[slot] = rng.state;
+    if (done) {
+      const int qd = warp_append(done_count(p, bounce + 1));
+      p.done_q[qd] = slot;
+    }
+  }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Framebuffer fb, int bounce,
+                                                unsigned long long* counters) {
+  const int n = *sh_count(p, bounce);
+  TraceCounters cnt{0u, 0u};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int slot = p.sh_q[i];
+    const float4 o = p.sh_o[slot], d = p.sh_d[slot];
+    const RayPre r = prepare_ray(xyz(o), xyz(d));
+    float t, b1, b2;
+    const int hit = trace<true, COUNT>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
+    if (hit >= 0) continue;
+    const float4 c = p.sh_c[slot];
+    const int target = __float_as_int(d.w);
+    if (target < 0) {
+      float4 a = p.accum[slot];
+      p.accum[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, 0.f);
+    } else {
+      const Lambda l = unpack_lambda(p.meta[slot].y);
+      const float3 rgb = selection_to_rgb(xyz(c), l);
+      atomicAdd(&fb.light[3 * target], rgb.x);
+      atomicAdd(&fb.light[3 * target + 1], rgb.y);
+      atomicAdd(&fb.light[3 * target + 2], rgb.z);
+    }
+  }
+  if (COUNT) {
+    atomicAdd(&counters[2], (unsigned long long)cnt.nodes);
+    atomicAdd(&counters[3], (unsigned long long)cnt.tris);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_flush(PathState p, Framebuffer fb, int bounce) {
+  const int n = *done_count(p, bounce);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int slot = p.done_q[i];
+    const uint4 meta = p.meta[slot];
+    const float3 rgb = selection_to_rgb(xyz(p.accum[slot]), unpack_lambda(meta.y));
+    const int px = (int)meta.x;
+    atomicAdd(&fb.accum[3 * px], rgb.x);
+    atomicAdd(&fb.accum[3 * px + 1], rgb.y);
+    atomicAdd(&fb.accum[3 * px + 2], rgb.z);
+  }
+}
+
+__global__ void k_accumulate(Framebuffer fb, double* acc, double* light, int n3) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
+    acc[i] += (double)fb.accum[i];
+    light[i] += (double)fb.light[i];
+    fb.accum[i] = 0.f;
+    fb.light[i] = 0.f;
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Batch queries and shader sampling for the parity tests.
+__global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* prim, float* t, float* u, float* v,
+                                 unsigned int* err) {
+  TraceCounters cnt{0u, 0u};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float* r = rays + 8 * (size_t)i;
+    const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
+    float tt = -1.f, b1 = 0.f, b2 = 0.f;
+    const int slot = trace<false, false>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
+    prim[i] = slot >= 0 ? __float_as_int(__ldg(&sc.tris[3 * slot]).w) : -1;
+    t[i] = slot >= 0 ? tt : -1.f;
+    u[i] = b1;
+    v[i] = b2;
+  }
+}
+
+__global__ void k_occluded_rays(DevScene sc, const float* rays, int n, unsigned char* occ, unsigned int* err) {
+  TraceCounters cnt{0u, 0u};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float* r = rays + 8 * (size_t)i;
+    const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
+    float tt, b1, b2;
+    occ[i] = trace<true, false>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt) >= 0 ? 1 : 0;
+  }
+}
+
+__global__ void k_count_rays(DevScene sc, const float* rays, int n, unsigned long long* counters,
+                             unsigned int* err) {
+  TraceCounters cnt{0u, 0u};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float* r = rays + 8 * (size_t)i;
+    const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
+    float tt, b1, b2;
+    trace<false, true>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
+  }
+  atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
+  atomicAdd(&counters[1], (unsigned long long)cnt.tris);
+}
+
+__device__ __forceinline__ Surf zup_surface(float3 wi) {
+  Surf s;
+  s.prim = 0;
+  s.material = 0;
+  s.pos = f3(0.f, 0.f, 0.f);
+  s.ng = f3(0.f, 0.f, 1.f);
+  s.ns_raw = s.ng;
+  s.bounds = f3(0.f, 0.f, 0.f);
+  orient(s, -wi);
+  return s;
+}
+
+__global__ void k_sample_bsdf(DevScene sc, int material, float3 wi, int3 li, int n, unsigned long long seed,
+                              float* dir, float* val, float* pdf) {
+  const Lambda l{li.x, li.y, li.z};
+  const Surf s = zup_surface(wi);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Rng rng;
+    rng.seed(seed, (unsigned long long)i);
+    ScatterSample ss = sample_bsdf(sc.materials[material], wi, s, rng, l);
+    dir[3 * i] = ss.dir.x; dir[3 * i + 1] = ss.dir.y; dir[3 * i + 2] = ss.dir.z;
+    val[3 * i] = ss.value.x; val[3 * i + 1] = ss.value.y; val[3 * i + 2] = ss.value.z;
+    pdf[i] = ss.delta ? -ss.pdf : ss.pdf;
+  }
+}
+
+__global__ void k_eval_bsdf(DevScene sc, int material, float3 wi, int3 li, const float* dirs, int n, float* val,
+                            float* pdf) {
+  const Lambda l{li.x, li.y, li.z};
+  const Surf s = zup_surface(wi);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float pp = 0.f;
+    const float3 v = eval_bsdf(sc.materials[material], wi, s, f3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]), l, &pp);
+    val[3 * i] = v.x; val[3 * i + 1] = v.y; val[3 * i + 2] = v.z;
+    pdf[i] = pp;
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// Host launchers.
+
+
+void upload_constant_tables() {
+  float m[3][NBINS], smits[7][NBINS];
+  for (int i = 0; i < 3; ++i)
+    for (int b = 0; b < NBINS; ++b) m[i][b] = (float)kSpectrumToRgb[i][b];
+  for (int i = 0; i < 7; ++i)
+    for (int b = 0; b < NBINS; ++b) smits[i][b] = (float)kSmitsBasis[i][b];
+  cudaMemcpyToSymbol(c_spec_to_rgb, m, sizeof(m));
+  cudaMemcpyToSymbol(c_smits, smits, sizeof(smits));
+}
+
+constexpr int kBlock = 256;
+
+void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
+                     cudaStream_t st) {
+  k_generate<<<grid, kBlock, 0, st>>>(s, p, fb, w);
+}
+void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
+                   cudaStream_t st) {
+  if (count) k_extend<true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+  else k_extend<false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+}
+void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
+  k_shade<<<grid, kBlock, 0, st>>>(s, p, bounce);
+}
+void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
+                   unsigned long long* stats, int grid, cudaStream_t st) {
+  if (count) k_shadow<true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+  else k_shadow<false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+}
+void launch_flush(const PathState& p, const Framebuffer& fb, int bounce, int grid, cudaStream_t st) {
+  k_flush<<<grid, kBlock, 0, st>>>(p, fb, bounce);
+}
+void launch_accumulate(const Framebuffer& fb, double* acc, double* light, int n3, cudaStream_t st) {
+  const int grid = (n3 + kBlock - 1) / kBlock;
+  if (grid > 0) k_accumulate<<<grid < 65535 ? grid : 65535, kBlock, 0, st>>>(fb, acc, light, n3);
+}
+static int grid_for(int n) {
+  int g = (n + kBlock - 1) / kBlock;
+  return g < 1 ? 1 : (g > 65535 ? 65535 : g);
+}
+void launch_intersect_rays(const DevScene& s, const float* rays, int n, int* prim, float* t, float* u, float* v,
+                           unsigned int* err, cudaStream_t st) {
+  if (n > 0) k_intersect_rays<<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v, err);
+}
+void launch_occluded_rays(const DevScene& s, const float* rays, int n, unsigned char* occ, unsigned int* err,
+                          cudaStream_t st) {
+  if (n > 0) k_occluded_rays<<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
+}
+void launch_count_rays(const DevScene& s, const float* rays, int n, unsigned long long* counters, unsigned int* err,
+                       cudaStream_t st) {
+  if (n > 0) k_count_rays<<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
+}
+void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, int n, unsigned long long seed,
+                        float* dir, float* val, float* pdf, cudaStream_t st) {
+  if (n > 0) k_sample_bsdf<<<grid_for(n), kBlock, 0, st>>>(s, material, wi, lambda, n, seed, dir, val, pdf);
+}
+void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, const float* dirs, int n, float* val,
+                      float* pdf, cudaStream_t st) {
+  if (n > 0) k_eval_bsdf<<<grid_for(n), kBlock, 0, st>>>(s, material, wi, lambda, dirs, n, val, pdf);
+}
+int kernel_blocks_per_sm() {
+  int b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade, kBlock, 0);
+  int e = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, k_extend<false>, kBlock, 0);
+  if (e < b) b = e;
+  return b < 1 ? 1 : b;
+}
+
+}  // namespace tt

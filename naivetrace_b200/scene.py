@@ -1,0 +1,238 @@
+"""Host-side scene model: the Scene / Material / light / camera objects of the reference
+(src/scene.hxx:134-315, src/light.hxx, src/camera.hxx) reduced to what the forward path
+tracer consumes, and their flattening into the C-ABI's tt_scene_desc.
+
+Geometry is stored the way the reference's Mesh stores it (float32 vertices, uint32 index
+triples, optional per-vertex normals, primitive.hxx:59-88).  Triangles keep the order in
+which they were added; that order defines the global primitive ids reported by the
+intersection entry points.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional
+
+import numpy as np
+
+from . import abi
+from .spectral import as_spectrum
+
+NBINS = abi.NBINS
+
+
+@dataclass
+class MaterialSpec:
+    """Shader + optional UniformAreaLight (struct Material, scene.hxx:45-54)."""
+
+    shader: int = abi.SHADER_DIFFUSE
+    reflectance: np.ndarray = field(default_factory=lambda: np.full(NBINS, 0.8))
+    alpha: float = 0.0
+    ior_ratio: float = 1.5
+    emission: Optional[np.ndarray] = None
+
+    def to_c(self) -> abi.Material:
+        m = abi.Material()
+        m.shader = int(self.shader)
+        m.reflectance[:] = [float(x) for x in as_spectrum(self.reflectance)]
+        m.alpha = float(self.alpha)
+        m.ior_ratio = float(self.ior_ratio)
+        if self.emission is not None:
+            m.emissive = 1
+            m.emission[:] = [float(x) for x in as_spectrum(self.emission)]
+        return m
+
+
+def diffuse(reflectance) -> MaterialSpec:
+    return MaterialSpec(shader=abi.SHADER_DIFFUSE, reflectance=as_spectrum(reflectance))
+
+
+def mirror(reflectance) -> MaterialSpec:
+    return MaterialSpec(shader=abi.SHADER_SPECULAR_REFLECTIVE, reflectance=as_spectrum(reflectance))
+
+
+def glass(ior_ratio: float) -> MaterialSpec:
+    return MaterialSpec(shader=abi.SHADER_SPECULAR_DIELECTRIC, reflectance=np.zeros(NBINS), ior_ratio=ior_ratio)
+
+
+def microfacet(reflectance, alpha: float) -> MaterialSpec:
+    return MaterialSpec(shader=abi.SHADER_MICROFACET, reflectance=as_spectrum(reflectance), alpha=alpha)
+
+
+def area_light(emission, reflectance=0.0) -> MaterialSpec:
+    return MaterialSpec(shader=abi.SHADER_DIFFUSE, reflectance=as_spectrum(reflectance), emission=as_spectrum(emission))
+
+
+@dataclass
+class EnvLightSpec:
+    kind: int
+    spectrum: np.ndarray = field(default_factory=lambda: np.zeros(NBINS))
+    dir: tuple = (0.0, 1.0, 0.0)
+    scalar: float = 0.0
+    scalar2: float = 0.0
+    texture: Optional[np.ndarray] = None  # (h, w, 3) float32, row 0 = top
+
+
+def dome_light(spectrum, up=(0.0, 1.0, 0.0)) -> EnvLightSpec:
+    return EnvLightSpec(kind=abi.ENV_DOME, spectrum=as_spectrum(spectrum), dir=tuple(up))
+
+
+def sun_light(total_power: float, dir_out, opening_angle_deg: float) -> EnvLightSpec:
+    """Sun (light.hxx:238-288).  dir_out: direction the light travels.  The opening angle
+    is the half angle of the cone of directions that receive light."""
+    return EnvLightSpec(kind=abi.ENV_SUN, dir=tuple(dir_out), scalar=total_power, scalar2=opening_angle_deg)
+
+
+def env_map(texture: np.ndarray, up=(0.0, 1.0, 0.0)) -> EnvLightSpec:
+    tex = np.ascontiguousarray(texture, dtype=np.float32)
+    assert tex.ndim == 3 and tex.shape[2] == 3
+    return EnvLightSpec(kind=abi.ENV_MAP, dir=tuple(up), texture=tex)
+
+
+def directional_light(spectrum, dir_out) -> EnvLightSpec:
+    return EnvLightSpec(kind=abi.ENV_DIRECTIONAL, spectrum=as_spectrum(spectrum), dir=tuple(dir_out))
+
+
+@dataclass
+class CameraSpec:
+    kind: int = abi.CAMERA_PINHOLE
+    pos: tuple = (0.0, 0.0, 0.0)
+    dir: tuple = (0.0, 0.0, 1.0)
+    up: tuple = (0.0, 1.0, 0.0)
+    fov_deg: float = 40.0
+    xres: int = 64
+    yres: int = 64
+
+    @property
+    def num_pixels(self) -> int:
+        return self.xres * self.yres
+
+
+class Scene:
+    """Triangle soup with per-triangle material, lights and one camera."""
+
+    def __init__(self):
+        self._verts: List[np.ndarray] = []
+        self._norms: List[Optional[np.ndarray]] = []
+        self._tris: List[np.ndarray] = []
+        self._mats_of_tris: List[np.ndarray] = []
+        self._nverts = 0
+        self.materials: List[MaterialSpec] = []
+        self.env_lights: List[EnvLightSpec] = []
+        self.point_lights: List[tuple] = []
+        self.camera = CameraSpec()
+        self.name = "scene"
+        self._flat = None
+
+    # -- building -----------------------------------------------------------------
+    def add_material(self, m: MaterialSpec) -> int:
+        self.materials.append(m)
+        self._flat = None
+        return len(self.materials) - 1
+
+    def add_mesh(self, vertices, triangles, material: int, normals=None) -> None:
+        v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
+        t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
+        if t.size and int(t.max()) >= len(v):
+            raise ValueError("triangle index out of range")
+        self._verts.append(v)
+        self._norms.append(None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3))
+        self._tris.append(t + np.uint32(self._nverts))
+        self._mats_of_tris.append(np.full(len(t), material, dtype=np.uint32))
+        self._nverts += len(v)
+        self._flat = None
+
+    def add_point_light(self, spectrum, pos) -> None:
+        self.point_lights.append((as_spectrum(spectrum), tuple(pos)))
+        self._flat = None
+
+    # -- flattening -----------------------------------------------------------------
+    def arrays(self):
+        if self._flat is None:
+            verts = np.concatenate(self._verts) if self._verts else np.zeros((0, 3), np.float32)
+            tris = np.concatenate(self._tris) if self._tris else np.zeros((0, 3), np.uint32)
+            mats = np.concatenate(self._mats_of_tris) if self._mats_of_tris else np.zeros(0, np.uint32)
+            if any(n is not None for n in self._norms):
+                norms = []
+                for v, n, t in zip(self._verts, self._norms, self._tris):
+                    if n is None:
+                        raise ValueError("either all meshes or none must carry normals")
+                    norms.append(n)
+                norms = np.ascontiguousarray(np.concatenate(norms))
+            else:
+                norms = None
+            self._flat = (np.ascontiguousarray(verts), norms, np.ascontiguousarray(tris), np.ascontiguousarray(mats))
+        return self._flat
+
+    @property
+    def num_triangles(self) -> int:
+        return int(sum(len(t) for t in self._tris))
+
+    def bounding_box(self):
+        v = self.arrays()[0]
+        return v.min(axis=0).astype(np.float64), v.max(axis=0).astype(np.float64)
+
+    def to_desc(self):
+        """Returns (tt_scene_desc, keepalive).  keepalive owns every array the descriptor
+        points to and must outlive its use."""
+        verts, norms, tris, mats = self.arrays()
+        keep = [verts, norms, tris, mats]
+        d = abi.SceneDesc()
+        d.num_vertices = len(verts)
+        d.vertices = verts.ctypes.data_as(C.POINTER(C.c_float))
+        d.normals = norms.ctypes.data_as(C.POINTER(C.c_float)) if norms is not None else None
+        d.num_triangles = len(tris)
+        d.indices = tris.ctypes.data_as(C.POINTER(C.c_uint32))
+        d.material_ids = mats.ctypes.data_as(C.POINTER(C.c_uint32))
+        mat_arr = (abi.Material * max(1, len(self.materials)))(*[m.to_c() for m in self.materials])
+        keep.append(mat_arr)
+        d.num_materials = len(self.materials)
+        d.materials = C.cast(mat_arr, C.POINTER(abi.Material))
+        envs = []
+        for e in self.env_lights:
+            c = abi.EnvLight()
+            c.kind = e.kind
+            c.spectrum[:] = [float(x) for x in as_spectrum(e.spectrum)]
+            c.dir[:] = [float(x) for x in e.dir]
+            c.scalar = float(e.scalar)
+            c.scalar2 = float(e.scalar2)
+            if e.texture is not None:
+                tex = np.ascontiguousarray(e.texture, dtype=np.float32)
+                keep.append(tex)
+                c.tex_height, c.tex_width = int(tex.shape[0]), int(tex.shape[1])
+                c.tex_rgb = tex.ctypes.data_as(C.POINTER(C.c_float))
+            envs.append(c)
+        env_arr = (abi.EnvLight * max(1, len(envs)))(*envs)
+        keep.append(env_arr)
+        d.num_env_lights = len(envs)
+        d.env_lights = C.cast(env_arr, C.POINTER(abi.EnvLight))
+        pts = []
+        for spec, pos in self.point_lights:
+            p = abi.PointLight()
+            p.spectrum[:] = [float(x) for x in spec]
+            p.pos[:] = [float(x) for x in pos]
+            pts.append(p)
+        pt_arr = (abi.PointLight * max(1, len(pts)))(*pts)
+        keep.append(pt_arr)
+        d.num_point_lights = len(pts)
+        d.point_lights = C.cast(pt_arr, C.POINTER(abi.PointLight))
+        cam = self.camera
+        d.camera.kind = cam.kind
+        d.camera.pos[:] = [float(x) for x in cam.pos]
+        d.camera.dir[:] = [float(x) for x in cam.dir]
+        d.camera.up[:] = [float(x) for x in cam.up]
+        d.camera.fov_deg = float(cam.fov_deg)
+        d.camera.xres = int(cam.xres)
+        d.camera.yres = int(cam.yres)
+        return d, keep
+
+
+def make_params(max_ray_depth: int = 25, pt_sample_mode: int = abi.SAMPLE_BOTH, max_spp: int = -1,
+                wave_paths: int = 0, device: int = 0) -> abi.Params:
+    p = abi.Params()
+    p.max_ray_depth = max_ray_depth
+    p.pt_sample_mode = pt_sample_mode
+    p.max_samples_per_pixel = max_spp
+    p.wave_paths = wave_paths
+    p.device = device
+    return p

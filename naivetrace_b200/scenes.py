@@ -1,0 +1,251 @@
+"""Seeded procedural scenes for the workloads the tracer is measured on.
+
+- cornell_box():     unit-cube Cornell box with two boxes and a ceiling area light
+                     (256x256, 16 spp, depth 10 as the standard small case).
+- terrain_spheres(): 1024x1024-vertex fBm heightfield (~2.1 M triangles) with 32
+                     tessellated spheres of 20 480 triangles each, lit by a float32
+                     equirect sky gradient plus a 0.53 degree sun (1920x1080, 64 spp,
+                     depth 16).
+- small scenes for parity tests.
+There is no public dataset involved; every input is generated here from a seed.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import abi
+from .scene import (CameraSpec, Scene, area_light, diffuse, env_map, glass, microfacet,
+                    mirror, sun_light)
+from .spectral import band_spectrum, rgb_to_spectrum
+
+
+def quad(p0, p1, p2, p3):
+    """Two triangles (p0,p1,p2), (p0,p2,p3); winding normal = (p1-p0) x (p2-p0)."""
+    v = np.array([p0, p1, p2, p3], dtype=np.float64)
+    t = np.array([[0, 1, 2], [0, 2, 3]], dtype=np.uint32)
+    return v, t
+
+
+def box_mesh(size, center_base, rot_y_deg):
+    """Closed axis-aligned box of `size` (sx, sy, sz) standing on y = center_base.y,
+    rotated about the vertical axis through its centre; outward winding."""
+    sx, sy, sz = size
+    x0, x1 = -sx / 2, sx / 2
+    y0, y1 = 0.0, sy
+    z0, z1 = -sz / 2, sz / 2
+    c = [
+        (x0, y0, z0), (x1, y0, z0), (x1, y1, z0), (x0, y1, z0),
+        (x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1),
+    ]
+    faces = [
+        (0, 3, 2, 1),  # -z
+        (4, 5, 6, 7),  # +z
+        (0, 4, 7, 3),  # -x
+        (1, 2, 6, 5),  # +x
+        (0, 1, 5, 4),  # -y
+        (3, 7, 6, 2),  # +y
+    ]
+    v = np.array(c, dtype=np.float64)
+    a = math.radians(rot_y_deg)
+    rot = np.array([[math.cos(a), 0, math.sin(a)], [0, 1, 0], [-math.sin(a), 0, math.cos(a)]])
+    v = v @ rot.T + np.asarray(center_base, dtype=np.float64)
+    tris = []
+    for f in faces:
+        tris.append([f[0], f[1], f[2]])
+        tris.append([f[0], f[2], f[3]])
+    return v, np.array(tris, dtype=np.uint32)
+
+
+def cornell_box(xres=256, yres=256) -> Scene:
+    """Unit-cube Cornell box: 5 walls as 2-triangle quads (open towards the camera at
+    z = 0), Lambert 0.75 white floor/ceiling/back wall, red left wall (0.75 in the bins
+    centred at >= 605 nm, 0.05 elsewhere), green right wall (0.75 for 505-565 nm), a
+    0.25 x 0.25 downward-facing area light just below the ceiling with flat emission 10,
+    a 0.3^3 box at (0.65, 0, 0.35) rotated 17 degrees and a 0.3 x 0.6 x 0.3 box at
+    (0.3, 0, 0.65) rotated -17 degrees.  Pinhole camera at (0.5, 0.5, -1.4) looking +z
+    with a 40 degree field of view."""
+    s = Scene()
+    s.name = "cornell_box"
+    white = s.add_material(diffuse(0.75))
+    red = s.add_material(diffuse(band_spectrum(0.75, 0.05, 23, 35)))
+    green = s.add_material(diffuse(band_spectrum(0.75, 0.05, 13, 19)))
+    light = s.add_material(area_light(10.0, reflectance=0.0))
+    boxes = s.add_material(diffuse(0.75))
+    # Walls with inward-facing winding normals.
+    s.add_mesh(*quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)), white)      # floor, +y
+    s.add_mesh(*quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)), white)      # ceiling, -y
+    s.add_mesh(*quad((0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1)), white)      # back, -z
+    s.add_mesh(*quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)), red)        # left x=0, +x
+    s.add_mesh(*quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)), green)      # right x=1, -x
+    q = 0.125
+    yl = 1.0 - 1e-4
+    s.add_mesh(*quad((0.5 - q, yl, 0.5 - q), (0.5 + q, yl, 0.5 - q), (0.5 + q, yl, 0.5 + q), (0.5 - q, yl, 0.5 + q)), light)
+    s.add_mesh(*box_mesh((0.3, 0.3, 0.3), (0.65, 0.0, 0.35), 17.0), boxes)
+    s.add_mesh(*box_mesh((0.3, 0.6, 0.3), (0.3, 0.0, 0.65), -17.0), boxes)
+    s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.5, 0.5, -1.4), dir=(0, 0, 1), up=(0, 1, 0),
+                          fov_deg=40.0, xres=xres, yres=yres)
+    return s
+
+
+def cornell_box_materials(xres=64, yres=64) -> Scene:
+    """The Cornell box with the tall box turned into glass and the small box into a
+    rough Beckmann metal plus a mirror back wall: exercises every shader."""
+    s = Scene()
+    s.name = "cornell_box_materials"
+    white = s.add_material(diffuse(0.75))
+    red = s.add_material(diffuse(band_spectrum(0.75, 0.05, 23, 35)))
+    green = s.add_material(diffuse(band_spectrum(0.75, 0.05, 13, 19)))
+    light = s.add_material(area_light(10.0, reflectance=0.0))
+    glass_m = s.add_material(glass(1.5))
+    metal = s.add_material(microfacet(rgb_to_spectrum((0.9, 0.7, 0.4)), 0.2))
+    mir = s.add_material(mirror(0.9))
+    s.add_mesh(*quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)), white)
+    s.add_mesh(*quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)), white)
+    s.add_mesh(*quad((0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1)), mir)
+    s.add_mesh(*quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)), red)
+    s.add_mesh(*quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)), green)
+    q = 0.125
+    yl = 1.0 - 1e-4
+    s.add_mesh(*quad((0.5 - q, yl, 0.5 - q), (0.5 + q, yl, 0.5 - q), (0.5 + q, yl, 0.5 + q), (0.5 - q, yl, 0.5 + q)), light)
+    s.add_mesh(*box_mesh((0.3, 0.3, 0.3), (0.65, 0.0, 0.35), 17.0), metal)
+    s.add_mesh(*box_mesh((0.3, 0.6, 0.3), (0.3, 0.0, 0.65), -17.0), glass_m)
+    s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.5, 0.5, -1.4), dir=(0, 0, 1), up=(0, 1, 0),
+                          fov_deg=40.0, xres=xres, yres=yres)
+    return s
+
+
+# --------------------------------------------------------------------------------------
+def icosphere(level: int):
+    """Unit icosphere: 20 * 4**level triangles, outward winding, shared vertices."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = np.array(v, dtype=np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    faces = np.array(f, dtype=np.int64)
+    for _ in range(level):
+        nv = len(verts)
+        e = np.concatenate([faces[:, [0, 1]], faces[:, [1, 2]], faces[:, [2, 0]]])
+        e.sort(axis=1)
+        keys = e[:, 0] * (nv + 1) + e[:, 1]
+        uniq, inv = np.unique(keys, return_inverse=True)
+        a = uniq // (nv + 1)
+        b = uniq % (nv + 1)
+        mid = verts[a] + verts[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        verts = np.concatenate([verts, mid])
+        nf = len(faces)
+        m01 = nv + inv[:nf]
+        m12 = nv + inv[nf:2 * nf]
+        m20 = nv + inv[2 * nf:]
+        v0, v1, v2 = faces[:, 0], faces[:, 1], faces[:, 2]
+        faces = np.concatenate([
+            np.stack([v0, m01, m20], 1), np.stack([v1, m12, m01], 1),
+            np.stack([v2, m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    return verts, faces.astype(np.uint32)
+
+
+def fbm_heightfield(n: int, octaves: int, rng: np.random.Generator) -> np.ndarray:
+    """n x n fractional Brownian motion from value noise: octave k has a (2^(k+2)+1)^2
+    random lattice interpolated bilinearly, amplitude 0.5^k; normalised to [-1, 1]."""
+    h = np.zeros((n, n))
+    xs = np.linspace(0.0, 1.0, n)
+    amp = 1.0
+    for k in range(octaves):
+        cells = 2 ** (k + 2)
+        lat = rng.uniform(-1.0, 1.0, size=(cells + 1, cells + 1))
+        g = xs * cells
+        i = np.minimum(g.astype(np.int64), cells - 1)
+        f = g - i
+        f = f * f * (3 - 2 * f)
+        a = lat[np.ix_(i, i)]
+        b = lat[np.ix_(i + 1, i)]
+        c = lat[np.ix_(i, i + 1)]
+        d = lat[np.ix_(i + 1, i + 1)]
+        fx = f[:, None]
+        fz = f[None, :]
+        h += amp * ((a * (1 - fx) + b * fx) * (1 - fz) + (c * (1 - fx) + d * fx) * fz)
+        amp *= 0.5
+    h -= h.min()
+    h /= max(h.max(), 1e-12)
+    return 2.0 * h - 1.0
+
+
+def sky_texture(width: int, height: int) -> np.ndarray:
+    """Equirect float32 RGB sky: deep blue at the zenith fading to a pale horizon, and a
+    dim ground below the horizon.  Row 0 is the zenith (EnvMapLight convention)."""
+    theta = (np.arange(height) + 0.5) / height * np.pi  # 0 = zenith
+    elev = np.pi / 2 - theta
+    tex = np.zeros((height, width, 3), dtype=np.float32)
+    zen = np.array([0.10, 0.25, 0.80])
+    hor = np.array([0.70, 0.80, 0.95])
+    gnd = np.array([0.25, 0.22, 0.20])
+    up = np.clip(elev / (np.pi / 2), 0, 1)[:, None]
+    col = np.where(elev[:, None] >= 0, hor * (1 - up) + zen * up, gnd * np.ones_like(up))
+    tex[:] = col[:, None, :].astype(np.float32)
+    return tex
+
+
+def terrain_spheres(xres=1920, yres=1080, terrain_n=1024, sphere_level=5, num_spheres=32,
+                    env_w=2048, env_h=1024, seed=1) -> Scene:
+    rng = np.random.default_rng(seed)
+    s = Scene()
+    s.name = "terrain_spheres"
+    extent = 10.0
+    amp = 0.2
+    hf = amp * fbm_heightfield(terrain_n, 6, rng)
+    xs = np.linspace(-extent / 2, extent / 2, terrain_n)
+    X, Z = np.meshgrid(xs, xs, indexing="ij")
+    verts = np.stack([X, hf, Z], axis=-1).reshape(-1, 3)
+    # Smooth normals from central differences.
+    dx = extent / (terrain_n - 1)
+    gx = np.gradient(hf, dx, axis=0)
+    gz = np.gradient(hf, dx, axis=1)
+    nrm = np.stack([-gx, np.ones_like(hf), -gz], axis=-1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    idx = np.arange(terrain_n * terrain_n, dtype=np.int64).reshape(terrain_n, terrain_n)
+    a = idx[:-1, :-1].ravel()
+    b = idx[1:, :-1].ravel()
+    c = idx[1:, 1:].ravel()
+    d = idx[:-1, 1:].ravel()
+    # Upward winding: (b - a) x (c - a) has +y for x increasing along i, z along j.
+    tris = np.concatenate([np.stack([a, d, c], 1), np.stack([a, c, b], 1)]).astype(np.uint32)
+    ground = s.add_material(diffuse(rgb_to_spectrum((0.35, 0.30, 0.22))))
+    s.add_mesh(verts, tris, ground, normals=nrm.reshape(-1, 3))
+    sv, sf = icosphere(sphere_level)
+    kinds = np.array([0] * 13 + [1] * 10 + [2] * 9)[:num_spheres]
+    rng.shuffle(kinds)
+    for k in range(num_spheres):
+        r = rng.uniform(0.1, 0.4)
+        px, pz = rng.uniform(-4.0, 4.0, size=2)
+        i = int(round((px + extent / 2) / dx))
+        j = int(round((pz + extent / 2) / dx))
+        py = hf[min(max(i, 0), terrain_n - 1), min(max(j, 0), terrain_n - 1)] + r
+        if kinds[k] == 0:
+            alb = rng.uniform(0.2, 0.8, size=3)
+            m = s.add_material(diffuse(rgb_to_spectrum(alb)))
+        elif kinds[k] == 1:
+            rough = rng.uniform(0.05, 0.5)
+            tint = rng.uniform(0.5, 0.95, size=3)
+            m = s.add_material(microfacet(rgb_to_spectrum(tint), rough))
+        else:
+            m = s.add_material(glass(1.5))
+        s.add_mesh(sv * r + np.array([px, py, pz]), sf, m, normals=sv)
+    s.env_lights.append(env_map(sky_texture(env_w, env_h), up=(0.0, 1.0, 0.0)))
+    elev = math.radians(35.0)
+    az = math.radians(30.0)
+    dir_out = (-math.cos(elev) * math.cos(az), -math.sin(elev), -math.cos(elev) * math.sin(az))
+    s.env_lights.append(sun_light(100.0, dir_out, 0.265))
+    s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.0, 2.2, -6.5), dir=(0.0, -0.3, 1.0), up=(0, 1, 0),
+                          fov_deg=60.0, xres=xres, yres=yres)
+    return s
+
+
+def terrain_spheres_small(xres=96, yres=54) -> Scene:
+    """Scaled-down terrain scene (same generator) for parity tests."""
+    return terrain_spheres(xres=xres, yres=yres, terrain_n=64, sphere_level=2, num_spheres=8, env_w=128, env_h=64)

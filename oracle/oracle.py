@@ -1,0 +1,170 @@
+"""ORACLE -- test infrastructure only.
+
+ctypes binding of the CPU double-precision restatement (tt_oracle.cpp) of ToyTrace's
+forward path tracer.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+may use it, as the checker; the product path never calls it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libtt_oracle.so"
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    lib = C.CDLL(str(LIB))
+    P = C.POINTER
+    d = P(C.c_double)
+    i32 = P(C.c_int32)
+    vp = C.c_void_p
+    sig = {
+        "or_create": ([vp, vp], vp),
+        "or_destroy": ([vp], None),
+        "or_last_error": ([], C.c_char_p),
+        "or_intersect": ([vp, d, C.c_int, C.c_int, i32, d, d, d], C.c_int),
+        "or_occluded": ([vp, d, C.c_int, P(C.c_uint8)], C.c_int),
+        "or_render": ([vp, C.c_int, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, d, d, P(C.c_uint64)], C.c_int),
+        "or_sample_bsdf": ([vp, C.c_int, d, i32, C.c_int, C.c_uint64, d, d, d], C.c_int),
+        "or_eval_bsdf": ([vp, C.c_int, d, i32, d, C.c_int, d, d], C.c_int),
+        "or_rgb_to_spectrum": ([d, d], None),
+        "or_spectrum_to_rgb": ([d, d], None),
+        "or_selection_to_rgb": ([d, i32, d], None),
+        "or_rgb_to_selection": ([d, i32, d], None),
+        "or_reflected": ([d, d, d], None),
+        "or_refracted": ([d, d, C.c_double, d], C.c_int),
+        "or_half_vector": ([d, d, d], None),
+        "or_half_vector_refracted": ([d, d, C.c_double, d], C.c_int),
+        "or_fresnel": ([C.c_double, C.c_double], C.c_double),
+        "or_pcg32_stream": ([C.c_uint64, C.c_uint64, C.c_int, P(C.c_uint32)], None),
+        "or_pcg32_nextdouble_first": ([C.c_uint64, C.c_uint64], C.c_double),
+        "or_uniform_int_stream": ([C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.c_int, i32], C.c_int),
+        "or_tables": ([d, d, d], None),
+        "or_eval_env": ([vp, d, i32, d, d], C.c_int),
+        "or_scene_info": ([vp, d, i32], C.c_int),
+    }
+    for name, (a, r) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = a
+        fn.restype = r
+    _lib = lib
+    return lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
+class OracleScene:
+    """CPU restatement bound to one scene (the same tt_scene_desc the GPU library takes)."""
+
+    def __init__(self, scene, params):
+        self.lib = load()
+        desc, keep = scene.to_desc()
+        self._keep = keep
+        self.scene = scene
+        self.params = params
+        self.h = self.lib.or_create(C.byref(desc), C.byref(params))
+        if not self.h:
+            raise RuntimeError("oracle rejected scene: " + self.lib.or_last_error().decode())
+        self.npix = scene.camera.xres * scene.camera.yres
+
+    def close(self):
+        if self.h:
+            self.lib.or_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def intersect(self, rays: np.ndarray, brute_force: bool = False):
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 8)
+        n = len(rays)
+        prim = np.zeros(n, np.int32)
+        t = np.zeros(n)
+        u = np.zeros(n)
+        v = np.zeros(n)
+        self.lib.or_intersect(self.h, _dp(rays), n, int(brute_force), _ip(prim), _dp(t), _dp(u), _dp(v))
+        return prim, t, u, v
+
+    def occluded(self, rays: np.ndarray):
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 8)
+        out = np.zeros(len(rays), np.uint8)
+        self.lib.or_occluded(self.h, _dp(rays), len(rays), out.ctypes.data_as(C.POINTER(C.c_uint8)))
+        return out.astype(bool)
+
+    def render(self, spp: int, seed: int = 1, sample_offset: int = 0, pixel_begin: int = 0, pixel_end=None,
+               nthreads: int = 0, accum=None, light_accum=None):
+        """Returns (accum, light_accum, splat_count) after adding spp samples per pixel."""
+        if pixel_end is None:
+            pixel_end = self.npix
+        accum = np.zeros(3 * self.npix) if accum is None else accum
+        light = np.zeros(3 * self.npix) if light_accum is None else light_accum
+        cnt = C.c_uint64(0)
+        rc = self.lib.or_render(self.h, spp, seed, sample_offset, pixel_begin, pixel_end, nthreads, _dp(accum),
+                                _dp(light), C.byref(cnt))
+        if rc != 0:
+            raise RuntimeError(self.lib.or_last_error().decode())
+        return accum, light, cnt.value
+
+    def sample_bsdf(self, material: int, wi, lambda_idx, n: int, seed: int):
+        wi = np.ascontiguousarray(wi, dtype=np.float64)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        d = np.zeros((n, 3))
+        val = np.zeros((n, 3))
+        pdf = np.zeros(n)
+        self.lib.or_sample_bsdf(self.h, material, _dp(wi), _ip(li), n, seed, _dp(d), _dp(val), _dp(pdf))
+        return d, val, pdf
+
+    def eval_bsdf(self, material: int, wi, lambda_idx, dirs):
+        wi = np.ascontiguousarray(wi, dtype=np.float64)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        n = len(dirs)
+        val = np.zeros((n, 3))
+        pdf = np.zeros(n)
+        self.lib.or_eval_bsdf(self.h, material, _dp(wi), _ip(li), _dp(dirs), n, _dp(val), _dp(pdf))
+        return val, pdf
+
+    def eval_env(self, dir_out, lambda_idx):
+        d = np.ascontiguousarray(dir_out, dtype=np.float64)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        val = np.zeros(3)
+        pdf = C.c_double(0)
+        self.lib.or_eval_env(self.h, _dp(d), _ip(li), _dp(val), C.byref(pdf))
+        return val, pdf.value
+
+    def info(self):
+        bb = np.zeros(6)
+        cnt = np.zeros(4, np.int32)
+        self.lib.or_scene_info(self.h, _dp(bb), _ip(cnt))
+        return bb, cnt
+
+
+def combine(accum, light, samples_per_pixel, splat_count, npix):
+    """Spectral3ImageBuffer::ToImage before the clamp (renderbuffer.hxx:172-200)."""
+    w = npix / splat_count if splat_count > 0 else 0.0
+    return accum / samples_per_pixel + w * light

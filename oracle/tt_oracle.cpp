@@ -1,0 +1,1695 @@
+// ORACLE -- test infrastructure only (see tt_oracle.h).
+//
+// A CPU, double-precision restatement of ToyTrace's forward path tracer with next-event
+// estimation (`--algo pt`).  Each function names the reference code it restates; paths
+// are relative to the reference project root.  Geometry is single precision as in the
+// reference (Mesh stores float vertices, primitive.hxx:62-72); everything else is double.
+//
+// Random numbers: the reference draws from two default-seeded PCG32 generators per
+// worker (Sampler's sequence and its RandGen, sampler.hxx:93-121), so its streams are not
+// reproducible per pixel.  Here every path owns one PCG32 stream, seeded with
+// (seed, sample_index * num_pixels + pixel), and draws happen in the reference's call
+// order.  The CUDA tracer uses the same streams, which makes per-path comparison possible.
+#include "tt_oracle.h"
+#include "../naivetrace_b200/csrc/tt_tables.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+constexpr double Pi = 3.14159265358979323846264338327950288;
+constexpr double Eps = std::numeric_limits<double>::epsilon();        // vec3f.hxx:15
+constexpr float EpsF = std::numeric_limits<float>::epsilon();         // vec3f.hxx:16
+constexpr double LargeNumber = std::numeric_limits<double>::max() / 16;  // vec3f.hxx:22
+constexpr int NBINS = 36;
+
+static thread_local std::string g_err;
+
+struct V3 {
+  double x = 0, y = 0, z = 0;
+  V3() = default;
+  V3(double a, double b, double c) : x(a), y(b), z(c) {}
+  double operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+  double& operator[](int i) { return i == 0 ? x : (i == 1 ? y : z); }
+};
+inline V3 operator+(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator-(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator-(V3 a) { return {-a.x, -a.y, -a.z}; }
+inline V3 operator*(double s, V3 a) { return {s * a.x, s * a.y, s * a.z}; }
+inline V3 operator*(V3 a, double s) { return {s * a.x, s * a.y, s * a.z}; }
+inline V3 operator/(V3 a, double s) { return {a.x / s, a.y / s, a.z / s}; }
+inline double Dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 Cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double Length(V3 a) { return std::sqrt(Dot(a, a)); }
+inline V3 Normalized(V3 a) { return a / Length(a); }
+inline V3 Abs(V3 a) { return {std::abs(a.x), std::abs(a.y), std::abs(a.z)}; }
+inline double Sqr(double a) { return a * a; }
+inline double Sign(double x) { return std::copysign(1.0, x); }  // util.hxx:116-119
+
+struct F3 { float x, y, z; };
+inline F3 Ff(V3 a) { return {(float)a.x, (float)a.y, (float)a.z}; }
+
+struct S3 {
+  double v[3] = {0, 0, 0};
+  S3() = default;
+  explicit S3(double a) { v[0] = v[1] = v[2] = a; }
+  S3(double a, double b, double c) { v[0] = a; v[1] = b; v[2] = c; }
+  double& operator[](int i) { return v[i]; }
+  double operator[](int i) const { return v[i]; }
+  bool IsZero() const { return v[0] == 0 && v[1] == 0 && v[2] == 0; }
+  double Max() const { return std::max(v[0], std::max(v[1], v[2])); }
+};
+inline S3 operator*(S3 a, S3 b) { return {a[0] * b[0], a[1] * b[1], a[2] * b[2]}; }
+inline S3 operator*(double s, S3 a) { return {s * a[0], s * a[1], s * a[2]}; }
+inline S3 operator*(S3 a, double s) { return {s * a[0], s * a[1], s * a[2]}; }
+inline S3 operator/(S3 a, double s) { return {a[0] / s, a[1] / s, a[2] / s}; }
+inline S3 operator+(S3 a, S3 b) { return {a[0] + b[0], a[1] + b[1], a[2] + b[2]}; }
+
+// Listing 3 of Duff et al. (2017), as used by OrthogonalSystemZAligned (vec3f.hxx:240-258).
+// Columns X, Y, Z.
+struct Frame {
+  V3 X, Y, Z;
+  V3 ToWorld(V3 v) const { return X * v.x + Y * v.y + Z * v.z; }
+  V3 ToLocal(V3 w) const { return {Dot(X, w), Dot(Y, w), Dot(Z, w)}; }
+};
+inline Frame OrthogonalSystemZAligned(V3 z) {
+  Frame f;
+  f.Z = z;
+  const double sign = std::copysign(1.0, z.z);
+  const double a = -1.0 / (sign + z.z);
+  const double b = z.x * z.y * a;
+  f.X = {1.0 + sign * z.x * z.x * a, sign * b, -sign * z.x};
+  f.Y = {b, sign + z.y * z.y * a, -z.y};
+  return f;
+}
+
+// ---------------------------------------------------------------------------------------
+// PCG32 (O'Neill 2014), with the interface of the pcg32 submodule the reference uses
+// (RandGen, sampler.cxx:366-393): seed(initstate, initseq), nextUInt, nextDouble
+// (32 random bits in the mantissa), nextUInt(bound) with rejection of the biased range.
+struct Pcg32 {
+  uint64_t state = 0x853c49e6748fea9bULL, inc = 0xda3e39cb94b95bdbULL;
+  void Seed(uint64_t initstate, uint64_t initseq) {
+    state = 0u;
+    inc = (initseq << 1u) | 1u;
+    NextUInt();
+    state += initstate;
+    NextUInt();
+  }
+  uint32_t NextUInt() {
+    uint64_t old = state;
+    state = old * 6364136223846793005ULL + inc;
+    uint32_t xorshifted = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    uint32_t rot = (uint32_t)(old >> 59u);
+    return (xorshifted >> rot) | (xorshifted << ((~rot + 1u) & 31));
+  }
+  double NextDouble() { return (double)NextUInt() * (1.0 / 4294967296.0); }
+  uint32_t NextBounded(uint32_t bound) {
+    uint32_t threshold = (~bound + 1u) % bound;
+    for (;;) {
+      uint32_t r = NextUInt();
+      if (r >= threshold) return r % bound;
+    }
+  }
+};
+
+// One stream per path; Uniform01 / UniformUnitSquare / UniformInt as Sampler and RandGen.
+struct Sampler {
+  Pcg32 g;
+  double Uniform01() { return g.NextDouble(); }
+  void UniformUnitSquare(double r[2]) { r[0] = g.NextDouble(); r[1] = g.NextDouble(); }
+  int UniformInt(int a, int b_inclusive) {  // RandGen::UniformInt, sampler.cxx:384-391
+    return a + (int)g.NextBounded((uint32_t)(b_inclusive + 1 - a));
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+// Warps, sampler.cxx:6-124.
+inline V3 ToUniformSphere(const double r[2]) {
+  double z = 1. - 2. * r[1];
+  double s = std::sqrt(r[1] * (1. - r[1]));
+  double omega = 2. * Pi * r[0];
+  return {2. * std::cos(omega) * s, 2. * std::sin(omega) * s, z};
+}
+inline V3 ToUniformHemisphere(const double r[2]) {
+  V3 v = ToUniformSphere(r);
+  v.z = v.z >= 0. ? v.z : -v.z;
+  return v;
+}
+inline V3 ToUniformSphereSection(double cos_opening, const double r[2]) {
+  double z = 1. - r[1] * (1. - cos_opening);
+  double s = std::sqrt(1. - z * z);
+  double omega = 2. * Pi * r[0];
+  return {std::cos(omega) * s, std::sin(omega) * s, z};
+}
+inline V3 ToUniformSphereSection(const double r[2], double phi0, double z0, double phi1, double z1) {
+  const double z = z0 + r[1] * (z1 - z0);
+  double s = std::sqrt(1. - z * z);
+  s = std::isnan(s) ? 0. : s;
+  double omega = phi0 + (phi1 - phi0) * r[0];
+  return {std::cos(omega) * s, std::sin(omega) * s, z};
+}
+inline V3 ToCosHemisphere(const double r[2]) {
+  double rho = std::sqrt(1. - r[0]);
+  double z = std::sqrt(r[0]);
+  double omega = 2. * Pi * r[1];
+  return {std::cos(omega) * rho, std::sin(omega) * rho, z};
+}
+inline V3 ToTriangleBarycentricCoords(const double r[2]) {
+  double s = std::sqrt(r[0]);
+  return {1. - s, (1. - r[1]) * s, r[1] * s};
+}
+inline V3 ToUniformDisc(const double r[2]) {
+  double s = std::sqrt(r[1]);
+  double omega = 2. * Pi * r[0];
+  return {s * std::cos(omega), s * std::sin(omega), 0};
+}
+// sampler.hxx:133-144
+inline double PowerHeuristic(double p, double other) {
+  double pp = p * p;
+  return pp / (pp + other * other + Eps);
+}
+// sampler.hxx:147-166
+inline int TowerSampling4(const double* probs, double r) {
+  int n = 3;
+  while (r >= probs[n] && n > 0) { r -= probs[n]; --n; }
+  return n;
+}
+// sampler.hxx:169-205 (float CMFs of the env map)
+inline int TowerSamplingBisection(const float* cmf, int size, float r) {
+  int upper;
+  if (r < cmf[0]) upper = 0;
+  else if (r >= cmf[size - 1]) upper = size;
+  else {
+    int first = 0, last = size - 1;
+    while (last > first + 1) {
+      int center = (first + last) / 2;
+      if (r < cmf[center]) last = center; else first = center;
+    }
+    upper = last;
+  }
+  return upper >= size ? size - 1 : upper;
+}
+inline float ProbFromCmf(const float* cmf, int idx) { return cmf[idx] - (idx > 0 ? cmf[idx - 1] : 0.f); }
+
+// ---------------------------------------------------------------------------------------
+// Spectral, spectral.cxx:81-140.
+inline void LinComb3(double* dst, double a, const double* sa, double b, const double* sb, double c,
+                     const double* sc, const int32_t* idx) {
+  for (int i = 0; i < 3; ++i) dst[i] = a * sa[idx[i]] + b * sb[idx[i]] + c * sc[idx[i]];
+}
+inline void LinCombN(double* dst, double a, const double* sa, double b, const double* sb, double c,
+                     const double* sc) {
+  for (int i = 0; i < NBINS; ++i) dst[i] = a * sa[i] + b * sb[i] + c * sc[i];
+}
+// Smits' case split (spectral.cxx:81-115) over either all bins or a selection.
+template <class F>
+inline void SmitsCases(double red, double green, double blue, F lincomb) {
+  if (red <= green && red <= blue) {
+    if (green <= blue) lincomb(red, TT_SMITS_WHITE, green - red, TT_SMITS_CYAN, blue - green, TT_SMITS_BLUE);
+    else lincomb(red, TT_SMITS_WHITE, blue - red, TT_SMITS_CYAN, green - blue, TT_SMITS_GREEN);
+  } else if (green <= red && green <= blue) {
+    if (red <= blue) lincomb(green, TT_SMITS_WHITE, red - green, TT_SMITS_MAGENTA, blue - red, TT_SMITS_BLUE);
+    else lincomb(green, TT_SMITS_WHITE, blue - green, TT_SMITS_MAGENTA, red - blue, TT_SMITS_RED);
+  } else {
+    if (red <= green) lincomb(blue, TT_SMITS_WHITE, red - blue, TT_SMITS_YELLOW, green - red, TT_SMITS_GREEN);
+    else lincomb(blue, TT_SMITS_WHITE, green - blue, TT_SMITS_YELLOW, red - green, TT_SMITS_RED);
+  }
+}
+inline S3 RGBToSpectralSelection(const double rgb[3], const int32_t idx[3]) {
+  S3 ret;
+  SmitsCases(rgb[0], rgb[1], rgb[2], [&](double a, int ia, double b, int ib, double c, int ic) {
+    LinComb3(ret.v, a, kSmitsBasis[ia], b, kSmitsBasis[ib], c, kSmitsBasis[ic], idx);
+  });
+  return ret;
+}
+inline void SpectralSelectionToRGB(const S3& val, const int32_t idx[3], double rgb[3]) {
+  for (int i = 0; i < 3; ++i) {
+    rgb[i] = 0;
+    for (int j = 0; j < 3; ++j) rgb[i] += val[j] * kSpectrumToRgb[i][idx[j]];
+  }
+}
+inline S3 Take(const float* spec, const int32_t idx[3]) { return {spec[idx[0]], spec[idx[1]], spec[idx[2]]}; }
+inline S3 TakeD(const double* spec, const int32_t idx[3]) { return {spec[idx[0]], spec[idx[1]], spec[idx[2]]}; }
+
+// ---------------------------------------------------------------------------------------
+// Reflection/refraction, shader_physics.hxx:10-148.
+inline V3 Reflected(V3 wi, V3 n) { return 2. * Dot(wi, n) * n - wi; }
+inline bool Refracted(V3 wi, V3 m, double eta, V3* out) {
+  const double c = Dot(m, wi);
+  const double t1 = 1. - c * c;
+  const double t2 = 1.0 - eta * eta * t1;
+  if (t2 < 0.) return false;
+  const double s = Dot(wi, m) >= 0. ? 1.0 : -1.0;
+  const double t3 = std::sqrt(t2);
+  *out = (eta * c - s * t3) * m - eta * wi;
+  return true;
+}
+inline V3 HalfVector(V3 wi, V3 wo) {
+  V3 ret = wo + wi;
+  double norm = Length(ret);
+  if (norm > 0) return ret / norm;
+  return OrthogonalSystemZAligned(wi).X;
+}
+inline bool HalfVectorRefracted(V3 wi, V3 wo, double eta, V3* out) {
+  V3 ret = -(eta * wi + wo);
+  double norm = Length(ret);
+  if (norm > 0) ret = ret / norm; else ret = wi;
+  if (Dot(ret, wi) * Dot(ret, wo) < 0.) { *out = ret; return true; }
+  return false;
+}
+inline double HalfVectorPdfToReflectedPdf(double pdf_wh, double wh_dot_in) {
+  return pdf_wh * 0.25 / (std::abs(wh_dot_in) + Eps);
+}
+inline double FresnelReflectivity(double cs_i, double cs_t, double eta) {
+  double rs_nom = eta * cs_i - cs_t, rs_den = eta * cs_i + cs_t;
+  double rp_nom = eta * cs_t - cs_i, rp_den = eta * cs_t + cs_i;
+  return 0.5 * (Sqr(rs_nom / rs_den) + Sqr(rp_nom / rp_den));
+}
+inline double FresnelReflectivityWalter(double cos_n_wi, double eta) {
+  double c = std::abs(cos_n_wi);
+  double tmp = Sqr(1.0 / eta) - 1.0 + c * c;
+  if (tmp < 0.) return 1.;
+  double g = std::sqrt(tmp);
+  if ((g == 0.) & (c == 0.)) return 1.;
+  double nom = c * (g + c) - 1.;
+  double denom = c * (g - c) + 1.;
+  return 0.5 * Sqr((g - c) / (g + c)) * (1. + Sqr(nom / denom));
+}
+
+// Beckmann NDF, G terms and VNDF selection, normaldistributionfunction.hxx:8-127.
+struct Beckman {
+  double alpha;
+  double EvalByHalfVector(double cs) const {
+    if (cs <= 0.) return 0.;
+    const double t1 = (cs * cs - 1.) / (cs * cs * alpha * alpha);
+    const double t2 = alpha * alpha * cs * cs * cs * cs * Pi;
+    return std::exp(t1) / t2;
+  }
+  V3 SampleHalfVector(const double r[2]) const {
+    const double t1 = -alpha * alpha * std::log(r[0]);
+    const double t = 1 / (t1 + 1);
+    const double z = std::sqrt(t);
+    const double rho = std::sqrt(1 - t);
+    const double omega = 2 * Pi * r[1];
+    return {std::cos(omega) * rho, std::sin(omega) * rho, z};
+  }
+};
+inline double G1VCavity(double cos_v_m, double cos_v_n, double cos_n_m) {
+  if (cos_v_m * cos_v_n < 0.) return 0.;
+  return std::min(1., 2. * std::abs(cos_n_m * cos_v_n) / (std::abs(cos_v_m) + Eps));
+}
+inline double G2VCavity(double wh_dot_in, double wh_dot_out, double ns_dot_in, double ns_dot_out, double ns_dot_wh) {
+  return std::min(G1VCavity(wh_dot_in, ns_dot_in, ns_dot_wh), G1VCavity(wh_dot_out, ns_dot_out, ns_dot_wh));
+}
+inline double ClampDot(V3 a, V3 b) { return std::max(0., Dot(a, b)); }
+constexpr double WI_BELOW_HORIZON_FIX_FACTOR = 1.e-6;
+inline void VndfSample(V3& wh, V3 wi, double r) {
+  V3 whp{-wh.x, -wh.y, wh.z};
+  double prob = ClampDot(wi, whp) / (ClampDot(wi, wh) + ClampDot(wi, whp) + WI_BELOW_HORIZON_FIX_FACTOR);
+  if (r < prob) wh = whp;
+}
+inline double VndfPdf(double ndf_val, V3 wh, V3 wi) {
+  V3 whp{-wh.x, -wh.y, wh.z};
+  const double a = ClampDot(wi, whp);
+  const double b = ClampDot(wh, wi);
+  const double prob = (2. * b + WI_BELOW_HORIZON_FIX_FACTOR) / (b + a + WI_BELOW_HORIZON_FIX_FACTOR);
+  return ndf_val * std::abs(wh.z) * prob;
+}
+
+// ---------------------------------------------------------------------------------------
+// Surface interaction, scene.hxx:77-95, scene.cxx:229-261.
+struct Surf {
+  int prim = -1;
+  V3 barry;            // HitId::barry
+  V3 pos;
+  V3 geometry_normal;  // raw winding normal
+  V3 smooth_normal;
+  V3 normal;           // oriented toward where the incident ray came from
+  V3 shading_normal;
+  V3 pos_bounds;
+};
+
+inline V3 AntiSelfIntersectionOffset(const Surf& s, V3 exitant_dir) {
+  const V3 n = s.geometry_normal;
+  const double delta = Dot(s.pos_bounds, Abs(n));
+  return delta * (Dot(exitant_dir, n) > 0. ? 1. : -1.) * n;
+}
+
+// util::Gamma<float>(7), util.hxx:124-127 (note: uses the full float epsilon).
+inline double Gamma7() { return (7 * (double)EpsF) / (1 - 7 * (double)EpsF); }
+
+struct EnvLight {
+  int kind;
+  double spectrum[NBINS];
+  V3 dir;
+  double scalar, scalar2;
+  // Sun
+  Frame frame;
+  double cos_opening, pdf_val;
+  double sun_emission[NBINS];
+  // Dome
+  V3 down_dir;
+  // Env map (float data as in EnvMapLight, light.cxx:88-189)
+  int w = 0, h = 0;
+  std::vector<float> tex;
+  std::vector<float> cmf_rows, cmf_cols;
+  float fX[3], fY[3], fZ[3];  // float frame columns
+};
+
+struct Material {
+  tt_material m;
+};
+
+struct Camera {
+  int kind;
+  V3 pos, up, dir, right;
+  int xres, yres;
+  double xmin, ymin, xperpixel, yperpixel;
+  double per_pixel_delta;
+};
+
+// ---------------------------------------------------------------------------------------
+// BVH over triangles for the oracle's own closest-hit / occlusion queries.  Binned SAH,
+// double-precision slab and watertight triangle tests (Woop, Benthin, Wald 2013).
+struct BNode {
+  double lo[3], hi[3];
+  int left = -1, right = -1, start = 0, count = 0;
+};
+
+struct Scene {
+  std::vector<V3> tv0, tv1, tv2;   // triangle vertices as double (from float)
+  std::vector<F3> vert, nrm;
+  std::vector<uint32_t> idx, mat_of_tri;
+  bool has_normals = false;
+  std::vector<Material> materials;
+  std::vector<EnvLight> env;
+  std::vector<tt_point_light> points;
+  std::vector<int> area_lights;    // global triangle index per area light number
+  Camera cam;
+  double bb_lo[3], bb_hi[3];
+  double diag = 0, long_distance = 0;
+  V3 box_center;
+  double type_probs[4];            // ENV, AREA, POINT, VOLUME (light.hxx:322-326)
+  double in_class[4];
+  tt_params params;
+  std::vector<BNode> nodes;
+  std::vector<int> tri_order;
+};
+
+inline void TriBounds(const Scene& s, int t, double lo[3], double hi[3]) {
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = std::min(s.tv0[t][k], std::min(s.tv1[t][k], s.tv2[t][k]));
+    hi[k] = std::max(s.tv0[t][k], std::max(s.tv1[t][k], s.tv2[t][k]));
+  }
+}
+
+static double HalfArea(const double lo[3], const double hi[3]) {
+  double d0 = hi[0] - lo[0], d1 = hi[1] - lo[1], d2 = hi[2] - lo[2];
+  if (d0 < 0 || d1 < 0 || d2 < 0) return 0;
+  return d0 * d1 + d1 * d2 + d2 * d0;
+}
+
+static void BuildBvh(Scene& s) {
+  const int n = (int)s.tv0.size();
+  s.tri_order.resize(n);
+  std::vector<double> cen(3 * (size_t)n), blo(3 * (size_t)n), bhi(3 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    s.tri_order[i] = i;
+    TriBounds(s, i, &blo[3 * i], &bhi[3 * i]);
+    for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5 * (blo[3 * i + k] + bhi[3 * i + k]);
+  }
+  s.nodes.clear();
+  s.nodes.reserve(2 * (size_t)std::max(n, 1));
+  struct Task { int node, start, count; };
+  std::vector<Task> stack;
+  s.nodes.push_back(BNode{});
+  stack.push_back({0, 0, n});
+  constexpr int NB = 16;
+  while (!stack.empty()) {
+    Task t = stack.back();
+    stack.pop_back();
+    BNode& nd = s.nodes[t.node];
+    double clo[3] = {1e300, 1e300, 1e300}, chi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < 3; ++k) { nd.lo[k] = 1e300; nd.hi[k] = -1e300; }
+    for (int i = t.start; i < t.start + t.count; ++i) {
+      int tri = s.tri_order[i];
+      for (int k = 0; k < 3; ++k) {
+        nd.lo[k] = std::min(nd.lo[k], blo[3 * tri + k]);
+        nd.hi[k] = std::max(nd.hi[k], bhi[3 * tri + k]);
+        clo[k] = std::min(clo[k], cen[3 * tri + k]);
+        chi[k] = std::max(chi[k], cen[3 * tri + k]);
+      }
+    }
+    if (t.count <= 4) { nd.start = t.start; nd.count = t.count; continue; }
+    int best_axis = -1, best_split = -1;
+    double best_cost = 1e300;
+    for (int axis = 0; axis < 3; ++axis) {
+      double ext = chi[axis] - clo[axis];
+      if (ext <= 0) continue;
+      int cnt[NB] = {0};
+      double bl[NB][3], bh[NB][3];
+      for (int b = 0; b < NB; ++b)
+        for (int k = 0; k < 3; ++k) { bl[b][k] = 1e300; bh[b][k] = -1e300; }
+      for (int i = t.start; i < t.start + t.count; ++i) {
+        int tri = s.tri_order[i];
+        int b = std::min(NB - 1, (int)(NB * (cen[3 * tri + axis] - clo[axis]) / ext));
+        cnt[b]++;
+        for (int k = 0; k < 3; ++k) {
+          bl[b][k] = std::min(bl[b][k], blo[3 * tri + k]);
+          bh[b][k] = std::max(bh[b][k], bhi[3 * tri + k]);
+        }
+      }
+      double rl[NB][3], rh[NB][3];
+      int rc[NB];
+      double al[3] = {1e300, 1e300, 1e300}, ah[3] = {-1e300, -1e300, -1e300};
+      int ac = 0;
+      for (int b = NB - 1; b >= 1; --b) {
+        for (int k = 0; k < 3; ++k) { al[k] = std::min(al[k], bl[b][k]); ah[k] = std::max(ah[k], bh[b][k]); }
+        ac += cnt[b];
+        for (int k = 0; k < 3; ++k) { rl[b][k] = al[k]; rh[b][k] = ah[k]; }
+        rc[b] = ac;
+      }
+      for (int k = 0; k < 3; ++k) { al[k] = 1e300; ah[k] = -1e300; }
+      ac = 0;
+      for (int b = 0; b < NB - 1; ++b) {
+        for (int k = 0; k < 3; ++k) { al[k] = std::min(al[k], bl[b][k]); ah[k] = std::max(ah[k], bh[b][k]); }
+        ac += cnt[b];
+        if (ac == 0 || rc[b + 1] == 0) continue;
+        double cost = ac * HalfArea(al, ah) + rc[b + 1] * HalfArea(rl[b + 1], rh[b + 1]);
+        if (cost < best_cost) { best_cost = cost; best_axis = axis; best_split = b; }
+      }
+    }
+    int mid;
+    if (best_axis < 0) {
+      mid = t.start + t.count / 2;  // all centroids coincide: split by count
+    } else {
+      double ext = chi[best_axis] - clo[best_axis];
+      auto it = std::partition(s.tri_order.begin() + t.start, s.tri_order.begin() + t.start + t.count, [&](int tri) {
+        int b = std::min(NB - 1, (int)(NB * (cen[3 * tri + best_axis] - clo[best_axis]) / ext));
+        return b <= best_split;
+      });
+      mid = (int)(it - s.tri_order.begin());
+      if (mid == t.start || mid == t.start + t.count) mid = t.start + t.count / 2;
+    }
+    int l = (int)s.nodes.size();
+    s.nodes.push_back(BNode{});
+    s.nodes.push_back(BNode{});
+    s.nodes[t.node].left = l;
+    s.nodes[t.node].right = l + 1;
+    stack.push_back({l, t.start, mid - t.start});
+    stack.push_back({l + 1, mid, t.start + t.count - mid});
+  }
+}
+
+// Watertight ray/triangle test (Woop et al. 2013) in double precision.  Returns true with
+// t in (tnear, tfar] and barycentrics (b1, b2) = Embree's (u, v).
+inline bool IntersectTri(V3 org, V3 dir, V3 v0, V3 v1, V3 v2, double tnear, double tfar, double* tout,
+                         double* uout, double* vout) {
+  int kz = 0;
+  double ad[3] = {std::abs(dir.x), std::abs(dir.y), std::abs(dir.z)};
+  if (ad[1] > ad[kz]) kz = 1;
+  if (ad[2] > ad[kz]) kz = 2;
+  int kx = (kz + 1) % 3, ky = (kx + 1) % 3;
+  if (dir[kz] < 0) std::swap(kx, ky);
+  const double Sx = dir[kx] / dir[kz], Sy = dir[ky] / dir[kz], Sz = 1.0 / dir[kz];
+  const V3 A = v0 - org, B = v1 - org, C = v2 - org;
+  const double Ax = A[kx] - Sx * A[kz], Ay = A[ky] - Sy * A[kz];
+  const double Bx = B[kx] - Sx * B[kz], By = B[ky] - Sy * B[kz];
+  const double Cx = C[kx] - Sx * C[kz], Cy = C[ky] - Sy * C[kz];
+  const double U = Cx * By - Cy * Bx;
+  const double V = Ax * Cy - Ay * Cx;
+  const double W = Bx * Ay - By * Ax;
+  if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
+  const double det = U + V + W;
+  if (det == 0) return false;
+  const double T = U * (Sz * A[kz]) + V * (Sz * B[kz]) + W * (Sz * C[kz]);
+  const double t = T / det;
+  if (!(t > tnear && t <= tfar)) return false;
+  *tout = t;
+  *uout = V / det;
+  *vout = W / det;
+  return true;
+}
+
+inline bool SlabHit(const BNode& nd, V3 org, V3 inv, double tnear, double tfar, double* tentry) {
+  double t0 = tnear, t1 = tfar;
+  for (int k = 0; k < 3; ++k) {
+    double a = (nd.lo[k] - org[k]) * inv[k];
+    double b = (nd.hi[k] - org[k]) * inv[k];
+    if (a > b) std::swap(a, b);
+    // NaN-safe: 0 * inf
+    if (!(a <= b)) { a = -1e300; b = 1e300; }
+    t0 = std::max(t0, a);
+    t1 = std::min(t1, b * (1 + 4 * Eps));
+    if (t0 > t1) return false;
+  }
+  *tentry = t0;
+  return true;
+}
+
+// Closest hit in (tnear, tfar].  any_hit: stop at the first hit (occlusion).
+static int Trace(const Scene& s, V3 org, V3 dir, double tnear, double tfar, bool any_hit, double* t_out,
+                 double* u_out, double* v_out) {
+  if (s.nodes.empty() || s.tv0.empty()) return -1;
+  V3 inv{1.0 / dir.x, 1.0 / dir.y, 1.0 / dir.z};
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  int best = -1;
+  double best_t = tfar, bu = 0, bv = 0;
+  while (sp > 0) {
+    const BNode& nd = s.nodes[stack[--sp]];
+    double te;
+    if (!SlabHit(nd, org, inv, tnear, best_t, &te)) continue;
+    if (nd.count > 0) {
+      for (int i = nd.start; i < nd.start + nd.count; ++i) {
+        int tri = s.tri_order[i];
+        double t, u, v;
+        if (IntersectTri(org, dir, s.tv0[tri], s.tv1[tri], s.tv2[tri], tnear, best_t, &t, &u, &v)) {
+          best = tri; best_t = t; bu = u; bv = v;
+          if (any_hit) { *t_out = t; return tri; }
+        }
+      }
+    } else {
+      if (sp + 2 > 128) return -2;
+      stack[sp++] = nd.right;
+      stack[sp++] = nd.left;
+    }
+  }
+  if (best >= 0) { *t_out = best_t; *u_out = bu; *v_out = bv; }
+  return best;
+}
+
+static int TraceBrute(const Scene& s, V3 org, V3 dir, double tnear, double tfar, double* t_out, double* u_out,
+                      double* v_out) {
+  int best = -1;
+  double best_t = tfar, bu = 0, bv = 0;
+  for (size_t tri = 0; tri < s.tv0.size(); ++tri) {
+    double t, u, v;
+    if (IntersectTri(org, dir, s.tv0[tri], s.tv1[tri], s.tv2[tri], tnear, best_t, &t, &u, &v)) {
+      best = (int)tri; best_t = t; bu = u; bv = v;
+    }
+  }
+  if (best >= 0) { *t_out = best_t; *u_out = bu; *v_out = bv; }
+  return best;
+}
+
+// ---------------------------------------------------------------------------------------
+// Geometry queries.
+inline V3 VertD(const Scene& s, uint32_t i) { return {s.vert[i].x, s.vert[i].y, s.vert[i].z}; }
+
+// FillPosBoundsTriangle, primitive.cxx:291-299 (barry weights p0, p1, p2 in that order).
+inline V3 PosBounds(V3 p0, V3 p1, V3 p2, V3 b) {
+  V3 r = Abs(p0 * b.x) + Abs(p1 * b.y) + Abs(p2 * b.z);
+  return r * Gamma7();
+}
+
+inline V3 SmoothNormal(const Scene& s, int prim, double w0, double w1, double w2, V3 ng) {
+  if (!s.has_normals) return ng;
+  uint32_t a = s.idx[3 * prim], b = s.idx[3 * prim + 1], c = s.idx[3 * prim + 2];
+  V3 na{s.nrm[a].x, s.nrm[a].y, s.nrm[a].z}, nb{s.nrm[b].x, s.nrm[b].y, s.nrm[b].z},
+      nc{s.nrm[c].x, s.nrm[c].y, s.nrm[c].z};
+  return Normalized(na * w0 + nb * w1 + nc * w2);
+}
+
+inline V3 GeometryNormal(const Scene& s, int prim) {
+  return Normalized(Cross(s.tv1[prim] - s.tv0[prim], s.tv2[prim] - s.tv0[prim]));
+}
+
+// EmbreeAccelerator::FirstIntersectionTriangle (embreeaccelerator.cxx:216-244) followed by
+// SurfaceInteraction::SetOrientedNormals (scene.cxx:240-245).
+inline Surf SurfaceFromHit(const Scene& s, int prim, double u, double v, V3 ray_dir) {
+  Surf si;
+  si.prim = prim;
+  si.barry = {u, v, 1. - u - v};
+  const V3 p0 = s.tv0[prim], p1 = s.tv1[prim], p2 = s.tv2[prim];
+  si.pos = p0 * (1. - u - v) + p1 * u + p2 * v;
+  si.geometry_normal = GeometryNormal(s, prim);
+  si.smooth_normal = SmoothNormal(s, prim, 1. - u - v, u, v, si.geometry_normal);
+  si.pos_bounds = PosBounds(p0, p1, p2, si.barry);
+  const double sign = -Sign(Dot(ray_dir, si.geometry_normal));
+  si.normal = sign * si.geometry_normal;
+  si.shading_normal = sign * si.smooth_normal;
+  return si;
+}
+
+// SurfaceInteraction(HitId) + Mesh::GetLocalGeometry (primitive.cxx:91-116).
+inline Surf SurfaceFromBarycentric(const Scene& s, int prim, V3 barry) {
+  Surf si;
+  si.prim = prim;
+  si.barry = barry;
+  const V3 p0 = s.tv0[prim], p1 = s.tv1[prim], p2 = s.tv2[prim];
+  si.pos = p0 * barry.x + p1 * barry.y + p2 * barry.z;
+  si.geometry_normal = GeometryNormal(s, prim);
+  si.smooth_normal = SmoothNormal(s, prim, barry.x, barry.y, barry.z, si.geometry_normal);
+  si.pos_bounds = PosBounds(p0, p1, p2, barry);
+  si.normal = si.geometry_normal;
+  si.shading_normal = si.smooth_normal;
+  return si;
+}
+
+inline double TriArea(const Scene& s, int prim) {  // Mesh::Area, primitive.cxx:129-137
+  return 0.5 * Length(Cross(s.tv1[prim] - s.tv0[prim], s.tv2[prim] - s.tv0[prim]));
+}
+
+// ---------------------------------------------------------------------------------------
+// Shaders (shader.cxx).
+struct ScatterSample {
+  V3 dir;
+  S3 value;
+  double pdf = 0;
+  bool delta = false;
+};
+
+// DiffuseShader::EvaluateBSDF / SampleBSDF, shader.cxx:280-318.
+// SpecularReflectiveShader, shader.cxx:338-366.
+// SpecularTransmissiveDielectricShader::SampleBsdfRegular, shader.cxx:401-473.
+// MicrofacetShader + MicrofacetShaderWrapper, shader.cxx:74-130, 676-707.
+static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const int32_t idx[3], double* pdf) {
+  switch (m.shader) {
+    case TT_SHADER_DIFFUSE: {
+      S3 ret(0.);
+      double n_dot_out = Dot(si.normal, wo);
+      double nsh_dot_out = Dot(si.shading_normal, wo);
+      if (n_dot_out > 0.) ret = Take(m.reflectance, idx) * (1. / Pi);
+      if (pdf) *pdf = std::max(0., nsh_dot_out) / Pi;
+      return ret;
+    }
+    case TT_SHADER_SPECULAR_REFLECTIVE:
+    case TT_SHADER_SPECULAR_DIELECTRIC:
+      if (pdf) *pdf = 0.;
+      return S3(0.);
+    case TT_SHADER_MICROFACET: {
+      const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
+      const V3 ng = fr.ToLocal(si.normal);
+      const Beckman ndf{(double)m.alpha};
+      const V3 lwi = fr.ToLocal(wi), lwo = fr.ToLocal(wo);
+      const V3 wh = Normalized(lwi + lwo);
+      const double n_dot_out = Dot(ng, lwo);
+      const double ns_dot_out = lwo.z, ns_dot_in = lwi.z, ns_dot_wh = wh.z;
+      const double wh_dot_out = Dot(lwo, wh), wh_dot_in = Dot(lwi, wh);
+      double D = ndf.EvalByHalfVector(std::abs(ns_dot_wh));
+      const double G = G2VCavity(wh_dot_in, wh_dot_out, ns_dot_in, ns_dot_out, ns_dot_wh);
+      if (pdf) {
+        V3 wh_flip = wh.z < 0 ? -wh : wh;
+        double sp = VndfPdf(D, wh_flip, lwi);
+        *pdf = HalfVectorPdfToReflectedPdf(sp, Dot(wh_flip, lwi));
+      }
+      if (n_dot_out <= 0.) return S3(0.);
+      const S3 kr = Take(m.reflectance, idx);
+      const double f5 = std::pow(1 - std::abs(wh_dot_in), 5.);
+      S3 fresnel{kr[0] + (1. - kr[0]) * f5, kr[1] + (1. - kr[1]) * f5, kr[2] + (1. - kr[2]) * f5};
+      double mono = G * D * 0.25 / (std::abs(ns_dot_in * ns_dot_out) + Eps);
+      return fresnel * mono;
+    }
+  }
+  if (pdf) *pdf = 0;
+  return S3(0.);
+}
+
+static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sampler& smp, const int32_t idx[3]) {
+  ScatterSample out;
+  switch (m.shader) {
+    case TT_SHADER_DIFFUSE: {
+      const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
+      double r[2];
+      smp.UniformUnitSquare(r);
+      V3 v = ToCosHemisphere(r);
+      out.pdf = v.z / Pi;
+      out.dir = fr.ToWorld(v);
+      out.value = Dot(si.normal, out.dir) > 0 ? Take(m.reflectance, idx) * (1. / Pi) : S3(0.);
+      return out;
+    }
+    case TT_SHADER_SPECULAR_REFLECTIVE: {
+      V3 r = Reflected(wi, si.shading_normal);
+      double cos_rn = Dot(si.normal, r);
+      out.dir = r;
+      out.pdf = 1.;
+      out.delta = true;
+      if (cos_rn < 0.) out.value = S3(0.);
+      else out.value = Take(m.reflectance, idx) / Dot(si.shading_normal, r);
+      return out;
+    }
+    case TT_SHADER_SPECULAR_DIELECTRIC: {
+      const double abs_shn_dot_i = std::abs(Dot(si.shading_normal, wi));
+      const bool entering = Dot(si.geometry_normal, wi) > 0.;
+      const double eta = entering ? 1. / m.ior_ratio : (double)m.ior_ratio;
+      const double radiance_weight = Sqr(eta);  // RADIANCE transport
+      double fr = 1.;
+      V3 wt;
+      const bool has_wt = Refracted(wi, si.shading_normal, eta, &wt);
+      if (has_wt) fr = FresnelReflectivity(abs_shn_dot_i, std::abs(Dot(wt, si.shading_normal)), eta);
+      const double prob_reflection = has_wt ? std::max(0.1, std::min(0.9, fr)) : 1.;
+      const bool do_reflect = has_wt ? smp.Uniform01() < prob_reflection : true;
+      double value;
+      out.delta = true;
+      if (do_reflect) {
+        out.dir = Reflected(wi, si.shading_normal);
+        out.pdf = prob_reflection;
+        value = fr;
+      } else {
+        out.dir = wt;
+        out.pdf = 1. - prob_reflection;
+        value = 1. - fr;
+      }
+      value /= std::abs(Dot(out.dir, si.shading_normal));
+      if (Dot(out.dir, si.normal) < 0) value *= radiance_weight;
+      out.value = S3(value);
+      return out;
+    }
+    case TT_SHADER_MICROFACET: {
+      const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
+      const Beckman ndf{(double)m.alpha};
+      const V3 lwi = fr.ToLocal(wi);
+      double r[2];
+      smp.UniformUnitSquare(r);
+      V3 wh = ndf.SampleHalfVector(r);
+      VndfSample(wh, lwi, smp.Uniform01());
+      const V3 lwo = Reflected(lwi, wh);
+      // MicrofacetShaderWrapper::Evaluate with the sampled half vector.
+      const V3 ng = fr.ToLocal(si.normal);
+      const double n_dot_out = Dot(ng, lwo);
+      const double ns_dot_out = lwo.z, ns_dot_in = lwi.z, ns_dot_wh = wh.z;
+      const double wh_dot_out = Dot(lwo, wh), wh_dot_in = Dot(lwi, wh);
+      const double D = ndf.EvalByHalfVector(std::abs(ns_dot_wh));
+      const double G = G2VCavity(wh_dot_in, wh_dot_out, ns_dot_in, ns_dot_out, ns_dot_wh);
+      V3 wh_flip = wh.z < 0 ? -wh : wh;
+      double sp = VndfPdf(D, wh_flip, lwi);
+      out.pdf = HalfVectorPdfToReflectedPdf(sp, Dot(wh_flip, lwi));
+      out.dir = fr.ToWorld(lwo);
+      if (n_dot_out <= 0.) { out.value = S3(0.); return out; }
+      const S3 kr = Take(m.reflectance, idx);
+      const double f5 = std::pow(1 - std::abs(wh_dot_in), 5.);
+      S3 fresnel{kr[0] + (1. - kr[0]) * f5, kr[1] + (1. - kr[1]) * f5, kr[2] + (1. - kr[2]) * f5};
+      double mono = G * D * 0.25 / (std::abs(ns_dot_in * ns_dot_out) + Eps);
+      out.value = fresnel * mono;
+      return out;
+    }
+  }
+  out.value = S3(0.);
+  return out;
+}
+
+// RadianceEstimatorBase::BsdfCorrectionFactor (rendering_randomwalk_impl.hxx:616-622),
+// RADIANCE transport: the light-incident direction is the exitant direction.
+inline double BsdfCorrectionFactor(const Surf& si, V3 exitant_dir) {
+  return std::abs(Dot(si.shading_normal, exitant_dir)) / (std::abs(Dot(si.normal, exitant_dir)) + Eps);
+}
+
+// ---------------------------------------------------------------------------------------
+// Environmental lights (light.hxx:146-304, light.cxx:10-189).
+// KartesianToSpherical (vec3f.hxx:298-321): the THIRD component is "up".
+inline void KartesianToSphericalF(const float xyz[3], float* phi, float* theta) {
+  const float x = xyz[0], z = xyz[1], y = xyz[2];
+  const float ax = std::abs(x), az = std::abs(z);
+  const float r = std::sqrt(xyz[0] * xyz[0] + xyz[1] * xyz[1] + xyz[2] * xyz[2]);
+  *theta = std::acos(y / r);
+  float p;
+  if (ax > az) {
+    p = std::atan2(z, ax);
+    p = (x > 0.f) ? p : (float)Pi - p;
+  } else {
+    p = std::atan2(x, az);
+    p = (z > 0.f) ? (float)(Pi / 2.) - p : (float)(3. / 2. * Pi) + p;
+  }
+  *phi = p;
+}
+// UvToPixel, texture.hxx:37-55.
+inline void UvToPixel(int w, int h, float u, float v, int* px, int* py) {
+  float dummy;
+  u = std::modf(u, &dummy);
+  v = std::modf(v, &dummy);
+  if (u < 0.f) u = 1.f + u;
+  if (v < 0.f) v = 1.f + v;
+  if (u > 1.f - EpsF) u -= EpsF;
+  if (v > 1.f - EpsF) v -= EpsF;
+  int x = (int)(u * w);
+  int y = (int)(v * h);
+  y = h - y - 1;
+  *px = x;
+  *py = y;
+}
+
+inline void EnvMapPixelOf(const EnvLight& L, V3 dir_out, int* px, int* py) {
+  // EnvMapLight::MapToImage, light.cxx:117-121 (float frame, transposed).
+  float d[3] = {(float)dir_out.x, (float)dir_out.y, (float)dir_out.z};
+  float loc[3] = {L.fX[0] * d[0] + L.fX[1] * d[1] + L.fX[2] * d[2],
+                  L.fY[0] * d[0] + L.fY[1] * d[1] + L.fY[2] * d[2],
+                  L.fZ[0] * d[0] + L.fZ[1] * d[1] + L.fZ[2] * d[2]};
+  float phi, theta;
+  KartesianToSphericalF(loc, &phi, &theta);
+  const float u = phi / (float)(2. * Pi), v = theta / (float)Pi;
+  UvToPixel(L.w, L.h, u, v, px, py);
+}
+
+inline void EnvMapPixelAngles(const EnvLight& L, int x, int y, float* phi0, float* z0, float* phi1, float* z1) {
+  // PixelToUvBounds (texture.hxx:71-86) + UvToSpherical.
+  float ul = (float)x / L.w, vl = (float)y / L.h;
+  float uu = ul + 1.f / L.w, vu = vl + 1.f / L.h;
+  vl = 1.f - vl;
+  vu = 1.f - vu;
+  float th_l = vl * (float)Pi, th_u = vu * (float)Pi;
+  *phi0 = ul * (float)(2. * Pi);
+  *phi1 = uu * (float)(2. * Pi);
+  *z0 = std::cos(th_l);
+  *z1 = std::cos(th_u);
+}
+
+inline S3 EnvMapValue(const EnvLight& L, int x, int y, const int32_t idx[3]) {
+  const float* p = &L.tex[3 * ((size_t)y * L.w + x)];
+  double rgb[3] = {p[0], p[1], p[2]};
+  return RGBToSpectralSelection(rgb, idx);
+}
+
+static double EnvEvaluatePdfOne(const EnvLight& L, V3 dir_out) {
+  switch (L.kind) {
+    case TT_ENV_DOME: return Dot(dir_out, L.down_dir) > 0. ? 1. / (2. * Pi) : 0.;
+    case TT_ENV_SUN: return Dot(dir_out, L.frame.Z) > L.cos_opening ? L.pdf_val : 0.;
+    case TT_ENV_DIRECTIONAL: return 0.;
+    case TT_ENV_MAP: {
+      int x, y;
+      EnvMapPixelOf(L, dir_out, &x, &y);
+      const float proby = ProbFromCmf(L.cmf_rows.data(), y);
+      const float probx = ProbFromCmf(&L.cmf_cols[(size_t)y * L.w], x);
+      float phi0, z0, phi1, z1;
+      EnvMapPixelAngles(L, x, y, &phi0, &z0, &phi1, &z1);
+      double pdf = (double)proby * probx;
+      pdf /= ((double)z1 - z0) * ((double)phi1 - phi0);
+      return pdf;
+    }
+  }
+  return 0;
+}
+
+static S3 EnvEvaluateOne(const EnvLight& L, V3 dir_out, const int32_t idx[3]) {
+  switch (L.kind) {
+    case TT_ENV_DOME: return Dot(dir_out, L.down_dir) > 0. ? TakeD(L.spectrum, idx) : S3(0.);
+    case TT_ENV_SUN: return Dot(dir_out, L.frame.Z) > L.cos_opening ? TakeD(L.sun_emission, idx) : S3(0.);
+    case TT_ENV_DIRECTIONAL: return S3(0.);
+    case TT_ENV_MAP: {
+      int x, y;
+      EnvMapPixelOf(L, dir_out, &x, &y);
+      return EnvMapValue(L, x, y, idx);
+    }
+  }
+  return S3(0.);
+}
+
+struct DirSample { V3 dir; S3 value; double pdf; bool delta; };
+
+static DirSample EnvTakeDirectionSampleOne(const EnvLight& L, Sampler& smp, const int32_t idx[3]) {
+  DirSample s{};
+  double r[2];
+  switch (L.kind) {
+    case TT_ENV_DOME:
+      smp.UniformUnitSquare(r);
+      s.dir = L.frame.ToWorld(ToUniformHemisphere(r));
+      s.value = TakeD(L.spectrum, idx);
+      s.pdf = 1. / (2. * Pi);
+      return s;
+    case TT_ENV_SUN:
+      smp.UniformUnitSquare(r);
+      s.dir = L.frame.ToWorld(ToUniformSphereSection(L.cos_opening, r));
+      s.value = TakeD(L.sun_emission, idx);
+      s.pdf = L.pdf_val;
+      return s;
+    case TT_ENV_DIRECTIONAL:
+      s.dir = L.dir;
+      s.value = TakeD(L.spectrum, idx);
+      s.pdf = 1.;
+      s.delta = true;
+      return s;
+    case TT_ENV_MAP: {
+      smp.UniformUnitSquare(r);
+      const int y = TowerSamplingBisection(L.cmf_rows.data(), L.h, (float)r[1]);
+      const float proby = ProbFromCmf(L.cmf_rows.data(), y);
+      const float* row = &L.cmf_cols[(size_t)y * L.w];
+      const int x = TowerSamplingBisection(row, L.w, (float)r[0]);
+      const float probx = ProbFromCmf(row, x);
+      float phi0, z0, phi1, z1;
+      EnvMapPixelAngles(L, x, y, &phi0, &z0, &phi1, &z1);
+      double r2[2];
+      smp.UniformUnitSquare(r2);
+      V3 loc = ToUniformSphereSection(r2, phi0, z0, phi1, z1);
+      float lf[3] = {(float)loc.x, (float)loc.y, (float)loc.z};
+      float d[3];
+      for (int k = 0; k < 3; ++k) d[k] = L.fX[k] * lf[0] + L.fY[k] * lf[1] + L.fZ[k] * lf[2];
+      s.dir = {d[0], d[1], d[2]};
+      double pdf = (double)proby * probx;
+      pdf /= ((double)z1 - z0) * ((double)phi1 - phi0);
+      s.pdf = pdf;
+      s.value = EnvMapValue(L, x, y, idx);
+      return s;
+    }
+  }
+  return s;
+}
+
+// TotalEnvironmentalRadianceField (light.cxx:28-85).
+static S3 EnvEvaluateTotal(const Scene& sc, V3 dir_out, const int32_t idx[3]) {
+  S3 acc(0.);
+  for (const auto& L : sc.env) acc = acc + EnvEvaluateOne(L, dir_out, idx);
+  return acc;
+}
+static double EnvEvaluatePdfTotal(const Scene& sc, V3 dir_out) {
+  const double sel = sc.env.size() > 0 ? 1. / sc.env.size() : 1.;
+  double sum = 0;
+  for (const auto& L : sc.env) sum += EnvEvaluatePdfOne(L, dir_out);
+  return sum * sel;
+}
+static DirSample EnvTakeDirectionSampleTotal(const Scene& sc, Sampler& smp, const int32_t idx[3]) {
+  const int n = (int)sc.env.size();
+  int i = smp.UniformInt(0, n - 1);
+  DirSample s = EnvTakeDirectionSampleOne(sc.env[i], smp, idx);
+  s.pdf *= 1. / n;
+  return s;
+}
+
+// ---------------------------------------------------------------------------------------
+// Path nodes (rendering_randomwalk_impl.hxx:32-188).
+enum NodeType { SURFACE_SCATTER, VOLUME_SCATTER, SURFACE_EMITTER, VOLUME_EMITTER, ENV, POINT_LIGHT, CAMERA, ZERO };
+
+struct Node {
+  NodeType type = ZERO;
+  V3 incident_dir;
+  Surf surf;
+  V3 coords;       // ENV: direction; POINT/CAMERA: position; surfaces use surf.pos
+  S3 radiance;     // ENV radiance
+  int unit = -1;   // CAMERA unit index
+  int point = -1;  // point light index
+  bool IsSurface() const { return type == SURFACE_EMITTER || type == SURFACE_SCATTER; }
+  bool IsScatter() const { return type == SURFACE_SCATTER || type == VOLUME_SCATTER; }
+  V3 Coordinates() const { return IsSurface() ? surf.pos : coords; }
+};
+
+struct PathCtx {
+  int32_t idx[3];
+};
+
+// Camera (camera.hxx).
+inline double PixelPdfWrtSolidAngle(const Camera& c, double x, double y) {
+  double area = c.xperpixel * c.yperpixel;
+  V3 v{x, y, 1.};
+  double l = Length(v);
+  v = v * (1. / l);
+  // PdfConversion::AreaToSolidAngle(l, v, (0,0,1)) = l^2 / (|v.z| + Eps)
+  return 1. / area * (Sqr(l) / std::abs(v.z + Eps));
+}
+
+struct CameraResponse { int unit; double pdf; };
+
+static CameraResponse CameraEvaluate(const Camera& c, V3 dir_out) {
+  CameraResponse r{-1, 0.};
+  if (c.kind != TT_CAMERA_PINHOLE) return r;  // FisheyeHemisphereCamera::Evaluate returns nothing
+  double z = Dot(dir_out, c.dir), x = Dot(dir_out, c.right), y = Dot(dir_out, c.up);
+  if (z <= 0.) return r;
+  x /= z;
+  y /= z;
+  int px = (int)((x - c.xmin) / c.xperpixel);
+  int py = (int)((y - c.ymin) / c.yperpixel);
+  if (px < 0 || px >= c.xres || py < 0 || py >= c.yres) return r;
+  r.pdf = PixelPdfWrtSolidAngle(c, x, y);
+  r.unit = py * c.xres + px;
+  return r;
+}
+
+static DirSample CameraTakeDirectionSample(const Camera& c, int unit, Sampler& smp) {
+  DirSample s{};
+  int py = unit / c.xres, px = unit - py * c.xres;
+  double r[2];
+  smp.UniformUnitSquare(r);
+  if (c.kind == TT_CAMERA_PINHOLE) {
+    V3 v{c.xmin + (r[0] + px) * c.xperpixel, c.ymin + (r[1] + py) * c.yperpixel, 1.0};
+    v = Normalized(v);
+    s.dir = c.right * v.x + c.up * v.y + c.dir * v.z;
+    double pdf = PixelPdfWrtSolidAngle(c, v.x, v.y);  // sic: normalized components
+    s.value = S3(pdf);
+    s.pdf = pdf;
+  } else {
+    double u = (r[0] + px) * c.per_pixel_delta - 1.0;
+    double v = (r[1] + py) * c.per_pixel_delta - 1.0;
+    double rho = u * u + v * v;
+    V3 w{2. * u, 2. * v, rho - 1.};
+    w = w * (1. / (1. + rho));
+    w.z = -w.z;
+    if (rho <= 1.) {
+      s.dir = c.right * w.x + c.up * w.y + c.dir * w.z;
+      s.value = S3(1.);
+    } else {
+      s.dir = c.dir;
+      s.value = S3(0.);
+    }
+    s.pdf = 1.;
+    s.delta = true;
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------------------------------
+// The estimator.
+struct Worker {
+  const Scene& sc;
+  Sampler smp;
+  PathCtx ctx;
+  int sensor_connection_unit = -1;
+  bool do_sample_brdf = true, do_sample_lights = true;
+  int max_path_node_count;
+  Worker(const Scene& s) : sc(s) {
+    max_path_node_count = s.params.max_ray_depth + 1;
+    if (s.params.pt_sample_mode == TT_SAMPLE_BSDF) do_sample_lights = false;
+    if (s.params.pt_sample_mode == TT_SAMPLE_LIGHTS) do_sample_brdf = false;
+  }
+
+  double DFactorOf(const Node& n, V3 dir) const {
+    if (n.IsSurface()) return std::abs(Dot(n.surf.geometry_normal, dir));
+    return 1.;
+  }
+  void AddAntiSelfIntersectionOffsetAt(V3& p, const Node& n, V3 dir) const {
+    if (n.IsSurface()) p = p + AntiSelfIntersectionOffset(n.surf, dir);
+  }
+
+  // EmitterSampleVisitor + TrivialLightPicker::PickLight (rendering_randomwalk_impl.hxx:192-250,
+  // lightpicker_trivial.hxx:66-114).
+  Node SampleEmissiveEnd(double* pdf, bool* delta) {
+    Node node;
+    int which = TowerSampling4(sc.type_probs, smp.Uniform01());
+    *delta = false;
+    switch (which) {
+      case 0: {
+        double prob = sc.type_probs[0];
+        DirSample s = EnvTakeDirectionSampleTotal(sc, smp, ctx.idx);
+        node.type = ENV;
+        node.coords = s.dir;
+        node.radiance = s.value;
+        *pdf = prob * s.pdf;
+        *delta = s.delta;
+        break;
+      }
+      case 2: {
+        int n = (int)sc.points.size();
+        int i = smp.UniformInt(0, n - 1);
+        double prob = sc.type_probs[2] / n;
+        node.type = POINT_LIGHT;
+        node.point = i;
+        node.coords = {sc.points[i].pos[0], sc.points[i].pos[1], sc.points[i].pos[2]};
+        *pdf = prob;
+        *delta = true;
+        break;
+      }
+      case 1: {
+        int n = (int)sc.area_lights.size();
+        int i = smp.UniformInt(0, n - 1);
+        int prim = sc.area_lights[i];
+        double prob = sc.type_probs[1] / n;
+        double r[2];
+        smp.UniformUnitSquare(r);
+        V3 b = ToTriangleBarycentricCoords(r);
+        node.type = SURFACE_EMITTER;
+        node.surf = SurfaceFromBarycentric(sc, prim, b);
+        *pdf = prob * (1. / TriArea(sc, prim));
+        break;
+      }
+      default:
+        *pdf = 0;
+        break;
+    }
+    return node;
+  }
+
+  // Emitter Evaluate for the non-scatter node kinds (rendering_randomwalk_impl.hxx:420-461).
+  S3 EvaluateEmitter(const Node& n, V3 out_dir, double* pdf) {
+    if (n.type == CAMERA) {
+      CameraResponse r = CameraEvaluate(sc.cam, out_dir);
+      sensor_connection_unit = r.unit;
+      if (pdf) *pdf = r.pdf;
+      return r.unit >= 0 ? S3(r.pdf) : S3(0.);
+    } else if (n.type == ENV) {
+      if (pdf) *pdf = 1. / (Pi * 0.25 * Sqr(sc.diag));
+      return n.radiance;
+    } else if (n.type == SURFACE_EMITTER) {
+      const tt_material& m = sc.materials[sc.mat_of_tri[n.surf.prim]].m;
+      // UniformAreaLightDirectionalPart::Evaluate, light.hxx:96-104 (uses the raw winding normal).
+      double vis = Dot(GeometryNormal(sc, n.surf.prim), out_dir) > 0. ? 1. : 0.;
+      if (pdf) *pdf = vis / (2. * Pi);
+      return Take(m.emission, ctx.idx) * (vis / (2. * Pi));
+    } else if (n.type == POINT_LIGHT) {
+      if (pdf) *pdf = 1. / (4. * Pi);
+      return Take(sc.points[n.point].spectrum, ctx.idx) * (1. / (4. * Pi));
+    }
+    return S3(0.);
+  }
+
+  S3 EvaluateScatterer(const Node& n, V3 out_dir, double* pdf) {
+    const V3 wi = -n.incident_dir;
+    const tt_material& m = sc.materials[sc.mat_of_tri[n.surf.prim]].m;
+    S3 fs = EvaluateBSDF(m, wi, n.surf, out_dir, ctx.idx, pdf);
+    return fs * BsdfCorrectionFactor(n.surf, out_dir);
+  }
+
+  S3 Evaluate(const Node& n, V3 out_dir, double* pdf) {
+    return n.IsScatter() ? EvaluateScatterer(n, out_dir, pdf) : EvaluateEmitter(n, out_dir, pdf);
+  }
+
+  // CalculateSegmentToTarget, rendering_randomwalk_impl.hxx:663-725.
+  void SegmentToTarget(const Node& src, const Node& tgt, V3* org, V3* dir, double* len) {
+    V3 cs = src.Coordinates(), ct = tgt.Coordinates();
+    auto figure = [&](V3* d, double* l) {
+      if (tgt.type != ENV) {
+        V3 dd = ct - cs;
+        double ll = Length(dd);
+        *d = dd / ll;
+        *l = ll;
+      } else {
+        *d = -ct;
+        *l = sc.long_distance;
+      }
+    };
+    V3 d;
+    double l;
+    figure(&d, &l);
+    AddAntiSelfIntersectionOffsetAt(cs, src, d);
+    AddAntiSelfIntersectionOffsetAt(ct, tgt, -d);
+    figure(&d, &l);
+    *org = cs;
+    *dir = d;
+    *len = l;
+  }
+
+  bool Occluded(V3 org, V3 dir, double len) {
+    double t, u, v;
+    return Trace(sc, org, dir, 0., len, true, &t, &u, &v) >= 0;
+  }
+
+  // CalculateConnection, rendering_randomwalk_impl.hxx:373-409.
+  S3 CalculateConnection(const Node& eye, const Node& light, double* pdf_source, V3* seg_dir, double* seg_len) {
+    V3 org, dir;
+    double len;
+    SegmentToTarget(eye, light, &org, &dir, &len);
+    *seg_dir = dir;
+    *seg_len = len;
+    S3 sf = Evaluate(eye, dir, pdf_source);
+    S3 tf = Evaluate(light, -dir, nullptr);
+    if (sf.IsZero() || tf.IsZero()) return S3(0.);
+    sf = sf * DFactorOf(eye, dir);
+    tf = tf * DFactorOf(light, -dir);
+    // TransmittanceEstimate, rendering_util.cxx:40-67 (vacuum: occlusion only).
+    double T = Occluded(org, dir, len * 0.9999) ? 0. : 1.;
+    bool wrt_solid_angle = eye.type == ENV || light.type == ENV;
+    double r2 = wrt_solid_angle ? 1. : 1. / Sqr(len);
+    return sf * tf * (r2 * T);
+  }
+
+  // PdfConversionFactor, rendering_randomwalk_impl.hxx:493-513 (vacuum coefficients = 1).
+  double PdfConversionFactor(const Node& src, const Node& tgt, V3 dir, double len, bool parallel) const {
+    double factor = DFactorOf(tgt, dir);
+    if (src.type != ENV && tgt.type != ENV && !parallel) factor /= (Sqr(len) + Eps);
+    return factor;
+  }
+
+  double MisWeight(double pdf_taken, bool taken_delta, double pdf_other) const {
+    if (!taken_delta && do_sample_brdf && do_sample_lights) return PowerHeuristic(pdf_taken, pdf_other);
+    return 1.;
+  }
+
+  struct Step {
+    Node node;
+    V3 ray_dir;
+    double seg_len = 0;
+    double scatter_pdf = 0;
+    bool scatter_delta = false;
+    S3 beta_factor;
+  };
+
+  // TakeRandomWalkStep, rendering_randomwalk_impl.hxx:285-363.
+  Step TakeRandomWalkStep(const Node& src) {
+    Step st;
+    V3 org = src.Coordinates();
+    V3 dir;
+    S3 value;
+    double pdf;
+    bool delta;
+    if (src.IsScatter()) {
+      const tt_material& m = sc.materials[sc.mat_of_tri[src.surf.prim]].m;
+      ScatterSample s = SampleBSDF(m, -src.incident_dir, src.surf, smp, ctx.idx);
+      s.value = s.value * BsdfCorrectionFactor(src.surf, s.dir);
+      dir = s.dir; value = s.value; pdf = s.pdf; delta = s.delta;
+    } else {  // camera
+      DirSample s = CameraTakeDirectionSample(sc.cam, src.unit, smp);
+      dir = s.dir; value = s.value; pdf = s.pdf; delta = s.delta;
+    }
+    value = value * DFactorOf(src, dir);
+    AddAntiSelfIntersectionOffsetAt(org, src, dir);
+    st.beta_factor = value / std::abs(pdf);
+    if (st.beta_factor.IsZero()) { st.node.type = ZERO; return st; }
+    double t = 0, u = 0, v = 0;
+    int prim = Trace(sc, org, dir, 0., LargeNumber, false, &t, &u, &v);
+    if (prim >= 0) {
+      st.node.type = SURFACE_SCATTER;
+      st.node.surf = SurfaceFromHit(sc, prim, u, v, dir);
+      st.seg_len = t;
+    } else {
+      st.node.type = ENV;
+      st.node.coords = -dir;
+      st.node.radiance = EnvEvaluateTotal(sc, -dir, ctx.idx);
+      st.seg_len = LargeNumber;
+    }
+    st.node.incident_dir = dir;
+    st.ray_dir = dir;
+    st.scatter_pdf = std::abs(pdf);
+    st.scatter_delta = delta;
+    return st;
+  }
+
+  // GetPdfOfGeneratingSampleOnEmitter, rendering_randomwalk_impl.hxx:624-651.
+  double PdfOfGeneratingSampleOnEmitter(const Node& n) const {
+    if (n.type == SURFACE_EMITTER) return (1. / TriArea(sc, n.surf.prim)) * sc.type_probs[1] * sc.in_class[1];
+    if (n.type == ENV) return EnvEvaluatePdfTotal(sc, n.coords) * sc.type_probs[0];
+    return 0.;
+  }
+
+  // PathTracingWorker::RenderPixel, renderingalgorithms_pathtracing.hxx:731-817.
+  void RenderPixel(int pixel, double rgb_out[3], std::vector<double>& light_accum) {
+    sensor_connection_unit = -1;
+    // LambdaSelectionStrategy::WithWeights, shader_util.hxx:83-91.
+    int main_idx = smp.UniformInt(0, 11);
+    int32_t idx[3] = {main_idx, main_idx + 12, main_idx + 24};
+    int rotation = smp.UniformInt(0, 2);
+    std::swap(idx[0], idx[rotation]);
+    for (int i = 0; i < 3; ++i) smp.Uniform01();  // SampleWavelengthStrata
+    std::memcpy(ctx.idx, idx, sizeof(idx));
+    S3 path_sample_values(0.);
+    Step step;
+    step.node.type = CAMERA;
+    step.node.coords = {sc.cam.pos.x, sc.cam.pos.y, sc.cam.pos.z};
+    step.node.unit = pixel;
+    S3 beta(12.);  // lambda weights (strata size) / delta pdf 1
+    int count = 1;
+    const int npix = sc.cam.xres * sc.cam.yres;
+    while (true) {
+      if (do_sample_lights) {
+        double pdf_light;
+        bool light_delta;
+        Node light = SampleEmissiveEnd(&pdf_light, &light_delta);
+        double pdf_scatter = 0;
+        V3 sdir;
+        double slen;
+        S3 w = CalculateConnection(step.node, light, &pdf_scatter, &sdir, &slen);
+        double pdf_due = pdf_scatter * PdfConversionFactor(step.node, light, sdir, slen, false);
+        double mis = MisWeight(pdf_light, light_delta, pdf_due);
+        S3 pw = w * (mis / pdf_light) * beta;
+        if (step.node.type == CAMERA) {
+          if (sensor_connection_unit >= 0) {
+            pw = pw / (double)npix;
+            double rgb[3];
+            SpectralSelectionToRGB(pw, ctx.idx, rgb);
+            for (int k = 0; k < 3; ++k) light_accum[3 * (size_t)sensor_connection_unit + k] += rgb[k];
+          }
+        } else {
+          path_sample_values = path_sample_values + pw;
+        }
+      }
+      Node prev = step.node;
+      step = TakeRandomWalkStep(prev);
+      beta = beta * step.beta_factor;
+      ++count;
+      if (do_sample_brdf) {
+        bool emitter = false;
+        if (step.node.type == SURFACE_SCATTER && sc.materials[sc.mat_of_tri[step.node.surf.prim]].m.emissive) {
+          step.node.type = SURFACE_EMITTER;
+          emitter = true;
+        } else if (step.node.type == ENV) {
+          emitter = true;
+        }
+        if (emitter) {
+          S3 end_weight = Evaluate(step.node, -step.ray_dir, nullptr);
+          double pdf_direct = PdfOfGeneratingSampleOnEmitter(step.node);
+          double pdf_due = PdfConversionFactor(prev, step.node, step.ray_dir, step.seg_len, step.scatter_delta) *
+                           step.scatter_pdf;
+          double mis = MisWeight(pdf_due, step.scatter_delta, pdf_direct);
+          path_sample_values = path_sample_values + end_weight * beta * mis;
+          if (step.node.type == SURFACE_EMITTER) step.node.type = SURFACE_SCATTER;
+        }
+      }
+      if (step.node.type == ZERO || step.node.type == ENV) break;
+      // SurvivalAtNthScatterNode, rendering_randomwalk_impl.hxx:736-755.
+      if (count < max_path_node_count) {
+        if (count > 5) {
+          double p = std::min(0.9, beta.Max());
+          if (smp.Uniform01() > p) break;
+          beta = beta * (1. / p);
+        }
+      } else {
+        break;
+      }
+    }
+    SpectralSelectionToRGB(path_sample_values, ctx.idx, rgb_out);
+  }
+};
+
+// ---------------------------------------------------------------------------------------
+static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
+  if (!d || !p) { g_err = "null argument"; return false; }
+  s.params = *p;
+  if (s.params.max_ray_depth <= 0) s.params.max_ray_depth = 25;
+  s.vert.resize(d->num_vertices);
+  for (uint32_t i = 0; i < d->num_vertices; ++i)
+    s.vert[i] = {d->vertices[3 * i], d->vertices[3 * i + 1], d->vertices[3 * i + 2]};
+  s.has_normals = d->normals != nullptr;
+  if (s.has_normals) {
+    s.nrm.resize(d->num_vertices);
+    for (uint32_t i = 0; i < d->num_vertices; ++i)
+      s.nrm[i] = {d->normals[3 * i], d->normals[3 * i + 1], d->normals[3 * i + 2]};
+  }
+  s.idx.assign(d->indices, d->indices + 3 * (size_t)d->num_triangles);
+  s.mat_of_tri.assign(d->material_ids, d->material_ids + d->num_triangles);
+  for (uint32_t i = 0; i < d->num_materials; ++i) s.materials.push_back(Material{d->materials[i]});
+  for (uint32_t t = 0; t < d->num_triangles; ++t) {
+    for (int k = 0; k < 3; ++k)
+      if (s.idx[3 * t + k] >= d->num_vertices) { g_err = "vertex index out of range"; return false; }
+    if (s.mat_of_tri[t] >= d->num_materials) { g_err = "material index out of range"; return false; }
+    s.tv0.push_back(VertD(s, s.idx[3 * t]));
+    s.tv1.push_back(VertD(s, s.idx[3 * t + 1]));
+    s.tv2.push_back(VertD(s, s.idx[3 * t + 2]));
+    if (s.materials[s.mat_of_tri[t]].m.emissive) s.area_lights.push_back((int)t);
+  }
+  for (int k = 0; k < 3; ++k) { s.bb_lo[k] = 1e300; s.bb_hi[k] = -1e300; }
+  for (auto& v : s.vert) {
+    double c[3] = {v.x, v.y, v.z};
+    for (int k = 0; k < 3; ++k) { s.bb_lo[k] = std::min(s.bb_lo[k], c[k]); s.bb_hi[k] = std::max(s.bb_hi[k], c[k]); }
+  }
+  if (s.vert.empty()) for (int k = 0; k < 3; ++k) { s.bb_lo[k] = 0; s.bb_hi[k] = 0; }
+  s.diag = std::sqrt(Sqr(s.bb_hi[0] - s.bb_lo[0]) + Sqr(s.bb_hi[1] - s.bb_lo[1]) + Sqr(s.bb_hi[2] - s.bb_lo[2]));
+  s.long_distance = 10. * s.diag;
+  s.box_center = {0.5 * (s.bb_lo[0] + s.bb_hi[0]), 0.5 * (s.bb_lo[1] + s.bb_hi[1]), 0.5 * (s.bb_lo[2] + s.bb_hi[2])};
+  for (uint32_t i = 0; i < d->num_point_lights; ++i) s.points.push_back(d->point_lights[i]);
+  for (uint32_t i = 0; i < d->num_env_lights; ++i) {
+    const tt_env_light& e = d->env_lights[i];
+    EnvLight L;
+    L.kind = e.kind;
+    for (int b = 0; b < NBINS; ++b) L.spectrum[b] = e.spectrum[b];
+    L.dir = {e.dir[0], e.dir[1], e.dir[2]};
+    L.scalar = e.scalar;
+    L.scalar2 = e.scalar2;
+    if (e.kind == TT_ENV_SUN) {
+      // Sun::Sun, light.hxx:253-263.
+      L.cos_opening = std::cos(Pi / 180. * L.scalar2);
+      L.pdf_val = 1. / (2. * Pi * (1. - L.cos_opening));
+      L.frame = OrthogonalSystemZAligned(Normalized(L.dir));
+      for (int b = 0; b < NBINS; ++b) L.sun_emission[b] = kSunSpectrum[b] * L.scalar * L.pdf_val;
+    } else if (e.kind == TT_ENV_DOME) {
+      L.down_dir = -Normalized(L.dir);
+      L.frame = OrthogonalSystemZAligned(L.down_dir);
+    } else if (e.kind == TT_ENV_DIRECTIONAL) {
+      L.dir = Normalized(L.dir);
+    } else if (e.kind == TT_ENV_MAP) {
+      if (!e.tex_rgb || e.tex_width <= 0 || e.tex_height <= 0) { g_err = "env map without texture"; return false; }
+      L.w = e.tex_width;
+      L.h = e.tex_height;
+      L.tex.assign(e.tex_rgb, e.tex_rgb + 3 * (size_t)L.w * L.h);
+      // Float frame, EnvMapLight ctor (light.cxx:88-115).
+      float up[3] = {(float)L.dir.x, (float)L.dir.y, (float)L.dir.z};
+      float sign = std::copysign(1.0f, up[2]);
+      const float a = -1.0f / (sign + up[2]);
+      const float b = up[0] * up[1] * a;
+      float X[3] = {1.0f + sign * up[0] * up[0] * a, sign * b, -sign * up[0]};
+      float Y[3] = {b, sign + up[1] * up[1] * a, -up[1]};
+      for (int k = 0; k < 3; ++k) { L.fX[k] = X[k]; L.fY[k] = Y[k]; L.fZ[k] = up[k]; }
+      L.cmf_rows.assign(L.h, 0.f);
+      L.cmf_cols.assign((size_t)L.w * L.h, 0.f);
+      for (int y = 0; y < L.h; ++y) {
+        double row_weight = 0.;
+        for (int x = 0; x < L.w; ++x) {
+          const float* px = &L.tex[3 * ((size_t)y * L.w + x)];
+          double mean = ((double)px[0] + px[1] + px[2]) / 3.;
+          // PixelCenterToUv + UvToSpherical: theta = v * pi, v = (h - 1 - y + 0.5) / h.
+          float v = ((float)(L.h - 1 - y) + 0.5f) / L.h;
+          float theta = v * (float)Pi;
+          double weight = std::sin(theta) * mean;
+          row_weight += weight;
+          L.cmf_cols[(size_t)y * L.w + x] = (float)row_weight;
+        }
+        for (int x = 0; x < L.w; ++x) L.cmf_cols[(size_t)y * L.w + x] /= (float)row_weight;
+        L.cmf_rows[y] = (float)row_weight;
+      }
+      for (int y = 1; y < L.h; ++y) L.cmf_rows[y] += L.cmf_rows[y - 1];
+      float inv = 1.f / L.cmf_rows[L.h - 1];
+      for (int y = 0; y < L.h; ++y) L.cmf_rows[y] *= inv;
+    } else {
+      g_err = "unknown env light kind";
+      return false;
+    }
+    s.env.push_back(std::move(L));
+  }
+  // TrivialLightPicker ctor, lightpicker_trivial.cxx:11-31.
+  const double nl = (double)s.points.size(), ne = s.env.empty() ? 0. : 1., na = (double)s.area_lights.size();
+  const double norm = 1. / (nl + ne + na);
+  s.type_probs[0] = ne * norm;
+  s.type_probs[1] = na * norm;
+  s.type_probs[2] = nl * norm;
+  s.type_probs[3] = 0.;
+  s.in_class[0] = ne > 0 ? 1. / ne : NAN;
+  s.in_class[1] = na > 0 ? 1. / na : NAN;
+  s.in_class[2] = nl > 0 ? 1. / nl : NAN;
+  s.in_class[3] = 0;
+  // Camera (camera.hxx:38-108, 159-175).
+  const tt_camera& c = d->camera;
+  Camera& cam = s.cam;
+  cam.kind = c.kind;
+  cam.pos = {c.pos[0], c.pos[1], c.pos[2]};
+  cam.xres = c.xres;
+  cam.yres = c.yres;
+  if (c.xres <= 0 || c.yres <= 0) { g_err = "bad camera resolution"; return false; }
+  V3 up = Normalized(V3{c.up[0], c.up[1], c.up[2]});
+  V3 dir = Normalized(V3{c.dir[0], c.dir[1], c.dir[2]});
+  double r = Dot(dir, up);
+  if (!(std::abs(r) > 1.0 - Eps)) up = Normalized(up - r * dir);
+  cam.up = up;
+  cam.dir = dir;
+  cam.right = Cross(up, dir);
+  double fov = c.fov_deg * Pi / 180.;
+  double aspect = (double)c.yres / c.xres;
+  double a = std::tan(fov * 0.5);
+  double b = a * aspect;
+  cam.xmin = -a;
+  cam.ymin = -b;
+  cam.xperpixel = 2. * a / c.xres;
+  cam.yperpixel = 2. * b / c.yres;
+  cam.per_pixel_delta = 2. / std::min(c.xres, c.yres);
+  BuildBvh(s);
+  return true;
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+struct or_scene {
+  Scene s;
+};
+
+extern "C" {
+
+const char* or_last_error(void) { return g_err.c_str(); }
+
+or_scene* or_create(const tt_scene_desc* scene, const tt_params* params) {
+  auto* o = new or_scene;
+  if (!BuildScene(o->s, scene, params)) {
+    delete o;
+    return nullptr;
+  }
+  return o;
+}
+
+void or_destroy(or_scene* s) { delete s; }
+
+int or_intersect(or_scene* s, const double* rays, int n, int brute_force, int32_t* prim, double* t, double* u,
+                 double* v) {
+  for (int i = 0; i < n; ++i) {
+    const double* r = rays + 8 * (size_t)i;
+    V3 org{r[0], r[1], r[2]}, dir{r[4], r[5], r[6]};
+    double tt = 0, uu = 0, vv = 0;
+    int p = brute_force ? TraceBrute(s->s, org, dir, r[3], r[7], &tt, &uu, &vv)
+                        : Trace(s->s, org, dir, r[3], r[7], false, &tt, &uu, &vv);
+    prim[i] = p;
+    t[i] = p >= 0 ? tt : -1;
+    u[i] = uu;
+    v[i] = vv;
+  }
+  return 0;
+}
+
+int or_occluded(or_scene* s, const double* rays, int n, uint8_t* occluded) {
+  for (int i = 0; i < n; ++i) {
+    const double* r = rays + 8 * (size_t)i;
+    double tt, uu, vv;
+    occluded[i] = Trace(s->s, {r[0], r[1], r[2]}, {r[4], r[5], r[6]}, r[3], r[7], true, &tt, &uu, &vv) >= 0;
+  }
+  return 0;
+}
+
+int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel_begin, int pixel_end, int nthreads,
+              double* accum, double* light_accum, uint64_t* splat_count) {
+  const Scene& sc = os->s;
+  const int npix = sc.cam.xres * sc.cam.yres;
+  if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) { g_err = "bad pixel range"; return 2; }
+  if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<int> next{pixel_begin};
+  constexpr int CHUNK = 64;
+  std::vector<std::vector<double>> light(nthreads, std::vector<double>(3 * (size_t)npix, 0.));
+  auto body = [&](int tid) {
+    Worker w(sc);
+    for (;;) {
+      int p0 = next.fetch_add(CHUNK);
+      if (p0 >= pixel_end) break;
+      int p1 = std::min(pixel_end, p0 + CHUNK);
+      for (int p = p0; p < p1; ++p) {
+        for (int sidx = 0; sidx < spp; ++sidx) {
+          uint64_t sample = (uint64_t)sample_offset + sidx;
+          w.smp.g.Seed(seed, sample * (uint64_t)npix + (uint64_t)p);
+          double rgb[3];
+          w.RenderPixel(p, rgb, light[tid]);
+          for (int k = 0; k < 3; ++k) accum[3 * (size_t)p + k] += rgb[k];
+        }
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 0; i < nthreads; ++i) th.emplace_back(body, i);
+  for (auto& t : th) t.join();
+  for (int i = 0; i < nthreads; ++i)
+    for (size_t k = 0; k < light[i].size(); ++k) light_accum[k] += light[i][k];
+  *splat_count += (uint64_t)spp * (uint64_t)(pixel_end - pixel_begin);
+  return 0;
+}
+
+static Surf ZUpSurface(V3 wi) {
+  Surf si;
+  si.prim = 0;
+  si.geometry_normal = {0, 0, 1};
+  si.smooth_normal = {0, 0, 1};
+  const double sign = -Sign(Dot(-wi, si.geometry_normal));
+  si.normal = sign * si.geometry_normal;
+  si.shading_normal = sign * si.smooth_normal;
+  return si;
+}
+
+int or_sample_bsdf(or_scene* s, int material, const double* wi, const int32_t* lambda_idx, int n, uint64_t seed,
+                   double* out_dir, double* out_value, double* out_pdf) {
+  if (material < 0 || material >= (int)s->s.materials.size()) return 2;
+  const tt_material& m = s->s.materials[material].m;
+  V3 w{wi[0], wi[1], wi[2]};
+  Surf si = ZUpSurface(w);
+  for (int i = 0; i < n; ++i) {
+    Sampler smp;
+    smp.g.Seed(seed, (uint64_t)i);
+    ScatterSample ss = SampleBSDF(m, w, si, smp, lambda_idx);
+    out_dir[3 * i] = ss.dir.x; out_dir[3 * i + 1] = ss.dir.y; out_dir[3 * i + 2] = ss.dir.z;
+    for (int k = 0; k < 3; ++k) out_value[3 * i + k] = ss.value[k];
+    out_pdf[i] = ss.delta ? -ss.pdf : ss.pdf;
+  }
+  return 0;
+}
+
+int or_eval_bsdf(or_scene* s, int material, const double* wi, const int32_t* lambda_idx, const double* dirs, int n,
+                 double* out_value, double* out_pdf) {
+  if (material < 0 || material >= (int)s->s.materials.size()) return 2;
+  const tt_material& m = s->s.materials[material].m;
+  V3 w{wi[0], wi[1], wi[2]};
+  Surf si = ZUpSurface(w);
+  for (int i = 0; i < n; ++i) {
+    V3 o{dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]};
+    double pdf = 0;
+    S3 val = EvaluateBSDF(m, w, si, o, lambda_idx, &pdf);
+    for (int k = 0; k < 3; ++k) out_value[3 * i + k] = val[k];
+    out_pdf[i] = pdf;
+  }
+  return 0;
+}
+
+void or_rgb_to_spectrum(const double* rgb, double* out) {
+  SmitsCases(rgb[0], rgb[1], rgb[2], [&](double a, int ia, double b, int ib, double c, int ic) {
+    LinCombN(out, a, kSmitsBasis[ia], b, kSmitsBasis[ib], c, kSmitsBasis[ic]);
+  });
+}
+void or_spectrum_to_rgb(const double* spec, double* rgb) {
+  for (int i = 0; i < 3; ++i) {
+    rgb[i] = 0;
+    for (int b = 0; b < NBINS; ++b) rgb[i] += spec[b] * kSpectrumToRgb[i][b];
+  }
+}
+void or_selection_to_rgb(const double* val3, const int32_t* idx3, double* rgb) {
+  SpectralSelectionToRGB(S3(val3[0], val3[1], val3[2]), idx3, rgb);
+}
+void or_rgb_to_selection(const double* rgb, const int32_t* idx3, double* val3) {
+  S3 r = RGBToSpectralSelection(rgb, idx3);
+  for (int k = 0; k < 3; ++k) val3[k] = r[k];
+}
+void or_reflected(const double* wi, const double* n, double* out) {
+  V3 r = Reflected({wi[0], wi[1], wi[2]}, {n[0], n[1], n[2]});
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+int or_refracted(const double* wi, const double* n, double eta, double* out) {
+  V3 r;
+  if (!Refracted({wi[0], wi[1], wi[2]}, {n[0], n[1], n[2]}, eta, &r)) return 0;
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+  return 1;
+}
+void or_half_vector(const double* wi, const double* wo, double* out) {
+  V3 r = HalfVector({wi[0], wi[1], wi[2]}, {wo[0], wo[1], wo[2]});
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+int or_half_vector_refracted(const double* wi, const double* wo, double eta, double* out) {
+  V3 r;
+  if (!HalfVectorRefracted({wi[0], wi[1], wi[2]}, {wo[0], wo[1], wo[2]}, eta, &r)) return 0;
+  out[0] = r.x; out[1] = r.y; out[2] = r.z;
+  return 1;
+}
+double or_fresnel(double cos_i, double eta) { return FresnelReflectivityWalter(cos_i, eta); }
+void or_pcg32_stream(uint64_t initstate, uint64_t initseq, int n, uint32_t* out) {
+  Pcg32 g;
+  g.Seed(initstate, initseq);
+  for (int i = 0; i < n; ++i) out[i] = g.NextUInt();
+}
+double or_pcg32_nextdouble_first(uint64_t initstate, uint64_t initseq) {
+  Pcg32 g;
+  g.Seed(initstate, initseq);
+  return g.NextDouble();
+}
+int or_uniform_int_stream(uint64_t initstate, uint64_t initseq, int a, int b, int n, int32_t* out) {
+  Sampler s;
+  s.g.Seed(initstate, initseq);
+  for (int i = 0; i < n; ++i) out[i] = s.UniformInt(a, b);
+  return 0;
+}
+void or_tables(double* smits, double* m, double* sun) {
+  std::memcpy(smits, kSmitsBasis, sizeof(kSmitsBasis));
+  std::memcpy(m, kSpectrumToRgb, sizeof(kSpectrumToRgb));
+  std::memcpy(sun, kSunSpectrum, sizeof(kSunSpectrum));
+}
+int or_eval_env(or_scene* s, const double* dir_out, const int32_t* lambda_idx, double* value3, double* pdf) {
+  V3 d{dir_out[0], dir_out[1], dir_out[2]};
+  S3 v = EnvEvaluateTotal(s->s, d, lambda_idx);
+  for (int k = 0; k < 3; ++k) value3[k] = v[k];
+  *pdf = EnvEvaluatePdfTotal(s->s, d);
+  return 0;
+}
+int or_scene_info(or_scene* s, double* bbox6, int32_t* counts4) {
+  for (int k = 0; k < 3; ++k) { bbox6[k] = s->s.bb_lo[k]; bbox6[3 + k] = s->s.bb_hi[k]; }
+  counts4[0] = (int32_t)s->s.tv0.size();
+  counts4[1] = (int32_t)s->s.area_lights.size();
+  counts4[2] = (int32_t)s->s.env.size();
+  counts4[3] = (int32_t)s->s.nodes.size();
+  return 0;
+}
+
+}  // extern "C"
