@@ -329,7 +329,7 @@ def run_ours(args):
         ge.lib.tt_read_framebuffer(ge.h, rgb.ctypes.data_as(C.POINTER(C.c_float)), None)
         ge.close()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    e2e_step = float(np.median(e2e_ms))
+    e2e_step = float(np.median(e2e_ms)) if e2e_ms else float("nan")
     if dist is not None:
         t = torch.tensor([e2e_step], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -390,6 +390,20 @@ def run_ours(args):
     return 0
 
 
+def profile_run(args):
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    scene, spp, depth, name = workload(args)
+    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave))
+    g.render(spp, 1)
+    st = g.stats()
+    print(json.dumps({"profile_run": name, "spp": spp, "extension_rays": st["extension_rays"],
+                      "shadow_rays": st["shadow_rays"], "kernel_launches": st["kernel_launches"],
+                      "error_flags": st["error_flags"]}))
+    g.close()
+    return 0 if st["error_flags"] == 0 else 1
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -402,7 +416,11 @@ def main(argv=None):
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="no timing: upload the workload and render one pass of --spp samples (for ncu captures)")
     args = ap.parse_args(argv)
+    if args.profile_run:
+        return profile_run(args)
     if args.warmup < 3 and not args.small:
         args.warmup = 3
     if args.impl == "reference":

@@ -72,7 +72,12 @@ __device__ __forceinline__ RayPre prepare_ray(float3 o, float3 d) {
   return r;
 }
 
-// Returns true with t, and barycentric weights (b0, b1, b2) for (v0, v1, v2).
+// Returns true with t and the barycentric weights (b1, b2) of v1 and v2.  Inside/outside
+// is decided with the watertight sheared edge functions of Woop, Benthin and Wald (2013),
+// so rays cannot slip through shared edges.  The hit distance comes from the plane
+// equation, t = Ng.(v0 - o) / Ng.d: a ray starting on the triangle's plane gets t = 0
+// exactly whenever the plane offset is exact (axis-aligned walls), so with tnear = 0 it
+// cannot re-hit the surface it leaves even when the anti-self-intersection offset is 0.
 __device__ __forceinline__ bool intersect_tri(const RayPre& r, float3 v0, float3 v1, float3 v2, float tnear,
                                               float tfar, float* tout, float* b1out, float* b2out) {
   const float3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
@@ -92,10 +97,12 @@ __device__ __forceinline__ bool intersect_tri(const RayPre& r, float3 v0, float3
   if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
   const float det = U + V + W;
   if (det == 0.f) return false;
-  const float T = U * (r.Sz * Az_) + V * (r.Sz * Bz_) + W * (r.Sz * Cz_);
-  const float inv = 1.f / det;
-  const float t = T * inv;
+  const float3 ng = cross3(v1 - v0, v2 - v0);
+  const float den = dot3(ng, r.d);
+  if (den == 0.f) return false;
+  const float t = dot3(ng, A) / den;
   if (!(t > tnear && t <= tfar)) return false;
+  const float inv = 1.f / det;
   *tout = t;
   *b1out = V * inv;
   *b2out = W * inv;

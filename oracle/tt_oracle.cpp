@@ -511,8 +511,11 @@ static void BuildBvh(Scene& s) {
   }
 }
 
-// Watertight ray/triangle test (Woop et al. 2013) in double precision.  Returns true with
-// t in (tnear, tfar] and barycentrics (b1, b2) = Embree's (u, v).
+// Ray/triangle test in double precision: inside/outside from the watertight sheared edge
+// functions of Woop, Benthin and Wald (2013); distance from the plane equation
+// t = Ng.(v0 - o) / Ng.d, exactly 0 for an origin on an axis-aligned triangle, so a ray
+// leaving such a surface with tnear = 0 does not re-hit it.  Returns true with t in
+// (tnear, tfar] and barycentrics (b1, b2) = Embree's (u, v).
 inline bool IntersectTri(V3 org, V3 dir, V3 v0, V3 v1, V3 v2, double tnear, double tfar, double* tout,
                          double* uout, double* vout) {
   int kz = 0;
@@ -521,7 +524,7 @@ inline bool IntersectTri(V3 org, V3 dir, V3 v0, V3 v1, V3 v2, double tnear, doub
   if (ad[2] > ad[kz]) kz = 2;
   int kx = (kz + 1) % 3, ky = (kx + 1) % 3;
   if (dir[kz] < 0) std::swap(kx, ky);
-  const double Sx = dir[kx] / dir[kz], Sy = dir[ky] / dir[kz], Sz = 1.0 / dir[kz];
+  const double Sx = dir[kx] / dir[kz], Sy = dir[ky] / dir[kz];
   const V3 A = v0 - org, B = v1 - org, C = v2 - org;
   const double Ax = A[kx] - Sx * A[kz], Ay = A[ky] - Sy * A[kz];
   const double Bx = B[kx] - Sx * B[kz], By = B[ky] - Sy * B[kz];
@@ -532,8 +535,10 @@ inline bool IntersectTri(V3 org, V3 dir, V3 v0, V3 v1, V3 v2, double tnear, doub
   if ((U < 0 || V < 0 || W < 0) && (U > 0 || V > 0 || W > 0)) return false;
   const double det = U + V + W;
   if (det == 0) return false;
-  const double T = U * (Sz * A[kz]) + V * (Sz * B[kz]) + W * (Sz * C[kz]);
-  const double t = T / det;
+  const V3 ng = Cross(v1 - v0, v2 - v0);
+  const double den = Dot(ng, dir);
+  if (den == 0) return false;
+  const double t = Dot(ng, A) / den;
   if (!(t > tnear && t <= tfar)) return false;
   *tout = t;
   *uout = V / det;
@@ -1278,7 +1283,8 @@ struct Worker {
   }
 
   // PathTracingWorker::RenderPixel, renderingalgorithms_pathtracing.hxx:731-817.
-  void RenderPixel(int pixel, double rgb_out[3], std::vector<double>& light_accum) {
+  template <class SplatVec>
+  void RenderPixel(int pixel, double rgb_out[3], SplatVec* splats) {
     sensor_connection_unit = -1;
     // LambdaSelectionStrategy::WithWeights, shader_util.hxx:83-91.
     int main_idx = smp.UniformInt(0, 11);
@@ -1310,9 +1316,10 @@ struct Worker {
         if (step.node.type == CAMERA) {
           if (sensor_connection_unit >= 0) {
             pw = pw / (double)npix;
-            double rgb[3];
-            SpectralSelectionToRGB(pw, ctx.idx, rgb);
-            for (int k = 0; k < 3; ++k) light_accum[3 * (size_t)sensor_connection_unit + k] += rgb[k];
+            typename SplatVec::value_type rec;
+            rec.unit = sensor_connection_unit;
+            SpectralSelectionToRGB(pw, ctx.idx, rec.rgb);
+            splats->push_back(rec);
           }
         } else {
           path_sample_values = path_sample_values + pw;
@@ -1545,9 +1552,13 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
   if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
   std::atomic<int> next{pixel_begin};
   constexpr int CHUNK = 64;
-  std::vector<std::vector<double>> light(nthreads, std::vector<double>(3 * (size_t)npix, 0.));
+  // Splats land on arbitrary pixels: each thread records (pixel, rgb) and the records are
+  // added to light_accum after the threads join.
+  struct Splat { int unit; double rgb[3]; };
+  std::vector<std::vector<Splat>> splats(nthreads);
   auto body = [&](int tid) {
     Worker w(sc);
+    std::vector<double> scratch;
     for (;;) {
       int p0 = next.fetch_add(CHUNK);
       if (p0 >= pixel_end) break;
@@ -1557,7 +1568,7 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
           uint64_t sample = (uint64_t)sample_offset + sidx;
           w.smp.g.Seed(seed, sample * (uint64_t)npix + (uint64_t)p);
           double rgb[3];
-          w.RenderPixel(p, rgb, light[tid]);
+          w.RenderPixel(p, rgb, &splats[tid]);
           for (int k = 0; k < 3; ++k) accum[3 * (size_t)p + k] += rgb[k];
         }
       }
@@ -1567,7 +1578,8 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
   for (int i = 0; i < nthreads; ++i) th.emplace_back(body, i);
   for (auto& t : th) t.join();
   for (int i = 0; i < nthreads; ++i)
-    for (size_t k = 0; k < light[i].size(); ++k) light_accum[k] += light[i][k];
+    for (const auto& sp : splats[i])
+      for (int k = 0; k < 3; ++k) light_accum[3 * (size_t)sp.unit + k] += sp.rgb[k];
   *splat_count += (uint64_t)spp * (uint64_t)(pixel_end - pixel_begin);
   return 0;
 }

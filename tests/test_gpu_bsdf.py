@@ -107,7 +107,7 @@ def cube_bin(d):
     return (face * CELLS + iu) * CELLS + iv
 
 
-def cube_cell_quadrature(sub=24):
+def cube_cell_quadrature(sub=128):
     """Directions and solid-angle weights of a midpoint rule over every cube cell."""
     g = (np.arange(CELLS * sub) + 0.5) / (CELLS * sub) * 2 - 1
     U, V = np.meshgrid(g, g, indexing="ij")
