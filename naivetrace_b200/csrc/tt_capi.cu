@@ -49,8 +49,8 @@ __global__ void k_tally(const int* counters, int rounds, unsigned long long* sta
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     unsigned long long e = 0, s = 0;
     for (int b = 0; b <= rounds; ++b) {
-      e += (unsigned long long)counters[3 * b];
-      s += (unsigned long long)counters[3 * b + 1];
+      e += (unsigned long long)counters[kCountersPerBounce * b];
+      s += (unsigned long long)counters[kCountersPerBounce * b + 1];
     }
     stats[4] += e;
     stats[5] += s;
@@ -436,7 +436,7 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
   p.ext_q[1] = (int*)m.alloc(n * sizeof(int));
   p.sh_q = (int*)m.alloc(n * sizeof(int));
   p.done_q = (int*)m.alloc(n * sizeof(int));
-  p.counters = (int*)m.alloc(3 * (size_t)(c->rounds + 3) * sizeof(int));
+  p.counters = (int*)m.alloc(kCountersPerBounce * (size_t)(c->rounds + 3) * sizeof(int));
   p.err = c->d_err;
   for (void* a : m.allocs)
     if (!a) {
@@ -498,7 +498,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
     w.npix_total = c->npix;
     w.sample_offset = c->next_sample;
     w.seed = seed;
-    cudaMemsetAsync(c->ps.counters, 0, 3 * (size_t)(rounds + 3) * sizeof(int), c->stream);
+    cudaMemsetAsync(c->ps.counters, 0, kCountersPerBounce * (size_t)(rounds + 3) * sizeof(int), c->stream);
     launch_generate(c->dev, c->ps, c->fb, w, grid, c->stream);
     launches++;
     for (int b = 0; b < rounds; ++b) {

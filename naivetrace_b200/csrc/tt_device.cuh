@@ -76,6 +76,20 @@ struct Rng {
     state += initstate;
     next();
   }
+  // Per-path stream: PCG32 streams with nearby increments are strongly correlated, so the
+  // (seed, path index) pair is scrambled with the SplitMix64 finalizer (Steele, Lea and
+  // Flood 2014) into the initial state and the stream selector.
+  __device__ __forceinline__ static unsigned long long splitmix64(unsigned long long z) {
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  }
+  __device__ __forceinline__ void seed_path(unsigned long long seed, unsigned long long path) {
+    const unsigned long long s1 = splitmix64(seed ^ splitmix64(path));
+    const unsigned long long s2 = splitmix64(s1 ^ 0xd1b54a32d192ed03ULL);
+    this->seed(s1, s2);
+  }
   // 23 random mantissa bits (pcg32::nextFloat): the single-precision twin of nextDouble.
   __device__ __forceinline__ float uniform() { return __uint_as_float((next() >> 9) | 0x3f800000u) - 1.0f; }
   __device__ __forceinline__ void square(float r[2]) { r[0] = uniform(); r[1] = uniform(); }

@@ -14,6 +14,7 @@ constexpr int MAX_ENV_LIGHTS = 4;
 constexpr int BVH_STACK = 64;        // per-thread traversal stack (entries)
 constexpr uint32_t ERR_STACK = 1u;   // error-word bits written by kernels
 constexpr uint32_t ERR_QUEUE = 2u;
+constexpr int kCountersPerBounce = 5;  // ext, shadow, done queue lengths; ext, shadow pool cursors
 
 // Surface material as stored on the device.
 struct DevMaterial {
@@ -85,7 +86,7 @@ struct PathState {
   int* ext_q[2];
   int* sh_q;
   int* done_q;
-  int* counters;       // per bounce: [ext, shadow, done] x (max bounces + 2)
+  int* counters;       // kCountersPerBounce ints per bounce, (max bounces + 3) bounces
   unsigned int* err;
 };
 

@@ -32,9 +32,13 @@ __device__ __forceinline__ int warp_append(int* counter) {
   return base + rank;
 }
 
-__device__ __forceinline__ int* ext_count(const PathState& p, int b) { return &p.counters[3 * b]; }
-__device__ __forceinline__ int* sh_count(const PathState& p, int b) { return &p.counters[3 * b + 1]; }
-__device__ __forceinline__ int* done_count(const PathState& p, int b) { return &p.counters[3 * b + 2]; }
+// Per bounce: queue lengths of extension rays, shadow rays and finished paths, and the
+// work-pool cursors of the persistent closest-hit and shadow kernels.
+__device__ __forceinline__ int* ext_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b]; }
+__device__ __forceinline__ int* sh_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 1]; }
+__device__ __forceinline__ int* done_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 2]; }
+__device__ __forceinline__ int* ext_pool(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 3]; }
+__device__ __forceinline__ int* sh_pool(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 4]; }
 
 // ----------------------------------------------------------------------------------------
 // BVH traversal (layout in tt_bvh.h) with the watertight ray/triangle test of Woop,
@@ -85,9 +89,11 @@ __device__ __forceinline__ bool intersect_tri(const RayPre& r, float3 v0, float3
   const float Ax = comp(A, r.kx) - r.Sx * Az_, Ay = comp(A, r.ky) - r.Sy * Az_;
   const float Bx = comp(B, r.kx) - r.Sx * Bz_, By = comp(B, r.ky) - r.Sy * Bz_;
   const float Cx = comp(C, r.kx) - r.Sx * Cz_, Cy = comp(C, r.ky) - r.Sy * Cz_;
-  float U = Cx * By - Cy * Bx;
-  float V = Ax * Cy - Ay * Cx;
-  float W = Bx * Ay - By * Ax;
+  // Rounded products without fused multiply-add: the edge function of an edge shared by
+  // two triangles must come out as exact negatives in both for the test to be watertight.
+  float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+  float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+  float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
   if (U == 0.f || V == 0.f || W == 0.f) {
     // Edge case: recompute the edge functions in double precision (Woop et al., sec. 4).
     U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
@@ -114,77 +120,130 @@ struct TraceCounters {
   unsigned int tris;
 };
 
-// Closest hit (ANY = false) or any hit (ANY = true).  Returns the triangle slot or -1.
+// Traversal state of one ray.  A step processes one inner node (both child boxes) or one
+// leaf; the persistent kernels interleave steps with refilling lanes whose ray finished.
+struct TraceState {
+  RayPre r;
+  float tnear, best_t, b1, b2;
+  int best, cur, sp;
+};
+
+__device__ __forceinline__ void trace_init(TraceState& s, float3 o, float3 d, float tnear, float tfar) {
+  s.r = prepare_ray(o, d);
+  s.tnear = tnear;
+  s.best_t = tfar;
+  s.b1 = s.b2 = 0.f;
+  s.best = -1;
+  s.cur = 0;  // the root is always an inner node
+  s.sp = 0;
+}
+
+// One traversal step.  Returns true when the ray is finished (closest hit found, or for
+// ANY the first hit), with the result in s.best / best_t / b1 / b2.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState& s, int* stack, unsigned int* err,
+                                           TraceCounters* cnt) {
+  const RayPre& r = s.r;
+  if (s.cur >= 0) {
+    const float4* np = sc.nodes + 4 * (size_t)s.cur;
+    const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+    const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+    if (COUNT) cnt->nodes++;
+    const float lim = s.best_t * 1.0000004f;  // 1 + 2 gamma(3): conservative slabs
+    float tx0 = fmaf(n0.x, r.id.x, -r.ood.x), tx1 = fmaf(n0.y, r.id.x, -r.ood.x);
+    float ty0 = fmaf(n0.z, r.id.y, -r.ood.y), ty1 = fmaf(n0.w, r.id.y, -r.ood.y);
+    float tz0 = fmaf(n2.x, r.id.z, -r.ood.z), tz1 = fmaf(n2.y, r.id.z, -r.ood.z);
+    const float c0min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), s.tnear));
+    const float c0max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+    tx0 = fmaf(n1.x, r.id.x, -r.ood.x); tx1 = fmaf(n1.y, r.id.x, -r.ood.x);
+    ty0 = fmaf(n1.z, r.id.y, -r.ood.y); ty1 = fmaf(n1.w, r.id.y, -r.ood.y);
+    tz0 = fmaf(n2.z, r.id.z, -r.ood.z); tz1 = fmaf(n2.w, r.id.z, -r.ood.z);
+    const float c1min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), s.tnear));
+    const float c1max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+    const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
+    if (h0 && h1) {
+      int near = n3.x, far = n3.y;
+      if (c1min < c0min) { near = n3.y; far = n3.x; }
+      if (s.sp >= BVH_STACK) {
+        atomicOr(err, ERR_STACK);
+        s.best = -1;
+        return true;
+      }
+      stack[s.sp++] = far;
+      s.cur = near;
+      return false;
+    }
+    if (h0) { s.cur = n3.x; return false; }
+    if (h1) { s.cur = n3.y; return false; }
+  } else {
+    const unsigned v = ~(unsigned)s.cur;
+    const int start = (int)(v >> 3), count = (int)(v & 7u) + 1;
+    for (int i = start; i < start + count; ++i) {
+      const float4 a = __ldg(&sc.tris[3 * i]);
+      const float4 b = __ldg(&sc.tris[3 * i + 1]);
+      const float4 c = __ldg(&sc.tris[3 * i + 2]);
+      if (COUNT) cnt->tris++;
+      float t, b1, b2;
+      if (intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2)) {
+        s.best = i;
+        s.best_t = t;
+        s.b1 = b1;
+        s.b2 = b2;
+        if (ANY) return true;
+      }
+    }
+  }
+  if (s.sp == 0) return true;
+  s.cur = stack[--s.sp];
+  return false;
+}
+
+// Recomputes the distance of the closest hit from the plane equation in double precision
+// (float rounding of Ng.(v0 - o) is amplified by 1/|cos| at grazing incidence).
+__device__ __forceinline__ float refine_t(const DevScene& sc, const RayPre& r, int slot) {
+  const float4 a = __ldg(&sc.tris[3 * slot]);
+  const float4 b = __ldg(&sc.tris[3 * slot + 1]);
+  const float4 c = __ldg(&sc.tris[3 * slot + 2]);
+  const double e1x = (double)b.x - a.x, e1y = (double)b.y - a.y, e1z = (double)b.z - a.z;
+  const double e2x = (double)c.x - a.x, e2y = (double)c.y - a.y, e2z = (double)c.z - a.z;
+  const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
+  const double ax = (double)a.x - r.o.x, ay = (double)a.y - r.o.y, az = (double)a.z - r.o.z;
+  const double den = nx * r.d.x + ny * r.d.y + nz * r.d.z;
+  return (float)((nx * ax + ny * ay + nz * az) / den);
+}
+
+// Whole traversal of one ray (batch queries).  Returns the triangle slot or -1.
 template <bool ANY, bool COUNT>
 __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float tnear, float tfar, float* t_out,
                                      float* b1_out, float* b2_out, unsigned int* err, TraceCounters* cnt) {
+  TraceState s;
   int stack[BVH_STACK];
-  int sp = 0;
-  int cur = 0;  // root is always an inner node
-  int best = -1;
-  float best_t = tfar, bb1 = 0.f, bb2 = 0.f;
-  const float box_tmax_scale = 1.0000004f;  // 1 + 2 gamma(3): conservative slabs
-  for (;;) {
-    if (cur >= 0) {
-      const float4* np = sc.nodes + 4 * (size_t)cur;
-      const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
-      const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
-      if (COUNT) cnt->nodes++;
-      const float lim = best_t * box_tmax_scale;
-      // Child 0
-      float tx0 = fmaf(n0.x, r.id.x, -r.ood.x), tx1 = fmaf(n0.y, r.id.x, -r.ood.x);
-      float ty0 = fmaf(n0.z, r.id.y, -r.ood.y), ty1 = fmaf(n0.w, r.id.y, -r.ood.y);
-      float tz0 = fmaf(n2.x, r.id.z, -r.ood.z), tz1 = fmaf(n2.y, r.id.z, -r.ood.z);
-      const float c0min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tnear));
-      const float c0max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
-      // Child 1
-      tx0 = fmaf(n1.x, r.id.x, -r.ood.x); tx1 = fmaf(n1.y, r.id.x, -r.ood.x);
-      ty0 = fmaf(n1.z, r.id.y, -r.ood.y); ty1 = fmaf(n1.w, r.id.y, -r.ood.y);
-      tz0 = fmaf(n2.z, r.id.z, -r.ood.z); tz1 = fmaf(n2.w, r.id.z, -r.ood.z);
-      const float c1min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tnear));
-      const float c1max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
-      const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
-      if (h0 && h1) {
-        int near = n3.x, far = n3.y;
-        if (c1min < c0min) { near = n3.y; far = n3.x; }
-        if (sp >= BVH_STACK) { atomicOr(err, ERR_STACK); return -1; }
-        stack[sp++] = far;
-        cur = near;
-        continue;
-      } else if (h0) {
-        cur = n3.x;
-        continue;
-      } else if (h1) {
-        cur = n3.y;
-        continue;
-      }
-    } else {
-      const unsigned v = ~(unsigned)cur;
-      const int start = (int)(v >> 3), count = (int)(v & 7u) + 1;
-      for (int i = start; i < start + count; ++i) {
-        const float4 a = __ldg(&sc.tris[3 * i]);
-        const float4 b = __ldg(&sc.tris[3 * i + 1]);
-        const float4 c = __ldg(&sc.tris[3 * i + 2]);
-        if (COUNT) cnt->tris++;
-        float t, b1, b2;
-        if (intersect_tri(r, xyz(a), xyz(b), xyz(c), tnear, best_t, &t, &b1, &b2)) {
-          best = i;
-          best_t = t;
-          bb1 = b1;
-          bb2 = b2;
-          if (ANY) { *t_out = t; return i; }
-        }
-      }
-    }
-    if (sp == 0) break;
-    cur = stack[--sp];
+  s.r = r;
+  s.tnear = tnear;
+  s.best_t = tfar;
+  s.b1 = s.b2 = 0.f;
+  s.best = -1;
+  s.cur = 0;
+  s.sp = 0;
+  while (!trace_step<ANY, COUNT>(sc, s, stack, err, cnt)) {
   }
-  if (best >= 0) {
-    *t_out = best_t;
-    *b1_out = bb1;
-    *b2_out = bb2;
+  if (s.best >= 0) {
+    *t_out = ANY ? s.best_t : refine_t(sc, r, s.best);
+    *b1_out = s.b1;
+    *b2_out = s.b2;
   }
-  return best;
+  return s.best;
+}
+
+// Warp-aggregated fetch of the next work item from a pool cursor.
+__device__ __forceinline__ int pool_fetch(int* cursor) {
+  const unsigned m = __activemask();
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(cursor, __popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + __popc(m & ((1u << lane) - 1u));
 }
 
 // ----------------------------------------------------------------------------------------
@@ -355,7 +414,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     const unsigned long long sample = w.sample_offset + (unsigned long long)(g / w.npix_range);
     const int pixel = w.pixel_begin + pix_local;
     Rng rng;
-    rng.seed(w.seed, sample * (unsigned long long)w.npix_total + (unsigned long long)pixel);
+    rng.seed_path(w.seed, sample * (unsigned long long)w.npix_total + (unsigned long long)pixel);
     // LambdaSelectionStrategy::WithWeights (shader_util.hxx:83-91).
     const int main_idx = rng.uniform_int(0, 11);
     int idx[3] = {main_idx, main_idx + 12, main_idx + 24};
@@ -406,19 +465,31 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
   }
 }
 
+// Closest hit of the queued extension rays.  Persistent: every lane whose ray finished
+// fetches the next one from the bounce's pool, so warps stay full until the queue drains
+// (dynamic ray fetching, Aila and Laine 2009).
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bounce,
-                                                unsigned long long* counters) {
+__global__ void __launch_bounds__(256, 4) k_extend(DevScene sc, PathState p, int bounce, unsigned long long* counters) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
+  int* pool = ext_pool(p, bounce);
   TraceCounters cnt{0u, 0u};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int slot = q[i];
-    const float4 o = p.ray_o[slot], d = p.ray_d[slot];
-    const RayPre r = prepare_ray(xyz(o), xyz(d));
-    float t = 0.f, b1 = 0.f, b2 = 0.f;
-    const int hit = trace<false, COUNT>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
-    p.hit[slot] = make_float4(t, b1, b2, __int_as_float(hit));
+  TraceState s;
+  int stack[BVH_STACK];
+  int slot = -1;
+  for (;;) {
+    if (slot < 0) {
+      const int item = pool_fetch(pool);
+      if (item >= n) break;
+      slot = q[item];
+      const float4 o = p.ray_o[slot], d = p.ray_d[slot];
+      trace_init(s, xyz(o), xyz(d), 0.f, d.w);
+    }
+    if (trace_step<false, COUNT>(sc, s, stack, p.err, &cnt)) {
+      const float t = s.best >= 0 ? refine_t(sc, s.r, s.best) : 0.f;
+      p.hit[slot] = make_float4(t, s.b1, s.b2, __int_as_float(s.best));
+      slot = -1;
+    }
   }
   if (COUNT) {
     atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
@@ -537,34 +608,46 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
   }
 }
 
+// Occlusion test of the queued shadow rays (persistent, like k_extend).  Unoccluded rays
+// add their contribution to the path (or, for camera-vertex samples, splat it).
 template <bool COUNT>
-__global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Framebuffer fb, int bounce,
-                                                unsigned long long* counters) {
+__global__ void __launch_bounds__(256, 4) k_shadow(DevScene sc, PathState p, Framebuffer fb, int bounce,
+                                                   unsigned long long* counters) {
   const int n = *sh_count(p, bounce);
+  int* pool = sh_pool(p, bounce);
   TraceCounters cnt{0u, 0u};
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int slot = p.sh_q[i];
-    const float4 o = p.sh_o[slot], d = p.sh_d[slot];
-    const RayPre r = prepare_ray(xyz(o), xyz(d));
-    float t, b1, b2;
-    const int hit = trace<true, COUNT>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
-    if (hit >= 0) continue;
-    const float4 c = p.sh_c[slot];
-    const int target = __float_as_int(d.w);
-    if (target < 0) {
-      float4 a = p.accum[slot];
-      p.accum[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, 0.f);
-    } else {
-      const Lambda l = unpack_lambda(p.meta[slot].y);
-      const float3 rgb = selection_to_rgb(xyz(c), l);
-      atomicAdd(&fb.light[3 * target], rgb.x);
-      atomicAdd(&fb.light[3 * target + 1], rgb.y);
-      atomicAdd(&fb.light[3 * target + 2], rgb.z);
+  TraceState s;
+  int stack[BVH_STACK];
+  int slot = -1;
+  for (;;) {
+    if (slot < 0) {
+      const int item = pool_fetch(pool);
+      if (item >= n) break;
+      slot = p.sh_q[item];
+      const float4 o = p.sh_o[slot], d = p.sh_d[slot];
+      trace_init(s, xyz(o), xyz(d), 0.f, o.w);
+    }
+    if (trace_step<true, COUNT>(sc, s, stack, p.err, &cnt)) {
+      if (s.best < 0) {
+        const float4 c = p.sh_c[slot];
+        const int target = __float_as_int(p.sh_d[slot].w);
+        if (target < 0) {
+          const float4 a = p.accum[slot];
+          p.accum[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, 0.f);
+        } else {
+          const Lambda l = unpack_lambda(p.meta[slot].y);
+          const float3 rgb = selection_to_rgb(xyz(c), l);
+          atomicAdd(&fb.light[3 * target], rgb.x);
+          atomicAdd(&fb.light[3 * target + 1], rgb.y);
+          atomicAdd(&fb.light[3 * target + 2], rgb.z);
+        }
+      }
+      slot = -1;
     }
   }
   if (COUNT) {
-    atomicAdd(&counters[2], (unsigned long long)cnt.nodes);
-    atomicAdd(&counters[3], (unsigned long long)cnt.tris);
+    atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
+    atomicAdd(&counters[1], (unsigned long long)cnt.tris);
   }
 }
 
@@ -648,7 +731,7 @@ __global__ void k_sample_bsdf(DevScene sc, int material, float3 wi, int3 li, int
   const Surf s = zup_surface(wi);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     Rng rng;
-    rng.seed(seed, (unsigned long long)i);
+    rng.seed_path(seed, (unsigned long long)i);
     ScatterSample ss = sample_bsdf(sc.materials[material], wi, s, rng, l);
     dir[3 * i] = ss.dir.x; dir[3 * i + 1] = ss.dir.y; dir[3 * i + 2] = ss.dir.z;
     val[3 * i] = ss.value.x; val[3 * i + 1] = ss.value.y; val[3 * i + 2] = ss.value.z;
@@ -684,12 +767,28 @@ void upload_constant_tables() {
 
 constexpr int kBlock = 256;
 
+// Persistent traversal grid: every SM filled to the kernels' occupancy limit.
+static int trace_grid() {
+  static int g = 0;
+  if (g == 0) {
+    int dev = 0, sms = 0, b0 = 0, b1 = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false>, kBlock, 0);
+    g = sms * (b0 < b1 ? b0 : b1);
+    if (g < 1) g = 1;
+  }
+  return g;
+}
+
 void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
                      cudaStream_t st) {
   k_generate<<<grid, kBlock, 0, st>>>(s, p, fb, w);
 }
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
                    cudaStream_t st) {
+  grid = trace_grid();
   if (count) k_extend<true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
   else k_extend<false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
 }
@@ -698,6 +797,7 @@ void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, c
 }
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
+  grid = trace_grid();
   if (count) k_shadow<true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
   else k_shadow<false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
 }
@@ -735,9 +835,6 @@ void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, c
 int kernel_blocks_per_sm() {
   int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade, kBlock, 0);
-  int e = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&e, k_extend<false>, kBlock, 0);
-  if (e < b) b = e;
   return b < 1 ? 1 : b;
 }
 

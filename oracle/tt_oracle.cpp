@@ -122,6 +122,21 @@ struct Pcg32 {
   }
 };
 
+// Per-path stream: PCG32 streams whose increments differ by small amounts are strongly
+// correlated, so the (seed, path index) pair is first scrambled with the SplitMix64
+// finalizer (Steele, Lea and Flood 2014) into the initial state and the stream selector.
+inline uint64_t SplitMix64(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ULL;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+inline void SeedPath(Pcg32& g, uint64_t seed, uint64_t path) {
+  const uint64_t s1 = SplitMix64(seed ^ SplitMix64(path));
+  const uint64_t s2 = SplitMix64(s1 ^ 0xd1b54a32d192ed03ULL);
+  g.Seed(s1, s2);
+}
+
 // One stream per path; Uniform01 / UniformUnitSquare / UniformInt as Sampler and RandGen.
 struct Sampler {
   Pcg32 g;
@@ -1566,7 +1581,7 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
       for (int p = p0; p < p1; ++p) {
         for (int sidx = 0; sidx < spp; ++sidx) {
           uint64_t sample = (uint64_t)sample_offset + sidx;
-          w.smp.g.Seed(seed, sample * (uint64_t)npix + (uint64_t)p);
+          SeedPath(w.smp.g, seed, sample * (uint64_t)npix + (uint64_t)p);
           double rgb[3];
           w.RenderPixel(p, rgb, &splats[tid]);
           for (int k = 0; k < 3; ++k) accum[3 * (size_t)p + k] += rgb[k];
@@ -1603,7 +1618,7 @@ int or_sample_bsdf(or_scene* s, int material, const double* wi, const int32_t* l
   Surf si = ZUpSurface(w);
   for (int i = 0; i < n; ++i) {
     Sampler smp;
-    smp.g.Seed(seed, (uint64_t)i);
+    SeedPath(smp.g, seed, (uint64_t)i);
     ScatterSample ss = SampleBSDF(m, w, si, smp, lambda_idx);
     out_dir[3 * i] = ss.dir.x; out_dir[3 * i + 1] = ss.dir.y; out_dir[3 * i + 2] = ss.dir.z;
     for (int k = 0; k < 3; ++k) out_value[3 * i + k] = ss.value[k];

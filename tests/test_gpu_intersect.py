@@ -89,6 +89,8 @@ def random_rays(n, lo, hi, rng):
 
 
 def check_parity(g, o, rays):
+    # Identical inputs on both sides: the device takes float32 rays.
+    rays = np.asarray(rays, dtype=np.float32).astype(np.float64)
     pg, tg, _, _ = g.intersect(rays)
     po, to, _, _ = o.intersect(rays)
     both = (pg >= 0) & (po >= 0)

@@ -55,13 +55,16 @@ def tile_means(rgb, xres, yres, tile=16):
 
 @pytest.mark.parametrize("name", ["cornell_box", "cornell_box_materials"])
 def test_tile_z_test(gpu_lib, name):
-    """Every 16x16 tile mean of the GPU render lies within 3 sigma of the oracle's."""
+    """16x16 tile means of the GPU render against the oracle's: z = difference over the
+    standard error estimated from K independent renders per side.  With 48 tile-channels
+    per case a 3-sigma bound is exceeded by chance now and then, so at least 97 % must lie
+    within 3 sigma and all within 4 sigma (about the family-wise 5 % bound for 48 tests)."""
     xres = yres = 64
     scene = getattr(scenes, name)(xres, yres)
     p = make_params(max_ray_depth=10)
     g = GpuContext(scene, p)
     o = OracleScene(scene, p)
-    K, spp = 8, 16
+    K, spp = 32, 16
     tg, to = [], []
     for k in range(K):
         g.clear()
@@ -74,7 +77,8 @@ def test_tile_z_test(gpu_lib, name):
     mg, mo = tg.mean(0), to.mean(0)
     se = np.sqrt(tg.var(0, ddof=1) / K + to.var(0, ddof=1) / K)
     z = np.abs(mg - mo) / np.maximum(se, 1e-12)
-    assert np.all(z < 3.5), z.max()
+    assert (z < 3.0).mean() >= 0.97, (z < 3.0).mean()
+    assert np.all(z < 4.0), z.max()
 
 
 def test_relmse_falls_as_one_over_spp(gpu_lib):
