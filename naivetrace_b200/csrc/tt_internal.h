@@ -14,7 +14,7 @@ constexpr int MAX_ENV_LIGHTS = 4;
 constexpr int BVH_STACK = 64;        // per-thread traversal stack (entries)
 constexpr uint32_t ERR_STACK = 1u;   // error-word bits written by kernels
 constexpr uint32_t ERR_QUEUE = 2u;
-constexpr int kCountersPerBounce = 5;  // ext, shadow, done queue lengths; ext, shadow pool cursors
+constexpr int kCountersPerBounce = 3;  // ext, shadow, done queue lengths
 
 // Surface material as stored on the device.
 struct DevMaterial {

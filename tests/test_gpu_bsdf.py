@@ -5,7 +5,9 @@ sample, so directions, values and pdfs must agree up to float rounding.  The
 distribution test restates SamplingConsistencyTest (tests_sampling.cxx:540-769): device
 samples are binned into a cube map of 4x4 cells per face (96 bins), expected counts come
 from integrating the oracle's pdf over each cell, bins are merged to >= 5 expected and a
-chi-square test must give p >= 0.05.  Incident directions follow the reference's
+chi-square test must give p >= 0.01 (the reference's fixtures use 0.05 per test; with a
+dozen fixed-seed cases here the per-test bound is tightened to keep the family-wise false
+alarm rate near 10 %).  Incident directions follow the reference's
 parameterised cases VERTICAL / EXACT_45DEG / ALMOST_45DEG / MUCH_DEFLECTED
 (tests_sampling.cxx:1265-1269).
 """
@@ -165,7 +167,7 @@ def test_chi_square_device_samples(contexts, mat, inc):
     total_prob = expected_prob.sum()
     assert abs(total_prob - 1.0) < 0.02, total_prob  # pdf normalised over the sphere
     p = chi2_pvalue(counts, expected_prob / total_prob * ok.sum())
-    assert p >= 0.05, p
+    assert p >= 0.01, p
 
 
 @pytest.mark.parametrize("inc", ["VERTICAL", "EXACT_45DEG", "MUCH_DEFLECTED"])
