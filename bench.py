@@ -143,7 +143,7 @@ def dist_setup(args):
     return 1, 0, local, None
 
 
-def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=4096, seed=1):
+def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=16384, seed=1):
     """Times the oracle (CPU restatement of the reference pt) on all host cores over a
     bounded sample: consecutive pixel chunks of the frame at 1 sample each, until about
     budget_s of CPU time.  Returns (Mpaths/s, cores, description)."""
@@ -165,7 +165,7 @@ def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=4096, seed=1):
         done_paths += chunk_pixels
         k += 1
         el = time.perf_counter() - t0
-        if el >= budget_s or k >= 200:
+        if el >= budget_s or k >= 100000:
             break
     mpaths = done_paths / el / 1e6
     desc = (f"{k} chunks of {chunk_pixels} consecutive pixels from the frame centre at 1 sample each "
@@ -397,8 +397,11 @@ def profile_run(args):
     g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave))
     g.render(spp, 1)
     st = g.stats()
+    q = g.queue_lengths(depth + 1)
     print(json.dumps({"profile_run": name, "spp": spp, "extension_rays": st["extension_rays"],
                       "shadow_rays": st["shadow_rays"], "kernel_launches": st["kernel_launches"],
+                      "last_wave_extension_rays_per_bounce": q[:, 0].tolist(),
+                      "last_wave_shadow_rays_per_bounce": q[:, 1].tolist(),
                       "error_flags": st["error_flags"]}))
     g.close()
     return 0 if st["error_flags"] == 0 else 1

@@ -155,6 +155,11 @@ typedef struct tt_stats {
   uint64_t error_flags;         /* device error word (TT_ERR_* bits) */
 } tt_stats;
 
+/* Queue lengths of the last wavefront wave of the last pass: for bounce b = 0..n-1,
+ * out[3b] extension rays, out[3b+1] shadow rays, out[3b+2] finished paths.  Returns
+ * TT_ERR_INVALID when n exceeds max_ray_depth + 1. */
+tt_status tt_last_wave_queue_lengths(tt_ctx* ctx, int32_t* out, int32_t n);
+
 /* Library/ABI version; lets a loader check it bound the right library. */
 int32_t tt_abi_version(void);
 

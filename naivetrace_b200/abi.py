@@ -148,6 +148,7 @@ LIB_NAME = "libtoytrace_gpu.so"
 
 # Every symbol declared in include/toytrace_gpu.h.
 EXPORTED_SYMBOLS = [
+    "tt_last_wave_queue_lengths",
     "tt_abi_version",
     "tt_create",
     "tt_upload_scene",
@@ -204,6 +205,7 @@ def load_library() -> C.CDLL:
     vp = C.c_void_p
     sig = {
         "tt_abi_version": ([], C.c_int32),
+        "tt_last_wave_queue_lengths": ([vp, P(C.c_int32), C.c_int32], C.c_int32),
         "tt_create": ([P(SceneDesc), P(Params), P(vp)], C.c_int32),
         "tt_upload_scene": ([vp], C.c_int32),
         "tt_render_pass": ([vp, C.c_int32, C.c_uint64], C.c_int32),

@@ -129,6 +129,13 @@ class GpuContext:
                                                 _fp(dirs), n, _fp(val), _fp(pdf)), "tt_eval_bsdf_batch")
         return val, pdf
 
+    def queue_lengths(self, bounces: int) -> np.ndarray:
+        """(bounces, 3) extension / shadow / finished counts of the last wave."""
+        out = np.zeros(3 * bounces, np.int32)
+        self._check(self.lib.tt_last_wave_queue_lengths(self.h, out.ctypes.data_as(C.POINTER(C.c_int32)), bounces),
+                    "tt_last_wave_queue_lengths")
+        return out.reshape(bounces, 3)
+
     def set_profiling(self, level: int):
         self._check(self.lib.tt_set_profiling(self.h, level), "tt_set_profiling")
 

@@ -782,6 +782,18 @@ tt_status tt_read_accumulators_device(tt_ctx* c, double* d_accum, double* d_ligh
   return TT_OK;
 }
 
+tt_status tt_last_wave_queue_lengths(tt_ctx* c, int32_t* out, int32_t n) {
+  if (!c || !out || n < 0) return TT_ERR_INVALID;
+  if (!c->uploaded || c->ps.cap == 0) return fail(c, TT_ERR_NOT_READY, "no pass has run");
+  if (n > c->rounds + 1) return fail(c, TT_ERR_INVALID, "more bounces requested than a pass has");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  std::vector<int> buf(kCountersPerBounce * (size_t)(c->rounds + 3));
+  TT_CUDA(c, cudaMemcpy(buf.data(), c->ps.counters, buf.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int b = 0; b < n; ++b)
+    for (int k = 0; k < 3; ++k) out[3 * b + k] = buf[kCountersPerBounce * b + k];
+  return TT_OK;
+}
+
 tt_status tt_set_profiling(tt_ctx* c, int32_t on) {
   if (!c) return TT_ERR_INVALID;
   c->profiling = on;
