@@ -180,6 +180,28 @@ tt_status tt_render_pass(tt_ctx* ctx, int32_t spp, uint64_t seed);
 tt_status tt_render_pass_range(tt_ctx* ctx, int32_t spp, uint64_t seed,
                                int32_t pixel_begin, int32_t pixel_end);
 
+/* Render pass that allocates no memory.  No counterpart in the reference: it exists for
+ * callers that cannot let a library call cudaMalloc at render time -- applications that
+ * own all GPU memory through their own pool or a fixed budget, or code where an
+ * allocation would synchronise the device and stall concurrent work.  The wavefront path
+ * state lives in one static device array inside the library (about 11.6 MB, held by every
+ * GPU that loads the library until the process exits) instead of memory the context
+ * allocates.  The caller passes the outputs: d_accum and d_light_accum are device buffers
+ * of xres*yres*3 floats to which the pass ADDS the unnormalised RGB sums of its samples and
+ * the camera-vertex splats (already weighted by 1/(xres*yres)), like one pass of
+ * tt_render_pass before it folds them into its own accumulators; sample numbers
+ * sample_offset .. sample_offset+spp-1 select the same random streams tt_render_pass uses.
+ * The context's own accumulators, counters and statistics are not touched.
+ * Limits: at most 65,536 camera samples (spp x pixels in [pixel_begin, pixel_end)) per
+ * call and max_ray_depth <= 1000, else TT_ERR_CAPACITY.  Calls on one device share the
+ * static array: calls that overlap on the GPU race.  The call returns after the work has
+ * finished on `stream` (a cudaStream_t; NULL = legacy default stream).  Its first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress) and must come before
+ * any stream capture.  Requires tt_upload_scene (which allocates the scene) to have run. */
+tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t seed, int32_t pixel_begin,
+                                 int32_t pixel_end, uint64_t sample_offset, float* d_accum,
+                                 float* d_light_accum, void* stream);
+
 /* RenderingAlgo::RequestInterrupt / RequestFullStop: lock-free flag writes, callable from
  * any thread, also before the first pass.  A stop makes the running and all later
  * passes return TT_ERR_INTERRUPTED at the next wave boundary. */

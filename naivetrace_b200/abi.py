@@ -154,6 +154,7 @@ EXPORTED_SYMBOLS = [
     "tt_upload_scene",
     "tt_render_pass",
     "tt_render_pass_range",
+    "tt_render_pass_noalloc",
     "tt_request_interrupt",
     "tt_request_stop",
     "tt_poll_interrupt",
@@ -210,6 +211,7 @@ def load_library() -> C.CDLL:
         "tt_upload_scene": ([vp], C.c_int32),
         "tt_render_pass": ([vp, C.c_int32, C.c_uint64], C.c_int32),
         "tt_render_pass_range": ([vp, C.c_int32, C.c_uint64, C.c_int32, C.c_int32], C.c_int32),
+        "tt_render_pass_noalloc": ([vp, C.c_int32, C.c_uint64, C.c_int32, C.c_int32, C.c_uint64, vp, vp, vp], C.c_int32),
         "tt_request_interrupt": ([vp], C.c_int32),
         "tt_request_stop": ([vp], C.c_int32),
         "tt_poll_interrupt": ([vp], C.c_int32),

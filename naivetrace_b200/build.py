@@ -19,7 +19,7 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_build"
 LIB = OUT_DIR / "libtoytrace_gpu.so"
 
-SOURCES = ["tt_kernels.cu", "tt_capi.cu", "tt_bvh.cpp"]
+SOURCES = ["tt_kernels.cu", "tt_capi.cu", "tt_noalloc.cu", "tt_bvh.cpp"]
 HEADERS = ["tt_internal.h", "tt_device.cuh", "tt_bvh.h", "tt_tables.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

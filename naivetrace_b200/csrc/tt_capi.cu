@@ -555,6 +555,22 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
   return TT_OK;
 }
 
+namespace tt {
+// Read access to an uploaded context's scene record for tt_render_pass_noalloc.
+bool context_scene(tt_ctx* c, DevScene* scene, int* device, int* npix, int* max_depth, std::string** err) {
+  if (!c->uploaded) {
+    c->err = "tt_upload_scene has not run";
+    return false;
+  }
+  *scene = c->dev;
+  *device = c->device;
+  *npix = c->npix;
+  *max_depth = c->rounds;
+  *err = &c->err;
+  return true;
+}
+}  // namespace tt
+
 extern "C" {
 
 tt_status tt_render_pass(tt_ctx* c, int32_t spp, uint64_t seed) {
