@@ -126,23 +126,6 @@ def hbm_peak():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        backend = "nccl" if torch.cuda.is_available() else "gloo"
-        if backend == "nccl":
-            torch.cuda.set_device(local)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
-        return world, rank, local, dist
-    return 1, 0, local, None
-
-
 def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=16384, seed=1):
     """Times the oracle (CPU restatement of the reference pt) on all host cores over a
     bounded sample: consecutive pixel chunks of the frame at 1 sample each, until about
@@ -174,10 +157,11 @@ def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=16384, seed=1):
 
 
 def run_reference_arm(args):
-    world, rank, local, dist = dist_setup(args)
+    from naivetrace_b200 import dist as nd
+    r = nd.init_from_env()
+    world, rank = r.world, r.rank
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        nd.shutdown(r)
         return 0
     scene, spp, depth, name = workload(args)
     vals = []
@@ -211,8 +195,7 @@ def run_reference_arm(args):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
-    if dist is not None:
-        dist.destroy_process_group()
+    nd.shutdown(r)
     return 0
 
 
@@ -229,15 +212,17 @@ def run_ours(args):
     import torch
 
     from naivetrace_b200 import abi
+    from naivetrace_b200 import dist as nd
     from naivetrace_b200.algo import GpuContext
     from naivetrace_b200.scene import make_params
 
-    world, rank, local, dist = dist_setup(args)
+    r = nd.init_from_env()
+    world, rank, local = r.world, r.rank, r.local
     device = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(device)
     scene, spp, depth, name = workload(args)
     params = make_params(max_ray_depth=depth, wave_paths=args.wave, device=device)
-    seed = 1 + rank
+    seed = nd.rank_seed(1, rank)
     g = GpuContext(scene, params)
     npix = g.npix
     paths_per_step = npix * spp
@@ -256,19 +241,18 @@ def run_ours(args):
     g.reset_stats()
 
     fb_tensors = None
-    if dist is not None:
+    if r.distributed:
         fb_tensors = (torch.zeros(3 * npix, dtype=torch.float64, device="cuda"),
                       torch.zeros(3 * npix, dtype=torch.float64, device="cuda"))
 
     def step():
         g.render(spp, seed)
-        if dist is not None:
+        if r.distributed:
             s = torch.cuda.current_stream().cuda_stream
             st = g.lib.tt_read_accumulators_device(g.h, C.c_void_p(fb_tensors[0].data_ptr()),
                                                    C.c_void_p(fb_tensors[1].data_ptr()), C.c_void_p(s))
             abi.check(g.lib, g.h, st, "tt_read_accumulators_device")
-            dist.all_reduce(fb_tensors[0])
-            dist.all_reduce(fb_tensors[1])
+            nd.allreduce_sum_(fb_tensors, r)
 
     for _ in range(args.warmup):
         step()
@@ -276,8 +260,7 @@ def run_ours(args):
     g.reset_stats()
     g.set_profiling(1)
     clocks = ClockSampler(device)
-    if dist is not None:
-        dist.barrier()
+    nd.barrier(r)
     torch.cuda.synchronize()
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -287,18 +270,14 @@ def run_ours(args):
         step()
     ev1.record()
     torch.cuda.synchronize()
-    if dist is not None:
-        dist.barrier()
+    nd.barrier(r)
     clk = clocks.stop()
     elapsed_ms = ev0.elapsed_time(ev1)
     st = g.stats()
     g.set_profiling(0)
-    if dist is not None:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = nd.max_over_ranks(elapsed_ms, r)
     ms_per_step = elapsed_ms / args.steps
-    value = world * paths_per_step / (ms_per_step * 1e-3) / 1e6
+    value = nd.weak_scaling_value(paths_per_step, world, ms_per_step)
     mrays = world * (st["extension_rays"] + st["shadow_rays"]) / args.steps / (ms_per_step * 1e-3) / 1e6
     # Roofline of the dominant kernel (closest-hit traversal).
     ext_launch_ms = st["extend_ms"] / max(st["extend_launches"], 1)
@@ -321,8 +300,7 @@ def run_ours(args):
     h2d = scene_bytes(scene)
     rgb = np.zeros(3 * npix, np.float32)
     for _ in range(args.e2e_steps):
-        if dist is not None:
-            dist.barrier()
+        nd.barrier(r)
         t0 = time.perf_counter()
         ge = GpuContext(scene, params)
         ge.render(spp, seed)
@@ -330,11 +308,8 @@ def run_ours(args):
         ge.close()
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_step = float(np.median(e2e_ms)) if e2e_ms else float("nan")
-    if dist is not None:
-        t = torch.tensor([e2e_step], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_step = float(t.item())
-    e2e_value = world * paths_per_step / (e2e_step * 1e-3) / 1e6
+    e2e_step = nd.max_over_ranks(e2e_step, r)
+    e2e_value = nd.weak_scaling_value(paths_per_step, world, e2e_step)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -385,8 +360,7 @@ def run_ours(args):
         }
         print(json.dumps(line))
     g.close()
-    if dist is not None:
-        dist.destroy_process_group()
+    nd.shutdown(r)
     return 0
 
 
