@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 1
+#define TT_ABI_VERSION 2
 
 typedef int32_t tt_status;
 enum {
@@ -49,16 +49,39 @@ enum {
   TT_SHADER_MICROFACET = 3           /* MicrofacetShader (Beckmann, VNDF) shader.cxx:634-707 */
 };
 
-/* A material = shader + optional area emitter (struct Material, src/scene.hxx:45-54). */
+/* A material = shader + optional area emitter + optional media on either side
+ * (struct Material, src/scene.hxx:45-54).  A material with volume_boundary set has no
+ * shader: its triangles only delimit media, are invisible to rays and live in a separate
+ * acceleration structure (Scene::BuildAccelStructure's volume scene, scene.cxx:131-137). */
 typedef struct tt_material {
-  int32_t shader;                  /* TT_SHADER_* */
+  int32_t shader;                  /* TT_SHADER_* (ignored for volume boundaries) */
   float reflectance[TT_NBINS];     /* kr_d / kr_s per bin (diffuse, mirror, microfacet) */
   float alpha;                     /* Beckmann roughness (microfacet) */
   float ior_ratio;                 /* inside / outside IOR (dielectric) */
   int32_t emissive;                /* nonzero: UniformAreaLight on every triangle */
   float emission[TT_NBINS];        /* UniformAreaLight spectrum (area power density;
                                       radiance = spectrum / 2pi, light.hxx:72-108) */
+  int32_t medium_inside;           /* 1 + index of the medium behind the winding normal,
+                                      0 = none (zero-initialised materials have no media) */
+  int32_t medium_outside;          /* 1 + index of the medium the normal points into, 0 = none */
+  int32_t volume_boundary;         /* nonzero: medium boundary only, no surface */
 } tt_material;
+
+/* Phase functions (src/phasefunctions.cxx). */
+enum { TT_PHASE_UNIFORM = 0, TT_PHASE_RAYLEIGH = 1, TT_PHASE_HENYEY_GREENSTEIN = 2 };
+enum { TT_MEDIUM_HOMOGENEOUS = 0 };
+
+/* HomogeneousMedium (shader.cxx:1234-1316): coefficients per bin, per unit length.
+ * Priority decides which of overlapping media is current (MediumTracker,
+ * rendering_util.hxx:18-126); empty space has priority -1. */
+typedef struct tt_medium {
+  int32_t kind;                    /* TT_MEDIUM_* */
+  int32_t priority;
+  float sigma_s[TT_NBINS];
+  float sigma_a[TT_NBINS];
+  int32_t phase;                   /* TT_PHASE_* */
+  float phase_g;                   /* Henyey-Greenstein asymmetry */
+} tt_medium;
 
 /* Environmental lights: the members of TotalEnvironmentalRadianceField (light.hxx:292-304). */
 enum {
@@ -116,6 +139,8 @@ typedef struct tt_scene_desc {
   const tt_env_light* env_lights;
   uint32_t num_point_lights;
   const tt_point_light* point_lights;
+  uint32_t num_media;
+  const tt_medium* media;
   tt_camera camera;
 } tt_scene_desc;
 

@@ -55,6 +55,26 @@ class Material(C.Structure):
         ("ior_ratio", C.c_float),
         ("emissive", C.c_int32),
         ("emission", C.c_float * NBINS),
+        ("medium_inside", C.c_int32),
+        ("medium_outside", C.c_int32),
+        ("volume_boundary", C.c_int32),
+    ]
+
+
+PHASE_UNIFORM = 0
+PHASE_RAYLEIGH = 1
+PHASE_HENYEY_GREENSTEIN = 2
+MEDIUM_HOMOGENEOUS = 0
+
+
+class Medium(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("priority", C.c_int32),
+        ("sigma_s", C.c_float * NBINS),
+        ("sigma_a", C.c_float * NBINS),
+        ("phase", C.c_int32),
+        ("phase_g", C.c_float),
     ]
 
 
@@ -101,6 +121,8 @@ class SceneDesc(C.Structure):
         ("env_lights", C.POINTER(EnvLight)),
         ("num_point_lights", C.c_uint32),
         ("point_lights", C.POINTER(PointLight)),
+        ("num_media", C.c_uint32),
+        ("media", C.POINTER(Medium)),
         ("camera", Camera),
     ]
 

@@ -160,7 +160,12 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
       return fail(nullptr, TT_ERR_INVALID, "microfacet roughness must be positive");
     if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && !(m.ior_ratio > 0.f))
       return fail(nullptr, TT_ERR_INVALID, "dielectric ior_ratio must be positive");
+    if (m.medium_inside < 0 || m.medium_inside > (int)d->num_media || m.medium_outside < 0 ||
+        m.medium_outside > (int)d->num_media)
+      return fail(nullptr, TT_ERR_INVALID, "medium index out of range in material " + std::to_string(i));
   }
+  if (d->num_media > 0 && !d->media) return fail(nullptr, TT_ERR_INVALID, "media missing");
+  if (d->num_media > 0) return fail(nullptr, TT_ERR_INVALID, "participating media are not supported by this build");
   auto* c = new tt_ctx;
   c->verts.assign(d->vertices, d->vertices + 3 * (size_t)d->num_vertices);
   if (d->normals) c->normals.assign(d->normals, d->normals + 3 * (size_t)d->num_vertices);

@@ -30,6 +30,9 @@ class MaterialSpec:
     alpha: float = 0.0
     ior_ratio: float = 1.5
     emission: Optional[np.ndarray] = None
+    medium_inside: int = -1
+    medium_outside: int = -1
+    volume_boundary: bool = False
 
     def to_c(self) -> abi.Material:
         m = abi.Material()
@@ -40,7 +43,37 @@ class MaterialSpec:
         if self.emission is not None:
             m.emissive = 1
             m.emission[:] = [float(x) for x in as_spectrum(self.emission)]
+        m.medium_inside = int(self.medium_inside) + 1  # C ABI: 0 = none, k = medium k-1
+        m.medium_outside = int(self.medium_outside) + 1
+        m.volume_boundary = int(bool(self.volume_boundary))
         return m
+
+
+@dataclass
+class MediumSpec:
+    """HomogeneousMedium (shader.cxx:1234-1316) with its phase function."""
+
+    sigma_s: np.ndarray
+    sigma_a: np.ndarray
+    phase: int = abi.PHASE_UNIFORM
+    phase_g: float = 0.0
+    priority: int = 1
+
+    def to_c(self) -> abi.Medium:
+        m = abi.Medium()
+        m.kind = abi.MEDIUM_HOMOGENEOUS
+        m.priority = int(self.priority)
+        m.sigma_s[:] = [float(x) for x in as_spectrum(self.sigma_s)]
+        m.sigma_a[:] = [float(x) for x in as_spectrum(self.sigma_a)]
+        m.phase = int(self.phase)
+        m.phase_g = float(self.phase_g)
+        return m
+
+
+def volume_boundary(medium_inside: int, medium_outside: int = -1) -> MaterialSpec:
+    """Invisible triangles that only delimit media (a material without shader)."""
+    return MaterialSpec(shader=abi.SHADER_DIFFUSE, reflectance=np.zeros(NBINS), medium_inside=medium_inside,
+                        medium_outside=medium_outside, volume_boundary=True)
 
 
 def diffuse(reflectance) -> MaterialSpec:
@@ -120,6 +153,7 @@ class Scene:
         self.materials: List[MaterialSpec] = []
         self.env_lights: List[EnvLightSpec] = []
         self.point_lights: List[tuple] = []
+        self.media: List[MediumSpec] = []
         self.camera = CameraSpec()
         self.name = "scene"
         self._flat = None
@@ -129,6 +163,10 @@ class Scene:
         self.materials.append(m)
         self._flat = None
         return len(self.materials) - 1
+
+    def add_medium(self, m: MediumSpec) -> int:
+        self.media.append(m)
+        return len(self.media) - 1
 
     def add_mesh(self, vertices, triangles, material: int, normals=None) -> None:
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
@@ -216,6 +254,10 @@ class Scene:
         keep.append(pt_arr)
         d.num_point_lights = len(pts)
         d.point_lights = C.cast(pt_arr, C.POINTER(abi.PointLight))
+        med_arr = (abi.Medium * max(1, len(self.media)))(*[m.to_c() for m in self.media])
+        keep.append(med_arr)
+        d.num_media = len(self.media)
+        d.media = C.cast(med_arr, C.POINTER(abi.Medium))
         cam = self.camera
         d.camera.kind = cam.kind
         d.camera.pos[:] = [float(x) for x in cam.pos]

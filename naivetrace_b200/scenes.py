@@ -16,8 +16,8 @@ import math
 import numpy as np
 
 from . import abi
-from .scene import (CameraSpec, Scene, area_light, diffuse, env_map, glass, microfacet,
-                    mirror, sun_light)
+from .scene import (CameraSpec, MediumSpec, Scene, area_light, diffuse, env_map, glass, microfacet,
+                    mirror, sun_light, volume_boundary)
 from .spectral import band_spectrum, rgb_to_spectrum
 
 
@@ -56,6 +56,14 @@ def box_mesh(size, center_base, rot_y_deg):
         tris.append([f[0], f[1], f[2]])
         tris.append([f[0], f[2], f[3]])
     return v, np.array(tris, dtype=np.uint32)
+
+
+def centered_box(center, half_extent):
+    """Closed axis-aligned box [center - h, center + h] with outward winding (12 triangles)."""
+    h = np.broadcast_to(np.asarray(half_extent, dtype=np.float64), (3,))
+    v, t = box_mesh(2 * h, (0.0, 0.0, 0.0), 0.0)
+    v = v + np.asarray(center, dtype=np.float64) - np.array([0.0, h[1], 0.0])
+    return v, t
 
 
 def cornell_box(xres=256, yres=256) -> Scene:
@@ -113,6 +121,22 @@ def cornell_box_materials(xres=64, yres=64) -> Scene:
     s.add_mesh(*box_mesh((0.3, 0.6, 0.3), (0.3, 0.0, 0.65), -17.0), glass_m)
     s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.5, 0.5, -1.4), dir=(0, 0, 1), up=(0, 1, 0),
                           fov_deg=40.0, xres=xres, yres=yres)
+    return s
+
+
+def cornell_box_medium(xres=256, yres=256) -> Scene:
+    """The Cornell box filled with a homogeneous chromatic medium: sigma_s rising linearly
+    from 0.5 to 2.0 per unit across the 36 bins, sigma_a = 0.1, Henyey-Greenstein g = 0.7.
+    The medium's boundary is a closed box 1e-3 outside the walls, so no wall coincides
+    with it; rays leave the medium through the open side of the box."""
+    s = cornell_box(xres, yres)
+    s.name = "cornell_box_medium"
+    sigma_s = 0.5 + 1.5 * np.arange(36) / 35.0
+    med = s.add_medium(MediumSpec(sigma_s=sigma_s, sigma_a=np.full(36, 0.1), phase=abi.PHASE_HENYEY_GREENSTEIN,
+                                  phase_g=0.7, priority=1))
+    bnd = s.add_material(volume_boundary(med))
+    e = 1e-3
+    s.add_mesh(*centered_box((0.5, 0.5, 0.5), 0.5 + e), bnd)
     return s
 
 

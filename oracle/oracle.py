@@ -58,6 +58,10 @@ def load():
         "or_tables": ([d, d, d], None),
         "or_eval_env": ([vp, d, i32, d, d], C.c_int),
         "or_scene_info": ([vp, d, i32], C.c_int),
+        "or_medium_walk": ([vp, d, d, C.c_double, C.c_int, i32, d, i32], C.c_int),
+        "or_transmittance": ([vp, d, d, C.c_double, i32, d, d], C.c_int),
+        "or_track": ([vp, d, d, i32, C.c_int, C.c_uint64, d], C.c_int),
+        "or_phase_sample": ([C.c_int, C.c_double, d, C.c_int, C.c_uint64, d, d, d], C.c_int),
     }
     for name, (a, r) in sig.items():
         fn = getattr(lib, name)
@@ -157,11 +161,51 @@ class OracleScene:
         self.lib.or_eval_env(self.h, _dp(d), _ip(li), _dp(val), C.byref(pdf))
         return val, pdf.value
 
+    def medium_walk(self, org, dir, tfar=1e30, max_crossings=64):
+        """(initial medium, [(t, medium after crossing)]) along a ray; -1 = vacuum."""
+        o = np.ascontiguousarray(org, dtype=np.float64)
+        dd = np.ascontiguousarray(dir, dtype=np.float64)
+        media = np.zeros(max_crossings, np.int32)
+        ts = np.zeros(max_crossings)
+        init = C.c_int32(0)
+        n = self.lib.or_medium_walk(self.h, _dp(o), _dp(dd), tfar, max_crossings, _ip(media), _dp(ts), C.byref(init))
+        return init.value, list(zip(ts[:n].tolist(), media[:n].tolist()))
+
+    def transmittance(self, org, dir, length, lambda_idx):
+        o = np.ascontiguousarray(org, dtype=np.float64)
+        dd = np.ascontiguousarray(dir, dtype=np.float64)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        T = np.zeros(3)
+        coeff = np.zeros(3)
+        self.lib.or_transmittance(self.h, _dp(o), _dp(dd), length, _ip(li), _dp(T), _dp(coeff))
+        return T, coeff
+
+    def track(self, org, dir, lambda_idx, n, seed=1):
+        """n samples of the next interaction: columns interacted, distance, weight[3],
+        sigma_s[3], volume pdf coefficients (forward, backward, transmittance)."""
+        o = np.ascontiguousarray(org, dtype=np.float64)
+        dd = np.ascontiguousarray(dir, dtype=np.float64)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        out = np.zeros((n, 11))
+        self.lib.or_track(self.h, _dp(o), _dp(dd), _ip(li), n, seed, _dp(out))
+        return out
+
     def info(self):
         bb = np.zeros(6)
         cnt = np.zeros(4, np.int32)
         self.lib.or_scene_info(self.h, _dp(bb), _ip(cnt))
         return bb, cnt
+
+
+def phase_sample(kind: int, g: float, wi, n: int, seed: int = 1):
+    """(dirs, pdf, value) of n phase-function samples about the reverse incident direction wi."""
+    lib = load()
+    w = np.ascontiguousarray(wi, dtype=np.float64)
+    dirs = np.zeros((n, 3))
+    pdf = np.zeros(n)
+    val = np.zeros(n)
+    lib.or_phase_sample(kind, g, _dp(w), n, seed, _dp(dirs), _dp(pdf), _dp(val))
+    return dirs, pdf, val
 
 
 def combine(accum, light, samples_per_pixel, splat_count, npix):

@@ -401,6 +401,14 @@ struct BNode {
   int left = -1, right = -1, start = 0, count = 0;
 };
 
+struct MediumDesc {
+  int priority;
+  double sigma_s[NBINS], sigma_a[NBINS], sigma_ext[NBINS];
+  bool is_scattering;
+  int phase;
+  double g;
+};
+
 struct Scene {
   std::vector<V3> tv0, tv1, tv2;   // triangle vertices as double (from float)
   std::vector<F3> vert, nrm;
@@ -417,8 +425,14 @@ struct Scene {
   double type_probs[4];            // ENV, AREA, POINT, VOLUME (light.hxx:322-326)
   double in_class[4];
   tt_params params;
-  std::vector<BNode> nodes;
-  std::vector<int> tri_order;
+  // Surfaces and medium boundaries are separate triangle sets with their own BVH, as in
+  // Scene::BuildAccelStructure (scene.cxx:116-141).  Entries are global triangle indices.
+  struct TriSet {
+    std::vector<int> tris;
+    std::vector<BNode> nodes;
+    std::vector<int> order;
+  } surf, vol;
+  std::vector<MediumDesc> media;
 };
 
 inline void TriBounds(const Scene& s, int t, double lo[3], double hi[3]) {
@@ -434,14 +448,15 @@ static double HalfArea(const double lo[3], const double hi[3]) {
   return d0 * d1 + d1 * d2 + d2 * d0;
 }
 
-static void BuildBvh(Scene& s) {
-  const int n = (int)s.tv0.size();
-  s.tri_order.resize(n);
-  std::vector<double> cen(3 * (size_t)n), blo(3 * (size_t)n), bhi(3 * (size_t)n);
+static void BuildBvh(const Scene& sc, Scene::TriSet& s) {
+  const int n = (int)s.tris.size();
+  s.order.resize(n);
+  std::vector<double> cen(3 * sc.tv0.size()), blo(3 * sc.tv0.size()), bhi(3 * sc.tv0.size());
   for (int i = 0; i < n; ++i) {
-    s.tri_order[i] = i;
-    TriBounds(s, i, &blo[3 * i], &bhi[3 * i]);
-    for (int k = 0; k < 3; ++k) cen[3 * i + k] = 0.5 * (blo[3 * i + k] + bhi[3 * i + k]);
+    const int g = s.tris[i];
+    s.order[i] = g;
+    TriBounds(sc, g, &blo[3 * (size_t)g], &bhi[3 * (size_t)g]);
+    for (int k = 0; k < 3; ++k) cen[3 * (size_t)g + k] = 0.5 * (blo[3 * (size_t)g + k] + bhi[3 * (size_t)g + k]);
   }
   s.nodes.clear();
   s.nodes.reserve(2 * (size_t)std::max(n, 1));
@@ -457,7 +472,7 @@ static void BuildBvh(Scene& s) {
     double clo[3] = {1e300, 1e300, 1e300}, chi[3] = {-1e300, -1e300, -1e300};
     for (int k = 0; k < 3; ++k) { nd.lo[k] = 1e300; nd.hi[k] = -1e300; }
     for (int i = t.start; i < t.start + t.count; ++i) {
-      int tri = s.tri_order[i];
+      int tri = s.order[i];
       for (int k = 0; k < 3; ++k) {
         nd.lo[k] = std::min(nd.lo[k], blo[3 * tri + k]);
         nd.hi[k] = std::max(nd.hi[k], bhi[3 * tri + k]);
@@ -476,7 +491,7 @@ static void BuildBvh(Scene& s) {
       for (int b = 0; b < NB; ++b)
         for (int k = 0; k < 3; ++k) { bl[b][k] = 1e300; bh[b][k] = -1e300; }
       for (int i = t.start; i < t.start + t.count; ++i) {
-        int tri = s.tri_order[i];
+        int tri = s.order[i];
         int b = std::min(NB - 1, (int)(NB * (cen[3 * tri + axis] - clo[axis]) / ext));
         cnt[b]++;
         for (int k = 0; k < 3; ++k) {
@@ -509,11 +524,11 @@ static void BuildBvh(Scene& s) {
       mid = t.start + t.count / 2;  // all centroids coincide: split by count
     } else {
       double ext = chi[best_axis] - clo[best_axis];
-      auto it = std::partition(s.tri_order.begin() + t.start, s.tri_order.begin() + t.start + t.count, [&](int tri) {
+      auto it = std::partition(s.order.begin() + t.start, s.order.begin() + t.start + t.count, [&](int tri) {
         int b = std::min(NB - 1, (int)(NB * (cen[3 * tri + best_axis] - clo[best_axis]) / ext));
         return b <= best_split;
       });
-      mid = (int)(it - s.tri_order.begin());
+      mid = (int)(it - s.order.begin());
       if (mid == t.start || mid == t.start + t.count) mid = t.start + t.count / 2;
     }
     int l = (int)s.nodes.size();
@@ -578,9 +593,9 @@ inline bool SlabHit(const BNode& nd, V3 org, V3 inv, double tnear, double tfar, 
 }
 
 // Closest hit in (tnear, tfar].  any_hit: stop at the first hit (occlusion).
-static int Trace(const Scene& s, V3 org, V3 dir, double tnear, double tfar, bool any_hit, double* t_out,
-                 double* u_out, double* v_out) {
-  if (s.nodes.empty() || s.tv0.empty()) return -1;
+static int Trace(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, double tnear, double tfar, bool any_hit,
+                 double* t_out, double* u_out, double* v_out) {
+  if (s.nodes.empty() || s.tris.empty()) return -1;
   V3 inv{1.0 / dir.x, 1.0 / dir.y, 1.0 / dir.z};
   int stack[128];
   int sp = 0;
@@ -593,9 +608,9 @@ static int Trace(const Scene& s, V3 org, V3 dir, double tnear, double tfar, bool
     if (!SlabHit(nd, org, inv, tnear, best_t, &te)) continue;
     if (nd.count > 0) {
       for (int i = nd.start; i < nd.start + nd.count; ++i) {
-        int tri = s.tri_order[i];
+        int tri = s.order[i];
         double t, u, v;
-        if (IntersectTri(org, dir, s.tv0[tri], s.tv1[tri], s.tv2[tri], tnear, best_t, &t, &u, &v)) {
+        if (IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, best_t, &t, &u, &v)) {
           best = tri; best_t = t; bu = u; bv = v;
           if (any_hit) { *t_out = t; return tri; }
         }
@@ -610,18 +625,65 @@ static int Trace(const Scene& s, V3 org, V3 dir, double tnear, double tfar, bool
   return best;
 }
 
-static int TraceBrute(const Scene& s, V3 org, V3 dir, double tnear, double tfar, double* t_out, double* u_out,
-                      double* v_out) {
+static int TraceBrute(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, double tnear, double tfar,
+                      double* t_out, double* u_out, double* v_out) {
   int best = -1;
   double best_t = tfar, bu = 0, bv = 0;
-  for (size_t tri = 0; tri < s.tv0.size(); ++tri) {
+  for (int tri : s.tris) {
     double t, u, v;
-    if (IntersectTri(org, dir, s.tv0[tri], s.tv1[tri], s.tv2[tri], tnear, best_t, &t, &u, &v)) {
-      best = (int)tri; best_t = t; bu = u; bv = v;
+    if (IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, best_t, &t, &u, &v)) {
+      best = tri; best_t = t; bu = u; bv = v;
     }
   }
   if (best >= 0) { *t_out = best_t; *u_out = bu; *v_out = bv; }
   return best;
+}
+
+// A medium-boundary (or surface) crossing: BoundaryIntersection (embreeaccelerator.hxx:27-35).
+struct Crossing {
+  int prim;
+  uint32_t material;
+  double t;
+  F3 n;  // unnormalised winding normal, float like Embree's Ng
+};
+
+// All intersections with t in (tnear, tfar], sorted by t, duplicates (same material, same
+// t) removed: EmbreeAccelerator::IntersectionsInOrder with its filter callback
+// (embreeaccelerator.cxx:134-213).
+static void AllHits(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, double tnear, double tfar,
+                    std::vector<Crossing>& out) {
+  out.clear();
+  if (s.nodes.empty() || s.tris.empty()) return;
+  V3 inv{1.0 / dir.x, 1.0 / dir.y, 1.0 / dir.z};
+  int stack[128];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const BNode& nd = s.nodes[stack[--sp]];
+    double te;
+    if (!SlabHit(nd, org, inv, tnear, tfar, &te)) continue;
+    if (nd.count > 0) {
+      for (int i = nd.start; i < nd.start + nd.count; ++i) {
+        const int tri = s.order[i];
+        double t, u, v;
+        if (!IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, tfar, &t, &u, &v)) continue;
+        Crossing c;
+        c.prim = tri;
+        c.material = sc.mat_of_tri[tri];
+        c.t = t;
+        const V3 ng = Cross(sc.tv1[tri] - sc.tv0[tri], sc.tv2[tri] - sc.tv0[tri]);
+        c.n = Ff(ng);
+        bool dup = false;
+        for (const auto& o : out) dup |= (o.material == c.material) & (o.t == c.t);
+        if (!dup) out.push_back(c);
+      }
+    } else {
+      if (sp + 2 > 128) return;
+      stack[sp++] = nd.right;
+      stack[sp++] = nd.left;
+    }
+  }
+  std::sort(out.begin(), out.end(), [](const Crossing& a, const Crossing& b) { return a.t < b.t; });
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1003,14 +1065,186 @@ struct Node {
   NodeType type = ZERO;
   V3 incident_dir;
   Surf surf;
-  V3 coords;       // ENV: direction; POINT/CAMERA: position; surfaces use surf.pos
+  V3 coords;       // ENV: direction; POINT/CAMERA/VOLUME: position; surfaces use surf.pos
   S3 radiance;     // ENV radiance
   int unit = -1;   // CAMERA unit index
   int point = -1;  // point light index
+  int medium = -1; // VOLUME_SCATTER: medium index
+  S3 sigma_s;      // VOLUME_SCATTER: scattering coefficient at the interaction
   bool IsSurface() const { return type == SURFACE_EMITTER || type == SURFACE_SCATTER; }
+  bool IsVolume() const { return type == VOLUME_SCATTER || type == VOLUME_EMITTER; }
   bool IsScatter() const { return type == SURFACE_SCATTER || type == VOLUME_SCATTER; }
   V3 Coordinates() const { return IsSurface() ? surf.pos : coords; }
 };
+
+// ---------------------------------------------------------------------------------------
+// Phase functions (phasefunctions.cxx:23-138).  Directions sampled about the incident
+// travel direction with mu_to_direction's (sin, cos, mu) layout.
+inline V3 MuToDirection(double mu, double r2) {
+  const double sn = std::sin(Pi * 2. * r2), cs = std::cos(Pi * 2. * r2);
+  const double rho = std::sqrt(1. - mu * mu);
+  return {sn * rho, cs * rho, mu};
+}
+inline double RayleighValue(double mu) { return (3. / (16. * Pi)) * (1. + mu * mu); }
+inline double RayleighSampleMu(double r) {
+  double a = std::pow(-2. + 4. * r + std::sqrt(5. - 16. * r + 16. * r * r), 1. / 3.);
+  return a - 1. / a;
+}
+inline double HgValue(double mu, double g) {
+  const double g2 = g * g;
+  const double term = 1.0 + g2 - 2.0 * g * mu;
+  return 1.0 / (4. * Pi) * (1.0 - g2) / (std::sqrt(term) * term);
+}
+inline double HgSampleMu(double r, double g) {
+  const double s = 2.0 * r - 1.0, g2 = g * g;
+  if (std::abs(g) > 1.0e-3) {
+    const double t1 = (1.0 - g2) / (1.0 + g * s);
+    return (1.0 + g2 - t1 * t1) / (2.0 * g);
+  }
+  const double s2 = s * s;
+  return s + 1.5 * g * (1.0 - s2) - 2.0 * g2 * s * (1.0 - s2);
+}
+
+static double PhaseEvaluate(const MediumDesc& m, V3 reverse_incident, V3 out) {
+  switch (m.phase) {
+    case TT_PHASE_RAYLEIGH: return RayleighValue(Dot(-reverse_incident, out));
+    case TT_PHASE_HENYEY_GREENSTEIN: return HgValue(Dot(-reverse_incident, out), m.g);
+    default: return 1. / (4. * Pi);
+  }
+}
+
+static ScatterSample PhaseSample(const MediumDesc& m, V3 reverse_incident, Sampler& smp) {
+  ScatterSample out;
+  double r[2];
+  smp.UniformUnitSquare(r);
+  if (m.phase == TT_PHASE_UNIFORM) {
+    out.dir = ToUniformSphere(r);
+    out.pdf = 1. / (4. * Pi);
+  } else {
+    const Frame f = OrthogonalSystemZAligned(-reverse_incident);
+    const double mu = m.phase == TT_PHASE_RAYLEIGH ? RayleighSampleMu(r[0]) : HgSampleMu(r[0], m.g);
+    out.dir = f.ToWorld(MuToDirection(mu, r[1]));
+    out.pdf = m.phase == TT_PHASE_RAYLEIGH ? RayleighValue(mu) : HgValue(mu, m.g);
+  }
+  out.value = S3(out.pdf);
+  return out;
+}
+
+// ---------------------------------------------------------------------------------------
+// MediumTracker (rendering_util.hxx:18-126, rendering_util.cxx:13-38).  Medium -1 is the
+// empty-space vacuum with priority -1; slots hold up to 4 overlapping media.
+struct MediumTracker {
+  int current = -1;
+  int media[4] = {-2, -2, -2, -2};  // -2 = empty slot
+};
+
+inline int MediumPriority(const Scene& sc, int m) { return m < 0 ? -1 : sc.media[m].priority; }
+
+static void GoingThroughSurface(const Scene& sc, MediumTracker& mt, V3 dir, F3 n, uint32_t material) {
+  const tt_material& mat = sc.materials[material].m;
+  int to_enter = mat.medium_inside - 1, to_exit = mat.medium_outside - 1;
+  if (to_enter < 0 && to_exit < 0) return;
+  const float d = (float)dir.x * n.x + (float)dir.y * n.y + (float)dir.z * n.z;
+  if (d > 0.f) std::swap(to_enter, to_exit);
+  if (to_exit >= 0) {
+    bool found = false;
+    for (int i = 0; i < 4 && !found; ++i) {
+      found = mt.media[i] == to_exit;
+      if (found) mt.media[i] = -2;
+    }
+    if (to_exit == mt.current) {
+      int best = -1;
+      for (int i = 0; i < 4; ++i)
+        if (mt.media[i] != -2 && MediumPriority(sc, best) < MediumPriority(sc, mt.media[i])) best = mt.media[i];
+      mt.current = best;
+    }
+  }
+  if (to_enter >= 0) {
+    bool inserted = false;
+    for (int i = 0; i < 4 && !inserted; ++i) {
+      inserted = mt.media[i] == -2;
+      if (inserted) mt.media[i] = to_enter;
+    }
+    if (inserted && MediumPriority(sc, to_enter) > MediumPriority(sc, mt.current)) mt.current = to_enter;
+  }
+}
+
+// MediumTracker::initializePosition: count the boundaries between a point outside the
+// bounding box (+x side) and pos.
+static void InitializeMediumTracker(const Scene& sc, MediumTracker& mt, V3 pos) {
+  mt = MediumTracker{};
+  const bool inside = pos.x >= sc.bb_lo[0] && pos.x <= sc.bb_hi[0] && pos.y >= sc.bb_lo[1] && pos.y <= sc.bb_hi[1] &&
+                      pos.z >= sc.bb_lo[2] && pos.z <= sc.bb_hi[2];
+  if (!inside) return;
+  const double go = 2. * std::max(sc.bb_hi[0] - sc.bb_lo[0], std::max(sc.bb_hi[1] - sc.bb_lo[1], sc.bb_hi[2] - sc.bb_lo[2]));
+  V3 org = pos;
+  org.x += go;
+  const V3 dir{-1., 0., 0.};
+  std::vector<Crossing> hits;
+  AllHits(sc, sc.vol, org, dir, 0., go, hits);
+  for (const auto& h : hits) GoingThroughSurface(sc, mt, dir, h.n, h.material);
+  AllHits(sc, sc.surf, org, dir, 0., go, hits);
+  for (const auto& h : hits) GoingThroughSurface(sc, mt, dir, h.n, h.material);
+}
+
+// VolumePdfCoefficients and Accumulate (shader.hxx:133-157).
+struct VolCoeffs {
+  double fwd = 1., bwd = 1., tr = 1.;
+};
+inline void Accumulate(VolCoeffs& acc, const VolCoeffs& seg, bool is_first, bool is_last) {
+  acc.fwd *= is_last ? seg.fwd : seg.tr;
+  acc.bwd *= is_first ? seg.bwd : seg.tr;
+  acc.tr *= seg.tr;
+}
+
+inline S3 TakeD3(const double* a, const int32_t idx[3]) { return {a[idx[0]], a[idx[1]], a[idx[2]]}; }
+inline S3 ExpNeg(S3 s, double x) { return {std::exp(-s[0] * x), std::exp(-s[1] * x), std::exp(-s[2] * x)}; }
+inline double Mean(S3 s) { return (s[0] + s[1] + s[2]) / 3.; }
+
+// VacuumMedium / HomogeneousMedium::ComputeVolumePdfCoefficients (shader.cxx:1204-1211, 1297-1309).
+static VolCoeffs VolumeCoeffs(const Scene& sc, int medium, double length, const int32_t idx[3]) {
+  if (medium < 0) return {0., 0., 1.};
+  const S3 se = TakeD3(sc.media[medium].sigma_ext, idx);
+  const double tr = Mean(ExpNeg(se, length)), e = Mean(se);
+  return {e * tr, e * tr, tr};
+}
+
+struct InteractionSample {
+  double t;
+  S3 weight;
+  S3 sigma_s;
+};
+
+// HomogeneousMedium::SampleInteractionPoint (shader.cxx:1259-1270) with
+// HomogeneousSpectralTracking (media_integrator.cxx:43-87), Kutz et al. 2017.
+static InteractionSample SampleInteraction(const Scene& sc, int medium, double length, S3 initial_weights,
+                                           Sampler& smp, const int32_t idx[3]) {
+  if (medium < 0) return {LargeNumber, S3(1.), S3(0.)};
+  const MediumDesc& m = sc.media[medium];
+  const S3 sigma_ext = TakeD3(m.sigma_ext, idx), sigma_s = TakeD3(m.sigma_s, idx);
+  if (!m.is_scattering) return {LargeNumber, ExpNeg(sigma_ext, length), S3(0.)};
+  InteractionSample smpl{0., S3(1.), S3(0.)};
+  const double majorant = sigma_ext.Max();
+  const S3 sigma_n{majorant - sigma_ext[0], majorant - sigma_ext[1], majorant - sigma_ext[2]};
+  const double inv_majorant = 1. / majorant;
+  int iteration = 0;
+  while (++iteration < 100) {
+    smpl.t -= std::log(smp.Uniform01()) * inv_majorant;
+    if (smpl.t > length) return smpl;
+    // ComputeProbabilitiesHistoryScheme (media_integrator.cxx:11-40).
+    const S3 w = smpl.weight * initial_weights;
+    double pt = Mean(sigma_s * w), pn = Mean(sigma_n * w);
+    const double norm = pt + pn;
+    if (norm > 0.) { pt /= norm; pn /= norm; } else { pt = pn = 0.5; }
+    if (smp.Uniform01() < pt) {
+      smpl.weight = smpl.weight * (inv_majorant / pt);
+      smpl.sigma_s = sigma_s;
+      return smpl;
+    }
+    smpl.weight = smpl.weight * sigma_n * (inv_majorant / pn);
+  }
+  return smpl;
+}
 
 struct PathCtx {
   int32_t idx[3];
@@ -1171,6 +1405,11 @@ struct Worker {
 
   S3 EvaluateScatterer(const Node& n, V3 out_dir, double* pdf) {
     const V3 wi = -n.incident_dir;
+    if (n.IsVolume()) {  // EvaluateScatterCoordinateOfScatterer, volume branch
+      const double v = PhaseEvaluate(sc.media[n.medium], wi, out_dir);
+      if (pdf) *pdf = v;
+      return n.sigma_s * v;
+    }
     const tt_material& m = sc.materials[sc.mat_of_tri[n.surf.prim]].m;
     S3 fs = EvaluateBSDF(m, wi, n.surf, out_dir, ctx.idx, pdf);
     return fs * BsdfCorrectionFactor(n.surf, out_dir);
@@ -1205,13 +1444,39 @@ struct Worker {
     *len = l;
   }
 
-  bool Occluded(V3 org, V3 dir, double len) {
+  // MaybeHandlePassageThroughSurface (rendering_randomwalk_impl.hxx:516-527).
+  void MaybeHandlePassage(const Node& n, V3 dir, MediumTracker& mt) const {
+    if (n.IsSurface() && Dot(dir, n.surf.normal) < 0.)
+      GoingThroughSurface(sc, mt, dir, Ff(n.surf.geometry_normal), sc.mat_of_tri[n.surf.prim]);
+  }
+
+  // TransmittanceEstimate (rendering_util.cxx:40-67): occlusion by surfaces, then the
+  // product of the media's transmittances over the boundary-delimited segments.
+  S3 TransmittanceEstimate(V3 org, V3 dir, double length, MediumTracker& mt, VolCoeffs* coeff) {
+    length *= 0.9999;
     double t, u, v;
-    return Trace(sc, org, dir, 0., len, true, &t, &u, &v) >= 0;
+    if (Trace(sc, sc.surf, org, dir, 0., length, true, &t, &u, &v) >= 0) return S3(0.);
+    std::vector<Crossing> hits;
+    AllHits(sc, sc.vol, org, dir, 0., length, hits);
+    S3 result(1.);
+    double snear = 0.;
+    size_t k = 0;
+    while (snear != length) {
+      const double sfar = k < hits.size() ? hits[k].t : length;
+      const int medium = mt.current;
+      if (coeff) Accumulate(*coeff, VolumeCoeffs(sc, medium, sfar - snear, ctx.idx), snear == 0., sfar == length);
+      if (medium >= 0) result = result * ExpNeg(TakeD3(sc.media[medium].sigma_ext, ctx.idx), sfar - snear);
+      if (k >= hits.size()) break;
+      GoingThroughSurface(sc, mt, dir, hits[k].n, hits[k].material);
+      snear = hits[k].t;
+      ++k;
+    }
+    return result;
   }
 
   // CalculateConnection, rendering_randomwalk_impl.hxx:373-409.
-  S3 CalculateConnection(const Node& eye, const Node& light, double* pdf_source, V3* seg_dir, double* seg_len) {
+  S3 CalculateConnection(const Node& eye, const MediumTracker& eye_mt, const Node& light, double* pdf_source,
+                         V3* seg_dir, double* seg_len, VolCoeffs* coeff) {
     V3 org, dir;
     double len;
     SegmentToTarget(eye, light, &org, &dir, &len);
@@ -1222,17 +1487,20 @@ struct Worker {
     if (sf.IsZero() || tf.IsZero()) return S3(0.);
     sf = sf * DFactorOf(eye, dir);
     tf = tf * DFactorOf(light, -dir);
-    // TransmittanceEstimate, rendering_util.cxx:40-67 (vacuum: occlusion only).
-    double T = Occluded(org, dir, len * 0.9999) ? 0. : 1.;
+    MediumTracker mt = eye_mt;
+    MaybeHandlePassage(eye, dir, mt);
+    const S3 T = TransmittanceEstimate(org, dir, len, mt, coeff);
     bool wrt_solid_angle = eye.type == ENV || light.type == ENV;
     double r2 = wrt_solid_angle ? 1. : 1. / Sqr(len);
-    return sf * tf * (r2 * T);
+    return T * sf * tf * r2;
   }
 
-  // PdfConversionFactor, rendering_randomwalk_impl.hxx:493-513 (vacuum coefficients = 1).
-  double PdfConversionFactor(const Node& src, const Node& tgt, V3 dir, double len, bool parallel) const {
+  // PdfConversionFactor, rendering_randomwalk_impl.hxx:493-513.
+  double PdfConversionFactor(const Node& src, const Node& tgt, V3 dir, double len, const VolCoeffs& coeff,
+                             bool parallel) const {
     double factor = DFactorOf(tgt, dir);
     if (src.type != ENV && tgt.type != ENV && !parallel) factor /= (Sqr(len) + Eps);
+    factor *= tgt.IsVolume() ? coeff.fwd : coeff.tr;
     return factor;
   }
 
@@ -1248,17 +1516,22 @@ struct Worker {
     double scatter_pdf = 0;
     bool scatter_delta = false;
     S3 beta_factor;
+    VolCoeffs coeff;
   };
 
-  // TakeRandomWalkStep, rendering_randomwalk_impl.hxx:285-363.
-  Step TakeRandomWalkStep(const Node& src) {
+  // TakeRandomWalkStep, rendering_randomwalk_impl.hxx:285-363, with TrackToNextInteraction
+  // (rendering_util.hxx:215-269).
+  Step TakeRandomWalkStep(const Node& src, MediumTracker& mt) {
     Step st;
     V3 org = src.Coordinates();
     V3 dir;
     S3 value;
     double pdf;
     bool delta;
-    if (src.IsScatter()) {
+    if (src.IsVolume()) {  // SamplePhaseFunction x sigma_s
+      ScatterSample s = PhaseSample(sc.media[src.medium], -src.incident_dir, smp);
+      dir = s.dir; value = s.value * src.sigma_s; pdf = s.pdf; delta = false;
+    } else if (src.IsScatter()) {
       const tt_material& m = sc.materials[sc.mat_of_tri[src.surf.prim]].m;
       ScatterSample s = SampleBSDF(m, -src.incident_dir, src.surf, smp, ctx.idx);
       s.value = s.value * BsdfCorrectionFactor(src.surf, s.dir);
@@ -1271,8 +1544,58 @@ struct Worker {
     AddAntiSelfIntersectionOffsetAt(org, src, dir);
     st.beta_factor = value / std::abs(pdf);
     if (st.beta_factor.IsZero()) { st.node.type = ZERO; return st; }
+    MaybeHandlePassage(src, dir, mt);
+    Step tr = TrackFrom(org, dir, mt);
+    tr.beta_factor = st.beta_factor * tr.beta_factor;
+    tr.scatter_pdf = std::abs(pdf);
+    tr.scatter_delta = delta;
+    return tr;
+  }
+
+  // TrackToNextInteraction (rendering_util.hxx:215-269): closest surface hit, then spectral
+  // tracking through the media between the boundary crossings in front of it.  Returns the
+  // node (volume, surface or environment), segment length, tracking weight and the
+  // accumulated volume pdf coefficients.
+  Step TrackFrom(V3 org, V3 dir, MediumTracker& mt) {
+    Step st;
+    st.beta_factor = S3(1.);
     double t = 0, u = 0, v = 0;
-    int prim = Trace(sc, org, dir, 0., LargeNumber, false, &t, &u, &v);
+    double tfar = LargeNumber;
+    int prim = Trace(sc, sc.surf, org, dir, 0., LargeNumber, false, &t, &u, &v);
+    if (prim >= 0) tfar = t;
+    // Volume segments up to 0.9999 of the surface distance.
+    const double vend = tfar * 0.9999;
+    std::vector<Crossing> hits;
+    AllHits(sc, sc.vol, org, dir, 0., vend, hits);
+    S3 weight(1.);
+    double snear = 0.;
+    size_t k = 0;
+    while (snear != vend) {
+      const double sfar = k < hits.size() ? hits[k].t : vend;
+      const int medium = mt.current;
+      const InteractionSample ms = SampleInteraction(sc, medium, sfar - snear, weight, smp, ctx.idx);
+      weight = weight * ms.weight;
+      const bool interacted = ms.t < sfar - snear;
+      const double seglen = interacted ? ms.t : sfar - snear;
+      Accumulate(st.coeff, VolumeCoeffs(sc, medium, seglen, ctx.idx), snear == 0., interacted);
+      if (interacted) {
+        const double dist = snear + ms.t;
+        st.node.type = VOLUME_SCATTER;
+        st.node.coords = org + dir * dist;
+        st.node.medium = medium;
+        st.node.sigma_s = ms.sigma_s;
+        st.seg_len = dist;
+        st.beta_factor = weight;
+        st.node.incident_dir = dir;
+        st.ray_dir = dir;
+        return st;
+      }
+      if (k >= hits.size()) break;
+      GoingThroughSurface(sc, mt, dir, hits[k].n, hits[k].material);
+      snear = hits[k].t;
+      ++k;
+    }
+    st.beta_factor = weight;
     if (prim >= 0) {
       st.node.type = SURFACE_SCATTER;
       st.node.surf = SurfaceFromHit(sc, prim, u, v, dir);
@@ -1285,8 +1608,6 @@ struct Worker {
     }
     st.node.incident_dir = dir;
     st.ray_dir = dir;
-    st.scatter_pdf = std::abs(pdf);
-    st.scatter_delta = delta;
     return st;
   }
 
@@ -1316,6 +1637,8 @@ struct Worker {
     S3 beta(12.);  // lambda weights (strata size) / delta pdf 1
     int count = 1;
     const int npix = sc.cam.xres * sc.cam.yres;
+    MediumTracker mt;
+    InitializeMediumTracker(sc, mt, step.node.coords);
     while (true) {
       if (do_sample_lights) {
         double pdf_light;
@@ -1324,8 +1647,9 @@ struct Worker {
         double pdf_scatter = 0;
         V3 sdir;
         double slen;
-        S3 w = CalculateConnection(step.node, light, &pdf_scatter, &sdir, &slen);
-        double pdf_due = pdf_scatter * PdfConversionFactor(step.node, light, sdir, slen, false);
+        VolCoeffs coeff;
+        S3 w = CalculateConnection(step.node, mt, light, &pdf_scatter, &sdir, &slen, &coeff);
+        double pdf_due = pdf_scatter * PdfConversionFactor(step.node, light, sdir, slen, coeff, false);
         double mis = MisWeight(pdf_light, light_delta, pdf_due);
         S3 pw = w * (mis / pdf_light) * beta;
         if (step.node.type == CAMERA) {
@@ -1341,7 +1665,7 @@ struct Worker {
         }
       }
       Node prev = step.node;
-      step = TakeRandomWalkStep(prev);
+      step = TakeRandomWalkStep(prev, mt);
       beta = beta * step.beta_factor;
       ++count;
       if (do_sample_brdf) {
@@ -1355,8 +1679,9 @@ struct Worker {
         if (emitter) {
           S3 end_weight = Evaluate(step.node, -step.ray_dir, nullptr);
           double pdf_direct = PdfOfGeneratingSampleOnEmitter(step.node);
-          double pdf_due = PdfConversionFactor(prev, step.node, step.ray_dir, step.seg_len, step.scatter_delta) *
-                           step.scatter_pdf;
+          double pdf_due =
+              PdfConversionFactor(prev, step.node, step.ray_dir, step.seg_len, step.coeff, step.scatter_delta) *
+              step.scatter_pdf;
           double mis = MisWeight(pdf_due, step.scatter_delta, pdf_direct);
           path_sample_values = path_sample_values + end_weight * beta * mis;
           if (step.node.type == SURFACE_EMITTER) step.node.type = SURFACE_SCATTER;
@@ -1394,7 +1719,30 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
   }
   s.idx.assign(d->indices, d->indices + 3 * (size_t)d->num_triangles);
   s.mat_of_tri.assign(d->material_ids, d->material_ids + d->num_triangles);
-  for (uint32_t i = 0; i < d->num_materials; ++i) s.materials.push_back(Material{d->materials[i]});
+  for (uint32_t i = 0; i < d->num_media; ++i) {
+    const tt_medium& m = d->media[i];
+    MediumDesc md;
+    md.priority = m.priority;
+    md.is_scattering = false;
+    for (int b = 0; b < NBINS; ++b) {
+      md.sigma_s[b] = m.sigma_s[b];
+      md.sigma_a[b] = m.sigma_a[b];
+      md.sigma_ext[b] = md.sigma_s[b] + md.sigma_a[b];
+      md.is_scattering |= md.sigma_s[b] > 0.;
+    }
+    md.phase = m.phase;
+    md.g = m.phase_g;
+    s.media.push_back(md);
+  }
+  for (uint32_t i = 0; i < d->num_materials; ++i) {
+    const tt_material& m = d->materials[i];
+    if (m.medium_inside < 0 || m.medium_inside > (int)d->num_media || m.medium_outside < 0 ||
+        m.medium_outside > (int)d->num_media) {
+      g_err = "medium index out of range";
+      return false;
+    }
+    s.materials.push_back(Material{m});
+  }
   for (uint32_t t = 0; t < d->num_triangles; ++t) {
     for (int k = 0; k < 3; ++k)
       if (s.idx[3 * t + k] >= d->num_vertices) { g_err = "vertex index out of range"; return false; }
@@ -1402,7 +1750,13 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
     s.tv0.push_back(VertD(s, s.idx[3 * t]));
     s.tv1.push_back(VertD(s, s.idx[3 * t + 1]));
     s.tv2.push_back(VertD(s, s.idx[3 * t + 2]));
-    if (s.materials[s.mat_of_tri[t]].m.emissive) s.area_lights.push_back((int)t);
+    const tt_material& m = s.materials[s.mat_of_tri[t]].m;
+    if (m.volume_boundary) {
+      s.vol.tris.push_back((int)t);
+    } else {
+      s.surf.tris.push_back((int)t);
+      if (m.emissive) s.area_lights.push_back((int)t);
+    }
   }
   for (int k = 0; k < 3; ++k) { s.bb_lo[k] = 1e300; s.bb_hi[k] = -1e300; }
   for (auto& v : s.vert) {
@@ -1507,7 +1861,8 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
   cam.xperpixel = 2. * a / c.xres;
   cam.yperpixel = 2. * b / c.yres;
   cam.per_pixel_delta = 2. / std::min(c.xres, c.yres);
-  BuildBvh(s);
+  BuildBvh(s, s.surf);
+  BuildBvh(s, s.vol);
   return true;
 }
 
@@ -1540,8 +1895,8 @@ int or_intersect(or_scene* s, const double* rays, int n, int brute_force, int32_
     const double* r = rays + 8 * (size_t)i;
     V3 org{r[0], r[1], r[2]}, dir{r[4], r[5], r[6]};
     double tt = 0, uu = 0, vv = 0;
-    int p = brute_force ? TraceBrute(s->s, org, dir, r[3], r[7], &tt, &uu, &vv)
-                        : Trace(s->s, org, dir, r[3], r[7], false, &tt, &uu, &vv);
+    int p = brute_force ? TraceBrute(s->s, s->s.surf, org, dir, r[3], r[7], &tt, &uu, &vv)
+                        : Trace(s->s, s->s.surf, org, dir, r[3], r[7], false, &tt, &uu, &vv);
     prim[i] = p;
     t[i] = p >= 0 ? tt : -1;
     u[i] = uu;
@@ -1554,7 +1909,7 @@ int or_occluded(or_scene* s, const double* rays, int n, uint8_t* occluded) {
   for (int i = 0; i < n; ++i) {
     const double* r = rays + 8 * (size_t)i;
     double tt, uu, vv;
-    occluded[i] = Trace(s->s, {r[0], r[1], r[2]}, {r[4], r[5], r[6]}, r[3], r[7], true, &tt, &uu, &vv) >= 0;
+    occluded[i] = Trace(s->s, s->s.surf, {r[0], r[1], r[2]}, {r[4], r[5], r[6]}, r[3], r[7], true, &tt, &uu, &vv) >= 0;
   }
   return 0;
 }
@@ -1710,12 +2065,97 @@ int or_eval_env(or_scene* s, const double* dir_out, const int32_t* lambda_idx, d
   *pdf = EnvEvaluatePdfTotal(s->s, d);
   return 0;
 }
+// Medium-tracker walk along a ray: initializes the tracker at the origin and records the
+// current medium (-1 = vacuum) after each volume-boundary crossing (MediaTransmission
+// tests, tests3.cxx:70-152).  Returns the number of crossings written.
+int or_medium_walk(or_scene* os, const double* org3, const double* dir3, double tfar, int max, int32_t* media,
+                   double* ts, int32_t* initial) {
+  const Scene& sc = os->s;
+  MediumTracker mt;
+  V3 o{org3[0], org3[1], org3[2]}, d{dir3[0], dir3[1], dir3[2]};
+  InitializeMediumTracker(sc, mt, o);
+  *initial = mt.current;
+  std::vector<Crossing> hits;
+  AllHits(sc, sc.vol, o, d, 0., tfar, hits);
+  int n = 0;
+  for (const auto& h : hits) {
+    if (n >= max) break;
+    GoingThroughSurface(sc, mt, d, h.n, h.material);
+    media[n] = mt.current;
+    ts[n] = h.t;
+    ++n;
+  }
+  return n;
+}
+
+// TransmittanceEstimate along a segment starting at org with a tracker initialized there.
+int or_transmittance(or_scene* os, const double* org3, const double* dir3, double length, const int32_t* idx,
+                     double* T3, double* coeff3) {
+  Worker w(os->s);
+  std::memcpy(w.ctx.idx, idx, 3 * sizeof(int32_t));
+  MediumTracker mt;
+  V3 o{org3[0], org3[1], org3[2]}, d{dir3[0], dir3[1], dir3[2]};
+  InitializeMediumTracker(os->s, mt, o);
+  VolCoeffs c;
+  S3 T = w.TransmittanceEstimate(o, d, length, mt, &c);
+  for (int k = 0; k < 3; ++k) T3[k] = T[k];
+  coeff3[0] = c.fwd; coeff3[1] = c.bwd; coeff3[2] = c.tr;
+  return 0;
+}
+
+// n independent TrackToNextInteraction samples from org along dir (stream i = sample i):
+// out[11 i ..] = interacted, distance, weight[3], sigma_s[3], coeff fwd, bwd, transmittance.
+int or_track(or_scene* os, const double* org3, const double* dir3, const int32_t* idx, int n, uint64_t seed,
+             double* out) {
+  for (int i = 0; i < n; ++i) {
+    Worker w(os->s);
+    std::memcpy(w.ctx.idx, idx, 3 * sizeof(int32_t));
+    SeedPath(w.smp.g, seed, (uint64_t)i);
+    Node src;
+    src.type = CAMERA;  // a point source that is not a surface: no offset, no passage
+    src.coords = {org3[0], org3[1], org3[2]};
+    MediumTracker mt;
+    InitializeMediumTracker(os->s, mt, src.coords);
+    // Track along the given direction: emulate TakeRandomWalkStep after the direction is
+    // chosen by calling the tracking part through a one-off source with a fixed ray.
+    V3 d{dir3[0], dir3[1], dir3[2]};
+    auto st = w.TrackFrom(src.coords, d, mt);
+    double* o = out + 11 * (size_t)i;
+    o[0] = st.node.type == VOLUME_SCATTER ? 1. : 0.;
+    o[1] = st.seg_len;
+    for (int k = 0; k < 3; ++k) { o[2 + k] = st.beta_factor[k]; o[5 + k] = st.node.sigma_s[k]; }
+    o[8] = st.coeff.fwd;
+    o[9] = st.coeff.bwd;
+    o[10] = st.coeff.tr;
+  }
+  return 0;
+}
+
+// n phase-function samples about the reverse incident direction wi (the direction back
+// towards the previous vertex) plus the pdf and value of each sampled direction.
+int or_phase_sample(int kind, double g, const double* wi3, int n, uint64_t seed, double* dirs, double* pdf,
+                    double* value) {
+  MediumDesc m{};
+  m.phase = kind;
+  m.g = g;
+  const V3 wi{wi3[0], wi3[1], wi3[2]};
+  for (int i = 0; i < n; ++i) {
+    Sampler smp;
+    SeedPath(smp.g, seed, (uint64_t)i);
+    const ScatterSample s = PhaseSample(m, wi, smp);
+    dirs[3 * i] = s.dir.x; dirs[3 * i + 1] = s.dir.y; dirs[3 * i + 2] = s.dir.z;
+    pdf[i] = s.pdf;
+    value[i] = PhaseEvaluate(m, wi, s.dir);
+  }
+  return 0;
+}
+
 int or_scene_info(or_scene* s, double* bbox6, int32_t* counts4) {
   for (int k = 0; k < 3; ++k) { bbox6[k] = s->s.bb_lo[k]; bbox6[3 + k] = s->s.bb_hi[k]; }
   counts4[0] = (int32_t)s->s.tv0.size();
   counts4[1] = (int32_t)s->s.area_lights.size();
   counts4[2] = (int32_t)s->s.env.size();
-  counts4[3] = (int32_t)s->s.nodes.size();
+  counts4[3] = (int32_t)s->s.surf.nodes.size();
   return 0;
 }
 

@@ -65,6 +65,14 @@ void or_tables(double* smits7x36, double* m3x36, double* sun36);
  * dir_out (the direction the light travels) and the NEE pdf (TotalEnv EvaluatePdf). */
 int or_eval_env(or_scene* s, const double* dir_out, const int32_t* lambda_idx, double* value3, double* pdf);
 int or_scene_info(or_scene* s, double* bbox6, int32_t* counts4);
+int or_medium_walk(or_scene* s, const double* org3, const double* dir3, double tfar, int max, int32_t* media,
+                   double* ts, int32_t* initial);
+int or_transmittance(or_scene* s, const double* org3, const double* dir3, double length, const int32_t* idx,
+                     double* T3, double* coeff3);
+int or_track(or_scene* s, const double* org3, const double* dir3, const int32_t* idx, int n, uint64_t seed,
+             double* out);
+int or_phase_sample(int kind, double g, const double* wi3, int n, uint64_t seed, double* dirs, double* pdf,
+                    double* value);
 
 #ifdef __cplusplus
 }
