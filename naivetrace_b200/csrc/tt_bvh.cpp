@@ -169,8 +169,15 @@ bool build_bvh(const BvhInput& in, int max_leaf, BvhOutput* out) {
   if (n > 0) b.build(nodes, 0, (int)n, 0, &depth);
   out->max_depth = depth;
 
-  // Triangle slots in leaf order.
-  out->tris.assign(12 * (size_t)n, 0.f);
+  // Triangle slots in leaf order.  An empty set still gets one slot: a degenerate triangle
+  // at the origin (prim id -1) that no ray can hit, so that the synthetic root's leaf
+  // reference to slot 0 stays in bounds.  (An empty child box is stored inverted, which
+  // the slab test does not reject, so traversal may visit slot 0 through it.)
+  out->tris.assign(12 * (size_t)std::max<uint32_t>(n, 1), 0.f);
+  if (n == 0) {
+    const int32_t none = -1;
+    std::memcpy(&out->tris[3], &none, 4);
+  }
   for (uint32_t i = 0; i < n; ++i) {
     const int t = b.order[i];
     float* dst = &out->tris[12 * (size_t)i];
@@ -180,7 +187,7 @@ bool build_bvh(const BvhInput& in, int max_leaf, BvhOutput* out) {
       dst[4 * j + 1] = v[1];
       dst[4 * j + 2] = v[2];
     }
-    int32_t prim = t, mat = (int32_t)in.material_ids[t];
+    int32_t prim = in.prim_ids ? (int32_t)in.prim_ids[t] : t, mat = (int32_t)in.material_ids[t];
     std::memcpy(&dst[3], &prim, 4);
     std::memcpy(&dst[7], &mat, 4);
   }

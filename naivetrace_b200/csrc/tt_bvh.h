@@ -10,7 +10,7 @@
 //   int4   n3 = (c0 ref, c1 ref, 0, 0)
 // A child ref >= 0 is an inner node index; a ref < 0 is a leaf: v = ~ref,
 // first triangle slot = v >> 3, triangle count = (v & 7) + 1.  An empty child has an
-// inverted box and never intersects.  Triangles are stored per leaf slot as three float4
+// inverted box and refers to slot 0; an empty triangle set gets one degenerate slot.  Triangles are stored per leaf slot as three float4
 // (v0.xyz | prim id, v1.xyz | material id, v2.xyz | 0).
 #pragma once
 
@@ -24,6 +24,7 @@ struct BvhInput {
   const uint32_t* indices;      // T x 3
   const uint32_t* material_ids; // T
   uint32_t num_triangles;
+  const uint32_t* prim_ids = nullptr;  // T ids stored in the slots (nullptr: 0 .. T-1)
 };
 
 struct BvhOutput {

@@ -64,6 +64,7 @@ struct tt_ctx {
   std::vector<float> verts, normals;
   std::vector<uint32_t> idx, mats;
   std::vector<tt_material> materials;
+  std::vector<tt_medium> media;
   std::vector<HostEnv> envs;
   std::vector<tt_point_light> points;
   tt_camera camera{};
@@ -165,13 +166,25 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
       return fail(nullptr, TT_ERR_INVALID, "medium index out of range in material " + std::to_string(i));
   }
   if (d->num_media > 0 && !d->media) return fail(nullptr, TT_ERR_INVALID, "media missing");
-  if (d->num_media > 0) return fail(nullptr, TT_ERR_INVALID, "participating media are not supported by this build");
+  if (d->num_media > (uint32_t)kMaxMedia) return fail(nullptr, TT_ERR_CAPACITY, "more than 254 media");
+  for (uint32_t i = 0; i < d->num_media; ++i) {
+    const tt_medium& m = d->media[i];
+    if (m.kind != TT_MEDIUM_HOMOGENEOUS) return fail(nullptr, TT_ERR_INVALID, "unknown medium kind");
+    if (m.phase < TT_PHASE_UNIFORM || m.phase > TT_PHASE_HENYEY_GREENSTEIN)
+      return fail(nullptr, TT_ERR_INVALID, "unknown phase function in medium " + std::to_string(i));
+    if (m.phase == TT_PHASE_HENYEY_GREENSTEIN && !(std::fabs(m.phase_g) < 1.f))
+      return fail(nullptr, TT_ERR_INVALID, "Henyey-Greenstein g must lie in (-1, 1)");
+    for (int b = 0; b < NBINS; ++b)
+      if (!(m.sigma_s[b] >= 0.f) || !(m.sigma_a[b] >= 0.f) || !std::isfinite(m.sigma_s[b] + m.sigma_a[b]))
+        return fail(nullptr, TT_ERR_INVALID, "medium coefficients must be finite and non-negative");
+  }
   auto* c = new tt_ctx;
   c->verts.assign(d->vertices, d->vertices + 3 * (size_t)d->num_vertices);
   if (d->normals) c->normals.assign(d->normals, d->normals + 3 * (size_t)d->num_vertices);
   c->idx.assign(d->indices, d->indices + 3 * (size_t)d->num_triangles);
   c->mats.assign(d->material_ids, d->material_ids + d->num_triangles);
   c->materials.assign(d->materials, d->materials + d->num_materials);
+  if (d->num_media > 0) c->media.assign(d->media, d->media + d->num_media);
   for (uint32_t i = 0; i < d->num_env_lights; ++i) {
     HostEnv e;
     e.desc = d->env_lights[i];
@@ -208,14 +221,28 @@ tt_status tt_upload_scene(tt_ctx* c) {
   upload_constant_tables();
   TT_CUDA(c, cudaGetLastError());
   const uint32_t ntri = (uint32_t)c->mats.size();
-  // BVH.
-  BvhInput bi{c->verts.data(), c->idx.data(), c->mats.data(), ntri};
+  // Surfaces and medium boundaries go into separate BVHs (Scene::BuildAccelStructure,
+  // scene.cxx:116-141); both store global triangle ids in their slots.
+  std::vector<uint32_t> sidx, smat, sid, vidx, vmat, vid;
+  for (uint32_t t = 0; t < ntri; ++t) {
+    const bool vol = c->materials[c->mats[t]].volume_boundary != 0;
+    std::vector<uint32_t>& ix = vol ? vidx : sidx;
+    ix.insert(ix.end(), &c->idx[3 * (size_t)t], &c->idx[3 * (size_t)t] + 3);
+    (vol ? vmat : smat).push_back(c->mats[t]);
+    (vol ? vid : sid).push_back(t);
+  }
+  BvhInput bi{c->verts.data(), sidx.data(), smat.data(), (uint32_t)sid.size(), sid.data()};
   BvhOutput bo;
   if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
   c->bvh_nodes = bo.num_nodes;
   c->bvh_depth = bo.max_depth;
   if (bo.max_depth + 2 >= (uint32_t)BVH_STACK)
     return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
+  BvhInput vbi{c->verts.data(), vidx.data(), vmat.data(), (uint32_t)vid.size(), vid.data()};
+  BvhOutput vbo;
+  if (!build_bvh(vbi, 4, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
+  if (vbo.max_depth + 2 >= (uint32_t)BVH_STACK)
+    return fail(c, TT_ERR_CAPACITY, "medium-boundary BVH deeper than the traversal stack");
   auto upload = [&](const void* src, size_t bytes) -> void* {
     void* p = c->scene_mem.alloc(bytes);
     if (p && bytes) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
@@ -224,6 +251,9 @@ tt_status tt_upload_scene(tt_ctx* c) {
   DevScene& s = c->dev;
   s.nodes = (const float4*)upload(bo.nodes.data(), bo.nodes.size() * sizeof(float));
   s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
+  s.vnodes = (const float4*)upload(vbo.nodes.data(), vbo.nodes.size() * sizeof(float));
+  s.vtris = (const float4*)upload(vbo.tris.data(), vbo.tris.size() * sizeof(float));
+  s.num_vol_tris = (int)vid.size();
   std::vector<uint32_t> ti(4 * (size_t)ntri);
   for (uint32_t t = 0; t < ntri; ++t) {
     ti[4 * t] = c->idx[3 * t];
@@ -233,7 +263,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   }
   s.tri_idx = (const uint4*)upload(ti.data(), ti.size() * sizeof(uint32_t));
   s.normals = c->normals.empty() ? nullptr : (const float*)upload(c->normals.data(), c->normals.size() * sizeof(float));
-  s.num_tris = (int)ntri;
+  s.num_tris = (int)sid.size();
   // Materials.
   std::vector<DevMaterial> dm(c->materials.size());
   for (size_t i = 0; i < dm.size(); ++i) {
@@ -242,16 +272,37 @@ tt_status tt_upload_scene(tt_ctx* c) {
     dm[i].emissive = m.emissive ? 1 : 0;
     dm[i].alpha = m.alpha;
     dm[i].ior_ratio = m.ior_ratio;
+    dm[i].med_in = m.medium_inside - 1;
+    dm[i].med_out = m.medium_outside - 1;
     std::memcpy(dm[i].reflectance, m.reflectance, sizeof(m.reflectance));
     std::memcpy(dm[i].emission, m.emission, sizeof(m.emission));
   }
   s.materials = (const DevMaterial*)upload(dm.data(), dm.size() * sizeof(DevMaterial));
+  // Media.
+  std::vector<DevMedium> dmed(c->media.size());
+  for (size_t i = 0; i < dmed.size(); ++i) {
+    const tt_medium& m = c->media[i];
+    DevMedium& o = dmed[i];
+    o.priority = m.priority;
+    o.phase = m.phase;
+    o.g = m.phase_g;
+    o.scattering = 0;
+    for (int b = 0; b < NBINS; ++b) {
+      o.sigma_s[b] = m.sigma_s[b];
+      o.sigma_ext[b] = m.sigma_s[b] + m.sigma_a[b];
+      o.scattering |= m.sigma_s[b] > 0.f;
+    }
+  }
+  s.media = (const DevMedium*)upload(dmed.data(), dmed.size() * sizeof(DevMedium));
+  s.num_media = (int)dmed.size();
+  s.cam_track = make_uint2(0xffffffffu, (unsigned)-1);
   // Area lights: every triangle of an emissive material, in triangle order
   // (Scene::UpdateEmissiveIndexOffset numbers emissive primitives consecutively).
   std::vector<int> al;
   std::vector<float> av;
   for (uint32_t t = 0; t < ntri; ++t) {
-    if (!c->materials[c->mats[t]].emissive) continue;
+    const tt_material& mt = c->materials[c->mats[t]];
+    if (!mt.emissive || mt.volume_boundary) continue;
     al.push_back((int)t);
     for (int j = 0; j < 3; ++j) {
       const float* v = &c->verts[3 * (size_t)c->idx[3 * t + j]];
@@ -391,6 +442,22 @@ tt_status tt_upload_scene(tt_ctx* c) {
   if (tot == 0. && s.sample_lights) s.sample_lights = 0;  // no light to sample
   for (void* p : c->scene_mem.allocs)
     if (!p) return fail(c, TT_ERR_CUDA, "device allocation failed");
+  c->d_err = (unsigned int*)c->scene_mem.alloc(sizeof(unsigned int));
+  if (!c->d_err) return fail(c, TT_ERR_CUDA, "device allocation failed");
+  TT_CUDA(c, cudaMemset(c->d_err, 0, sizeof(unsigned int)));
+  if (s.num_media > 0) {
+    // Medium tracker at the camera (every camera path starts there).
+    uint2* d_track = (uint2*)c->scene_mem.alloc(sizeof(uint2));
+    if (!d_track) return fail(c, TT_ERR_CUDA, "device allocation failed");
+    launch_init_tracker(s, make_float3(c->camera.pos[0], c->camera.pos[1], c->camera.pos[2]),
+                        make_float3((float)lo[0], (float)lo[1], (float)lo[2]),
+                        make_float3((float)hi[0], (float)hi[1], (float)hi[2]), d_track, c->d_err, c->stream);
+    TT_CUDA(c, cudaGetLastError());
+    uint2 h_track;
+    TT_CUDA(c, cudaMemcpyAsync(&h_track, d_track, sizeof(uint2), cudaMemcpyDeviceToHost, c->stream));
+    TT_CUDA(c, cudaStreamSynchronize(c->stream));
+    s.cam_track = h_track;
+  }
   // Framebuffers and counters.
   const size_t n3 = 3 * (size_t)c->npix;
   c->fb.accum = (float*)c->scene_mem.alloc(n3 * sizeof(float));
@@ -398,15 +465,13 @@ tt_status tt_upload_scene(tt_ctx* c) {
   c->d_acc = (double*)c->scene_mem.alloc(n3 * sizeof(double));
   c->d_light = (double*)c->scene_mem.alloc(n3 * sizeof(double));
   c->d_stats = (unsigned long long*)c->scene_mem.alloc(8 * sizeof(unsigned long long));
-  c->d_err = (unsigned int*)c->scene_mem.alloc(sizeof(unsigned int));
-  if (!c->fb.accum || !c->fb.light || !c->d_acc || !c->d_light || !c->d_stats || !c->d_err)
+  if (!c->fb.accum || !c->fb.light || !c->d_acc || !c->d_light || !c->d_stats)
     return fail(c, TT_ERR_CUDA, "device allocation failed");
   TT_CUDA(c, cudaMemset(c->fb.accum, 0, n3 * sizeof(float)));
   TT_CUDA(c, cudaMemset(c->fb.light, 0, n3 * sizeof(float)));
   TT_CUDA(c, cudaMemset(c->d_acc, 0, n3 * sizeof(double)));
   TT_CUDA(c, cudaMemset(c->d_light, 0, n3 * sizeof(double)));
   TT_CUDA(c, cudaMemset(c->d_stats, 0, 8 * sizeof(unsigned long long)));
-  TT_CUDA(c, cudaMemset(c->d_err, 0, sizeof(unsigned int)));
   int sms = 0;
   TT_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   c->grid = sms * kernel_blocks_per_sm();
@@ -442,6 +507,12 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
   p.sh_q = (int*)m.alloc(n * sizeof(int));
   p.done_q = (int*)m.alloc(n * sizeof(int));
   p.counters = (int*)m.alloc(kCountersPerBounce * (size_t)(c->rounds + 3) * sizeof(int));
+  if (c->dev.num_media > 0) {
+    p.track = (uint2*)m.alloc(n * sizeof(uint2));
+    p.vol = (float4*)m.alloc(n * sizeof(float4));
+    p.sh_track = (uint2*)m.alloc(n * sizeof(uint2));
+    p.sh_mis = (float2*)m.alloc(n * sizeof(float2));
+  }
   p.err = c->d_err;
   for (void* a : m.allocs)
     if (!a) {
@@ -510,6 +581,10 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
       timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, b, counting, c->d_stats + 2, grid, c->stream); });
       launch_flush(c->ps, c->fb, b, grid, c->stream);
       timed(0, [&] { launch_extend(c->dev, c->ps, b, counting, c->d_stats, grid, c->stream); });
+      if (c->dev.num_media > 0) {
+        launch_track(c->dev, c->ps, b, grid, c->stream);
+        launches++;
+      }
       launch_shade(c->dev, c->ps, b, grid, c->stream);
       launches += 4;
     }

@@ -654,4 +654,155 @@ __device__ __forceinline__ int camera_evaluate(const DevCamera& c, float3 dir_ou
   return py * c.xres + px;
 }
 
+// ----------------------------------------------------------------------------------------
+// Participating media.
+
+// Phase functions (phasefunctions.cxx:23-138).  mu is the cosine between the direction of
+// travel before and after scattering.
+__device__ __forceinline__ float phase_value(const DevMedium& m, float mu) {
+  if (m.phase == TT_PHASE_RAYLEIGH) return (3.f / (16.f * kPi)) * (1.f + mu * mu);
+  if (m.phase == TT_PHASE_HENYEY_GREENSTEIN) {
+    const float g = m.g, g2 = g * g;
+    const float term = 1.f + g2 - 2.f * g * mu;
+    return (1.f / (4.f * kPi)) * (1.f - g2) / (sqrtf(term) * term);
+  }
+  return 1.f / (4.f * kPi);
+}
+
+// Evaluate at a volume vertex: wi = reverse incident direction, wo = outgoing direction.
+__device__ __forceinline__ float phase_eval(const DevMedium& m, float3 wi, float3 wo) {
+  return phase_value(m, dot3(-wi, wo));
+}
+
+// Sample about the direction of travel -wi.  Rayleigh inverts its cdf in closed form;
+// Henyey-Greenstein uses its textbook inversion with a series for |g| <= 1e-3.
+// Directions are laid out as (sin(2 pi r1) rho, cos(2 pi r1) rho, mu) in the frame whose
+// z axis is the direction of travel.
+__device__ __forceinline__ float3 phase_sample(const DevMedium& m, float3 wi, Rng& rng, float* pdf) {
+  float r[2];
+  rng.square(r);
+  if (m.phase == TT_PHASE_UNIFORM) {
+    *pdf = 1.f / (4.f * kPi);
+    return to_uniform_sphere(r);
+  }
+  float mu;
+  if (m.phase == TT_PHASE_RAYLEIGH) {
+    const float a = cbrtf(-2.f + 4.f * r[0] + sqrtf(5.f - 16.f * r[0] + 16.f * r[0] * r[0]));
+    mu = a - 1.f / a;
+  } else {
+    const float g = m.g, g2 = g * g, x = 2.f * r[0] - 1.f;
+    if (fabsf(g) > 1.0e-3f) {
+      const float t1 = (1.f - g2) / (1.f + g * x);
+      mu = (1.f + g2 - t1 * t1) / (2.f * g);
+    } else {
+      const float x2 = x * x;
+      mu = x + 1.5f * g * (1.f - x2) - 2.f * g2 * x * (1.f - x2);
+    }
+  }
+  mu = fminf(1.f, fmaxf(-1.f, mu));
+  const float rho = sqrtf(fmaxf(0.f, 1.f - mu * mu));
+  float sn, cs;
+  sincosf(2.f * kPi * r[1], &sn, &cs);
+  const Frame fr = frame_z(-wi);
+  *pdf = phase_value(m, mu);
+  return normalize3(fr.to_world(f3(sn * rho, cs * rho, mu)));
+}
+
+// MediumTracker (rendering_util.hxx:18-126): up to four overlapping media in byte slots
+// (0xff empty) and the current one (-1 = the vacuum of empty space, priority -1).
+struct MTracker {
+  uint32_t slots;
+  int cur;
+};
+__device__ __forceinline__ MTracker load_tracker(uint2 v) { return MTracker{v.x, (int)v.y}; }
+__device__ __forceinline__ uint2 store_tracker(const MTracker& t) { return make_uint2(t.slots, (unsigned)t.cur); }
+__device__ __forceinline__ int medium_priority(const DevScene& sc, int m) {
+  return m < 0 ? -1 : sc.media[m].priority;
+}
+
+// goingThroughSurface: crossing a surface of material `mat` along dir, with the winding
+// normal ng deciding which side is entered.
+__device__ __forceinline__ void going_through(const DevScene& sc, MTracker& t, float3 dir, float3 ng, int mat) {
+  const DevMaterial& M = sc.materials[mat];
+  int to_enter = M.med_in, to_exit = M.med_out;
+  if (to_enter < 0 && to_exit < 0) return;
+  if (dot3(dir, ng) > 0.f) { const int x = to_enter; to_enter = to_exit; to_exit = x; }
+  if (to_exit >= 0) {
+    for (int i = 0; i < 4; ++i)
+      if ((int)((t.slots >> (8 * i)) & 0xffu) == to_exit) { t.slots |= 0xffu << (8 * i); break; }
+    if (to_exit == t.cur) {
+      int best = -1;
+      for (int i = 0; i < 4; ++i) {
+        const int m = (int)((t.slots >> (8 * i)) & 0xffu);
+        if (m != 0xff && medium_priority(sc, best) < medium_priority(sc, m)) best = m;
+      }
+      t.cur = best;
+    }
+  }
+  if (to_enter >= 0) {
+    bool inserted = false;
+    for (int i = 0; i < 4; ++i)
+      if (((t.slots >> (8 * i)) & 0xffu) == 0xffu) {
+        t.slots = (t.slots & ~(0xffu << (8 * i))) | ((uint32_t)to_enter << (8 * i));
+        inserted = true;
+        break;
+      }
+    if (inserted && medium_priority(sc, to_enter) > medium_priority(sc, t.cur)) t.cur = to_enter;
+  }
+}
+
+__device__ __forceinline__ float mean3(float3 a) { return (a.x + a.y + a.z) * (1.f / 3.f); }
+__device__ __forceinline__ float3 exp_neg(float3 s, float x) { return f3(expf(-s.x * x), expf(-s.y * x), expf(-s.z * x)); }
+
+struct InteractionSample {
+  float t;
+  float3 weight;
+  float3 sigma_s;
+};
+
+// HomogeneousMedium::SampleInteractionPoint (shader.cxx:1259-1270) with
+// HomogeneousSpectralTracking (media_integrator.cxx:43-87; Kutz et al. 2017, history-aware
+// collision probabilities).  `hist` is the tracking weight accumulated so far on this ray.
+// At most 99 collisions are simulated; the capped sample reports an interaction with zero
+// sigma_s, as the reference's emergency abort does.
+__device__ __forceinline__ InteractionSample sample_interaction(const DevMedium& m, float length, float3 hist,
+                                                                 Rng& rng, Lambda l) {
+  InteractionSample out;
+  const float3 se = take(m.sigma_ext, l);
+  if (!m.scattering) {
+    out.t = kLargeNumber;
+    out.weight = exp_neg(se, length);
+    out.sigma_s = f3(0.f, 0.f, 0.f);
+    return out;
+  }
+  const float3 ss = take(m.sigma_s, l);
+  const float maj = max3(se);
+  const float3 sn = f3(maj - se.x, maj - se.y, maj - se.z);
+  const float inv = 1.f / maj;
+  out.t = 0.f;
+  out.weight = f3(1.f, 1.f, 1.f);
+  out.sigma_s = f3(0.f, 0.f, 0.f);
+  for (int it = 1; it < 100; ++it) {
+    out.t -= logf(rng.uniform()) * inv;
+    if (out.t > length) return out;
+    const float3 w = mul(out.weight, hist);
+    float pt = mean3(mul(ss, w)), pn = mean3(mul(sn, w));
+    const float norm = pt + pn;
+    if (norm > 0.f) { pt /= norm; pn /= norm; } else { pt = pn = 0.5f; }
+    if (rng.uniform() < pt) {
+      out.weight = out.weight * (inv / pt);
+      out.sigma_s = ss;
+      return out;
+    }
+    out.weight = mul(out.weight, sn) * (inv / pn);
+  }
+  return out;
+}
+
+// VolumePdfCoefficients::transmittance of one segment (ComputeVolumePdfCoefficients,
+// shader.cxx:1297-1309): the mean over the three wavelengths.
+__device__ __forceinline__ float segment_tr(const DevMedium& m, float len, Lambda l) {
+  return mean3(exp_neg(take(m.sigma_ext, l), len));
+}
+
 }  // namespace tt

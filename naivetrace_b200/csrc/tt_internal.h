@@ -14,6 +14,9 @@ constexpr int MAX_ENV_LIGHTS = 4;
 constexpr int BVH_STACK = 64;        // per-thread traversal stack (entries)
 constexpr uint32_t ERR_STACK = 1u;   // error-word bits written by kernels
 constexpr uint32_t ERR_QUEUE = 2u;
+constexpr uint32_t ERR_CROSSINGS = 4u;  // a ray crossed more medium boundaries than the cap
+constexpr int kMaxCrossings = 256;      // boundary crossings followed along one ray
+constexpr int kMaxMedia = 254;          // medium indices are stored in bytes (0xff = empty)
 constexpr int kCountersPerBounce = 3;  // ext, shadow, done queue lengths
 
 // Surface material as stored on the device.
@@ -22,8 +25,21 @@ struct DevMaterial {
   int emissive;
   float alpha;
   float ior_ratio;
+  int med_in;        // medium entered through the front side (winding normal), -1 none
+  int med_out;       // medium on the front side, -1 none
+  int pad[2];
   float reflectance[NBINS];
   float emission[NBINS];
+};
+
+// Homogeneous medium (HomogeneousMedium, shader.cxx:1234-1316) with its phase function.
+struct DevMedium {
+  int priority;
+  int phase;         // TT_PHASE_*
+  float g;           // Henyey-Greenstein asymmetry
+  int scattering;    // any sigma_s > 0
+  float sigma_s[NBINS];
+  float sigma_ext[NBINS];
 };
 
 struct DevEnvLight {
@@ -67,6 +83,14 @@ struct DevScene {
   int max_path_nodes;         // max_ray_depth + 1
   int sample_lights;
   int sample_bsdf;
+  // Participating media: medium boundaries live in their own BVH (same layout as the
+  // surface BVH), as in Scene::BuildAccelStructure (scene.cxx:116-141).
+  const float4* vnodes;
+  const float4* vtris;
+  int num_vol_tris;
+  int num_media;
+  const DevMedium* media;
+  uint2 cam_track;            // medium tracker at the camera position
 };
 
 // Wavefront path state, structure of arrays, capacity `cap` paths.
@@ -88,6 +112,11 @@ struct PathState {
   int* done_q;
   int* counters;       // kCountersPerBounce ints per bounce, (max bounces + 3) bounces
   unsigned int* err;
+  // Media scenes only (null otherwise).
+  uint2* track;        // medium tracker: x = 4 slot bytes (0xff empty), y = current medium (-1 vacuum)
+  float4* vol;         // sigma_s at a volume interaction (xyz); w = transmittance pdf factor of the step
+  uint2* sh_track;     // medium tracker of the shadow ray at its origin
+  float2* sh_mis;      // x = light pdf (< 0: MIS weight 1), y = scatter pdf before the transmittance factor
 };
 
 struct Framebuffer {
@@ -116,6 +145,11 @@ void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, c
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st);
 void launch_flush(const PathState& p, const Framebuffer& fb, int bounce, int grid, cudaStream_t st);
+// Media scenes: spectral tracking from each extension ray's origin to its surface hit.
+void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);
+// Medium tracker at `pos` (MediumTracker::initializePosition); writes one uint2 to `out`.
+void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_hi, uint2* out, unsigned int* err,
+                         cudaStream_t st);
 void launch_accumulate(const Framebuffer& fb, double* acc, double* light, int n3, cudaStream_t st);
 void launch_intersect_rays(const DevScene& s, const float* rays, int n, int* prim, float* t, float* u, float* v,
                            unsigned int* err, cudaStream_t st);

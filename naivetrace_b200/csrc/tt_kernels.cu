@@ -138,12 +138,20 @@ __device__ __forceinline__ void trace_init(TraceState& s, float3 o, float3 d, fl
 
 // One traversal step.  Returns true when the ray is finished (closest hit found, or for
 // ANY the first hit), with the result in s.best / best_t / b1 / b2.
+// A BVH in device layout: the surface BVH or the medium-boundary BVH.
+struct BvhRef {
+  const float4* nodes;
+  const float4* tris;
+};
+__device__ __forceinline__ BvhRef surface_bvh(const DevScene& sc) { return BvhRef{sc.nodes, sc.tris}; }
+__device__ __forceinline__ BvhRef volume_bvh(const DevScene& sc) { return BvhRef{sc.vnodes, sc.vtris}; }
+
 template <bool ANY, bool COUNT>
-__device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState& s, int* stack, unsigned int* err,
+__device__ __forceinline__ bool trace_step(const BvhRef& bvh, TraceState& s, int* stack, unsigned int* err,
                                            TraceCounters* cnt) {
   const RayPre& r = s.r;
   if (s.cur >= 0) {
-    const float4* np = sc.nodes + 4 * (size_t)s.cur;
+    const float4* np = bvh.nodes + 4 * (size_t)s.cur;
     const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
     const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
     if (COUNT) cnt->nodes++;
@@ -177,9 +185,9 @@ __device__ __forceinline__ bool trace_step(const DevScene& sc, TraceState& s, in
     const unsigned v = ~(unsigned)s.cur;
     const int start = (int)(v >> 3), count = (int)(v & 7u) + 1;
     for (int i = start; i < start + count; ++i) {
-      const float4 a = __ldg(&sc.tris[3 * i]);
-      const float4 b = __ldg(&sc.tris[3 * i + 1]);
-      const float4 c = __ldg(&sc.tris[3 * i + 2]);
+      const float4 a = __ldg(&bvh.tris[3 * i]);
+      const float4 b = __ldg(&bvh.tris[3 * i + 1]);
+      const float4 c = __ldg(&bvh.tris[3 * i + 2]);
       if (COUNT) cnt->tris++;
       float t, b1, b2;
       if (intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2)) {
@@ -214,6 +222,7 @@ __device__ __forceinline__ float refine_t(const DevScene& sc, const RayPre& r, i
 template <bool ANY, bool COUNT>
 __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float tnear, float tfar, float* t_out,
                                      float* b1_out, float* b2_out, unsigned int* err, TraceCounters* cnt) {
+  const BvhRef bvh = surface_bvh(sc);
   TraceState s;
   int stack[BVH_STACK];
   s.r = r;
@@ -223,7 +232,7 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
   s.best = -1;
   s.cur = 0;
   s.sp = 0;
-  while (!trace_step<ANY, COUNT>(sc, s, stack, err, cnt)) {
+  while (!trace_step<ANY, COUNT>(bvh, s, stack, err, cnt)) {
   }
   if (s.best >= 0) {
     *t_out = ANY ? s.best_t : refine_t(sc, r, s.best);
@@ -231,6 +240,46 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
     *b2_out = s.b2;
   }
   return s.best;
+}
+
+// Nearest hit with tnear < t <= tfar in `bvh`, with the single-precision plane distance
+// (no refinement, so that the next query can start exactly at the returned t).  Returns
+// the triangle slot or -1.
+__device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, float tnear, float tfar, float* t_out,
+                                        unsigned int* err) {
+  TraceState s;
+  int stack[BVH_STACK];
+  s.r = r;
+  s.tnear = tnear;
+  s.best_t = tfar;
+  s.b1 = s.b2 = 0.f;
+  s.best = -1;
+  s.cur = 0;
+  s.sp = 0;
+  while (!trace_step<false, false>(bvh, s, stack, err, nullptr)) {
+  }
+  *t_out = s.best_t;
+  return s.best;
+}
+
+// Nearest medium-boundary crossing after tnear: the next entry of
+// EmbreeAccelerator::IntersectionsInOrder (embreeaccelerator.cxx:134-213).  Walking the
+// crossings one query at a time with tnear = the previous crossing drops repeated hits at
+// the same distance, as the reference's (geometry, t) de-duplication does for the two
+// triangles that share an edge the ray passes through.
+__device__ __forceinline__ int next_crossing(const DevScene& sc, const RayPre& r, float tnear, float tfar,
+                                             float* t_out, unsigned int* err) {
+  if (sc.num_vol_tris == 0) return -1;
+  return next_hit(volume_bvh(sc), r, tnear, tfar, t_out, err);
+}
+
+// Winding normal and material of a medium-boundary triangle slot.
+__device__ __forceinline__ void crossing_info(const DevScene& sc, int slot, float3* ng, int* material) {
+  const float4 a = __ldg(&sc.vtris[3 * slot]);
+  const float4 b = __ldg(&sc.vtris[3 * slot + 1]);
+  const float4 c = __ldg(&sc.vtris[3 * slot + 2]);
+  *ng = cross3(xyz(b) - xyz(a), xyz(c) - xyz(a));
+  *material = __float_as_int(b.w);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -265,10 +314,13 @@ struct Connection {
 
 struct Eye {
   bool is_camera;
-  float3 pos;       // camera position or surface position
+  bool is_volume;   // a scattering event inside a medium
+  float3 pos;       // camera or volume-vertex position
   Surf surf;        // surface eye
-  float3 wi;        // reverse incident direction (surface eye)
+  float3 wi;        // reverse incident direction (surface and volume eyes)
   const DevMaterial* mat;
+  const DevMedium* med;  // volume eye: its medium
+  float3 sigma_s;        // volume eye: scattering coefficient at the vertex
 };
 
 __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye, const LightNode& L, Lambda l) {
@@ -278,7 +330,8 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
   c.pdf_due = 0.f;
   c.weight = f3(0.f, 0.f, 0.f);
   const bool light_env = L.type == LIGHT_ENV;
-  float3 cs = eye.is_camera ? eye.pos : eye.surf.pos;
+  const bool point_eye = eye.is_camera || eye.is_volume;  // no surface offset, DFactor 1
+  float3 cs = point_eye ? eye.pos : eye.surf.pos;
   float3 ct = L.coord;
   // CalculateSegmentToTarget: direction, offsets on surface nodes, recompute.
   float3 d;
@@ -291,7 +344,7 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
     d = -ct;
     len = sc.long_distance;
   }
-  if (!eye.is_camera) cs = cs + offset_at(eye.surf, d);
+  if (!point_eye) cs = cs + offset_at(eye.surf, d);
   if (L.type == LIGHT_AREA) {
     const float delta = dot3(L.bounds, abs3(L.ng));
     ct = ct + (delta * (dot3(-d, L.ng) > 0.f ? 1.f : -1.f)) * L.ng;
@@ -311,6 +364,10 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
     const int unit = camera_evaluate(sc.cam, d, &pdf_eye);
     c.unit = unit;
     sf = unit >= 0 ? f3(pdf_eye, pdf_eye, pdf_eye) : f3(0.f, 0.f, 0.f);
+  } else if (eye.is_volume) {
+    // EvaluateScatterCoordinateOfScatterer, volume branch: sigma_s x phase function.
+    pdf_eye = phase_eval(*eye.med, eye.wi, d);
+    sf = eye.sigma_s * pdf_eye;
   } else {
     sf = eval_bsdf(*eye.mat, eye.wi, eye.surf, d, l, &pdf_eye) * bsdf_correction(eye.surf, d);
   }
@@ -329,7 +386,7 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
   // infinity.
   c.pdf_due = light_env ? pdf_eye * dfac_light : pdf_eye * dfac_light / (len * len + kEps);
   if (is_zero(sf) || is_zero(tf)) return c;
-  const float dfac_eye = eye.is_camera ? 1.f : fabsf(dot3(eye.surf.ng, d));
+  const float dfac_eye = point_eye ? 1.f : fabsf(dot3(eye.surf.ng, d));
   const float r2 = light_env ? 1.f : 1.f / (len * len);
   c.weight = mul(sf * dfac_eye, tf * dfac_light) * r2;
   c.valid = true;
@@ -394,8 +451,33 @@ __device__ __forceinline__ LightNode pick_light(const DevScene& sc, Rng& rng, La
 }
 
 // ----------------------------------------------------------------------------------------
+// Queues a shadow ray for the connection c.  Without media the MIS weight is final here;
+// with media it depends on the transmittance pdf factor of the segment, which the shadow
+// kernel computes, so the light pdf and the scatter pdf travel with the ray.
+template <bool MEDIA>
+__device__ __forceinline__ void emit_shadow(const DevScene& sc, const PathState& p, int qbounce, int slot,
+                                            const Connection& c, const LightNode& L, float3 beta, float scale,
+                                            int target, const MTracker& mt) {
+  float3 contrib;
+  if (MEDIA) {
+    contrib = mul(c.weight, beta) * (scale / L.pdf);
+    const bool mis_on = !L.delta && sc.sample_bsdf && sc.sample_lights;
+    p.sh_mis[slot] = make_float2(mis_on ? L.pdf : -1.f, c.pdf_due);
+    p.sh_track[slot] = store_tracker(mt);
+  } else {
+    const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
+    contrib = mul(c.weight, beta) * (mis * scale / L.pdf);
+  }
+  const int q = warp_append(sh_count(p, qbounce));
+  p.sh_q[q] = slot;
+  p.sh_o[slot] = make_float4(c.org.x, c.org.y, c.org.z, c.len * 0.9999f);
+  p.sh_d[slot] = make_float4(c.dir.x, c.dir.y, c.dir.z, __int_as_float(target));
+  p.sh_c[slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+}
+
+template <bool MEDIA>
 __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Framebuffer fb, WaveArgs w) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.wave_paths; i += gridDim.x * blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.wave_paths; i += gridDim.x * blockDim.x) {
     const long long g = w.wave_start + i;
     const int pix_local = (int)(g % w.npix_range);
     const unsigned long long sample = w.sample_offset + (unsigned long long)(g / w.npix_range);
@@ -411,6 +493,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     const Lambda l{idx[0], idx[1], idx[2]};
     const float3 beta = f3(12.f, 12.f, 12.f);
     const float3 cam_pos = f3(sc.cam.pos[0], sc.cam.pos[1], sc.cam.pos[2]);
+    const MTracker cam_mt = load_tracker(sc.cam_track);
     p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     // Next-event estimation at the camera vertex: a light sample seen directly by the
     // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
@@ -419,17 +502,11 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
       if (L.type != LIGHT_NONE) {
         Eye eye;
         eye.is_camera = true;
+        eye.is_volume = false;
         eye.pos = cam_pos;
         Connection c = connect(sc, eye, L, l);
-        if (c.valid && c.unit >= 0) {
-          const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
-          const float3 contrib = mul(c.weight, beta) * (mis / L.pdf / (float)w.npix_total);
-          const int q = warp_append(sh_count(p, 0));
-          p.sh_q[q] = i;
-          p.sh_o[i] = make_float4(c.org.x, c.org.y, c.org.z, c.len * 0.9999f);
-          p.sh_d[i] = make_float4(c.dir.x, c.dir.y, c.dir.z, __int_as_float(c.unit));
-          p.sh_c[i] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
-        }
+        if (c.valid && c.unit >= 0)
+          emit_shadow<MEDIA>(sc, p, 0, i, c, L, beta, 1.f / (float)w.npix_total, c.unit, cam_mt);
       }
     }
     // Camera ray (TakeRandomWalkStep from the camera node).
@@ -438,6 +515,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), 1u, s.delta ? 1u : 0u);
     p.rng_state[i] = rng.state;
     p.rng_inc[i] = rng.inc;
+    if (MEDIA) p.track[i] = sc.cam_track;
     if (is_zero(bf)) {
       const int q = warp_append(done_count(p, 0));
       p.done_q[q] = i;
@@ -474,8 +552,72 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
   }
 }
 
+// Media scenes, after k_extend: TrackToNextInteraction (rendering_util.hxx:215-269).  The
+// medium-boundary crossings in front of the surface hit (up to 0.9999 of its distance) are
+// walked in order; in each segment spectral tracking samples a collision in the current
+// medium.  A collision turns the hit into a volume vertex (hit.w = -2 - medium, hit.x =
+// distance, vol.xyz = sigma_s); otherwise the tracker ends past every crossing.  The
+// tracking weight multiplies the throughput, and vol.w receives the product of the
+// segments' mean transmittances (the pdf factor of PdfConversionFactor).
+__global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bounce) {
+  const int n = *ext_count(p, bounce);
+  const int* q = p.ext_q[bounce & 1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int slot = q[i];
+    float4 h = p.hit[slot];
+    const float4 o = p.ray_o[slot], d = p.ray_d[slot];
+    const int tri = __float_as_int(h.w);
+    const float vend = (tri >= 0 ? h.x : kLargeNumber) * 0.9999f;
+    MTracker mt = load_tracker(p.track[slot]);
+    const Lambda l = unpack_lambda(p.meta[slot].y);
+    Rng rng{p.rng_state[slot], p.rng_inc[slot]};
+    const RayPre r = prepare_ray(xyz(o), xyz(d));
+    float3 weight = f3(1.f, 1.f, 1.f);
+    float ctr = 1.f;
+    float snear = 0.f;
+    bool interacted = false;
+    float3 sig_s = f3(0.f, 0.f, 0.f);
+    for (int k = 0;; ++k) {
+      float tc;
+      const int cs = next_crossing(sc, r, snear, vend, &tc, p.err);
+      const float sfar = cs >= 0 ? tc : vend;
+      const int m = mt.cur;
+      if (m >= 0) {
+        const DevMedium& M = sc.media[m];
+        const InteractionSample ms = sample_interaction(M, sfar - snear, weight, rng, l);
+        weight = mul(weight, ms.weight);
+        interacted = ms.t < sfar - snear;
+        ctr *= segment_tr(M, interacted ? ms.t : sfar - snear, l);
+        if (interacted) {
+          h = make_float4(snear + ms.t, 0.f, 0.f, __int_as_float(-2 - m));
+          sig_s = ms.sigma_s;
+          break;
+        }
+      }
+      if (cs < 0) break;
+      if (k >= kMaxCrossings) {
+        atomicOr(p.err, ERR_CROSSINGS);
+        weight = f3(0.f, 0.f, 0.f);
+        break;
+      }
+      float3 ng;
+      int mat;
+      crossing_info(sc, cs, &ng, &mat);
+      going_through(sc, mt, xyz(d), ng, mat);
+      snear = sfar;
+    }
+    if (interacted) p.hit[slot] = h;
+    p.vol[slot] = make_float4(sig_s.x, sig_s.y, sig_s.z, ctr);
+    p.track[slot] = store_tracker(mt);
+    p.rng_state[slot] = rng.state;
+    const float4 b = p.beta[slot];
+    p.beta[slot] = make_float4(b.x * weight.x, b.y * weight.y, b.z * weight.z, b.w);
+  }
+}
+
+template <bool MEDIA>
 __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bounce) {
-    const int n = *ext_count(p, bounce);
+  const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = q[i];
@@ -495,7 +637,15 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
     const int tri = __float_as_int(h.w);
     bool done = false;
     Surf s;
-    if (tri >= 0) {
+    // Media: the step's transmittance pdf factor and, at a volume vertex, sigma_s.
+    const float4 vol = MEDIA ? p.vol[slot] : make_float4(0.f, 0.f, 0.f, 1.f);
+    const float ctr = vol.w;
+    const bool is_volume = MEDIA && tri <= -2;
+    const int medium = is_volume ? -2 - tri : -1;
+    float3 vpos = f3(0.f, 0.f, 0.f);
+    if (is_volume) {
+      vpos = xyz(p.ray_o[slot]) + dir * h.x;
+    } else if (tri >= 0) {
       const float u = h.y, v = h.z;
       s = make_surface(sc, tri, 1.f - u - v, u, v, f3(u, v, 1.f - u - v));
       orient(s, dir);
@@ -508,7 +658,8 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
         const float area = tri_area(xyz(a), xyz(b), xyz(c));
         const float pdf_direct = (1.f / area) * sc.type_probs[1] * sc.in_class_area;
         const float dfac = fabsf(dot3(s.ng, dir));
-        const float pdf_due = prev_delta ? dfac * prev_pdf : dfac / (h.x * h.x + kEps) * prev_pdf;
+        float pdf_due = prev_delta ? dfac * prev_pdf : dfac / (h.x * h.x + kEps) * prev_pdf;
+        if (MEDIA) pdf_due *= ctr;
         const float mis = mis_weight(sc, pdf_due, prev_delta, pdf_direct);
         acc = acc + mul(end_weight, beta) * mis;
       }
@@ -517,7 +668,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       if (sc.sample_bsdf && sc.num_env > 0) {
         const float3 end_weight = env_eval_total(sc, -dir, l);
         const float pdf_direct = env_pdf_total(sc, -dir) * sc.type_probs[0];
-        const float mis = mis_weight(sc, prev_pdf, prev_delta, pdf_direct);
+        const float mis = mis_weight(sc, MEDIA ? prev_pdf * ctr : prev_pdf, prev_delta, pdf_direct);
         acc = acc + mul(end_weight, beta) * mis;
       }
       done = true;
@@ -535,42 +686,69 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       }
     }
     if (!done) {
-      const DevMaterial& m = sc.materials[s.material];
       const float3 wi = -dir;
+      MTracker mt;
+      if (MEDIA) mt = load_tracker(p.track[slot]);
       if (sc.sample_lights) {
         LightNode L = pick_light(sc, rng, l);
         if (L.type != LIGHT_NONE) {
           Eye eye;
           eye.is_camera = false;
-          eye.surf = s;
+          eye.is_volume = is_volume;
           eye.wi = wi;
-          eye.mat = &m;
+          if (is_volume) {
+            eye.pos = vpos;
+            eye.med = &sc.media[medium];
+            eye.sigma_s = xyz(vol);
+          } else {
+            eye.surf = s;
+            eye.mat = &sc.materials[s.material];
+          }
           Connection c = connect(sc, eye, L, l);
           if (c.valid) {
-            const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
-            const float3 contrib = mul(c.weight, beta) * (mis / L.pdf);
-            const int qs = warp_append(sh_count(p, bounce + 1));
-            p.sh_q[qs] = slot;
-            p.sh_o[slot] = make_float4(c.org.x, c.org.y, c.org.z, c.len * 0.9999f);
-            p.sh_d[slot] = make_float4(c.dir.x, c.dir.y, c.dir.z, __int_as_float(-1));
-            p.sh_c[slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
+            MTracker smt;
+            if (MEDIA) {
+              // MaybeHandlePassageThroughSurface at the eye (rendering_randomwalk_impl.hxx:517-527).
+              smt = mt;
+              if (!is_volume && dot3(c.dir, s.n) < 0.f) going_through(sc, smt, c.dir, s.ng, s.material);
+            }
+            emit_shadow<MEDIA>(sc, p, bounce + 1, slot, c, L, beta, 1.f, -1, smt);
           }
         }
       }
-      // BSDF sample (TakeRandomWalkStep from a surface scatter node).
-      ScatterSample ss = sample_bsdf(m, wi, s, rng, l);
-      const float3 val = ss.value * (bsdf_correction(s, ss.dir) * fabsf(dot3(s.ng, ss.dir)));
-      const float3 bf = val * (1.f / ss.pdf);
-      if (is_zero(bf) || !(ss.pdf > 0.f)) {
+      // Scatter: BSDF sample at a surface, phase-function sample at a volume vertex
+      // (TakeRandomWalkStep from a scatter node).
+      float3 ndir, bf, org;
+      float pdf;
+      bool delta;
+      if (is_volume) {
+        ndir = phase_sample(sc.media[medium], wi, rng, &pdf);
+        bf = xyz(vol);  // sigma_s x phase / phase pdf
+        delta = false;
+        org = vpos;
+      } else {
+        const DevMaterial& m = sc.materials[s.material];
+        ScatterSample ss = sample_bsdf(m, wi, s, rng, l);
+        const float3 val = ss.value * (bsdf_correction(s, ss.dir) * fabsf(dot3(s.ng, ss.dir)));
+        bf = val * (1.f / ss.pdf);
+        pdf = ss.pdf;
+        delta = ss.delta;
+        ndir = ss.dir;
+        org = s.pos + offset_at(s, ss.dir);
+      }
+      if (is_zero(bf) || !(pdf > 0.f)) {
         done = true;
       } else {
         beta = mul(beta, bf);
-        const float3 org = s.pos + offset_at(s, ss.dir);
+        if (MEDIA && !is_volume && dot3(ndir, s.n) < 0.f) {
+          going_through(sc, mt, ndir, s.ng, s.material);
+          p.track[slot] = store_tracker(mt);
+        }
         p.ray_o[slot] = make_float4(org.x, org.y, org.z, 0.f);
-        p.ray_d[slot] = make_float4(ss.dir.x, ss.dir.y, ss.dir.z, kLargeNumber);
-        p.beta[slot] = make_float4(beta.x, beta.y, beta.z, ss.pdf);
+        p.ray_d[slot] = make_float4(ndir.x, ndir.y, ndir.z, kLargeNumber);
+        p.beta[slot] = make_float4(beta.x, beta.y, beta.z, pdf);
         meta.z = (unsigned)count;
-        meta.w = ss.delta ? 1u : 0u;
+        meta.w = delta ? 1u : 0u;
         p.meta[slot] = meta;
         const int qe = warp_append(ext_count(p, bounce + 1));
         p.ext_q[(bounce + 1) & 1][qe] = slot;
@@ -586,8 +764,11 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
 }
 
 // Occlusion test of the queued shadow rays.  Unoccluded rays add their contribution to
-// the path (or, for camera-vertex samples, splat it to the pixel they project to).
-template <bool COUNT>
+// the path (or, for camera-vertex samples, splat it to the pixel they project to).  In
+// media scenes the contribution is multiplied by the transmittance through the media
+// between the medium-boundary crossings (TransmittanceEstimate, rendering_util.cxx:40-67)
+// and by the MIS weight that the segment's transmittance pdf factor completes.
+template <bool MEDIA, bool COUNT>
 __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Framebuffer fb, int bounce,
                                                 unsigned long long* counters) {
   const int n = *sh_count(p, bounce);
@@ -599,14 +780,45 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
     float t, b1, b2;
     const int hit = trace<true, COUNT>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
     if (hit >= 0) continue;
-    const float4 c = p.sh_c[slot];
+    const float4 c4 = p.sh_c[slot];
+    float3 c = xyz(c4);
     const int target = __float_as_int(d.w);
+    if (MEDIA) {
+      const Lambda l = unpack_lambda(p.meta[slot].y);
+      MTracker mt = load_tracker(p.sh_track[slot]);
+      float3 T = f3(1.f, 1.f, 1.f);
+      float ctr = 1.f, snear = 0.f;
+      for (int k = 0;; ++k) {
+        float tc;
+        const int cs = next_crossing(sc, r, snear, o.w, &tc, p.err);
+        const float sfar = cs >= 0 ? tc : o.w;
+        if (mt.cur >= 0) {
+          const float3 e = exp_neg(take(sc.media[mt.cur].sigma_ext, l), sfar - snear);
+          T = mul(T, e);
+          ctr *= mean3(e);
+        }
+        if (cs < 0) break;
+        if (k >= kMaxCrossings) {
+          atomicOr(p.err, ERR_CROSSINGS);
+          T = f3(0.f, 0.f, 0.f);
+          break;
+        }
+        float3 ng;
+        int mat;
+        crossing_info(sc, cs, &ng, &mat);
+        going_through(sc, mt, xyz(d), ng, mat);
+        snear = sfar;
+      }
+      const float2 mi = p.sh_mis[slot];
+      const float mis = mi.x < 0.f ? 1.f : power_heuristic(mi.x, mi.y * ctr);
+      c = mul(c, T) * mis;
+    }
     if (target < 0) {
       const float4 a = p.accum[slot];
       p.accum[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, 0.f);
     } else {
       const Lambda l = unpack_lambda(p.meta[slot].y);
-      const float3 rgb = selection_to_rgb(xyz(c), l);
+      const float3 rgb = selection_to_rgb(c, l);
       atomicAdd(&fb.light[3 * target], rgb.x);
       atomicAdd(&fb.light[3 * target + 1], rgb.y);
       atomicAdd(&fb.light[3 * target + 2], rgb.z);
@@ -616,6 +828,36 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
     atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
     atomicAdd(&counters[1], (unsigned long long)cnt.tris);
   }
+}
+
+// MediumTracker::initializePosition (rendering_util.cxx:13-38): walks a ray from outside
+// the scene bounds (+x side) to `pos` through every medium boundary, then every surface,
+// updating the tracker at each crossing.  One thread.
+__global__ void k_init_tracker(DevScene sc, float3 pos, float3 lo, float3 hi, uint2* out, unsigned int* err) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  MTracker mt{0xffffffffu, -1};
+  const bool inside = pos.x >= lo.x && pos.x <= hi.x && pos.y >= lo.y && pos.y <= hi.y && pos.z >= lo.z &&
+                      pos.z <= hi.z;
+  if (inside) {
+    const float go = 2.f * fmaxf(hi.x - lo.x, fmaxf(hi.y - lo.y, hi.z - lo.z));
+    const float3 dir = f3(-1.f, 0.f, 0.f);
+    const RayPre r = prepare_ray(f3(pos.x + go, pos.y, pos.z), dir);
+    for (int pass = 0; pass < 2; ++pass) {
+      const BvhRef bvh = pass == 0 ? volume_bvh(sc) : surface_bvh(sc);
+      float t = 0.f;
+      for (int k = 0; k < kMaxCrossings; ++k) {
+        float tc;
+        const int slot = next_hit(bvh, r, t, go, &tc, err);
+        if (slot < 0) break;
+        const float4 a = __ldg(&bvh.tris[3 * slot]);
+        const float4 b = __ldg(&bvh.tris[3 * slot + 1]);
+        const float4 c = __ldg(&bvh.tris[3 * slot + 2]);
+        going_through(sc, mt, dir, cross3(xyz(b) - xyz(a), xyz(c) - xyz(a)), __float_as_int(b.w));
+        t = tc;
+      }
+    }
+  }
+  out[0] = store_tracker(mt);
 }
 
 __global__ void __launch_bounds__(256) k_flush(PathState p, Framebuffer fb, int bounce) {
@@ -742,7 +984,7 @@ static int trace_grid() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false>, kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false>, kBlock, 0);
     g = sms * (b0 < b1 ? b0 : b1);
     if (g < 1) g = 1;
   }
@@ -751,7 +993,8 @@ static int trace_grid() {
 
 void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
                      cudaStream_t st) {
-  k_generate<<<grid, kBlock, 0, st>>>(s, p, fb, w);
+  if (s.num_media > 0) k_generate<true><<<grid, kBlock, 0, st>>>(s, p, fb, w);
+  else k_generate<false><<<grid, kBlock, 0, st>>>(s, p, fb, w);
 }
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
                    cudaStream_t st) {
@@ -760,13 +1003,26 @@ void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count
   else k_extend<false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
-  k_shade<<<grid, kBlock, 0, st>>>(s, p, bounce);
+  if (s.num_media > 0) k_shade<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
+  else k_shade<false><<<grid, kBlock, 0, st>>>(s, p, bounce);
 }
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
   grid = trace_grid();
-  if (count) k_shadow<true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-  else k_shadow<false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+  if (s.num_media > 0) {
+    if (count) k_shadow<true, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    else k_shadow<true, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+  } else {
+    if (count) k_shadow<false, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    else k_shadow<false, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+  }
+}
+void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
+  k_track<<<grid, kBlock, 0, st>>>(s, p, bounce);
+}
+void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_hi, uint2* out, unsigned int* err,
+                         cudaStream_t st) {
+  k_init_tracker<<<1, 32, 0, st>>>(s, pos, bb_lo, bb_hi, out, err);
 }
 void launch_flush(const PathState& p, const Framebuffer& fb, int bounce, int grid, cudaStream_t st) {
   k_flush<<<grid, kBlock, 0, st>>>(p, fb, bounce);
@@ -801,7 +1057,7 @@ void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, c
 }
 int kernel_blocks_per_sm() {
   int b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade, kBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false>, kBlock, 0);
   return b < 1 ? 1 : b;
 }
 

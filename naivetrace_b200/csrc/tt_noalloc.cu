@@ -11,7 +11,7 @@
 // Limits and sharing:
 //  - at most kNoAllocMaxPaths = 65,536 camera samples (spp x pixels) per call, and
 //    max_ray_depth <= kNoAllocMaxDepth; larger requests return TT_ERR_CAPACITY;
-//  - the scratch array (about 11.6 MB) is part of the library image, so every GPU that
+//  - the scratch array (about 14.2 MB) is part of the library image, so every GPU that
 //    loads the library holds it until the process exits;
 //  - all calls on a device share the one array: calls that overlap on the GPU (different
 //    streams or host threads without ordering) race and corrupt each other;
@@ -36,12 +36,14 @@ constexpr int kNoAllocMaxPaths = 1 << 16;
 constexpr int kNoAllocMaxDepth = 1000;
 constexpr int kNoAllocMaxDevices = 64;
 
-// Per-path bytes: 8 float4 + 1 uint4 + 2 u64 + 4 int queues = 176 B; each of the 17
-// arrays is padded to a 256-byte boundary.
-constexpr size_t kPathBytes = 8 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(unsigned long long) + 4 * sizeof(int);
+// Per-path bytes: 9 float4 + 1 uint4 + 2 u64 + 2 uint2 + 1 float2 + 4 int queues = 216 B
+// (the medium-tracking arrays are carved for every scene); each of the 21 arrays is padded
+// to a 256-byte boundary.
+constexpr size_t kPathBytes = 9 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(unsigned long long) +
+                              2 * sizeof(uint2) + sizeof(float2) + 4 * sizeof(int);
 constexpr size_t kCounterBytes = (size_t)kCountersPerBounce * (kNoAllocMaxDepth + 3) * sizeof(int);
 constexpr size_t kErrBytes = 256;
-constexpr size_t kPadBytes = 17 * 256;
+constexpr size_t kPadBytes = 21 * 256;
 constexpr size_t kNoAllocScratchBytes = kNoAllocMaxPaths * kPathBytes + kCounterBytes + kErrBytes + kPadBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
@@ -88,6 +90,10 @@ PathState carve(unsigned char* base, int cap) {
   p.ext_q[1] = (int*)take(n * sizeof(int));
   p.sh_q = (int*)take(n * sizeof(int));
   p.done_q = (int*)take(n * sizeof(int));
+  p.track = (uint2*)take(n * sizeof(uint2));
+  p.vol = (float4*)take(n * sizeof(float4));
+  p.sh_track = (uint2*)take(n * sizeof(uint2));
+  p.sh_mis = (float2*)take(n * sizeof(float2));
   p.counters = (int*)take(kCounterBytes);
   p.err = (unsigned int*)take(kErrBytes);
   return p;
@@ -158,6 +164,7 @@ extern "C" tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t s
     launch_shadow(scene, p, fb, b, false, nullptr, grid, st);
     launch_flush(p, fb, b, grid, st);
     launch_extend(scene, p, b, false, nullptr, grid, st);
+    if (scene.num_media > 0) launch_track(scene, p, b, grid, st);
     launch_shade(scene, p, b, grid, st);
   }
   launch_shadow(scene, p, fb, depth, false, nullptr, grid, st);

@@ -140,6 +140,29 @@ def cornell_box_medium(xres=256, yres=256) -> Scene:
     return s
 
 
+def cornell_box_media_mix(xres=64, yres=64) -> Scene:
+    """The Cornell box and its camera inside a thin fog (sigma_s 0.1, sigma_a 0.02,
+    isotropic, priority 1, box from (-0.2, -0.2, -1.6) to (1.2, 1.2, 1.2)), with a glass
+    sphere of radius 0.15 at (0.65, 0.5, 0.35) filled with a dense Rayleigh medium
+    (sigma_s 3.0, sigma_a 0.5, priority 3: the glass surface itself changes the medium), and
+    a purely absorbing chromatic box (sigma_a 4.0 in the long-wavelength half, 0.5 below,
+    priority 2) of half size 0.1 at (0.5, 0.75, 0.6)."""
+    s = cornell_box(xres, yres)
+    s.name = "cornell_box_media_mix"
+    fog = s.add_medium(MediumSpec(sigma_s=np.full(36, 0.1), sigma_a=np.full(36, 0.02), priority=1))
+    dense = s.add_medium(MediumSpec(sigma_s=np.full(36, 3.0), sigma_a=np.full(36, 0.5),
+                                    phase=abi.PHASE_RAYLEIGH, priority=3))
+    absorb = s.add_medium(MediumSpec(sigma_s=np.zeros(36), sigma_a=band_spectrum(4.0, 0.5, 18, 35), priority=2))
+    lo, hi = np.array([-0.2, -0.2, -1.6]), np.array([1.2, 1.2, 1.2])
+    s.add_mesh(*centered_box((lo + hi) / 2, (hi - lo) / 2), s.add_material(volume_boundary(fog)))
+    g = glass(1.5)
+    g.medium_inside = dense
+    v, t = icosphere(3)
+    s.add_mesh(v * 0.15 + np.array([0.65, 0.5, 0.35]), t, s.add_material(g))
+    s.add_mesh(*centered_box((0.5, 0.75, 0.6), 0.1), s.add_material(volume_boundary(absorb)))
+    return s
+
+
 # --------------------------------------------------------------------------------------
 def icosphere(level: int):
     """Unit icosphere: 20 * 4**level triangles, outward winding, shared vertices."""

@@ -31,9 +31,10 @@ def noalloc_pass(g, spp, seed, pixel_begin, pixel_end, sample_offset=0):
     return st, acc.cpu().numpy().astype(np.float64), light.cpu().numpy().astype(np.float64)
 
 
-@pytest.mark.parametrize("name,spp,depth", [("cornell_box", 4, 10), ("terrain_spheres_small", 8, 16)])
+@pytest.mark.parametrize("name,spp,depth", [("cornell_box", 4, 10), ("terrain_spheres_small", 8, 16),
+                                            ("cornell_box_media_mix", 4, 10)])
 def test_noalloc_matches_render_pass(gpu_lib, name, spp, depth):
-    scene = scenes.cornell_box(32, 32) if name == "cornell_box" else scenes.terrain_spheres_small(64, 36)
+    scene = scenes.terrain_spheres_small(64, 36) if name == "terrain_spheres_small" else getattr(scenes, name)(32, 32)
     params = make_params(max_ray_depth=depth)
     ref = GpuContext(scene, params)
     ref.render(spp, seed=7)
