@@ -76,13 +76,16 @@ def test_media_sample_modes_agree(gpu_lib):
 
 
 def test_media_change_the_image(gpu_lib):
-    """The medium darkens the walls seen through it relative to the empty box, and the
-    pass reports the medium-tracking launches."""
+    """Seen through the medium the area light is attenuated (its pixels lose most of their
+    radiance), and the pass runs the medium-tracking launches."""
     a = GpuContext(scenes.cornell_box(32, 32), make_params(max_ray_depth=10))
     a.render(256, seed=3)
     b = GpuContext(scenes.cornell_box_medium(32, 32), make_params(max_ray_depth=10))
     b.render(256, seed=3)
-    ia, ib = a.framebuffer().reshape(32, 32, 3), b.framebuffer().reshape(32, 32, 3)
-    # The back wall region (centre of the image, below the light) loses energy.
-    assert ib[12:20, 12:20].mean() < 0.9 * ia[12:20, 12:20].mean()
+    ia, ib = a.framebuffer().reshape(-1, 3).sum(1), b.framebuffer().reshape(-1, 3).sum(1)
+    light = ia > 20 * np.median(ia)
+    assert light.sum() > 0
+    # Extinction 0.6 .. 2.1 per unit over about 0.7 units of medium (the camera is outside
+    # the medium box), partly made up by light scattered into the view ray.
+    assert ib[light].mean() < 0.85 * ia[light].mean()
     assert b.stats()["kernel_launches"] > a.stats()["kernel_launches"]
