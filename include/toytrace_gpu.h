@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 2
+#define TT_ABI_VERSION 3
 
 typedef int32_t tt_status;
 enum {
@@ -69,11 +69,25 @@ typedef struct tt_material {
 
 /* Phase functions (src/phasefunctions.cxx). */
 enum { TT_PHASE_UNIFORM = 0, TT_PHASE_RAYLEIGH = 1, TT_PHASE_HENYEY_GREENSTEIN = 2 };
-enum { TT_MEDIUM_HOMOGENEOUS = 0 };
+enum {
+  TT_MEDIUM_HOMOGENEOUS = 0,       /* HomogeneousMedium, shader.cxx:1234-1316 */
+  TT_MEDIUM_ATMOSPHERE = 1         /* Atmosphere::Tabulated, atmosphere.cxx:18-126, 234-348 */
+};
 
-/* HomogeneousMedium (shader.cxx:1234-1316): coefficients per bin, per unit length.
- * Priority decides which of overlapping media is current (MediumTracker,
- * rendering_util.hxx:18-126); empty space has priority -1. */
+/* A participating medium.  Priority decides which of overlapping media is current
+ * (MediumTracker, rendering_util.hxx:18-126); empty space has priority -1.
+ *
+ * TT_MEDIUM_HOMOGENEOUS: constant sigma_s, sigma_a per bin and per unit length, with the
+ * phase function `phase` (phase_g for Henyey-Greenstein).
+ *
+ * TT_MEDIUM_ATMOSPHERE: a spherical planet's atmosphere with collision coefficients
+ * tabulated over altitude (TabulatedConstituents + SphereGeometry, atmosphere.hxx:79-123),
+ * lengths in km.  Altitude = distance to planet_center - planet_radius.  Row i of the
+ * tables holds the coefficients per km at altitude table_h0 + i * table_dh, linearly
+ * interpolated in between, clamped to row 0 below and zero above the last row.  Molecules
+ * scatter with the Rayleigh phase function, aerosols with Henyey-Greenstein(phase_g)
+ * (the reference hard-codes g = 0.7, atmosphere.cxx:26).  sigma_s, sigma_a and phase are
+ * unused.  The tables are copied by tt_create. */
 typedef struct tt_medium {
   int32_t kind;                    /* TT_MEDIUM_* */
   int32_t priority;
@@ -81,6 +95,14 @@ typedef struct tt_medium {
   float sigma_a[TT_NBINS];
   int32_t phase;                   /* TT_PHASE_* */
   float phase_g;                   /* Henyey-Greenstein asymmetry */
+  float planet_center[3];          /* atmosphere only, from here on */
+  float planet_radius;
+  int32_t table_size;              /* altitude rows, >= 2 */
+  float table_h0;
+  float table_dh;
+  const float* sigma_t;            /* table_size x TT_NBINS, total extinction */
+  const float* sigma_s_molecules;  /* table_size x TT_NBINS */
+  const float* sigma_s_aerosols;   /* table_size x TT_NBINS */
 } tt_medium;
 
 /* Environmental lights: the members of TotalEnvironmentalRadianceField (light.hxx:292-304). */
@@ -123,9 +145,12 @@ typedef struct tt_camera {
   int32_t yres;
 } tt_camera;
 
-/* Flat scene.  Triangles are numbered in the order given; tt_intersect_batch reports
- * these global indices.  normals may be NULL (flat shading: smooth normal = geometry
- * normal, like Mesh::MakeFlatNormals, primitive.cxx:18-46). */
+/* Flat scene.  Triangles are numbered in the order given, spheres after them (sphere i
+ * is primitive num_triangles + i); tt_intersect_batch reports these global indices.
+ * normals may be NULL (flat shading: smooth normal = geometry normal, like
+ * Mesh::MakeFlatNormals, primitive.cxx:18-46).  Spheres are the reference's analytic
+ * Spheres geometry (primitive.hxx:94-136): surfaces, area lights or medium boundaries
+ * depending on their material, with outward normals. */
 typedef struct tt_scene_desc {
   uint32_t num_vertices;
   const float* vertices;        /* num_vertices * 3 */
@@ -141,6 +166,9 @@ typedef struct tt_scene_desc {
   const tt_point_light* point_lights;
   uint32_t num_media;
   const tt_medium* media;
+  uint32_t num_spheres;
+  const float* spheres;                /* num_spheres * 4: centre x, y, z, radius */
+  const uint32_t* sphere_material_ids; /* num_spheres */
   tt_camera camera;
 } tt_scene_desc;
 

@@ -65,6 +65,7 @@ PHASE_UNIFORM = 0
 PHASE_RAYLEIGH = 1
 PHASE_HENYEY_GREENSTEIN = 2
 MEDIUM_HOMOGENEOUS = 0
+MEDIUM_ATMOSPHERE = 1
 
 
 class Medium(C.Structure):
@@ -75,6 +76,14 @@ class Medium(C.Structure):
         ("sigma_a", C.c_float * NBINS),
         ("phase", C.c_int32),
         ("phase_g", C.c_float),
+        ("planet_center", C.c_float * 3),
+        ("planet_radius", C.c_float),
+        ("table_size", C.c_int32),
+        ("table_h0", C.c_float),
+        ("table_dh", C.c_float),
+        ("sigma_t", C.POINTER(C.c_float)),
+        ("sigma_s_molecules", C.POINTER(C.c_float)),
+        ("sigma_s_aerosols", C.POINTER(C.c_float)),
     ]
 
 
@@ -123,6 +132,9 @@ class SceneDesc(C.Structure):
         ("point_lights", C.POINTER(PointLight)),
         ("num_media", C.c_uint32),
         ("media", C.POINTER(Medium)),
+        ("num_spheres", C.c_uint32),
+        ("spheres", C.POINTER(C.c_float)),
+        ("sphere_material_ids", C.POINTER(C.c_uint32)),
         ("camera", Camera),
     ]
 

@@ -166,6 +166,7 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
       return fail(nullptr, TT_ERR_INVALID, "medium index out of range in material " + std::to_string(i));
   }
   if (d->num_media > 0 && !d->media) return fail(nullptr, TT_ERR_INVALID, "media missing");
+  if (d->num_spheres > 0) return fail(nullptr, TT_ERR_INVALID, "spheres are not supported by this build");
   if (d->num_media > (uint32_t)kMaxMedia) return fail(nullptr, TT_ERR_CAPACITY, "more than 254 media");
   for (uint32_t i = 0; i < d->num_media; ++i) {
     const tt_medium& m = d->media[i];

@@ -59,7 +59,7 @@ class MediumSpec:
     phase_g: float = 0.0
     priority: int = 1
 
-    def to_c(self) -> abi.Medium:
+    def to_c(self, keep: list) -> abi.Medium:
         m = abi.Medium()
         m.kind = abi.MEDIUM_HOMOGENEOUS
         m.priority = int(self.priority)
@@ -67,6 +67,46 @@ class MediumSpec:
         m.sigma_a[:] = [float(x) for x in as_spectrum(self.sigma_a)]
         m.phase = int(self.phase)
         m.phase_g = float(self.phase_g)
+        return m
+
+
+@dataclass
+class AtmosphereSpec:
+    """Atmosphere::Tabulated (atmosphere.cxx:234-348 with SphereGeometry,
+    atmosphere.hxx:95-123), lengths in km: rows of sigma_t, sigma_s of molecules (Rayleigh
+    phase) and of aerosols (Henyey-Greenstein g) per km at altitudes h0 + i * dh."""
+
+    planet_center: tuple
+    planet_radius: float
+    h0: float
+    dh: float
+    sigma_t: np.ndarray            # (n, 36)
+    sigma_s_molecules: np.ndarray  # (n, 36)
+    sigma_s_aerosols: np.ndarray   # (n, 36)
+    g: float = 0.7
+    priority: int = 1
+
+    @property
+    def top_altitude(self) -> float:
+        return self.h0 + self.dh * (len(self.sigma_t) - 1)
+
+    def to_c(self, keep: list) -> abi.Medium:
+        m = abi.Medium()
+        m.kind = abi.MEDIUM_ATMOSPHERE
+        m.priority = int(self.priority)
+        m.phase = abi.PHASE_HENYEY_GREENSTEIN
+        m.phase_g = float(self.g)
+        m.planet_center[:] = [float(x) for x in self.planet_center]
+        m.planet_radius = float(self.planet_radius)
+        tabs = [np.ascontiguousarray(a, dtype=np.float32).reshape(-1, NBINS)
+                for a in (self.sigma_t, self.sigma_s_molecules, self.sigma_s_aerosols)]
+        if not (len(tabs[0]) == len(tabs[1]) == len(tabs[2]) >= 2):
+            raise ValueError("atmosphere tables need the same number (>= 2) of altitude rows")
+        keep.extend(tabs)
+        m.table_size = len(tabs[0])
+        m.table_h0 = float(self.h0)
+        m.table_dh = float(self.dh)
+        m.sigma_t, m.sigma_s_molecules, m.sigma_s_aerosols = [t.ctypes.data_as(C.POINTER(C.c_float)) for t in tabs]
         return m
 
 
@@ -153,7 +193,8 @@ class Scene:
         self.materials: List[MaterialSpec] = []
         self.env_lights: List[EnvLightSpec] = []
         self.point_lights: List[tuple] = []
-        self.media: List[MediumSpec] = []
+        self.media: list = []  # MediumSpec or AtmosphereSpec
+        self._spheres: List[tuple] = []  # (cx, cy, cz, r, material)
         self.camera = CameraSpec()
         self.name = "scene"
         self._flat = None
@@ -164,9 +205,25 @@ class Scene:
         self._flat = None
         return len(self.materials) - 1
 
-    def add_medium(self, m: MediumSpec) -> int:
+    def add_medium(self, m) -> int:
         self.media.append(m)
         return len(self.media) - 1
+
+    def add_sphere(self, center, radius: float, material: int) -> int:
+        """Analytic sphere (Spheres, primitive.hxx:94-136); returns its global primitive id
+        (spheres are numbered after all triangles)."""
+        self._spheres.append((float(center[0]), float(center[1]), float(center[2]), float(radius), int(material)))
+        return len(self._spheres) - 1
+
+    @property
+    def num_spheres(self) -> int:
+        return len(self._spheres)
+
+    def sphere_arrays(self):
+        if not self._spheres:
+            return np.zeros((0, 4), np.float32), np.zeros(0, np.uint32)
+        a = np.array(self._spheres, dtype=np.float64)
+        return np.ascontiguousarray(a[:, :4], dtype=np.float32), np.ascontiguousarray(a[:, 4], dtype=np.uint32)
 
     def add_mesh(self, vertices, triangles, material: int, normals=None) -> None:
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
@@ -207,8 +264,14 @@ class Scene:
         return int(sum(len(t) for t in self._tris))
 
     def bounding_box(self):
-        v = self.arrays()[0]
-        return v.min(axis=0).astype(np.float64), v.max(axis=0).astype(np.float64)
+        v = self.arrays()[0].astype(np.float64)
+        sph, _ = self.sphere_arrays()
+        pts = [v]
+        if len(sph):
+            c, r = sph[:, :3].astype(np.float64), sph[:, 3:4].astype(np.float64)
+            pts += [c - r, c + r]
+        p = np.concatenate(pts)
+        return p.min(axis=0), p.max(axis=0)
 
     def to_desc(self):
         """Returns (tt_scene_desc, keepalive).  keepalive owns every array the descriptor
@@ -254,10 +317,15 @@ class Scene:
         keep.append(pt_arr)
         d.num_point_lights = len(pts)
         d.point_lights = C.cast(pt_arr, C.POINTER(abi.PointLight))
-        med_arr = (abi.Medium * max(1, len(self.media)))(*[m.to_c() for m in self.media])
+        med_arr = (abi.Medium * max(1, len(self.media)))(*[m.to_c(keep) for m in self.media])
         keep.append(med_arr)
         d.num_media = len(self.media)
         d.media = C.cast(med_arr, C.POINTER(abi.Medium))
+        sph, smat = self.sphere_arrays()
+        keep += [sph, smat]
+        d.num_spheres = len(sph)
+        d.spheres = sph.ctypes.data_as(C.POINTER(C.c_float)) if len(sph) else None
+        d.sphere_material_ids = smat.ctypes.data_as(C.POINTER(C.c_uint32)) if len(sph) else None
         cam = self.camera
         d.camera.kind = cam.kind
         d.camera.pos[:] = [float(x) for x in cam.pos]

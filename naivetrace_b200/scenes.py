@@ -16,8 +16,8 @@ import math
 import numpy as np
 
 from . import abi
-from .scene import (CameraSpec, MediumSpec, Scene, area_light, diffuse, env_map, glass, microfacet,
-                    mirror, sun_light, volume_boundary)
+from .scene import (AtmosphereSpec, CameraSpec, MediumSpec, Scene, area_light, diffuse, env_map, glass,
+                    microfacet, mirror, sun_light, volume_boundary)
 from .spectral import band_spectrum, rgb_to_spectrum
 
 
@@ -296,3 +296,77 @@ def terrain_spheres(xres=1920, yres=1080, terrain_n=1024, sphere_level=5, num_sp
 def terrain_spheres_small(xres=96, yres=54) -> Scene:
     """Scaled-down terrain scene (same generator) for parity tests."""
     return terrain_spheres(xres=xres, yres=yres, terrain_n=64, sphere_level=2, num_spheres=8, env_w=128, env_h=64)
+
+
+# --------------------------------------------------------------------------------------
+# Spheres and planetary atmospheres.
+WAVELENGTHS_NM = 375.0 + 10.0 * np.arange(36)
+
+
+def earth_atmosphere_table(h0=-1.0, dh=0.5, rows=403, rayleigh_680=5.8e-3, rayleigh_height=8.0, mie=2.0e-2,
+                           mie_height=1.2, ozone_peak=2.5e-3, ozone_altitude=25.0, ozone_width=8.0):
+    """Collision coefficients per km at altitudes h0 + i * dh (the row layout of the
+    reference's earth_atmosphere_collision_coefficients.json): Rayleigh scattering
+    5.8e-6 /m at 680 nm scaled as lambda^-4 with an 8 km scale height; Mie scattering
+    2e-5 /m with a 1.2 km scale height; ozone absorption with a Gaussian altitude profile
+    peaking at 25 km and a Gaussian Chappuis band centred at 600 nm.  Returns
+    (sigma_t, sigma_s_molecules, sigma_s_aerosols), each (rows, 36)."""
+    h = h0 + dh * np.arange(rows)
+    lam = WAVELENGTHS_NM
+    mol = rayleigh_680 * (680.0 / lam)[None, :] ** 4 * np.exp(-h / rayleigh_height)[:, None]
+    aer = mie * np.exp(-h / mie_height)[:, None] * np.ones((1, 36))
+    ozone = ozone_peak * np.exp(-(((h - ozone_altitude) / ozone_width) ** 2))[:, None] * \
+        np.exp(-(((lam - 600.0) / 60.0) ** 2))[None, :]
+    return mol + aer + ozone, mol, aer
+
+
+def simple_atmosphere_table(h0=-1.0, dh=0.05, rows=4021):
+    """The reference's ExponentialConstituentDistribution (atmosphere.cxx:127-188)
+    tabulated: molecular Rayleigh scattering from the refractive index of air
+    (n = 1.00028, 1.225 kg/m^3 of 29 g/mol) with an 8 km scale height; aerosols with
+    sigma_s 20e-3 /km and sigma_a 2.22e-3 /km at sea level and a 1.2 km scale height."""
+    h = h0 + dh * np.arange(rows)
+    n_air = 1.225 * 6.022e23 / 29e-3
+    prefactor = 8.0 * math.pi ** 3 / 3.0 * (1.00028 ** 2 - 1.0) ** 2 / n_air * 1e27 * 1e12
+    mol = (prefactor / WAVELENGTHS_NM ** 4)[None, :] * np.exp(-h / 8.0)[:, None]
+    aer_s = 20e-3 * np.exp(-h / 1.2)[:, None] * np.ones((1, 36))
+    aer_a = 2.22e-3 * np.exp(-h / 1.2)[:, None] * np.ones((1, 36))
+    return mol + aer_s + aer_a, mol, aer_s
+
+
+def planet_atmosphere(xres=64, yres=64, radius=6371.0, camera_height=0.002, sun_elevation_deg=10.0, g=0.76,
+                      table=None, h0=-1.0, dh=0.5, camera_kind=abi.CAMERA_FISHEYE, ground_albedo=0.3,
+                      sun_power=20.0) -> Scene:
+    """A spherical planet (radius in km) under a tabulated atmosphere, lit by the sun at
+    `sun_elevation_deg` above the horizon of the camera, which stands `camera_height` km
+    above the ground looking up (fisheye by default).  The ground is an analytic sphere
+    with a Lambert albedo; the atmosphere's boundary is a concentric sphere at the top of
+    the table."""
+    s = Scene()
+    s.name = "planet_atmosphere"
+    tab = earth_atmosphere_table(h0=h0, dh=dh) if table is None else table
+    atm = AtmosphereSpec(planet_center=(0.0, 0.0, 0.0), planet_radius=radius, h0=h0, dh=dh, sigma_t=tab[0],
+                         sigma_s_molecules=tab[1], sigma_s_aerosols=tab[2], g=g, priority=1)
+    mid = s.add_medium(atm)
+    s.add_sphere((0.0, 0.0, 0.0), radius, s.add_material(diffuse(ground_albedo)))
+    s.add_sphere((0.0, 0.0, 0.0), radius + atm.top_altitude, s.add_material(volume_boundary(mid)))
+    e = math.radians(sun_elevation_deg)
+    s.env_lights.append(sun_light(sun_power, (-math.cos(e), -math.sin(e), 0.0), 0.265))
+    s.camera = CameraSpec(kind=camera_kind, pos=(0.0, radius + camera_height, 0.0), dir=(0.0, 1.0, 0.0),
+                          up=(0.0, 0.0, 1.0), fov_deg=90.0, xres=xres, yres=yres)
+    return s
+
+
+def spheres_box(xres=64, yres=64) -> Scene:
+    """The Cornell box with analytic spheres: a mirror sphere, a glass sphere filled with
+    a homogeneous medium, a diffuse sphere, and a small emissive sphere as a second light."""
+    s = cornell_box(xres, yres)
+    s.name = "spheres_box"
+    s.add_sphere((0.25, 0.15, 0.3), 0.15, s.add_material(mirror(0.9)))
+    g = glass(1.5)
+    g.medium_inside = s.add_medium(MediumSpec(sigma_s=np.full(36, 2.0), sigma_a=band_spectrum(1.5, 0.2, 0, 17),
+                                              phase=abi.PHASE_HENYEY_GREENSTEIN, phase_g=0.5, priority=1))
+    s.add_sphere((0.72, 0.45, 0.35), 0.12, s.add_material(g))
+    s.add_sphere((0.55, 0.1, 0.75), 0.1, s.add_material(diffuse(rgb_to_spectrum((0.2, 0.4, 0.8)))))
+    s.add_sphere((0.2, 0.8, 0.5), 0.04, s.add_material(area_light(30.0)))
+    return s

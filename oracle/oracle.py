@@ -59,7 +59,9 @@ def load():
         "or_eval_env": ([vp, d, i32, d, d], C.c_int),
         "or_scene_info": ([vp, d, i32], C.c_int),
         "or_medium_walk": ([vp, d, d, C.c_double, C.c_int, i32, d, i32], C.c_int),
-        "or_transmittance": ([vp, d, d, C.c_double, i32, d, d], C.c_int),
+        "or_transmittance": ([vp, d, d, C.c_double, i32, C.c_uint64, d, d], C.c_int),
+        "or_atmosphere_query": ([vp, C.c_int, d, d, d, C.c_double, i32, d], C.c_int),
+        "or_medium_phase_sample": ([vp, C.c_int, d, d, i32, C.c_int, C.c_uint64, d, d, d], C.c_int),
         "or_track": ([vp, d, d, i32, C.c_int, C.c_uint64, d], C.c_int),
         "or_phase_sample": ([C.c_int, C.c_double, d, C.c_int, C.c_uint64, d, d, d], C.c_int),
     }
@@ -171,14 +173,27 @@ class OracleScene:
         n = self.lib.or_medium_walk(self.h, _dp(o), _dp(dd), tfar, max_crossings, _ip(media), _dp(ts), C.byref(init))
         return init.value, list(zip(ts[:n].tolist(), media[:n].tolist()))
 
-    def transmittance(self, org, dir, length, lambda_idx):
+    def transmittance(self, org, dir, length, lambda_idx, seed=1):
+        """TransmittanceEstimate from org over length: (T per wavelength, (fwd, bwd, tr))."""
         o = np.ascontiguousarray(org, dtype=np.float64)
         dd = np.ascontiguousarray(dir, dtype=np.float64)
         li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
         T = np.zeros(3)
         coeff = np.zeros(3)
-        self.lib.or_transmittance(self.h, _dp(o), _dp(dd), length, _ip(li), _dp(T), _dp(coeff))
+        self.lib.or_transmittance(self.h, _dp(o), _dp(dd), length, _ip(li), seed, _dp(T), _dp(coeff))
         return T, coeff
+
+    def atmosphere_query(self, medium, pos, org, dir, length, lambda_idx):
+        """Dict of the atmosphere model's quantities (see or_atmosphere_query)."""
+        out = np.zeros(18)
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (pos, org, dir)]
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        rc = self.lib.or_atmosphere_query(self.h, medium, _dp(args[0]), _dp(args[1]), _dp(args[2]), length, _ip(li),
+                                          _dp(out))
+        if rc != 0:
+            raise ValueError("not an atmosphere medium")
+        return dict(altitude=out[0], lowest=out[1:4], sigma_s=out[4:7], sigma_t=out[7:10], sigma_s_mol=out[10:13],
+                    sigma_s_aer=out[13:16], segment_majorant=out[16], majorant=out[17])
 
     def track(self, org, dir, lambda_idx, n, seed=1):
         """n samples of the next interaction: columns interacted, distance, weight[3],
@@ -189,6 +204,16 @@ class OracleScene:
         out = np.zeros((n, 11))
         self.lib.or_track(self.h, _dp(o), _dp(dd), _ip(li), n, seed, _dp(out))
         return out
+
+    def medium_phase_sample(self, medium, pos, wi, lambda_idx, n, seed=1):
+        """(dirs, values per wavelength, pdf) of n phase samples at a volume vertex at pos."""
+        p = np.ascontiguousarray(pos, dtype=np.float64)
+        w = np.ascontiguousarray(wi, dtype=np.float64)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        dirs, val, pdf = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+        self.lib.or_medium_phase_sample(self.h, medium, _dp(p), _dp(w), _ip(li), n, seed, _dp(dirs), _dp(val),
+                                        _dp(pdf))
+        return dirs, val, pdf
 
     def info(self):
         bb = np.zeros(6)

@@ -67,6 +67,7 @@ struct S3 {
   double operator[](int i) const { return v[i]; }
   bool IsZero() const { return v[0] == 0 && v[1] == 0 && v[2] == 0; }
   double Max() const { return std::max(v[0], std::max(v[1], v[2])); }
+  double Sum() const { return v[0] + v[1] + v[2]; }
 };
 inline S3 operator*(S3 a, S3 b) { return {a[0] * b[0], a[1] * b[1], a[2] * b[2]}; }
 inline S3 operator*(double s, S3 a) { return {s * a[0], s * a[1], s * a[2]}; }
@@ -402,22 +403,34 @@ struct BNode {
 };
 
 struct MediumDesc {
+  int kind = TT_MEDIUM_HOMOGENEOUS;
   int priority;
   double sigma_s[NBINS], sigma_a[NBINS], sigma_ext[NBINS];
   bool is_scattering;
   int phase;
   double g;
+  // Atmosphere (TabulatedConstituents + SphereGeometry, atmosphere.hxx:79-123), km units.
+  V3 center;
+  double radius = 0;
+  int n = 0;                                  // altitude rows
+  double h0 = 0, dh = 1, inv_dh = 1;
+  std::vector<double> sig_t, sig_mol, sig_aer;  // n x NBINS
+  std::vector<double> maj;                    // per-row majorant, non-increasing with altitude
 };
 
 struct Scene {
+  // Primitives: triangles 0 .. ntri-1, then spheres (global id ntri + i).
+  uint32_t ntri = 0;
+  std::vector<V3> sph_c;           // sphere centres (from float)
+  std::vector<double> sph_r;       // sphere radii (from float)
   std::vector<V3> tv0, tv1, tv2;   // triangle vertices as double (from float)
   std::vector<F3> vert, nrm;
-  std::vector<uint32_t> idx, mat_of_tri;
+  std::vector<uint32_t> idx, mat_of_tri;  // mat_of_tri: per primitive (triangles, then spheres)
   bool has_normals = false;
   std::vector<Material> materials;
   std::vector<EnvLight> env;
   std::vector<tt_point_light> points;
-  std::vector<int> area_lights;    // global triangle index per area light number
+  std::vector<int> area_lights;    // global primitive id per area light number
   Camera cam;
   double bb_lo[3], bb_hi[3];
   double diag = 0, long_distance = 0;
@@ -435,7 +448,15 @@ struct Scene {
   std::vector<MediumDesc> media;
 };
 
+inline bool IsSphere(const Scene& s, int prim) { return (uint32_t)prim >= s.ntri; }
+
 inline void TriBounds(const Scene& s, int t, double lo[3], double hi[3]) {
+  if (IsSphere(s, t)) {
+    const V3 c = s.sph_c[t - s.ntri];
+    const double r = s.sph_r[t - s.ntri];
+    for (int k = 0; k < 3; ++k) { lo[k] = c[k] - r; hi[k] = c[k] + r; }
+    return;
+  }
   for (int k = 0; k < 3; ++k) {
     lo[k] = std::min(s.tv0[t][k], std::min(s.tv1[t][k], s.tv2[t][k]));
     hi[k] = std::max(s.tv0[t][k], std::max(s.tv1[t][k], s.tv2[t][k]));
@@ -451,7 +472,8 @@ static double HalfArea(const double lo[3], const double hi[3]) {
 static void BuildBvh(const Scene& sc, Scene::TriSet& s) {
   const int n = (int)s.tris.size();
   s.order.resize(n);
-  std::vector<double> cen(3 * sc.tv0.size()), blo(3 * sc.tv0.size()), bhi(3 * sc.tv0.size());
+  const size_t np = sc.mat_of_tri.size();
+  std::vector<double> cen(3 * np), blo(3 * np), bhi(3 * np);
   for (int i = 0; i < n; ++i) {
     const int g = s.tris[i];
     s.order[i] = g;
@@ -576,6 +598,35 @@ inline bool IntersectTri(V3 org, V3 dir, V3 v0, V3 v1, V3 v2, double tnear, doub
   return true;
 }
 
+// Ray/sphere roots in double precision: t^2 |d|^2 + 2 t (v.d) + |v|^2 - r^2 = 0 with
+// v = org - centre, solved with the cancellation-free pairing q = -(b + sign(b) sqrt(D)),
+// t = q / a and c / q (PBRT's Quadratic, util.hxx:131-144).  The reference tests spheres in
+// single precision with PBRT error bounds (embreeaccelerator.cxx:307-427); double
+// precision keeps planet-sized spheres usable a few metres above the ground.
+inline bool SphereRoots(V3 org, V3 dir, V3 c, double r, double* t0, double* t1) {
+  const V3 v = org - c;
+  const double a = Dot(dir, dir), b = Dot(v, dir), cc = Dot(v, v) - r * r;
+  const double D = b * b - a * cc;
+  if (D < 0) return false;
+  const double q = -(b + std::copysign(std::sqrt(D), b));
+  if (q == 0) { *t0 = *t1 = 0; return true; }
+  *t0 = q / a;
+  *t1 = cc / q;
+  if (*t0 > *t1) std::swap(*t0, *t1);
+  return true;
+}
+
+inline bool IntersectPrim(const Scene& sc, int prim, V3 org, V3 dir, double tnear, double tfar, double* t,
+                          double* u, double* v) {
+  if (!IsSphere(sc, prim)) return IntersectTri(org, dir, sc.tv0[prim], sc.tv1[prim], sc.tv2[prim], tnear, tfar, t, u, v);
+  double t0, t1;
+  if (!SphereRoots(org, dir, sc.sph_c[prim - sc.ntri], sc.sph_r[prim - sc.ntri], &t0, &t1)) return false;
+  *u = *v = 0;
+  if (t0 > tnear && t0 <= tfar) { *t = t0; return true; }
+  if (t1 > tnear && t1 <= tfar) { *t = t1; return true; }
+  return false;
+}
+
 inline bool SlabHit(const BNode& nd, V3 org, V3 inv, double tnear, double tfar, double* tentry) {
   double t0 = tnear, t1 = tfar;
   for (int k = 0; k < 3; ++k) {
@@ -610,7 +661,7 @@ static int Trace(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, double
       for (int i = nd.start; i < nd.start + nd.count; ++i) {
         int tri = s.order[i];
         double t, u, v;
-        if (IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, best_t, &t, &u, &v)) {
+        if (IntersectPrim(sc, tri, org, dir, tnear, best_t, &t, &u, &v)) {
           best = tri; best_t = t; bu = u; bv = v;
           if (any_hit) { *t_out = t; return tri; }
         }
@@ -631,7 +682,7 @@ static int TraceBrute(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, d
   double best_t = tfar, bu = 0, bv = 0;
   for (int tri : s.tris) {
     double t, u, v;
-    if (IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, best_t, &t, &u, &v)) {
+    if (IntersectPrim(sc, tri, org, dir, tnear, best_t, &t, &u, &v)) {
       best = tri; best_t = t; bu = u; bv = v;
     }
   }
@@ -665,17 +716,31 @@ static void AllHits(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, dou
     if (nd.count > 0) {
       for (int i = nd.start; i < nd.start + nd.count; ++i) {
         const int tri = s.order[i];
-        double t, u, v;
-        if (!IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, tfar, &t, &u, &v)) continue;
-        Crossing c;
-        c.prim = tri;
-        c.material = sc.mat_of_tri[tri];
-        c.t = t;
-        const V3 ng = Cross(sc.tv1[tri] - sc.tv0[tri], sc.tv2[tri] - sc.tv0[tri]);
-        c.n = Ff(ng);
-        bool dup = false;
-        for (const auto& o : out) dup |= (o.material == c.material) & (o.t == c.t);
-        if (!dup) out.push_back(c);
+        double ts[2];
+        int nt = 0;
+        if (IsSphere(sc, tri)) {
+          // Both roots of a sphere are crossings (the intersect callback reports t0, then t1).
+          double t0, t1;
+          if (SphereRoots(org, dir, sc.sph_c[tri - sc.ntri], sc.sph_r[tri - sc.ntri], &t0, &t1)) {
+            if (t0 > tnear && t0 <= tfar) ts[nt++] = t0;
+            if (t1 > tnear && t1 <= tfar && t1 != t0) ts[nt++] = t1;
+          }
+        } else {
+          double t, u, v;
+          if (IntersectTri(org, dir, sc.tv0[tri], sc.tv1[tri], sc.tv2[tri], tnear, tfar, &t, &u, &v)) ts[nt++] = t;
+        }
+        for (int j = 0; j < nt; ++j) {
+          Crossing c;
+          c.prim = tri;
+          c.material = sc.mat_of_tri[tri];
+          c.t = ts[j];
+          const V3 ng = IsSphere(sc, tri) ? org + dir * ts[j] - sc.sph_c[tri - sc.ntri]
+                                          : Cross(sc.tv1[tri] - sc.tv0[tri], sc.tv2[tri] - sc.tv0[tri]);
+          c.n = Ff(ng);
+          bool dup = false;
+          for (const auto& o : out) dup |= (o.material == c.material) & (o.t == c.t);
+          if (!dup) out.push_back(c);
+        }
       }
     } else {
       if (sp + 2 > 128) return;
@@ -697,7 +762,7 @@ inline V3 PosBounds(V3 p0, V3 p1, V3 p2, V3 b) {
 }
 
 inline V3 SmoothNormal(const Scene& s, int prim, double w0, double w1, double w2, V3 ng) {
-  if (!s.has_normals) return ng;
+  if (!s.has_normals || IsSphere(s, prim)) return ng;
   uint32_t a = s.idx[3 * prim], b = s.idx[3 * prim + 1], c = s.idx[3 * prim + 2];
   V3 na{s.nrm[a].x, s.nrm[a].y, s.nrm[a].z}, nb{s.nrm[b].x, s.nrm[b].y, s.nrm[b].z},
       nc{s.nrm[c].x, s.nrm[c].y, s.nrm[c].z};
@@ -708,9 +773,38 @@ inline V3 GeometryNormal(const Scene& s, int prim) {
   return Normalized(Cross(s.tv1[prim] - s.tv0[prim], s.tv2[prim] - s.tv0[prim]));
 }
 
+// FillPosBoundsSphere, primitive.cxx:302-306: |pos| (as float) x Gamma<float>(5).
+inline double Gamma5() { return (5 * (double)EpsF) / (1 - 5 * (double)EpsF); }
+inline V3 SphereBounds(V3 pos) {
+  const F3 p = Ff(pos);
+  return V3{std::abs((double)p.x), std::abs((double)p.y), std::abs((double)p.z)} * Gamma5();
+}
+
+// Sphere surface point with outward normal n (Spheres::GetLocalGeometry,
+// primitive.cxx:214-223, and FirstIntersectionSphere, embreeaccelerator.cxx:247-260: the
+// position is projected onto the sphere along the normal).
+inline Surf SphereSurface(const Scene& s, int prim, V3 n) {
+  Surf si;
+  si.prim = prim;
+  si.barry = n;
+  si.pos = s.sph_c[prim - s.ntri] + n * s.sph_r[prim - s.ntri];
+  si.geometry_normal = n;
+  si.smooth_normal = n;
+  si.pos_bounds = SphereBounds(si.pos);
+  return si;
+}
+
 // EmbreeAccelerator::FirstIntersectionTriangle (embreeaccelerator.cxx:216-244) followed by
-// SurfaceInteraction::SetOrientedNormals (scene.cxx:240-245).
-inline Surf SurfaceFromHit(const Scene& s, int prim, double u, double v, V3 ray_dir) {
+// SurfaceInteraction::SetOrientedNormals (scene.cxx:240-245).  Spheres take the hit
+// distance t along (org, ray_dir).
+inline Surf SurfaceFromHit(const Scene& s, int prim, double u, double v, V3 org, V3 ray_dir, double t) {
+  if (IsSphere(s, prim)) {
+    Surf si = SphereSurface(s, prim, Normalized(org + ray_dir * t - s.sph_c[prim - s.ntri]));
+    const double sign = -Sign(Dot(ray_dir, si.geometry_normal));
+    si.normal = sign * si.geometry_normal;
+    si.shading_normal = sign * si.smooth_normal;
+    return si;
+  }
   Surf si;
   si.prim = prim;
   si.barry = {u, v, 1. - u - v};
@@ -725,8 +819,17 @@ inline Surf SurfaceFromHit(const Scene& s, int prim, double u, double v, V3 ray_
   return si;
 }
 
-// SurfaceInteraction(HitId) + Mesh::GetLocalGeometry (primitive.cxx:91-116).
+// SurfaceInteraction(HitId) + Mesh::GetLocalGeometry (primitive.cxx:91-116).  For a
+// sphere `barry` is the offset from the centre (Spheres::SampleUniformPosition).
 inline Surf SurfaceFromBarycentric(const Scene& s, int prim, V3 barry) {
+  if (IsSphere(s, prim)) {
+    Surf si = SphereSurface(s, prim, Normalized(barry));
+    si.pos = s.sph_c[prim - s.ntri] + barry;
+    si.pos_bounds = SphereBounds(si.pos);
+    si.normal = si.geometry_normal;
+    si.shading_normal = si.smooth_normal;
+    return si;
+  }
   Surf si;
   si.prim = prim;
   si.barry = barry;
@@ -740,7 +843,11 @@ inline Surf SurfaceFromBarycentric(const Scene& s, int prim, V3 barry) {
   return si;
 }
 
-inline double TriArea(const Scene& s, int prim) {  // Mesh::Area, primitive.cxx:129-137
+inline double TriArea(const Scene& s, int prim) {  // Mesh::Area, primitive.cxx:129-137; Spheres::Area :206-211
+  if (IsSphere(s, prim)) {
+    const double r = s.sph_r[prim - s.ntri];
+    return r * r * 4. * Pi;
+  }
   return 0.5 * Length(Cross(s.tv1[prim] - s.tv0[prim], s.tv2[prim] - s.tv0[prim]));
 }
 
@@ -1130,6 +1237,63 @@ static ScatterSample PhaseSample(const MediumDesc& m, V3 reverse_incident, Sampl
   return out;
 }
 
+// SimpleCombined (phasefunctions.cxx:206-273) of the atmosphere's constituents at `pos`:
+// Rayleigh for molecules, Henyey-Greenstein(g) for aerosols, mixed in proportion to their
+// sigma_s (AtmosphereTemplate::SamplePhaseFunction / EvaluatePhaseFunction,
+// atmosphere.cxx:101-123).
+struct CombinedPhase {
+  MediumDesc pf[2];
+  double sel[2];
+  S3 w[2];
+};
+static void MakeCombinedPhase(const MediumDesc& m, V3 pos, const int32_t idx[3], CombinedPhase* c);
+static void AtmSigmaS(const MediumDesc& m, double alt, const int32_t idx[3], S3 out[2]);
+inline double Altitude(const MediumDesc& m, V3 p);
+static void MakeCombinedPhase(const MediumDesc& m, V3 pos, const int32_t idx[3], CombinedPhase* c) {
+  c->pf[0].phase = TT_PHASE_RAYLEIGH;
+  c->pf[1].phase = TT_PHASE_HENYEY_GREENSTEIN;
+  c->pf[1].g = m.g;
+  AtmSigmaS(m, Altitude(m, pos), idx, c->w);
+  const double s0 = c->w[0].Sum(), s1 = c->w[1].Sum();
+  if (s0 + s1 > 0.) {
+    c->sel[0] = s0 / (s0 + s1);
+    c->sel[1] = s1 / (s0 + s1);
+    const S3 tot = c->w[0] + c->w[1];
+    for (int i = 0; i < 2; ++i)
+      for (int k = 0; k < 3; ++k) c->w[i][k] = c->w[i][k] * (1. / tot[k]);
+  } else {
+    c->sel[0] = c->sel[1] = 0.5;
+  }
+}
+
+// Phase function of medium m at a volume vertex at pos (value per wavelength, pdf).
+static S3 MediumPhaseEvaluate(const MediumDesc& m, V3 pos, V3 wi, V3 out, const int32_t idx[3], double* pdf) {
+  if (m.kind != TT_MEDIUM_ATMOSPHERE) {
+    const double v = PhaseEvaluate(m, wi, out);
+    if (pdf) *pdf = v;
+    return S3(v);
+  }
+  CombinedPhase c;
+  MakeCombinedPhase(m, pos, idx, &c);
+  const double p0 = PhaseEvaluate(c.pf[0], wi, out), p1 = PhaseEvaluate(c.pf[1], wi, out);
+  if (pdf) *pdf = c.sel[0] * p0 + c.sel[1] * p1;
+  return c.w[0] * p0 + c.w[1] * p1;
+}
+static ScatterSample MediumPhaseSample(const MediumDesc& m, V3 pos, V3 wi, Sampler& smp, const int32_t idx[3]) {
+  if (m.kind != TT_MEDIUM_ATMOSPHERE) return PhaseSample(m, wi, smp);
+  CombinedPhase c;
+  MakeCombinedPhase(m, pos, idx, &c);
+  const double r = smp.Uniform01();
+  const int k = r >= c.sel[1] ? 0 : 1;  // TowerSampling over two bins
+  ScatterSample s = PhaseSample(c.pf[k], wi, smp);
+  double pdfs[2];
+  pdfs[k] = s.pdf;
+  pdfs[1 - k] = PhaseEvaluate(c.pf[1 - k], wi, s.dir);
+  s.value = c.w[k] * s.pdf + c.w[1 - k] * pdfs[1 - k];
+  s.pdf = c.sel[0] * pdfs[0] + c.sel[1] * pdfs[1];
+  return s;
+}
+
 // ---------------------------------------------------------------------------------------
 // MediumTracker (rendering_util.hxx:18-126, rendering_util.cxx:13-38).  Medium -1 is the
 // empty-space vacuum with priority -1; slots hold up to 4 overlapping media.
@@ -1201,10 +1365,87 @@ inline S3 TakeD3(const double* a, const int32_t idx[3]) { return {a[idx[0]], a[i
 inline S3 ExpNeg(S3 s, double x) { return {std::exp(-s[0] * x), std::exp(-s[1] * x), std::exp(-s[2] * x)}; }
 inline double Mean(S3 s) { return (s[0] + s[1] + s[2]) / 3.; }
 
-// VacuumMedium / HomogeneousMedium::ComputeVolumePdfCoefficients (shader.cxx:1204-1211, 1297-1309).
-static VolCoeffs VolumeCoeffs(const Scene& sc, int medium, double length, const int32_t idx[3]) {
+// ---------------------------------------------------------------------------------------
+// Atmosphere::Tabulated (atmosphere.cxx:18-126, 234-348; atmosphere.hxx:95-123), km units.
+inline double Altitude(const MediumDesc& m, V3 p) { return Length(p - m.center) - m.radius; }
+inline V3 LowestPoint(const MediumDesc& m, V3 org, V3 dir, double length) {
+  double t = -Dot(org - m.center, dir);
+  if (t > length) t = length;
+  else if (t < 0.) t = 0.;
+  return org + dir * t;
+}
+inline double TabLerp(const std::vector<double>& tab, int row, double f, int bin) {
+  return (1. - f) * tab[(size_t)row * NBINS + bin] + f * tab[(size_t)(row + 1) * NBINS + bin];
+}
+// ComputeCollisionCoefficients followed by EvaluateCoeffs' sigma_t = sigma_a + sigma_s.
+// The row index truncates toward zero, so altitudes less than one row below h0 are
+// extrapolated from rows 0 and 1, as the reference's (int) cast does.
+static void AtmCoeffs(const MediumDesc& m, double alt, const int32_t idx[3], S3* sigma_s, S3* sigma_t) {
+  const double ri = (alt - m.h0) * m.inv_dh;
+  if (ri >= (double)(m.n - 1)) { *sigma_s = S3(0.); *sigma_t = S3(0.); return; }
+  const int i = (int)ri;
+  for (int k = 0; k < 3; ++k) {
+    double ss, st;
+    if (i >= 0) {
+      const double f = ri - i;
+      ss = TabLerp(m.sig_aer, i, f, idx[k]) + TabLerp(m.sig_mol, i, f, idx[k]);
+      st = TabLerp(m.sig_t, i, f, idx[k]);
+    } else {
+      ss = m.sig_aer[idx[k]] + m.sig_mol[idx[k]];
+      st = m.sig_t[idx[k]];
+    }
+    const double sa = st - ss;
+    (*sigma_s)[k] = ss;
+    (*sigma_t)[k] = sa + ss;
+  }
+}
+// ComputeSigmaS: per constituent (0 molecules, 1 aerosols).
+static void AtmSigmaS(const MediumDesc& m, double alt, const int32_t idx[3], S3 out[2]) {
+  const double ri = (alt - m.h0) * m.inv_dh;
+  const int i = (int)ri;
+  const std::vector<double>* tabs[2] = {&m.sig_mol, &m.sig_aer};
+  for (int c = 0; c < 2; ++c)
+    for (int k = 0; k < 3; ++k) {
+      if (i >= 0 && i < m.n - 1) out[c][k] = TabLerp(*tabs[c], i, ri - i, idx[k]);
+      else if (i < 0) out[c][k] = (*tabs[c])[idx[k]];
+      else out[c][k] = 0.;
+    }
+}
+// ComputeSigmaTMajorante: the per-row maximum over all bins, made non-increasing upwards.
+static double AtmMajorant(const MediumDesc& m, double alt) {
+  const double ri = (alt - m.h0) * m.inv_dh;
+  const int i = (int)ri;
+  if (i >= 0 && i < m.n - 1) {
+    const double f = ri - i;
+    return (1. - f) * m.maj[i] + f * m.maj[i + 1];
+  }
+  return i < 0 ? m.maj[0] : 0.;
+}
+// AtmosphereTemplate::ComputeMajorante: at the lowest point of the segment, clamped to the
+// table's lower altitude.
+inline double AtmSegmentMajorant(const MediumDesc& m, V3 org, V3 dir, double length) {
+  return AtmMajorant(m, std::max(m.h0, Altitude(m, LowestPoint(m, org, dir, length))));
+}
+
+// ComputeProbabilitiesHistoryScheme (media_integrator.cxx:11-40) for two collision types.
+inline void HistoryProbabilities(S3 w, S3 a, S3 b, double* pa, double* pb) {
+  *pa = Mean(a * w);
+  *pb = Mean(b * w);
+  const double norm = *pa + *pb;
+  if (norm > 0.) { *pa /= norm; *pb /= norm; } else { *pa = *pb = 0.5; }
+}
+
+// VacuumMedium / HomogeneousMedium / AtmosphereTemplate::ComputeVolumePdfCoefficients
+// (shader.cxx:1204-1211, 1297-1309; atmosphere.cxx:66-80).
+static VolCoeffs VolumeCoeffs(const Scene& sc, int medium, V3 org, V3 dir, double length, const int32_t idx[3]) {
   if (medium < 0) return {0., 0., 1.};
-  const S3 se = TakeD3(sc.media[medium].sigma_ext, idx);
+  const MediumDesc& m = sc.media[medium];
+  if (m.kind == TT_MEDIUM_ATMOSPHERE) {
+    const double maj = AtmMajorant(m, Altitude(m, LowestPoint(m, org, dir, length)));
+    const double tr = std::exp(-maj * length);
+    return {maj * tr, maj * tr, tr};
+  }
+  const S3 se = TakeD3(m.sigma_ext, idx);
   const double tr = Mean(ExpNeg(se, length)), e = Mean(se);
   return {e * tr, e * tr, tr};
 }
@@ -1215,12 +1456,81 @@ struct InteractionSample {
   S3 sigma_s;
 };
 
-// HomogeneousMedium::SampleInteractionPoint (shader.cxx:1259-1270) with
-// HomogeneousSpectralTracking (media_integrator.cxx:43-87), Kutz et al. 2017.
-static InteractionSample SampleInteraction(const Scene& sc, int medium, double length, S3 initial_weights,
-                                           Sampler& smp, const int32_t idx[3]) {
+// SpectralTracking (media_integrator.cxx:90-147), the atmosphere's SampleInteractionPoint:
+// null-collision tracking against the segment majorant with spectral MIS.  The weight
+// starts at initial_weights, as in the reference.
+static InteractionSample AtmTracking(const MediumDesc& m, V3 org, V3 dir, double length, S3 initial_weights,
+                                     Sampler& smp, const int32_t idx[3]) {
+  InteractionSample smpl{0., initial_weights, S3(0.)};
+  const double maj = AtmSegmentMajorant(m, org, dir, length);
+  if (maj <= 0.) { smpl.t = LargeNumber; return smpl; }
+  const double mfp = 1. / maj;
+  int iteration = 0;
+  while (++iteration < 1000) {
+    smpl.t -= std::log(smp.Uniform01()) * mfp;
+    if (smpl.t > length) return smpl;
+    S3 ss, st;
+    AtmCoeffs(m, Altitude(m, org + dir * smpl.t), idx, &ss, &st);
+    S3 sn;
+    for (int k = 0; k < 3; ++k) sn[k] = std::max(0., maj - st[k]);
+    double pt, pn;
+    HistoryProbabilities(smpl.weight, ss, sn, &pt, &pn);
+    if (smp.Uniform01() < pt) {
+      smpl.weight = smpl.weight * (mfp / pt);
+      smpl.sigma_s = ss;
+      return smpl;
+    }
+    smpl.weight = smpl.weight * sn * (mfp / pn);
+  }
+  return smpl;
+}
+
+// EstimateTransmission (media_integrator.cxx:150-187): ratio tracking with Russian
+// roulette after five steps (RussianRouletteSurvival, media_integrator.hxx:15-33).
+static S3 AtmTransmission(const MediumDesc& m, V3 org, V3 dir, double length, Sampler& smp, const int32_t idx[3]) {
+  S3 est(1.);
+  const double maj = AtmSegmentMajorant(m, org, dir, length);
+  if (maj <= 0.) return est;
+  const double inv = 1. / maj;
+  double t = 0.;
+  int iteration = 0;
+  for (;;) {
+    t -= std::log(smp.Uniform01()) * inv;
+    if (t > length) break;
+    S3 ss, st;
+    AtmCoeffs(m, Altitude(m, org + dir * t), idx, &ss, &st);
+    S3 sn;
+    for (int k = 0; k < 3; ++k) sn[k] = maj - st[k];
+    est = est * sn * inv;
+    const double w = est.Max();
+    const int it = iteration++;
+    if (w <= 0.) break;
+    if (it < 5) continue;
+    const double p = std::min(w, 1.);
+    if (smp.Uniform01() < p) est = est * (1. / p);
+    else { est = est * 0.; break; }
+  }
+  return est;
+}
+
+// Medium::EvaluateTransmission of one segment: closed form for homogeneous media, ratio
+// tracking for the atmosphere.
+static S3 SegmentTransmission(const Scene& sc, int medium, V3 org, V3 dir, double length, Sampler& smp,
+                              const int32_t idx[3]) {
+  if (medium < 0) return S3(1.);
+  const MediumDesc& m = sc.media[medium];
+  if (m.kind == TT_MEDIUM_ATMOSPHERE) return AtmTransmission(m, org, dir, length, smp, idx);
+  return ExpNeg(TakeD3(m.sigma_ext, idx), length);
+}
+
+// Medium::SampleInteractionPoint of one segment: HomogeneousMedium (shader.cxx:1259-1270)
+// with HomogeneousSpectralTracking (media_integrator.cxx:43-87, Kutz et al. 2017), or the
+// atmosphere's SpectralTracking.
+static InteractionSample SampleInteraction(const Scene& sc, int medium, V3 org, V3 dir, double length,
+                                           S3 initial_weights, Sampler& smp, const int32_t idx[3]) {
   if (medium < 0) return {LargeNumber, S3(1.), S3(0.)};
   const MediumDesc& m = sc.media[medium];
+  if (m.kind == TT_MEDIUM_ATMOSPHERE) return AtmTracking(m, org, dir, length, initial_weights, smp, idx);
   const S3 sigma_ext = TakeD3(m.sigma_ext, idx), sigma_s = TakeD3(m.sigma_s, idx);
   if (!m.is_scattering) return {LargeNumber, ExpNeg(sigma_ext, length), S3(0.)};
   InteractionSample smpl{0., S3(1.), S3(0.)};
@@ -1367,7 +1677,7 @@ struct Worker {
         double prob = sc.type_probs[1] / n;
         double r[2];
         smp.UniformUnitSquare(r);
-        V3 b = ToTriangleBarycentricCoords(r);
+        V3 b = IsSphere(sc, prim) ? ToUniformSphere(r) * sc.sph_r[prim - sc.ntri] : ToTriangleBarycentricCoords(r);
         node.type = SURFACE_EMITTER;
         node.surf = SurfaceFromBarycentric(sc, prim, b);
         *pdf = prob * (1. / TriArea(sc, prim));
@@ -1393,7 +1703,7 @@ struct Worker {
     } else if (n.type == SURFACE_EMITTER) {
       const tt_material& m = sc.materials[sc.mat_of_tri[n.surf.prim]].m;
       // UniformAreaLightDirectionalPart::Evaluate, light.hxx:96-104 (uses the raw winding normal).
-      double vis = Dot(GeometryNormal(sc, n.surf.prim), out_dir) > 0. ? 1. : 0.;
+      double vis = Dot(n.surf.geometry_normal, out_dir) > 0. ? 1. : 0.;
       if (pdf) *pdf = vis / (2. * Pi);
       return Take(m.emission, ctx.idx) * (vis / (2. * Pi));
     } else if (n.type == POINT_LIGHT) {
@@ -1406,9 +1716,7 @@ struct Worker {
   S3 EvaluateScatterer(const Node& n, V3 out_dir, double* pdf) {
     const V3 wi = -n.incident_dir;
     if (n.IsVolume()) {  // EvaluateScatterCoordinateOfScatterer, volume branch
-      const double v = PhaseEvaluate(sc.media[n.medium], wi, out_dir);
-      if (pdf) *pdf = v;
-      return n.sigma_s * v;
+      return MediumPhaseEvaluate(sc.media[n.medium], n.coords, wi, out_dir, ctx.idx, pdf) * n.sigma_s;
     }
     const tt_material& m = sc.materials[sc.mat_of_tri[n.surf.prim]].m;
     S3 fs = EvaluateBSDF(m, wi, n.surf, out_dir, ctx.idx, pdf);
@@ -1452,7 +1760,10 @@ struct Worker {
 
   // TransmittanceEstimate (rendering_util.cxx:40-67): occlusion by surfaces, then the
   // product of the media's transmittances over the boundary-delimited segments.
-  S3 TransmittanceEstimate(V3 org, V3 dir, double length, MediumTracker& mt, VolCoeffs* coeff) {
+  // Ratio tracking through heterogeneous media draws from `shadow`, a stream seeded from
+  // the path's stream at the connection, so that the path's own stream advances as it
+  // would without media.
+  S3 TransmittanceEstimate(V3 org, V3 dir, double length, MediumTracker& mt, VolCoeffs* coeff, Sampler& shadow) {
     length *= 0.9999;
     double t, u, v;
     if (Trace(sc, sc.surf, org, dir, 0., length, true, &t, &u, &v) >= 0) return S3(0.);
@@ -1464,8 +1775,9 @@ struct Worker {
     while (snear != length) {
       const double sfar = k < hits.size() ? hits[k].t : length;
       const int medium = mt.current;
-      if (coeff) Accumulate(*coeff, VolumeCoeffs(sc, medium, sfar - snear, ctx.idx), snear == 0., sfar == length);
-      if (medium >= 0) result = result * ExpNeg(TakeD3(sc.media[medium].sigma_ext, ctx.idx), sfar - snear);
+      const V3 sorg = org + dir * snear;
+      if (coeff) Accumulate(*coeff, VolumeCoeffs(sc, medium, sorg, dir, sfar - snear, ctx.idx), snear == 0., sfar == length);
+      result = result * SegmentTransmission(sc, medium, sorg, dir, sfar - snear, shadow, ctx.idx);
       if (k >= hits.size()) break;
       GoingThroughSurface(sc, mt, dir, hits[k].n, hits[k].material);
       snear = hits[k].t;
@@ -1489,7 +1801,9 @@ struct Worker {
     tf = tf * DFactorOf(light, -dir);
     MediumTracker mt = eye_mt;
     MaybeHandlePassage(eye, dir, mt);
-    const S3 T = TransmittanceEstimate(org, dir, len, mt, coeff);
+    Sampler shadow;
+    SeedPath(shadow.g, smp.g.state, smp.g.inc);
+    const S3 T = TransmittanceEstimate(org, dir, len, mt, coeff, shadow);
     bool wrt_solid_angle = eye.type == ENV || light.type == ENV;
     double r2 = wrt_solid_angle ? 1. : 1. / Sqr(len);
     return T * sf * tf * r2;
@@ -1529,7 +1843,7 @@ struct Worker {
     double pdf;
     bool delta;
     if (src.IsVolume()) {  // SamplePhaseFunction x sigma_s
-      ScatterSample s = PhaseSample(sc.media[src.medium], -src.incident_dir, smp);
+      ScatterSample s = MediumPhaseSample(sc.media[src.medium], src.coords, -src.incident_dir, smp, ctx.idx);
       dir = s.dir; value = s.value * src.sigma_s; pdf = s.pdf; delta = false;
     } else if (src.IsScatter()) {
       const tt_material& m = sc.materials[sc.mat_of_tri[src.surf.prim]].m;
@@ -1573,11 +1887,12 @@ struct Worker {
     while (snear != vend) {
       const double sfar = k < hits.size() ? hits[k].t : vend;
       const int medium = mt.current;
-      const InteractionSample ms = SampleInteraction(sc, medium, sfar - snear, weight, smp, ctx.idx);
+      const V3 sorg = org + dir * snear;
+      const InteractionSample ms = SampleInteraction(sc, medium, sorg, dir, sfar - snear, weight, smp, ctx.idx);
       weight = weight * ms.weight;
       const bool interacted = ms.t < sfar - snear;
       const double seglen = interacted ? ms.t : sfar - snear;
-      Accumulate(st.coeff, VolumeCoeffs(sc, medium, seglen, ctx.idx), snear == 0., interacted);
+      Accumulate(st.coeff, VolumeCoeffs(sc, medium, sorg, dir, seglen, ctx.idx), snear == 0., interacted);
       if (interacted) {
         const double dist = snear + ms.t;
         st.node.type = VOLUME_SCATTER;
@@ -1598,7 +1913,7 @@ struct Worker {
     st.beta_factor = weight;
     if (prim >= 0) {
       st.node.type = SURFACE_SCATTER;
-      st.node.surf = SurfaceFromHit(sc, prim, u, v, dir);
+      st.node.surf = SurfaceFromHit(sc, prim, u, v, org, dir, t);
       st.seg_len = t;
     } else {
       st.node.type = ENV;
@@ -1732,6 +2047,34 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
     }
     md.phase = m.phase;
     md.g = m.phase_g;
+    md.kind = m.kind;
+    if (m.kind == TT_MEDIUM_ATMOSPHERE) {
+      // TabulatedConstituents::TabulatedConstituents, atmosphere.cxx:234-276.
+      if (m.table_size < 2 || !m.sigma_t || !m.sigma_s_molecules || !m.sigma_s_aerosols || !(m.table_dh > 0.f)) {
+        g_err = "bad atmosphere table";
+        return false;
+      }
+      md.is_scattering = true;
+      md.center = {m.planet_center[0], m.planet_center[1], m.planet_center[2]};
+      md.radius = m.planet_radius;
+      md.n = m.table_size;
+      md.h0 = m.table_h0;
+      md.dh = m.table_dh;
+      md.inv_dh = 1. / md.dh;
+      md.sig_t.assign(m.sigma_t, m.sigma_t + (size_t)md.n * NBINS);
+      md.sig_mol.assign(m.sigma_s_molecules, m.sigma_s_molecules + (size_t)md.n * NBINS);
+      md.sig_aer.assign(m.sigma_s_aerosols, m.sigma_s_aerosols + (size_t)md.n * NBINS);
+      md.maj.resize(md.n);
+      for (int r = 0; r < md.n; ++r) {
+        double mx = 0.;
+        for (int b = 0; b < NBINS; ++b) mx = std::max(mx, md.sig_t[(size_t)r * NBINS + b]);
+        md.maj[r] = mx;
+      }
+      for (int r = md.n - 2; r >= 0; --r) md.maj[r] = std::max(md.maj[r], md.maj[r + 1]);
+    } else if (m.kind != TT_MEDIUM_HOMOGENEOUS) {
+      g_err = "unknown medium kind";
+      return false;
+    }
     s.media.push_back(md);
   }
   for (uint32_t i = 0; i < d->num_materials; ++i) {
@@ -1758,12 +2101,36 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
       if (m.emissive) s.area_lights.push_back((int)t);
     }
   }
+  s.ntri = d->num_triangles;
+  if (d->num_spheres > 0 && (!d->spheres || !d->sphere_material_ids)) { g_err = "sphere arrays missing"; return false; }
+  for (uint32_t i = 0; i < d->num_spheres; ++i) {
+    const float* q = d->spheres + 4 * (size_t)i;
+    const uint32_t mat = d->sphere_material_ids[i];
+    if (mat >= d->num_materials) { g_err = "sphere material index out of range"; return false; }
+    if (!(q[3] > 0.f)) { g_err = "sphere radius must be positive"; return false; }
+    s.sph_c.push_back({q[0], q[1], q[2]});
+    s.sph_r.push_back(q[3]);
+    s.mat_of_tri.push_back(mat);
+    const int prim = (int)(d->num_triangles + i);
+    const tt_material& m = s.materials[mat].m;
+    if (m.volume_boundary) {
+      s.vol.tris.push_back(prim);
+    } else {
+      s.surf.tris.push_back(prim);
+      if (m.emissive) s.area_lights.push_back(prim);
+    }
+  }
   for (int k = 0; k < 3; ++k) { s.bb_lo[k] = 1e300; s.bb_hi[k] = -1e300; }
   for (auto& v : s.vert) {
     double c[3] = {v.x, v.y, v.z};
     for (int k = 0; k < 3; ++k) { s.bb_lo[k] = std::min(s.bb_lo[k], c[k]); s.bb_hi[k] = std::max(s.bb_hi[k], c[k]); }
   }
-  if (s.vert.empty()) for (int k = 0; k < 3; ++k) { s.bb_lo[k] = 0; s.bb_hi[k] = 0; }
+  for (size_t i = 0; i < s.sph_c.size(); ++i)
+    for (int k = 0; k < 3; ++k) {
+      s.bb_lo[k] = std::min(s.bb_lo[k], s.sph_c[i][k] - s.sph_r[i]);
+      s.bb_hi[k] = std::max(s.bb_hi[k], s.sph_c[i][k] + s.sph_r[i]);
+    }
+  if (s.vert.empty() && s.sph_c.empty()) for (int k = 0; k < 3; ++k) { s.bb_lo[k] = 0; s.bb_hi[k] = 0; }
   s.diag = std::sqrt(Sqr(s.bb_hi[0] - s.bb_lo[0]) + Sqr(s.bb_hi[1] - s.bb_lo[1]) + Sqr(s.bb_hi[2] - s.bb_lo[2]));
   s.long_distance = 10. * s.diag;
   s.box_center = {0.5 * (s.bb_lo[0] + s.bb_hi[0]), 0.5 * (s.bb_lo[1] + s.bb_hi[1]), 0.5 * (s.bb_lo[2] + s.bb_hi[2])};
@@ -2090,14 +2457,16 @@ int or_medium_walk(or_scene* os, const double* org3, const double* dir3, double 
 
 // TransmittanceEstimate along a segment starting at org with a tracker initialized there.
 int or_transmittance(or_scene* os, const double* org3, const double* dir3, double length, const int32_t* idx,
-                     double* T3, double* coeff3) {
+                     uint64_t seed, double* T3, double* coeff3) {
   Worker w(os->s);
   std::memcpy(w.ctx.idx, idx, 3 * sizeof(int32_t));
   MediumTracker mt;
   V3 o{org3[0], org3[1], org3[2]}, d{dir3[0], dir3[1], dir3[2]};
   InitializeMediumTracker(os->s, mt, o);
   VolCoeffs c;
-  S3 T = w.TransmittanceEstimate(o, d, length, mt, &c);
+  Sampler shadow;
+  SeedPath(shadow.g, seed, 0u);
+  S3 T = w.TransmittanceEstimate(o, d, length, mt, &c, shadow);
   for (int k = 0; k < 3; ++k) T3[k] = T[k];
   coeff3[0] = c.fwd; coeff3[1] = c.bwd; coeff3[2] = c.tr;
   return 0;
@@ -2146,6 +2515,51 @@ int or_phase_sample(int kind, double g, const double* wi3, int n, uint64_t seed,
     dirs[3 * i] = s.dir.x; dirs[3 * i + 1] = s.dir.y; dirs[3 * i + 2] = s.dir.z;
     pdf[i] = s.pdf;
     value[i] = PhaseEvaluate(m, wi, s.dir);
+  }
+  return 0;
+}
+
+// Atmosphere model of medium `medium` (tests): out[0] altitude of pos, out[1..3] lowest
+// point of the segment (org, dir, length), out[4..6] sigma_s and out[7..9] sigma_t at pos,
+// out[10..12] molecular and out[13..15] aerosol sigma_s at pos, out[16] the segment
+// majorant, out[17] the majorant at pos's altitude.
+int or_atmosphere_query(or_scene* os, int medium, const double* pos3, const double* org3, const double* dir3,
+                        double length, const int32_t* idx, double* out) {
+  const Scene& sc = os->s;
+  if (medium < 0 || medium >= (int)sc.media.size() || sc.media[medium].kind != TT_MEDIUM_ATMOSPHERE) return 2;
+  const MediumDesc& m = sc.media[medium];
+  const V3 pos{pos3[0], pos3[1], pos3[2]}, org{org3[0], org3[1], org3[2]}, dir{dir3[0], dir3[1], dir3[2]};
+  out[0] = Altitude(m, pos);
+  const V3 lp = LowestPoint(m, org, dir, length);
+  out[1] = lp.x; out[2] = lp.y; out[3] = lp.z;
+  S3 ss, st, c[2];
+  AtmCoeffs(m, out[0], idx, &ss, &st);
+  AtmSigmaS(m, out[0], idx, c);
+  for (int k = 0; k < 3; ++k) {
+    out[4 + k] = ss[k];
+    out[7 + k] = st[k];
+    out[10 + k] = c[0][k];
+    out[13 + k] = c[1][k];
+  }
+  out[16] = AtmSegmentMajorant(m, org, dir, length);
+  out[17] = AtmMajorant(m, out[0]);
+  return 0;
+}
+
+// n phase samples of medium `medium` at a volume vertex at pos (the atmosphere's phase
+// function depends on the altitude): directions, values per wavelength and pdfs.
+int or_medium_phase_sample(or_scene* os, int medium, const double* pos3, const double* wi3, const int32_t* idx, int n,
+                           uint64_t seed, double* dirs, double* value3, double* pdf) {
+  const Scene& sc = os->s;
+  if (medium < 0 || medium >= (int)sc.media.size()) return 2;
+  const V3 pos{pos3[0], pos3[1], pos3[2]}, wi{wi3[0], wi3[1], wi3[2]};
+  for (int i = 0; i < n; ++i) {
+    Sampler smp;
+    SeedPath(smp.g, seed, (uint64_t)i);
+    const ScatterSample s = MediumPhaseSample(sc.media[medium], pos, wi, smp, idx);
+    dirs[3 * i] = s.dir.x; dirs[3 * i + 1] = s.dir.y; dirs[3 * i + 2] = s.dir.z;
+    for (int k = 0; k < 3; ++k) value3[3 * i + k] = s.value[k];
+    pdf[i] = s.pdf;
   }
   return 0;
 }

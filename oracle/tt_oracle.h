@@ -68,9 +68,13 @@ int or_scene_info(or_scene* s, double* bbox6, int32_t* counts4);
 int or_medium_walk(or_scene* s, const double* org3, const double* dir3, double tfar, int max, int32_t* media,
                    double* ts, int32_t* initial);
 int or_transmittance(or_scene* s, const double* org3, const double* dir3, double length, const int32_t* idx,
-                     double* T3, double* coeff3);
+                     uint64_t seed, double* T3, double* coeff3);
 int or_track(or_scene* s, const double* org3, const double* dir3, const int32_t* idx, int n, uint64_t seed,
              double* out);
+int or_atmosphere_query(or_scene* s, int medium, const double* pos3, const double* org3, const double* dir3,
+                        double length, const int32_t* idx, double* out);
+int or_medium_phase_sample(or_scene* s, int medium, const double* pos3, const double* wi3, const int32_t* idx, int n,
+                           uint64_t seed, double* dirs, double* value3, double* pdf);
 int or_phase_sample(int kind, double g, const double* wi3, int n, uint64_t seed, double* dirs, double* pdf,
                     double* value);
 
