@@ -237,7 +237,7 @@ tt_status tt_render_pass_range(tt_ctx* ctx, int32_t spp, uint64_t seed,
  * callers that cannot let a library call cudaMalloc at render time -- applications that
  * own all GPU memory through their own pool or a fixed budget, or code where an
  * allocation would synchronise the device and stall concurrent work.  The wavefront path
- * state lives in one static device array inside the library (about 14.2 MB, held by every
+ * state lives in one static device array inside the library (about 14.7 MB, held by every
  * GPU that loads the library until the process exits) instead of memory the context
  * allocates.  The caller passes the outputs: d_accum and d_light_accum are device buffers
  * of xres*yres*3 floats to which the pass ADDS the unnormalised RGB sums of its samples and

@@ -149,7 +149,10 @@ struct Builder {
 
 bool build_bvh(const BvhInput& in, int max_leaf, BvhOutput* out) {
   if (max_leaf < 1 || max_leaf > 8 || !out) return false;
-  const uint32_t n = in.num_triangles;
+  if (in.num_spheres > 0 && (!in.spheres || !in.sphere_material_ids || !in.sphere_prim_ids)) return false;
+  // Primitive p < T is triangle p, p >= T is sphere p - T.
+  const uint32_t T = in.num_triangles;
+  const uint32_t n = T + in.num_spheres;
   Builder b;
   b.max_leaf = max_leaf;
   b.tri_box.resize(n);
@@ -158,7 +161,16 @@ bool build_bvh(const BvhInput& in, int max_leaf, BvhOutput* out) {
   for (uint32_t t = 0; t < n; ++t) {
     Box bx;
     bx.reset();
-    for (int j = 0; j < 3; ++j) bx.grow(&in.vertices[3 * (size_t)in.indices[3 * (size_t)t + j]]);
+    if (t < T) {
+      for (int j = 0; j < 3; ++j) bx.grow(&in.vertices[3 * (size_t)in.indices[3 * (size_t)t + j]]);
+    } else {
+      // Bounds one ulp outside centre -/+ radius (SphereBoundsFunc, embreeaccelerator.cxx:263-281).
+      const float* q = &in.spheres[4 * (size_t)(t - T)];
+      for (int k = 0; k < 3; ++k) {
+        bx.lo[k] = std::nextafter(q[k] - q[3], -std::numeric_limits<float>::infinity());
+        bx.hi[k] = std::nextafter(q[k] + q[3], std::numeric_limits<float>::infinity());
+      }
+    }
     b.tri_box[t] = bx;
     for (int k = 0; k < 3; ++k) b.cen[3 * (size_t)t + k] = 0.5f * (bx.lo[k] + bx.hi[k]);
     b.order[t] = (int)t;
@@ -181,6 +193,19 @@ bool build_bvh(const BvhInput& in, int max_leaf, BvhOutput* out) {
   for (uint32_t i = 0; i < n; ++i) {
     const int t = b.order[i];
     float* dst = &out->tris[12 * (size_t)i];
+    if ((uint32_t)t >= T) {
+      const uint32_t k = (uint32_t)t - T;
+      const float* q = &in.spheres[4 * (size_t)k];
+      dst[0] = q[0];
+      dst[1] = q[1];
+      dst[2] = q[2];
+      dst[4] = q[3];
+      const int32_t prim = (int32_t)in.sphere_prim_ids[k], mat = (int32_t)in.sphere_material_ids[k], tag = 1;
+      std::memcpy(&dst[3], &prim, 4);
+      std::memcpy(&dst[7], &mat, 4);
+      std::memcpy(&dst[11], &tag, 4);
+      continue;
+    }
     for (int j = 0; j < 3; ++j) {
       const float* v = &in.vertices[3 * (size_t)in.indices[3 * (size_t)t + j]];
       dst[4 * j] = v[0];

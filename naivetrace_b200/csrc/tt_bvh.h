@@ -10,7 +10,9 @@
 //   int4   n3 = (c0 ref, c1 ref, 0, 0)
 // A child ref >= 0 is an inner node index; a ref < 0 is a leaf: v = ~ref,
 // first triangle slot = v >> 3, triangle count = (v & 7) + 1.  An empty child has an
-// inverted box and refers to slot 0; an empty triangle set gets one degenerate slot.  Triangles are stored per leaf slot as three float4
+// inverted box and refers to slot 0; an empty triangle set gets one degenerate slot.
+// Spheres share the slot array: (centre.xyz | prim id, radius, 0, 0 | material id,
+// 0, 0, 0 | 1); a triangle slot has 0 in the last word, a sphere slot the integer 1.  Triangles are stored per leaf slot as three float4
 // (v0.xyz | prim id, v1.xyz | material id, v2.xyz | 0).
 #pragma once
 
@@ -25,6 +27,10 @@ struct BvhInput {
   const uint32_t* material_ids; // T
   uint32_t num_triangles;
   const uint32_t* prim_ids = nullptr;  // T ids stored in the slots (nullptr: 0 .. T-1)
+  uint32_t num_spheres = 0;
+  const float* spheres = nullptr;              // S x 4: centre, radius
+  const uint32_t* sphere_material_ids = nullptr;
+  const uint32_t* sphere_prim_ids = nullptr;   // S ids stored in the slots
 };
 
 struct BvhOutput {

@@ -65,6 +65,9 @@ struct tt_ctx {
   std::vector<uint32_t> idx, mats;
   std::vector<tt_material> materials;
   std::vector<tt_medium> media;
+  std::vector<std::vector<float>> media_tables;  // per medium: sigma_t, molecules, aerosols (rows x 36 each)
+  std::vector<float> spheres;                    // 4 per sphere
+  std::vector<uint32_t> sphere_mats;
   std::vector<HostEnv> envs;
   std::vector<tt_point_light> points;
   tt_camera camera{};
@@ -166,10 +169,31 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
       return fail(nullptr, TT_ERR_INVALID, "medium index out of range in material " + std::to_string(i));
   }
   if (d->num_media > 0 && !d->media) return fail(nullptr, TT_ERR_INVALID, "media missing");
-  if (d->num_spheres > 0) return fail(nullptr, TT_ERR_INVALID, "spheres are not supported by this build");
+  if (d->num_spheres > (1u << 26)) return fail(nullptr, TT_ERR_CAPACITY, "more than 2^26 spheres");
+  if (d->num_spheres > 0 && (!d->spheres || !d->sphere_material_ids))
+    return fail(nullptr, TT_ERR_INVALID, "sphere arrays missing");
+  for (uint32_t i = 0; i < d->num_spheres; ++i) {
+    const float* q = d->spheres + 4 * (size_t)i;
+    if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]) || !(q[3] > 0.f) || !std::isfinite(q[3]))
+      return fail(nullptr, TT_ERR_INVALID, "sphere " + std::to_string(i) + " needs a finite centre and positive radius");
+    if (d->sphere_material_ids[i] >= d->num_materials)
+      return fail(nullptr, TT_ERR_INVALID, "material index out of range in sphere " + std::to_string(i));
+  }
   if (d->num_media > (uint32_t)kMaxMedia) return fail(nullptr, TT_ERR_CAPACITY, "more than 254 media");
   for (uint32_t i = 0; i < d->num_media; ++i) {
     const tt_medium& m = d->media[i];
+    if (m.kind == TT_MEDIUM_ATMOSPHERE) {
+      if (m.table_size < 2 || !m.sigma_t || !m.sigma_s_molecules || !m.sigma_s_aerosols)
+        return fail(nullptr, TT_ERR_INVALID, "atmosphere " + std::to_string(i) + " needs tables of at least 2 rows");
+      if (!(m.table_dh > 0.f) || !(m.planet_radius > 0.f) || !(std::fabs(m.phase_g) < 1.f))
+        return fail(nullptr, TT_ERR_INVALID, "atmosphere needs positive row spacing and radius and |g| < 1");
+      const float* tabs[3] = {m.sigma_t, m.sigma_s_molecules, m.sigma_s_aerosols};
+      for (const float* t : tabs)
+        for (size_t k = 0; k < (size_t)m.table_size * NBINS; ++k)
+          if (!(t[k] >= 0.f) || !std::isfinite(t[k]))
+            return fail(nullptr, TT_ERR_INVALID, "atmosphere tables must be finite and non-negative");
+      continue;
+    }
     if (m.kind != TT_MEDIUM_HOMOGENEOUS) return fail(nullptr, TT_ERR_INVALID, "unknown medium kind");
     if (m.phase < TT_PHASE_UNIFORM || m.phase > TT_PHASE_HENYEY_GREENSTEIN)
       return fail(nullptr, TT_ERR_INVALID, "unknown phase function in medium " + std::to_string(i));
@@ -186,6 +210,21 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   c->mats.assign(d->material_ids, d->material_ids + d->num_triangles);
   c->materials.assign(d->materials, d->materials + d->num_materials);
   if (d->num_media > 0) c->media.assign(d->media, d->media + d->num_media);
+  for (auto& m : c->media) {
+    std::vector<float> tab;
+    if (m.kind == TT_MEDIUM_ATMOSPHERE) {
+      const size_t n = (size_t)m.table_size * NBINS;
+      tab.insert(tab.end(), m.sigma_t, m.sigma_t + n);
+      tab.insert(tab.end(), m.sigma_s_molecules, m.sigma_s_molecules + n);
+      tab.insert(tab.end(), m.sigma_s_aerosols, m.sigma_s_aerosols + n);
+    }
+    m.sigma_t = m.sigma_s_molecules = m.sigma_s_aerosols = nullptr;
+    c->media_tables.push_back(std::move(tab));
+  }
+  if (d->num_spheres > 0) {
+    c->spheres.assign(d->spheres, d->spheres + 4 * (size_t)d->num_spheres);
+    c->sphere_mats.assign(d->sphere_material_ids, d->sphere_material_ids + d->num_spheres);
+  }
   for (uint32_t i = 0; i < d->num_env_lights; ++i) {
     HostEnv e;
     e.desc = d->env_lights[i];
@@ -232,7 +271,20 @@ tt_status tt_upload_scene(tt_ctx* c) {
     (vol ? vmat : smat).push_back(c->mats[t]);
     (vol ? vid : sid).push_back(t);
   }
+  std::vector<float> ssph, vsph;
+  std::vector<uint32_t> ssmat, ssid, vsmat, vsid;
+  const uint32_t nsph = (uint32_t)c->sphere_mats.size();
+  for (uint32_t i = 0; i < nsph; ++i) {
+    const bool vol = c->materials[c->sphere_mats[i]].volume_boundary != 0;
+    (vol ? vsph : ssph).insert((vol ? vsph : ssph).end(), &c->spheres[4 * (size_t)i], &c->spheres[4 * (size_t)i] + 4);
+    (vol ? vsmat : ssmat).push_back(c->sphere_mats[i]);
+    (vol ? vsid : ssid).push_back(ntri + i);
+  }
   BvhInput bi{c->verts.data(), sidx.data(), smat.data(), (uint32_t)sid.size(), sid.data()};
+  bi.num_spheres = (uint32_t)ssid.size();
+  bi.spheres = ssph.data();
+  bi.sphere_material_ids = ssmat.data();
+  bi.sphere_prim_ids = ssid.data();
   BvhOutput bo;
   if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
   c->bvh_nodes = bo.num_nodes;
@@ -240,6 +292,10 @@ tt_status tt_upload_scene(tt_ctx* c) {
   if (bo.max_depth + 2 >= (uint32_t)BVH_STACK)
     return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
   BvhInput vbi{c->verts.data(), vidx.data(), vmat.data(), (uint32_t)vid.size(), vid.data()};
+  vbi.num_spheres = (uint32_t)vsid.size();
+  vbi.spheres = vsph.data();
+  vbi.sphere_material_ids = vsmat.data();
+  vbi.sphere_prim_ids = vsid.data();
   BvhOutput vbo;
   if (!build_bvh(vbi, 4, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
   if (vbo.max_depth + 2 >= (uint32_t)BVH_STACK)
@@ -254,17 +310,20 @@ tt_status tt_upload_scene(tt_ctx* c) {
   s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
   s.vnodes = (const float4*)upload(vbo.nodes.data(), vbo.nodes.size() * sizeof(float));
   s.vtris = (const float4*)upload(vbo.tris.data(), vbo.tris.size() * sizeof(float));
-  s.num_vol_tris = (int)vid.size();
-  std::vector<uint32_t> ti(4 * (size_t)ntri);
+  s.num_vol_tris = (int)(vid.size() + vsid.size());
+  s.num_spheres = (int)nsph;
+  // Per global primitive: vertex indices and material (spheres: material only).
+  std::vector<uint32_t> ti(4 * ((size_t)ntri + nsph), 0u);
   for (uint32_t t = 0; t < ntri; ++t) {
     ti[4 * t] = c->idx[3 * t];
     ti[4 * t + 1] = c->idx[3 * t + 1];
     ti[4 * t + 2] = c->idx[3 * t + 2];
     ti[4 * t + 3] = c->mats[t];
   }
+  for (uint32_t i = 0; i < nsph; ++i) ti[4 * ((size_t)ntri + i) + 3] = c->sphere_mats[i];
   s.tri_idx = (const uint4*)upload(ti.data(), ti.size() * sizeof(uint32_t));
   s.normals = c->normals.empty() ? nullptr : (const float*)upload(c->normals.data(), c->normals.size() * sizeof(float));
-  s.num_tris = (int)sid.size();
+  s.num_tris = (int)(sid.size() + ssid.size());
   // Materials.
   std::vector<DevMaterial> dm(c->materials.size());
   for (size_t i = 0; i < dm.size(); ++i) {
@@ -284,6 +343,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   for (size_t i = 0; i < dmed.size(); ++i) {
     const tt_medium& m = c->media[i];
     DevMedium& o = dmed[i];
+    o.kind = m.kind;
     o.priority = m.priority;
     o.phase = m.phase;
     o.g = m.phase_g;
@@ -292,6 +352,30 @@ tt_status tt_upload_scene(tt_ctx* c) {
       o.sigma_s[b] = m.sigma_s[b];
       o.sigma_ext[b] = m.sigma_s[b] + m.sigma_a[b];
       o.scattering |= m.sigma_s[b] > 0.f;
+    }
+    if (m.kind == TT_MEDIUM_ATMOSPHERE) {
+      // Rows of (sigma_t, molecules, aerosols) per bin as float4, and the majorant per row
+      // made non-increasing upwards (TabulatedConstituents, atmosphere.cxx:260-272).
+      const int rows = m.table_size;
+      const std::vector<float>& t = c->media_tables[i];
+      const size_t n = (size_t)rows * NBINS;
+      std::vector<float> inter(4 * n, 0.f), maj(rows, 0.f);
+      for (size_t k = 0; k < n; ++k) {
+        inter[4 * k] = t[k];
+        inter[4 * k + 1] = t[n + k];
+        inter[4 * k + 2] = t[2 * n + k];
+      }
+      for (int r = 0; r < rows; ++r)
+        for (int b = 0; b < NBINS; ++b) maj[r] = std::max(maj[r], t[(size_t)r * NBINS + b]);
+      for (int r = rows - 2; r >= 0; --r) maj[r] = std::max(maj[r], maj[r + 1]);
+      o.scattering = 1;
+      o.rows = rows;
+      o.h0 = m.table_h0;
+      o.inv_dh = 1.f / m.table_dh;
+      for (int k = 0; k < 3; ++k) o.center[k] = m.planet_center[k];
+      o.radius = m.planet_radius;
+      o.table = (const float4*)upload(inter.data(), inter.size() * sizeof(float));
+      o.maj = (const float*)upload(maj.data(), maj.size() * sizeof(float));
     }
   }
   s.media = (const DevMedium*)upload(dmed.data(), dmed.size() * sizeof(DevMedium));
@@ -312,6 +396,14 @@ tt_status tt_upload_scene(tt_ctx* c) {
       av.push_back(v[2]);
       av.push_back(0.f);
     }
+  }
+  for (uint32_t i = 0; i < nsph; ++i) {
+    const tt_material& mt = c->materials[c->sphere_mats[i]];
+    if (!mt.emissive || mt.volume_boundary) continue;
+    const float* q = &c->spheres[4 * (size_t)i];
+    al.push_back((int)(ntri + i));
+    const float rec[12] = {q[0], q[1], q[2], 1.f, q[3], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    av.insert(av.end(), rec, rec + 12);
   }
   s.area_lights = (const int*)upload(al.data(), al.size() * sizeof(int));
   s.area_verts = (const float4*)upload(av.data(), av.size() * sizeof(float));
@@ -433,7 +525,12 @@ tt_status tt_upload_scene(tt_ctx* c) {
       lo[k] = std::min(lo[k], (double)c->verts[3 * v + k]);
       hi[k] = std::max(hi[k], (double)c->verts[3 * v + k]);
     }
-  if (c->verts.empty()) for (int k = 0; k < 3; ++k) { lo[k] = hi[k] = 0; }
+  for (uint32_t i = 0; i < nsph; ++i)
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], (double)c->spheres[4 * (size_t)i + k] - c->spheres[4 * (size_t)i + 3]);
+      hi[k] = std::max(hi[k], (double)c->spheres[4 * (size_t)i + k] + c->spheres[4 * (size_t)i + 3]);
+    }
+  if (c->verts.empty() && nsph == 0) for (int k = 0; k < 3; ++k) { lo[k] = hi[k] = 0; }
   const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
                                 (hi[2] - lo[2]) * (hi[2] - lo[2]));
   s.long_distance = (float)(10. * diag);
@@ -512,7 +609,7 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
     p.track = (uint2*)m.alloc(n * sizeof(uint2));
     p.vol = (float4*)m.alloc(n * sizeof(float4));
     p.sh_track = (uint2*)m.alloc(n * sizeof(uint2));
-    p.sh_mis = (float2*)m.alloc(n * sizeof(float2));
+    p.sh_med = (float4*)m.alloc(n * sizeof(float4));
   }
   p.err = c->d_err;
   for (void* a : m.allocs)

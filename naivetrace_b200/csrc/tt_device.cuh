@@ -659,10 +659,10 @@ __device__ __forceinline__ int camera_evaluate(const DevCamera& c, float3 dir_ou
 
 // Phase functions (phasefunctions.cxx:23-138).  mu is the cosine between the direction of
 // travel before and after scattering.
-__device__ __forceinline__ float phase_value(const DevMedium& m, float mu) {
-  if (m.phase == TT_PHASE_RAYLEIGH) return (3.f / (16.f * kPi)) * (1.f + mu * mu);
-  if (m.phase == TT_PHASE_HENYEY_GREENSTEIN) {
-    const float g = m.g, g2 = g * g;
+__device__ __forceinline__ float phase_value(int kind, float g, float mu) {
+  if (kind == TT_PHASE_RAYLEIGH) return (3.f / (16.f * kPi)) * (1.f + mu * mu);
+  if (kind == TT_PHASE_HENYEY_GREENSTEIN) {
+    const float g2 = g * g;
     const float term = 1.f + g2 - 2.f * g * mu;
     return (1.f / (4.f * kPi)) * (1.f - g2) / (sqrtf(term) * term);
   }
@@ -670,27 +670,27 @@ __device__ __forceinline__ float phase_value(const DevMedium& m, float mu) {
 }
 
 // Evaluate at a volume vertex: wi = reverse incident direction, wo = outgoing direction.
-__device__ __forceinline__ float phase_eval(const DevMedium& m, float3 wi, float3 wo) {
-  return phase_value(m, dot3(-wi, wo));
+__device__ __forceinline__ float phase_eval(int kind, float g, float3 wi, float3 wo) {
+  return phase_value(kind, g, dot3(-wi, wo));
 }
 
 // Sample about the direction of travel -wi.  Rayleigh inverts its cdf in closed form;
 // Henyey-Greenstein uses its textbook inversion with a series for |g| <= 1e-3.
 // Directions are laid out as (sin(2 pi r1) rho, cos(2 pi r1) rho, mu) in the frame whose
 // z axis is the direction of travel.
-__device__ __forceinline__ float3 phase_sample(const DevMedium& m, float3 wi, Rng& rng, float* pdf) {
+__device__ __forceinline__ float3 phase_sample(int kind, float g, float3 wi, Rng& rng, float* pdf) {
   float r[2];
   rng.square(r);
-  if (m.phase == TT_PHASE_UNIFORM) {
+  if (kind == TT_PHASE_UNIFORM) {
     *pdf = 1.f / (4.f * kPi);
     return to_uniform_sphere(r);
   }
   float mu;
-  if (m.phase == TT_PHASE_RAYLEIGH) {
+  if (kind == TT_PHASE_RAYLEIGH) {
     const float a = cbrtf(-2.f + 4.f * r[0] + sqrtf(5.f - 16.f * r[0] + 16.f * r[0] * r[0]));
     mu = a - 1.f / a;
   } else {
-    const float g = m.g, g2 = g * g, x = 2.f * r[0] - 1.f;
+    const float g2 = g * g, x = 2.f * r[0] - 1.f;
     if (fabsf(g) > 1.0e-3f) {
       const float t1 = (1.f - g2) / (1.f + g * x);
       mu = (1.f + g2 - t1 * t1) / (2.f * g);
@@ -704,7 +704,7 @@ __device__ __forceinline__ float3 phase_sample(const DevMedium& m, float3 wi, Rn
   float sn, cs;
   sincosf(2.f * kPi * r[1], &sn, &cs);
   const Frame fr = frame_z(-wi);
-  *pdf = phase_value(m, mu);
+  *pdf = phase_value(kind, g, mu);
   return normalize3(fr.to_world(f3(sn * rho, cs * rho, mu)));
 }
 
@@ -803,6 +803,282 @@ __device__ __forceinline__ InteractionSample sample_interaction(const DevMedium&
 // shader.cxx:1297-1309): the mean over the three wavelengths.
 __device__ __forceinline__ float segment_tr(const DevMedium& m, float len, Lambda l) {
   return mean3(exp_neg(take(m.sigma_ext, l), len));
+}
+
+// ----------------------------------------------------------------------------------------
+// Analytic spheres (Spheres, primitive.hxx:94-136).
+
+// FillPosBoundsSphere (primitive.cxx:302-306): Gamma<float>(5).
+__device__ __forceinline__ float gamma5() { return (5.f * kEpsF) / (1.f - 5.f * kEpsF); }
+
+// Slot tag of the BVH slot arrays: triangles 0, spheres 1 (tt_bvh.h).
+__device__ __forceinline__ bool is_sphere_slot(const float4* tris, int slot) {
+  return __float_as_int(__ldg(&tris[3 * slot + 2]).w) != 0;
+}
+
+// Interaction on the sphere at `slot` from the outward direction (nx, ny, nz) (unit, in
+// double): the position is the centre plus radius times the normal, as
+// FirstIntersectionSphere and Spheres::GetLocalGeometry place it.
+__device__ __forceinline__ Surf sphere_surface(const float4* tris, int slot, double nx, double ny, double nz) {
+  const float4 a = __ldg(&tris[3 * slot]);
+  const float4 b = __ldg(&tris[3 * slot + 1]);
+  Surf s;
+  s.prim = __float_as_int(a.w);
+  s.material = __float_as_int(b.w);
+  s.pos = f3((float)(a.x + b.x * nx), (float)(a.y + b.x * ny), (float)(a.z + b.x * nz));
+  s.ng = f3((float)nx, (float)ny, (float)nz);
+  s.ns_raw = s.ng;
+  s.bounds = abs3(s.pos) * gamma5();
+  s.n = s.ng;
+  s.ns = s.ns_raw;
+  return s;
+}
+
+// Hit at distance t along (o, d).
+__device__ __forceinline__ Surf sphere_hit_surface(const float4* tris, int slot, float3 o, float3 d, float t) {
+  const float4 a = __ldg(&tris[3 * slot]);
+  double nx = (double)o.x + (double)t * d.x - a.x, ny = (double)o.y + (double)t * d.y - a.y,
+         nz = (double)o.z + (double)t * d.z - a.z;
+  const double inv = 1.0 / sqrt(nx * nx + ny * ny + nz * nz);
+  return sphere_surface(tris, slot, nx * inv, ny * inv, nz * inv);
+}
+
+// ----------------------------------------------------------------------------------------
+// Tabulated atmosphere (TabulatedConstituents + SphereGeometry, atmosphere.hxx:79-123,
+// atmosphere.cxx:234-348).  Distances to the planet centre are taken in double: at a
+// radius of thousands of km single precision would leave altitude errors of metres.
+__device__ __forceinline__ float atm_altitude(const DevMedium& m, float3 p) {
+  const double dx = (double)p.x - m.center[0], dy = (double)p.y - m.center[1], dz = (double)p.z - m.center[2];
+  return (float)(sqrt(dx * dx + dy * dy + dz * dz) - (double)m.radius);
+}
+
+// SphereGeometry::ComputeLowestPointAlong.
+__device__ __forceinline__ float3 atm_lowest_point(const DevMedium& m, float3 org, float3 dir, float len) {
+  double t = -(((double)org.x - m.center[0]) * dir.x + ((double)org.y - m.center[1]) * dir.y +
+               ((double)org.z - m.center[2]) * dir.z);
+  if (t > len) t = len;
+  else if (t < 0.0) t = 0.0;
+  return f3((float)(org.x + t * dir.x), (float)(org.y + t * dir.y), (float)(org.z + t * dir.z));
+}
+
+// ComputeCollisionCoefficients with EvaluateCoeffs' sigma_t = sigma_a + sigma_s.  The row
+// index truncates toward zero like the reference's (int) cast, so the first row below h0
+// extrapolates.
+__device__ __forceinline__ void atm_coeffs(const DevMedium& m, float alt, Lambda l, float3* ss, float3* st) {
+  const float ri = (alt - m.h0) * m.inv_dh;
+  if (ri >= (float)(m.rows - 1)) {
+    *ss = f3(0.f, 0.f, 0.f);
+    *st = f3(0.f, 0.f, 0.f);
+    return;
+  }
+  const int i = (int)ri;
+  const int bins[3] = {l.i0, l.i1, l.i2};
+  float s3[3], t3[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    float s_, t_;
+    if (i >= 0) {
+      const float f = ri - (float)i;
+      const float4 A = __ldg(&m.table[(size_t)i * NBINS + bins[k]]);
+      const float4 B = __ldg(&m.table[(size_t)(i + 1) * NBINS + bins[k]]);
+      s_ = ((1.f - f) * A.z + f * B.z) + ((1.f - f) * A.y + f * B.y);
+      t_ = (1.f - f) * A.x + f * B.x;
+    } else {
+      const float4 A = __ldg(&m.table[bins[k]]);
+      s_ = A.z + A.y;
+      t_ = A.x;
+    }
+    s3[k] = s_;
+    t3[k] = (t_ - s_) + s_;
+  }
+  *ss = f3(s3[0], s3[1], s3[2]);
+  *st = f3(t3[0], t3[1], t3[2]);
+}
+
+// ComputeSigmaS: molecular and aerosol scattering separately.
+__device__ __forceinline__ void atm_sigma_s(const DevMedium& m, float alt, Lambda l, float3* mol, float3* aer) {
+  const float ri = (alt - m.h0) * m.inv_dh;
+  const int i = (int)ri;
+  const int bins[3] = {l.i0, l.i1, l.i2};
+  float m3[3], a3[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (i >= 0 && i < m.rows - 1) {
+      const float f = ri - (float)i;
+      const float4 A = __ldg(&m.table[(size_t)i * NBINS + bins[k]]);
+      const float4 B = __ldg(&m.table[(size_t)(i + 1) * NBINS + bins[k]]);
+      m3[k] = (1.f - f) * A.y + f * B.y;
+      a3[k] = (1.f - f) * A.z + f * B.z;
+    } else if (i < 0) {
+      const float4 A = __ldg(&m.table[bins[k]]);
+      m3[k] = A.y;
+      a3[k] = A.z;
+    } else {
+      m3[k] = a3[k] = 0.f;
+    }
+  }
+  *mol = f3(m3[0], m3[1], m3[2]);
+  *aer = f3(a3[0], a3[1], a3[2]);
+}
+
+// ComputeSigmaTMajorante.
+__device__ __forceinline__ float atm_majorant(const DevMedium& m, float alt) {
+  const float ri = (alt - m.h0) * m.inv_dh;
+  const int i = (int)ri;
+  if (i >= 0 && i < m.rows - 1) {
+    const float f = ri - (float)i;
+    return (1.f - f) * __ldg(&m.maj[i]) + f * __ldg(&m.maj[i + 1]);
+  }
+  return i < 0 ? __ldg(&m.maj[0]) : 0.f;
+}
+
+// AtmosphereTemplate::ComputeMajorante: at the segment's lowest point, clamped to h0.
+__device__ __forceinline__ float atm_segment_majorant(const DevMedium& m, float3 org, float3 dir, float len) {
+  return atm_majorant(m, fmaxf(m.h0, atm_altitude(m, atm_lowest_point(m, org, dir, len))));
+}
+
+__device__ __forceinline__ void history_probabilities(float3 w, float3 a, float3 b, float* pa, float* pb) {
+  *pa = mean3(mul(a, w));
+  *pb = mean3(mul(b, w));
+  const float norm = *pa + *pb;
+  if (norm > 0.f) { *pa /= norm; *pb /= norm; } else { *pa = *pb = 0.5f; }
+}
+
+// SpectralTracking (media_integrator.cxx:90-147) against the segment majorant; the weight
+// starts at `initial`, as in the reference.  At most 999 collisions.
+__device__ __forceinline__ InteractionSample atm_tracking(const DevMedium& m, float3 org, float3 dir, float len,
+                                                          float3 initial, Rng& rng, Lambda l) {
+  InteractionSample out;
+  out.t = 0.f;
+  out.weight = initial;
+  out.sigma_s = f3(0.f, 0.f, 0.f);
+  const float maj = atm_segment_majorant(m, org, dir, len);
+  if (!(maj > 0.f)) {
+    out.t = kLargeNumber;
+    return out;
+  }
+  const float mfp = 1.f / maj;
+  for (int it = 1; it < 1000; ++it) {
+    out.t -= logf(rng.uniform()) * mfp;
+    if (out.t > len) return out;
+    float3 ss, st;
+    atm_coeffs(m, atm_altitude(m, org + dir * out.t), l, &ss, &st);
+    const float3 sn = f3(fmaxf(0.f, maj - st.x), fmaxf(0.f, maj - st.y), fmaxf(0.f, maj - st.z));
+    float pt, pn;
+    history_probabilities(out.weight, ss, sn, &pt, &pn);
+    if (rng.uniform() < pt) {
+      out.weight = out.weight * (mfp / pt);
+      out.sigma_s = ss;
+      return out;
+    }
+    out.weight = mul(out.weight, sn) * (mfp / pn);
+  }
+  return out;
+}
+
+// EstimateTransmission (media_integrator.cxx:150-187): ratio tracking with Russian roulette
+// after five steps.  Capped at 2^16 steps (error bit ERR_CROSSINGS).
+__device__ __forceinline__ float3 atm_transmission(const DevMedium& m, float3 org, float3 dir, float len, Rng& rng,
+                                                   Lambda l, unsigned int* err) {
+  float3 est = f3(1.f, 1.f, 1.f);
+  const float maj = atm_segment_majorant(m, org, dir, len);
+  if (!(maj > 0.f)) return est;
+  const float inv = 1.f / maj;
+  float t = 0.f;
+  for (int it = 0;; ++it) {
+    if (it >= (1 << 16)) {
+      atomicOr(err, ERR_CROSSINGS);
+      return f3(0.f, 0.f, 0.f);
+    }
+    t -= logf(rng.uniform()) * inv;
+    if (t > len) break;
+    float3 ss, st;
+    atm_coeffs(m, atm_altitude(m, org + dir * t), l, &ss, &st);
+    est = mul(est, f3(maj - st.x, maj - st.y, maj - st.z)) * inv;
+    const float w = max3(est);
+    if (!(w > 0.f)) break;
+    if (it < 5) continue;
+    const float p = fminf(w, 1.f);
+    if (rng.uniform() < p) est = est * (1.f / p);
+    else return f3(0.f, 0.f, 0.f);
+  }
+  return est;
+}
+
+// Medium-generic operations on a segment (org, dir, len) and at a volume vertex.
+__device__ __forceinline__ InteractionSample medium_interaction(const DevMedium& m, float3 org, float3 dir, float len,
+                                                                float3 hist, Rng& rng, Lambda l) {
+  if (m.kind == TT_MEDIUM_ATMOSPHERE) return atm_tracking(m, org, dir, len, hist, rng, l);
+  return sample_interaction(m, len, hist, rng, l);
+}
+__device__ __forceinline__ float medium_segment_tr(const DevMedium& m, float3 org, float3 dir, float len, Lambda l) {
+  if (m.kind == TT_MEDIUM_ATMOSPHERE) {
+    // AtmosphereTemplate::ComputeVolumePdfCoefficients (atmosphere.cxx:66-80): the
+    // majorant at the lowest point, unclamped, as a homogeneous extinction.
+    return expf(-atm_majorant(m, atm_altitude(m, atm_lowest_point(m, org, dir, len))) * len);
+  }
+  return segment_tr(m, len, l);
+}
+__device__ __forceinline__ float3 medium_transmission(const DevMedium& m, float3 org, float3 dir, float len, Rng& rng,
+                                                      Lambda l, unsigned int* err) {
+  if (m.kind == TT_MEDIUM_ATMOSPHERE) return atm_transmission(m, org, dir, len, rng, l, err);
+  return exp_neg(take(m.sigma_ext, l), len);
+}
+
+// SimpleCombined (phasefunctions.cxx:206-273) of Rayleigh (molecules) and
+// Henyey-Greenstein (aerosols) in proportion to their sigma_s at the vertex.
+struct CombinedPhase {
+  float sel0, sel1;
+  float3 w0, w1;
+};
+__device__ __forceinline__ CombinedPhase atm_phase(const DevMedium& m, float3 pos, Lambda l) {
+  CombinedPhase c;
+  atm_sigma_s(m, atm_altitude(m, pos), l, &c.w0, &c.w1);
+  const float s0 = c.w0.x + c.w0.y + c.w0.z, s1 = c.w1.x + c.w1.y + c.w1.z;
+  if (s0 + s1 > 0.f) {
+    c.sel0 = s0 / (s0 + s1);
+    c.sel1 = s1 / (s0 + s1);
+    const float3 tot = c.w0 + c.w1;
+    const float3 inv = f3(1.f / tot.x, 1.f / tot.y, 1.f / tot.z);
+    c.w0 = mul(c.w0, inv);
+    c.w1 = mul(c.w1, inv);
+  } else {
+    c.sel0 = c.sel1 = 0.5f;
+  }
+  return c;
+}
+
+// Phase function value per wavelength and pdf at a volume vertex at pos.
+__device__ __forceinline__ float3 medium_phase_eval(const DevMedium& m, float3 pos, float3 wi, float3 wo, Lambda l,
+                                                    float* pdf) {
+  if (m.kind != TT_MEDIUM_ATMOSPHERE) {
+    const float v = phase_eval(m.phase, m.g, wi, wo);
+    *pdf = v;
+    return f3(v, v, v);
+  }
+  const CombinedPhase c = atm_phase(m, pos, l);
+  const float p0 = phase_eval(TT_PHASE_RAYLEIGH, 0.f, wi, wo), p1 = phase_eval(TT_PHASE_HENYEY_GREENSTEIN, m.g, wi, wo);
+  *pdf = c.sel0 * p0 + c.sel1 * p1;
+  return c.w0 * p0 + c.w1 * p1;
+}
+
+__device__ __forceinline__ float3 medium_phase_sample(const DevMedium& m, float3 pos, float3 wi, Rng& rng, Lambda l,
+                                                      float3* value, float* pdf) {
+  if (m.kind != TT_MEDIUM_ATMOSPHERE) {
+    const float3 d = phase_sample(m.phase, m.g, wi, rng, pdf);
+    *value = f3(*pdf, *pdf, *pdf);
+    return d;
+  }
+  const CombinedPhase c = atm_phase(m, pos, l);
+  const bool aer = !(rng.uniform() >= c.sel1);  // TowerSampling over (molecules, aerosols)
+  float pk;
+  const float3 d = aer ? phase_sample(TT_PHASE_HENYEY_GREENSTEIN, m.g, wi, rng, &pk)
+                       : phase_sample(TT_PHASE_RAYLEIGH, 0.f, wi, rng, &pk);
+  const float po = aer ? phase_eval(TT_PHASE_RAYLEIGH, 0.f, wi, d) : phase_eval(TT_PHASE_HENYEY_GREENSTEIN, m.g, wi, d);
+  const float p0 = aer ? po : pk, p1 = aer ? pk : po;
+  *value = c.w0 * p0 + c.w1 * p1;
+  *pdf = c.sel0 * p0 + c.sel1 * p1;
+  return d;
 }
 
 }  // namespace tt

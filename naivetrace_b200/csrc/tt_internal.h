@@ -32,12 +32,23 @@ struct DevMaterial {
   float emission[NBINS];
 };
 
-// Homogeneous medium (HomogeneousMedium, shader.cxx:1234-1316) with its phase function.
+// A participating medium: homogeneous (HomogeneousMedium, shader.cxx:1234-1316) with its
+// phase function, or a tabulated planetary atmosphere (Atmosphere::Tabulated,
+// atmosphere.cxx:18-126, 234-348; lengths in km).
 struct DevMedium {
+  int kind;          // TT_MEDIUM_*
   int priority;
-  int phase;         // TT_PHASE_*
-  float g;           // Henyey-Greenstein asymmetry
+  int phase;         // TT_PHASE_* (homogeneous)
+  float g;           // Henyey-Greenstein asymmetry (homogeneous HG; atmosphere aerosols)
   int scattering;    // any sigma_s > 0
+  // Atmosphere.
+  int rows;          // altitude rows
+  float h0, inv_dh;  // altitude of row 0, 1 / row spacing
+  float center[3];
+  float radius;
+  const float4* table;  // rows x NBINS: (sigma_t, sigma_s molecules, sigma_s aerosols, 0)
+  const float* maj;     // rows: majorant, non-increasing with altitude
+  // Homogeneous.
   float sigma_s[NBINS];
   float sigma_ext[NBINS];
 };
@@ -88,6 +99,7 @@ struct DevScene {
   const float4* vnodes;
   const float4* vtris;
   int num_vol_tris;
+  int num_spheres;            // spheres share the BVH slot arrays (tt_bvh.h)
   int num_media;
   const DevMedium* media;
   uint2 cam_track;            // medium tracker at the camera position
@@ -116,7 +128,8 @@ struct PathState {
   uint2* track;        // medium tracker: x = 4 slot bytes (0xff empty), y = current medium (-1 vacuum)
   float4* vol;         // sigma_s at a volume interaction (xyz); w = transmittance pdf factor of the step
   uint2* sh_track;     // medium tracker of the shadow ray at its origin
-  float2* sh_mis;      // x = light pdf (< 0: MIS weight 1), y = scatter pdf before the transmittance factor
+  float4* sh_med;      // x = light pdf (< 0: MIS weight 1), y = scatter pdf before the transmittance
+                       // factor, z/w = the path's random state at the connection (low/high words)
 };
 
 struct Framebuffer {

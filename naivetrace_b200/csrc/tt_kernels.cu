@@ -113,6 +113,34 @@ __device__ __forceinline__ bool intersect_tri(const RayPre& r, float3 v0, float3
   return true;
 }
 
+// Ray/sphere test of a sphere slot (centre a.xyz, radius b.x) in double precision: the
+// roots of t^2 |d|^2 + 2 t (v.d) + |v|^2 - r^2 = 0, v = o - centre, from the
+// cancellation-free pair q = -(b + sign(b) sqrt(D)), t = q / a and c / q (PBRT's
+// Quadratic, util.hxx:131-144).  The nearer root in (tnear, tfar] is the hit.  (The
+// reference tests spheres in single precision with error bounds,
+// embreeaccelerator.cxx:307-427; single precision loses planet-sized spheres near the
+// ground.)
+__device__ __forceinline__ bool intersect_sphere(const RayPre& r, float4 a, float4 b, float tnear, float tfar,
+                                                 float* tout) {
+  const double vx = (double)r.o.x - a.x, vy = (double)r.o.y - a.y, vz = (double)r.o.z - a.z;
+  const double dx = r.d.x, dy = r.d.y, dz = r.d.z;
+  const double A = dx * dx + dy * dy + dz * dz;
+  const double B = vx * dx + vy * dy + vz * dz;
+  const double C = vx * vx + vy * vy + vz * vz - (double)b.x * b.x;
+  const double D = B * B - A * C;
+  if (D < 0.0) return false;
+  const double q = -(B + copysign(sqrt(D), B));
+  double t0 = q / A, t1 = q != 0.0 ? C / q : 0.0;
+  if (t0 > t1) { const double x = t0; t0 = t1; t1 = x; }
+  float t = (float)t0;
+  if (!(t > tnear && t <= tfar)) {
+    t = (float)t1;
+    if (!(t > tnear && t <= tfar)) return false;
+  }
+  *tout = t;
+  return true;
+}
+
 struct TraceCounters {
   unsigned int nodes;
   unsigned int tris;
@@ -146,7 +174,7 @@ struct BvhRef {
 __device__ __forceinline__ BvhRef surface_bvh(const DevScene& sc) { return BvhRef{sc.nodes, sc.tris}; }
 __device__ __forceinline__ BvhRef volume_bvh(const DevScene& sc) { return BvhRef{sc.vnodes, sc.vtris}; }
 
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, bool SPH>
 __device__ __forceinline__ bool trace_step(const BvhRef& bvh, TraceState& s, int* stack, unsigned int* err,
                                            TraceCounters* cnt) {
   const RayPre& r = s.r;
@@ -189,8 +217,11 @@ __device__ __forceinline__ bool trace_step(const BvhRef& bvh, TraceState& s, int
       const float4 b = __ldg(&bvh.tris[3 * i + 1]);
       const float4 c = __ldg(&bvh.tris[3 * i + 2]);
       if (COUNT) cnt->tris++;
-      float t, b1, b2;
-      if (intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2)) {
+      float t, b1 = 0.f, b2 = 0.f;
+      bool hit;
+      if (SPH && __float_as_int(c.w) != 0) hit = intersect_sphere(r, a, b, s.tnear, s.best_t, &t);
+      else hit = intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2);
+      if (hit) {
         s.best = i;
         s.best_t = t;
         s.b1 = b1;
@@ -219,7 +250,7 @@ __device__ __forceinline__ float refine_t(const DevScene& sc, const RayPre& r, i
 }
 
 // Whole traversal of one ray (batch queries).  Returns the triangle slot or -1.
-template <bool ANY, bool COUNT>
+template <bool ANY, bool COUNT, bool SPH>
 __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float tnear, float tfar, float* t_out,
                                      float* b1_out, float* b2_out, unsigned int* err, TraceCounters* cnt) {
   const BvhRef bvh = surface_bvh(sc);
@@ -232,10 +263,10 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
   s.best = -1;
   s.cur = 0;
   s.sp = 0;
-  while (!trace_step<ANY, COUNT>(bvh, s, stack, err, cnt)) {
+  while (!trace_step<ANY, COUNT, SPH>(bvh, s, stack, err, cnt)) {
   }
   if (s.best >= 0) {
-    *t_out = ANY ? s.best_t : refine_t(sc, r, s.best);
+    *t_out = (ANY || (SPH && is_sphere_slot(sc.tris, s.best))) ? s.best_t : refine_t(sc, r, s.best);
     *b1_out = s.b1;
     *b2_out = s.b2;
   }
@@ -245,6 +276,7 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
 // Nearest hit with tnear < t <= tfar in `bvh`, with the single-precision plane distance
 // (no refinement, so that the next query can start exactly at the returned t).  Returns
 // the triangle slot or -1.
+template <bool SPH>
 __device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, float tnear, float tfar, float* t_out,
                                         unsigned int* err) {
   TraceState s;
@@ -256,7 +288,7 @@ __device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, floa
   s.best = -1;
   s.cur = 0;
   s.sp = 0;
-  while (!trace_step<false, false>(bvh, s, stack, err, nullptr)) {
+  while (!trace_step<false, false, SPH>(bvh, s, stack, err, nullptr)) {
   }
   *t_out = s.best_t;
   return s.best;
@@ -267,18 +299,20 @@ __device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, floa
 // crossings one query at a time with tnear = the previous crossing drops repeated hits at
 // the same distance, as the reference's (geometry, t) de-duplication does for the two
 // triangles that share an edge the ray passes through.
+template <bool SPH>
 __device__ __forceinline__ int next_crossing(const DevScene& sc, const RayPre& r, float tnear, float tfar,
                                              float* t_out, unsigned int* err) {
   if (sc.num_vol_tris == 0) return -1;
-  return next_hit(volume_bvh(sc), r, tnear, tfar, t_out, err);
+  return next_hit<SPH>(volume_bvh(sc), r, tnear, tfar, t_out, err);
 }
 
-// Winding normal and material of a medium-boundary triangle slot.
-__device__ __forceinline__ void crossing_info(const DevScene& sc, int slot, float3* ng, int* material) {
-  const float4 a = __ldg(&sc.vtris[3 * slot]);
-  const float4 b = __ldg(&sc.vtris[3 * slot + 1]);
-  const float4 c = __ldg(&sc.vtris[3 * slot + 2]);
-  *ng = cross3(xyz(b) - xyz(a), xyz(c) - xyz(a));
+// Winding normal (a sphere's: outward at o + t d) and material of a slot.
+__device__ __forceinline__ void crossing_info(const float4* tris, int slot, float3 o, float3 d, float t, float3* ng,
+                                              int* material) {
+  const float4 a = __ldg(&tris[3 * slot]);
+  const float4 b = __ldg(&tris[3 * slot + 1]);
+  const float4 c = __ldg(&tris[3 * slot + 2]);
+  *ng = __float_as_int(c.w) != 0 ? (o + d * t) - xyz(a) : cross3(xyz(b) - xyz(a), xyz(c) - xyz(a));
   *material = __float_as_int(b.w);
 }
 
@@ -366,8 +400,7 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
     sf = unit >= 0 ? f3(pdf_eye, pdf_eye, pdf_eye) : f3(0.f, 0.f, 0.f);
   } else if (eye.is_volume) {
     // EvaluateScatterCoordinateOfScatterer, volume branch: sigma_s x phase function.
-    pdf_eye = phase_eval(*eye.med, eye.wi, d);
-    sf = eye.sigma_s * pdf_eye;
+    sf = mul(eye.sigma_s, medium_phase_eval(*eye.med, eye.pos, eye.wi, d, l, &pdf_eye));
   } else {
     sf = eval_bsdf(*eye.mat, eye.wi, eye.surf, d, l, &pdf_eye) * bsdf_correction(eye.surf, d);
   }
@@ -394,11 +427,21 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
 }
 
 // Completes an area light sample: position, winding normal, error bound and pdf.  The
-// vertices come from the per-light table (area light order), not from the leaf slots.
+// vertices come from the per-light table (area light order), not from the leaf slots.  A
+// sphere light (a.w = 1: centre a.xyz, radius b.x) takes L.coord as a uniform direction
+// (Spheres::SampleUniformPosition, primitive.cxx:193-203).
 __device__ __forceinline__ void resolve_area(const DevScene& sc, int light_index, LightNode& L) {
   const float4 a = __ldg(&sc.area_verts[3 * light_index]);
   const float4 b = __ldg(&sc.area_verts[3 * light_index + 1]);
   const float4 c = __ldg(&sc.area_verts[3 * light_index + 2]);
+  if (a.w != 0.f) {
+    const float3 off = L.coord * b.x;
+    L.coord = xyz(a) + off;
+    L.ng = normalize3(off);
+    L.bounds = abs3(L.coord) * gamma5();
+    L.pdf = (sc.type_probs[1] / sc.num_area_lights) * (1.f / (b.x * b.x * 4.f * kPi));
+    return;
+  }
   const float3 p0 = xyz(a), p1 = xyz(b), p2 = xyz(c);
   const float3 w = L.coord;
   L.coord = p0 * w.x + p1 * w.y + p2 * w.z;
@@ -444,7 +487,7 @@ __device__ __forceinline__ LightNode pick_light(const DevScene& sc, Rng& rng, La
     rng.square(r);
     L.type = LIGHT_AREA;
     L.prim = __ldg(&sc.area_lights[i]);
-    L.coord = to_triangle_barycentric(r);
+    L.coord = __ldg(&sc.area_verts[3 * i]).w != 0.f ? to_uniform_sphere(r) : to_triangle_barycentric(r);
     resolve_area(sc, i, L);
   }
   return L;
@@ -457,12 +500,14 @@ __device__ __forceinline__ LightNode pick_light(const DevScene& sc, Rng& rng, La
 template <bool MEDIA>
 __device__ __forceinline__ void emit_shadow(const DevScene& sc, const PathState& p, int qbounce, int slot,
                                             const Connection& c, const LightNode& L, float3 beta, float scale,
-                                            int target, const MTracker& mt) {
+                                            int target, const MTracker& mt, const Rng& rng) {
   float3 contrib;
   if (MEDIA) {
     contrib = mul(c.weight, beta) * (scale / L.pdf);
     const bool mis_on = !L.delta && sc.sample_bsdf && sc.sample_lights;
-    p.sh_mis[slot] = make_float2(mis_on ? L.pdf : -1.f, c.pdf_due);
+    // The path's random state here seeds the shadow ray's own stream for ratio tracking.
+    p.sh_med[slot] = make_float4(mis_on ? L.pdf : -1.f, c.pdf_due, __uint_as_float((unsigned)(rng.state & 0xffffffffu)),
+                                 __uint_as_float((unsigned)(rng.state >> 32)));
     p.sh_track[slot] = store_tracker(mt);
   } else {
     const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
@@ -506,7 +551,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
         eye.pos = cam_pos;
         Connection c = connect(sc, eye, L, l);
         if (c.valid && c.unit >= 0)
-          emit_shadow<MEDIA>(sc, p, 0, i, c, L, beta, 1.f / (float)w.npix_total, c.unit, cam_mt);
+          emit_shadow<MEDIA>(sc, p, 0, i, c, L, beta, 1.f / (float)w.npix_total, c.unit, cam_mt, rng);
       }
     }
     // Camera ray (TakeRandomWalkStep from the camera node).
@@ -533,7 +578,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
 // Closest hit of the queued extension rays, one ray per thread over a grid-stride loop
 // sized to the SM count times the kernel's resident blocks.  (A persistent variant that
 // refilled finished lanes after every traversal step measured 20 % slower.)
-template <bool COUNT>
+template <bool COUNT, bool SPH>
 __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bounce, unsigned long long* counters) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
@@ -543,7 +588,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
     const float4 o = p.ray_o[slot], d = p.ray_d[slot];
     const RayPre r = prepare_ray(xyz(o), xyz(d));
     float t = 0.f, b1 = 0.f, b2 = 0.f;
-    const int hit = trace<false, COUNT>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
+    const int hit = trace<false, COUNT, SPH>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
     p.hit[slot] = make_float4(t, b1, b2, __int_as_float(hit));
   }
   if (COUNT) {
@@ -559,6 +604,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
 // distance, vol.xyz = sigma_s); otherwise the tracker ends past every crossing.  The
 // tracking weight multiplies the throughput, and vol.w receives the product of the
 // segments' mean transmittances (the pdf factor of PdfConversionFactor).
+template <bool SPH>
 __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
@@ -579,15 +625,16 @@ __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bou
     float3 sig_s = f3(0.f, 0.f, 0.f);
     for (int k = 0;; ++k) {
       float tc;
-      const int cs = next_crossing(sc, r, snear, vend, &tc, p.err);
+      const int cs = next_crossing<SPH>(sc, r, snear, vend, &tc, p.err);
       const float sfar = cs >= 0 ? tc : vend;
       const int m = mt.cur;
       if (m >= 0) {
         const DevMedium& M = sc.media[m];
-        const InteractionSample ms = sample_interaction(M, sfar - snear, weight, rng, l);
+        const float3 sorg = xyz(o) + xyz(d) * snear;
+        const InteractionSample ms = medium_interaction(M, sorg, xyz(d), sfar - snear, weight, rng, l);
         weight = mul(weight, ms.weight);
         interacted = ms.t < sfar - snear;
-        ctr *= segment_tr(M, interacted ? ms.t : sfar - snear, l);
+        ctr *= medium_segment_tr(M, sorg, xyz(d), interacted ? ms.t : sfar - snear, l);
         if (interacted) {
           h = make_float4(snear + ms.t, 0.f, 0.f, __int_as_float(-2 - m));
           sig_s = ms.sigma_s;
@@ -602,7 +649,7 @@ __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bou
       }
       float3 ng;
       int mat;
-      crossing_info(sc, cs, &ng, &mat);
+      crossing_info(sc.vtris, cs, xyz(o), xyz(d), sfar, &ng, &mat);
       going_through(sc, mt, xyz(d), ng, mat);
       snear = sfar;
     }
@@ -647,7 +694,9 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       vpos = xyz(p.ray_o[slot]) + dir * h.x;
     } else if (tri >= 0) {
       const float u = h.y, v = h.z;
-      s = make_surface(sc, tri, 1.f - u - v, u, v, f3(u, v, 1.f - u - v));
+      const bool sphere = sc.num_spheres > 0 && is_sphere_slot(sc.tris, tri);
+      s = sphere ? sphere_hit_surface(sc.tris, tri, xyz(p.ray_o[slot]), dir, h.x)
+                 : make_surface(sc, tri, 1.f - u - v, u, v, f3(u, v, 1.f - u - v));
       orient(s, dir);
       const DevMaterial& m = sc.materials[s.material];
       if (sc.sample_bsdf && m.emissive) {
@@ -655,7 +704,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
         const float vis = dot3(s.ng, -dir) > 0.f ? 1.f : 0.f;
         const float3 end_weight = take(m.emission, l) * (vis / (2.f * kPi));
         const float4 a = __ldg(&sc.tris[3 * tri]), b = __ldg(&sc.tris[3 * tri + 1]), c = __ldg(&sc.tris[3 * tri + 2]);
-        const float area = tri_area(xyz(a), xyz(b), xyz(c));
+        const float area = __float_as_int(c.w) != 0 ? b.x * b.x * 4.f * kPi : tri_area(xyz(a), xyz(b), xyz(c));
         const float pdf_direct = (1.f / area) * sc.type_probs[1] * sc.in_class_area;
         const float dfac = fabsf(dot3(s.ng, dir));
         float pdf_due = prev_delta ? dfac * prev_pdf : dfac / (h.x * h.x + kEps) * prev_pdf;
@@ -712,7 +761,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
               smt = mt;
               if (!is_volume && dot3(c.dir, s.n) < 0.f) going_through(sc, smt, c.dir, s.ng, s.material);
             }
-            emit_shadow<MEDIA>(sc, p, bounce + 1, slot, c, L, beta, 1.f, -1, smt);
+            emit_shadow<MEDIA>(sc, p, bounce + 1, slot, c, L, beta, 1.f, -1, smt, rng);
           }
         }
       }
@@ -722,8 +771,11 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       float pdf;
       bool delta;
       if (is_volume) {
-        ndir = phase_sample(sc.media[medium], wi, rng, &pdf);
-        bf = xyz(vol);  // sigma_s x phase / phase pdf
+        const DevMedium& M = sc.media[medium];
+        float3 pval;
+        ndir = medium_phase_sample(M, vpos, wi, rng, l, &pval, &pdf);
+        // sigma_s x phase value / pdf; a single phase function's value is its pdf.
+        bf = M.kind == TT_MEDIUM_ATMOSPHERE ? mul(xyz(vol), pval) * (1.f / pdf) : xyz(vol);
         delta = false;
         org = vpos;
       } else {
@@ -768,7 +820,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
 // media scenes the contribution is multiplied by the transmittance through the media
 // between the medium-boundary crossings (TransmittanceEstimate, rendering_util.cxx:40-67)
 // and by the MIS weight that the segment's transmittance pdf factor completes.
-template <bool MEDIA, bool COUNT>
+template <bool MEDIA, bool COUNT, bool SPH>
 __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Framebuffer fb, int bounce,
                                                 unsigned long long* counters) {
   const int n = *sh_count(p, bounce);
@@ -778,7 +830,7 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
     const float4 o = p.sh_o[slot], d = p.sh_d[slot];
     const RayPre r = prepare_ray(xyz(o), xyz(d));
     float t, b1, b2;
-    const int hit = trace<true, COUNT>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
+    const int hit = trace<true, COUNT, SPH>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
     if (hit >= 0) continue;
     const float4 c4 = p.sh_c[slot];
     float3 c = xyz(c4);
@@ -786,16 +838,20 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
     if (MEDIA) {
       const Lambda l = unpack_lambda(p.meta[slot].y);
       MTracker mt = load_tracker(p.sh_track[slot]);
+      const float4 med = p.sh_med[slot];
+      Rng srng;
+      srng.seed_path(((unsigned long long)__float_as_uint(med.w) << 32) | __float_as_uint(med.z), p.rng_inc[slot]);
       float3 T = f3(1.f, 1.f, 1.f);
       float ctr = 1.f, snear = 0.f;
       for (int k = 0;; ++k) {
         float tc;
-        const int cs = next_crossing(sc, r, snear, o.w, &tc, p.err);
+        const int cs = next_crossing<SPH>(sc, r, snear, o.w, &tc, p.err);
         const float sfar = cs >= 0 ? tc : o.w;
         if (mt.cur >= 0) {
-          const float3 e = exp_neg(take(sc.media[mt.cur].sigma_ext, l), sfar - snear);
-          T = mul(T, e);
-          ctr *= mean3(e);
+          const DevMedium& M = sc.media[mt.cur];
+          const float3 sorg = xyz(o) + xyz(d) * snear;
+          ctr *= medium_segment_tr(M, sorg, xyz(d), sfar - snear, l);
+          T = mul(T, medium_transmission(M, sorg, xyz(d), sfar - snear, srng, l, p.err));
         }
         if (cs < 0) break;
         if (k >= kMaxCrossings) {
@@ -805,12 +861,11 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
         }
         float3 ng;
         int mat;
-        crossing_info(sc, cs, &ng, &mat);
+        crossing_info(sc.vtris, cs, xyz(o), xyz(d), sfar, &ng, &mat);
         going_through(sc, mt, xyz(d), ng, mat);
         snear = sfar;
       }
-      const float2 mi = p.sh_mis[slot];
-      const float mis = mi.x < 0.f ? 1.f : power_heuristic(mi.x, mi.y * ctr);
+      const float mis = med.x < 0.f ? 1.f : power_heuristic(med.x, med.y * ctr);
       c = mul(c, T) * mis;
     }
     if (target < 0) {
@@ -847,12 +902,12 @@ __global__ void k_init_tracker(DevScene sc, float3 pos, float3 lo, float3 hi, ui
       float t = 0.f;
       for (int k = 0; k < kMaxCrossings; ++k) {
         float tc;
-        const int slot = next_hit(bvh, r, t, go, &tc, err);
+        const int slot = next_hit<true>(bvh, r, t, go, &tc, err);
         if (slot < 0) break;
-        const float4 a = __ldg(&bvh.tris[3 * slot]);
-        const float4 b = __ldg(&bvh.tris[3 * slot + 1]);
-        const float4 c = __ldg(&bvh.tris[3 * slot + 2]);
-        going_through(sc, mt, dir, cross3(xyz(b) - xyz(a), xyz(c) - xyz(a)), __float_as_int(b.w));
+        float3 ng;
+        int mat;
+        crossing_info(bvh.tris, slot, r.o, dir, tc, &ng, &mat);
+        going_through(sc, mt, dir, ng, mat);
         t = tc;
       }
     }
@@ -884,6 +939,7 @@ __global__ void k_accumulate(Framebuffer fb, double* acc, double* light, int n3)
 
 // ----------------------------------------------------------------------------------------
 // Batch queries and shader sampling for the parity tests.
+template <bool SPH>
 __global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* prim, float* t, float* u, float* v,
                                  unsigned int* err) {
   TraceCounters cnt{0u, 0u};
@@ -891,7 +947,7 @@ __global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* pri
     const float* r = rays + 8 * (size_t)i;
     const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
     float tt = -1.f, b1 = 0.f, b2 = 0.f;
-    const int slot = trace<false, false>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
+    const int slot = trace<false, false, SPH>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
     prim[i] = slot >= 0 ? __float_as_int(__ldg(&sc.tris[3 * slot]).w) : -1;
     t[i] = slot >= 0 ? tt : -1.f;
     u[i] = b1;
@@ -899,16 +955,18 @@ __global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* pri
   }
 }
 
+template <bool SPH>
 __global__ void k_occluded_rays(DevScene sc, const float* rays, int n, unsigned char* occ, unsigned int* err) {
   TraceCounters cnt{0u, 0u};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float* r = rays + 8 * (size_t)i;
     const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
     float tt, b1, b2;
-    occ[i] = trace<true, false>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt) >= 0 ? 1 : 0;
+    occ[i] = trace<true, false, SPH>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt) >= 0 ? 1 : 0;
   }
 }
 
+template <bool SPH>
 __global__ void k_count_rays(DevScene sc, const float* rays, int n, unsigned long long* counters,
                              unsigned int* err) {
   TraceCounters cnt{0u, 0u};
@@ -916,7 +974,7 @@ __global__ void k_count_rays(DevScene sc, const float* rays, int n, unsigned lon
     const float* r = rays + 8 * (size_t)i;
     const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
     float tt, b1, b2;
-    trace<false, true>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
+    trace<false, true, SPH>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
   }
   atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
   atomicAdd(&counters[1], (unsigned long long)cnt.tris);
@@ -983,8 +1041,8 @@ static int trace_grid() {
     int dev = 0, sms = 0, b0 = 0, b1 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false>, kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false, false>, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false, false>, kBlock, 0);
     g = sms * (b0 < b1 ? b0 : b1);
     if (g < 1) g = 1;
   }
@@ -999,8 +1057,14 @@ void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& f
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
                    cudaStream_t st) {
   grid = trace_grid();
-  if (count) k_extend<true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
-  else k_extend<false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+  const bool sph = s.num_spheres > 0;
+  if (count) {
+    if (sph) k_extend<true, true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+    else k_extend<true, false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+  } else {
+    if (sph) k_extend<false, true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+    else k_extend<false, false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+  }
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
   if (s.num_media > 0) k_shade<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
@@ -1009,16 +1073,30 @@ void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, c
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
   grid = trace_grid();
+  const bool sph = s.num_spheres > 0;
+  // Media and sphere variants are launched only for scenes that have them; the surface-
+  // and triangle-only variant keeps the traversal lean for mesh scenes.
   if (s.num_media > 0) {
-    if (count) k_shadow<true, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-    else k_shadow<true, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    if (sph) {
+      if (count) k_shadow<true, true, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+      else k_shadow<true, false, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    } else {
+      if (count) k_shadow<true, true, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+      else k_shadow<true, false, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    }
   } else {
-    if (count) k_shadow<false, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-    else k_shadow<false, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    if (sph) {
+      if (count) k_shadow<false, true, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+      else k_shadow<false, false, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    } else {
+      if (count) k_shadow<false, true, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+      else k_shadow<false, false, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+    }
   }
 }
 void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
-  k_track<<<grid, kBlock, 0, st>>>(s, p, bounce);
+  if (s.num_spheres > 0) k_track<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
+  else k_track<false><<<grid, kBlock, 0, st>>>(s, p, bounce);
 }
 void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_hi, uint2* out, unsigned int* err,
                          cudaStream_t st) {
@@ -1037,15 +1115,21 @@ static int grid_for(int n) {
 }
 void launch_intersect_rays(const DevScene& s, const float* rays, int n, int* prim, float* t, float* u, float* v,
                            unsigned int* err, cudaStream_t st) {
-  if (n > 0) k_intersect_rays<<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v, err);
+  if (n <= 0) return;
+  if (s.num_spheres > 0) k_intersect_rays<true><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v, err);
+  else k_intersect_rays<false><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v, err);
 }
 void launch_occluded_rays(const DevScene& s, const float* rays, int n, unsigned char* occ, unsigned int* err,
                           cudaStream_t st) {
-  if (n > 0) k_occluded_rays<<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
+  if (n <= 0) return;
+  if (s.num_spheres > 0) k_occluded_rays<true><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
+  else k_occluded_rays<false><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
 }
 void launch_count_rays(const DevScene& s, const float* rays, int n, unsigned long long* counters, unsigned int* err,
                        cudaStream_t st) {
-  if (n > 0) k_count_rays<<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
+  if (n <= 0) return;
+  if (s.num_spheres > 0) k_count_rays<true><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
+  else k_count_rays<false><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
 }
 void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, int n, unsigned long long seed,
                         float* dir, float* val, float* pdf, cudaStream_t st) {

@@ -11,7 +11,7 @@
 // Limits and sharing:
 //  - at most kNoAllocMaxPaths = 65,536 camera samples (spp x pixels) per call, and
 //    max_ray_depth <= kNoAllocMaxDepth; larger requests return TT_ERR_CAPACITY;
-//  - the scratch array (about 14.2 MB) is part of the library image, so every GPU that
+//  - the scratch array (about 14.7 MB) is part of the library image, so every GPU that
 //    loads the library holds it until the process exits;
 //  - all calls on a device share the one array: calls that overlap on the GPU (different
 //    streams or host threads without ordering) race and corrupt each other;
@@ -36,11 +36,11 @@ constexpr int kNoAllocMaxPaths = 1 << 16;
 constexpr int kNoAllocMaxDepth = 1000;
 constexpr int kNoAllocMaxDevices = 64;
 
-// Per-path bytes: 9 float4 + 1 uint4 + 2 u64 + 2 uint2 + 1 float2 + 4 int queues = 216 B
-// (the medium-tracking arrays are carved for every scene); each of the 21 arrays is padded
-// to a 256-byte boundary.
-constexpr size_t kPathBytes = 9 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(unsigned long long) +
-                              2 * sizeof(uint2) + sizeof(float2) + 4 * sizeof(int);
+// Per-path bytes: 10 float4 + 1 uint4 + 2 u64 + 2 uint2 + 4 int queues = 224 B (the
+// medium-tracking arrays are carved for every scene); each of the 21 arrays is padded to a
+// 256-byte boundary.
+constexpr size_t kPathBytes = 10 * sizeof(float4) + sizeof(uint4) + 2 * sizeof(unsigned long long) +
+                              2 * sizeof(uint2) + 4 * sizeof(int);
 constexpr size_t kCounterBytes = (size_t)kCountersPerBounce * (kNoAllocMaxDepth + 3) * sizeof(int);
 constexpr size_t kErrBytes = 256;
 constexpr size_t kPadBytes = 21 * 256;
@@ -93,7 +93,7 @@ PathState carve(unsigned char* base, int cap) {
   p.track = (uint2*)take(n * sizeof(uint2));
   p.vol = (float4*)take(n * sizeof(float4));
   p.sh_track = (uint2*)take(n * sizeof(uint2));
-  p.sh_mis = (float2*)take(n * sizeof(float2));
+  p.sh_med = (float4*)take(n * sizeof(float4));
   p.counters = (int*)take(kCounterBytes);
   p.err = (unsigned int*)take(kErrBytes);
   return p;

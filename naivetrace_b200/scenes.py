@@ -357,6 +357,17 @@ def planet_atmosphere(xres=64, yres=64, radius=6371.0, camera_height=0.002, sun_
     return s
 
 
+def planet_from_space(xres=64, yres=64, distance=5.0) -> Scene:
+    """The planet of planet_atmosphere seen from `distance` planet radii away with a 30
+    degree pinhole camera: rays enter the atmosphere from empty space."""
+    s = planet_atmosphere(xres, yres, camera_kind=abi.CAMERA_PINHOLE)
+    s.name = "planet_from_space"
+    R = 6371.0
+    s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(-distance * R * 0.8, distance * R * 0.6, 0.0),
+                          dir=(0.8, -0.6, 0.0), up=(0.0, 0.0, 1.0), fov_deg=30.0, xres=xres, yres=yres)
+    return s
+
+
 def spheres_box(xres=64, yres=64) -> Scene:
     """The Cornell box with analytic spheres: a mirror sphere, a glass sphere filled with
     a homogeneous medium, a diffuse sphere, and a small emissive sphere as a second light."""

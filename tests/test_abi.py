@@ -36,16 +36,16 @@ def test_library_exports_every_symbol(gpu_lib):
 def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text(f'#include "{HEADER}"\n#include <stdio.h>\n#include <stddef.h>\n'
-                   "int main(){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
+                   "int main(){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n\","
                    "sizeof(tt_material),sizeof(tt_env_light),sizeof(tt_point_light),sizeof(tt_camera),"
                    "sizeof(tt_scene_desc),sizeof(tt_params),sizeof(tt_stats),offsetof(tt_scene_desc,camera),"
-                   "offsetof(tt_env_light,tex_rgb));return 0;}\n")
+                   "offsetof(tt_env_light,tex_rgb),sizeof(tt_medium),offsetof(tt_medium,sigma_t));return 0;}\n")
     exe = tmp_path / "sz"
     subprocess.run(["gcc", str(src), "-o", str(exe)], check=True)
     vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     mine = [C.sizeof(abi.Material), C.sizeof(abi.EnvLight), C.sizeof(abi.PointLight), C.sizeof(abi.Camera),
             C.sizeof(abi.SceneDesc), C.sizeof(abi.Params), C.sizeof(abi.Stats), abi.SceneDesc.camera.offset,
-            abi.EnvLight.tex_rgb.offset]
+            abi.EnvLight.tex_rgb.offset, C.sizeof(abi.Medium), abi.Medium.sigma_t.offset]
     assert vals == mine
 
 
