@@ -44,4 +44,26 @@ struct BvhOutput {
 // max_leaf <= 8.  Returns false on invalid input.
 bool build_bvh(const BvhInput& in, int max_leaf, BvhOutput* out);
 
+// 8-wide BVH with quantised child boxes (80 bytes per node), collapsed from the binary SAH
+// tree (leaves of at most 3 primitives).  Node words:
+//   0-2  origin p (float x, y, z) = lower corner of the node box
+//   3    exponents e_x, e_y, e_z (biased by 127) and the inner-child mask (bits 24-31)
+//   4    index of the first inner child node (inner children are consecutive, slot order)
+//   5    first primitive slot of the node's leaf children (consecutive, slot order)
+//   6-7  meta byte per child slot: leaf = (slot offset from word 5) << 2 | count (1..3),
+//        0 for inner and empty slots
+//   8-13 quantised lower bounds per axis (x: 8-9, y: 10-11, z: 12-13), one byte per slot
+//   14-19 quantised upper bounds (x: 14-15, y: 16-17, z: 18-19)
+// Child box = p + q * 2^e per axis, containing the child's exact box.  Slot s holds the
+// child nearest the box corner whose axes with bit set in s are on the + side, so that
+// visiting slot ^ octant(ray) in increasing order approximates near-to-far.  Primitive
+// slots as in the binary layout.
+struct Bvh8Output {
+  std::vector<uint32_t> nodes;  // 20 words per node
+  std::vector<float> tris;      // 12 floats per primitive slot
+  uint32_t num_nodes = 0;
+  uint32_t max_depth = 0;
+};
+bool build_bvh8(const BvhInput& in, Bvh8Output* out);
+
 }  // namespace tt

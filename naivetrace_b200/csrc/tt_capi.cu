@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -98,7 +99,7 @@ struct tt_ctx {
   int profiling = 0;
   tt_stats stats{};
   std::string err;
-  uint32_t bvh_nodes = 0, bvh_depth = 0;
+  uint32_t bvh_nodes = 0, bvh_depth = 0, bvh_node_bytes = 64;
 };
 
 static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
@@ -285,31 +286,48 @@ tt_status tt_upload_scene(tt_ctx* c) {
   bi.spheres = ssph.data();
   bi.sphere_material_ids = ssmat.data();
   bi.sphere_prim_ids = ssid.data();
-  BvhOutput bo;
-  if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
-  c->bvh_nodes = bo.num_nodes;
-  c->bvh_depth = bo.max_depth;
-  if (bo.max_depth + 2 >= (uint32_t)BVH_STACK)
-    return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
   BvhInput vbi{c->verts.data(), vidx.data(), vmat.data(), (uint32_t)vid.size(), vid.data()};
   vbi.num_spheres = (uint32_t)vsid.size();
   vbi.spheres = vsph.data();
   vbi.sphere_material_ids = vsmat.data();
   vbi.sphere_prim_ids = vsid.data();
-  BvhOutput vbo;
-  if (!build_bvh(vbi, 4, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
-  if (vbo.max_depth + 2 >= (uint32_t)BVH_STACK)
-    return fail(c, TT_ERR_CAPACITY, "medium-boundary BVH deeper than the traversal stack");
   auto upload = [&](const void* src, size_t bytes) -> void* {
     void* p = c->scene_mem.alloc(bytes);
     if (p && bytes) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
     return p;
   };
   DevScene& s = c->dev;
-  s.nodes = (const float4*)upload(bo.nodes.data(), bo.nodes.size() * sizeof(float));
-  s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
-  s.vnodes = (const float4*)upload(vbo.nodes.data(), vbo.nodes.size() * sizeof(float));
-  s.vtris = (const float4*)upload(vbo.tris.data(), vbo.tris.size() * sizeof(float));
+  // The 8-wide compressed BVH is the default layout; TT_BVH_WIDTH=2 selects the binary
+  // BVH (kept for comparison).
+  const char* width_env = std::getenv("TT_BVH_WIDTH");
+  s.wide = !(width_env && std::atoi(width_env) == 2);
+  if (s.wide) {
+    Bvh8Output bo, vbo;
+    if (!build_bvh8(bi, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
+    if (!build_bvh8(vbi, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
+    c->bvh_nodes = bo.num_nodes;
+    c->bvh_depth = bo.max_depth;
+    c->bvh_node_bytes = 80;
+    if (bo.max_depth + 2 >= (uint32_t)BVH8_STACK || vbo.max_depth + 2 >= (uint32_t)BVH8_STACK)
+      return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
+    s.nodes8 = (const uint4*)upload(bo.nodes.data(), bo.nodes.size() * sizeof(uint32_t));
+    s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
+    s.vnodes8 = (const uint4*)upload(vbo.nodes.data(), vbo.nodes.size() * sizeof(uint32_t));
+    s.vtris = (const float4*)upload(vbo.tris.data(), vbo.tris.size() * sizeof(float));
+  } else {
+    BvhOutput bo, vbo;
+    if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
+    if (!build_bvh(vbi, 4, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
+    c->bvh_nodes = bo.num_nodes;
+    c->bvh_depth = bo.max_depth;
+    c->bvh_node_bytes = 64;
+    if (bo.max_depth + 2 >= (uint32_t)BVH_STACK || vbo.max_depth + 2 >= (uint32_t)BVH_STACK)
+      return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
+    s.nodes = (const float4*)upload(bo.nodes.data(), bo.nodes.size() * sizeof(float));
+    s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
+    s.vnodes = (const float4*)upload(vbo.nodes.data(), vbo.nodes.size() * sizeof(float));
+    s.vtris = (const float4*)upload(vbo.tris.data(), vbo.tris.size() * sizeof(float));
+  }
   s.num_vol_tris = (int)(vid.size() + vsid.size());
   s.num_spheres = (int)nsph;
   // Per global primitive: vertex indices and material (spheres: material only).
@@ -1012,7 +1030,7 @@ tt_status tt_get_stats(tt_ctx* c, tt_stats* out) {
     out->error_flags |= errw;
   }
   out->bvh_nodes = c->bvh_nodes;
-  out->bvh_node_bytes = 64;
+  out->bvh_node_bytes = c->bvh_node_bytes;
   out->tri_bytes = 48;
   out->bvh_depth = c->bvh_depth;
   return TT_OK;

@@ -11,7 +11,8 @@ namespace tt {
 
 constexpr int NBINS = TT_NBINS;
 constexpr int MAX_ENV_LIGHTS = 4;
-constexpr int BVH_STACK = 64;        // per-thread traversal stack (entries)
+constexpr int BVH_STACK = 64;        // per-thread traversal stack (entries), binary BVH
+constexpr int BVH8_STACK = 32;       // per-thread stack of node groups, 8-wide BVH
 constexpr uint32_t ERR_STACK = 1u;   // error-word bits written by kernels
 constexpr uint32_t ERR_QUEUE = 2u;
 constexpr uint32_t ERR_CROSSINGS = 4u;  // a ray crossed more medium boundaries than the cap
@@ -74,8 +75,11 @@ struct DevCamera {
 
 // Everything a kernel needs to know about the scene; passed by value (constant bank).
 struct DevScene {
-  const float4* nodes;        // BVH2, 4 float4 per node
-  const float4* tris;         // 3 float4 per triangle in leaf order: v0 (w=prim), v1 (w=material), v2
+  int wide;                   // 1: the 8-wide BVH (nodes8 / vnodes8) is the active layout
+  const uint4* nodes8;        // 8-wide BVH, 5 uint4 per node (tt_bvh.h)
+  const uint4* vnodes8;
+  const float4* nodes;        // BVH2, 4 float4 per node (when wide == 0)
+  const float4* tris;         // 3 float4 per primitive slot of the active layout: v0 (w=prim), v1 (w=material), v2
   const uint4* tri_idx;       // per prim: vertex indices a, b, c and material
   const float* normals;       // per vertex xyz, or nullptr
   const DevMaterial* materials;

@@ -14,6 +14,8 @@
 // device-side count, so launch shapes are fixed (a multiple of the SM count).
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "tt_device.cuh"
 #include "tt_internal.h"
 #include "tt_tables.h"
@@ -237,10 +239,10 @@ __device__ __forceinline__ bool trace_step(const BvhRef& bvh, TraceState& s, int
 
 // Recomputes the distance of the closest hit from the plane equation in double precision
 // (float rounding of Ng.(v0 - o) is amplified by 1/|cos| at grazing incidence).
-__device__ __forceinline__ float refine_t(const DevScene& sc, const RayPre& r, int slot) {
-  const float4 a = __ldg(&sc.tris[3 * slot]);
-  const float4 b = __ldg(&sc.tris[3 * slot + 1]);
-  const float4 c = __ldg(&sc.tris[3 * slot + 2]);
+__device__ __forceinline__ float refine_t(const float4* tris, const RayPre& r, int slot) {
+  const float4 a = __ldg(&tris[3 * slot]);
+  const float4 b = __ldg(&tris[3 * slot + 1]);
+  const float4 c = __ldg(&tris[3 * slot + 2]);
   const double e1x = (double)b.x - a.x, e1y = (double)b.y - a.y, e1z = (double)b.z - a.z;
   const double e2x = (double)c.x - a.x, e2y = (double)c.y - a.y, e2z = (double)c.z - a.z;
   const double nx = e1y * e2z - e1z * e2y, ny = e1z * e2x - e1x * e2z, nz = e1x * e2y - e1y * e2x;
@@ -249,10 +251,144 @@ __device__ __forceinline__ float refine_t(const DevScene& sc, const RayPre& r, i
   return (float)((nx * ax + ny * ay + nz * az) / den);
 }
 
-// Whole traversal of one ray (batch queries).  Returns the triangle slot or -1.
+// ----------------------------------------------------------------------------------------
+// 8-wide BVH traversal (layout in tt_bvh.h), after the compressed wide BVH of Ylitie, Karras
+// and Laine (2017): one 80-byte node gives the quantised boxes of eight children; hit
+// inner children form a "node group" (first child index, inner mask, hit bits in
+// octant-permuted order) that is consumed nearest-first, with the rest pushed on a short
+// stack; hit leaf children form a primitive group tested right away.  Slab distances are
+// (p - o) / d + q * 2^e / d per axis, widened by 1 + 2 gamma(3) for conservative culling.
+
+// Maps bit s of an 8-bit mask to bit s ^ oct.
+__device__ __forceinline__ unsigned permute8(unsigned m, unsigned oct) {
+  if (oct & 1u) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
+  if (oct & 2u) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
+  if (oct & 4u) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
+  return m;
+}
+
+struct Trace8State {
+  uint2 ng;     // node group: x = first child node, y = inner mask << 8 | permuted hit bits
+  uint2 pg;     // primitive group: x = first slot, y = slots still to test (bit i = x + i)
+  int best, sp;
+  float tnear, best_t, b1, b2;
+};
+
+template <bool COUNT>
+__device__ __forceinline__ void visit_node8(const uint4* __restrict__ nodes, const RayPre& r, unsigned oct,
+                                            unsigned node, Trace8State& s, TraceCounters* cnt) {
+  const uint4* np = nodes + 5 * (size_t)node;
+  const uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+  if (COUNT) cnt->nodes++;
+  const float ax = (__uint_as_float(n0.x) - r.o.x) * r.id.x;
+  const float ay = (__uint_as_float(n0.y) - r.o.y) * r.id.y;
+  const float az = (__uint_as_float(n0.z) - r.o.z) * r.id.z;
+  const float sx = __uint_as_float((n0.w & 0xffu) << 23) * r.id.x;
+  const float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * r.id.y;
+  const float sz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * r.id.z;
+  const unsigned imask = n0.w >> 24;
+  // Near and far planes per axis follow the ray direction's signs.
+  const uint2 lox = make_uint2(n2.x, n2.y), loy = make_uint2(n2.z, n2.w), loz = make_uint2(n3.x, n3.y);
+  const uint2 hix = make_uint2(n3.z, n3.w), hiy = make_uint2(n4.x, n4.y), hiz = make_uint2(n4.z, n4.w);
+  const uint2 nx = (oct & 1u) ? hix : lox, fx = (oct & 1u) ? lox : hix;
+  const uint2 ny = (oct & 2u) ? hiy : loy, fy = (oct & 2u) ? loy : hiy;
+  const uint2 nz = (oct & 4u) ? hiz : loz, fz = (oct & 4u) ? loz : hiz;
+  unsigned hits = 0u;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const unsigned sh = 8u * (unsigned)(c & 3);
+    const unsigned wnx = c < 4 ? nx.x : nx.y, wny = c < 4 ? ny.x : ny.y, wnz = c < 4 ? nz.x : nz.y;
+    const unsigned wfx = c < 4 ? fx.x : fx.y, wfy = c < 4 ? fy.x : fy.y, wfz = c < 4 ? fz.x : fz.y;
+    const float tnx = fmaf((float)((wnx >> sh) & 0xffu), sx, ax);
+    const float tny = fmaf((float)((wny >> sh) & 0xffu), sy, ay);
+    const float tnz = fmaf((float)((wnz >> sh) & 0xffu), sz, az);
+    const float tfx = fmaf((float)((wfx >> sh) & 0xffu), sx, ax);
+    const float tfy = fmaf((float)((wfy >> sh) & 0xffu), sy, ay);
+    const float tfz = fmaf((float)((wfz >> sh) & 0xffu), sz, az);
+    const float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tnear));
+    const float tmax = fminf(fminf(tfx, tfy), fminf(tfz, s.best_t)) * 1.0000011f;
+    hits |= (tmin <= tmax ? 1u : 0u) << c;
+  }
+  // Leaf children (nonzero meta bytes) that were hit contribute their primitive slots.
+  unsigned prims = 0u;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const unsigned m = ((c < 4 ? n1.z : n1.w) >> (8u * (unsigned)(c & 3))) & 0xffu;
+    if (m != 0u && ((hits >> c) & 1u)) prims |= ((1u << (m & 3u)) - 1u) << (m >> 2);
+  }
+  s.ng = make_uint2(n1.x, (imask << 8) | permute8(hits & imask, oct));
+  s.pg = make_uint2(n1.y, prims);
+}
+
 template <bool ANY, bool COUNT, bool SPH>
+__device__ __forceinline__ void trace8_run(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
+                                           const RayPre& r, Trace8State& s, unsigned int* err, TraceCounters* cnt) {
+  const unsigned oct = (r.d.x < 0.f ? 1u : 0u) | (r.d.y < 0.f ? 2u : 0u) | (r.d.z < 0.f ? 4u : 0u);
+  uint2 stack[BVH8_STACK];
+  s.ng = make_uint2(0u, (1u << 8) | (1u << oct));  // the root as the single inner child of slot 0
+  s.pg = make_uint2(0u, 0u);
+  s.sp = 0;
+  for (;;) {
+    if (s.ng.y & 0xffu) {
+      const unsigned p = (unsigned)__ffs(s.ng.y & 0xffu) - 1u;
+      const unsigned slot = p ^ oct;
+      const unsigned node = s.ng.x + (unsigned)__popc((s.ng.y >> 8) & ((1u << slot) - 1u));
+      s.ng.y &= ~(1u << p);
+      if (s.ng.y & 0xffu) {
+        if (s.sp >= BVH8_STACK) {
+          atomicOr(err, ERR_STACK);
+          s.best = -1;
+          return;
+        }
+        stack[s.sp++] = s.ng;
+      }
+      visit_node8<COUNT>(nodes, r, oct, node, s, cnt);
+    }
+    while (s.pg.y) {
+      const int k = __ffs(s.pg.y) - 1;
+      s.pg.y &= s.pg.y - 1u;
+      const int i = (int)s.pg.x + k;
+      const float4 a = __ldg(&tris[3 * i]);
+      const float4 b = __ldg(&tris[3 * i + 1]);
+      const float4 c = __ldg(&tris[3 * i + 2]);
+      if (COUNT) cnt->tris++;
+      float t, b1 = 0.f, b2 = 0.f;
+      bool hit;
+      if (SPH && __float_as_int(c.w) != 0) hit = intersect_sphere(r, a, b, s.tnear, s.best_t, &t);
+      else hit = intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2);
+      if (hit) {
+        s.best = i;
+        s.best_t = t;
+        s.b1 = b1;
+        s.b2 = b2;
+        if (ANY) return;
+      }
+    }
+    if (!(s.ng.y & 0xffu)) {
+      if (s.sp == 0) return;
+      s.ng = stack[--s.sp];
+    }
+  }
+}
+
+// Whole traversal of one ray (batch queries).  Returns the triangle slot or -1.
+template <bool ANY, bool COUNT, bool SPH, bool WIDE>
 __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float tnear, float tfar, float* t_out,
                                      float* b1_out, float* b2_out, unsigned int* err, TraceCounters* cnt) {
+  if (WIDE) {
+    Trace8State s;
+    s.tnear = tnear;
+    s.best_t = tfar;
+    s.best = -1;
+    s.b1 = s.b2 = 0.f;
+    trace8_run<ANY, COUNT, SPH>(sc.nodes8, sc.tris, r, s, err, cnt);
+    if (s.best >= 0) {
+      *t_out = (ANY || (SPH && is_sphere_slot(sc.tris, s.best))) ? s.best_t : refine_t(sc.tris, r, s.best);
+      *b1_out = s.b1;
+      *b2_out = s.b2;
+    }
+    return s.best;
+  }
   const BvhRef bvh = surface_bvh(sc);
   TraceState s;
   int stack[BVH_STACK];
@@ -266,7 +402,7 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
   while (!trace_step<ANY, COUNT, SPH>(bvh, s, stack, err, cnt)) {
   }
   if (s.best >= 0) {
-    *t_out = (ANY || (SPH && is_sphere_slot(sc.tris, s.best))) ? s.best_t : refine_t(sc, r, s.best);
+    *t_out = (ANY || (SPH && is_sphere_slot(sc.tris, s.best))) ? s.best_t : refine_t(sc.tris, r, s.best);
     *b1_out = s.b1;
     *b2_out = s.b2;
   }
@@ -276,6 +412,19 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
 // Nearest hit with tnear < t <= tfar in `bvh`, with the single-precision plane distance
 // (no refinement, so that the next query can start exactly at the returned t).  Returns
 // the triangle slot or -1.
+template <bool SPH>
+__device__ __forceinline__ int next_hit8(const uint4* nodes, const float4* tris, const RayPre& r, float tnear,
+                                         float tfar, float* t_out, unsigned int* err) {
+  Trace8State s;
+  s.tnear = tnear;
+  s.best_t = tfar;
+  s.best = -1;
+  s.b1 = s.b2 = 0.f;
+  trace8_run<false, false, SPH>(nodes, tris, r, s, err, nullptr);
+  *t_out = s.best_t;
+  return s.best;
+}
+
 template <bool SPH>
 __device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, float tnear, float tfar, float* t_out,
                                         unsigned int* err) {
@@ -299,10 +448,11 @@ __device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, floa
 // crossings one query at a time with tnear = the previous crossing drops repeated hits at
 // the same distance, as the reference's (geometry, t) de-duplication does for the two
 // triangles that share an edge the ray passes through.
-template <bool SPH>
+template <bool SPH, bool WIDE>
 __device__ __forceinline__ int next_crossing(const DevScene& sc, const RayPre& r, float tnear, float tfar,
                                              float* t_out, unsigned int* err) {
   if (sc.num_vol_tris == 0) return -1;
+  if (WIDE) return next_hit8<SPH>(sc.vnodes8, sc.vtris, r, tnear, tfar, t_out, err);
   return next_hit<SPH>(volume_bvh(sc), r, tnear, tfar, t_out, err);
 }
 
@@ -578,7 +728,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
 // Closest hit of the queued extension rays, one ray per thread over a grid-stride loop
 // sized to the SM count times the kernel's resident blocks.  (A persistent variant that
 // refilled finished lanes after every traversal step measured 20 % slower.)
-template <bool COUNT, bool SPH>
+template <bool COUNT, bool SPH, bool WIDE>
 __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bounce, unsigned long long* counters) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
@@ -588,7 +738,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
     const float4 o = p.ray_o[slot], d = p.ray_d[slot];
     const RayPre r = prepare_ray(xyz(o), xyz(d));
     float t = 0.f, b1 = 0.f, b2 = 0.f;
-    const int hit = trace<false, COUNT, SPH>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
+    const int hit = trace<false, COUNT, SPH, WIDE>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
     p.hit[slot] = make_float4(t, b1, b2, __int_as_float(hit));
   }
   if (COUNT) {
@@ -604,7 +754,7 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
 // distance, vol.xyz = sigma_s); otherwise the tracker ends past every crossing.  The
 // tracking weight multiplies the throughput, and vol.w receives the product of the
 // segments' mean transmittances (the pdf factor of PdfConversionFactor).
-template <bool SPH>
+template <bool SPH, bool WIDE>
 __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
@@ -625,7 +775,7 @@ __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bou
     float3 sig_s = f3(0.f, 0.f, 0.f);
     for (int k = 0;; ++k) {
       float tc;
-      const int cs = next_crossing<SPH>(sc, r, snear, vend, &tc, p.err);
+      const int cs = next_crossing<SPH, WIDE>(sc, r, snear, vend, &tc, p.err);
       const float sfar = cs >= 0 ? tc : vend;
       const int m = mt.cur;
       if (m >= 0) {
@@ -820,7 +970,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
 // media scenes the contribution is multiplied by the transmittance through the media
 // between the medium-boundary crossings (TransmittanceEstimate, rendering_util.cxx:40-67)
 // and by the MIS weight that the segment's transmittance pdf factor completes.
-template <bool MEDIA, bool COUNT, bool SPH>
+template <bool MEDIA, bool COUNT, bool SPH, bool WIDE>
 __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Framebuffer fb, int bounce,
                                                 unsigned long long* counters) {
   const int n = *sh_count(p, bounce);
@@ -830,7 +980,7 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
     const float4 o = p.sh_o[slot], d = p.sh_d[slot];
     const RayPre r = prepare_ray(xyz(o), xyz(d));
     float t, b1, b2;
-    const int hit = trace<true, COUNT, SPH>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
+    const int hit = trace<true, COUNT, SPH, WIDE>(sc, r, 0.f, o.w, &t, &b1, &b2, p.err, &cnt);
     if (hit >= 0) continue;
     const float4 c4 = p.sh_c[slot];
     float3 c = xyz(c4);
@@ -845,7 +995,7 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
       float ctr = 1.f, snear = 0.f;
       for (int k = 0;; ++k) {
         float tc;
-        const int cs = next_crossing<SPH>(sc, r, snear, o.w, &tc, p.err);
+        const int cs = next_crossing<SPH, WIDE>(sc, r, snear, o.w, &tc, p.err);
         const float sfar = cs >= 0 ? tc : o.w;
         if (mt.cur >= 0) {
           const DevMedium& M = sc.media[mt.cur];
@@ -899,10 +1049,12 @@ __global__ void k_init_tracker(DevScene sc, float3 pos, float3 lo, float3 hi, ui
     const RayPre r = prepare_ray(f3(pos.x + go, pos.y, pos.z), dir);
     for (int pass = 0; pass < 2; ++pass) {
       const BvhRef bvh = pass == 0 ? volume_bvh(sc) : surface_bvh(sc);
+      const uint4* nodes8 = pass == 0 ? sc.vnodes8 : sc.nodes8;
       float t = 0.f;
       for (int k = 0; k < kMaxCrossings; ++k) {
         float tc;
-        const int slot = next_hit<true>(bvh, r, t, go, &tc, err);
+        const int slot = sc.wide ? next_hit8<true>(nodes8, bvh.tris, r, t, go, &tc, err)
+                                 : next_hit<true>(bvh, r, t, go, &tc, err);
         if (slot < 0) break;
         float3 ng;
         int mat;
@@ -939,7 +1091,7 @@ __global__ void k_accumulate(Framebuffer fb, double* acc, double* light, int n3)
 
 // ----------------------------------------------------------------------------------------
 // Batch queries and shader sampling for the parity tests.
-template <bool SPH>
+template <bool SPH, bool WIDE>
 __global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* prim, float* t, float* u, float* v,
                                  unsigned int* err) {
   TraceCounters cnt{0u, 0u};
@@ -947,7 +1099,7 @@ __global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* pri
     const float* r = rays + 8 * (size_t)i;
     const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
     float tt = -1.f, b1 = 0.f, b2 = 0.f;
-    const int slot = trace<false, false, SPH>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
+    const int slot = trace<false, false, SPH, WIDE>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
     prim[i] = slot >= 0 ? __float_as_int(__ldg(&sc.tris[3 * slot]).w) : -1;
     t[i] = slot >= 0 ? tt : -1.f;
     u[i] = b1;
@@ -955,18 +1107,18 @@ __global__ void k_intersect_rays(DevScene sc, const float* rays, int n, int* pri
   }
 }
 
-template <bool SPH>
+template <bool SPH, bool WIDE>
 __global__ void k_occluded_rays(DevScene sc, const float* rays, int n, unsigned char* occ, unsigned int* err) {
   TraceCounters cnt{0u, 0u};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float* r = rays + 8 * (size_t)i;
     const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
     float tt, b1, b2;
-    occ[i] = trace<true, false, SPH>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt) >= 0 ? 1 : 0;
+    occ[i] = trace<true, false, SPH, WIDE>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt) >= 0 ? 1 : 0;
   }
 }
 
-template <bool SPH>
+template <bool SPH, bool WIDE>
 __global__ void k_count_rays(DevScene sc, const float* rays, int n, unsigned long long* counters,
                              unsigned int* err) {
   TraceCounters cnt{0u, 0u};
@@ -974,7 +1126,7 @@ __global__ void k_count_rays(DevScene sc, const float* rays, int n, unsigned lon
     const float* r = rays + 8 * (size_t)i;
     const RayPre rp = prepare_ray(f3(r[0], r[1], r[2]), f3(r[4], r[5], r[6]));
     float tt, b1, b2;
-    trace<false, true, SPH>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
+    trace<false, true, SPH, WIDE>(sc, rp, r[3], r[7], &tt, &b1, &b2, err, &cnt);
   }
   atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
   atomicAdd(&counters[1], (unsigned long long)cnt.tris);
@@ -1034,19 +1186,32 @@ void upload_constant_tables() {
 
 constexpr int kBlock = 256;
 
-// Traversal grid: every SM filled to the traversal kernels' occupancy limit.
-static int trace_grid() {
-  static int g = 0;
-  if (g == 0) {
+// Calls f with std::integral_constant<bool, b>: picks a kernel instantiation at run time.
+template <class F>
+static void with_bool(bool b, F&& f) {
+  if (b) f(std::true_type{});
+  else f(std::false_type{});
+}
+
+// Traversal grid: every SM filled to the traversal kernels' occupancy limit (per layout).
+static int trace_grid(bool wide) {
+  static int g[2] = {0, 0};
+  int& gg = g[wide ? 1 : 0];
+  if (gg == 0) {
     int dev = 0, sms = 0, b0 = 0, b1 = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false, false>, kBlock, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false, false>, kBlock, 0);
-    g = sms * (b0 < b1 ? b0 : b1);
-    if (g < 1) g = 1;
+    if (wide) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false, false, true>, kBlock, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false, false, true>, kBlock, 0);
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false, false, false>, kBlock, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false, false, false>, kBlock, 0);
+    }
+    gg = sms * (b0 < b1 ? b0 : b1);
+    if (gg < 1) gg = 1;
   }
-  return g;
+  return gg;
 }
 
 void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
@@ -1056,15 +1221,14 @@ void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& f
 }
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
                    cudaStream_t st) {
-  grid = trace_grid();
-  const bool sph = s.num_spheres > 0;
-  if (count) {
-    if (sph) k_extend<true, true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
-    else k_extend<true, false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
-  } else {
-    if (sph) k_extend<false, true><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
-    else k_extend<false, false><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
-  }
+  grid = trace_grid(s.wide != 0);
+  with_bool(count, [&](auto C) {
+    with_bool(s.num_spheres > 0, [&](auto S) {
+      with_bool(s.wide != 0, [&](auto W) {
+        k_extend<decltype(C)::value, decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+      });
+    });
+  });
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
   if (s.num_media > 0) k_shade<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
@@ -1072,31 +1236,26 @@ void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, c
 }
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
-  grid = trace_grid();
-  const bool sph = s.num_spheres > 0;
-  // Media and sphere variants are launched only for scenes that have them; the surface-
-  // and triangle-only variant keeps the traversal lean for mesh scenes.
-  if (s.num_media > 0) {
-    if (sph) {
-      if (count) k_shadow<true, true, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-      else k_shadow<true, false, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-    } else {
-      if (count) k_shadow<true, true, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-      else k_shadow<true, false, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-    }
-  } else {
-    if (sph) {
-      if (count) k_shadow<false, true, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-      else k_shadow<false, false, true><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-    } else {
-      if (count) k_shadow<false, true, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-      else k_shadow<false, false, false><<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
-    }
-  }
+  grid = trace_grid(s.wide != 0);
+  // Media, sphere and layout variants are instantiated separately so that the surface-only,
+  // triangle-only traversal stays lean for mesh scenes.
+  with_bool(s.num_media > 0, [&](auto M) {
+    with_bool(count, [&](auto C) {
+      with_bool(s.num_spheres > 0, [&](auto S) {
+        with_bool(s.wide != 0, [&](auto W) {
+          k_shadow<decltype(M)::value, decltype(C)::value, decltype(S)::value, decltype(W)::value>
+              <<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+        });
+      });
+    });
+  });
 }
 void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
-  if (s.num_spheres > 0) k_track<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
-  else k_track<false><<<grid, kBlock, 0, st>>>(s, p, bounce);
+  with_bool(s.num_spheres > 0, [&](auto S) {
+    with_bool(s.wide != 0, [&](auto W) {
+      k_track<decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);
+    });
+  });
 }
 void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_hi, uint2* out, unsigned int* err,
                          cudaStream_t st) {
@@ -1116,20 +1275,30 @@ static int grid_for(int n) {
 void launch_intersect_rays(const DevScene& s, const float* rays, int n, int* prim, float* t, float* u, float* v,
                            unsigned int* err, cudaStream_t st) {
   if (n <= 0) return;
-  if (s.num_spheres > 0) k_intersect_rays<true><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v, err);
-  else k_intersect_rays<false><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v, err);
+  with_bool(s.num_spheres > 0, [&](auto S) {
+    with_bool(s.wide != 0, [&](auto W) {
+      k_intersect_rays<decltype(S)::value, decltype(W)::value><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, prim, t, u, v,
+                                                                                               err);
+    });
+  });
 }
 void launch_occluded_rays(const DevScene& s, const float* rays, int n, unsigned char* occ, unsigned int* err,
                           cudaStream_t st) {
   if (n <= 0) return;
-  if (s.num_spheres > 0) k_occluded_rays<true><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
-  else k_occluded_rays<false><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
+  with_bool(s.num_spheres > 0, [&](auto S) {
+    with_bool(s.wide != 0, [&](auto W) {
+      k_occluded_rays<decltype(S)::value, decltype(W)::value><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, occ, err);
+    });
+  });
 }
 void launch_count_rays(const DevScene& s, const float* rays, int n, unsigned long long* counters, unsigned int* err,
                        cudaStream_t st) {
   if (n <= 0) return;
-  if (s.num_spheres > 0) k_count_rays<true><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
-  else k_count_rays<false><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
+  with_bool(s.num_spheres > 0, [&](auto S) {
+    with_bool(s.wide != 0, [&](auto W) {
+      k_count_rays<decltype(S)::value, decltype(W)::value><<<grid_for(n), kBlock, 0, st>>>(s, rays, n, counters, err);
+    });
+  });
 }
 void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, int n, unsigned long long seed,
                         float* dir, float* val, float* pdf, cudaStream_t st) {
