@@ -106,7 +106,13 @@ __device__ __forceinline__ bool intersect_tri(const RayPre& r, float3 v0, float3
   const float3 ng = cross3(v1 - v0, v2 - v0);
   const float den = dot3(ng, r.d);
   if (den == 0.f) return false;
-  const float t = dot3(ng, A) / den;
+  // Axis-aligned planes: the distance along that axis alone, so that coplanar faces of
+  // any size yield bitwise-equal distances and the primitive-id tie rule applies.
+  float t;
+  if (ng.y == 0.f && ng.z == 0.f) t = A.x / r.d.x;
+  else if (ng.x == 0.f && ng.z == 0.f) t = A.y / r.d.y;
+  else if (ng.x == 0.f && ng.y == 0.f) t = A.z / r.d.z;
+  else t = dot3(ng, A) / den;
   if (!(t > tnear && t <= tfar)) return false;
   const float inv = 1.f / det;
   *tout = t;
@@ -153,8 +159,15 @@ struct TraceCounters {
 struct TraceState {
   RayPre r;
   float tnear, best_t, b1, b2;
-  int best, cur, sp;
+  int best, best_prim, cur, sp;
 };
+
+// Closest-hit acceptance for a candidate at t <= best_t: nearer, or at the same distance
+// with a lower primitive id.  Coplanar overlapping faces (a box standing on the floor) then
+// resolve the same way whatever the traversal order or tree shape.
+__device__ __forceinline__ bool closer(float t, int prim, float best_t, int best_prim) {
+  return t < best_t || prim < best_prim;
+}
 
 __device__ __forceinline__ void trace_init(TraceState& s, float3 o, float3 d, float tnear, float tfar) {
   s.r = prepare_ray(o, d);
@@ -162,6 +175,7 @@ __device__ __forceinline__ void trace_init(TraceState& s, float3 o, float3 d, fl
   s.best_t = tfar;
   s.b1 = s.b2 = 0.f;
   s.best = -1;
+  s.best_prim = 0x7fffffff;
   s.cur = 0;  // the root is always an inner node
   s.sp = 0;
 }
@@ -223,8 +237,9 @@ __device__ __forceinline__ bool trace_step(const BvhRef& bvh, TraceState& s, int
       bool hit;
       if (SPH && __float_as_int(c.w) != 0) hit = intersect_sphere(r, a, b, s.tnear, s.best_t, &t);
       else hit = intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2);
-      if (hit) {
+      if (hit && (ANY || closer(t, __float_as_int(a.w), s.best_t, s.best_prim))) {
         s.best = i;
+        s.best_prim = __float_as_int(a.w);
         s.best_t = t;
         s.b1 = b1;
         s.b2 = b2;
@@ -270,7 +285,7 @@ __device__ __forceinline__ unsigned permute8(unsigned m, unsigned oct) {
 struct Trace8State {
   uint2 ng;     // node group: x = first child node, y = inner mask << 8 | permuted hit bits
   uint2 pg;     // primitive group: x = first slot, y = slots still to test (bit i = x + i)
-  int best, sp;
+  int best, best_prim, sp;
   float tnear, best_t, b1, b2;
 };
 
@@ -323,7 +338,9 @@ __device__ __forceinline__ void visit_node8(const uint4* __restrict__ nodes, con
 template <bool ANY, bool COUNT, bool SPH>
 __device__ __forceinline__ void trace8_run(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                            const RayPre& r, Trace8State& s, unsigned int* err, TraceCounters* cnt) {
-  const unsigned oct = (r.d.x < 0.f ? 1u : 0u) | (r.d.y < 0.f ? 2u : 0u) | (r.d.z < 0.f ? 4u : 0u);
+  // Octant from the signs of the reciprocal direction, which carry the sign of a -0
+  // component (safe_inv), so near and far planes are chosen consistently with it.
+  const unsigned oct = (r.id.x < 0.f ? 1u : 0u) | (r.id.y < 0.f ? 2u : 0u) | (r.id.z < 0.f ? 4u : 0u);
   uint2 stack[BVH8_STACK];
   s.ng = make_uint2(0u, (1u << 8) | (1u << oct));  // the root as the single inner child of slot 0
   s.pg = make_uint2(0u, 0u);
@@ -356,8 +373,9 @@ __device__ __forceinline__ void trace8_run(const uint4* __restrict__ nodes, cons
       bool hit;
       if (SPH && __float_as_int(c.w) != 0) hit = intersect_sphere(r, a, b, s.tnear, s.best_t, &t);
       else hit = intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2);
-      if (hit) {
+      if (hit && (ANY || closer(t, __float_as_int(a.w), s.best_t, s.best_prim))) {
         s.best = i;
+        s.best_prim = __float_as_int(a.w);
         s.best_t = t;
         s.b1 = b1;
         s.b2 = b2;
@@ -380,6 +398,7 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
     s.tnear = tnear;
     s.best_t = tfar;
     s.best = -1;
+    s.best_prim = 0x7fffffff;
     s.b1 = s.b2 = 0.f;
     trace8_run<ANY, COUNT, SPH>(sc.nodes8, sc.tris, r, s, err, cnt);
     if (s.best >= 0) {
@@ -397,6 +416,7 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
   s.best_t = tfar;
   s.b1 = s.b2 = 0.f;
   s.best = -1;
+  s.best_prim = 0x7fffffff;
   s.cur = 0;
   s.sp = 0;
   while (!trace_step<ANY, COUNT, SPH>(bvh, s, stack, err, cnt)) {
@@ -419,6 +439,7 @@ __device__ __forceinline__ int next_hit8(const uint4* nodes, const float4* tris,
   s.tnear = tnear;
   s.best_t = tfar;
   s.best = -1;
+  s.best_prim = 0x7fffffff;
   s.b1 = s.b2 = 0.f;
   trace8_run<false, false, SPH>(nodes, tris, r, s, err, nullptr);
   *t_out = s.best_t;
@@ -435,6 +456,7 @@ __device__ __forceinline__ int next_hit(const BvhRef& bvh, const RayPre& r, floa
   s.best_t = tfar;
   s.b1 = s.b2 = 0.f;
   s.best = -1;
+  s.best_prim = 0x7fffffff;
   s.cur = 0;
   s.sp = 0;
   while (!trace_step<false, false, SPH>(bvh, s, stack, err, nullptr)) {

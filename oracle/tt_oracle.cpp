@@ -590,7 +590,12 @@ inline bool IntersectTri(V3 org, V3 dir, V3 v0, V3 v1, V3 v2, double tnear, doub
   const V3 ng = Cross(v1 - v0, v2 - v0);
   const double den = Dot(ng, dir);
   if (den == 0) return false;
-  const double t = Dot(ng, A) / den;
+  // Axis-aligned planes: the distance along that axis alone (coplanar faces tie exactly).
+  double t;
+  if (ng.y == 0 && ng.z == 0) t = A.x / dir.x;
+  else if (ng.x == 0 && ng.z == 0) t = A.y / dir.y;
+  else if (ng.x == 0 && ng.y == 0) t = A.z / dir.z;
+  else t = Dot(ng, A) / den;
   if (!(t > tnear && t <= tfar)) return false;
   *tout = t;
   *uout = V / det;
@@ -643,7 +648,9 @@ inline bool SlabHit(const BNode& nd, V3 org, V3 inv, double tnear, double tfar, 
   return true;
 }
 
-// Closest hit in (tnear, tfar].  any_hit: stop at the first hit (occlusion).
+// Closest hit in (tnear, tfar].  any_hit: stop at the first hit (occlusion).  Hits at the
+// same distance resolve to the lower primitive id, so coplanar overlapping faces give the
+// same answer whatever the traversal order (Embree leaves such ties to its traversal).
 static int Trace(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, double tnear, double tfar, bool any_hit,
                  double* t_out, double* u_out, double* v_out) {
   if (s.nodes.empty() || s.tris.empty()) return -1;
@@ -661,7 +668,7 @@ static int Trace(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, double
       for (int i = nd.start; i < nd.start + nd.count; ++i) {
         int tri = s.order[i];
         double t, u, v;
-        if (IntersectPrim(sc, tri, org, dir, tnear, best_t, &t, &u, &v)) {
+        if (IntersectPrim(sc, tri, org, dir, tnear, best_t, &t, &u, &v) && (any_hit || t < best_t || best < 0 || tri < best)) {
           best = tri; best_t = t; bu = u; bv = v;
           if (any_hit) { *t_out = t; return tri; }
         }
@@ -682,7 +689,7 @@ static int TraceBrute(const Scene& sc, const Scene::TriSet& s, V3 org, V3 dir, d
   double best_t = tfar, bu = 0, bv = 0;
   for (int tri : s.tris) {
     double t, u, v;
-    if (IntersectPrim(sc, tri, org, dir, tnear, best_t, &t, &u, &v)) {
+    if (IntersectPrim(sc, tri, org, dir, tnear, best_t, &t, &u, &v) && (t < best_t || best < 0 || tri < best)) {
       best = tri; best_t = t; bu = u; bv = v;
     }
   }
