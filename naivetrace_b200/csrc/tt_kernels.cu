@@ -282,6 +282,12 @@ __device__ __forceinline__ unsigned permute8(unsigned m, unsigned oct) {
   return m;
 }
 
+// Byte k of w as a float, exactly: the byte becomes the low mantissa bits of 2^23 (one
+// byte permute) and 2^23 is subtracted, which avoids an integer-to-float conversion.
+__device__ __forceinline__ float qbyte(unsigned w, int k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (unsigned)k)) - 8388608.f;
+}
+
 struct Trace8State {
   uint2 ng;     // node group: x = first child node, y = inner mask << 8 | permuted hit bits
   uint2 pg;     // primitive group: x = first slot, y = slots still to test (bit i = x + i)
@@ -311,15 +317,14 @@ __device__ __forceinline__ void visit_node8(const uint4* __restrict__ nodes, con
   unsigned hits = 0u;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
-    const unsigned sh = 8u * (unsigned)(c & 3);
     const unsigned wnx = c < 4 ? nx.x : nx.y, wny = c < 4 ? ny.x : ny.y, wnz = c < 4 ? nz.x : nz.y;
     const unsigned wfx = c < 4 ? fx.x : fx.y, wfy = c < 4 ? fy.x : fy.y, wfz = c < 4 ? fz.x : fz.y;
-    const float tnx = fmaf((float)((wnx >> sh) & 0xffu), sx, ax);
-    const float tny = fmaf((float)((wny >> sh) & 0xffu), sy, ay);
-    const float tnz = fmaf((float)((wnz >> sh) & 0xffu), sz, az);
-    const float tfx = fmaf((float)((wfx >> sh) & 0xffu), sx, ax);
-    const float tfy = fmaf((float)((wfy >> sh) & 0xffu), sy, ay);
-    const float tfz = fmaf((float)((wfz >> sh) & 0xffu), sz, az);
+    const float tnx = fmaf(qbyte(wnx, c & 3), sx, ax);
+    const float tny = fmaf(qbyte(wny, c & 3), sy, ay);
+    const float tnz = fmaf(qbyte(wnz, c & 3), sz, az);
+    const float tfx = fmaf(qbyte(wfx, c & 3), sx, ax);
+    const float tfy = fmaf(qbyte(wfy, c & 3), sy, ay);
+    const float tfz = fmaf(qbyte(wfz, c & 3), sz, az);
     const float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tnear));
     const float tmax = fminf(fminf(tfx, tfy), fminf(tfz, s.best_t)) * 1.0000011f;
     hits |= (tmin <= tmax ? 1u : 0u) << c;
