@@ -282,10 +282,16 @@ __device__ __forceinline__ unsigned permute8(unsigned m, unsigned oct) {
   return m;
 }
 
-// Byte k of w as a float, exactly: the byte becomes the low mantissa bits of 2^23 (one
-// byte permute) and 2^23 is subtracted, which avoids an integer-to-float conversion.
-__device__ __forceinline__ float qbyte(unsigned w, int k) {
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (unsigned)k)) - 8388608.f;
+// Three-input minimum and maximum (PTX ISA 8.8, sm_100+).
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float fmin3(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
 }
 
 struct Trace8State {
@@ -307,6 +313,11 @@ __device__ __forceinline__ void visit_node8(const uint4* __restrict__ nodes, con
   const float sx = __uint_as_float((n0.w & 0xffu) << 23) * r.id.x;
   const float sy = __uint_as_float(((n0.w >> 8) & 0xffu) << 23) * r.id.y;
   const float sz = __uint_as_float(((n0.w >> 16) & 0xffu) << 23) * r.id.z;
+  // Far planes carry the 1 + 2 gamma(3) widening through their per-node constants.
+  constexpr float kWiden = 1.0000011f;
+  const float fax = ax * kWiden, fay = ay * kWiden, faz = az * kWiden;
+  const float fsx = sx * kWiden, fsy = sy * kWiden, fsz = sz * kWiden;
+  const float lim = s.best_t * kWiden;
   const unsigned imask = n0.w >> 24;
   // Near and far planes per axis follow the ray direction's signs.
   const uint2 lox = make_uint2(n2.x, n2.y), loy = make_uint2(n2.z, n2.w), loz = make_uint2(n3.x, n3.y);
@@ -317,16 +328,17 @@ __device__ __forceinline__ void visit_node8(const uint4* __restrict__ nodes, con
   unsigned hits = 0u;
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
+    const unsigned sh = 8u * (unsigned)(c & 3);
     const unsigned wnx = c < 4 ? nx.x : nx.y, wny = c < 4 ? ny.x : ny.y, wnz = c < 4 ? nz.x : nz.y;
     const unsigned wfx = c < 4 ? fx.x : fx.y, wfy = c < 4 ? fy.x : fy.y, wfz = c < 4 ? fz.x : fz.y;
-    const float tnx = fmaf(qbyte(wnx, c & 3), sx, ax);
-    const float tny = fmaf(qbyte(wny, c & 3), sy, ay);
-    const float tnz = fmaf(qbyte(wnz, c & 3), sz, az);
-    const float tfx = fmaf(qbyte(wfx, c & 3), sx, ax);
-    const float tfy = fmaf(qbyte(wfy, c & 3), sy, ay);
-    const float tfz = fmaf(qbyte(wfz, c & 3), sz, az);
-    const float tmin = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tnear));
-    const float tmax = fminf(fminf(tfx, tfy), fminf(tfz, s.best_t)) * 1.0000011f;
+    const float tnx = fmaf((float)((wnx >> sh) & 0xffu), sx, ax);
+    const float tny = fmaf((float)((wny >> sh) & 0xffu), sy, ay);
+    const float tnz = fmaf((float)((wnz >> sh) & 0xffu), sz, az);
+    const float tfx = fmaf((float)((wfx >> sh) & 0xffu), fsx, fax);
+    const float tfy = fmaf((float)((wfy >> sh) & 0xffu), fsy, fay);
+    const float tfz = fmaf((float)((wfz >> sh) & 0xffu), fsz, faz);
+    const float tmin = fmax3(tnx, tny, fmaxf(tnz, s.tnear));
+    const float tmax = fmin3(tfx, tfy, fminf(tfz, lim));
     hits |= (tmin <= tmax ? 1u : 0u) << c;
   }
   // Leaf children (nonzero meta bytes) that were hit contribute their primitive slots.

@@ -162,3 +162,28 @@ def test_traversal_counts(gpu_lib):
     assert st["counted_rays"] == 10000
     assert st["node_visits"] > 10000 and st["tri_tests"] > 0
     assert st["bvh_nodes"] > 0 and st["bvh_node_bytes"] in (64, 80) and st["tri_bytes"] == 48
+
+
+@pytest.fixture
+def wide_bvh(monkeypatch):
+    """Selects the 8-wide compressed BVH for contexts created in the test."""
+    monkeypatch.setenv("TT_BVH_WIDTH", "8")
+
+
+def test_wide_bvh_matches_oracle(gpu_lib, wide_bvh):
+    s = scenes.terrain_spheres_small()
+    g = GpuContext(s)
+    assert g.stats()["bvh_node_bytes"] == 80
+    o = OracleScene(s, make_params())
+    rng = np.random.default_rng(12)
+    rays = random_rays(200000, -4.5, 4.5, rng)
+    rays[:, 1] = rng.uniform(0.3, 2.0, size=len(rays))
+    check_parity(g, o, rays)
+    a = rng.uniform(-4.5, 4.5, (50000, 3))
+    b = rng.uniform(-4.5, 4.5, (50000, 3))
+    a[:, 1] = rng.uniform(0.0, 1.5, 50000)
+    b[:, 1] = rng.uniform(0.0, 1.5, 50000)
+    d = b - a
+    ln = np.linalg.norm(d, axis=1, keepdims=True)
+    seg = np.concatenate([a, np.zeros((len(a), 1)), d / ln, ln * 0.9999], axis=1).astype(np.float32).astype(np.float64)
+    assert (g.occluded(seg) == o.occluded(seg)).mean() >= 0.9999

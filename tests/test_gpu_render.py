@@ -173,3 +173,17 @@ def test_no_device_errors(gpu_lib):
     assert st["extension_rays"] >= 64 * 36 * 8
     rgb = g.framebuffer()
     assert np.all(np.isfinite(rgb))
+
+
+@pytest.mark.parametrize("name", ["cornell_box_materials", "terrain_spheres_small"])
+def test_per_path_parity_wide_bvh(gpu_lib, monkeypatch, name):
+    """The same per-path parity with the 8-wide compressed BVH as the traversal layout."""
+    monkeypatch.setenv("TT_BVH_WIDTH", "8")
+    scene = scenes.cornell_box_materials(32, 32) if name != "terrain_spheres_small" else scenes.terrain_spheres_small(48, 27)
+    (ag, lg, sg), (ao, lo, so), g, o = render_both(scene, 4, 10)
+    assert g.stats()["bvh_node_bytes"] == 80
+    ag = ag.reshape(-1, 3)
+    ao = ao.reshape(-1, 3)
+    scale = max(np.abs(ao).mean(), 1e-6)
+    close = np.all(np.abs(ag - ao) <= 1e-3 * np.abs(ao) + 1e-3 * scale, axis=1)
+    assert close.mean() >= 0.97, close.mean()
