@@ -1,0 +1,507 @@
+// Device BVH construction: PLOC (parallel locally-ordered clustering, Meister and Bittner
+// 2018) over Morton-ordered primitives, a bottom-up SAH pass that collapses small subtrees
+// into leaves of at most four primitives, and emission in the binary layout of tt_bvh.h.
+// Replaces the Embree scene commit (Scene::BuildAccelStructure, scene.cxx:116-141) on the
+// GPU: the host sends the mesh once and the tree is built next to it.
+//
+// Clustering: clusters sit in Morton order; each finds the neighbour within kRadius
+// positions whose merged box has the least surface area (ties broken by the pair's
+// positions, so the relation is a strict order and the globally best pair is always
+// mutual); mutual nearest neighbours merge into a new node at the lower position, and the
+// array is compacted.  Node ids grow with the iteration that created them, so children
+// always precede parents, and one kernel per iteration range walks the tree bottom-up or
+// top-down.
+#include <cub/cub.cuh>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "tt_build.h"
+#include "tt_internal.h"
+
+namespace tt {
+namespace {
+
+constexpr int kRadius = 16;      // PLOC neighbourhood (positions on either side)
+constexpr int kMaxLeaf = 4;
+constexpr int kMaxIterations = 4096;
+constexpr int kThreads = 256;
+
+struct Aabb {
+  float3 lo, hi;
+};
+
+__device__ __forceinline__ float half_area(const Aabb& b) {
+  const float dx = b.hi.x - b.lo.x, dy = b.hi.y - b.lo.y, dz = b.hi.z - b.lo.z;
+  return dx * dy + dy * dz + dz * dx;
+}
+__device__ __forceinline__ Aabb merge(const Aabb& a, const Aabb& b) {
+  return Aabb{make_float3(fminf(a.lo.x, b.lo.x), fminf(a.lo.y, b.lo.y), fminf(a.lo.z, b.lo.z)),
+              make_float3(fmaxf(a.hi.x, b.hi.x), fmaxf(a.hi.y, b.hi.y), fmaxf(a.hi.z, b.hi.z))};
+}
+
+// Order-preserving map of floats to unsigned ints (for atomic min / max of floats).
+__device__ __forceinline__ unsigned ordered(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unordered(unsigned u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ __forceinline__ Aabb prim_box(const BuildInput& in, uint32_t global) {
+  Aabb b;
+  if (global < in.num_triangles) {
+    const uint32_t* t = in.indices + 3 * (size_t)global;
+    const float* v0 = in.vertices + 3 * (size_t)t[0];
+    const float* v1 = in.vertices + 3 * (size_t)t[1];
+    const float* v2 = in.vertices + 3 * (size_t)t[2];
+    b.lo = make_float3(fminf(v0[0], fminf(v1[0], v2[0])), fminf(v0[1], fminf(v1[1], v2[1])),
+                       fminf(v0[2], fminf(v1[2], v2[2])));
+    b.hi = make_float3(fmaxf(v0[0], fmaxf(v1[0], v2[0])), fmaxf(v0[1], fmaxf(v1[1], v2[1])),
+                       fmaxf(v0[2], fmaxf(v1[2], v2[2])));
+  } else {
+    // One ulp outside centre -/+ radius (SphereBoundsFunc, embreeaccelerator.cxx:263-281).
+    const float* q = in.spheres + 4 * (size_t)(global - in.num_triangles);
+    b.lo = make_float3(nextafterf(q[0] - q[3], -INFINITY), nextafterf(q[1] - q[3], -INFINITY),
+                       nextafterf(q[2] - q[3], -INFINITY));
+    b.hi = make_float3(nextafterf(q[0] + q[3], INFINITY), nextafterf(q[1] + q[3], INFINITY),
+                       nextafterf(q[2] + q[3], INFINITY));
+  }
+  return b;
+}
+
+__global__ void k_prim_boxes(BuildInput in, const uint32_t* set, uint32_t n, Aabb* boxes, unsigned* cbounds) {
+  unsigned lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Aabb b = prim_box(in, set[i]);
+    boxes[i] = b;
+    const float c[3] = {0.5f * (b.lo.x + b.hi.x), 0.5f * (b.lo.y + b.hi.y), 0.5f * (b.lo.z + b.hi.z)};
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = min(lo[k], ordered(c[k]));
+      hi[k] = max(hi[k], ordered(c[k]));
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicMin(&cbounds[k], lo[k]);
+      atomicMax(&cbounds[3 + k], hi[k]);
+    }
+  }
+}
+
+__device__ __forceinline__ uint64_t spread21(uint64_t x) {
+  x &= 0x1fffffull;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+
+// 63-bit Morton code of the box centre in the centroid bounds.
+__global__ void k_morton(const Aabb* boxes, uint32_t n, const unsigned* cbounds, uint64_t* keys, uint32_t* vals) {
+  float lo[3], ext[3];
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = unordered(cbounds[k]);
+    ext[k] = unordered(cbounds[3 + k]) - lo[k];
+  }
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const Aabb b = boxes[i];
+    const float c[3] = {0.5f * (b.lo.x + b.hi.x), 0.5f * (b.lo.y + b.hi.y), 0.5f * (b.lo.z + b.hi.z)};
+    uint64_t code = 0;
+    for (int k = 0; k < 3; ++k) {
+      const float f = ext[k] > 0.f ? (c[k] - lo[k]) / ext[k] : 0.f;
+      const uint64_t q = (uint64_t)fminf(fmaxf(f * 2097152.f, 0.f), 2097151.f);
+      code |= spread21(q) << (2 - k);
+    }
+    keys[i] = code;
+    vals[i] = i;
+  }
+}
+
+// Leaves 0..n-1 in Morton order: node box = primitive box, left = -1 - (set position).
+__global__ void k_init_leaves(const Aabb* prim_boxes, const uint32_t* perm, uint32_t n, Aabb* node_box,
+                              int* left, int* right, int* clusters) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    node_box[i] = prim_boxes[perm[i]];
+    left[i] = -1 - (int)perm[i];
+    right[i] = -1;
+    clusters[i] = (int)i;
+  }
+}
+
+// Pair order: merged area, then the pair's lower and higher positions.
+__device__ __forceinline__ bool pair_less(float a, int lo, int hi, float b, int blo, int bhi) {
+  return a < b || (a == b && (lo < blo || (lo == blo && hi < bhi)));
+}
+
+__global__ void k_nearest(const int* clusters, int c, const Aabb* node_box, int* nn) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    const Aabb bi = node_box[clusters[i]];
+    float best = INFINITY;
+    int bj = -1;
+    const int j0 = max(0, i - kRadius), j1 = min(c - 1, i + kRadius);
+    for (int j = j0; j <= j1; ++j) {
+      if (j == i) continue;
+      const float a = half_area(merge(bi, node_box[clusters[j]]));
+      if (bj < 0 || pair_less(a, min(i, j), max(i, j), best, min(i, bj), max(i, bj))) {
+        best = a;
+        bj = j;
+      }
+    }
+    nn[i] = bj;
+  }
+}
+
+// create[i]: i is the lower end of a mutual pair (it makes the new node); keep[i]: i stays
+// a cluster after the merge (everything except the higher end of a mutual pair).
+__global__ void k_merge_flags(const int* nn, int c, int* create, int* keep) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    const int j = nn[i];
+    const bool mutual = j >= 0 && nn[j] == i;
+    create[i] = (mutual && i < j) ? 1 : 0;
+    keep[i] = (mutual && i > j) ? 0 : 1;
+  }
+}
+
+__global__ void k_merge(const int* clusters, int c, const int* nn, const int* create, const int* create_off,
+                        const int* keep, const int* keep_off, int next_node, Aabb* node_box, int* left, int* right,
+                        int* out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c; i += gridDim.x * blockDim.x) {
+    if (!keep[i]) continue;
+    int id = clusters[i];
+    if (create[i]) {
+      const int j = nn[i];
+      const int k = next_node + create_off[i];
+      const int a = clusters[i], b = clusters[j];
+      node_box[k] = merge(node_box[a], node_box[b]);
+      left[k] = a;
+      right[k] = b;
+      id = k;
+    }
+    out[keep_off[i]] = id;
+  }
+}
+
+// Bottom-up over one creation range: subtree sizes and SAH costs (traversal step 1,
+// primitive test 1 per primitive), and whether a subtree of at most kMaxLeaf primitives
+// is cheaper as one leaf.
+__global__ void k_costs(int first, int count, uint32_t n, const Aabb* node_box, const int* left, const int* right,
+                        int* size, float* cost, unsigned char* collapse) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    const int k = first + t;
+    const int l = left[k], r = right[k];
+    const int sl = l < (int)n ? 1 : size[l], sr = r < (int)n ? 1 : size[r];
+    const float cl = l < (int)n ? 1.f : cost[l], cr = r < (int)n ? 1.f : cost[r];
+    const float a = half_area(node_box[k]);
+    const float split = a > 0.f ? 1.f + (half_area(node_box[l]) * cl + half_area(node_box[r]) * cr) / a
+                                : 1.f + cl + cr;
+    const int s = sl + sr;
+    const float leaf = (float)s;
+    const bool as_leaf = s <= kMaxLeaf && leaf <= split;
+    size[k] = s;
+    cost[k] = as_leaf ? leaf : split;
+    collapse[k] = as_leaf ? 1 : 0;
+  }
+}
+
+// Top-down over one creation range: primitive offsets (depth-first order) and whether the
+// node is emitted as an inner node, lies inside a leaf, or is a leaf itself.
+// state: bit 0 = inside a leaf (set by an ancestor that became a leaf).
+__global__ void k_topdown(int first, int count, uint32_t n, const int* left, const int* right, const int* size,
+                          const unsigned char* collapse, int* offset, unsigned char* state, int* depth,
+                          unsigned char* emit, unsigned* max_depth) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    const int k = first + t;
+    const bool inside = state[k] & 1u;
+    const bool leafnode = inside || collapse[k];
+    emit[k] = leafnode ? 0 : 1;
+    const int l = left[k], r = right[k];
+    const int sl = l < (int)n ? 1 : size[l];
+    offset[l] = offset[k];
+    offset[r] = offset[k] + sl;
+    state[l] = leafnode ? 1 : 0;
+    state[r] = leafnode ? 1 : 0;
+    if (!leafnode) {
+      depth[l] = depth[k] + 1;
+      depth[r] = depth[k] + 1;
+      atomicMax(max_depth, (unsigned)(depth[k] + 1));
+    }
+  }
+}
+
+// Primitive slots in depth-first order (layout in tt_bvh.h).
+__global__ void k_write_slots(BuildInput in, const uint32_t* set, const int* left, const int* offset, uint32_t n,
+                              float4* tris) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t pos = (uint32_t)(-1 - left[i]);
+    const uint32_t g = set[pos];
+    float4* dst = tris + 3 * (size_t)offset[i];
+    if (g < in.num_triangles) {
+      const uint32_t* t = in.indices + 3 * (size_t)g;
+      const float* v0 = in.vertices + 3 * (size_t)t[0];
+      const float* v1 = in.vertices + 3 * (size_t)t[1];
+      const float* v2 = in.vertices + 3 * (size_t)t[2];
+      dst[0] = make_float4(v0[0], v0[1], v0[2], __int_as_float((int)in.prim_ids[pos]));
+      dst[1] = make_float4(v1[0], v1[1], v1[2], __int_as_float((int)in.material_ids[g]));
+      dst[2] = make_float4(v2[0], v2[1], v2[2], 0.f);
+    } else {
+      const uint32_t k = g - in.num_triangles;
+      const float* q = in.spheres + 4 * (size_t)k;
+      dst[0] = make_float4(q[0], q[1], q[2], __int_as_float((int)in.prim_ids[pos]));
+      dst[1] = make_float4(q[3], 0.f, 0.f, __int_as_float((int)in.sphere_material_ids[k]));
+      dst[2] = make_float4(0.f, 0.f, 0.f, __int_as_float(1));
+    }
+  }
+}
+
+__device__ __forceinline__ int child_ref(int c, uint32_t n, const int* size, const int* offset,
+                                         const unsigned char* emit, const int* index) {
+  if (c >= (int)n && emit[c]) return index[c];
+  const int cnt = c < (int)n ? 1 : size[c];
+  return ~(int)(((unsigned)offset[c] << 3) | (unsigned)(cnt - 1));
+}
+
+// Emitted inner node k -> device node index[k] (the root is node 0).
+__global__ void k_write_nodes(int first, int count, uint32_t n, const Aabb* node_box, const int* left,
+                              const int* right, const int* size, const int* offset, const unsigned char* emit,
+                              const int* index, float4* nodes) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    const int k = first + t;
+    if (!emit[k]) continue;
+    const int l = left[k], r = right[k];
+    const Aabb a = node_box[l], b = node_box[r];
+    float4* d = nodes + 4 * (size_t)index[k];
+    d[0] = make_float4(a.lo.x, a.hi.x, a.lo.y, a.hi.y);
+    d[1] = make_float4(b.lo.x, b.hi.x, b.lo.y, b.hi.y);
+    d[2] = make_float4(a.lo.z, a.hi.z, b.lo.z, b.hi.z);
+    d[3] = make_float4(__int_as_float(child_ref(l, n, size, offset, emit, index)),
+                       __int_as_float(child_ref(r, n, size, offset, emit, index)), 0.f, 0.f);
+  }
+}
+
+// index[k] = number of emitted nodes with a larger id (so the root, the last node, is 0).
+__global__ void k_reverse_flags(const unsigned char* emit, int total, int* rev) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+    rev[i] = emit[total - 1 - i];
+}
+__global__ void k_reverse_index(const int* rev_off, int total, int* index) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+    index[total - 1 - i] = rev_off[i];
+}
+
+// Root handling for trees whose root is a leaf: one node with the leaf as child 0 and an
+// empty child 1 (inverted box, reference to slot 0 with count 1).
+__global__ void k_leaf_root(const Aabb* node_box, int root, int count, float4* nodes) {
+  const Aabb a = node_box[root];
+  const float inf = INFINITY;
+  nodes[0] = make_float4(a.lo.x, a.hi.x, a.lo.y, a.hi.y);
+  nodes[1] = make_float4(inf, -inf, inf, -inf);
+  nodes[2] = make_float4(a.lo.z, a.hi.z, inf, -inf);
+  nodes[3] = make_float4(__int_as_float(~(int)(unsigned)(count - 1)), __int_as_float(~0), 0.f, 0.f);
+}
+
+int grid_for(long long n) {
+  long long g = (n + kThreads - 1) / kThreads;
+  return (int)(g < 1 ? 1 : (g > 4096 ? 4096 : g));
+}
+
+// Scratch allocations released on scope exit.
+struct Scratch {
+  std::vector<void*> ptrs;
+  template <class T>
+  T* alloc(size_t count) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, (count ? count : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+  ~Scratch() {
+    for (void* p : ptrs) cudaFree(p);
+  }
+};
+
+}  // namespace
+
+bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, DeviceBvh* out, cudaStream_t st,
+                       std::string* err) {
+  auto fail = [&](const std::string& m) {
+    *err = "device BVH build: " + m;
+    return false;
+  };
+  auto ok = [&](cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    *err = std::string("device BVH build: ") + what + ": " + cudaGetErrorString(e);
+    return false;
+  };
+  out->num_nodes = 0;
+  out->max_depth = 0;
+  out->nodes = nullptr;
+  out->tris = nullptr;
+  if (n == 0) {
+    // No primitives: a root with two empty children and one degenerate slot (prim -1).
+    float host_node[16];
+    const float inf = INFINITY;
+    const float h[12] = {inf, -inf, inf, -inf, inf, -inf, inf, -inf, inf, -inf, inf, -inf};
+    for (int k = 0; k < 12; ++k) host_node[k] = h[k];
+    const int32_t r0 = ~0, zero = 0;
+    std::memcpy(&host_node[12], &r0, 4);
+    std::memcpy(&host_node[13], &r0, 4);
+    std::memcpy(&host_node[14], &zero, 4);
+    std::memcpy(&host_node[15], &zero, 4);
+    float host_tri[12] = {0.f};
+    const int32_t none = -1;
+    std::memcpy(&host_tri[3], &none, 4);
+    if (!ok(cudaMalloc(&out->nodes, sizeof(host_node)), "cudaMalloc") ||
+        !ok(cudaMalloc(&out->tris, sizeof(host_tri)), "cudaMalloc"))
+      return false;
+    if (!ok(cudaMemcpyAsync(out->nodes, host_node, sizeof(host_node), cudaMemcpyHostToDevice, st), "copy") ||
+        !ok(cudaMemcpyAsync(out->tris, host_tri, sizeof(host_tri), cudaMemcpyHostToDevice, st), "copy") ||
+        !ok(cudaStreamSynchronize(st), "sync"))
+      return false;
+    out->num_nodes = 1;
+    return true;
+  }
+  Scratch sc;
+  const uint32_t total = 2 * n - 1;
+  Aabb* prim_boxes = sc.alloc<Aabb>(n);
+  unsigned* cbounds = sc.alloc<unsigned>(6);
+  uint64_t* keys = sc.alloc<uint64_t>(n);
+  uint64_t* keys2 = sc.alloc<uint64_t>(n);
+  uint32_t* vals = sc.alloc<uint32_t>(n);
+  uint32_t* perm = sc.alloc<uint32_t>(n);
+  Aabb* node_box = sc.alloc<Aabb>(total);
+  int* left = sc.alloc<int>(total);
+  int* right = sc.alloc<int>(total);
+  int* clusters = sc.alloc<int>(n);
+  int* clusters2 = sc.alloc<int>(n);
+  int* nn = sc.alloc<int>(n);
+  int* create = sc.alloc<int>(n);
+  int* create_off = sc.alloc<int>(n);
+  int* keep = sc.alloc<int>(n);
+  int* keep_off = sc.alloc<int>(n);
+  if (!prim_boxes || !cbounds || !keys || !keys2 || !vals || !perm || !node_box || !left || !right || !clusters ||
+      !clusters2 || !nn || !create || !create_off || !keep || !keep_off)
+    return fail("out of device memory");
+  const unsigned init_bounds[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+  if (!ok(cudaMemcpyAsync(cbounds, init_bounds, sizeof(init_bounds), cudaMemcpyHostToDevice, st), "copy")) return false;
+  k_prim_boxes<<<grid_for(n), kThreads, 0, st>>>(in, set, n, prim_boxes, cbounds);
+  k_morton<<<grid_for(n), kThreads, 0, st>>>(prim_boxes, n, cbounds, keys, vals);
+  // Sort primitives by Morton code (CUB radix sort).
+  size_t sort_bytes = 0, scan_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys2, vals, perm, (int)n, 0, 63, st);
+  cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, create, create_off, (int)n, st);
+  void* temp = sc.alloc<unsigned char>(std::max(sort_bytes, scan_bytes));
+  if (!temp) return fail("out of device memory");
+  if (!ok(cub::DeviceRadixSort::SortPairs(temp, sort_bytes, keys, keys2, vals, perm, (int)n, 0, 63, st), "sort"))
+    return false;
+  k_init_leaves<<<grid_for(n), kThreads, 0, st>>>(prim_boxes, perm, n, node_box, left, right, clusters);
+  // Clustering iterations; ranges[] records the node ids each iteration created.
+  std::vector<std::pair<int, int>> ranges;
+  int c = (int)n, next_node = (int)n;
+  int* cur = clusters;
+  int* nxt = clusters2;
+  int iterations = 0;
+  while (c > 1) {
+    if (++iterations > kMaxIterations) return fail("clustering did not converge");
+    k_nearest<<<grid_for(c), kThreads, 0, st>>>(cur, c, node_box, nn);
+    k_merge_flags<<<grid_for(c), kThreads, 0, st>>>(nn, c, create, keep);
+    size_t tb = std::max(sort_bytes, scan_bytes);
+    cub::DeviceScan::ExclusiveSum(temp, tb, create, create_off, c, st);
+    tb = std::max(sort_bytes, scan_bytes);
+    cub::DeviceScan::ExclusiveSum(temp, tb, keep, keep_off, c, st);
+    int tail[4];
+    cudaMemcpyAsync(&tail[0], create_off + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&tail[1], create + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&tail[2], keep_off + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&tail[3], keep + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    k_merge<<<grid_for(c), kThreads, 0, st>>>(cur, c, nn, create, create_off, keep, keep_off, next_node, node_box, left,
+                                             right, nxt);
+    if (!ok(cudaStreamSynchronize(st), "clustering")) return false;
+    const int made = tail[0] + tail[1], kept = tail[2] + tail[3];
+    if (made <= 0 || next_node + made > (int)total) return fail("clustering made no progress");
+    ranges.push_back({next_node, made});
+    next_node += made;
+    c = kept;
+    std::swap(cur, nxt);
+  }
+  int root = 0;
+  if (!ok(cudaMemcpyAsync(&root, cur, sizeof(int), cudaMemcpyDeviceToHost, st), "copy") ||
+      !ok(cudaStreamSynchronize(st), "sync"))
+    return false;
+  // Bottom-up costs, top-down offsets and emission.
+  int* size = sc.alloc<int>(total);
+  float* cost = sc.alloc<float>(total);
+  unsigned char* collapse = sc.alloc<unsigned char>(total);
+  int* offset = sc.alloc<int>(total);
+  unsigned char* state = sc.alloc<unsigned char>(total);
+  int* depth = sc.alloc<int>(total);
+  unsigned char* emit = sc.alloc<unsigned char>(total);
+  int* rev = sc.alloc<int>(total);
+  int* rev_off = sc.alloc<int>(total);
+  int* index = sc.alloc<int>(total);
+  unsigned* max_depth = sc.alloc<unsigned>(1);
+  if (!size || !cost || !collapse || !offset || !state || !depth || !emit || !rev || !rev_off || !index || !max_depth)
+    return fail("out of device memory");
+  cudaMemsetAsync(collapse, 1, n, st);  // primitive leaves
+  cudaMemsetAsync(emit, 0, total, st);
+  cudaMemsetAsync(max_depth, 0, sizeof(unsigned), st);
+  for (const auto& r : ranges)
+    k_costs<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, cost, collapse);
+  const int zero = 0;
+  const unsigned char none = 0;
+  cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(state + root, &none, 1, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(depth + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  for (auto it = ranges.rbegin(); it != ranges.rend(); ++it)
+    k_topdown<<<grid_for(it->second), kThreads, 0, st>>>(it->first, it->second, n, left, right, size, collapse, offset,
+                                                          state, depth, emit, max_depth);
+  // Node indices: emitted nodes numbered from the root down.
+  k_reverse_flags<<<grid_for(total), kThreads, 0, st>>>(emit, (int)total, rev);
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, rev, rev_off, (int)total, st);
+  void* temp2 = sc.alloc<unsigned char>(tb);
+  if (!temp2) return fail("out of device memory");
+  cub::DeviceScan::ExclusiveSum(temp2, tb, rev, rev_off, (int)total, st);
+  k_reverse_index<<<grid_for(total), kThreads, 0, st>>>(rev_off, (int)total, index);
+  int emitted_tail[2] = {0, 0};
+  unsigned depth_host = 0;
+  unsigned char root_emit = 0;
+  cudaMemcpyAsync(&emitted_tail[0], rev_off + total - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&emitted_tail[1], rev + total - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&depth_host, max_depth, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&root_emit, emit + root, 1, cudaMemcpyDeviceToHost, st);
+  if (!ok(cudaStreamSynchronize(st), "emission")) return false;
+  const int emitted = emitted_tail[0] + emitted_tail[1];
+  const int num_nodes = root_emit ? emitted : 1;
+  if (!ok(cudaMalloc(&out->nodes, 4 * sizeof(float4) * (size_t)num_nodes), "cudaMalloc") ||
+      !ok(cudaMalloc(&out->tris, 3 * sizeof(float4) * (size_t)n), "cudaMalloc"))
+    return false;
+  // The root is a leaf when the whole tree collapses (or n == 1): its subtree starts at 0.
+  if (!root_emit) {
+    cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    k_leaf_root<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes);
+  } else {
+    for (const auto& r : ranges)
+      k_write_nodes<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, offset,
+                                                              emit, index, out->nodes);
+  }
+  k_write_slots<<<grid_for(n), kThreads, 0, st>>>(in, set, left, offset, n, out->tris);
+  if (!ok(cudaStreamSynchronize(st), "emission") || !ok(cudaGetLastError(), "kernels")) return false;
+  out->num_nodes = (uint32_t)num_nodes;
+  out->max_depth = root_emit ? depth_host : 0;
+  return true;
+}
+
+}  // namespace tt

@@ -1,0 +1,36 @@
+// Device BVH construction (tt_build.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+namespace tt {
+
+// Device pointers to the whole scene's primitives; a build covers the subset `set` of
+// global primitive ids (triangles 0..T-1, spheres T..T+S-1) and stores prim_ids[i] as the
+// id of set position i.
+struct BuildInput {
+  const float* vertices;              // V x 3
+  const uint32_t* indices;            // T x 3
+  const uint32_t* material_ids;       // T
+  uint32_t num_triangles;
+  const float* spheres;               // S x 4
+  const uint32_t* sphere_material_ids;
+  const uint32_t* prim_ids;           // per set position: the id written into the slot
+};
+
+struct DeviceBvh {
+  float4* nodes;        // binary layout of tt_bvh.h, cudaMalloc'd (caller frees)
+  float4* tris;         // primitive slots, cudaMalloc'd (caller frees)
+  uint32_t num_nodes;
+  uint32_t max_depth;
+};
+
+// Builds the binary BVH of the `n` primitives whose global ids are in `set` (device array).
+// Synchronises `st`.  Returns false with a message on failure.
+bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, DeviceBvh* out, cudaStream_t st,
+                       std::string* err);
+
+}  // namespace tt

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/toytrace_gpu.h"
+#include "tt_build.h"
 #include "tt_bvh.h"
 #include "tt_internal.h"
 #include "tt_tables.h"
@@ -302,6 +303,9 @@ tt_status tt_upload_scene(tt_ctx* c) {
   // measured a few percent slower on the terrain workload).
   const char* width_env = std::getenv("TT_BVH_WIDTH");
   s.wide = width_env && std::atoi(width_env) == 8;
+  // The binary BVH is built on the device (PLOC) unless TT_BVH_BUILD=host asks for the
+  // host binned-SAH builder.
+  const char* build_env = std::getenv("TT_BVH_BUILD");
   if (s.wide) {
     Bvh8Output bo, vbo;
     if (!build_bvh8(bi, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
@@ -315,6 +319,55 @@ tt_status tt_upload_scene(tt_ctx* c) {
     s.tris = (const float4*)upload(bo.tris.data(), bo.tris.size() * sizeof(float));
     s.vnodes8 = (const uint4*)upload(vbo.nodes.data(), vbo.nodes.size() * sizeof(uint32_t));
     s.vtris = (const float4*)upload(vbo.tris.data(), vbo.tris.size() * sizeof(float));
+  } else if (!(build_env && std::string(build_env) == "host")) {
+    // Build on the device: the mesh goes up once, the tree is built next to it.
+    DeviceBuffers tmp;
+    auto up = [&](const void* src, size_t bytes) -> void* {
+      void* p = tmp.alloc(bytes);
+      if (p && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
+      return p;
+    };
+    std::vector<uint32_t> sset(sid), vset(vid);
+    sset.insert(sset.end(), ssid.begin(), ssid.end());
+    vset.insert(vset.end(), vsid.begin(), vsid.end());
+    BuildInput in{};
+    in.vertices = (const float*)up(c->verts.data(), c->verts.size() * sizeof(float));
+    in.indices = (const uint32_t*)up(c->idx.data(), c->idx.size() * sizeof(uint32_t));
+    in.material_ids = (const uint32_t*)up(c->mats.data(), c->mats.size() * sizeof(uint32_t));
+    in.num_triangles = ntri;
+    in.spheres = (const float*)up(c->spheres.data(), c->spheres.size() * sizeof(float));
+    in.sphere_material_ids = (const uint32_t*)up(c->sphere_mats.data(), c->sphere_mats.size() * sizeof(uint32_t));
+    const uint32_t* d_sset = (const uint32_t*)up(sset.data(), sset.size() * sizeof(uint32_t));
+    const uint32_t* d_vset = (const uint32_t*)up(vset.data(), vset.size() * sizeof(uint32_t));
+    for (void* p : tmp.allocs)
+      if (!p) {
+        tmp.free_all();
+        return fail(c, TT_ERR_CUDA, "device allocation failed");
+      }
+    DeviceBvh sb{}, vb{};
+    std::string berr;
+    in.prim_ids = d_sset;
+    bool built = device_build_bvh2(in, d_sset, (uint32_t)sset.size(), &sb, c->stream, &berr);
+    if (sb.nodes) c->scene_mem.allocs.push_back(sb.nodes);
+    if (sb.tris) c->scene_mem.allocs.push_back(sb.tris);
+    if (built) {
+      in.prim_ids = d_vset;
+      built = device_build_bvh2(in, d_vset, (uint32_t)vset.size(), &vb, c->stream, &berr);
+      if (vb.nodes) c->scene_mem.allocs.push_back(vb.nodes);
+      if (vb.tris) c->scene_mem.allocs.push_back(vb.tris);
+    }
+    cudaStreamSynchronize(c->stream);
+    tmp.free_all();
+    if (!built) return fail(c, TT_ERR_CUDA, berr);
+    c->bvh_nodes = sb.num_nodes;
+    c->bvh_depth = sb.max_depth;
+    c->bvh_node_bytes = 64;
+    if (sb.max_depth + 2 >= (uint32_t)BVH_STACK || vb.max_depth + 2 >= (uint32_t)BVH_STACK)
+      return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
+    s.nodes = sb.nodes;
+    s.tris = sb.tris;
+    s.vnodes = vb.nodes;
+    s.vtris = vb.tris;
   } else {
     BvhOutput bo, vbo;
     if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
