@@ -15,7 +15,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <utility>
@@ -375,6 +378,13 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   }
   Scratch sc;
   const uint32_t total = 2 * n - 1;
+  // TT_BUILD_VERBOSE=1 prints the phase times and the iteration count to stderr.
+  const bool verbose = std::getenv("TT_BUILD_VERBOSE") != nullptr;
+  const auto t_start = std::chrono::steady_clock::now();
+  auto ms_since = [&](std::chrono::steady_clock::time_point t0) {
+    cudaStreamSynchronize(st);
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  };
   Aabb* prim_boxes = sc.alloc<Aabb>(n);
   unsigned* cbounds = sc.alloc<unsigned>(6);
   uint64_t* keys = sc.alloc<uint64_t>(n);
@@ -407,6 +417,7 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   if (!ok(cub::DeviceRadixSort::SortPairs(temp, sort_bytes, keys, keys2, vals, perm, (int)n, 0, 63, st), "sort"))
     return false;
   k_init_leaves<<<grid_for(n), kThreads, 0, st>>>(prim_boxes, perm, n, node_box, left, right, clusters);
+  const double t_sorted = verbose ? ms_since(t_start) : 0.0;
   // Clustering iterations; ranges[] records the node ids each iteration created.
   std::vector<std::pair<int, int>> ranges;
   int c = (int)n, next_node = (int)n;
@@ -436,6 +447,7 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     c = kept;
     std::swap(cur, nxt);
   }
+  const double t_clustered = verbose ? ms_since(t_start) : 0.0;
   int root = 0;
   if (!ok(cudaMemcpyAsync(&root, cur, sizeof(int), cudaMemcpyDeviceToHost, st), "copy") ||
       !ok(cudaStreamSynchronize(st), "sync"))
@@ -501,6 +513,9 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   if (!ok(cudaStreamSynchronize(st), "emission") || !ok(cudaGetLastError(), "kernels")) return false;
   out->num_nodes = (uint32_t)num_nodes;
   out->max_depth = root_emit ? depth_host : 0;
+  if (verbose)
+    std::fprintf(stderr, "device BVH build: %u prims, %d iterations, %d nodes, depth %u; sorted %.1f ms, clustered %.1f ms, done %.1f ms\n",
+                 n, iterations, num_nodes, out->max_depth, t_sorted, t_clustered, ms_since(t_start));
   return true;
 }
 
