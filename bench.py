@@ -351,7 +351,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_step, "ms_each": [round(x, 1) for x in e2e_ms],
-                    "what": "tt_create + tt_upload_scene (host BVH build, scene H2D) + tt_render_pass + "
+                    "what": "tt_create + tt_upload_scene (scene H2D, device BVH build) + tt_render_pass + "
                             "tt_read_framebuffer + tt_destroy"},
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": clk,
