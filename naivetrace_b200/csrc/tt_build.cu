@@ -326,18 +326,20 @@ int grid_for(long long n) {
   return (int)(g < 1 ? 1 : (g > 4096 ? 4096 : g));
 }
 
-// Scratch allocations released on scope exit.
+// Scratch allocations from the library's memory pool, released on scope exit.
 struct Scratch {
+  cudaStream_t st;
   std::vector<void*> ptrs;
+  explicit Scratch(cudaStream_t s) : st(s) {}
   template <class T>
   T* alloc(size_t count) {
     void* p = nullptr;
-    if (cudaMalloc(&p, (count ? count : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+    if (pool_malloc(&p, (count ? count : 1) * sizeof(T), st) != cudaSuccess) return nullptr;
     ptrs.push_back(p);
     return static_cast<T*>(p);
   }
   ~Scratch() {
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) pool_free(p, st);
   }
 };
 
@@ -372,8 +374,8 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     float host_tri[12] = {0.f};
     const int32_t none = -1;
     std::memcpy(&host_tri[3], &none, 4);
-    if (!ok(cudaMalloc(&out->nodes, sizeof(host_node)), "cudaMalloc") ||
-        !ok(cudaMalloc(&out->tris, sizeof(host_tri)), "cudaMalloc"))
+    if (!ok(pool_malloc((void**)&out->nodes, sizeof(host_node), st), "allocation") ||
+        !ok(pool_malloc((void**)&out->tris, sizeof(host_tri), st), "allocation"))
       return false;
     if (!ok(cudaMemcpyAsync(out->nodes, host_node, sizeof(host_node), cudaMemcpyHostToDevice, st), "copy") ||
         !ok(cudaMemcpyAsync(out->tris, host_tri, sizeof(host_tri), cudaMemcpyHostToDevice, st), "copy") ||
@@ -382,7 +384,7 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     out->num_nodes = 1;
     return true;
   }
-  Scratch sc;
+  Scratch sc(st);
   const uint32_t total = 2 * n - 1;
   // TT_BUILD_VERBOSE=1 prints the phase times and the iteration count to stderr.
   const bool verbose = std::getenv("TT_BUILD_VERBOSE") != nullptr;
@@ -505,8 +507,8 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   if (!ok(cudaStreamSynchronize(st), "emission")) return false;
   const int emitted = emitted_tail[0] + emitted_tail[1];
   const int num_nodes = root_emit ? emitted : 1;
-  if (!ok(cudaMalloc(&out->nodes, 4 * sizeof(float4) * (size_t)num_nodes), "cudaMalloc") ||
-      !ok(cudaMalloc(&out->tris, 3 * sizeof(float4) * (size_t)n), "cudaMalloc"))
+  if (!ok(pool_malloc((void**)&out->nodes, 4 * sizeof(float4) * (size_t)num_nodes, st), "allocation") ||
+      !ok(pool_malloc((void**)&out->tris, 3 * sizeof(float4) * (size_t)n, st), "allocation"))
     return false;
   // The root is a leaf when the whole tree collapses (or n == 1): its subtree starts at 0.
   if (!root_emit) {

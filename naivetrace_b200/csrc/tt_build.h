@@ -22,8 +22,8 @@ struct BuildInput {
 };
 
 struct DeviceBvh {
-  float4* nodes;        // binary layout of tt_bvh.h, cudaMalloc'd (caller frees)
-  float4* tris;         // primitive slots, cudaMalloc'd (caller frees)
+  float4* nodes;        // binary layout of tt_bvh.h, from the memory pool (caller frees)
+  float4* tris;         // primitive slots, from the memory pool (caller frees)
   uint32_t num_nodes;
   uint32_t max_depth;
 };

@@ -32,20 +32,25 @@ struct HostEnv {
   std::vector<float> tex;
 };
 
+// Device buffers owned by a context, from the library's memory pool, ordered on `stream`.
 struct DeviceBuffers {
   std::vector<void*> allocs;
+  cudaStream_t stream = nullptr;
   void* alloc(size_t bytes) {
     void* p = nullptr;
     if (bytes == 0) bytes = 16;
-    if (cudaMalloc(&p, bytes) != cudaSuccess) return nullptr;
+    if (pool_malloc(&p, bytes, stream) != cudaSuccess) return nullptr;
     allocs.push_back(p);
     return p;
   }
   void free_all() {
-    for (void* p : allocs) cudaFree(p);
+    for (void* p : allocs) pool_free(p, stream);
     allocs.clear();
   }
 };
+
+std::mutex g_pool_mutex;
+cudaMemPool_t g_pools[64] = {nullptr};
 
 __global__ void k_tally(const int* counters, int rounds, unsigned long long* stats) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -60,6 +65,35 @@ __global__ void k_tally(const int* counters, int rounds, unsigned long long* sta
 }
 
 }  // namespace
+
+namespace tt {
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t st) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    if (!g_pools[dev]) {
+      cudaMemPoolProps props{};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&g_pools[dev], &props);
+      if (e != cudaSuccess) {
+        g_pools[dev] = nullptr;
+        return e;
+      }
+      uint64_t threshold = UINT64_MAX;
+      cudaMemPoolSetAttribute(g_pools[dev], cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+  }
+  return cudaMallocFromPoolAsync(p, bytes, g_pools[dev], st);
+}
+void pool_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+}  // namespace tt
 
 struct tt_ctx {
   // Host copy of the scene.
@@ -260,6 +294,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
   TT_CUDA(c, cudaSetDevice(c->device));
   if (c->uploaded) return TT_OK;
   TT_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  c->scene_mem.stream = c->stream;
+  c->path_mem.stream = c->stream;
   upload_constant_tables();
   TT_CUDA(c, cudaGetLastError());
   const uint32_t ntri = (uint32_t)c->mats.size();
@@ -294,7 +330,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   vbi.sphere_prim_ids = vsid.data();
   auto upload = [&](const void* src, size_t bytes) -> void* {
     void* p = c->scene_mem.alloc(bytes);
-    if (p && bytes) cudaMemcpy(p, src, bytes, cudaMemcpyHostToDevice);
+    if (p && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
     return p;
   };
   DevScene& s = c->dev;
@@ -322,6 +358,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   } else if (!(build_env && std::string(build_env) == "host")) {
     // Build on the device: the mesh goes up once, the tree is built next to it.
     DeviceBuffers tmp;
+    tmp.stream = c->stream;
     auto up = [&](const void* src, size_t bytes) -> void* {
       void* p = tmp.alloc(bytes);
       if (p && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
@@ -614,7 +651,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     if (!p) return fail(c, TT_ERR_CUDA, "device allocation failed");
   c->d_err = (unsigned int*)c->scene_mem.alloc(sizeof(unsigned int));
   if (!c->d_err) return fail(c, TT_ERR_CUDA, "device allocation failed");
-  TT_CUDA(c, cudaMemset(c->d_err, 0, sizeof(unsigned int)));
+  TT_CUDA(c, cudaMemsetAsync(c->d_err, 0, sizeof(unsigned int), c->stream));
   if (s.num_media > 0) {
     // Medium tracker at the camera (every camera path starts there).
     uint2* d_track = (uint2*)c->scene_mem.alloc(sizeof(uint2));
@@ -637,11 +674,11 @@ tt_status tt_upload_scene(tt_ctx* c) {
   c->d_stats = (unsigned long long*)c->scene_mem.alloc(8 * sizeof(unsigned long long));
   if (!c->fb.accum || !c->fb.light || !c->d_acc || !c->d_light || !c->d_stats)
     return fail(c, TT_ERR_CUDA, "device allocation failed");
-  TT_CUDA(c, cudaMemset(c->fb.accum, 0, n3 * sizeof(float)));
-  TT_CUDA(c, cudaMemset(c->fb.light, 0, n3 * sizeof(float)));
-  TT_CUDA(c, cudaMemset(c->d_acc, 0, n3 * sizeof(double)));
-  TT_CUDA(c, cudaMemset(c->d_light, 0, n3 * sizeof(double)));
-  TT_CUDA(c, cudaMemset(c->d_stats, 0, 8 * sizeof(unsigned long long)));
+  TT_CUDA(c, cudaMemsetAsync(c->fb.accum, 0, n3 * sizeof(float), c->stream));
+  TT_CUDA(c, cudaMemsetAsync(c->fb.light, 0, n3 * sizeof(float), c->stream));
+  TT_CUDA(c, cudaMemsetAsync(c->d_acc, 0, n3 * sizeof(double), c->stream));
+  TT_CUDA(c, cudaMemsetAsync(c->d_light, 0, n3 * sizeof(double), c->stream));
+  TT_CUDA(c, cudaMemsetAsync(c->d_stats, 0, 8 * sizeof(unsigned long long), c->stream));
   int sms = 0;
   TT_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   c->grid = sms * kernel_blocks_per_sm();
@@ -859,19 +896,37 @@ tt_status tt_read_accumulators(tt_ctx* c, double* accum, double* light, uint64_t
   return TT_OK;
 }
 
+// Spectral3ImageBuffer::ToImage before the clamp (renderbuffer.hxx:172-200), resolved on
+// the device: average the pixel samples, add the camera splats weighted by
+// npix / splat_count, and copy back npix x 3 floats.
 tt_status tt_read_framebuffer(tt_ctx* c, float* rgb, uint64_t* counts) {
   if (!c || !rgb) return TT_ERR_INVALID;
-  std::vector<double> acc(3 * (size_t)c->npix), light(3 * (size_t)c->npix);
-  tt_status st = tt_read_accumulators(c, acc.data(), light.data(), nullptr, nullptr);
-  if (st != TT_OK) return st;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
   const double sw = c->splat_count > 0 ? (double)c->npix / (double)c->splat_count : 0.;
-  for (int p = 0; p < c->npix; ++p) {
-    const double n = (double)c->spp_count[p];
-    for (int k = 0; k < 3; ++k) {
-      const double avg = n > 0 ? acc[3 * (size_t)p + k] / n : 0.;
-      rgb[3 * (size_t)p + k] = (float)(avg + sw * light[3 * (size_t)p + k]);
-    }
+  bool uniform = true;
+  for (int p = 1; p < c->npix && uniform; ++p) uniform = c->spp_count[p] == c->spp_count[0];
+  DeviceBuffers tmp;
+  tmp.stream = c->stream;
+  double* inv_px = nullptr;
+  double inv_all = 0.;
+  if (uniform) {
+    inv_all = c->npix > 0 && c->spp_count[0] > 0 ? 1.0 / (double)c->spp_count[0] : 0.;
+  } else {
+    std::vector<double> inv(c->npix);
+    for (int p = 0; p < c->npix; ++p) inv[p] = c->spp_count[p] > 0 ? 1.0 / (double)c->spp_count[p] : 0.;
+    inv_px = (double*)tmp.alloc(inv.size() * sizeof(double));
+    if (!inv_px) return fail(c, TT_ERR_CUDA, "device allocation failed");
+    TT_CUDA(c, cudaMemcpyAsync(inv_px, inv.data(), inv.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    TT_CUDA(c, cudaStreamSynchronize(c->stream));
   }
+  float* d_rgb = (float*)tmp.alloc(3 * (size_t)c->npix * sizeof(float));
+  if (!d_rgb) return fail(c, TT_ERR_CUDA, "device allocation failed");
+  launch_resolve(c->d_acc, c->d_light, inv_px, inv_all, sw, c->npix, d_rgb, c->stream);
+  TT_CUDA(c, cudaGetLastError());
+  TT_CUDA(c, cudaMemcpyAsync(rgb, d_rgb, 3 * (size_t)c->npix * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  tmp.free_all();
   if (counts) std::memcpy(counts, c->spp_count.data(), c->npix * sizeof(uint64_t));
   return TT_OK;
 }
@@ -900,8 +955,9 @@ tt_status tt_clear_framebuffer(tt_ctx* c) {
   if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
   TT_CUDA(c, cudaSetDevice(c->device));
   const size_t n3 = 3 * (size_t)c->npix;
-  TT_CUDA(c, cudaMemset(c->d_acc, 0, n3 * sizeof(double)));
-  TT_CUDA(c, cudaMemset(c->d_light, 0, n3 * sizeof(double)));
+  TT_CUDA(c, cudaMemsetAsync(c->d_acc, 0, n3 * sizeof(double), c->stream));
+  TT_CUDA(c, cudaMemsetAsync(c->d_light, 0, n3 * sizeof(double), c->stream));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
   std::fill(c->spp_count.begin(), c->spp_count.end(), 0);
   c->splat_count = 0;
   c->next_sample = 0;
@@ -1095,7 +1151,8 @@ tt_status tt_reset_stats(tt_ctx* c) {
   c->stats = tt_stats{};
   if (c->uploaded) {
     TT_CUDA(c, cudaSetDevice(c->device));
-    TT_CUDA(c, cudaMemset(c->d_stats, 0, 8 * sizeof(unsigned long long)));
+    TT_CUDA(c, cudaMemsetAsync(c->d_stats, 0, 8 * sizeof(unsigned long long), c->stream));
+    TT_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   return TT_OK;
 }
@@ -1118,7 +1175,10 @@ void tt_destroy(tt_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->path_mem.free_all();
   c->scene_mem.free_all();
-  if (c->stream) cudaStreamDestroy(c->stream);
+  if (c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
   delete c;
 }
 

@@ -180,5 +180,15 @@ void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, c
                       float* pdf, cudaStream_t st);
 // Blocks per SM that the shading kernel sustains (for grid sizing).
 int kernel_blocks_per_sm();
+// Framebuffer resolve: rgb = accum * inv_spp + splat_weight * light, per pixel.  inv_spp
+// is per pixel when `inv_spp_px` is not null, else the scalar applies to all pixels.
+void launch_resolve(const double* accum, const double* light, const double* inv_spp_px, double inv_spp,
+                    double splat_weight, int npix, float* rgb, cudaStream_t st);
+
+// Device memory from a per-device stream-ordered pool that keeps freed memory for reuse
+// (unlimited release threshold): contexts created and destroyed in a loop do not pay for
+// cudaMalloc / cudaFree of their path state each time.
+cudaError_t pool_malloc(void** p, size_t bytes, cudaStream_t st);
+void pool_free(void* p, cudaStream_t st);
 
 }  // namespace tt

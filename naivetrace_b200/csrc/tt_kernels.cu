@@ -1347,6 +1347,18 @@ void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, c
                       float* pdf, cudaStream_t st) {
   if (n > 0) k_eval_bsdf<<<grid_for(n), kBlock, 0, st>>>(s, material, wi, lambda, dirs, n, val, pdf);
 }
+__global__ void k_resolve(const double* accum, const double* light, const double* inv_spp_px, double inv_spp,
+                          double splat_weight, int npix, float* rgb) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * npix; i += gridDim.x * blockDim.x) {
+    const double inv = inv_spp_px ? inv_spp_px[i / 3] : inv_spp;
+    rgb[i] = (float)(accum[i] * inv + splat_weight * light[i]);
+  }
+}
+void launch_resolve(const double* accum, const double* light, const double* inv_spp_px, double inv_spp,
+                    double splat_weight, int npix, float* rgb, cudaStream_t st) {
+  if (npix > 0) k_resolve<<<grid_for(3 * npix), kBlock, 0, st>>>(accum, light, inv_spp_px, inv_spp, splat_weight, npix, rgb);
+}
+
 int kernel_blocks_per_sm() {
   int b = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_shade<false>, kBlock, 0);
