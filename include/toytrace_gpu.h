@@ -206,6 +206,10 @@ typedef struct tt_stats {
   uint32_t tri_bytes;
   uint32_t bvh_depth;
   uint64_t error_flags;         /* device error word (TT_ERR_* bits) */
+  uint64_t guide_records;       /* training records collected (learned guiding) */
+  uint64_t guide_steps;         /* Adam steps taken */
+  double guide_loss;            /* mean loss of the last training step */
+  double guide_train_ms;        /* summed CUDA-event time of training steps */
 } tt_stats;
 
 /* Queue lengths of the last wavefront wave of the last pass: for bounce b = 0..n-1,
@@ -323,6 +327,50 @@ tt_status tt_reset_stats(tt_ctx* ctx);
 
 /* Last error message of this context (or of the last failed tt_create when ctx is NULL). */
 tt_status tt_last_error(tt_ctx* ctx, char* buf, int32_t n);
+
+/* ---- Learned path guiding ----------------------------------------------------------
+ * The reference's guided path tracer (renderingalgorithms_pathtracing_guided.cxx) samples
+ * non-delta surface vertices from a vMF mixture combined with the BSDF by one-sample MIS
+ * (SampleWithBinaryMixtureDensity, :474-524), the mixtures being fitted per spatial cell
+ * from radiance records (path_guiding.cxx).  Here a small MLP maps (position, normal,
+ * outgoing direction) to an 8-lobe vMF mixture and to the probability of sampling it; it is
+ * trained online on the paths' own records by BF16 tensor-core kernels.  These entry
+ * points have no counterparts in the reference. */
+typedef struct tt_guiding_params {
+  int32_t enabled;              /* 1: guided sampling at diffuse and microfacet surfaces */
+  int32_t train;                /* 1: collect records and train after every pass;
+                                   2: collect records only (tt_guide_read_records) */
+  float learning_rate;          /* Adam step size (0: 1e-2) */
+  int32_t records_per_step;     /* record buffer and training batch (0: 262144) */
+  int32_t steps_per_pass;       /* Adam steps after each pass (0: 1) */
+  uint64_t seed;                /* weight initialisation */
+} tt_guiding_params;
+
+/* Enables or disables guiding.  The network is created (He-uniform weights from `seed`) on
+ * first use and keeps its trained weights while guiding is switched off and on again. */
+tt_status tt_set_guiding(tt_ctx* ctx, const tt_guiding_params* params);
+/* Number of network parameters (FP32 layout: per layer W[out][in] then b[out]). */
+int32_t tt_guide_num_params(void);
+tt_status tt_guide_get_params(tt_ctx* ctx, float* out, int32_t n);
+tt_status tt_guide_set_params(tt_ctx* ctx, const float* in, int32_t n);
+/* Network outputs (n x 48) for n rows of 96 input features (host buffers). */
+tt_status tt_guide_forward_batch(tt_ctx* ctx, const float* features, int32_t n, float* out);
+/* Mean-loss gradient (tt_guide_num_params floats) and the loss for n training records of
+ * 14 floats each: position in [0,1]^3, normal, outgoing direction, sampled direction,
+ * BSDF pdf of the sampled direction, F/q (host buffers). */
+tt_status tt_guide_gradient_batch(tt_ctx* ctx, const float* records, int32_t n, float* grad, float* loss);
+/* `steps` Adam steps of size learning_rate on n training records (layout as above; host
+ * buffer), the optimiser state carried over from earlier steps; *loss = the loss of the
+ * last step's gradient (may be NULL). */
+tt_status tt_guide_train_batch(tt_ctx* ctx, const float* records, int32_t n, int32_t steps, float learning_rate,
+                               float* loss);
+/* Copies up to max_records collected training records (14 floats each, layout above) to
+ * `out`, *n = the number copied, and empties the record buffer. */
+tt_status tt_guide_read_records(tt_ctx* ctx, float* out, int32_t max_records, int32_t* n);
+/* Feature encoding of n points (position in [0,1]^3, normal, outgoing direction: 9 floats
+ * each) into n x 96 features, as the renderer computes them. */
+tt_status tt_guide_features_batch(tt_ctx* ctx, const float* points, int32_t n, float* features);
+
 void tt_destroy(tt_ctx* ctx);
 
 #ifdef __cplusplus

@@ -170,6 +170,10 @@ class Stats(C.Structure):
         ("tri_bytes", C.c_uint32),
         ("bvh_depth", C.c_uint32),
         ("error_flags", C.c_uint64),
+        ("guide_records", C.c_uint64),
+        ("guide_steps", C.c_uint64),
+        ("guide_loss", C.c_double),
+        ("guide_train_ms", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -209,7 +213,28 @@ EXPORTED_SYMBOLS = [
     "tt_reset_stats",
     "tt_last_error",
     "tt_destroy",
+    "tt_set_guiding",
+    "tt_guide_num_params",
+    "tt_guide_get_params",
+    "tt_guide_set_params",
+    "tt_guide_forward_batch",
+    "tt_guide_gradient_batch",
+    "tt_guide_train_batch",
+    "tt_guide_read_records",
+    "tt_guide_features_batch",
 ]
+
+
+class GuidingParams(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_int32),
+        ("train", C.c_int32),
+        ("learning_rate", C.c_float),
+        ("records_per_step", C.c_int32),
+        ("steps_per_pass", C.c_int32),
+        ("seed", C.c_uint64),
+    ]
+
 
 _lib = None
 
@@ -266,6 +291,15 @@ def load_library() -> C.CDLL:
         "tt_reset_stats": ([vp], C.c_int32),
         "tt_last_error": ([vp, C.c_char_p, C.c_int32], C.c_int32),
         "tt_destroy": ([vp], None),
+        "tt_set_guiding": ([vp, P(GuidingParams)], C.c_int32),
+        "tt_guide_num_params": ([], C.c_int32),
+        "tt_guide_get_params": ([vp, P(C.c_float), C.c_int32], C.c_int32),
+        "tt_guide_set_params": ([vp, P(C.c_float), C.c_int32], C.c_int32),
+        "tt_guide_forward_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
+        "tt_guide_gradient_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_guide_train_batch": ([vp, P(C.c_float), C.c_int32, C.c_int32, C.c_float, P(C.c_float)], C.c_int32),
+        "tt_guide_read_records": ([vp, P(C.c_float), C.c_int32, P(C.c_int32)], C.c_int32),
+        "tt_guide_features_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
     }
     for name, (argtypes, restype) in sig.items():
         fn = getattr(lib, name)

@@ -147,6 +147,57 @@ class GpuContext:
     def reset_stats(self):
         self._check(self.lib.tt_reset_stats(self.h), "tt_reset_stats")
 
+    # Learned guiding ---------------------------------------------------------------
+    def set_guiding(self, enabled: bool = True, train: int = 1, learning_rate: float = 1e-2,
+                    records_per_step: int = 1 << 18, steps_per_pass: int = 1, seed: int = 1):
+        """train: 0 frozen, 1 collect records and train after every pass, 2 collect only."""
+        gp = abi.GuidingParams(int(enabled), int(train), learning_rate, records_per_step, steps_per_pass, seed)
+        self._check(self.lib.tt_set_guiding(self.h, C.byref(gp)), "tt_set_guiding")
+
+    def guide_params(self) -> np.ndarray:
+        n = self.lib.tt_guide_num_params()
+        out = np.zeros(n, np.float32)
+        self._check(self.lib.tt_guide_get_params(self.h, _fp(out), n), "tt_guide_get_params")
+        return out
+
+    def guide_set_params(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        self._check(self.lib.tt_guide_set_params(self.h, _fp(p), len(p)), "tt_guide_set_params")
+
+    def guide_forward(self, features: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 96)
+        out = np.zeros((len(x), 48), np.float32)
+        self._check(self.lib.tt_guide_forward_batch(self.h, _fp(x), len(x), _fp(out)), "tt_guide_forward_batch")
+        return out
+
+    def guide_gradient(self, records: np.ndarray):
+        r = np.ascontiguousarray(records, dtype=np.float32).reshape(-1, 14)
+        g = np.zeros(self.lib.tt_guide_num_params(), np.float32)
+        loss = C.c_float(0.0)
+        self._check(self.lib.tt_guide_gradient_batch(self.h, _fp(r), len(r), _fp(g), C.byref(loss)),
+                    "tt_guide_gradient_batch")
+        return float(loss.value), g
+
+    def guide_train(self, records: np.ndarray, steps: int, learning_rate: float) -> float:
+        r = np.ascontiguousarray(records, dtype=np.float32).reshape(-1, 14)
+        loss = C.c_float(0.0)
+        self._check(self.lib.tt_guide_train_batch(self.h, _fp(r), len(r), steps, learning_rate, C.byref(loss)),
+                    "tt_guide_train_batch")
+        return float(loss.value)
+
+    def guide_records(self, max_records: int = 1 << 20) -> np.ndarray:
+        """Collected training records (train = 2 collects without training), as (n, 14)."""
+        out = np.zeros((max_records, 14), np.float32)
+        n = C.c_int32(0)
+        self._check(self.lib.tt_guide_read_records(self.h, _fp(out), max_records, C.byref(n)), "tt_guide_read_records")
+        return out[: n.value]
+
+    def guide_features(self, points: np.ndarray) -> np.ndarray:
+        q = np.ascontiguousarray(points, dtype=np.float32).reshape(-1, 9)
+        out = np.zeros((len(q), 96), np.float32)
+        self._check(self.lib.tt_guide_features_batch(self.h, _fp(q), len(q), _fp(out)), "tt_guide_features_batch")
+        return out
+
     def request_interrupt(self):
         self.lib.tt_request_interrupt(self.h)
 
@@ -238,3 +289,59 @@ class GpuPathTracer:
 
 def to_image_host(rgb, xres, yres, linear_output=False):
     return to_image(rgb, xres, yres, linear_output)
+
+
+class GpuGuidedPathTracer(GpuPathTracer):
+    """RenderingAlgo for the learned-guided CUDA tracer (`--algo gpug`), with the pass
+    structure of the reference's guided tracer (PathTracingAlgo2::Run,
+    renderingalgorithms_pathtracing_guided.cxx:1110-1211): one initial pass, then training
+    sweeps of 2, 4, ... up to `guide_max_spp` one-sample passes, each starting from a cleared
+    framebuffer; then guiding is frozen (no more records) and the regular samples-per-pixel
+    schedule renders into a cleared framebuffer.  Training happens after every pass of a
+    sweep: `steps_per_pass` Adam steps on that pass's records."""
+
+    def __init__(self, scene: Scene, params: Optional[abi.Params] = None, seed: int = 1, linear_output: bool = False,
+                 guide_max_spp: int = 16, learning_rate: float = 1e-2, records_per_step: int = 1 << 18,
+                 steps_per_pass: int = 4, guide_seed: int = 1):
+        super().__init__(scene, params, seed, linear_output)
+        self.guide_max_spp = guide_max_spp
+        self.guiding = dict(learning_rate=learning_rate, records_per_step=records_per_step,
+                            steps_per_pass=steps_per_pass, seed=guide_seed)
+        self._pass_seed = seed
+
+    def _pass(self, spp: int) -> bool:
+        st = self.ctx.render_pass(spp, self._pass_seed)
+        self._pass_seed += 1
+        self.last_status = st
+        if st == abi.TT_ERR_INTERRUPTED:
+            return False
+        self.ctx._check(st, "tt_render_pass")
+        if self.ctx.poll_interrupt() and self._cb:
+            self._cb(False)
+        return True
+
+    def run(self):
+        self.initialize_scene()
+        self.ctx.set_guiding(True, 1, **self.guiding)
+        if not self.ctx.stop_requested():
+            if not self._pass(1):
+                return
+            if self._cb:
+                self._cb(True)
+        n = 2
+        while not self.ctx.stop_requested() and n <= self.guide_max_spp:
+            self.ctx.clear()
+            for _ in range(n):
+                if self.ctx.stop_requested() or not self._pass(1):
+                    return
+            if self._cb:
+                self._cb(True)
+            n *= 2
+        self.ctx.set_guiding(True, 0, **self.guiding)
+        self.ctx.clear()
+        while not self.ctx.stop_requested() and self.schedule.spp > 0:
+            if not self._pass(self.schedule.spp):
+                break
+            if self._cb:
+                self._cb(True)
+            self.schedule.update_for_next_pass()

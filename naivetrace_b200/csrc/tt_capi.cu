@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -15,6 +16,8 @@
 #include "../../include/toytrace_gpu.h"
 #include "tt_build.h"
 #include "tt_bvh.h"
+#include "tt_guide.cuh"
+#include "tt_guide.h"
 #include "tt_internal.h"
 #include "tt_tables.h"
 
@@ -135,6 +138,13 @@ struct tt_ctx {
   tt_stats stats{};
   std::string err;
   uint32_t bvh_nodes = 0, bvh_depth = 0, bvh_node_bytes = 64;
+  // Learned guiding.
+  std::unique_ptr<GuideNet> gnet;
+  tt_guiding_params gparams{};
+  GuideRecord* d_records = nullptr;
+  int* d_rec_count = nullptr;
+  int rec_cap = 0;
+  bool ps_guided = false;      // the path state carries the guiding arrays
 };
 
 static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
@@ -642,6 +652,10 @@ tt_status tt_upload_scene(tt_ctx* c) {
   if (c->verts.empty() && nsph == 0) for (int k = 0; k < 3; ++k) { lo[k] = hi[k] = 0; }
   const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
                                 (hi[2] - lo[2]) * (hi[2] - lo[2]));
+  for (int k = 0; k < 3; ++k) {
+    s.box_lo[k] = (float)lo[k];
+    s.box_inv[k] = hi[k] > lo[k] ? (float)(1.0 / (hi[k] - lo[k])) : 1.f;
+  }
   s.long_distance = (float)(10. * diag);
   s.max_path_nodes = c->params.max_ray_depth + 1;
   s.sample_lights = c->params.pt_sample_mode != TT_SAMPLE_BSDF;
@@ -691,7 +705,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
 }  // extern "C"
 
 static tt_status ensure_path_state(tt_ctx* c, int cap) {
-  if (c->ps.cap >= cap) return TT_OK;
+  const bool guided = c->dev.guide != 0;
+  if (c->ps.cap >= cap && c->ps_guided == guided) return TT_OK;
   cudaStreamSynchronize(c->stream);
   c->path_mem.free_all();
   PathState& p = c->ps;
@@ -720,6 +735,15 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
     p.sh_track = (uint2*)m.alloc(n * sizeof(uint2));
     p.sh_med = (float4*)m.alloc(n * sizeof(float4));
   }
+  if (guided) {
+    p.ginp = (float4*)m.alloc(n * 3 * sizeof(float4));
+    p.guide_q = (int*)m.alloc(n * sizeof(int));
+    p.grec = (float4*)m.alloc(n * 6 * sizeof(float4));
+    p.gnee = (float4*)m.alloc(n * sizeof(float4));
+    p.records = c->d_records;
+    p.rec_count = c->d_rec_count;
+    p.rec_cap = c->rec_cap;
+  }
   p.err = c->d_err;
   for (void* a : m.allocs)
     if (!a) {
@@ -728,6 +752,43 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
       return fail(c, TT_ERR_CUDA, "path state allocation failed (capacity " + std::to_string(cap) + ")");
     }
   p.cap = cap;
+  c->ps_guided = guided;
+  return TT_OK;
+}
+
+// Training on the records of the last pass: `steps_per_pass` Adam steps on one batch.
+static tt_status guide_train(tt_ctx* c) {
+  int n = 0;
+  TT_CUDA(c, cudaMemcpyAsync(&n, c->d_rec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  n = std::min(n, c->rec_cap);
+  if (n >= 256) {
+    std::string gerr;
+    if (!c->gnet->ensure_capacity(n, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, c->stream);
+    const int steps = c->gparams.steps_per_pass > 0 ? c->gparams.steps_per_pass : 1;
+    const float lr = c->gparams.learning_rate > 0.f ? c->gparams.learning_rate : 1e-2f;
+    for (int k = 0; k < steps; ++k) {
+      c->gnet->gradient(c->d_records, n, c->stream);
+      c->gnet->adam(lr, c->stream);
+    }
+    cudaEventRecord(b, c->stream);
+    float loss = 0.f, ms = 0.f;
+    cudaMemcpyAsync(&loss, c->gnet->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
+    TT_CUDA(c, cudaStreamSynchronize(c->stream));
+    TT_CUDA(c, cudaGetLastError());
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    c->stats.guide_records += (uint64_t)n;
+    c->stats.guide_steps += (uint64_t)steps;
+    c->stats.guide_loss = loss;
+    c->stats.guide_train_ms += ms;
+  }
+  TT_CUDA(c, cudaMemsetAsync(c->d_rec_count, 0, sizeof(int), c->stream));
   return TT_OK;
 }
 
@@ -741,6 +802,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
   const long long total = (long long)spp * npix_range;
   const int wave_limit = c->params.wave_paths > 0 ? c->params.wave_paths : kDefaultWave;
   const int cap = (int)std::min<long long>(total, wave_limit);
+  if (c->dev.guide_record) c->dev.guide_keep = (float)std::min(1.0, (double)c->rec_cap / (double)total);
   tt_status st = ensure_path_state(c, cap);
   if (st != TT_OK) return st;
   const bool counting = c->profiling >= 2;
@@ -786,17 +848,21 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
     launches++;
     for (int b = 0; b < rounds; ++b) {
       timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, b, counting, c->d_stats + 2, grid, c->stream); });
-      launch_flush(c->ps, c->fb, b, grid, c->stream);
+      launch_flush(c->dev, c->ps, c->fb, b, grid, c->stream);
       timed(0, [&] { launch_extend(c->dev, c->ps, b, counting, c->d_stats, grid, c->stream); });
       if (c->dev.num_media > 0) {
         launch_track(c->dev, c->ps, b, grid, c->stream);
         launches++;
       }
       launch_shade(c->dev, c->ps, b, grid, c->stream);
+      if (c->dev.guide) {
+        launch_guide(c->dev, c->ps, b, c->stream);
+        launches++;
+      }
       launches += 4;
     }
     timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, rounds, counting, c->d_stats + 2, grid, c->stream); });
-    launch_flush(c->ps, c->fb, rounds, grid, c->stream);
+    launch_flush(c->dev, c->ps, c->fb, rounds, grid, c->stream);
     k_tally<<<1, 32, 0, c->stream>>>(c->ps.counters, rounds, c->d_stats);
     launches += 3;
     cudaEventRecord(wave_ev[wave_index & 1], c->stream);
@@ -832,6 +898,10 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
   for (int px = pb; px < pe; ++px) c->spp_count[px] += (uint64_t)spp;
   c->splat_count += (uint64_t)spp * (uint64_t)npix_range;
   c->next_sample += (uint64_t)spp;
+  if (c->dev.guide_record && !stopped && c->gparams.train == 1) {
+    const tt_status gs = guide_train(c);
+    if (gs != TT_OK) return gs;
+  }
   unsigned int errw = 0;
   TT_CUDA(c, cudaMemcpy(&errw, c->d_err, sizeof(errw), cudaMemcpyDeviceToHost));
   if (errw) {
@@ -1173,6 +1243,9 @@ void tt_destroy(tt_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->d_records) cudaFree(c->d_records);
+  if (c->d_rec_count) cudaFree(c->d_rec_count);
+  c->gnet.reset();
   c->path_mem.free_all();
   c->scene_mem.free_all();
   if (c->stream) {
@@ -1180,6 +1253,180 @@ void tt_destroy(tt_ctx* c) {
     cudaStreamDestroy(c->stream);
   }
   delete c;
+}
+
+// ---- Learned guiding ----------------------------------------------------------------
+tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
+  if (!c || !gp) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (!gp->enabled) {
+    c->dev.guide = 0;
+    c->dev.guide_record = 0;
+    c->gparams = *gp;
+    return TT_OK;
+  }
+  if (gp->records_per_step < 0 || gp->steps_per_pass < 0 || !(gp->learning_rate >= 0.f) || gp->train < 0 ||
+      gp->train > 2)
+    return fail(c, TT_ERR_INVALID, "bad guiding parameters");
+  const int cap = gp->records_per_step > 0 ? gp->records_per_step : (1 << 18);
+  if (!c->gnet) {
+    c->gnet = std::make_unique<GuideNet>();
+    std::string gerr;
+    if (!c->gnet->init(gp->seed, &gerr)) {
+      c->gnet.reset();
+      return fail(c, TT_ERR_CUDA, gerr);
+    }
+  }
+  if (cap != c->rec_cap) {
+    if (c->d_records) cudaFree(c->d_records);
+    c->d_records = nullptr;
+    c->rec_cap = 0;
+    TT_CUDA(c, cudaMalloc(&c->d_records, (size_t)cap * sizeof(GuideRecord)));
+    if (!c->d_rec_count) TT_CUDA(c, cudaMalloc(&c->d_rec_count, sizeof(int)));
+    c->rec_cap = cap;
+    c->ps_guided = false;  // the path state picks up the new record buffer
+  }
+  TT_CUDA(c, cudaMemset(c->d_rec_count, 0, sizeof(int)));
+  c->gparams = *gp;
+  c->dev.guide_w16 = c->gnet->params16;
+  c->dev.guide_w32 = c->gnet->params;
+  c->dev.guide = 1;
+  c->dev.guide_record = gp->train ? 1 : 0;
+  return TT_OK;
+}
+
+int32_t tt_guide_num_params(void) { return kGParams; }
+
+static tt_status guide_prep(tt_ctx* c) {
+  if (!c) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  if (!c->gnet) {
+    c->gnet = std::make_unique<GuideNet>();
+    std::string gerr;
+    if (!c->gnet->init(1, &gerr)) {
+      c->gnet.reset();
+      return fail(c, TT_ERR_CUDA, gerr);
+    }
+  }
+  return TT_OK;
+}
+
+tt_status tt_guide_get_params(tt_ctx* c, float* out, int32_t n) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!out || n != kGParams) return fail(c, TT_ERR_INVALID, "parameter count mismatch");
+  TT_CUDA(c, cudaMemcpy(out, c->gnet->params, kGParams * sizeof(float), cudaMemcpyDeviceToHost));
+  return TT_OK;
+}
+
+tt_status tt_guide_set_params(tt_ctx* c, const float* in, int32_t n) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!in || n != kGParams) return fail(c, TT_ERR_INVALID, "parameter count mismatch");
+  std::string gerr;
+  if (!c->gnet->set_params(in, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
+  return TT_OK;
+}
+
+tt_status tt_guide_forward_batch(tt_ctx* c, const float* features, int32_t n, float* out) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!features || !out || n <= 0) return fail(c, TT_ERR_INVALID, "bad batch");
+  std::string gerr;
+  if (!c->gnet->ensure_capacity(n, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
+  std::vector<__nv_bfloat16> x((size_t)n * kGIn);
+  for (size_t i = 0; i < x.size(); ++i) x[i] = __float2bfloat16(features[i]);
+  TT_CUDA(c, cudaMemcpy(c->gnet->x0, x.data(), x.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
+  c->gnet->forward(c->gnet->x0, n, c->gnet->out, c->stream);
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  TT_CUDA(c, cudaGetLastError());
+  TT_CUDA(c, cudaMemcpy(out, c->gnet->out, (size_t)n * kGOut * sizeof(float), cudaMemcpyDeviceToHost));
+  return TT_OK;
+}
+
+// Copies n host records to a temporary device buffer, runs `steps` gradients (and Adam
+// steps when train is set) and releases the buffer.
+static tt_status guide_batch(tt_ctx* c, const float* records, int32_t n, int32_t steps, bool train, float lr) {
+  static_assert(sizeof(GuideRecord) == 14 * sizeof(float), "record layout");
+  std::string gerr;
+  if (!c->gnet->ensure_capacity(n, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
+  GuideRecord* d = nullptr;
+  TT_CUDA(c, cudaMalloc(&d, (size_t)n * sizeof(GuideRecord)));
+  cudaError_t e = cudaMemcpy(d, records, (size_t)n * sizeof(GuideRecord), cudaMemcpyHostToDevice);
+  for (int k = 0; k < steps && e == cudaSuccess; ++k) {
+    c->gnet->gradient(d, n, c->stream);
+    if (train) c->gnet->adam(lr, c->stream);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+tt_status tt_guide_gradient_batch(tt_ctx* c, const float* records, int32_t n, float* grad, float* loss) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!records || !grad || n <= 0) return fail(c, TT_ERR_INVALID, "bad batch");
+  st = guide_batch(c, records, n, 1, false, 0.f);
+  if (st != TT_OK) return st;
+  TT_CUDA(c, cudaMemcpy(grad, c->gnet->grad, kGParams * sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) TT_CUDA(c, cudaMemcpy(loss, c->gnet->loss, sizeof(float), cudaMemcpyDeviceToHost));
+  return TT_OK;
+}
+
+tt_status tt_guide_train_batch(tt_ctx* c, const float* records, int32_t n, int32_t steps, float lr, float* loss) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!records || n <= 0 || steps < 0 || !(lr >= 0.f)) return fail(c, TT_ERR_INVALID, "bad batch");
+  st = guide_batch(c, records, n, steps, true, lr);
+  if (st != TT_OK) return st;
+  if (loss) TT_CUDA(c, cudaMemcpy(loss, c->gnet->loss, sizeof(float), cudaMemcpyDeviceToHost));
+  return TT_OK;
+}
+
+tt_status tt_guide_read_records(tt_ctx* c, float* out, int32_t max_records, int32_t* n) {
+  if (!c || !out || !n || max_records < 0) return TT_ERR_INVALID;
+  *n = 0;
+  if (!c->d_rec_count) return TT_OK;
+  TT_CUDA(c, cudaSetDevice(c->device));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  int cnt = 0;
+  TT_CUDA(c, cudaMemcpy(&cnt, c->d_rec_count, sizeof(int), cudaMemcpyDeviceToHost));
+  cnt = std::min(std::min(cnt, c->rec_cap), max_records);
+  if (cnt > 0) TT_CUDA(c, cudaMemcpy(out, c->d_records, (size_t)cnt * sizeof(GuideRecord), cudaMemcpyDeviceToHost));
+  TT_CUDA(c, cudaMemset(c->d_rec_count, 0, sizeof(int)));
+  *n = cnt;
+  return TT_OK;
+}
+
+tt_status tt_guide_features_batch(tt_ctx* c, const float* points, int32_t n, float* features) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!points || !features || n <= 0) return fail(c, TT_ERR_INVALID, "bad batch");
+  float* dp = nullptr;
+  __nv_bfloat16* dx = nullptr;
+  TT_CUDA(c, cudaMalloc(&dp, (size_t)n * 9 * sizeof(float)));
+  if (cudaMalloc(&dx, (size_t)n * kGIn * sizeof(__nv_bfloat16)) != cudaSuccess) {
+    cudaFree(dp);
+    return fail(c, TT_ERR_CUDA, "allocation failed");
+  }
+  cudaError_t e = cudaMemcpy(dp, points, (size_t)n * 9 * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    c->gnet->features(dp, n, dx, c->stream);
+    e = cudaStreamSynchronize(c->stream);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  std::vector<__nv_bfloat16> hx((size_t)n * kGIn);
+  if (e == cudaSuccess) e = cudaMemcpy(hx.data(), dx, hx.size() * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost);
+  cudaFree(dp);
+  cudaFree(dx);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  for (size_t i = 0; i < hx.size(); ++i) features[i] = __bfloat162float(hx[i]);
+  return TT_OK;
 }
 
 }  // extern "C"

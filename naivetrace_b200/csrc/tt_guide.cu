@@ -1,0 +1,541 @@
+// Training and batch evaluation of the guiding network on the GPU.  Training follows the
+// KL-divergence objective of neural importance sampling (Mueller et al. 2019): for a record
+// sampled with density q at direction wi with target value F, minimise -(F / q) log p(wi)
+// with p = (1 - c) p_bsdf + c p_vmf, which also learns the selection probability c.
+//
+// One training step is four launches:
+//   k_train   persistent; per warp 32 records: features in registers, the five layers
+//             (guide_mlp_tile, activations kept in global memory for the weight gradients),
+//             the loss gradient per record, and the backward pass through the layers on the
+//             same tensor-core tiles (B fragments of W^T by ldmatrix.trans from the forward
+//             weight image), storing each layer's output gradient;
+//   k_wgrad   dW_l = sum over records of dH_l^T X_l and the bias sums, split over chunks of
+//             512 records (mma.sync with ldmatrix.trans fragments of both operands);
+//   k_reduce  sum of the chunk partials;
+//   k_adam    Adam on the FP32 master parameters, refreshing the BF16 copy.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "tt_guide.cuh"
+#include "tt_guide.h"
+#include "tt_internal.h"
+
+namespace tt {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ void ldsm_x4_trans(uint32_t (&r)[4], const void* row) {
+  const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(row));
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(a));
+}
+
+__device__ __forceinline__ float lo_bf16(uint32_t v) { return __uint_as_float(v << 16); }
+__device__ __forceinline__ float hi_bf16(uint32_t v) { return __uint_as_float(v & 0xffff0000u); }
+
+// Loss -(F/q) log p(wi), p = (1 - c) p_bsdf + c p_vmf, of one record with network outputs o,
+// and its gradient with respect to the 41 outputs into d[0..47] (padded columns zero).
+__device__ float guide_loss_row(const GuideRecord& r, const float* o, float* d) {
+  const float w = r.f_over_q;
+  const float3 x = f3(r.wi[0], r.wi[1], r.wi[2]);
+  float mx = -INFINITY;
+  for (int k = 0; k < kGLobes; ++k) mx = fmaxf(mx, o[5 * k]);
+  float pi_[kGLobes], sum = 0.f;
+  for (int k = 0; k < kGLobes; ++k) {
+    pi_[k] = expf(o[5 * k] - mx);
+    sum += pi_[k];
+  }
+  float v[kGLobes], pv = 0.f, mlen[kGLobes], kap[kGLobes], kslope[kGLobes];
+  float3 mu[kGLobes];
+  for (int k = 0; k < kGLobes; ++k) {
+    pi_[k] /= sum;
+    const float3 m = f3(o[5 * k + 1], o[5 * k + 2], o[5 * k + 3]);
+    mlen[k] = len3(m);
+    mu[k] = mlen[k] > 1e-12f ? m * (1.f / mlen[k]) : f3(0.f, 0.f, 1.f);
+    const float th = tanhf((o[5 * k + 4] - kGLogKappaMid) / kGLogKappaHalf);
+    kslope[k] = 1.f - th * th;  // d log kappa / d output
+    kap[k] = expf(kGLogKappaMid + kGLogKappaHalf * th);
+    v[k] = kap[k] / (2.f * kPi * (1.f - expf(-2.f * kap[k]))) * expf(kap[k] * (dot3(mu[k], x) - 1.f));
+    pv += pi_[k] * v[k];
+  }
+  const float sg = 1.f / (1.f + expf(-o[5 * kGLobes]));
+  const float c = kGGuideProbMin + kGGuideProbSpan * sg;
+  const float pp = fmaxf((1.f - c) * r.p_bsdf + c * pv, 1e-20f);
+  const float loss = w > 0.f ? -w * logf(pp) : 0.f;
+  const float dLdp = w > 0.f ? -w / pp : 0.f;
+  const float dLdpv = dLdp * c;
+  for (int k = 0; k < kGLobes; ++k) {
+    // Softmax: d pv / d a_k = pi_k (v_k - pv).
+    d[5 * k] = dLdpv * pi_[k] * (v[k] - pv);
+    // d v_k / d mu_k = v_k kappa_k x, projected through the normalisation of m.
+    const float s = dLdpv * pi_[k] * v[k] * kap[k];
+    float3 dm = f3(0.f, 0.f, 0.f);
+    if (mlen[k] > 1e-12f) {
+      const float3 gx = x * s;
+      dm = (gx - mu[k] * dot3(mu[k], gx)) * (1.f / mlen[k]);
+    }
+    d[5 * k + 1] = dm.x;
+    d[5 * k + 2] = dm.y;
+    d[5 * k + 3] = dm.z;
+    // d log v_k / d kappa = 1/kappa - 2 exp(-2 kappa) / (1 - exp(-2 kappa)) + (mu.x - 1),
+    // times d kappa / d output = kappa kslope.
+    const float e2 = expf(-2.f * kap[k]);
+    const float dlogv = 1.f / kap[k] - 2.f * e2 / (1.f - e2) + (dot3(mu[k], x) - 1.f);
+    d[5 * k + 4] = dLdpv * pi_[k] * v[k] * dlogv * kap[k] * kslope[k];
+  }
+  d[5 * kGLobes] = dLdp * (pv - r.p_bsdf) * kGGuideProbSpan * sg * (1.f - sg);
+  for (int k = 5 * kGLobes + 1; k < kGOut; ++k) d[k] = 0.f;
+  return loss;
+}
+
+struct TrainBufs {
+  bf16* x;       // features (kGIn per record)
+  bf16* h[4];    // hidden activations (kGHid)
+  bf16* dh[4];   // gradients of the hidden layers' pre-activations (kGHid)
+  bf16* dy;      // gradient of the outputs (kGOut)
+  float* loss;   // mean loss
+};
+
+// Backward pass of one 16-row tile: dY (shared memory, 16 x kGOut BF16, row stride dys)
+// through layers 4..1: dH_{l-1} = (dH_l W_l) masked by H_{l-1} > 0, rounded to BF16,
+// stored for the weight gradients.
+__device__ __forceinline__ void guide_bwd_tile(const bf16* sw, const bf16* dyt, int dys, const TrainBufs& b,
+                                               int row0, int rows) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  uint32_t af[4][4];
+#pragma unroll
+  for (int kc = 0; kc < 3; ++kc) {
+    const int c = kc * 16 + 2 * t;
+    af[kc][0] = ld_u32(dyt + g * dys + c);
+    af[kc][1] = ld_u32(dyt + (g + 8) * dys + c);
+    af[kc][2] = ld_u32(dyt + g * dys + c + 8);
+    af[kc][3] = ld_u32(dyt + (g + 8) * dys + c + 8);
+  }
+  af[3][0] = af[3][1] = af[3][2] = af[3][3] = 0u;
+  // ldmatrix lane roles: matrix mi = lane / 8 gets its row (lane % 8) address from this lane.
+  const int mi = lane >> 3, mr = lane & 7;
+#pragma unroll 1
+  for (int l = kGLayers - 1; l >= 1; --l) {
+    const int nk = l == kGLayers - 1 ? 3 : 4;  // K chunks over this layer's outputs
+    float acc[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+    const bf16* w = sw + guide_sm_w(l);
+    const int ws = guide_sm_stride(l);
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {
+      if (kc >= nk) break;
+#pragma unroll
+      for (int jp = 0; jp < 4; ++jp) {
+        // Blocks of W (rows k = outputs, columns n = inputs): (k 0-7, n 0-7), (k 8-15, n 0-7),
+        // (k 0-7, n 8-15), (k 8-15, n 8-15): b0, b1 of n-tile 2jp, then of 2jp + 1.
+        uint32_t bf[4];
+        ldsm_x4_trans(bf, w + (kc * 16 + (mi & 1) * 8 + mr) * ws + jp * 16 + (mi >> 1) * 8);
+        mma_bf16_16816(acc[2 * jp], af[kc], bf[0], bf[1]);
+        mma_bf16_16816(acc[2 * jp + 1], af[kc], bf[2], bf[3]);
+      }
+    }
+    // Mask by the ReLU of H_{l-1}, read in the A-fragment layout that matches the
+    // accumulator of the two 8-column tiles 2kc and 2kc + 1.
+    const bf16* hp = b.h[l - 1];
+    const int ra = row0 + g, rb = ra + 8;
+#pragma unroll
+    for (int kc = 0; kc < 4; ++kc) {
+      const int c = kc * 16 + 2 * t;
+      const uint32_t h0 = g < rows ? ld_u32(hp + (size_t)ra * kGHid + c) : 0u;
+      const uint32_t h1 = g + 8 < rows ? ld_u32(hp + (size_t)rb * kGHid + c) : 0u;
+      const uint32_t h2 = g < rows ? ld_u32(hp + (size_t)ra * kGHid + c + 8) : 0u;
+      const uint32_t h3 = g + 8 < rows ? ld_u32(hp + (size_t)rb * kGHid + c + 8) : 0u;
+      af[kc][0] = pack_bf16x2(lo_bf16(h0) > 0.f ? acc[2 * kc][0] : 0.f, hi_bf16(h0) > 0.f ? acc[2 * kc][1] : 0.f);
+      af[kc][1] = pack_bf16x2(lo_bf16(h1) > 0.f ? acc[2 * kc][2] : 0.f, hi_bf16(h1) > 0.f ? acc[2 * kc][3] : 0.f);
+      af[kc][2] = pack_bf16x2(lo_bf16(h2) > 0.f ? acc[2 * kc + 1][0] : 0.f, hi_bf16(h2) > 0.f ? acc[2 * kc + 1][1] : 0.f);
+      af[kc][3] = pack_bf16x2(lo_bf16(h3) > 0.f ? acc[2 * kc + 1][2] : 0.f, hi_bf16(h3) > 0.f ? acc[2 * kc + 1][3] : 0.f);
+    }
+    guide_store_frags<4>(b.dh[l - 1], kGHid, af, row0, rows);
+  }
+}
+
+constexpr int kTrainWarps = 4;
+constexpr int kDyStride = kGOut + 8;  // BF16 output-gradient row in shared memory
+constexpr int kTrainWarpBytes = 32 * kGInputs * 4 + 32 * kGOutStride * 4 + 32 * kDyStride * 2;
+constexpr int kTrainSmem = kGSmBytes + kTrainWarps * kTrainWarpBytes;
+static_assert(kTrainWarpBytes % 16 == 0, "per-warp regions stay 16-byte aligned");
+
+__global__ void __launch_bounds__(kTrainWarps * 32) k_train(const GuideRecord* __restrict__ rec, int n,
+                                                            const bf16* __restrict__ w16,
+                                                            const float* __restrict__ w32, TrainBufs b) {
+  extern __shared__ __align__(16) unsigned char tsm[];
+  bf16* sw = reinterpret_cast<bf16*>(tsm);
+  float* sb = reinterpret_cast<float*>(tsm + kGSmW * 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  unsigned char* wsm = tsm + kGSmBytes + warp * kTrainWarpBytes;
+  float* q = reinterpret_cast<float*>(wsm);
+  float* o = q + 32 * kGInputs;
+  bf16* dys = reinterpret_cast<bf16*>(o + 32 * kGOutStride);
+  if (blockIdx.x * kTrainWarps * 32 >= n) return;
+  guide_smem_load(w16, w32, sw, sb);
+  __syncthreads();
+  const float inv_n = 1.f / (float)n;
+  float lsum = 0.f;
+  for (int base = (blockIdx.x * kTrainWarps + warp) * 32; base < n; base += gridDim.x * kTrainWarps * 32) {
+    const int i = base + lane;
+    GuideRecord r{};
+    if (i < n) r = rec[i];
+    float* qr = q + lane * kGInputs;
+    qr[0] = r.pos[0]; qr[1] = r.pos[1]; qr[2] = r.pos[2];
+    qr[3] = r.n[0]; qr[4] = r.n[1]; qr[5] = r.n[2];
+    qr[6] = r.wo[0]; qr[7] = r.wo[1]; qr[8] = r.wo[2];
+    __syncwarp();
+#pragma unroll 1
+    for (int mt = 0; mt < 2; ++mt) {
+      GuideTileStore st{b.x, {b.h[0], b.h[1], b.h[2], b.h[3]}, base + mt * 16, n - (base + mt * 16)};
+      uint32_t xf[6][4];
+      guide_tile_features(q + mt * 16 * kGInputs, kGInputs, xf);
+      guide_mlp_tile(sw, sb, xf, o + mt * 16 * kGOutStride, kGOutStride, &st);
+    }
+    __syncwarp();
+    // Loss and output gradient of record `lane`, divided by n and rounded to BF16.
+    {
+      float d[kGOut];
+      if (i < n) {
+        lsum += guide_loss_row(r, o + lane * kGOutStride, d);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kGOut; ++k) d[k] = 0.f;
+      }
+      uint32_t pk[kGOut / 2];
+#pragma unroll
+      for (int k = 0; k < kGOut / 2; ++k) pk[k] = pack_bf16x2(d[2 * k] * inv_n, d[2 * k + 1] * inv_n);
+      uint4* srow = reinterpret_cast<uint4*>(dys + lane * kDyStride);
+#pragma unroll
+      for (int k = 0; k < kGOut / 8; ++k) srow[k] = make_uint4(pk[4 * k], pk[4 * k + 1], pk[4 * k + 2], pk[4 * k + 3]);
+      if (i < n) {
+        uint4* grow = reinterpret_cast<uint4*>(b.dy + (size_t)i * kGOut);
+#pragma unroll
+        for (int k = 0; k < kGOut / 8; ++k) grow[k] = srow[k];
+      }
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int mt = 0; mt < 2; ++mt)
+      guide_bwd_tile(sw, dys + mt * 16 * kDyStride, kDyStride, b, base + mt * 16, n - (base + mt * 16));
+    __syncwarp();
+  }
+  for (int s = 16; s > 0; s >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, s);
+  if (lane == 0 && lsum != 0.f) atomicAdd(b.loss, lsum * inv_n);
+}
+
+// Weight and bias gradients of layer blockIdx.y over records [blockIdx.x * kWgChunk, +kWgChunk):
+// dW[o][i] = sum_r G[r][o] X[r][i] (G = the layer's output gradient, X its input) as an
+// M = outputs, N = inputs, K = records product; both operands are staged record-major in
+// shared memory and read transposed by ldmatrix.trans.  Partials go to
+// partial[blockIdx.x][guide_w_offset / guide_b_offset].
+constexpr int kWgRows = 32;
+constexpr int kWgChunk = 512;
+constexpr int kWgGs = kGHid + 8;
+constexpr int kWgXs = kGIn + 8;
+
+__global__ void __launch_bounds__(128) k_wgrad(int n, TrainBufs b, float* __restrict__ partial) {
+  __shared__ __align__(16) bf16 Gs[kWgRows * kWgGs];
+  __shared__ __align__(16) bf16 Xs[kWgRows * kWgXs];
+  const int l = blockIdx.y;
+  const int out = guide_out(l), in = guide_in(l);
+  const bf16* G = l == kGLayers - 1 ? b.dy : b.dh[l];
+  const bf16* X = l == 0 ? b.x : b.h[l - 1];
+  const int r0 = blockIdx.x * kWgChunk, r1 = min(n, r0 + kWgChunk);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int mi = lane >> 3, mr = lane & 7;
+  const bool active = warp * 16 < out;
+  float acc[12][4];
+#pragma unroll
+  for (int j = 0; j < 12; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  float bsum = 0.f;
+  const int gch = out / 8, xch = in / 8;  // 16-byte chunks per row
+  for (int rr = r0; rr < r1; rr += kWgRows) {
+    for (int e = tid; e < kWgRows * gch; e += blockDim.x) {
+      const int r = e / gch, c = e - r * gch;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (rr + r < r1) v = *reinterpret_cast<const uint4*>(G + (size_t)(rr + r) * out + c * 8);
+      *reinterpret_cast<uint4*>(Gs + r * kWgGs + c * 8) = v;
+    }
+    for (int e = tid; e < kWgRows * xch; e += blockDim.x) {
+      const int r = e / xch, c = e - r * xch;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (rr + r < r1) v = *reinterpret_cast<const uint4*>(X + (size_t)(rr + r) * in + c * 8);
+      *reinterpret_cast<uint4*>(Xs + r * kWgXs + c * 8) = v;
+    }
+    __syncthreads();
+    if (tid < out)
+      for (int r = 0; r < kWgRows; ++r) bsum += __bfloat162float(Gs[r * kWgGs + tid]);
+    if (active) {
+#pragma unroll
+      for (int ks = 0; ks < kWgRows; ks += 16) {
+        // A(m = output, k = record) from Gs[record][output]: blocks (m 0-7, k 0-7),
+        // (m 8-15, k 0-7), (m 0-7, k 8-15), (m 8-15, k 8-15).
+        uint32_t a[4];
+        ldsm_x4_trans(a, Gs + (ks + (mi >> 1) * 8 + mr) * kWgGs + warp * 16 + (mi & 1) * 8);
+#pragma unroll
+        for (int jp = 0; jp < 6; ++jp) {
+          if (jp * 16 >= in) break;
+          // B(k = record, n = input) from Xs[record][input]: blocks (k 0-7, n 0-7),
+          // (k 8-15, n 0-7), (k 0-7, n 8-15), (k 8-15, n 8-15).
+          uint32_t bb[4];
+          ldsm_x4_trans(bb, Xs + (ks + (mi & 1) * 8 + mr) * kWgXs + jp * 16 + (mi >> 1) * 8);
+          mma_bf16_16816(acc[2 * jp], a, bb[0], bb[1]);
+          mma_bf16_16816(acc[2 * jp + 1], a, bb[2], bb[3]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  float* pw = partial + (size_t)blockIdx.x * kGParams;
+  if (active) {
+    const int m = warp * 16 + g;
+#pragma unroll
+    for (int j = 0; j < 12; ++j) {
+      if (j * 8 >= in) break;
+      const int c = j * 8 + 2 * t;
+      pw[guide_w_offset(l) + m * in + c] = acc[j][0];
+      pw[guide_w_offset(l) + m * in + c + 1] = acc[j][1];
+      pw[guide_w_offset(l) + (m + 8) * in + c] = acc[j][2];
+      pw[guide_w_offset(l) + (m + 8) * in + c + 1] = acc[j][3];
+    }
+  }
+  if (tid < out) pw[guide_b_offset(l) + tid] = bsum;
+}
+
+__global__ void k_reduce(const float* __restrict__ part, int z, float* __restrict__ g) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGParams; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int k = 0; k < z; ++k) s += part[(size_t)k * kGParams + i];
+    g[i] = s;
+  }
+}
+
+// Forward pass of n rows of BF16 features (kGIn per row) into FP32 outputs (kGOut per row).
+constexpr int kFwdWarps = 4;
+constexpr int kFwdSmem = kGSmBytes + kFwdWarps * 16 * kGOutStride * 4;
+
+__global__ void __launch_bounds__(kFwdWarps * 32) k_forward_x(const bf16* __restrict__ x, int n,
+                                                              const bf16* __restrict__ w16,
+                                                              const float* __restrict__ w32, float* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char fsm[];
+  bf16* sw = reinterpret_cast<bf16*>(fsm);
+  float* sb = reinterpret_cast<float*>(fsm + kGSmW * 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* o = reinterpret_cast<float*>(fsm + kGSmBytes) + warp * 16 * kGOutStride;
+  guide_smem_load(w16, w32, sw, sb);
+  __syncthreads();
+  for (int row0 = (blockIdx.x * kFwdWarps + warp) * 16; row0 < n; row0 += gridDim.x * kFwdWarps * 16) {
+    uint32_t xf[6][4];
+    guide_tile_load_x(x + (size_t)row0 * kGIn, n - row0, xf);
+    guide_mlp_tile(sw, sb, xf, o, kGOutStride, nullptr);
+    __syncwarp();
+    for (int e = lane; e < 16 * kGOut; e += 32) {
+      const int r = e / kGOut, c = e - r * kGOut;
+      if (row0 + r < n) out[(size_t)(row0 + r) * kGOut + c] = o[r * kGOutStride + c];
+    }
+    __syncwarp();
+  }
+}
+
+// Feature rows (BF16, kGIn) of n points given as 9 floats (p01, normal, wo): the input
+// fragments the kernels above build, stored.
+__global__ void __launch_bounds__(128) k_features(const float* __restrict__ pts, int n, bf16* __restrict__ x) {
+  __shared__ float q[4][16 * kGInputs];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int row0 = (blockIdx.x * 4 + warp) * 16; row0 < n; row0 += gridDim.x * 4 * 16) {
+    for (int e = lane; e < 16 * kGInputs; e += 32) {
+      const int r = e / kGInputs;
+      q[warp][e] = row0 + r < n ? pts[(size_t)row0 * kGInputs + e] : 0.f;
+    }
+    __syncwarp();
+    uint32_t xf[6][4];
+    guide_tile_features(q[warp], kGInputs, xf);
+    guide_store_frags<6>(x, kGIn, xf, row0, n - row0);
+    __syncwarp();
+  }
+}
+
+// Adam (Kingma and Ba 2015) on the FP32 master parameters, refreshing the BF16 copy.
+__global__ void k_adam(float* p, float* m, float* v, const float* g, int n, float lr, float b1, float b2, float eps,
+                       float bc1, float bc2, bf16* w16) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+    p[i] = pi;
+    w16[i] = __float2bfloat16(pi);
+  }
+}
+
+__global__ void k_to_bf16(const float* p, int n, bf16* w16) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w16[i] = __float2bfloat16(p[i]);
+}
+
+int grid1(long long n) {
+  long long g = (n + 255) / 256;
+  return (int)(g < 1 ? 1 : (g > 8192 ? 8192 : g));
+}
+
+int persistent_grid(const void* fn, int threads, int smem, long long work_blocks) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+  const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  return (int)std::max(1LL, std::min(cap, work_blocks));
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------------------
+GuideNet::~GuideNet() { release(); }
+
+void GuideNet::release() {
+  for (void* p : allocs) cudaFree(p);
+  allocs.clear();
+  for (void* p : scratch) cudaFree(p);
+  scratch.clear();
+  params = adam_m = adam_v = grad = loss = nullptr;
+  params16 = nullptr;
+  cap = 0;
+}
+
+template <class T>
+static T* galloc(std::vector<void*>& allocs, size_t n) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, (n ? n : 1) * sizeof(T)) != cudaSuccess) return nullptr;
+  allocs.push_back(p);
+  return static_cast<T*>(p);
+}
+
+bool GuideNet::init(uint64_t seed, std::string* err) {
+  release();
+  static bool attrs = false;
+  if (!attrs) {
+    cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, kTrainSmem);
+    cudaFuncSetAttribute(k_forward_x, cudaFuncAttributeMaxDynamicSharedMemorySize, kFwdSmem);
+    attrs = true;
+  }
+  params = galloc<float>(allocs, kGParams);
+  adam_m = galloc<float>(allocs, kGParams);
+  adam_v = galloc<float>(allocs, kGParams);
+  grad = galloc<float>(allocs, kGParams);
+  params16 = galloc<bf16>(allocs, kGParams);
+  loss = galloc<float>(allocs, 1);
+  if (!params || !adam_m || !adam_v || !grad || !params16 || !loss) {
+    *err = "guiding network: device allocation failed";
+    return false;
+  }
+  // He-uniform initialisation (the output layer scaled by 0.1); zero biases.
+  std::vector<float> h(kGParams, 0.f);
+  std::mt19937_64 rng(seed);
+  for (int l = 0; l < kGLayers; ++l) {
+    const float lim = std::sqrt(6.f / (float)guide_in(l)) * (l == kGLayers - 1 ? 0.1f : 1.f);
+    std::uniform_real_distribution<float> U(-lim, lim);
+    for (int i = 0; i < guide_in(l) * guide_out(l); ++i) h[guide_w_offset(l) + i] = U(rng);
+  }
+  cudaMemcpy(params, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice);
+  cudaMemset(adam_m, 0, kGParams * sizeof(float));
+  cudaMemset(adam_v, 0, kGParams * sizeof(float));
+  k_to_bf16<<<grid1(kGParams), 256>>>(params, kGParams, params16);
+  step = 0;
+  const cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    *err = std::string("guiding network init: ") + cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+bool GuideNet::set_params(const float* host, std::string* err) {
+  cudaMemcpy(params, host, kGParams * sizeof(float), cudaMemcpyHostToDevice);
+  k_to_bf16<<<grid1(kGParams), 256>>>(params, kGParams, params16);
+  const cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    *err = cudaGetErrorString(e);
+    return false;
+  }
+  return true;
+}
+
+bool GuideNet::ensure_capacity(int n, std::string* err) {
+  if (n <= cap) return true;
+  for (void*& p : scratch) cudaFree(p);
+  scratch.clear();
+  auto al = [&](size_t bytes) {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes ? bytes : 16) != cudaSuccess) return (void*)nullptr;
+    scratch.push_back(p);
+    return p;
+  };
+  const size_t rows = (size_t)n;
+  x0 = (bf16*)al(rows * kGIn * sizeof(bf16));
+  for (int l = 0; l < 4; ++l) {
+    h[l] = (bf16*)al(rows * kGHid * sizeof(bf16));
+    dh[l] = (bf16*)al(rows * kGHid * sizeof(bf16));
+  }
+  out = (float*)al(rows * kGOut * sizeof(float));
+  dy = (bf16*)al(rows * kGOut * sizeof(bf16));
+  const int z = (n + kWgChunk - 1) / kWgChunk;
+  partial = (float*)al((size_t)z * kGParams * sizeof(float));
+  bool ok = x0 && out && dy && partial;
+  for (int l = 0; l < 4; ++l) ok = ok && h[l] && dh[l];
+  if (!ok) {
+    for (void*& p : scratch) cudaFree(p);
+    scratch.clear();
+    cap = 0;
+    *err = "guiding network: scratch allocation failed";
+    return false;
+  }
+  cap = n;
+  return true;
+}
+
+void GuideNet::forward(const bf16* x, int n, float* out_rows, cudaStream_t st) {
+  const int grid = persistent_grid((const void*)k_forward_x, kFwdWarps * 32, kFwdSmem,
+                                   (n + kFwdWarps * 16 - 1) / (kFwdWarps * 16));
+  k_forward_x<<<grid, kFwdWarps * 32, kFwdSmem, st>>>(x, n, params16, params, out_rows);
+}
+
+void GuideNet::features(const float* pts, int n, bf16* x, cudaStream_t st) {
+  k_features<<<std::max(1, std::min(4096, (n + 63) / 64)), 128, 0, st>>>(pts, n, x);
+}
+
+void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st) {
+  TrainBufs b{x0, {h[0], h[1], h[2], h[3]}, {dh[0], dh[1], dh[2], dh[3]}, dy, loss};
+  cudaMemsetAsync(loss, 0, sizeof(float), st);
+  const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
+                                   (n + kTrainWarps * 32 - 1) / (kTrainWarps * 32));
+  k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b);
+  const int z = (n + kWgChunk - 1) / kWgChunk;
+  k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
+  k_reduce<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad);
+}
+
+void GuideNet::adam(float lr, cudaStream_t st) {
+  ++step;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float bc1 = 1.f - std::pow(b1, (float)step), bc2 = 1.f - std::pow(b2, (float)step);
+  k_adam<<<grid1(kGParams), 256, 0, st>>>(params, adam_m, adam_v, grad, kGParams, lr, b1, b2, 1e-8f, bc1, bc2,
+                                           params16);
+}
+
+}  // namespace tt

@@ -1,0 +1,49 @@
+// Host side of the guiding network (tt_guide.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "tt_internal.h"
+
+namespace tt {
+
+struct GuideNet {
+  std::vector<void*> allocs, scratch;
+  float* params = nullptr;       // FP32 master parameters (guide_w_offset / guide_b_offset)
+  __nv_bfloat16* params16 = nullptr;
+  float* adam_m = nullptr;
+  float* adam_v = nullptr;
+  float* grad = nullptr;
+  float* loss = nullptr;         // mean loss of the last gradient
+  int step = 0;
+  // Training scratch for up to `cap` records: features, hidden activations, their
+  // gradients, output gradients, FP32 outputs (batch forward) and the weight-gradient
+  // partials of the record chunks.
+  int cap = 0;
+  __nv_bfloat16* x0 = nullptr;
+  __nv_bfloat16* h[4] = {nullptr, nullptr, nullptr, nullptr};
+  __nv_bfloat16* dh[4] = {nullptr, nullptr, nullptr, nullptr};
+  float* out = nullptr;
+  __nv_bfloat16* dy = nullptr;
+  float* partial = nullptr;
+
+  ~GuideNet();
+  void release();
+  bool init(uint64_t seed, std::string* err);
+  bool set_params(const float* host, std::string* err);
+  bool ensure_capacity(int n, std::string* err);
+  // Forward pass of n rows of BF16 features into FP32 outputs.
+  void forward(const __nv_bfloat16* x, int n, float* out_rows, cudaStream_t st);
+  // Feature rows of n points (9 floats each: position in [0,1]^3, normal, outgoing direction).
+  void features(const float* pts, int n, __nv_bfloat16* x, cudaStream_t st);
+  // Mean-loss gradient over n records into `grad` and the loss into `loss`.
+  void gradient(const GuideRecord* rec, int n, cudaStream_t st);
+  void adam(float lr, cudaStream_t st);
+};
+
+}  // namespace tt

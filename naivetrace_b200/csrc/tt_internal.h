@@ -2,6 +2,7 @@
 // wavefront path-state layout and the kernel entry points.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -18,7 +19,20 @@ constexpr uint32_t ERR_QUEUE = 2u;
 constexpr uint32_t ERR_CROSSINGS = 4u;  // a ray crossed more medium boundaries than the cap
 constexpr int kMaxCrossings = 256;      // boundary crossings followed along one ray
 constexpr int kMaxMedia = 254;          // medium indices are stored in bytes (0xff = empty)
-constexpr int kCountersPerBounce = 3;  // ext, shadow, done queue lengths
+constexpr int kCountersPerBounce = 4;  // ext, shadow, done, guided queue lengths
+
+// One training record of the learned guide: a guided surface vertex (position normalised to
+// the scene box, shading normal, outgoing direction), the sampled incident direction, the
+// BSDF density of that direction, and F / q = (path contribution after the vertex) /
+// (throughput before it) averaged over the path's wavelengths.
+struct GuideRecord {
+  float pos[3];
+  float n[3];
+  float wo[3];
+  float wi[3];
+  float p_bsdf;
+  float f_over_q;
+};
 
 // Surface material as stored on the device.
 struct DevMaterial {
@@ -107,6 +121,16 @@ struct DevScene {
   int num_media;
   const DevMedium* media;
   uint2 cam_track;            // medium tracker at the camera position
+  // Learned guiding (tt_guide.cuh): sample diffuse and microfacet surfaces by one-sample
+  // MIS of the BSDF and the network's vMF mixture.
+  int guide;                  // 1: guided scattering
+  int guide_record;           // 1: collect training records
+  float guide_keep;           // probability that a finished path keeps its record (uniform
+                              // subsample of a pass down to the record buffer's size)
+  const __nv_bfloat16* guide_w16;  // network weights (BF16, flat layout of tt_guide.cuh)
+  const float* guide_w32;          // FP32 master copy (the biases are read from it)
+  float box_lo[3];            // scene box, for the position encoding
+  float box_inv[3];           // 1 / extent per axis
 };
 
 // Wavefront path state, structure of arrays, capacity `cap` paths.
@@ -134,6 +158,16 @@ struct PathState {
   uint2* sh_track;     // medium tracker of the shadow ray at its origin
   float4* sh_med;      // x = light pdf (< 0: MIS weight 1), y = scatter pdf before the transmittance
                        // factor, z/w = the path's random state at the connection (low/high words)
+  // Guided scenes only (null otherwise).
+  float4* ginp;        // network inputs per guided-queue entry: 3 float4 holding p01 xyz,
+                       // shading normal xyz, outgoing direction xyz
+  int* guide_q;        // guided-vertex queue (slots)
+  float4* grec;        // pending training record per path: 6 float4 (tt_kernels.cu)
+  float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion,
+                       // BSDF pdf of the shadow direction, emitted flag
+  GuideRecord* records;  // committed training records
+  int* rec_count;
+  int rec_cap;
 };
 
 struct Framebuffer {
@@ -161,7 +195,11 @@ void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st);
-void launch_flush(const PathState& p, const Framebuffer& fb, int bounce, int grid, cudaStream_t st);
+void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, int grid,
+                  cudaStream_t st);
+// Guided scenes: network evaluation and one-sample MIS scattering of the queued guided
+// vertices (persistent kernel, as many CTAs as fit on the SMs).
+void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st);
 // Media scenes: spectral tracking from each extension ray's origin to its surface hit.
 void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);
 // Medium tracker at `pos` (MediumTracker::initializePosition); writes one uint2 to `out`.

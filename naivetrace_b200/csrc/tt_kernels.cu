@@ -9,7 +9,10 @@
 //   shade     - MIS-weighted emission at the hit, Russian roulette, next-event estimation
 //               (emits a shadow ray), BSDF sampling (emits the next extension ray).
 //   shadow    - occlusion test; adds the NEE contribution of unoccluded rays.
-//   flush     - converts finished paths to RGB and adds them to the framebuffer.
+//   guide     - (guided scenes) the network on the vertices shade queued for guiding, then
+//               one-sample MIS of the BSDF and the learned mixture (emits the next ray).
+//   flush     - converts finished paths to RGB and adds them to the framebuffer; commits
+//               the path's training record when the guide is being trained.
 // Queues are appended with warp-aggregated atomics.  All kernels loop grid-stride over a
 // device-side count, so launch shapes are fixed (a multiple of the SM count).
 #include <cuda_runtime.h>
@@ -17,6 +20,7 @@
 #include <type_traits>
 
 #include "tt_device.cuh"
+#include "tt_guide.cuh"
 #include "tt_internal.h"
 #include "tt_tables.h"
 
@@ -38,6 +42,17 @@ __device__ __forceinline__ int warp_append(int* counter) {
 __device__ __forceinline__ int* ext_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b]; }
 __device__ __forceinline__ int* sh_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 1]; }
 __device__ __forceinline__ int* done_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 2]; }
+__device__ __forceinline__ int* guide_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 3]; }
+
+// Pending training record of a guided path (PathState::grec, 6 float4 per slot):
+//   0: position normalised to the scene box (xyz), shading normal x
+//   1: shading normal yz, outgoing direction xy
+//   2: outgoing direction z, sampled direction xyz
+//   3: BSDF pdf of the sampled direction, vertex depth (int bits), guided vertices seen on
+//      the path (int bits), valid flag
+//   4: path contribution before the vertex (spectral, 3)
+//   5: throughput before the vertex (spectral, 3)
+constexpr int kRecF4 = 6;
 
 
 // ----------------------------------------------------------------------------------------
@@ -531,6 +546,8 @@ struct Connection {
   float len;
   float3 weight;    // scatter * target * DFactors * r2 (transmittance excluded)
   float pdf_due;    // pdf of sampling the light vertex by scattering, light's measure
+  float pdf_eye;    // scatter density of the direction at the eye (solid angle)
+  float conv;       // pdf_due / pdf_eye: DFactor(light) / distance^2 (DFactor alone for an env light)
   bool valid;       // nonzero weight: a shadow ray is needed
   int unit;         // camera eye: pixel the connection lands in
 };
@@ -551,6 +568,8 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
   c.valid = false;
   c.unit = -1;
   c.pdf_due = 0.f;
+  c.pdf_eye = 0.f;
+  c.conv = 0.f;
   c.weight = f3(0.f, 0.f, 0.f);
   const bool light_env = L.type == LIGHT_ENV;
   const bool point_eye = eye.is_camera || eye.is_volume;  // no surface offset, DFactor 1
@@ -606,7 +625,9 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
   }
   // PdfConversionFactor(eye, light): DFactor(light) / (len^2 + eps) unless the light is at
   // infinity.
-  c.pdf_due = light_env ? pdf_eye * dfac_light : pdf_eye * dfac_light / (len * len + kEps);
+  c.conv = light_env ? dfac_light : dfac_light / (len * len + kEps);
+  c.pdf_eye = pdf_eye;
+  c.pdf_due = pdf_eye * c.conv;
   if (is_zero(sf) || is_zero(tf)) return c;
   const float dfac_eye = point_eye ? 1.f : fabsf(dot3(eye.surf.ng, d));
   const float r2 = light_env ? 1.f : 1.f / (len * len);
@@ -689,8 +710,15 @@ __device__ __forceinline__ LightNode pick_light(const DevScene& sc, Rng& rng, La
 template <bool MEDIA>
 __device__ __forceinline__ void emit_shadow(const DevScene& sc, const PathState& p, int qbounce, int slot,
                                             const Connection& c, const LightNode& L, float3 beta, float scale,
-                                            int target, const MTracker& mt, const Rng& rng) {
+                                            int target, const MTracker& mt, const Rng& rng,
+                                            bool defer_mis = false) {
   float3 contrib;
+  if (defer_mis) {
+    // Guided vertex: the scatter density is the one-sample-MIS mixture, known only after
+    // the network ran; k_guide completes the weight.
+    const bool mis_on = !L.delta && sc.sample_bsdf && sc.sample_lights;
+    p.gnee[slot] = make_float4(mis_on ? L.pdf : -1.f, c.conv, c.pdf_eye, 1.f);
+  }
   if (MEDIA) {
     contrib = mul(c.weight, beta) * (scale / L.pdf);
     const bool mis_on = !L.delta && sc.sample_bsdf && sc.sample_lights;
@@ -699,7 +727,7 @@ __device__ __forceinline__ void emit_shadow(const DevScene& sc, const PathState&
                                  __uint_as_float((unsigned)(rng.state >> 32)));
     p.sh_track[slot] = store_tracker(mt);
   } else {
-    const float mis = mis_weight(sc, L.pdf, L.delta, c.pdf_due);
+    const float mis = defer_mis ? 1.f : mis_weight(sc, L.pdf, L.delta, c.pdf_due);
     contrib = mul(c.weight, beta) * (mis * scale / L.pdf);
   }
   const int q = warp_append(sh_count(p, qbounce));
@@ -729,6 +757,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     const float3 cam_pos = f3(sc.cam.pos[0], sc.cam.pos[1], sc.cam.pos[2]);
     const MTracker cam_mt = load_tracker(sc.cam_track);
     p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sc.guide_record) p.grec[(size_t)kRecF4 * i + 3] = make_float4(0.f, 0.f, 0.f, 0.f);
     // Next-event estimation at the camera vertex: a light sample seen directly by the
     // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
     if (sc.sample_lights) {
@@ -927,6 +956,11 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       const float3 wi = -dir;
       MTracker mt;
       if (MEDIA) mt = load_tracker(p.track[slot]);
+      // Guided scattering at diffuse and microfacet surfaces.
+      const bool guided = sc.guide && !is_volume &&
+                          (sc.materials[s.material].shader == TT_SHADER_DIFFUSE ||
+                           sc.materials[s.material].shader == TT_SHADER_MICROFACET);
+      if (guided) p.gnee[slot].w = 0.f;
       if (sc.sample_lights) {
         LightNode L = pick_light(sc, rng, l);
         if (L.type != LIGHT_NONE) {
@@ -950,9 +984,27 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
               smt = mt;
               if (!is_volume && dot3(c.dir, s.n) < 0.f) going_through(sc, smt, c.dir, s.ng, s.material);
             }
-            emit_shadow<MEDIA>(sc, p, bounce + 1, slot, c, L, beta, 1.f, -1, smt, rng);
+            emit_shadow<MEDIA>(sc, p, bounce + 1, slot, c, L, beta, 1.f, -1, smt, rng, guided);
           }
         }
+      }
+      // At a guided vertex the network inputs are queued, and k_guide evaluates the network
+      // and samples the mixture.
+      if (guided) {
+        const int qg = warp_append(guide_count(p, bounce));
+        p.guide_q[qg] = slot;
+        const float3 p01 = f3((s.pos.x - sc.box_lo[0]) * sc.box_inv[0], (s.pos.y - sc.box_lo[1]) * sc.box_inv[1],
+                              (s.pos.z - sc.box_lo[2]) * sc.box_inv[2]);
+        float4* gi = p.ginp + 3 * (size_t)qg;
+        gi[0] = make_float4(p01.x, p01.y, p01.z, s.ns.x);
+        gi[1] = make_float4(s.ns.y, s.ns.z, wi.x, wi.y);
+        gi[2] = make_float4(wi.z, 0.f, 0.f, 0.f);
+        p.beta[slot] = make_float4(beta.x, beta.y, beta.z, b4.w);
+        meta.z = (unsigned)count;
+        p.meta[slot] = meta;
+        p.accum[slot] = make_float4(acc.x, acc.y, acc.z, 0.f);
+        p.rng_state[slot] = rng.state;
+        continue;
       }
       // Scatter: BSDF sample at a surface, phase-function sample at a volume vertex
       // (TakeRandomWalkStep from a scatter node).
@@ -1001,6 +1053,142 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       const int qd = warp_append(done_count(p, bounce + 1));
       p.done_q[qd] = slot;
     }
+  }
+}
+
+// One guided vertex with network outputs `gout`: one-sample MIS of the BSDF and the learned
+// vMF mixture, as SampleWithBinaryMixtureDensity (renderingalgorithms_pathtracing_guided.cxx:
+// 474-524): with probability c the mixture is sampled, else the BSDF; the density is
+// (1 - c) p_bsdf + c p_mixture either way.  NEE from the vertex gets its MIS weight against
+// the same density (the reference's MaybeAddNeeLighting evaluates the same binary mixture,
+// :1824-1840).  A reservoir of size one keeps one training record per path.
+template <bool MEDIA>
+__device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const PathState& p, int bounce, int slot,
+                                                  const float* gout) {
+  const float4 h = p.hit[slot];
+  const float3 dir = xyz(p.ray_d[slot]);
+  uint4 meta = p.meta[slot];
+  const Lambda l = unpack_lambda(meta.y);
+  const float4 b4 = p.beta[slot];
+  float3 beta = xyz(b4);
+  Rng rng{p.rng_state[slot], p.rng_inc[slot]};
+  const int tri = __float_as_int(h.w);
+  const bool sphere = sc.num_spheres > 0 && is_sphere_slot(sc.tris, tri);
+  Surf s = sphere ? sphere_hit_surface(sc.tris, tri, xyz(p.ray_o[slot]), dir, h.x)
+                  : make_surface(sc, tri, 1.f - h.y - h.z, h.y, h.z, f3(h.y, h.z, 1.f - h.y - h.z));
+  orient(s, dir);
+  const DevMaterial& m = sc.materials[s.material];
+  const float3 wi = -dir;
+  const GuideMixture mix = guide_decode(gout);
+  float3 ndir, val;
+  float pb = 0.f;
+  if (rng.uniform() < mix.c) {
+    ndir = guide_mixture_sample(mix, rng);
+    val = eval_bsdf(m, wi, s, ndir, l, &pb);
+  } else {
+    const ScatterSample ss = sample_bsdf(m, wi, s, rng, l);
+    ndir = ss.dir;
+    val = ss.value;
+    pb = ss.pdf;
+  }
+  const float pg = guide_mixture_pdf(mix, ndir);
+  const float pdf = (1.f - mix.c) * pb + mix.c * pg;
+  const float4 nee = p.gnee[slot];
+  if (nee.w != 0.f) {
+    const float3 sd = xyz(p.sh_d[slot]);
+    const float pdf_due = ((1.f - mix.c) * nee.z + mix.c * guide_mixture_pdf(mix, sd)) * nee.y;
+    if (MEDIA) {
+      p.sh_med[slot].y = pdf_due;
+    } else if (nee.x > 0.f) {
+      const float w = power_heuristic(nee.x, pdf_due);
+      const float4 c4 = p.sh_c[slot];
+      p.sh_c[slot] = make_float4(c4.x * w, c4.y * w, c4.z * w, c4.w);
+    }
+  }
+  const float3 f = val * (bsdf_correction(s, ndir) * fabsf(dot3(s.ng, ndir)));
+  const float3 bf = f * (1.f / pdf);
+  const bool done = !(pdf > 0.f) || is_zero(bf) || !isfinite(bf.x + bf.y + bf.z);
+  if (!done && sc.guide_record) {
+    // Reservoir sampling over the path's guided vertices.
+    float4* r = p.grec + (size_t)kRecF4 * slot;
+    const float4 r3 = r[3];
+    const int seen = (r3.w != 0.f ? __float_as_int(r3.z) : 0) + 1;
+    const bool take = rng.uniform() * (float)seen < 1.f;
+    if (take) {
+      const float3 p01 = f3((s.pos.x - sc.box_lo[0]) * sc.box_inv[0], (s.pos.y - sc.box_lo[1]) * sc.box_inv[1],
+                            (s.pos.z - sc.box_lo[2]) * sc.box_inv[2]);
+      const float4 a = p.accum[slot];
+      r[0] = make_float4(p01.x, p01.y, p01.z, s.ns.x);
+      r[1] = make_float4(s.ns.y, s.ns.z, wi.x, wi.y);
+      r[2] = make_float4(wi.z, ndir.x, ndir.y, ndir.z);
+      r[3] = make_float4(pb, __int_as_float(bounce), __int_as_float(seen), 1.f);
+      r[4] = make_float4(a.x, a.y, a.z, 0.f);
+      r[5] = make_float4(beta.x, beta.y, beta.z, 0.f);
+    } else {
+      r[3] = make_float4(r3.x, r3.y, __int_as_float(seen), 1.f);
+    }
+  }
+  if (done) {
+    const int qd = warp_append(done_count(p, bounce + 1));
+    p.done_q[qd] = slot;
+  } else {
+    beta = mul(beta, bf);
+    if (MEDIA && dot3(ndir, s.n) < 0.f) {
+      MTracker mt = load_tracker(p.track[slot]);
+      going_through(sc, mt, ndir, s.ng, s.material);
+      p.track[slot] = store_tracker(mt);
+    }
+    const float3 org = s.pos + offset_at(s, ndir);
+    p.ray_o[slot] = make_float4(org.x, org.y, org.z, 0.f);
+    p.ray_d[slot] = make_float4(ndir.x, ndir.y, ndir.z, kLargeNumber);
+    p.beta[slot] = make_float4(beta.x, beta.y, beta.z, pdf);
+    meta.w = 0u;
+    p.meta[slot] = meta;
+    const int qe = warp_append(ext_count(p, bounce + 1));
+    p.ext_q[(bounce + 1) & 1][qe] = slot;
+  }
+  p.rng_state[slot] = rng.state;
+}
+
+// Guided scattering of the vertices k_shade queued this bounce: a persistent kernel whose
+// warps take 32 queue entries at a time, evaluate the network on them (two 16-row tiles
+// with the weights in shared memory, guide_mlp_tile) and then scatter one entry per lane.
+constexpr int kGuideWarps = 8;
+constexpr int kGuideSmem = kGSmBytes + kGuideWarps * 32 * (kGInputs + kGOutStride) * 4;
+
+template <bool MEDIA>
+__global__ void __launch_bounds__(kGuideWarps * 32) k_guide(DevScene sc, PathState p, int bounce) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  __nv_bfloat16* sw = reinterpret_cast<__nv_bfloat16*>(gsm);
+  float* sb = reinterpret_cast<float*>(gsm + kGSmW * 2);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* q = reinterpret_cast<float*>(gsm + kGSmBytes) + warp * 32 * kGInputs;
+  float* o = reinterpret_cast<float*>(gsm + kGSmBytes) + kGuideWarps * 32 * kGInputs + warp * 32 * kGOutStride;
+  const int n = *guide_count(p, bounce);
+  if (blockIdx.x * kGuideWarps * 32 >= n) return;
+  guide_smem_load(sc.guide_w16, sc.guide_w32, sw, sb);
+  __syncthreads();
+  for (int base = (blockIdx.x * kGuideWarps + warp) * 32; base < n; base += gridDim.x * kGuideWarps * 32) {
+    const int i = base + lane;
+    float* r = q + lane * kGInputs;
+    if (i < n) {
+      const float4* gi = p.ginp + 3 * (size_t)i;
+      const float4 a = gi[0], b = gi[1], c = gi[2];
+      r[0] = a.x; r[1] = a.y; r[2] = a.z; r[3] = a.w; r[4] = b.x; r[5] = b.y; r[6] = b.z; r[7] = b.w; r[8] = c.x;
+    } else {
+#pragma unroll
+      for (int k = 0; k < kGInputs; ++k) r[k] = 0.f;
+    }
+    __syncwarp();
+#pragma unroll 1
+    for (int mt = 0; mt < 2; ++mt) {
+      uint32_t xf[6][4];
+      guide_tile_features(q + mt * 16 * kGInputs, kGInputs, xf);
+      guide_mlp_tile(sw, sb, xf, o + mt * 16 * kGOutStride, kGOutStride, nullptr);
+    }
+    __syncwarp();
+    if (i < n) guide_scatter_one<MEDIA>(sc, p, bounce, p.guide_q[i], o + lane * kGOutStride);
+    __syncwarp();
   }
 }
 
@@ -1060,6 +1248,14 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
     if (target < 0) {
       const float4 a = p.accum[slot];
       p.accum[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, 0.f);
+      if (sc.guide_record) {
+        // Direct light at the recorded vertex is not radiance along its sampled direction.
+        const float4 r3 = p.grec[(size_t)kRecF4 * slot + 3];
+        if (r3.w != 0.f && __float_as_int(r3.y) == bounce - 1) {
+          const float4 r4 = p.grec[(size_t)kRecF4 * slot + 4];
+          p.grec[(size_t)kRecF4 * slot + 4] = make_float4(r4.x + c.x, r4.y + c.y, r4.z + c.z, 0.f);
+        }
+      }
     } else {
       const Lambda l = unpack_lambda(p.meta[slot].y);
       const float3 rgb = selection_to_rgb(c, l);
@@ -1106,11 +1302,43 @@ __global__ void k_init_tracker(DevScene sc, float3 pos, float3 lo, float3 hi, ui
   out[0] = store_tracker(mt);
 }
 
-__global__ void __launch_bounds__(256) k_flush(PathState p, Framebuffer fb, int bounce) {
+__global__ void __launch_bounds__(256) k_flush(DevScene sc, PathState p, Framebuffer fb, int bounce) {
   const int n = *done_count(p, bounce);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = p.done_q[i];
     const uint4 meta = p.meta[slot];
+    if (sc.guide_record) {
+      // Commit the path's pending record (kept with probability guide_keep): F / q =
+      // (contribution after the vertex) / (throughput before it), averaged over the
+      // wavelengths with nonzero throughput.
+      const float4* r = p.grec + (size_t)kRecF4 * slot;
+      const float4 r3 = r[3];
+      Rng krng{p.rng_state[slot], p.rng_inc[slot]};
+      if (r3.w != 0.f && (sc.guide_keep >= 1.f || krng.uniform() < sc.guide_keep)) {
+        const float4 r0 = r[0], r1 = r[1], r2 = r[2], r4 = r[4], r5 = r[5];
+        const float4 a = p.accum[slot];
+        float fq = 0.f;
+        int nz = 0;
+        const float da[3] = {a.x - r4.x, a.y - r4.y, a.z - r4.z}, bb[3] = {r5.x, r5.y, r5.z};
+        for (int k = 0; k < 3; ++k)
+          if (bb[k] > 0.f) {
+            fq += fmaxf(da[k], 0.f) / bb[k];
+            ++nz;
+          }
+        fq = nz > 0 ? fq / nz : 0.f;
+        const int idx = atomicAdd(p.rec_count, 1);
+        if (idx < p.rec_cap && isfinite(fq)) {
+          GuideRecord rec;
+          rec.pos[0] = r0.x; rec.pos[1] = r0.y; rec.pos[2] = r0.z;
+          rec.n[0] = r0.w; rec.n[1] = r1.x; rec.n[2] = r1.y;
+          rec.wo[0] = r1.z; rec.wo[1] = r1.w; rec.wo[2] = r2.x;
+          rec.wi[0] = r2.y; rec.wi[1] = r2.z; rec.wi[2] = r2.w;
+          rec.p_bsdf = r3.x;
+          rec.f_over_q = fq;
+          p.records[idx] = rec;
+        }
+      }
+    }
     const float3 rgb = selection_to_rgb(xyz(p.accum[slot]), unpack_lambda(meta.y));
     const int px = (int)meta.x;
     atomicAdd(&fb.accum[3 * px], rgb.x);
@@ -1300,8 +1528,24 @@ void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_
                          cudaStream_t st) {
   k_init_tracker<<<1, 32, 0, st>>>(s, pos, bb_lo, bb_hi, out, err);
 }
-void launch_flush(const PathState& p, const Framebuffer& fb, int bounce, int grid, cudaStream_t st) {
-  k_flush<<<grid, kBlock, 0, st>>>(p, fb, bounce);
+void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, int grid,
+                  cudaStream_t st) {
+  k_flush<<<grid, kBlock, 0, st>>>(s, p, fb, bounce);
+}
+
+void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st) {
+  static int grid = 0;
+  if (grid == 0) {
+    cudaFuncSetAttribute(k_guide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
+    cudaFuncSetAttribute(k_guide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide<true>, kGuideWarps * 32, kGuideSmem);
+    grid = sms * (per_sm > 0 ? per_sm : 1);
+  }
+  if (s.num_media > 0) k_guide<true><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
+  else k_guide<false><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
 }
 void launch_accumulate(const Framebuffer& fb, double* acc, double* light, int n3, cudaStream_t st) {
   const int grid = (n3 + kBlock - 1) / kBlock;

@@ -119,6 +119,9 @@ extern "C" tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t s
   std::string* err = nullptr;
   if (!ctx) return TT_ERR_INVALID;
   if (!context_scene(ctx, &scene, &device, &npix, &depth, &err)) return TT_ERR_NOT_READY;
+  // The learned guide needs buffers of its own; this pass renders unguided.
+  scene.guide = 0;
+  scene.guide_record = 0;
   auto fail = [err](tt_status s, const std::string& msg) {
     *err = msg;
     return s;
@@ -162,13 +165,13 @@ extern "C" tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t s
   launch_generate(scene, p, fb, w, grid, st);
   for (int b = 0; b < depth; ++b) {
     launch_shadow(scene, p, fb, b, false, nullptr, grid, st);
-    launch_flush(p, fb, b, grid, st);
+    launch_flush(scene, p, fb, b, grid, st);
     launch_extend(scene, p, b, false, nullptr, grid, st);
     if (scene.num_media > 0) launch_track(scene, p, b, grid, st);
     launch_shade(scene, p, b, grid, st);
   }
   launch_shadow(scene, p, fb, depth, false, nullptr, grid, st);
-  launch_flush(p, fb, depth, grid, st);
+  launch_flush(scene, p, fb, depth, grid, st);
   unsigned int errw = 0;
   e = cudaMemcpyAsync(&errw, p.err, sizeof(errw), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -381,3 +381,40 @@ def spheres_box(xres=64, yres=64) -> Scene:
     s.add_sphere((0.55, 0.1, 0.75), 0.1, s.add_material(diffuse(rgb_to_spectrum((0.2, 0.4, 0.8)))))
     s.add_sphere((0.2, 0.8, 0.5), 0.04, s.add_material(area_light(30.0)))
     return s
+
+
+def guiding_room(xres=1280, yres=720) -> Scene:
+    """A 4 x 3 x 4 room (x, y up, z) lit only through a 0.5 x 0.5 gap in a partition wall at
+    x = 3: behind it a closet (x in [3, 4]) holds a 0.6 x 0.6 area light (flat emission 4000)
+    facing the closet's back wall, so no point of the room sees the light and every path
+    that brings light into the room leaves the closet through the gap.  Lambert 0.6 room
+    walls and ceiling, Lambert 0.8 closet walls and partition, a glossy Beckmann floor
+    (reflectance 0.5, alpha 0.1).  The case where BSDF sampling rarely finds the light and a
+    learned guide pays.  Pinhole camera in the corner at (0.3, 1.6, 0.3) looking at
+    (3.0, 1.0, 3.0) with a 75 degree field of view."""
+    s = Scene()
+    s.name = "guiding_room"
+    wall = s.add_material(diffuse(0.6))
+    closet = s.add_material(diffuse(0.8))
+    floor = s.add_material(microfacet(0.5, 0.1))
+    light = s.add_material(area_light(4000.0, reflectance=0.0))
+    X, Y, Z, P = 4.0, 3.0, 4.0, 3.0
+    s.add_mesh(*quad((0, 0, 0), (0, 0, Z), (X, 0, Z), (X, 0, 0)), floor)
+    s.add_mesh(*quad((0, Y, 0), (X, Y, 0), (X, Y, Z), (0, Y, Z)), wall)
+    s.add_mesh(*quad((0, 0, 0), (0, Y, 0), (0, Y, Z), (0, 0, Z)), wall)          # x = 0
+    s.add_mesh(*quad((0, 0, 0), (P, 0, 0), (P, Y, 0), (0, Y, 0)), wall)          # z = 0, room part
+    s.add_mesh(*quad((0, 0, Z), (0, Y, Z), (P, Y, Z), (P, 0, Z)), wall)          # z = 4, room part
+    s.add_mesh(*quad((P, 0, 0), (X, 0, 0), (X, Y, 0), (P, Y, 0)), closet)        # z = 0, closet part
+    s.add_mesh(*quad((P, 0, Z), (P, Y, Z), (X, Y, Z), (X, 0, Z)), closet)        # z = 4, closet part
+    s.add_mesh(*quad((X, 0, 0), (X, 0, Z), (X, Y, Z), (X, Y, 0)), closet)        # x = 4
+    # Partition at x = P around the gap y in [1.0, 1.5], z in [1.75, 2.25].
+    y0, y1, z0, z1 = 1.0, 1.5, 1.75, 2.25
+    s.add_mesh(*quad((P, 0, 0), (P, y0, 0), (P, y0, Z), (P, 0, Z)), closet)
+    s.add_mesh(*quad((P, y1, 0), (P, Y, 0), (P, Y, Z), (P, y1, Z)), closet)
+    s.add_mesh(*quad((P, y0, 0), (P, y1, 0), (P, y1, z0), (P, y0, z0)), closet)
+    s.add_mesh(*quad((P, y0, z1), (P, y1, z1), (P, y1, Z), (P, y0, Z)), closet)
+    # Light at x = 3.5 facing +x (winding normal (p1 - p0) x (p2 - p0) = +x).
+    s.add_mesh(*quad((3.5, 2.0, 1.7), (3.5, 2.6, 1.7), (3.5, 2.6, 2.3), (3.5, 2.0, 2.3)), light)
+    s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.3, 1.6, 0.3), dir=(2.7, -0.6, 2.7), up=(0, 1, 0),
+                          fov_deg=75.0, xres=xres, yres=yres)
+    return s

@@ -1,0 +1,201 @@
+"""The learned guider on the GPU against the CPU oracle (oracle/guiding.py), and guided
+rendering against plain rendering.
+
+1. Feature encoding, forward pass and loss gradient through the C ABI against the oracle
+   that rounds to bfloat16 where the GPU stores bfloat16 (differences: accumulation order
+   only), and against the float64 oracle (the size of the bfloat16 error).
+2. One Adam step of the device optimiser against the oracle's Adam on the same gradient.
+3. Training on synthetic records lowers the loss and concentrates the mixture.
+4. Training records collected by a render: layout, positivity, the fraction that carries
+   light.
+5. Guided rendering is unbiased: tile means of guided renders (network training between
+   passes, and frozen) agree with plain renders within a z-test, with and without media.
+6. The guided RenderingAlgo schedule (training sweeps, then frozen passes).
+"""
+import numpy as np
+import pytest
+
+from naivetrace_b200 import scenes
+from naivetrace_b200.algo import GpuContext, GpuGuidedPathTracer
+from naivetrace_b200.scene import make_params
+from oracle import guiding as G
+from oracle.oracle import combine
+
+pytestmark = pytest.mark.gpu
+
+
+def _ctx(scene=None):
+    scene = scene if scene is not None else scenes.cornell_box(16, 16)
+    return GpuContext(scene, make_params(max_ray_depth=10))
+
+
+def _params(seed=3, bias=0.05):
+    p = G.init_params(seed)
+    rng = np.random.default_rng(seed + 100)
+    for l in range(G.N_LAYERS):
+        o = G.layer_out(l)
+        p[G.b_offset(l):G.b_offset(l) + o] = rng.normal(0, bias, o)
+    return p.astype(np.float32)
+
+
+def test_num_params(gpu_lib):
+    assert gpu_lib.tt_guide_num_params() == G.N_PARAMS
+
+
+def test_features_match_oracle(gpu_lib):
+    g = _ctx()
+    rec = G.random_records(4096, seed=2)
+    xg = g.guide_features(rec[:, 0:9])
+    xo = G.record_features(rec)
+    diff = xg != xo
+    # Sines of the same float32 argument may round to neighbouring bfloat16 values.
+    assert diff.mean() < 2e-3, diff.mean()
+    # At most one bfloat16 step apart (8 significant bits).
+    assert np.all(np.abs(xg - xo)[diff] <= 2 ** -7 * np.abs(xo)[diff])
+
+
+def test_forward_matches_oracle(gpu_lib):
+    g = _ctx()
+    p = _params()
+    g.guide_set_params(p)
+    assert np.array_equal(g.guide_params(), p)
+    rec = G.random_records(3000, seed=4)       # not a multiple of the 16-row tile
+    x = G.record_features(rec)
+    og = g.guide_forward(x)
+    oo, _, _ = G.forward(p, x, True)
+    err = np.linalg.norm(og - oo) / np.linalg.norm(oo)
+    assert err < 5e-3, err
+    assert np.abs(og - oo).max() < 0.05 * np.abs(oo).max()
+    of, _, _ = G.forward(p, x, False)
+    assert np.linalg.norm(og - of) / np.linalg.norm(of) < 3e-2
+
+
+@pytest.mark.parametrize("n", [777, 9000])
+def test_gradient_matches_oracle(gpu_lib, n):
+    """9000 records span 18 chunks of the split weight-gradient kernel, the last one ragged."""
+    g = _ctx()
+    p = _params()
+    g.guide_set_params(p)
+    rec = G.random_records(n, seed=n)
+    loss_g, grad_g = g.guide_gradient(rec)
+    loss_o, grad_o = G.gradient(p, rec, bf16_round=True)
+    assert abs(loss_g - loss_o) <= 2e-3 * abs(loss_o), (loss_g, loss_o)
+    err = np.linalg.norm(grad_g - grad_o) / np.linalg.norm(grad_o)
+    cos = grad_g @ grad_o / (np.linalg.norm(grad_g) * np.linalg.norm(grad_o))
+    assert err < 3e-2 and cos > 0.999, (err, cos)
+    # Per layer, so that no layer hides behind a larger one.
+    for l in range(G.N_LAYERS):
+        a, b = G.w_offset(l), G.b_offset(l) + G.layer_out(l)
+        e = np.linalg.norm(grad_g[a:b] - grad_o[a:b]) / np.linalg.norm(grad_o[a:b])
+        assert e < 5e-2, (l, e)
+    # The bfloat16 network stays close to the exact float64 gradient.
+    _, grad_f = G.gradient(p, rec, bf16_round=False)
+    cos_f = grad_g @ grad_f / (np.linalg.norm(grad_g) * np.linalg.norm(grad_f))
+    assert cos_f > 0.99, cos_f
+
+
+def test_adam_step_matches_oracle(gpu_lib):
+    g = _ctx()
+    p = _params(seed=8)
+    g.guide_set_params(p)
+    rec = G.random_records(2048, seed=8)
+    _, grad = g.guide_gradient(rec)
+    g.guide_train(rec, steps=1, learning_rate=1e-3)
+    p1 = g.guide_params()
+    e, _, _ = G.adam(p.astype(np.float64), 0.0, 0.0, grad.astype(np.float64), 1, 1e-3)
+    np.testing.assert_allclose(p1, e, atol=2e-6)
+
+
+def test_training_on_gpu_lowers_loss(gpu_lib):
+    g = _ctx()
+    g.guide_set_params(G.init_params(2))
+    rec = G.random_records(1024, seed=1)
+    rec[:, 0:9] = rec[np.arange(1024) % 8, 0:9]
+    L0 = G.loss(G.init_params(2).astype(np.float64), rec)
+    L1 = g.guide_train(rec, steps=120, learning_rate=5e-3)
+    assert L1 < L0 - 0.5, (L0, L1)
+    mu = np.array([0.3, 0.5, 0.8]) / np.linalg.norm([0.3, 0.5, 0.8])
+    out = g.guide_forward(G.record_features(rec[:64]))
+    assert np.median(G.mixture_pdf(out, np.broadcast_to(mu, (64, 3)))) > 1.0
+
+
+def test_render_records(gpu_lib):
+    """Records of one guided pass in the gap-lit room: normalised positions, unit vectors,
+    nonnegative weights, some carrying light, at most one per path."""
+    scene = scenes.guiding_room(64, 36)
+    g = GpuContext(scene, make_params(max_ray_depth=12))
+    g.set_guiding(True, 2, records_per_step=1 << 16, seed=3)
+    g.render(4, seed=1)
+    r = g.guide_records()
+    assert 0 < len(r) <= 64 * 36 * 4
+    assert np.all((r[:, 0:3] >= -1e-4) & (r[:, 0:3] <= 1 + 1e-4))
+    for a in (3, 6, 9):
+        np.testing.assert_allclose(np.linalg.norm(r[:, a:a + 3], axis=1), 1.0, atol=1e-3)
+    assert np.all(r[:, 12] >= 0) and np.all(r[:, 13] >= 0) and np.all(np.isfinite(r[:, 13]))
+    assert (r[:, 13] > 0).sum() > 0
+    assert len(g.guide_records()) == 0            # reading empties the buffer
+
+
+def tile_means(rgb, xres, yres, tile):
+    a = rgb.reshape(yres, xres, 3)
+    ty, tx = yres // tile, xres // tile
+    return a[: ty * tile, : tx * tile].reshape(ty, tile, tx, tile, 3).mean(axis=(1, 3))
+
+
+def _batches(ctx, K, spp, seed0, xres, yres, tile):
+    out = []
+    for k in range(K):
+        ctx.clear()
+        ctx.render(spp, seed=seed0 + k)
+        acc, light, sppc, splat = ctx.accumulators()
+        out.append(tile_means(combine(acc, light, spp, splat, ctx.npix), xres, yres, tile))
+    return np.array(out)
+
+
+@pytest.mark.parametrize("name,train_during", [("cornell_box", True), ("cornell_box", False),
+                                               ("cornell_box_medium", False), ("guiding_room", True)])
+def test_guided_render_unbiased(gpu_lib, name, train_during):
+    """Tile means of guided and plain renders: z = difference over the standard error from
+    K independent renders per side; at least 97 % of the tile-channels within 3 sigma and
+    all within 4.5 sigma."""
+    xres, yres, tile = (64, 64, 16) if name != "guiding_room" else (96, 54, 18)
+    scene = getattr(scenes, name)(xres, yres)
+    p = make_params(max_ray_depth=10 if name != "guiding_room" else 12)
+    plain = GpuContext(scene, p)
+    guided = GpuContext(scene, p)
+    guided.set_guiding(True, 1, learning_rate=1e-2, steps_per_pass=4, seed=5)
+    for k in range(8):                       # train before the measured batches
+        guided.render(4, seed=900 + k)
+    st = guided.stats()
+    assert st["guide_records"] > 0 and st["guide_steps"] == 32 and np.isfinite(st["guide_loss"])
+    if not train_during:
+        guided.set_guiding(True, 0, learning_rate=1e-2, steps_per_pass=4, seed=5)
+    K = 16
+    spp = 16 if name != "guiding_room" else 64
+    tp = _batches(plain, K, spp, 100, xres, yres, tile)
+    tg = _batches(guided, K, spp, 300, xres, yres, tile)
+    steps_after = guided.stats()["guide_steps"]
+    assert (steps_after > 32) == train_during
+    mp, mg = tp.mean(0), tg.mean(0)
+    se = np.sqrt(tp.var(0, ddof=1) / K + tg.var(0, ddof=1) / K)
+    z = np.abs(mg - mp) / np.maximum(se, 1e-12)
+    assert (z < 3.0).mean() >= 0.97, ((z < 3.0).mean(), z.max())
+    assert np.all(z < 4.5), z.max()
+    assert guided.stats()["error_flags"] == 0
+
+
+def test_guided_algo_schedule(gpu_lib):
+    scene = scenes.cornell_box(32, 32)
+    algo = GpuGuidedPathTracer(scene, make_params(max_ray_depth=8, max_spp=12), guide_max_spp=4,
+                               steps_per_pass=2)
+    calls = []
+    algo.set_interrupt_callback(lambda complete: calls.append(complete))
+    algo.run()
+    # One initial pass, sweeps of 2 and 4 passes, then the schedule 1 + 2 + 4 + 5 = 12.
+    assert calls == [True] * 7, calls
+    acc, light, spp, splat = algo.ctx.accumulators()
+    assert np.all(spp == 12)
+    st = algo.ctx.stats()
+    assert st["guide_steps"] == 2 * (1 + 2 + 4)
+    img = algo.generate_image()
+    assert img.shape == (32, 32, 3) and img.mean() > 5
