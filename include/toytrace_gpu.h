@@ -340,9 +340,11 @@ typedef struct tt_guiding_params {
   int32_t enabled;              /* 1: guided sampling at diffuse and microfacet surfaces */
   int32_t train;                /* 1: collect records and train after every pass;
                                    2: collect records only (tt_guide_read_records) */
-  float learning_rate;          /* Adam step size (0: 1e-2) */
-  int32_t records_per_step;     /* record buffer and training batch (0: 262144) */
-  int32_t steps_per_pass;       /* Adam steps after each pass (0: 1) */
+  float learning_rate;          /* Adam step size (0: 2e-3) */
+  int32_t record_pool;          /* records kept across passes, a ring that overwrites the
+                                   oldest (0: 65536); only records that carry light are kept */
+  int32_t batch;                /* records per Adam step, drawn at random from the pool (0: 8192) */
+  int32_t steps_per_pass;       /* Adam steps after each pass (0: 4) */
   uint64_t seed;                /* weight initialisation */
 } tt_guiding_params;
 
@@ -364,8 +366,8 @@ tt_status tt_guide_gradient_batch(tt_ctx* ctx, const float* records, int32_t n, 
  * last step's gradient (may be NULL). */
 tt_status tt_guide_train_batch(tt_ctx* ctx, const float* records, int32_t n, int32_t steps, float learning_rate,
                                float* loss);
-/* Copies up to max_records collected training records (14 floats each, layout above) to
- * `out`, *n = the number copied, and empties the record buffer. */
+/* Copies up to max_records training records of the pool (14 floats each, layout above) to
+ * `out`, *n = the number copied, and empties the pool. */
 tt_status tt_guide_read_records(tt_ctx* ctx, float* out, int32_t max_records, int32_t* n);
 /* Feature encoding of n points (position in [0,1]^3, normal, outgoing direction: 9 floats
  * each) into n x 96 features, as the renderer computes them. */

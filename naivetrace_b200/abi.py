@@ -230,7 +230,8 @@ class GuidingParams(C.Structure):
         ("enabled", C.c_int32),
         ("train", C.c_int32),
         ("learning_rate", C.c_float),
-        ("records_per_step", C.c_int32),
+        ("record_pool", C.c_int32),
+        ("batch", C.c_int32),
         ("steps_per_pass", C.c_int32),
         ("seed", C.c_uint64),
     ]

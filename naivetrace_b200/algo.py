@@ -148,10 +148,10 @@ class GpuContext:
         self._check(self.lib.tt_reset_stats(self.h), "tt_reset_stats")
 
     # Learned guiding ---------------------------------------------------------------
-    def set_guiding(self, enabled: bool = True, train: int = 1, learning_rate: float = 1e-2,
-                    records_per_step: int = 1 << 18, steps_per_pass: int = 1, seed: int = 1):
+    def set_guiding(self, enabled: bool = True, train: int = 1, learning_rate: float = 2e-3,
+                    record_pool: int = 1 << 16, batch: int = 8192, steps_per_pass: int = 4, seed: int = 1):
         """train: 0 frozen, 1 collect records and train after every pass, 2 collect only."""
-        gp = abi.GuidingParams(int(enabled), int(train), learning_rate, records_per_step, steps_per_pass, seed)
+        gp = abi.GuidingParams(int(enabled), int(train), learning_rate, record_pool, batch, steps_per_pass, seed)
         self._check(self.lib.tt_set_guiding(self.h, C.byref(gp)), "tt_set_guiding")
 
     def guide_params(self) -> np.ndarray:
@@ -298,14 +298,14 @@ class GpuGuidedPathTracer(GpuPathTracer):
     sweeps of 2, 4, ... up to `guide_max_spp` one-sample passes, each starting from a cleared
     framebuffer; then guiding is frozen (no more records) and the regular samples-per-pixel
     schedule renders into a cleared framebuffer.  Training happens after every pass of a
-    sweep: `steps_per_pass` Adam steps on that pass's records."""
+    sweep: `steps_per_pass` Adam steps on mini-batches of the record pool."""
 
     def __init__(self, scene: Scene, params: Optional[abi.Params] = None, seed: int = 1, linear_output: bool = False,
-                 guide_max_spp: int = 16, learning_rate: float = 1e-2, records_per_step: int = 1 << 18,
-                 steps_per_pass: int = 4, guide_seed: int = 1):
+                 guide_max_spp: int = 16, learning_rate: float = 2e-3, record_pool: int = 1 << 16,
+                 batch: int = 8192, steps_per_pass: int = 4, guide_seed: int = 1):
         super().__init__(scene, params, seed, linear_output)
         self.guide_max_spp = guide_max_spp
-        self.guiding = dict(learning_rate=learning_rate, records_per_step=records_per_step,
+        self.guiding = dict(learning_rate=learning_rate, record_pool=record_pool, batch=batch,
                             steps_per_pass=steps_per_pass, seed=guide_seed)
         self._pass_seed = seed
 

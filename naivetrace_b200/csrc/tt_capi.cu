@@ -141,9 +141,12 @@ struct tt_ctx {
   // Learned guiding.
   std::unique_ptr<GuideNet> gnet;
   tt_guiding_params gparams{};
-  GuideRecord* d_records = nullptr;
+  GuideRecord* d_records = nullptr;   // record pool (ring)
   int* d_rec_count = nullptr;
   int rec_cap = 0;
+  long long rec_seen = 0;             // pool counter at the end of the last pass
+  double rec_rate = 0.0;              // records committed per path in the last training pass
+  uint64_t draw_seed = 0;
   bool ps_guided = false;      // the path state carries the guiding arrays
 };
 
@@ -756,23 +759,40 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
   return TT_OK;
 }
 
-// Training on the records of the last pass: `steps_per_pass` Adam steps on one batch.
-static tt_status guide_train(tt_ctx* c) {
-  int n = 0;
-  TT_CUDA(c, cudaMemcpyAsync(&n, c->d_rec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+// After a pass: `steps_per_pass` Adam steps, each on a mini-batch drawn from the record
+// pool; also updates the pool's yield per path, from which the next pass's keep
+// probability follows.
+static tt_status guide_train(tt_ctx* c, long long paths) {
+  int cnt = 0;
+  TT_CUDA(c, cudaMemcpyAsync(&cnt, c->d_rec_count, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   TT_CUDA(c, cudaStreamSynchronize(c->stream));
-  n = std::min(n, c->rec_cap);
-  if (n >= 256) {
+  const long long count = (long long)(unsigned)cnt;
+  const long long fresh = count - c->rec_seen;
+  if (paths > 0 && fresh >= 0) c->rec_rate = (double)fresh / ((double)paths * std::max(1e-6, (double)c->dev.guide_keep));
+  if (count > (1ll << 30)) {
+    // Keep the ring position and a full pool while the counter stays far from overflow.
+    const int wrapped = (int)(c->rec_cap + count % c->rec_cap);
+    TT_CUDA(c, cudaMemcpyAsync(c->d_rec_count, &wrapped, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    TT_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->rec_seen = wrapped;
+  } else {
+    c->rec_seen = count;
+  }
+  const int pool = (int)std::min<long long>(count, c->rec_cap);
+  if (pool >= 256) {
+    const int n = std::min(pool, c->gparams.batch > 0 ? c->gparams.batch : 8192);
     std::string gerr;
     if (!c->gnet->ensure_capacity(n, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, c->stream);
-    const int steps = c->gparams.steps_per_pass > 0 ? c->gparams.steps_per_pass : 1;
-    const float lr = c->gparams.learning_rate > 0.f ? c->gparams.learning_rate : 1e-2f;
+    const int steps = c->gparams.steps_per_pass > 0 ? c->gparams.steps_per_pass : 4;
+    const float lr = c->gparams.learning_rate > 0.f ? c->gparams.learning_rate : 2e-3f;
     for (int k = 0; k < steps; ++k) {
-      c->gnet->gradient(c->d_records, n, c->stream);
+      c->gnet->draw_batch(c->d_records, pool, n, c->gparams.seed * 0x9e3779b97f4a7c15ull + (++c->draw_seed),
+                          c->stream);
+      c->gnet->gradient(c->gnet->batch, n, c->stream);
       c->gnet->adam(lr, c->stream);
     }
     cudaEventRecord(b, c->stream);
@@ -783,12 +803,11 @@ static tt_status guide_train(tt_ctx* c) {
     cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    c->stats.guide_records += (uint64_t)n;
+    c->stats.guide_records += (uint64_t)std::max(0ll, fresh);
     c->stats.guide_steps += (uint64_t)steps;
     c->stats.guide_loss = loss;
     c->stats.guide_train_ms += ms;
   }
-  TT_CUDA(c, cudaMemsetAsync(c->d_rec_count, 0, sizeof(int), c->stream));
   return TT_OK;
 }
 
@@ -802,7 +821,11 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
   const long long total = (long long)spp * npix_range;
   const int wave_limit = c->params.wave_paths > 0 ? c->params.wave_paths : kDefaultWave;
   const int cap = (int)std::min<long long>(total, wave_limit);
-  if (c->dev.guide_record) c->dev.guide_keep = (float)std::min(1.0, (double)c->rec_cap / (double)total);
+  if (c->dev.guide_record) {
+    // Keep about 80 % of a pool's worth of this pass's records at most.
+    const double expected = c->rec_rate * (double)total;
+    c->dev.guide_keep = expected > 0.0 ? (float)std::min(1.0, 0.8 * c->rec_cap / expected) : 1.f;
+  }
   tt_status st = ensure_path_state(c, cap);
   if (st != TT_OK) return st;
   const bool counting = c->profiling >= 2;
@@ -899,7 +922,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
   c->splat_count += (uint64_t)spp * (uint64_t)npix_range;
   c->next_sample += (uint64_t)spp;
   if (c->dev.guide_record && !stopped && c->gparams.train == 1) {
-    const tt_status gs = guide_train(c);
+    const tt_status gs = guide_train(c, total);
     if (gs != TT_OK) return gs;
   }
   unsigned int errw = 0;
@@ -1267,10 +1290,10 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     c->gparams = *gp;
     return TT_OK;
   }
-  if (gp->records_per_step < 0 || gp->steps_per_pass < 0 || !(gp->learning_rate >= 0.f) || gp->train < 0 ||
-      gp->train > 2)
+  if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || !(gp->learning_rate >= 0.f) ||
+      gp->train < 0 || gp->train > 2)
     return fail(c, TT_ERR_INVALID, "bad guiding parameters");
-  const int cap = gp->records_per_step > 0 ? gp->records_per_step : (1 << 18);
+  const int cap = gp->record_pool > 0 ? gp->record_pool : (1 << 16);
   if (!c->gnet) {
     c->gnet = std::make_unique<GuideNet>();
     std::string gerr;
@@ -1287,8 +1310,10 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     if (!c->d_rec_count) TT_CUDA(c, cudaMalloc(&c->d_rec_count, sizeof(int)));
     c->rec_cap = cap;
     c->ps_guided = false;  // the path state picks up the new record buffer
+    TT_CUDA(c, cudaMemset(c->d_rec_count, 0, sizeof(int)));
+    c->rec_seen = 0;
+    c->rec_rate = 0.0;
   }
-  TT_CUDA(c, cudaMemset(c->d_rec_count, 0, sizeof(int)));
   c->gparams = *gp;
   c->dev.guide_w16 = c->gnet->params16;
   c->dev.guide_w32 = c->gnet->params;
@@ -1396,9 +1421,10 @@ tt_status tt_guide_read_records(tt_ctx* c, float* out, int32_t max_records, int3
   TT_CUDA(c, cudaStreamSynchronize(c->stream));
   int cnt = 0;
   TT_CUDA(c, cudaMemcpy(&cnt, c->d_rec_count, sizeof(int), cudaMemcpyDeviceToHost));
-  cnt = std::min(std::min(cnt, c->rec_cap), max_records);
+  cnt = (int)std::min<long long>(std::min<long long>((long long)(unsigned)cnt, c->rec_cap), max_records);
   if (cnt > 0) TT_CUDA(c, cudaMemcpy(out, c->d_records, (size_t)cnt * sizeof(GuideRecord), cudaMemcpyDeviceToHost));
   TT_CUDA(c, cudaMemset(c->d_rec_count, 0, sizeof(int)));
+  c->rec_seen = 0;
   *n = cnt;
   return TT_OK;
 }

@@ -381,6 +381,15 @@ __global__ void k_adam(float* p, float* m, float* v, const float* g, int n, floa
   }
 }
 
+// batch[i] = pool[h(seed, i) mod pool_n], h the SplitMix64 finalizer.
+__global__ void k_draw(const GuideRecord* __restrict__ pool, int pool_n, GuideRecord* __restrict__ batch, int n,
+                       unsigned long long seed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const unsigned long long h = Rng::splitmix64(seed ^ Rng::splitmix64((unsigned long long)i));
+    batch[i] = pool[(int)(h % (unsigned long long)pool_n)];
+  }
+}
+
 __global__ void k_to_bf16(const float* p, int n, bf16* w16) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w16[i] = __float2bfloat16(p[i]);
 }
@@ -494,9 +503,10 @@ bool GuideNet::ensure_capacity(int n, std::string* err) {
   }
   out = (float*)al(rows * kGOut * sizeof(float));
   dy = (bf16*)al(rows * kGOut * sizeof(bf16));
+  batch = (GuideRecord*)al(rows * sizeof(GuideRecord));
   const int z = (n + kWgChunk - 1) / kWgChunk;
   partial = (float*)al((size_t)z * kGParams * sizeof(float));
-  bool ok = x0 && out && dy && partial;
+  bool ok = x0 && out && dy && partial && batch;
   for (int l = 0; l < 4; ++l) ok = ok && h[l] && dh[l];
   if (!ok) {
     for (void*& p : scratch) cudaFree(p);
@@ -528,6 +538,10 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st) {
   const int z = (n + kWgChunk - 1) / kWgChunk;
   k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
   k_reduce<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad);
+}
+
+void GuideNet::draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t seed, cudaStream_t st) {
+  k_draw<<<grid1(n), 256, 0, st>>>(pool, pool_n, batch, n, seed);
 }
 
 void GuideNet::adam(float lr, cudaStream_t st) {

@@ -31,6 +31,7 @@ struct GuideNet {
   float* out = nullptr;
   __nv_bfloat16* dy = nullptr;
   float* partial = nullptr;
+  GuideRecord* batch = nullptr;  // mini-batch drawn from the record pool
 
   ~GuideNet();
   void release();
@@ -43,6 +44,9 @@ struct GuideNet {
   void features(const float* pts, int n, __nv_bfloat16* x, cudaStream_t st);
   // Mean-loss gradient over n records into `grad` and the loss into `loss`.
   void gradient(const GuideRecord* rec, int n, cudaStream_t st);
+  // `batch` <- n records drawn uniformly (with replacement) from pool[0, pool_n); needs
+  // ensure_capacity(n).
+  void draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t seed, cudaStream_t st);
   void adam(float lr, cudaStream_t st);
 };
 

@@ -125,8 +125,8 @@ struct DevScene {
   // MIS of the BSDF and the network's vMF mixture.
   int guide;                  // 1: guided scattering
   int guide_record;           // 1: collect training records
-  float guide_keep;           // probability that a finished path keeps its record (uniform
-                              // subsample of a pass down to the record buffer's size)
+  float guide_keep;           // probability that a finished path keeps its record (a uniform
+                              // subsample when a pass would yield more than the pool holds)
   const __nv_bfloat16* guide_w16;  // network weights (BF16, flat layout of tt_guide.cuh)
   const float* guide_w32;          // FP32 master copy (the biases are read from it)
   float box_lo[3];            // scene box, for the position encoding
@@ -165,8 +165,8 @@ struct PathState {
   float4* grec;        // pending training record per path: 6 float4 (tt_kernels.cu)
   float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion,
                        // BSDF pdf of the shadow direction, emitted flag
-  GuideRecord* records;  // committed training records
-  int* rec_count;
+  GuideRecord* records;  // training-record pool, a ring of rec_cap records
+  int* rec_count;        // records committed since the pool was emptied (index = count % rec_cap)
   int rec_cap;
 };
 

@@ -1062,16 +1062,39 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
 // (1 - c) p_bsdf + c p_mixture either way.  NEE from the vertex gets its MIS weight against
 // the same density (the reference's MaybeAddNeeLighting evaluates the same binary mixture,
 // :1824-1840).  A reservoir of size one keeps one training record per path.
+// Per-slot path state a guided vertex needs, loaded before the network runs so that the
+// loads' latency overlaps the tensor-core work.
+struct GuidePre {
+  int slot;
+  float4 h, d4, b4, nee;
+  uint4 meta;
+  unsigned long long rs, ri;
+};
+
+__device__ __forceinline__ GuidePre guide_prefetch(const PathState& p, int slot) {
+  GuidePre g;
+  g.slot = slot;
+  g.h = p.hit[slot];
+  g.d4 = p.ray_d[slot];
+  g.b4 = p.beta[slot];
+  g.nee = p.gnee[slot];
+  g.meta = p.meta[slot];
+  g.rs = p.rng_state[slot];
+  g.ri = p.rng_inc[slot];
+  return g;
+}
+
 template <bool MEDIA>
-__device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const PathState& p, int bounce, int slot,
-                                                  const float* gout) {
-  const float4 h = p.hit[slot];
-  const float3 dir = xyz(p.ray_d[slot]);
-  uint4 meta = p.meta[slot];
+__device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const PathState& p, int bounce,
+                                                  const GuidePre& pre, const float* gout) {
+  const int slot = pre.slot;
+  const float4 h = pre.h;
+  const float3 dir = xyz(pre.d4);
+  uint4 meta = pre.meta;
   const Lambda l = unpack_lambda(meta.y);
-  const float4 b4 = p.beta[slot];
+  const float4 b4 = pre.b4;
   float3 beta = xyz(b4);
-  Rng rng{p.rng_state[slot], p.rng_inc[slot]};
+  Rng rng{pre.rs, pre.ri};
   const int tri = __float_as_int(h.w);
   const bool sphere = sc.num_spheres > 0 && is_sphere_slot(sc.tris, tri);
   Surf s = sphere ? sphere_hit_surface(sc.tris, tri, xyz(p.ray_o[slot]), dir, h.x)
@@ -1093,7 +1116,7 @@ __device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const Path
   }
   const float pg = guide_mixture_pdf(mix, ndir);
   const float pdf = (1.f - mix.c) * pb + mix.c * pg;
-  const float4 nee = p.gnee[slot];
+  const float4 nee = pre.nee;
   if (nee.w != 0.f) {
     const float3 sd = xyz(p.sh_d[slot]);
     const float pdf_due = ((1.f - mix.c) * nee.z + mix.c * guide_mixture_pdf(mix, sd)) * nee.y;
@@ -1171,6 +1194,8 @@ __global__ void __launch_bounds__(kGuideWarps * 32) k_guide(DevScene sc, PathSta
   for (int base = (blockIdx.x * kGuideWarps + warp) * 32; base < n; base += gridDim.x * kGuideWarps * 32) {
     const int i = base + lane;
     float* r = q + lane * kGInputs;
+    GuidePre pre;
+    if (i < n) pre = guide_prefetch(p, p.guide_q[i]);
     if (i < n) {
       const float4* gi = p.ginp + 3 * (size_t)i;
       const float4 a = gi[0], b = gi[1], c = gi[2];
@@ -1187,7 +1212,7 @@ __global__ void __launch_bounds__(kGuideWarps * 32) k_guide(DevScene sc, PathSta
       guide_mlp_tile(sw, sb, xf, o + mt * 16 * kGOutStride, kGOutStride, nullptr);
     }
     __syncwarp();
-    if (i < n) guide_scatter_one<MEDIA>(sc, p, bounce, p.guide_q[i], o + lane * kGOutStride);
+    if (i < n) guide_scatter_one<MEDIA>(sc, p, bounce, pre, o + lane * kGOutStride);
     __syncwarp();
   }
 }
@@ -1308,9 +1333,10 @@ __global__ void __launch_bounds__(256) k_flush(DevScene sc, PathState p, Framebu
     const int slot = p.done_q[i];
     const uint4 meta = p.meta[slot];
     if (sc.guide_record) {
-      // Commit the path's pending record (kept with probability guide_keep): F / q =
+      // Commit the path's pending record if it carries light (a record with F = 0 adds
+      // nothing to the loss or its gradient), kept with probability guide_keep: F / q =
       // (contribution after the vertex) / (throughput before it), averaged over the
-      // wavelengths with nonzero throughput.
+      // wavelengths with nonzero throughput.  The pool is a ring: the oldest records give way.
       const float4* r = p.grec + (size_t)kRecF4 * slot;
       const float4 r3 = r[3];
       Rng krng{p.rng_state[slot], p.rng_inc[slot]};
@@ -1326,8 +1352,8 @@ __global__ void __launch_bounds__(256) k_flush(DevScene sc, PathState p, Framebu
             ++nz;
           }
         fq = nz > 0 ? fq / nz : 0.f;
-        const int idx = atomicAdd(p.rec_count, 1);
-        if (idx < p.rec_cap && isfinite(fq)) {
+        if (fq > 0.f && isfinite(fq)) {
+          const unsigned idx = atomicAdd(reinterpret_cast<unsigned*>(p.rec_count), 1u) % (unsigned)p.rec_cap;
           GuideRecord rec;
           rec.pos[0] = r0.x; rec.pos[1] = r0.y; rec.pos[2] = r0.z;
           rec.n[0] = r0.w; rec.n[1] = r1.x; rec.n[2] = r1.y;

@@ -80,16 +80,17 @@ def unpack(params):
     return out
 
 
-_QUARTER = [np.float32(1.0), np.float32(1.18920712), np.float32(1.41421356), np.float32(1.68179283)]
+_EIGHTH = [np.float32(v) for v in (1.0, 1.09050773, 1.18920712, 1.29683955, 1.41421356, 1.54221083,
+                                    1.68179283, 1.83400809)]
 
 
 def freq(j: int) -> np.float32:
-    """Band multiplier 2^(j/4), as the float32 the device computes."""
-    return np.float32(_QUARTER[j & 3] * np.float32(1 << (j >> 2)))
+    """Band multiplier 2^(j/8), as the float32 the device computes."""
+    return np.float32(_EIGHTH[j & 7] * np.float32(1 << (j >> 3)))
 
 
 def features(p01, n, wo, round_bf16: bool = True) -> np.ndarray:
-    """Encoded surface points (rows of 96): sin/cos of pi 2^(j/4) x for 12 bands j of each
+    """Encoded surface points (rows of 96): sin/cos of pi 2^(j/8) x for 12 bands j of each
     normalised coordinate x, the coordinates, the normal, the outgoing direction and a
     constant 1, zero padded."""
     p01 = np.asarray(p01, np.float32).reshape(-1, 3)

@@ -48,10 +48,11 @@ def test_features_match_oracle(gpu_lib):
     xg = g.guide_features(rec[:, 0:9])
     xo = G.record_features(rec)
     diff = xg != xo
-    # Sines of the same float32 argument may round to neighbouring bfloat16 values.
+    # The device's hardware sine (absolute error about 1e-6) may round to a neighbouring
+    # bfloat16 value.
     assert diff.mean() < 2e-3, diff.mean()
-    # At most one bfloat16 step apart (8 significant bits).
-    assert np.all(np.abs(xg - xo)[diff] <= 2 ** -7 * np.abs(xo)[diff])
+    # At most one bfloat16 step apart (8 significant bits), or within the sine's error.
+    assert np.all(np.abs(xg - xo)[diff] <= 2 ** -7 * np.abs(xo)[diff] + 4e-6)
 
 
 def test_forward_matches_oracle(gpu_lib):
@@ -120,20 +121,24 @@ def test_training_on_gpu_lowers_loss(gpu_lib):
 
 
 def test_render_records(gpu_lib):
-    """Records of one guided pass in the gap-lit room: normalised positions, unit vectors,
-    nonnegative weights, some carrying light, at most one per path."""
+    """Records of guided passes in the gap-lit room: normalised positions, unit vectors,
+    positive finite weights (only records that carry light are kept), at most one per path;
+    the pool is a ring that keeps the newest records."""
     scene = scenes.guiding_room(64, 36)
     g = GpuContext(scene, make_params(max_ray_depth=12))
-    g.set_guiding(True, 2, records_per_step=1 << 16, seed=3)
-    g.render(4, seed=1)
+    g.set_guiding(True, 2, record_pool=1 << 16, seed=3)
+    g.render(16, seed=1)
     r = g.guide_records()
-    assert 0 < len(r) <= 64 * 36 * 4
+    assert 0 < len(r) <= 64 * 36 * 16
     assert np.all((r[:, 0:3] >= -1e-4) & (r[:, 0:3] <= 1 + 1e-4))
     for a in (3, 6, 9):
         np.testing.assert_allclose(np.linalg.norm(r[:, a:a + 3], axis=1), 1.0, atol=1e-3)
-    assert np.all(r[:, 12] >= 0) and np.all(r[:, 13] >= 0) and np.all(np.isfinite(r[:, 13]))
-    assert (r[:, 13] > 0).sum() > 0
-    assert len(g.guide_records()) == 0            # reading empties the buffer
+    assert np.all(r[:, 12] >= 0) and np.all(r[:, 13] > 0) and np.all(np.isfinite(r[:, 13]))
+    assert len(g.guide_records()) == 0            # reading empties the pool
+    # A pool smaller than one pass's yield holds exactly its capacity.
+    g.set_guiding(True, 2, record_pool=64, seed=3)
+    g.render(16, seed=2)
+    assert len(g.guide_records()) == 64
 
 
 def tile_means(rgb, xres, yres, tile):
@@ -167,7 +172,9 @@ def test_guided_render_unbiased(gpu_lib, name, train_during):
     for k in range(8):                       # train before the measured batches
         guided.render(4, seed=900 + k)
     st = guided.stats()
-    assert st["guide_records"] > 0 and st["guide_steps"] == 32 and np.isfinite(st["guide_loss"])
+    steps_before = st["guide_steps"]
+    assert st["guide_records"] > 0 and 0 < steps_before <= 32 and steps_before % 4 == 0
+    assert np.isfinite(st["guide_loss"])
     if not train_during:
         guided.set_guiding(True, 0, learning_rate=1e-2, steps_per_pass=4, seed=5)
     K = 16
@@ -175,7 +182,7 @@ def test_guided_render_unbiased(gpu_lib, name, train_during):
     tp = _batches(plain, K, spp, 100, xres, yres, tile)
     tg = _batches(guided, K, spp, 300, xres, yres, tile)
     steps_after = guided.stats()["guide_steps"]
-    assert (steps_after > 32) == train_during
+    assert (steps_after > steps_before) == train_during
     mp, mg = tp.mean(0), tg.mean(0)
     se = np.sqrt(tp.var(0, ddof=1) / K + tg.var(0, ddof=1) / K)
     z = np.abs(mg - mp) / np.maximum(se, 1e-12)
@@ -196,6 +203,6 @@ def test_guided_algo_schedule(gpu_lib):
     acc, light, spp, splat = algo.ctx.accumulators()
     assert np.all(spp == 12)
     st = algo.ctx.stats()
-    assert st["guide_steps"] == 2 * (1 + 2 + 4)
+    assert 0 < st["guide_steps"] <= 2 * (1 + 2 + 4) and st["guide_steps"] % 2 == 0
     img = algo.generate_image()
     assert img.shape == (32, 32, 3) and img.mean() > 5

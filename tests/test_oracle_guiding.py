@@ -40,8 +40,8 @@ def test_features_layout():
     x = G.features(p, n, wo, round_bf16=False)[0]
     assert x.shape == (96,)
     assert np.isclose(x[0], np.sin(np.pi * 0.25), atol=1e-6) and np.isclose(x[1], np.cos(np.pi * 0.25), atol=1e-6)
-    assert np.isclose(x[2], np.sin(2 ** 0.25 * np.pi * 0.25), atol=1e-6)
-    assert np.isclose(x[8], np.sin(2 * np.pi * 0.25), atol=1e-6)
+    assert np.isclose(x[2], np.sin(2 ** 0.125 * np.pi * 0.25), atol=1e-6)
+    assert np.isclose(x[16], np.sin(2 * np.pi * 0.25), atol=1e-6)
     assert np.allclose(x[72:75], p[0]) and np.allclose(x[75:78], n[0]) and np.allclose(x[78:81], wo[0])
     assert x[81] == 1.0 and np.all(x[82:] == 0)
 
