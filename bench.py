@@ -156,6 +156,110 @@ def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=16384, seed=1):
     return mpaths, cores, desc
 
 
+def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth=12, train_passes=8,
+                       train_steps=16, lr=1e-3, guide_depth=2):
+    """Learned-guided against plain GPU tracing on the guiding workload (a room lit through a
+    0.3 x 0.3 gap, 1280x720, depth 12): relMSE against a 4096-spp plain render after every
+    pass, with the wall time of the render calls (training included) summed.  Plain passes
+    double their spp (1, 2, 4, ...); the guided run first renders `train_passes` one-sample
+    passes that train the network after each pass, then freezes it and doubles like plain.
+    Every sample, training passes included, stays in the image (each is unbiased).  Reports
+    the time to reach relMSE `target` and the relMSE of both at equal time."""
+    from naivetrace_b200 import scenes
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    scene = scenes.guiding_room(xres, yres)
+    p = make_params(max_ray_depth=depth)
+    ref = GpuContext(scene, p)
+    for k in range(16):
+        ref.render(256, seed=1_000_000 + k)
+    R = ref.framebuffer().astype(np.float64)
+    ref.close()
+
+    def relmse(g):
+        I = g.framebuffer().astype(np.float64)
+        return float(np.mean((I - R) ** 2 / (R * R + 1e-2)))
+
+    def timed(g, spp, seed):
+        t = time.perf_counter()
+        g.render(spp, seed)
+        return (time.perf_counter() - t) * 1e3
+
+    # Warm-up contexts: kernels loaded, memory pool filled.
+    w = GpuContext(scene, p)
+    w.render(4, 1)
+    w.set_guiding(True, 1, learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+    w.render(1, 2)
+    w.close()
+
+    def run(guided):
+        g = GpuContext(scene, p)
+        # One untimed pass at the largest wave size allocates the path state (with the
+        # guiding arrays for the guided run); the network is not trained by it.
+        if guided:
+            g.set_guiding(True, 0, max_depth=guide_depth, seed=7)
+        g.render(8, 3)
+        g.clear()
+        g.reset_stats()
+        pts, el, spp_total, seed = [], 0.0, 0, 10
+        if guided:
+            g.set_guiding(True, 1, learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+            for k in range(train_passes):
+                el += timed(g, 1, seed)
+                seed += 1
+                spp_total += 1
+                pts.append((el, spp_total, relmse(g)))
+            g.set_guiding(True, 0, learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+        spp = 1
+        while el < budget_ms and spp_total < 1 << 14:
+            el += timed(g, spp, seed)
+            seed += 1
+            spp_total += spp
+            pts.append((el, spp_total, relmse(g)))
+            spp *= 2
+        st = g.stats()
+        g.close()
+        return pts, st
+
+    def time_to(pts, tgt):
+        prev = None
+        for t, s, e in pts:
+            if e <= tgt:
+                if prev is None or prev[2] <= e:
+                    return t
+                # log-log interpolation between the bracketing passes
+                a = (np.log(prev[2]) - np.log(tgt)) / (np.log(prev[2]) - np.log(e))
+                return float(np.exp(np.log(prev[0]) + a * (np.log(t) - np.log(prev[0]))))
+            prev = (t, s, e)
+        return None
+
+    def at_time(pts, t0):
+        ts = np.log([x[0] for x in pts])
+        es = np.log([x[2] for x in pts])
+        return float(np.exp(np.interp(np.log(t0), ts, es)))
+
+    plain, _ = run(False)
+    guided, gst = run(True)
+    t_eq = min(plain[-1][0], guided[-1][0])
+    tp, tg = time_to(plain, target), time_to(guided, target)
+    ep, eg = at_time(plain, t_eq), at_time(guided, t_eq)
+    return {
+        "workload": f"guiding_room: 4x3x4 room lit through a 0.3x0.3 gap, {xres}x{yres}, max depth {depth}, "
+                    f"relMSE = mean((I-R)^2/(R^2+1e-2)) against a 4096-spp plain render",
+        "target_relmse": target,
+        "time_to_target_ms": {"plain": tp, "guided": tg},
+        "time_ratio_guided_over_plain": (tg / tp) if (tp and tg) else None,
+        "equal_time_ms": t_eq,
+        "relmse_at_equal_time": {"plain": ep, "guided": eg},
+        "gain_equal_time": ep / eg if eg > 0 else None,
+        "guided_bounces": guide_depth,
+        "training": {"passes": train_passes, "adam_steps": int(gst["guide_steps"]), "learning_rate": lr,
+                     "records": int(gst["guide_records"]), "train_kernel_ms": gst["guide_train_ms"]},
+        "curve_plain": [[round(t, 2), s, round(e, 6)] for t, s, e in plain],
+        "curve_guided": [[round(t, 2), s, round(e, 6)] for t, s, e in guided],
+    }
+
+
 def run_reference_arm(args):
     from naivetrace_b200 import dist as nd
     r = nd.init_from_env()
@@ -312,6 +416,10 @@ def run_ours(args):
     e2e_step = nd.max_over_ranks(e2e_step, r)
     e2e_value = nd.weak_scaling_value(paths_per_step, world, e2e_step)
 
+    guiding = None
+    if rank == 0 and world == 1 and not args.no_guiding:
+        guiding = guiding_comparison()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         v, cores, desc = cpu_reference(scene, spp, depth, budget_s=args.cpu_budget)
@@ -353,6 +461,7 @@ def run_ours(args):
                     "ms_per_step": e2e_step, "ms_each": [round(x, 1) for x in e2e_ms],
                     "what": "tt_create + tt_upload_scene (scene H2D, device BVH build) + tt_render_pass + "
                             "tt_read_framebuffer + tt_destroy"},
+            "guiding": guiding,
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": clk,
             "stats": {k: st[k] for k in ("extension_rays", "shadow_rays", "extend_launches", "extend_ms",
@@ -393,6 +502,7 @@ def main(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")
     ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing: upload the workload and render one pass of --spp samples (for ncu captures)")

@@ -340,11 +340,13 @@ typedef struct tt_guiding_params {
   int32_t enabled;              /* 1: guided sampling at diffuse and microfacet surfaces */
   int32_t train;                /* 1: collect records and train after every pass;
                                    2: collect records only (tt_guide_read_records) */
-  float learning_rate;          /* Adam step size (0: 2e-3) */
+  float learning_rate;          /* Adam step size (0: 1e-3) */
   int32_t record_pool;          /* records kept across passes, a ring that overwrites the
                                    oldest (0: 65536); only records that carry light are kept */
   int32_t batch;                /* records per Adam step, drawn at random from the pool (0: 8192) */
-  int32_t steps_per_pass;       /* Adam steps after each pass (0: 4) */
+  int32_t steps_per_pass;       /* Adam steps after each pass (0: 16) */
+  int32_t max_depth;            /* guide the vertices of the first max_depth bounces only, BSDF
+                                   sampling beyond (0: every bounce) */
   uint64_t seed;                /* weight initialisation */
 } tt_guiding_params;
 

@@ -233,6 +233,7 @@ class GuidingParams(C.Structure):
         ("record_pool", C.c_int32),
         ("batch", C.c_int32),
         ("steps_per_pass", C.c_int32),
+        ("max_depth", C.c_int32),
         ("seed", C.c_uint64),
     ]
 

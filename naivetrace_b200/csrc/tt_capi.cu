@@ -743,6 +743,7 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
     p.guide_q = (int*)m.alloc(n * sizeof(int));
     p.grec = (float4*)m.alloc(n * 6 * sizeof(float4));
     p.gnee = (float4*)m.alloc(n * sizeof(float4));
+    p.rr = (float*)m.alloc(n * sizeof(float));
     p.records = c->d_records;
     p.rec_count = c->d_rec_count;
     p.rec_cap = c->rec_cap;
@@ -787,8 +788,8 @@ static tt_status guide_train(tt_ctx* c, long long paths) {
     cudaEventCreate(&a);
     cudaEventCreate(&b);
     cudaEventRecord(a, c->stream);
-    const int steps = c->gparams.steps_per_pass > 0 ? c->gparams.steps_per_pass : 4;
-    const float lr = c->gparams.learning_rate > 0.f ? c->gparams.learning_rate : 2e-3f;
+    const int steps = c->gparams.steps_per_pass > 0 ? c->gparams.steps_per_pass : 16;
+    const float lr = c->gparams.learning_rate > 0.f ? c->gparams.learning_rate : 1e-3f;
     for (int k = 0; k < steps; ++k) {
       c->gnet->draw_batch(c->d_records, pool, n, c->gparams.seed * 0x9e3779b97f4a7c15ull + (++c->draw_seed),
                           c->stream);
@@ -1290,7 +1291,8 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     c->gparams = *gp;
     return TT_OK;
   }
-  if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || !(gp->learning_rate >= 0.f) ||
+  if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || gp->max_depth < 0 ||
+      !(gp->learning_rate >= 0.f) ||
       gp->train < 0 || gp->train > 2)
     return fail(c, TT_ERR_INVALID, "bad guiding parameters");
   const int cap = gp->record_pool > 0 ? gp->record_pool : (1 << 16);
@@ -1314,11 +1316,18 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     c->rec_seen = 0;
     c->rec_rate = 0.0;
   }
+  if (gp->train == 1) {
+    // Training scratch for one mini-batch now, not inside the first pass.
+    std::string gerr;
+    if (!c->gnet->ensure_capacity(std::min(cap, gp->batch > 0 ? gp->batch : 8192), &gerr))
+      return fail(c, TT_ERR_CUDA, gerr);
+  }
   c->gparams = *gp;
   c->dev.guide_w16 = c->gnet->params16;
   c->dev.guide_w32 = c->gnet->params;
   c->dev.guide = 1;
   c->dev.guide_record = gp->train ? 1 : 0;
+  c->dev.guide_depth = gp->max_depth > 0 ? gp->max_depth : (1 << 30);
   return TT_OK;
 }
 

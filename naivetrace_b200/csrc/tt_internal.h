@@ -125,6 +125,7 @@ struct DevScene {
   // MIS of the BSDF and the network's vMF mixture.
   int guide;                  // 1: guided scattering
   int guide_record;           // 1: collect training records
+  int guide_depth;            // guided vertices only at bounces < guide_depth
   float guide_keep;           // probability that a finished path keeps its record (a uniform
                               // subsample when a pass would yield more than the pool holds)
   const __nv_bfloat16* guide_w16;  // network weights (BF16, flat layout of tt_guide.cuh)
@@ -165,6 +166,8 @@ struct PathState {
   float4* grec;        // pending training record per path: 6 float4 (tt_kernels.cu)
   float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion,
                        // BSDF pdf of the shadow direction, emitted flag
+  float* rr;           // Russian-roulette throughput factor: (throughput with BSDF densities at
+                       // the guided vertices) / beta
   GuideRecord* records;  // training-record pool, a ring of rec_cap records
   int* rec_count;        // records committed since the pool was emptied (index = count % rec_cap)
   int rec_cap;

@@ -758,6 +758,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     const MTracker cam_mt = load_tracker(sc.cam_track);
     p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (sc.guide_record) p.grec[(size_t)kRecF4 * i + 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (sc.guide) p.rr[i] = 1.f;
     // Next-event estimation at the camera vertex: a light sample seen directly by the
     // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
     if (sc.sample_lights) {
@@ -941,10 +942,15 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       done = true;
     }
     // Russian roulette (SurvivalAtNthScatterNode, rendering_randomwalk_impl.hxx:736-755).
+    // In guided scenes the survival probability uses the throughput the path would have
+    // had with the BSDF densities in place of the one-sample-MIS mixture (beta times
+    // p.rr): sampling half the time from the BSDF divides its samples' weights by (1 - c),
+    // which would keep beta high and let paths run to the depth cap.  Any survival
+    // probability leaves the estimator unbiased.
     if (!done) {
       if (count < sc.max_path_nodes) {
         if (count > 5) {
-          const float pr = fminf(0.9f, max3(beta));
+          const float pr = fminf(0.9f, max3(beta) * (sc.guide ? p.rr[slot] : 1.f));
           if (rng.uniform() > pr) done = true;
           else beta = beta * (1.f / pr);
         }
@@ -957,7 +963,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       MTracker mt;
       if (MEDIA) mt = load_tracker(p.track[slot]);
       // Guided scattering at diffuse and microfacet surfaces.
-      const bool guided = sc.guide && !is_volume &&
+      const bool guided = sc.guide && bounce < sc.guide_depth && !is_volume &&
                           (sc.materials[s.material].shader == TT_SHADER_DIFFUSE ||
                            sc.materials[s.material].shader == TT_SHADER_MICROFACET);
       if (guided) p.gnee[slot].w = 0.f;
@@ -1066,6 +1072,7 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
 // loads' latency overlaps the tensor-core work.
 struct GuidePre {
   int slot;
+  float rr;
   float4 h, d4, b4, nee;
   uint4 meta;
   unsigned long long rs, ri;
@@ -1078,6 +1085,7 @@ __device__ __forceinline__ GuidePre guide_prefetch(const PathState& p, int slot)
   g.d4 = p.ray_d[slot];
   g.b4 = p.beta[slot];
   g.nee = p.gnee[slot];
+  g.rr = p.rr[slot];
   g.meta = p.meta[slot];
   g.rs = p.rng_state[slot];
   g.ri = p.rng_inc[slot];
@@ -1165,6 +1173,8 @@ __device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const Path
     p.ray_o[slot] = make_float4(org.x, org.y, org.z, 0.f);
     p.ray_d[slot] = make_float4(ndir.x, ndir.y, ndir.z, kLargeNumber);
     p.beta[slot] = make_float4(beta.x, beta.y, beta.z, pdf);
+    // Roulette throughput: the BSDF weight f / p_bsdf in place of f / pdf.
+    if (pb > 0.f) p.rr[slot] = pre.rr * (pdf / pb);
     meta.w = 0u;
     p.meta[slot] = meta;
     const int qe = warp_append(ext_count(p, bounce + 1));

@@ -161,8 +161,9 @@ def _batches(ctx, K, spp, seed0, xres, yres, tile):
                                                ("cornell_box_medium", False), ("guiding_room", True)])
 def test_guided_render_unbiased(gpu_lib, name, train_during):
     """Tile means of guided and plain renders: z = difference over the standard error from
-    K independent renders per side; at least 97 % of the tile-channels within 3 sigma and
-    all within 4.5 sigma."""
+    K independent renders per side (t-distributed with about 2K - 2 degrees of freedom; the
+    three channels of a tile are strongly correlated): at least 93 % of the tile-channels
+    within 3 sigma and all within 4.5 sigma."""
     xres, yres, tile = (64, 64, 16) if name != "guiding_room" else (96, 54, 18)
     scene = getattr(scenes, name)(xres, yres)
     p = make_params(max_ray_depth=10 if name != "guiding_room" else 12)
@@ -186,9 +187,49 @@ def test_guided_render_unbiased(gpu_lib, name, train_during):
     mp, mg = tp.mean(0), tg.mean(0)
     se = np.sqrt(tp.var(0, ddof=1) / K + tg.var(0, ddof=1) / K)
     z = np.abs(mg - mp) / np.maximum(se, 1e-12)
-    assert (z < 3.0).mean() >= 0.97, ((z < 3.0).mean(), z.max())
+    assert (z < 3.0).mean() >= 0.93, ((z < 3.0).mean(), z.max())
     assert np.all(z < 4.5), z.max()
     assert guided.stats()["error_flags"] == 0
+
+
+def test_guiding_gain(gpu_lib):
+    """What the trained network gains: on the gap-lit room, relMSE against a 4096-spp plain
+    render at 64 spp, guided (after 32 two-sample training passes) against plain.  The
+    same network switched off must render like plain (no gain from anything else)."""
+    xres, yres = 160, 90
+    scene = scenes.guiding_room(xres, yres)
+    p = make_params(max_ray_depth=12)
+    ref = GpuContext(scene, p)
+    for k in range(16):
+        ref.render(256, seed=10_000 + k)
+    R = ref.framebuffer().astype(np.float64)
+
+    def relmse(g):
+        I = g.framebuffer().astype(np.float64)
+        return float(np.mean((I - R) ** 2 / (R * R + 1e-2)))
+
+    plain = GpuContext(scene, p)
+    e_plain = []
+    for k in range(3):
+        plain.clear()
+        plain.render(64, seed=100 + k)
+        e_plain.append(relmse(plain))
+    g = GpuContext(scene, p)
+    g.set_guiding(True, 1, learning_rate=1e-3, steps_per_pass=16, seed=7)
+    for k in range(32):
+        g.render(2, seed=200 + k)
+    g.set_guiding(True, 0, learning_rate=1e-3, steps_per_pass=16, seed=7)
+    e_guided = []
+    for k in range(3):
+        g.clear()
+        g.render(64, seed=300 + k)
+        e_guided.append(relmse(g))
+    gain = np.mean(e_plain) / np.mean(e_guided)
+    assert gain > 1.5, (e_plain, e_guided)
+    g.set_guiding(False)
+    g.clear()
+    g.render(64, seed=400)
+    assert 0.6 < np.mean(e_plain) / relmse(g) < 1.6
 
 
 def test_guided_algo_schedule(gpu_lib):
