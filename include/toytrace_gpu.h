@@ -375,6 +375,40 @@ tt_status tt_guide_read_records(tt_ctx* ctx, float* out, int32_t max_records, in
  * each) into n x 96 features, as the renderer computes them. */
 tt_status tt_guide_features_batch(tt_ctx* ctx, const float* points, int32_t n, float* features);
 
+/* ---- Multi-view batches ------------------------------------------------------------
+ * No counterpart in the reference (it renders one camera per RenderingAlgo).  A batch of
+ * views of the uploaded scene, each with its own camera, resolution and samples per pixel,
+ * is rendered as one wavefront: the waves run over the concatenation of the views' pixel
+ * and sample ranges, so many small views fill the GPU like one large frame.  The per-wave
+ * launch sequence runs as one captured CUDA graph, replayed for every wave. */
+typedef struct tt_view {
+  tt_camera camera;
+  int32_t spp;
+} tt_view;
+
+/* Renders views[0..n) and writes their linear RGB images (row 0 at the bottom, as
+ * tt_read_framebuffer) one after the other into rgb (host; 3 * sum(xres * yres) floats).
+ * View v uses the random streams of a single-camera tt_render_pass of that camera with
+ * seed + v and sample numbers 0..spp-1.  The context's own framebuffer is not touched. */
+tt_status tt_render_views(tt_ctx* ctx, const tt_view* views, int32_t n, uint64_t seed, float* rgb);
+
+#define TT_TUNE_MAX 16
+typedef struct tt_tune_result {
+  int32_t wave_paths;           /* chosen paths per wave (queue capacity) */
+  int32_t grid;                 /* chosen blocks per wavefront launch */
+  double ms;                    /* probe time of the chosen configuration */
+  int32_t candidates;
+  int32_t candidate_wave[TT_TUNE_MAX];
+  int32_t candidate_grid[TT_TUNE_MAX];
+  double candidate_ms[TT_TUNE_MAX];
+} tt_tune_result;
+
+/* Autotuner: times one-sample probes of the batch over queue capacities (2^20 .. 2^23 paths
+ * per wave) and launch widths (0.5, 1, 2 x the occupancy grid) and keeps the fastest for
+ * this context's later passes.  The BVH layout stays binary: the 8-wide layout measured a
+ * few percent slower on the mesh workloads (TT_BVH_WIDTH=8 selects it at upload). */
+tt_status tt_autotune_views(tt_ctx* ctx, const tt_view* views, int32_t n, tt_tune_result* out);
+
 void tt_destroy(tt_ctx* ctx);
 
 #ifdef __cplusplus

@@ -222,7 +222,28 @@ EXPORTED_SYMBOLS = [
     "tt_guide_train_batch",
     "tt_guide_read_records",
     "tt_guide_features_batch",
+    "tt_render_views",
+    "tt_autotune_views",
 ]
+
+
+class View(C.Structure):
+    _fields_ = [("camera", Camera), ("spp", C.c_int32)]
+
+
+TUNE_MAX = 16
+
+
+class TuneResult(C.Structure):
+    _fields_ = [
+        ("wave_paths", C.c_int32),
+        ("grid", C.c_int32),
+        ("ms", C.c_double),
+        ("candidates", C.c_int32),
+        ("candidate_wave", C.c_int32 * TUNE_MAX),
+        ("candidate_grid", C.c_int32 * TUNE_MAX),
+        ("candidate_ms", C.c_double * TUNE_MAX),
+    ]
 
 
 class GuidingParams(C.Structure):
@@ -302,6 +323,8 @@ def load_library() -> C.CDLL:
         "tt_guide_train_batch": ([vp, P(C.c_float), C.c_int32, C.c_int32, C.c_float, P(C.c_float)], C.c_int32),
         "tt_guide_read_records": ([vp, P(C.c_float), C.c_int32, P(C.c_int32)], C.c_int32),
         "tt_guide_features_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
+        "tt_render_views": ([vp, P(View), C.c_int32, C.c_uint64, P(C.c_float)], C.c_int32),
+        "tt_autotune_views": ([vp, P(View), C.c_int32, P(TuneResult)], C.c_int32),
     }
     for name, (argtypes, restype) in sig.items():
         fn = getattr(lib, name)

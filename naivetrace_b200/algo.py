@@ -203,6 +203,39 @@ class GpuContext:
         self._check(self.lib.tt_guide_features_batch(self.h, _fp(q), len(q), _fp(out)), "tt_guide_features_batch")
         return out
 
+    # Multi-view batches -------------------------------------------------------------
+    @staticmethod
+    def _views(views):
+        arr = (abi.View * len(views))()
+        npix = 0
+        for k, (cam, spp) in enumerate(views):
+            arr[k].camera = cam.to_c()
+            arr[k].spp = int(spp)
+            npix += cam.xres * cam.yres
+        return arr, npix
+
+    def render_views(self, views, seed: int = 1):
+        """views: [(CameraSpec, spp)].  Returns one (yres, xres, 3) linear float image per
+        view (row 0 at the bottom, as framebuffer())."""
+        arr, npix = self._views(views)
+        rgb = np.zeros(3 * npix, np.float32)
+        self._check(self.lib.tt_render_views(self.h, arr, len(views), seed, _fp(rgb)), "tt_render_views")
+        out, o = [], 0
+        for cam, _ in views:
+            n = cam.xres * cam.yres
+            out.append(rgb[3 * o:3 * (o + n)].reshape(cam.yres, cam.xres, 3))
+            o += n
+        return out
+
+    def autotune_views(self, views) -> dict:
+        arr, _ = self._views(views)
+        r = abi.TuneResult()
+        self._check(self.lib.tt_autotune_views(self.h, arr, len(views), C.byref(r)), "tt_autotune_views")
+        k = min(r.candidates, abi.TUNE_MAX)
+        return {"wave_paths": r.wave_paths, "grid": r.grid, "ms": r.ms,
+                "candidates": [{"wave_paths": r.candidate_wave[i], "grid": r.candidate_grid[i],
+                                "ms": r.candidate_ms[i]} for i in range(k)]}
+
     def request_interrupt(self):
         self.lib.tt_request_interrupt(self.h)
 

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstddef>
 #include <cstdlib>
 #include <memory>
 #include <mutex>
@@ -148,6 +149,7 @@ struct tt_ctx {
   double rec_rate = 0.0;              // records committed per path in the last training pass
   uint64_t draw_seed = 0;
   bool ps_guided = false;      // the path state carries the guiding arrays
+  float bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0};  // scene bounds (medium trackers of views)
 };
 
 static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
@@ -179,6 +181,39 @@ static void frame_z_d(const double z[3], float X[3], float Y[3], float Z[3]) {
 static void normalize_d(double v[3]) {
   const double l = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   for (int k = 0; k < 3; ++k) v[k] /= l;
+}
+
+// Camera frame and pixel geometry (camera.hxx:38-108, 159-175), computed in double.
+static DevCamera make_dev_camera(const tt_camera& cm) {
+  DevCamera cam{};
+  cam.kind = cm.kind;
+  cam.xres = cm.xres;
+  cam.yres = cm.yres;
+  double up[3] = {cm.up[0], cm.up[1], cm.up[2]}, dir[3] = {cm.dir[0], cm.dir[1], cm.dir[2]};
+  normalize_d(up);
+  normalize_d(dir);
+  const double r = up[0] * dir[0] + up[1] * dir[1] + up[2] * dir[2];
+  if (!(std::fabs(r) > 1.0 - 2.220446049250313e-16)) {
+    for (int k = 0; k < 3; ++k) up[k] -= r * dir[k];
+    normalize_d(up);
+  }
+  const double right[3] = {up[1] * dir[2] - up[2] * dir[1], up[2] * dir[0] - up[0] * dir[2],
+                           up[0] * dir[1] - up[1] * dir[0]};
+  for (int k = 0; k < 3; ++k) {
+    cam.pos[k] = cm.pos[k];
+    cam.up[k] = (float)up[k];
+    cam.dir[k] = (float)dir[k];
+    cam.right[k] = (float)right[k];
+  }
+  const double fov = cm.fov_deg * M_PI / 180.;
+  const double aspect = (double)cm.yres / cm.xres;
+  const double a = std::tan(fov * 0.5), b = a * aspect;
+  cam.xmin = (float)-a;
+  cam.ymin = (float)-b;
+  cam.xperpixel = (float)(2. * a / cm.xres);
+  cam.yperpixel = (float)(2. * b / cm.yres);
+  cam.per_pixel_delta = (float)(2. / std::min(cm.xres, cm.yres));
+  return cam;
 }
 
 extern "C" {
@@ -601,37 +636,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     }
   }
   // Camera (camera.hxx:38-108, 159-175), computed in double.
-  {
-    const tt_camera& cm = c->camera;
-    DevCamera& cam = s.cam;
-    cam.kind = cm.kind;
-    cam.xres = cm.xres;
-    cam.yres = cm.yres;
-    double up[3] = {cm.up[0], cm.up[1], cm.up[2]}, dir[3] = {cm.dir[0], cm.dir[1], cm.dir[2]};
-    normalize_d(up);
-    normalize_d(dir);
-    const double r = up[0] * dir[0] + up[1] * dir[1] + up[2] * dir[2];
-    if (!(std::fabs(r) > 1.0 - 2.220446049250313e-16)) {
-      for (int k = 0; k < 3; ++k) up[k] -= r * dir[k];
-      normalize_d(up);
-    }
-    const double right[3] = {up[1] * dir[2] - up[2] * dir[1], up[2] * dir[0] - up[0] * dir[2],
-                             up[0] * dir[1] - up[1] * dir[0]};
-    for (int k = 0; k < 3; ++k) {
-      cam.pos[k] = cm.pos[k];
-      cam.up[k] = (float)up[k];
-      cam.dir[k] = (float)dir[k];
-      cam.right[k] = (float)right[k];
-    }
-    const double fov = cm.fov_deg * M_PI / 180.;
-    const double aspect = (double)cm.yres / cm.xres;
-    const double a = std::tan(fov * 0.5), b = a * aspect;
-    cam.xmin = (float)-a;
-    cam.ymin = (float)-b;
-    cam.xperpixel = (float)(2. * a / cm.xres);
-    cam.yperpixel = (float)(2. * b / cm.yres);
-    cam.per_pixel_delta = (float)(2. / std::min(cm.xres, cm.yres));
-  }
+  s.cam = make_dev_camera(c->camera);
   // Light picker (TrivialLightPicker, lightpicker_trivial.cxx:11-31) and scene bounds.
   const double nl = (double)c->points.size(), ne = c->envs.empty() ? 0. : 1., na = (double)al.size();
   const double tot = nl + ne + na;
@@ -656,6 +661,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
   const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
                                 (hi[2] - lo[2]) * (hi[2] - lo[2]));
   for (int k = 0; k < 3; ++k) {
+    c->bb_lo[k] = (float)lo[k];
+    c->bb_hi[k] = (float)hi[k];
     s.box_lo[k] = (float)lo[k];
     s.box_inv[k] = hi[k] > lo[k] ? (float)(1.0 / (hi[k] - lo[k])) : 1.f;
   }
@@ -1461,6 +1468,215 @@ tt_status tt_guide_features_batch(tt_ctx* c, const float* points, int32_t n, flo
   cudaFree(dx);
   if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
   for (size_t i = 0; i < hx.size(); ++i) features[i] = __bfloat162float(hx[i]);
+  return TT_OK;
+}
+
+// ---- Multi-view batches ---------------------------------------------------------------
+// All views of a batch are rendered as one wavefront over the concatenation of their
+// (pixel, sample) ranges.  The first wave runs eagerly (it loads the kernels and does the
+// one-time launch set-up); the per-wave launch sequence is then captured once into a CUDA
+// graph whose kernels read the wave's arguments from device memory and which advances the
+// wave index itself, and the graph is replayed for every further wave.
+static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64_t seed, float* rgb,
+                              int wave_limit, int grid, float* ms_out) {
+  if (!c || !views || n <= 0) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  std::vector<DevView> hv((size_t)n);
+  long long paths = 0, npix_total = 0;
+  for (int v = 0; v < n; ++v) {
+    const tt_camera& cm = views[v].camera;
+    if (cm.xres <= 0 || cm.yres <= 0 || views[v].spp <= 0 ||
+        (cm.kind != TT_CAMERA_PINHOLE && cm.kind != TT_CAMERA_FISHEYE))
+      return fail(c, TT_ERR_INVALID, "view " + std::to_string(v) + ": bad camera or spp");
+    hv[v].cam = make_dev_camera(cm);
+    hv[v].npix = cm.xres * cm.yres;
+    hv[v].spp = views[v].spp;
+    hv[v].pix_begin = (int)npix_total;
+    hv[v].path_begin = paths;
+    hv[v].seed = seed + (uint64_t)v;
+    hv[v].cam_track = c->dev.cam_track;
+    npix_total += hv[v].npix;
+    paths += (long long)hv[v].npix * hv[v].spp;
+    if (npix_total > (1ll << 30)) return fail(c, TT_ERR_CAPACITY, "views hold more than 2^30 pixels");
+  }
+  const int cap = (int)std::min<long long>(paths, wave_limit);
+  if (c->dev.guide_record) {
+    const double expected = c->rec_rate * (double)paths;
+    c->dev.guide_keep = expected > 0.0 ? (float)std::min(1.0, 0.8 * c->rec_cap / expected) : 1.f;
+  }
+  tt_status st = ensure_path_state(c, cap);
+  if (st != TT_OK) return st;
+  const int nwaves = (int)((paths + cap - 1) / cap);
+  std::vector<ViewWave> hw((size_t)nwaves);
+  for (int k = 0; k < nwaves; ++k) {
+    hw[k].wave_start = (long long)k * cap;
+    hw[k].wave_paths = (int)std::min<long long>(cap, paths - hw[k].wave_start);
+  }
+  DeviceBuffers m;
+  m.stream = c->stream;
+  DevView* d_views = (DevView*)m.alloc(hv.size() * sizeof(DevView));
+  ViewWave* d_waves = (ViewWave*)m.alloc(hw.size() * sizeof(ViewWave));
+  int* d_idx = (int*)m.alloc(sizeof(int));
+  float* d_acc = (float*)m.alloc(3 * (size_t)npix_total * sizeof(float));
+  float* d_light = (float*)m.alloc(3 * (size_t)npix_total * sizeof(float));
+  float* d_rgb = (float*)m.alloc(3 * (size_t)npix_total * sizeof(float));
+  if (!d_views || !d_waves || !d_idx || !d_acc || !d_light || !d_rgb) {
+    m.free_all();
+    return fail(c, TT_ERR_CUDA, "device allocation failed");
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  auto cleanup = [&]() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    m.free_all();
+  };
+  auto check = [&](cudaError_t e) -> tt_status {
+    if (e == cudaSuccess) return TT_OK;
+    cleanup();
+    return fail(c, TT_ERR_CUDA, std::string("multi-view pass: ") + cudaGetErrorString(e));
+  };
+  if ((st = check(cudaMemcpyAsync(d_views, hv.data(), hv.size() * sizeof(DevView), cudaMemcpyHostToDevice,
+                                  c->stream))) != TT_OK)
+    return st;
+  if ((st = check(cudaMemcpyAsync(d_waves, hw.data(), hw.size() * sizeof(ViewWave), cudaMemcpyHostToDevice,
+                                  c->stream))) != TT_OK)
+    return st;
+  cudaMemsetAsync(d_idx, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(d_acc, 0, 3 * (size_t)npix_total * sizeof(float), c->stream);
+  cudaMemsetAsync(d_light, 0, 3 * (size_t)npix_total * sizeof(float), c->stream);
+  if (c->dev.num_media > 0) {
+    // Medium tracker at each view's camera, written into its DevView.
+    for (int v = 0; v < n; ++v) {
+      const tt_camera& cm = views[v].camera;
+      uint2* dst = reinterpret_cast<uint2*>(reinterpret_cast<char*>(d_views + v) + offsetof(DevView, cam_track));
+      launch_init_tracker(c->dev, make_float3(cm.pos[0], cm.pos[1], cm.pos[2]),
+                          make_float3(c->bb_lo[0], c->bb_lo[1], c->bb_lo[2]),
+                          make_float3(c->bb_hi[0], c->bb_hi[1], c->bb_hi[2]), dst, c->d_err, c->stream);
+    }
+  }
+  Framebuffer fb{d_acc, d_light};
+  const int rounds = c->rounds;
+  const DevScene& sc = c->dev;
+  PathState& ps = c->ps;
+  auto wave = [&](cudaStream_t s) {
+    cudaMemsetAsync(ps.counters, 0, kCountersPerBounce * (size_t)(rounds + 3) * sizeof(int), s);
+    launch_generate_views(sc, ps, d_waves, d_idx, d_views, n, grid, s);
+    for (int b = 0; b < rounds; ++b) {
+      launch_shadow(sc, ps, fb, b, false, nullptr, grid, s);
+      launch_flush(sc, ps, fb, b, grid, s);
+      launch_extend(sc, ps, b, false, nullptr, grid, s);
+      if (sc.num_media > 0) launch_track(sc, ps, b, grid, s);
+      launch_shade(sc, ps, b, grid, s);
+      if (sc.guide) launch_guide(sc, ps, b, s);
+    }
+    launch_shadow(sc, ps, fb, rounds, false, nullptr, grid, s);
+    launch_flush(sc, ps, fb, rounds, grid, s);
+    k_tally<<<1, 32, 0, s>>>(ps.counters, rounds, c->d_stats);
+    launch_wave_advance(d_idx, s);
+  };
+  const int per_wave = 4 + rounds * (4 + (sc.num_media > 0) + (sc.guide != 0)) + 2;
+  cudaEventCreate(&ev0);
+  cudaEventCreate(&ev1);
+  cudaEventRecord(ev0, c->stream);
+  bool stopped = false;
+  int done_waves = 0;
+  wave(c->stream);  // eager first wave
+  ++done_waves;
+  if ((st = check(cudaGetLastError())) != TT_OK) return st;
+  if (nwaves > 1) {
+    if ((st = check(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal))) != TT_OK) return st;
+    wave(c->stream);
+    cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+    if ((st = check(ce)) != TT_OK) return st;
+    for (; done_waves < nwaves; ++done_waves) {
+      if (c->stop.load()) { stopped = true; break; }
+      if ((st = check(cudaGraphLaunch(exec, c->stream))) != TT_OK) return st;
+    }
+  }
+  launch_resolve_views(d_acc, d_light, d_views, n, (int)npix_total, d_rgb, c->stream);
+  cudaEventRecord(ev1, c->stream);
+  if ((st = check(cudaMemcpyAsync(rgb, d_rgb, 3 * (size_t)npix_total * sizeof(float), cudaMemcpyDeviceToHost,
+                                  c->stream))) != TT_OK)
+    return st;
+  if ((st = check(cudaStreamSynchronize(c->stream))) != TT_OK) return st;
+  if ((st = check(cudaGetLastError())) != TT_OK) return st;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ev0, ev1);
+  if (ms_out) *ms_out = ms;
+  c->stats.pass_ms += ms;
+  c->stats.kernel_launches += (uint64_t)done_waves * per_wave + 1;
+  c->stats.extend_launches += (uint64_t)done_waves * rounds;
+  c->stats.shadow_launches += (uint64_t)done_waves * (rounds + 1);
+  c->stats.paths += (uint64_t)std::min<long long>(paths, (long long)done_waves * cap);
+  cleanup();
+  if (c->dev.guide_record && !stopped && c->gparams.train == 1) {
+    const tt_status gs = guide_train(c, paths);
+    if (gs != TT_OK) return gs;
+  }
+  unsigned int errw = 0;
+  TT_CUDA(c, cudaMemcpy(&errw, c->d_err, sizeof(errw), cudaMemcpyDeviceToHost));
+  if (errw) {
+    c->stats.error_flags |= errw;
+    return fail(c, TT_ERR_LOOP_CAP, "a device loop hit its cap (error word " + std::to_string(errw) + ")");
+  }
+  if (stopped) return fail(c, TT_ERR_INTERRUPTED, "stopped by tt_request_stop");
+  return TT_OK;
+}
+
+tt_status tt_render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64_t seed, float* rgb) {
+  if (!c || !rgb) return TT_ERR_INVALID;
+  const int wave_limit = c->params.wave_paths > 0 ? c->params.wave_paths : kDefaultWave;
+  return render_views(c, views, n, seed, rgb, wave_limit, c->grid, nullptr);
+}
+
+tt_status tt_autotune_views(tt_ctx* c, const tt_view* views, int32_t n, tt_tune_result* out) {
+  if (!c || !views || n <= 0 || !out) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  // Probe batch: every view at one sample.
+  std::vector<tt_view> probe(views, views + n);
+  long long npix = 0;
+  for (auto& v : probe) {
+    v.spp = 1;
+    npix += (long long)v.camera.xres * v.camera.yres;
+  }
+  if (npix <= 0 || npix > (1ll << 30)) return fail(c, TT_ERR_INVALID, "bad views");
+  std::vector<float> rgb(3 * (size_t)npix);
+  const int waves[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
+  const int base_grid = c->grid;
+  const int grids[] = {base_grid / 2 > 0 ? base_grid / 2 : base_grid, base_grid, 2 * base_grid};
+  *out = tt_tune_result{};
+  double best = 1e300;
+  int k = 0;
+  // One untimed call first (path state at the largest size, kernels loaded).
+  tt_status st = render_views(c, probe.data(), n, 1, rgb.data(), waves[3], base_grid, nullptr);
+  if (st != TT_OK) return st;
+  for (int w : waves)
+    for (int g : grids) {
+      float ms = 0.f;
+      st = render_views(c, probe.data(), n, 1, rgb.data(), w, g, &ms);
+      if (st != TT_OK) return st;
+      if (k < TT_TUNE_MAX) {
+        out->candidate_wave[k] = w;
+        out->candidate_grid[k] = g;
+        out->candidate_ms[k] = ms;
+      }
+      ++k;
+      if (ms < best) {
+        best = ms;
+        out->wave_paths = w;
+        out->grid = g;
+        out->ms = ms;
+      }
+    }
+  out->candidates = k;
+  c->params.wave_paths = out->wave_paths;
+  c->grid = out->grid;
   return TT_OK;
 }
 

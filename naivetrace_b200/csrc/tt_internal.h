@@ -178,6 +178,22 @@ struct Framebuffer {
   float* light;        // npix * 3, this pass
 };
 
+// One camera view of a multi-view batch (tt_render_views).
+struct DevView {
+  DevCamera cam;
+  long long path_begin;        // first path of the view in the batch's path numbering
+  int pix_begin;               // first pixel of the view in the concatenated framebuffer
+  int npix;
+  int spp;
+  uint2 cam_track;             // medium tracker at the camera
+  unsigned long long seed;
+};
+
+struct ViewWave {
+  long long wave_start;
+  int wave_paths;
+};
+
 struct WaveArgs {
   long long wave_start;      // first path of this wave within the pass
   int wave_paths;
@@ -193,6 +209,14 @@ struct WaveArgs {
 void upload_constant_tables();
 void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
                      cudaStream_t st);
+// Multi-view batch: generate from waves[*wave_idx]; advance *wave_idx; per-view resolve.
+void launch_generate_views(const DevScene& s, const PathState& p, const ViewWave* waves, const int* wave_idx,
+                           const DevView* views, int nviews, int grid, cudaStream_t st);
+void launch_wave_advance(int* wave_idx, cudaStream_t st);
+void launch_resolve_views(const float* accum, const float* light, const DevView* views, int nviews, int npix,
+                          float* rgb, cudaStream_t st);
+// One-time launch set-up of the guided scatter (attributes, grid) outside stream capture.
+void prepare_guide_launch();
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats,
                    int grid, cudaStream_t st);
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);

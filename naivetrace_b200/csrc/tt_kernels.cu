@@ -17,6 +17,7 @@
 // device-side count, so launch shapes are fixed (a multiple of the SM count).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "tt_device.cuh"
@@ -561,6 +562,7 @@ struct Eye {
   const DevMaterial* mat;
   const DevMedium* med;  // volume eye: its medium
   float3 sigma_s;        // volume eye: scattering coefficient at the vertex
+  const DevCamera* cam;  // camera eye: its camera
 };
 
 __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye, const LightNode& L, Lambda l) {
@@ -603,7 +605,7 @@ __device__ __forceinline__ Connection connect(const DevScene& sc, const Eye& eye
   float3 sf;
   float pdf_eye = 0.f;
   if (eye.is_camera) {
-    const int unit = camera_evaluate(sc.cam, d, &pdf_eye);
+    const int unit = camera_evaluate(*eye.cam, d, &pdf_eye);
     c.unit = unit;
     sf = unit >= 0 ? f3(pdf_eye, pdf_eye, pdf_eye) : f3(0.f, 0.f, 0.f);
   } else if (eye.is_volume) {
@@ -737,6 +739,66 @@ __device__ __forceinline__ void emit_shadow(const DevScene& sc, const PathState&
   p.sh_c[slot] = make_float4(contrib.x, contrib.y, contrib.z, 0.f);
 }
 
+// One camera sample: wavelength selection, next-event estimation at the camera vertex
+// (splatted to the pixel the light sample projects to, scaled by splat_scale), camera ray.
+// `slot` is the path's slot, `pixel` its index in the framebuffer, `unit` the pixel within
+// the camera; the random stream is (seed, path_id).
+template <bool MEDIA>
+__device__ __forceinline__ void generate_one(const DevScene& sc, const PathState& p, int slot, int pixel, int unit,
+                                             unsigned long long seed, unsigned long long path_id,
+                                             const DevCamera& cam, uint2 cam_track, float splat_scale,
+                                             int splat_base) {
+  const int i = slot;
+  Rng rng;
+  rng.seed_path(seed, path_id);
+  // LambdaSelectionStrategy::WithWeights (shader_util.hxx:83-91).
+  const int main_idx = rng.uniform_int(0, 11);
+  int idx[3] = {main_idx, main_idx + 12, main_idx + 24};
+  const int rot = rng.uniform_int(0, 2);
+  { const int t = idx[0]; idx[0] = idx[rot]; idx[rot] = t; }
+  rng.uniform(); rng.uniform(); rng.uniform();  // SampleWavelengthStrata
+  const Lambda l{idx[0], idx[1], idx[2]};
+  const float3 beta = f3(12.f, 12.f, 12.f);
+  const float3 cam_pos = f3(cam.pos[0], cam.pos[1], cam.pos[2]);
+  const MTracker cam_mt = load_tracker(cam_track);
+  p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sc.guide_record) p.grec[(size_t)kRecF4 * i + 3] = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (sc.guide) p.rr[i] = 1.f;
+  // Next-event estimation at the camera vertex: a light sample seen directly by the
+  // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
+  if (sc.sample_lights) {
+    LightNode L = pick_light(sc, rng, l);
+    if (L.type != LIGHT_NONE) {
+      Eye eye;
+      eye.is_camera = true;
+      eye.is_volume = false;
+      eye.pos = cam_pos;
+      eye.cam = &cam;
+      Connection c = connect(sc, eye, L, l);
+      if (c.valid && c.unit >= 0)
+        emit_shadow<MEDIA>(sc, p, 0, i, c, L, beta, splat_scale, splat_base + c.unit, cam_mt, rng);
+    }
+  }
+  // Camera ray (TakeRandomWalkStep from the camera node).
+  DirSample s = camera_sample(cam, unit, rng);
+  const float3 bf = s.value * (1.f / s.pdf);
+  p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), 1u, s.delta ? 1u : 0u);
+  p.rng_state[i] = rng.state;
+  p.rng_inc[i] = rng.inc;
+  if (MEDIA) p.track[i] = cam_track;
+  if (is_zero(bf)) {
+    const int q = warp_append(done_count(p, 0));
+    p.done_q[q] = i;
+    return;
+  }
+  const float3 nb = mul(beta, bf);
+  p.beta[i] = make_float4(nb.x, nb.y, nb.z, s.pdf);
+  p.ray_o[i] = make_float4(cam_pos.x, cam_pos.y, cam_pos.z, 0.f);
+  p.ray_d[i] = make_float4(s.dir.x, s.dir.y, s.dir.z, kLargeNumber);
+  const int q = warp_append(ext_count(p, 0));
+  p.ext_q[0][q] = i;
+}
+
 template <bool MEDIA>
 __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Framebuffer fb, WaveArgs w) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.wave_paths; i += gridDim.x * blockDim.x) {
@@ -744,53 +806,61 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     const int pix_local = (int)(g % w.npix_range);
     const unsigned long long sample = w.sample_offset + (unsigned long long)(g / w.npix_range);
     const int pixel = w.pixel_begin + pix_local;
-    Rng rng;
-    rng.seed_path(w.seed, sample * (unsigned long long)w.npix_total + (unsigned long long)pixel);
-    // LambdaSelectionStrategy::WithWeights (shader_util.hxx:83-91).
-    const int main_idx = rng.uniform_int(0, 11);
-    int idx[3] = {main_idx, main_idx + 12, main_idx + 24};
-    const int rot = rng.uniform_int(0, 2);
-    { const int t = idx[0]; idx[0] = idx[rot]; idx[rot] = t; }
-    rng.uniform(); rng.uniform(); rng.uniform();  // SampleWavelengthStrata
-    const Lambda l{idx[0], idx[1], idx[2]};
-    const float3 beta = f3(12.f, 12.f, 12.f);
-    const float3 cam_pos = f3(sc.cam.pos[0], sc.cam.pos[1], sc.cam.pos[2]);
-    const MTracker cam_mt = load_tracker(sc.cam_track);
-    p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (sc.guide_record) p.grec[(size_t)kRecF4 * i + 3] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (sc.guide) p.rr[i] = 1.f;
-    // Next-event estimation at the camera vertex: a light sample seen directly by the
-    // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
-    if (sc.sample_lights) {
-      LightNode L = pick_light(sc, rng, l);
-      if (L.type != LIGHT_NONE) {
-        Eye eye;
-        eye.is_camera = true;
-        eye.is_volume = false;
-        eye.pos = cam_pos;
-        Connection c = connect(sc, eye, L, l);
-        if (c.valid && c.unit >= 0)
-          emit_shadow<MEDIA>(sc, p, 0, i, c, L, beta, 1.f / (float)w.npix_total, c.unit, cam_mt, rng);
-      }
+    generate_one<MEDIA>(sc, p, i, pixel, pixel, w.seed, sample * (unsigned long long)w.npix_total + (unsigned long long)pixel,
+                        sc.cam, sc.cam_track, 1.f / (float)w.npix_total, 0);
+  }
+}
+
+// Multi-view batches: the wave's paths are numbered over the concatenation of the views'
+// (pixel, sample) ranges; a path finds its view by binary search over the views' first
+// path indices (staged in shared memory).  View v's paths use the random streams that a
+// single-view pass of that camera with seed views[v].seed would use.  The wave arguments
+// come from device memory (waves[*wave_idx]) so that one captured graph serves every wave.
+constexpr int kMaxViewsSmem = 1024;
+
+template <bool MEDIA>
+__global__ void __launch_bounds__(256) k_generate_views(DevScene sc, PathState p, const ViewWave* waves,
+                                                        const int* wave_idx, const DevView* views, int nviews) {
+  __shared__ long long sbeg[kMaxViewsSmem];
+  const bool staged = nviews <= kMaxViewsSmem;
+  if (staged)
+    for (int v = threadIdx.x; v < nviews; v += blockDim.x) sbeg[v] = views[v].path_begin;
+  __syncthreads();
+  const ViewWave w = waves[*wave_idx];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < w.wave_paths; i += gridDim.x * blockDim.x) {
+    const long long g = w.wave_start + i;
+    int lo = 0, hi = nviews - 1;
+    while (lo < hi) {  // last view whose first path <= g
+      const int mid = (lo + hi + 1) >> 1;
+      const long long b = staged ? sbeg[mid] : views[mid].path_begin;
+      if (b <= g) lo = mid;
+      else hi = mid - 1;
     }
-    // Camera ray (TakeRandomWalkStep from the camera node).
-    DirSample s = camera_sample(sc.cam, pixel, rng);
-    const float3 bf = s.value * (1.f / s.pdf);
-    p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), 1u, s.delta ? 1u : 0u);
-    p.rng_state[i] = rng.state;
-    p.rng_inc[i] = rng.inc;
-    if (MEDIA) p.track[i] = sc.cam_track;
-    if (is_zero(bf)) {
-      const int q = warp_append(done_count(p, 0));
-      p.done_q[q] = i;
-      continue;
+    const DevView& V = views[lo];
+    const long long li = g - V.path_begin;
+    const int pix = (int)(li % V.npix);
+    const unsigned long long sample = (unsigned long long)(li / V.npix);
+    generate_one<MEDIA>(sc, p, i, V.pix_begin + pix, pix, V.seed, sample * (unsigned long long)V.npix + (unsigned long long)pix,
+                        V.cam, V.cam_track, 1.f / (float)V.npix, V.pix_begin);
+  }
+}
+
+__global__ void k_wave_advance(int* wave_idx) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) ++*wave_idx;
+}
+
+// rgb = (accum + splats) / spp of the pixel's view.
+__global__ void k_resolve_views(const float* accum, const float* light, const DevView* views, int nviews, int npix,
+                                float* rgb) {
+  for (int px = blockIdx.x * blockDim.x + threadIdx.x; px < npix; px += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nviews - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (views[mid].pix_begin <= px) lo = mid;
+      else hi = mid - 1;
     }
-    const float3 nb = mul(beta, bf);
-    p.beta[i] = make_float4(nb.x, nb.y, nb.z, s.pdf);
-    p.ray_o[i] = make_float4(cam_pos.x, cam_pos.y, cam_pos.z, 0.f);
-    p.ray_d[i] = make_float4(s.dir.x, s.dir.y, s.dir.z, kLargeNumber);
-    const int q = warp_append(ext_count(p, 0));
-    p.ext_q[0][q] = i;
+    const float inv = 1.f / (float)views[lo].spp;
+    for (int k = 0; k < 3; ++k) rgb[3 * px + k] = (accum[3 * px + k] + light[3 * px + k]) * inv;
   }
 }
 
@@ -1569,17 +1639,36 @@ void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, 
   k_flush<<<grid, kBlock, 0, st>>>(s, p, fb, bounce);
 }
 
+void launch_generate_views(const DevScene& s, const PathState& p, const ViewWave* waves, const int* wave_idx,
+                           const DevView* views, int nviews, int grid, cudaStream_t st) {
+  if (s.num_media > 0) k_generate_views<true><<<grid, kBlock, 0, st>>>(s, p, waves, wave_idx, views, nviews);
+  else k_generate_views<false><<<grid, kBlock, 0, st>>>(s, p, waves, wave_idx, views, nviews);
+}
+
+void launch_wave_advance(int* wave_idx, cudaStream_t st) { k_wave_advance<<<1, 32, 0, st>>>(wave_idx); }
+
+void launch_resolve_views(const float* accum, const float* light, const DevView* views, int nviews, int npix,
+                          float* rgb, cudaStream_t st) {
+  const int grid = std::max(1, std::min(65535, (npix + 255) / 256));
+  k_resolve_views<<<grid, 256, 0, st>>>(accum, light, views, nviews, npix, rgb);
+}
+
+static int g_guide_grid = 0;
+
+void prepare_guide_launch() {
+  if (g_guide_grid != 0) return;
+  cudaFuncSetAttribute(k_guide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
+  cudaFuncSetAttribute(k_guide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide<true>, kGuideWarps * 32, kGuideSmem);
+  g_guide_grid = sms * (per_sm > 0 ? per_sm : 1);
+}
+
 void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st) {
-  static int grid = 0;
-  if (grid == 0) {
-    cudaFuncSetAttribute(k_guide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
-    cudaFuncSetAttribute(k_guide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide<true>, kGuideWarps * 32, kGuideSmem);
-    grid = sms * (per_sm > 0 ? per_sm : 1);
-  }
+  prepare_guide_launch();
+  const int grid = g_guide_grid;
   if (s.num_media > 0) k_guide<true><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
   else k_guide<false><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
 }

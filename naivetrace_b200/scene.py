@@ -180,6 +180,17 @@ class CameraSpec:
     def num_pixels(self) -> int:
         return self.xres * self.yres
 
+    def to_c(self) -> abi.Camera:
+        c = abi.Camera()
+        c.kind = self.kind
+        c.pos[:] = [float(x) for x in self.pos]
+        c.dir[:] = [float(x) for x in self.dir]
+        c.up[:] = [float(x) for x in self.up]
+        c.fov_deg = float(self.fov_deg)
+        c.xres = int(self.xres)
+        c.yres = int(self.yres)
+        return c
+
 
 class Scene:
     """Triangle soup with per-triangle material, lights and one camera."""

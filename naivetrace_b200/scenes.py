@@ -414,3 +414,26 @@ def guiding_room(xres=1280, yres=720, emission=60.0) -> Scene:
     s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(3.7, 1.6, 0.4), dir=(-3.7, -0.8, 2.6), up=(0, 1, 0),
                           fov_deg=75.0, xres=xres, yres=yres)
     return s
+
+
+VIEW_RESOLUTIONS = (128, 256, 512, 768, 1024)
+
+
+def terrain_views(n=96, seed=4, spp_range=(4, 64), resolutions=VIEW_RESOLUTIONS):
+    """The multi-view workload: n seeded camera poses over the terrain_spheres scene, each
+    a square view with its side drawn uniformly from `resolutions` and its samples per pixel
+    uniformly from spp_range (inclusive).  Cameras sit 0.8-3.0 above the terrain within the
+    central 8 x 8 and look at a point near the centre.  Returns [(CameraSpec, spp)]."""
+    rng = np.random.default_rng(seed)
+    views = []
+    for _ in range(n):
+        side = int(rng.choice(resolutions))
+        spp = int(rng.integers(spp_range[0], spp_range[1] + 1))
+        pos = np.array([rng.uniform(-4, 4), rng.uniform(0.8, 3.0), rng.uniform(-4, 4)])
+        target = np.array([rng.uniform(-2, 2), 0.0, rng.uniform(-2, 2)])
+        d = target - pos
+        if np.linalg.norm(d[[0, 2]]) < 0.5:
+            d[0] += 1.0
+        views.append((CameraSpec(kind=abi.CAMERA_PINHOLE, pos=tuple(pos), dir=tuple(d / np.linalg.norm(d)),
+                                 up=(0.0, 1.0, 0.0), fov_deg=float(rng.uniform(40, 75)), xres=side, yres=side), spp))
+    return views
