@@ -260,6 +260,41 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
     }
 
 
+def multiview_comparison(g, n_views=96, seed=4):
+    """The multi-view workload on the already uploaded terrain scene: n seeded views, square
+    sides from {128, 256, 512, 768, 1024}, 4-64 spp, max depth of the context.  The batch
+    runs as one wavefront after the autotuner picked the queue capacity and launch width;
+    the same views are then rendered one call per view.  Both timed on the device (CUDA
+    events around the calls, synchronised on both sides)."""
+    import torch
+    from naivetrace_b200 import scenes
+    views = scenes.terrain_views(n_views, seed=seed)
+    paths = sum(c.xres * c.yres * s for c, s in views)
+    tune = g.autotune_views(views)
+    g.render_views(views[:4], seed=1)  # warm-up at the tuned configuration
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3
+
+    batch_ms = timed(lambda: g.render_views(views, seed=seed))
+    seq_ms = timed(lambda: [g.render_views([v], seed=seed + k) for k, v in enumerate(views)])
+    return {
+        "workload": f"terrain_views: {n_views} seeded views of the terrain_spheres scene, sides "
+                    f"{{128..1024}}, 4-64 spp, {sum(c.xres * c.yres for c, _ in views)} pixels, {paths} paths",
+        "paths": paths,
+        "batched": {"ms": batch_ms, "mpaths_per_s": paths / (batch_ms * 1e-3) / 1e6},
+        "one_call_per_view": {"ms": seq_ms, "mpaths_per_s": paths / (seq_ms * 1e-3) / 1e6},
+        "speedup": seq_ms / batch_ms,
+        "autotune": {"wave_paths": tune["wave_paths"], "grid": tune["grid"], "probe_ms": tune["ms"],
+                     "candidates": tune["candidates"]},
+        "timing": "wall clock around synchronised calls (host-side view upload and image read-back included)",
+    }
+
+
 def run_reference_arm(args):
     from naivetrace_b200 import dist as nd
     r = nd.init_from_env()
@@ -419,6 +454,9 @@ def run_ours(args):
     guiding = None
     if rank == 0 and world == 1 and not args.no_guiding:
         guiding = guiding_comparison()
+    multiview = None
+    if rank == 0 and world == 1 and not args.no_multiview and not args.small:
+        multiview = multiview_comparison(g)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -462,6 +500,7 @@ def run_ours(args):
                     "what": "tt_create + tt_upload_scene (scene H2D, device BVH build) + tt_render_pass + "
                             "tt_read_framebuffer + tt_destroy"},
             "guiding": guiding,
+            "multiview": multiview,
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": clk,
             "stats": {k: st[k] for k in ("extension_rays", "shadow_rays", "extend_launches", "extend_ms",
@@ -503,6 +542,7 @@ def main(argv=None):
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")
+    ap.add_argument("--no-multiview", action="store_true", help="skip the multi-view batch comparison")
     ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing: upload the workload and render one pass of --spp samples (for ncu captures)")
