@@ -530,6 +530,26 @@ def profile_run(args):
     return 0 if st["error_flags"] == 0 else 1
 
 
+def profile_guiding(args):
+    """No timing: the guiding workload at 640x360 (depth 12), four one-sample training passes
+    (16 Adam steps each) and one frozen four-sample pass; for ncu captures of the guider's
+    kernels."""
+    from naivetrace_b200 import scenes
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    g = GpuContext(scenes.guiding_room(640, 360), make_params(max_ray_depth=12))
+    g.set_guiding(True, 1, seed=7)
+    for k in range(4):
+        g.render(1, seed=100 + k)
+    g.set_guiding(True, 0, seed=7)
+    g.render(4, seed=3)
+    st = g.stats()
+    print(json.dumps({"profile_guiding": "guiding_room 640x360", "guide_steps": st["guide_steps"],
+                      "guide_records": st["guide_records"], "error_flags": st["error_flags"]}))
+    g.close()
+    return 0 if st["error_flags"] == 0 else 1
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -544,11 +564,15 @@ def main(argv=None):
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")
     ap.add_argument("--no-multiview", action="store_true", help="skip the multi-view batch comparison")
     ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
+    ap.add_argument("--profile-guiding", action="store_true",
+                    help="no timing: training and frozen passes of the guiding workload (for ncu captures)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing: upload the workload and render one pass of --spp samples (for ncu captures)")
     args = ap.parse_args(argv)
     if args.profile_run:
         return profile_run(args)
+    if args.profile_guiding:
+        return profile_guiding(args)
     if args.warmup < 3 and not args.small:
         args.warmup = 3
     if args.impl == "reference":

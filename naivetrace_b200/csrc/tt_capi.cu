@@ -886,7 +886,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
         launches++;
       }
       launch_shade(c->dev, c->ps, b, grid, c->stream);
-      if (c->dev.guide) {
+      if (c->dev.guide && b < c->dev.guide_depth) {
         launch_guide(c->dev, c->ps, b, c->stream);
         launches++;
       }
@@ -1572,14 +1572,14 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
       launch_extend(sc, ps, b, false, nullptr, grid, s);
       if (sc.num_media > 0) launch_track(sc, ps, b, grid, s);
       launch_shade(sc, ps, b, grid, s);
-      if (sc.guide) launch_guide(sc, ps, b, s);
+      if (sc.guide && b < sc.guide_depth) launch_guide(sc, ps, b, s);
     }
     launch_shadow(sc, ps, fb, rounds, false, nullptr, grid, s);
     launch_flush(sc, ps, fb, rounds, grid, s);
     k_tally<<<1, 32, 0, s>>>(ps.counters, rounds, c->d_stats);
     launch_wave_advance(d_idx, s);
   };
-  const int per_wave = 4 + rounds * (4 + (sc.num_media > 0) + (sc.guide != 0)) + 2;
+  const int per_wave = 4 + rounds * (4 + (sc.num_media > 0)) + (sc.guide ? std::min(rounds, sc.guide_depth) : 0) + 2;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0, c->stream);

@@ -4,13 +4,13 @@
 // with p = (1 - c) p_bsdf + c p_vmf, which also learns the selection probability c.
 //
 // One training step is four launches:
-//   k_train   persistent; per warp 32 records: features in registers, the five layers
+//   k_train   persistent; per warp 16 records: features in registers, the five layers
 //             (guide_mlp_tile, activations kept in global memory for the weight gradients),
 //             the loss gradient per record, and the backward pass through the layers on the
 //             same tensor-core tiles (B fragments of W^T by ldmatrix.trans from the forward
 //             weight image), storing each layer's output gradient;
 //   k_wgrad   dW_l = sum over records of dH_l^T X_l and the bias sums, split over chunks of
-//             512 records (mma.sync with ldmatrix.trans fragments of both operands);
+//             128 records (mma.sync with ldmatrix.trans fragments of both operands);
 //   k_reduce  sum of the chunk partials;
 //   k_adam    Adam on the FP32 master parameters, refreshing the BF16 copy.
 #include <cuda_bf16.h>
@@ -165,8 +165,9 @@ __device__ __forceinline__ void guide_bwd_tile(const bf16* sw, const bf16* dyt, 
 }
 
 constexpr int kTrainWarps = 4;
+constexpr int kTrainRows = 16;        // records per warp iteration (one tile)
 constexpr int kDyStride = kGOut + 8;  // BF16 output-gradient row in shared memory
-constexpr int kTrainWarpBytes = 32 * kGInputs * 4 + 32 * kGOutStride * 4 + 32 * kDyStride * 2;
+constexpr int kTrainWarpBytes = kTrainRows * (kGInputs * 4 + kGOutStride * 4 + kDyStride * 2);
 constexpr int kTrainSmem = kGSmBytes + kTrainWarps * kTrainWarpBytes;
 static_assert(kTrainWarpBytes % 16 == 0, "per-warp regions stay 16-byte aligned");
 
@@ -179,34 +180,37 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_train(const GuideRecord* _
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   unsigned char* wsm = tsm + kGSmBytes + warp * kTrainWarpBytes;
   float* q = reinterpret_cast<float*>(wsm);
-  float* o = q + 32 * kGInputs;
-  bf16* dys = reinterpret_cast<bf16*>(o + 32 * kGOutStride);
-  if (blockIdx.x * kTrainWarps * 32 >= n) return;
+  float* o = q + kTrainRows * kGInputs;
+  bf16* dys = reinterpret_cast<bf16*>(o + kTrainRows * kGOutStride);
+  if (blockIdx.x * kTrainWarps * kTrainRows >= n) return;
   guide_smem_load(w16, w32, sw, sb);
   __syncthreads();
   const float inv_n = 1.f / (float)n;
   float lsum = 0.f;
-  for (int base = (blockIdx.x * kTrainWarps + warp) * 32; base < n; base += gridDim.x * kTrainWarps * 32) {
+  for (int base = (blockIdx.x * kTrainWarps + warp) * kTrainRows; base < n;
+       base += gridDim.x * kTrainWarps * kTrainRows) {
     const int i = base + lane;
+    const bool mine = lane < kTrainRows && i < n;  // lanes 0..15 own the tile's records
     GuideRecord r{};
-    if (i < n) r = rec[i];
-    float* qr = q + lane * kGInputs;
-    qr[0] = r.pos[0]; qr[1] = r.pos[1]; qr[2] = r.pos[2];
-    qr[3] = r.n[0]; qr[4] = r.n[1]; qr[5] = r.n[2];
-    qr[6] = r.wo[0]; qr[7] = r.wo[1]; qr[8] = r.wo[2];
+    if (mine) r = rec[i];
+    if (lane < kTrainRows) {
+      float* qr = q + lane * kGInputs;
+      qr[0] = r.pos[0]; qr[1] = r.pos[1]; qr[2] = r.pos[2];
+      qr[3] = r.n[0]; qr[4] = r.n[1]; qr[5] = r.n[2];
+      qr[6] = r.wo[0]; qr[7] = r.wo[1]; qr[8] = r.wo[2];
+    }
     __syncwarp();
-#pragma unroll 1
-    for (int mt = 0; mt < 2; ++mt) {
-      GuideTileStore st{b.x, {b.h[0], b.h[1], b.h[2], b.h[3]}, base + mt * 16, n - (base + mt * 16)};
+    {
+      GuideTileStore st{b.x, {b.h[0], b.h[1], b.h[2], b.h[3]}, base, n - base};
       uint32_t xf[6][4];
-      guide_tile_features(q + mt * 16 * kGInputs, kGInputs, xf);
-      guide_mlp_tile(sw, sb, xf, o + mt * 16 * kGOutStride, kGOutStride, &st);
+      guide_tile_features(q, kGInputs, xf);
+      guide_mlp_tile(sw, sb, xf, o, kGOutStride, &st);
     }
     __syncwarp();
     // Loss and output gradient of record `lane`, divided by n and rounded to BF16.
-    {
+    if (lane < kTrainRows) {
       float d[kGOut];
-      if (i < n) {
+      if (mine) {
         lsum += guide_loss_row(r, o + lane * kGOutStride, d);
       } else {
 #pragma unroll
@@ -218,16 +222,14 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_train(const GuideRecord* _
       uint4* srow = reinterpret_cast<uint4*>(dys + lane * kDyStride);
 #pragma unroll
       for (int k = 0; k < kGOut / 8; ++k) srow[k] = make_uint4(pk[4 * k], pk[4 * k + 1], pk[4 * k + 2], pk[4 * k + 3]);
-      if (i < n) {
+      if (mine) {
         uint4* grow = reinterpret_cast<uint4*>(b.dy + (size_t)i * kGOut);
 #pragma unroll
         for (int k = 0; k < kGOut / 8; ++k) grow[k] = srow[k];
       }
     }
     __syncwarp();
-#pragma unroll 1
-    for (int mt = 0; mt < 2; ++mt)
-      guide_bwd_tile(sw, dys + mt * 16 * kDyStride, kDyStride, b, base + mt * 16, n - (base + mt * 16));
+    guide_bwd_tile(sw, dys, kDyStride, b, base, n - base);
     __syncwarp();
   }
   for (int s = 16; s > 0; s >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, s);
@@ -240,7 +242,7 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_train(const GuideRecord* _
 // shared memory and read transposed by ldmatrix.trans.  Partials go to
 // partial[blockIdx.x][guide_w_offset / guide_b_offset].
 constexpr int kWgRows = 32;
-constexpr int kWgChunk = 512;
+constexpr int kWgChunk = 128;
 constexpr int kWgGs = kGHid + 8;
 constexpr int kWgXs = kGIn + 8;
 
@@ -533,7 +535,7 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st) {
   TrainBufs b{x0, {h[0], h[1], h[2], h[3]}, {dh[0], dh[1], dh[2], dh[3]}, dy, loss};
   cudaMemsetAsync(loss, 0, sizeof(float), st);
   const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
-                                   (n + kTrainWarps * 32 - 1) / (kTrainWarps * 32));
+                                   (n + kTrainWarps * kTrainRows - 1) / (kTrainWarps * kTrainRows));
   k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b);
   const int z = (n + kWgChunk - 1) / kWgChunk;
   k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);

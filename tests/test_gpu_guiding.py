@@ -73,7 +73,7 @@ def test_forward_matches_oracle(gpu_lib):
 
 @pytest.mark.parametrize("n", [777, 9000])
 def test_gradient_matches_oracle(gpu_lib, n):
-    """9000 records span 18 chunks of the split weight-gradient kernel, the last one ragged."""
+    """9000 records span 71 chunks of the split weight-gradient kernel, the last one ragged."""
     g = _ctx()
     p = _params()
     g.guide_set_params(p)
