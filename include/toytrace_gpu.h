@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 3
+#define TT_ABI_VERSION 4
 
 typedef int32_t tt_status;
 enum {
@@ -173,6 +173,9 @@ typedef struct tt_scene_desc {
 } tt_scene_desc;
 
 enum { TT_SAMPLE_BOTH = 0, TT_SAMPLE_BSDF = 1, TT_SAMPLE_LIGHTS = 2 }; /* --pt-sample-mode */
+/* --algo: the forward path tracer with NEE (pt, renderingalgorithms_pathtracing.cxx) or its
+ * null-path variant (pt2, renderingalgorithms_pathtracing2.cxx). */
+enum { TT_ALGO_PT = 0, TT_ALGO_PT2 = 1 };
 
 /* RenderingParameters subset used by the path (src/scene.hxx:24-43). */
 typedef struct tt_params {
@@ -181,6 +184,7 @@ typedef struct tt_params {
   int32_t max_samples_per_pixel;/* --spp; <= 0 means unbounded (Run loops until stopped) */
   int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default */
   int32_t device;               /* CUDA device ordinal */
+  int32_t algo;                 /* TT_ALGO_* */
 } tt_params;
 
 typedef struct tt_ctx tt_ctx;

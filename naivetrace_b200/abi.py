@@ -42,6 +42,8 @@ ENV_DIRECTIONAL = 3
 CAMERA_PINHOLE = 0
 CAMERA_FISHEYE = 1
 
+ALGO_PT = 0
+ALGO_PT2 = 1
 SAMPLE_BOTH = 0
 SAMPLE_BSDF = 1
 SAMPLE_LIGHTS = 2
@@ -146,6 +148,7 @@ class Params(C.Structure):
         ("max_samples_per_pixel", C.c_int32),
         ("wave_paths", C.c_int32),
         ("device", C.c_int32),
+        ("algo", C.c_int32),
     ]
 
 

@@ -325,6 +325,19 @@ class GpuPathTracer:
         return self.ctx.framebuffer()
 
 
+class GpuPathTracer2(GpuPathTracer):
+    """RenderingAlgo for the null-path CUDA tracer (`--algo pt2`, PathTracingAlgo2,
+    renderingalgorithms_pathtracing2.cxx): the same pass schedule with params.algo set to
+    ALGO_PT2."""
+
+    def __init__(self, scene: Scene, params: Optional[abi.Params] = None, seed: int = 1, linear_output: bool = False):
+        p = make_params()
+        if params is not None:
+            C.memmove(C.byref(p), C.byref(params), C.sizeof(p))
+        p.algo = abi.ALGO_PT2
+        super().__init__(scene, p, seed, linear_output)
+
+
 def to_image_host(rgb, xres, yres, linear_output=False):
     return to_image(rgb, xres, yres, linear_output)
 

@@ -232,6 +232,7 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   if ((int64_t)d->camera.xres * d->camera.yres > (1ll << 30)) return fail(nullptr, TT_ERR_CAPACITY, "too many pixels");
   if (d->num_env_lights > (uint32_t)MAX_ENV_LIGHTS) return fail(nullptr, TT_ERR_CAPACITY, "too many env lights");
   if (p->pt_sample_mode < 0 || p->pt_sample_mode > 2) return fail(nullptr, TT_ERR_INVALID, "bad pt_sample_mode");
+  if (p->algo != TT_ALGO_PT && p->algo != TT_ALGO_PT2) return fail(nullptr, TT_ERR_INVALID, "unknown algo");
   if (p->max_ray_depth > 1000) return fail(nullptr, TT_ERR_INVALID, "max_ray_depth above 1000");
   for (uint32_t t = 0; t < d->num_triangles; ++t) {
     for (int k = 0; k < 3; ++k)
@@ -668,6 +669,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   }
   s.long_distance = (float)(10. * diag);
   s.max_path_nodes = c->params.max_ray_depth + 1;
+  s.algo = c->params.algo;
   s.sample_lights = c->params.pt_sample_mode != TT_SAMPLE_BSDF;
   s.sample_bsdf = c->params.pt_sample_mode != TT_SAMPLE_LIGHTS;
   if (tot == 0. && s.sample_lights) s.sample_lights = 0;  // no light to sample
@@ -744,6 +746,13 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
     p.vol = (float4*)m.alloc(n * sizeof(float4));
     p.sh_track = (uint2*)m.alloc(n * sizeof(uint2));
     p.sh_med = (float4*)m.alloc(n * sizeof(float4));
+  }
+  if (c->dev.algo == TT_ALGO_PT2) {
+    p.rough = (float*)m.alloc(n * sizeof(float));
+    if (c->dev.num_media > 0) {
+      p.wt2 = (float*)m.alloc(n * 9 * sizeof(float));
+      p.sh_wt = (float*)m.alloc(n * 9 * sizeof(float));
+    }
   }
   if (guided) {
     p.ginp = (float4*)m.alloc(n * 3 * sizeof(float4));
@@ -1298,6 +1307,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     c->gparams = *gp;
     return TT_OK;
   }
+  if (c->dev.algo != TT_ALGO_PT) return fail(c, TT_ERR_INVALID, "guiding needs algo pt");
   if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || gp->max_depth < 0 ||
       !(gp->learning_rate >= 0.f) ||
       gp->train < 0 || gp->train > 2)

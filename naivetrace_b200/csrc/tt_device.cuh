@@ -320,10 +320,46 @@ struct ScatterSample {
   bool delta;
 };
 
+// pt2's path regularisation (ShaderQuery::minimum_roughness): a dielectric met after a
+// rough bounce spreads its specular lobes into uniform cones of cos opening 1 - r
+// (SpecularTransmissiveDielectricShader::Sample/EvaluateBsdfMollified, shader.cxx:482-605).
+__device__ __forceinline__ float3 eval_dielectric_mollified(const DevMaterial& m, float3 wi, const Surf& s, float3 wo,
+                                                            float rough, float* pdf) {
+  const float opening_cos = 1.f - rough;
+  const bool entering = dot3(s.ng, wi) > 0.f;
+  const float eta = entering ? 1.f / m.ior_ratio : m.ior_ratio;
+  const float abs_i = fabsf(dot3(s.ns, wi));
+  float fr = 1.f;
+  float3 wt;
+  const bool has_wt = refracted(wi, s.ns, eta, &wt);
+  if (has_wt) fr = fresnel_reflectivity(abs_i, fabsf(dot3(wt, s.ns)), eta);
+  const float prob_reflection = has_wt ? fmaxf(0.1f, fminf(0.9f, fr)) : 1.f;
+  const float section_pdf = 1.f / (2.f * kPi * (1.f - opening_cos));
+  const bool maybe_reflected = dot3(reflected(wi, s.ns), wo) > opening_cos;
+  float total_pdf = maybe_reflected ? section_pdf * prob_reflection : 0.f;
+  float total_val = maybe_reflected ? prob_reflection * fr : 0.f;
+  if (has_wt && dot3(wt, wo) > opening_cos) {
+    total_val += (1.f - fr) * section_pdf;
+    total_pdf += (1.f - prob_reflection) * section_pdf;
+  }
+  if (dot3(wo, s.n) < 0.f) total_val *= eta * eta;
+  total_val /= fabsf(dot3(wo, s.ns));
+  if (pdf) *pdf = total_pdf;
+  return f3(total_val, total_val, total_val);
+}
+
+// Shader::MyRoughness (shader.cxx:244-247, 666-670): the microfacet's alpha, 0 otherwise.
+__device__ __forceinline__ float my_roughness(const DevMaterial& m) {
+  return m.shader == TT_SHADER_MICROFACET ? m.alpha : 0.f;
+}
+
 // EvaluateBSDF of DiffuseShader (shader.cxx:280-297), the delta shaders, and
 // MicrofacetShader (shader.cxx:676-689 with MicrofacetShaderWrapper::Evaluate :74-113).
+// min_rough > 0 (pt2 only) raises the microfacet's alpha and mollifies the dielectric.
 __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, const Surf& s, float3 wo, Lambda l,
-                                            float* pdf) {
+                                            float* pdf, float min_rough = 0.f) {
+  if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && min_rough > 0.f)
+    return eval_dielectric_mollified(m, wi, s, wo, min_rough, pdf);
   if (m.shader == TT_SHADER_DIFFUSE) {
     float3 ret = f3(0.f, 0.f, 0.f);
     if (dot3(s.n, wo) > 0.f) ret = take(m.reflectance, l) * (1.f / kPi);
@@ -337,7 +373,7 @@ __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, con
     const float3 wh = normalize3(lwi + lwo);
     const float ns_out = lwo.z, ns_in = lwi.z, ns_wh = wh.z;
     const float wh_out = dot3(lwo, wh), wh_in = dot3(lwi, wh);
-    const float d = beckmann_d(m.alpha, fabsf(ns_wh));
+    const float d = beckmann_d(fmaxf(m.alpha, min_rough), fabsf(ns_wh));
     const float g = g2_vcavity(wh_in, wh_out, ns_in, ns_out, ns_wh);
     if (pdf) {
       const float3 whf = wh.z < 0.f ? -wh : wh;
@@ -358,9 +394,39 @@ __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, con
 // SpecularTransmissiveDielectricShader::SampleBsdfRegular (:401-473), MicrofacetShader
 // (:692-707).  Draw order matches the reference: square, then single uniforms.
 __device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float3 wi, const Surf& s, Rng& rng,
-                                                     Lambda l) {
+                                                     Lambda l, float min_rough = 0.f) {
   ScatterSample out;
   out.delta = false;
+  if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && min_rough > 0.f) {
+    // SampleBsdfMollified (shader.cxx:482-549): lobe choice, then a direction in its cone.
+    const float opening_cos = 1.f - min_rough;
+    const float abs_i = fabsf(dot3(s.ns, wi));
+    const bool entering = dot3(s.ng, wi) > 0.f;
+    const float eta = entering ? 1.f / m.ior_ratio : m.ior_ratio;
+    float fr = 1.f;
+    float3 wt;
+    const bool has_wt = refracted(wi, s.ns, eta, &wt);
+    if (has_wt) fr = fresnel_reflectivity(abs_i, fabsf(dot3(wt, s.ns)), eta);
+    const float prob_reflection = has_wt ? fmaxf(0.1f, fminf(0.9f, fr)) : 1.f;
+    const bool do_reflect = has_wt ? rng.uniform() < prob_reflection : true;
+    const float section_pdf = 1.f / (2.f * kPi * (1.f - opening_cos));
+    float r[2];
+    rng.square(r);
+    const float3 axis = do_reflect ? reflected(wi, s.ns) : wt;
+    out.dir = frame_z(axis).to_world(to_sphere_section(opening_cos, r));
+    float value;
+    if (do_reflect) {
+      out.pdf = prob_reflection * section_pdf;
+      value = fr * section_pdf;
+    } else {
+      out.pdf = (1.f - prob_reflection) * section_pdf;
+      value = (1.f - fr) * section_pdf;
+    }
+    value /= fabsf(dot3(out.dir, s.ns));
+    if (dot3(out.dir, s.n) < 0.f) value *= eta * eta;
+    out.value = f3(value, value, value);
+    return out;
+  }
   if (m.shader == TT_SHADER_DIFFUSE) {
     const Frame fr = frame_z(s.ns);
     float r[2];
@@ -410,7 +476,8 @@ __device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float
   const float3 lwi = fr.to_local(wi);
   float r[2];
   rng.square(r);
-  float3 wh = beckmann_sample_wh(m.alpha, r);
+  const float alpha = fmaxf(m.alpha, min_rough);
+  float3 wh = beckmann_sample_wh(alpha, r);
   {
     // VisibleNdfVCavity::Sample
     const float3 whp = f3(-wh.x, -wh.y, wh.z);
@@ -421,7 +488,7 @@ __device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float
   const float3 ng = fr.to_local(s.n);
   const float ns_out = lwo.z, ns_in = lwi.z, ns_wh = wh.z;
   const float wh_out = dot3(lwo, wh), wh_in = dot3(lwi, wh);
-  const float d = beckmann_d(m.alpha, fabsf(ns_wh));
+  const float d = beckmann_d(alpha, fabsf(ns_wh));
   const float g = g2_vcavity(wh_in, wh_out, ns_in, ns_out, ns_wh);
   const float3 whf = wh.z < 0.f ? -wh : wh;
   out.pdf = vndf_pdf(d, whf, lwi) * 0.25f / (fabsf(dot3(whf, lwi)) + kEps);

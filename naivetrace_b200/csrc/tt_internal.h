@@ -132,6 +132,7 @@ struct DevScene {
   const float* guide_w32;          // FP32 master copy (the biases are read from it)
   float box_lo[3];            // scene box, for the position encoding
   float box_inv[3];           // 1 / extent per axis
+  int algo;                   // TT_ALGO_PT or TT_ALGO_PT2 (tt_pt2.cuh)
 };
 
 // Wavefront path state, structure of arrays, capacity `cap` paths.
@@ -171,6 +172,10 @@ struct PathState {
   GuideRecord* records;  // training-record pool, a ring of rec_cap records
   int* rec_count;        // records committed since the pool was emptied (index = count % rec_cap)
   int rec_cap;
+  // Null-path tracer (TT_ALGO_PT2) only.
+  float* rough;        // path roughness: largest microfacet alpha met so far
+  float* wt2;          // media scenes: weights_track, 9 floats per path (row-major 3 x 3)
+  float* sh_wt;        // media scenes: the path's weights_track at the shadow ray's vertex
 };
 
 struct Framebuffer {

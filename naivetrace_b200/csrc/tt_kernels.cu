@@ -764,9 +764,17 @@ __device__ __forceinline__ void generate_one(const DevScene& sc, const PathState
   p.accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (sc.guide_record) p.grec[(size_t)kRecF4 * i + 3] = make_float4(0.f, 0.f, 0.f, 0.f);
   if (sc.guide) p.rr[i] = 1.f;
+  const bool pt2 = sc.algo == TT_ALGO_PT2;
+  if (pt2) {
+    // CameraRenderWorker::InitializePathState (renderingalgorithms_pathtracing2.cxx:378-405):
+    // node count 2, unit track weights, no roughness; no next-event estimation at the camera.
+    p.rough[i] = 0.f;
+    if (MEDIA)
+      for (int k = 0; k < 9; ++k) p.wt2[9 * (size_t)i + k] = 1.f;
+  }
   // Next-event estimation at the camera vertex: a light sample seen directly by the
   // camera is splatted to the pixel it projects to, scaled by 1/(xres*yres).
-  if (sc.sample_lights) {
+  if (sc.sample_lights && !pt2) {
     LightNode L = pick_light(sc, rng, l);
     if (L.type != LIGHT_NONE) {
       Eye eye;
@@ -782,7 +790,8 @@ __device__ __forceinline__ void generate_one(const DevScene& sc, const PathState
   // Camera ray (TakeRandomWalkStep from the camera node).
   DirSample s = camera_sample(cam, unit, rng);
   const float3 bf = s.value * (1.f / s.pdf);
-  p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), 1u, s.delta ? 1u : 0u);
+  // meta.z: node count; meta.w bit 0: last scatter was a delta (pt2: bit 1 = has one).
+  p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), pt2 ? 2u : 1u, pt2 ? 0u : (s.delta ? 1u : 0u));
   p.rng_state[i] = rng.state;
   p.rng_inc[i] = rng.inc;
   if (MEDIA) p.track[i] = cam_track;
@@ -1557,6 +1566,8 @@ void upload_constant_tables() {
   cudaMemcpyToSymbol(c_smits, smits, sizeof(smits));
 }
 
+#include "tt_pt2.cuh"
+
 constexpr int kBlock = 256;
 
 // Calls f with std::integral_constant<bool, b>: picks a kernel instantiation at run time.
@@ -1604,12 +1615,32 @@ void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count
   });
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
+  if (s.algo == TT_ALGO_PT2) {
+    if (s.num_media == 0) {
+      k_shade2<false, false, false><<<grid, kBlock, 0, st>>>(s, p, bounce);
+      return;
+    }
+    with_bool(s.num_spheres > 0, [&](auto S) {
+      with_bool(s.wide != 0, [&](auto W) {
+        k_shade2<true, decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);
+      });
+    });
+    return;
+  }
   if (s.num_media > 0) k_shade<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
   else k_shade<false><<<grid, kBlock, 0, st>>>(s, p, bounce);
 }
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
   grid = trace_grid(s.wide != 0);
+  if (s.algo == TT_ALGO_PT2 && s.num_media > 0) {
+    with_bool(s.num_spheres > 0, [&](auto S) {
+      with_bool(s.wide != 0, [&](auto W) {
+        k_shadow2<decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);
+      });
+    });
+    return;
+  }
   // Media, sphere and layout variants are instantiated separately so that the surface-only,
   // triangle-only traversal stays lean for mesh scenes.
   with_bool(s.num_media > 0, [&](auto M) {
@@ -1624,6 +1655,7 @@ void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb,
   });
 }
 void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
+  if (s.algo == TT_ALGO_PT2) return;  // the null-path tracer tracks inside its shade stage
   with_bool(s.num_spheres > 0, [&](auto S) {
     with_bool(s.wide != 0, [&](auto W) {
       k_track<decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);

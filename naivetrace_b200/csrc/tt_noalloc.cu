@@ -127,6 +127,8 @@ extern "C" tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t s
     return s;
   };
   if (!d_accum || !d_light_accum) return fail(TT_ERR_INVALID, "tt_render_pass_noalloc: output buffer is NULL");
+  // The null-path tracer's per-path matrices have no room in the static array.
+  if (scene.algo != TT_ALGO_PT) return fail(TT_ERR_INVALID, "tt_render_pass_noalloc: algo pt only");
   if (spp <= 0) return fail(TT_ERR_INVALID, "tt_render_pass_noalloc: spp must be positive");
   if (pixel_begin < 0 || pixel_end > npix || pixel_begin >= pixel_end)
     return fail(TT_ERR_INVALID, "tt_render_pass_noalloc: bad pixel range");

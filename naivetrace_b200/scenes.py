@@ -66,14 +66,15 @@ def centered_box(center, half_extent):
     return v, t
 
 
-def cornell_box(xres=256, yres=256) -> Scene:
+def cornell_box(xres=256, yres=256, one_light_triangle=False) -> Scene:
     """Unit-cube Cornell box: 5 walls as 2-triangle quads (open towards the camera at
     z = 0), Lambert 0.75 white floor/ceiling/back wall, red left wall (0.75 in the bins
     centred at >= 605 nm, 0.05 elsewhere), green right wall (0.75 for 505-565 nm), a
     0.25 x 0.25 downward-facing area light just below the ceiling with flat emission 10,
     a 0.3^3 box at (0.65, 0, 0.35) rotated 17 degrees and a 0.3 x 0.6 x 0.3 box at
     (0.3, 0, 0.65) rotated -17 degrees.  Pinhole camera at (0.5, 0.5, -1.4) looking +z
-    with a 40 degree field of view."""
+    with a 40 degree field of view.  one_light_triangle keeps only the first triangle of
+    the light quad: a scene with exactly one light, whose selection probability is 1."""
     s = Scene()
     s.name = "cornell_box"
     white = s.add_material(diffuse(0.75))
@@ -89,7 +90,8 @@ def cornell_box(xres=256, yres=256) -> Scene:
     s.add_mesh(*quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0)), green)      # right x=1, -x
     q = 0.125
     yl = 1.0 - 1e-4
-    s.add_mesh(*quad((0.5 - q, yl, 0.5 - q), (0.5 + q, yl, 0.5 - q), (0.5 + q, yl, 0.5 + q), (0.5 - q, yl, 0.5 + q)), light)
+    lv, lt = quad((0.5 - q, yl, 0.5 - q), (0.5 + q, yl, 0.5 - q), (0.5 + q, yl, 0.5 + q), (0.5 - q, yl, 0.5 + q))
+    s.add_mesh(lv, lt[:1] if one_light_triangle else lt, light)
     s.add_mesh(*box_mesh((0.3, 0.3, 0.3), (0.65, 0.0, 0.35), 17.0), boxes)
     s.add_mesh(*box_mesh((0.3, 0.6, 0.3), (0.3, 0.0, 0.65), -17.0), boxes)
     s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.5, 0.5, -1.4), dir=(0, 0, 1), up=(0, 1, 0),
@@ -124,12 +126,12 @@ def cornell_box_materials(xres=64, yres=64) -> Scene:
     return s
 
 
-def cornell_box_medium(xres=256, yres=256) -> Scene:
+def cornell_box_medium(xres=256, yres=256, one_light_triangle=False) -> Scene:
     """The Cornell box filled with a homogeneous chromatic medium: sigma_s rising linearly
     from 0.5 to 2.0 per unit across the 36 bins, sigma_a = 0.1, Henyey-Greenstein g = 0.7.
     The medium's boundary is a closed box 1e-3 outside the walls, so no wall coincides
     with it; rays leave the medium through the open side of the box."""
-    s = cornell_box(xres, yres)
+    s = cornell_box(xres, yres, one_light_triangle)
     s.name = "cornell_box_medium"
     sigma_s = 0.5 + 1.5 * np.arange(36) / 35.0
     med = s.add_medium(MediumSpec(sigma_s=sigma_s, sigma_a=np.full(36, 0.1), phase=abi.PHASE_HENYEY_GREENSTEIN,

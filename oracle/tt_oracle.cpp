@@ -30,6 +30,7 @@ constexpr double Pi = 3.14159265358979323846264338327950288;
 constexpr double Eps = std::numeric_limits<double>::epsilon();        // vec3f.hxx:15
 constexpr float EpsF = std::numeric_limits<float>::epsilon();         // vec3f.hxx:16
 constexpr double LargeNumber = std::numeric_limits<double>::max() / 16;  // vec3f.hxx:22
+constexpr double Infinity = std::numeric_limits<double>::infinity();
 constexpr int NBINS = 36;
 
 static thread_local std::string g_err;
@@ -871,7 +872,44 @@ struct ScatterSample {
 // SpecularReflectiveShader, shader.cxx:338-366.
 // SpecularTransmissiveDielectricShader::SampleBsdfRegular, shader.cxx:401-473.
 // MicrofacetShader + MicrofacetShaderWrapper, shader.cxx:74-130, 676-707.
-static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const int32_t idx[3], double* pdf) {
+// Shader::MyRoughness (shader.cxx:244-247, 666-670): the microfacet's alpha, 0 otherwise.
+inline double MyRoughness(const tt_material& m) { return m.shader == TT_SHADER_MICROFACET ? (double)m.alpha : 0.; }
+
+// SpecularTransmissiveDielectricShader::Sample/EvaluateBsdfMollified (shader.cxx:482-605):
+// with a path roughness r > 0 (pt2's path regularisation) the specular lobes become
+// uniform cones of cos opening 1 - r around the reflected and refracted directions.
+static S3 EvaluateDielectricMollified(const tt_material& m, V3 wi, const Surf& si, V3 wo, double roughness,
+                                      double* pdf) {
+  const double opening_cos = 1. - roughness;
+  const bool entering = Dot(si.geometry_normal, wi) > 0.;
+  const double eta = entering ? 1. / m.ior_ratio : (double)m.ior_ratio;
+  const double radiance_weight = Sqr(eta);
+  const double abs_shn_dot_i = std::abs(Dot(si.shading_normal, wi));
+  double fr = 1.;
+  V3 wt;
+  const bool has_wt = Refracted(wi, si.shading_normal, eta, &wt);
+  if (has_wt) fr = FresnelReflectivity(abs_shn_dot_i, std::abs(Dot(wt, si.shading_normal)), eta);
+  const double prob_reflection = has_wt ? std::max(0.1, std::min(0.9, fr)) : 1.;
+  const double section_pdf = 1. / (2. * Pi * (1. - opening_cos));
+  const V3 refl = Reflected(wi, si.shading_normal);
+  const bool maybe_reflected = Dot(refl, wo) > opening_cos;
+  double total_pdf = maybe_reflected ? section_pdf * prob_reflection : 0.;
+  double total_val = maybe_reflected ? prob_reflection * fr : 0.;
+  if (has_wt) {
+    const bool maybe_refracted = Dot(wt, wo) > opening_cos;
+    total_val += maybe_refracted ? (1. - fr) * section_pdf : 0.;
+    total_pdf += maybe_refracted ? (1. - prob_reflection) * section_pdf : 0.;
+  }
+  if (Dot(wo, si.normal) < 0) total_val *= radiance_weight;
+  total_val /= std::abs(Dot(wo, si.shading_normal));
+  if (pdf) *pdf = total_pdf;
+  return S3(total_val);
+}
+
+static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const int32_t idx[3], double* pdf,
+                       double min_roughness = 0.) {
+  if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && min_roughness > 0.)
+    return EvaluateDielectricMollified(m, wi, si, wo, min_roughness, pdf);
   switch (m.shader) {
     case TT_SHADER_DIFFUSE: {
       S3 ret(0.);
@@ -888,7 +926,7 @@ static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const
     case TT_SHADER_MICROFACET: {
       const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
       const V3 ng = fr.ToLocal(si.normal);
-      const Beckman ndf{(double)m.alpha};
+      const Beckman ndf{std::max((double)m.alpha, min_roughness)};
       const V3 lwi = fr.ToLocal(wi), lwo = fr.ToLocal(wo);
       const V3 wh = Normalized(lwi + lwo);
       const double n_dot_out = Dot(ng, lwo);
@@ -913,8 +951,40 @@ static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const
   return S3(0.);
 }
 
-static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sampler& smp, const int32_t idx[3]) {
+static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sampler& smp, const int32_t idx[3],
+                                double min_roughness = 0.) {
   ScatterSample out;
+  if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && min_roughness > 0.) {
+    // SampleBsdfMollified (shader.cxx:482-549).
+    const double opening_cos = 1. - min_roughness;
+    const double abs_shn_dot_i = std::abs(Dot(si.shading_normal, wi));
+    const bool entering = Dot(si.geometry_normal, wi) > 0.;
+    const double eta = entering ? 1. / m.ior_ratio : (double)m.ior_ratio;
+    const double radiance_weight = Sqr(eta);
+    double fr = 1.;
+    V3 wt;
+    const bool has_wt = Refracted(wi, si.shading_normal, eta, &wt);
+    if (has_wt) fr = FresnelReflectivity(abs_shn_dot_i, std::abs(Dot(wt, si.shading_normal)), eta);
+    const double prob_reflection = has_wt ? std::max(0.1, std::min(0.9, fr)) : 1.;
+    const bool do_reflect = has_wt ? smp.Uniform01() < prob_reflection : true;
+    const double section_pdf = 1. / (2. * Pi * (1. - opening_cos));
+    double r[2];
+    double value;
+    const V3 axis = do_reflect ? Reflected(wi, si.shading_normal) : wt;
+    smp.UniformUnitSquare(r);
+    out.dir = OrthogonalSystemZAligned(axis).ToWorld(ToUniformSphereSection(opening_cos, r));
+    if (do_reflect) {
+      out.pdf = prob_reflection * section_pdf;
+      value = fr * section_pdf;
+    } else {
+      out.pdf = (1. - prob_reflection) * section_pdf;
+      value = (1. - fr) * section_pdf;
+    }
+    value /= std::abs(Dot(out.dir, si.shading_normal));
+    if (Dot(out.dir, si.normal) < 0) value *= radiance_weight;
+    out.value = S3(value);
+    return out;
+  }
   switch (m.shader) {
     case TT_SHADER_DIFFUSE: {
       const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
@@ -965,7 +1035,7 @@ static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sam
     }
     case TT_SHADER_MICROFACET: {
       const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
-      const Beckman ndf{(double)m.alpha};
+      const Beckman ndf{std::max((double)m.alpha, min_roughness)};
       const V3 lwi = fr.ToLocal(wi);
       double r[2];
       smp.UniformUnitSquare(r);
@@ -2026,6 +2096,384 @@ struct Worker {
 };
 
 // ---------------------------------------------------------------------------------------
+// pt2: PathTracingAlgo2 (renderingalgorithms_pathtracing2.cxx:126-700) with the null-path
+// estimators of media_integrator.cxx:216-420.  Per wavelength i and sampling wavelength j a
+// 3x3 matrix accumulates p_j / f_i over the tracked events (AccumulateContributions); the
+// contribution of a path is divided by the row mean, a balance heuristic over the hero
+// wavelengths, and NEE against BSDF sampling is weighted with those matrices (MisWeight,
+// :452-476).  No Russian roulette (RayTermination::SurvivalAtNthScatterNode with its
+// roulette commented out, rendering_util.hxx:383-412), no NEE from the camera, path
+// regularisation by the largest microfacet roughness met so far (ShaderQuery::minimum_roughness).
+struct M33 {
+  double a[3][3];
+  static M33 Ones() { M33 m; for (auto& r : m.a) for (double& x : r) x = 1.; return m; }
+  static M33 Inf() { M33 m; for (auto& r : m.a) for (double& x : r) x = Infinity; return m; }
+};
+inline void FixNan(M33& m) { for (auto& r : m.a) for (double& x : r) if (std::isnan(x)) x = Infinity; }
+inline void Acc(M33& w, const M33& x) {  // AccumulateContributions(w, x), media_integrator.cxx:223-229
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) w.a[i][j] *= x.a[i][j];
+  FixNan(w);
+}
+inline void Acc(M33& w, S3 f, S3 p) {  // AccumulateContributions(w, f, p), :231-238
+  M33 t;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      t.a[i][j] = (1. / f[i]) * p[j];
+      if (std::isnan(t.a[i][j])) t.a[i][j] = Infinity;
+    }
+  Acc(w, t);
+}
+inline S3 RowMean(const M33& m) {
+  return {(m.a[0][0] + m.a[0][1] + m.a[0][2]) / 3., (m.a[1][0] + m.a[1][1] + m.a[1][2]) / 3.,
+          (m.a[2][0] + m.a[2][1] + m.a[2][2]) / 3.};
+}
+inline S3 RowMeanScaledFixNan(const M33& m, double s) {
+  M33 t = m;
+  for (auto& r : t.a) for (double& x : r) x *= s;
+  FixNan(t);
+  return RowMean(t);
+}
+
+struct Factors { M33 track = M33::Ones(), nulls = M33::Ones(); };
+
+struct Worker2 {
+  const Scene& sc;
+  Sampler smp;
+  PathCtx ctx;
+  bool use_nee = true, use_emission = true;
+  int max_node_count;
+  explicit Worker2(const Scene& s) : sc(s) {
+    max_node_count = s.params.max_ray_depth;
+    if (s.params.pt_sample_mode == TT_SAMPLE_BSDF) use_nee = false;
+    if (s.params.pt_sample_mode == TT_SAMPLE_LIGHTS) use_emission = false;
+  }
+
+  // Medium::ComputeMajorante and EvaluateCoeffs; medium -1 is the vacuum.
+  S3 Majorant(int medium, V3 org, V3 dir, double len) const {
+    if (medium < 0) return S3(0.);
+    const MediumDesc& m = sc.media[medium];
+    if (m.kind == TT_MEDIUM_ATMOSPHERE) return S3(AtmSegmentMajorant(m, org, dir, len));
+    return TakeD3(m.sigma_ext, ctx.idx);
+  }
+  void Coeffs(int medium, V3 pos, S3* ss, S3* st) const {
+    if (medium < 0) { *ss = S3(0.); *st = S3(0.); return; }
+    const MediumDesc& m = sc.media[medium];
+    if (m.kind == TT_MEDIUM_ATMOSPHERE) { AtmCoeffs(m, Altitude(m, pos), ctx.idx, ss, st); return; }
+    *ss = TakeD3(m.sigma_s, ctx.idx);
+    *st = TakeD3(m.sigma_ext, ctx.idx);
+  }
+  static S3 Exp(S3 maj, double x) { return {std::exp(-x * maj[0]), std::exp(-x * maj[1]), std::exp(-x * maj[2])}; }
+  static S3 Sub(S3 a, S3 b) { return {a[0] - b[0], a[1] - b[1], a[2] - b[2]}; }
+
+  // nullpath::Tracking on one segment (media_integrator.cxx:240-286): hero-wavelength delta
+  // tracking.  Returns true at a real collision (distance *t, scattering coefficient *ss).
+  bool TrackSegment(int medium, V3 org, V3 dir, double len, Factors& f, double* t_out, S3* ss_out) {
+    const S3 maj = Majorant(medium, org, dir, len);
+    const double mfp = 1. / maj[0];
+    double t = 0.;
+    for (int it = 1; it < 10000; ++it) {
+      const double tlocal = std::min(LargeNumber, -std::log(1.0 - smp.Uniform01()) * mfp);
+      const S3 tr = Exp(maj, std::min(tlocal, len - t));
+      t += tlocal;
+      S3 ss, st;
+      Coeffs(medium, org + dir * t, &ss, &st);
+      if (t >= len) {
+        Acc(f.track, tr, tr);
+        Acc(f.nulls, tr, tr);
+        return false;
+      }
+      const S3 sn = Sub(maj, st);
+      const double prob_n = sn[0] * mfp;
+      if (smp.Uniform01() < prob_n) {
+        Acc(f.track, tr * sn, tr * sn);
+        Acc(f.nulls, tr * sn, tr * maj);
+      } else {
+        Acc(f.track, tr * st, tr * st);
+        Acc(f.nulls, tr * st, tr);
+        *t_out = t;
+        *ss_out = ss;
+        return true;
+      }
+    }
+    return false;  // iteration cap: no collision
+  }
+
+  // nullpath::Transmission on one segment (:288-325).
+  void TransmitSegment(int medium, V3 org, V3 dir, double len, Factors& f, Sampler& s) {
+    const S3 maj = Majorant(medium, org, dir, len);
+    const double mfp = 1. / maj[0];
+    double t = 0.;
+    for (int it = 1; it < 10000; ++it) {
+      const double tlocal = std::min(LargeNumber, -std::log(1.0 - s.Uniform01()) * mfp);
+      const S3 tr = Exp(maj, std::min(tlocal, len - t));
+      t += tlocal;
+      if (t >= len) {
+        Acc(f.track, tr, tr);
+        Acc(f.nulls, tr, tr);
+        return;
+      }
+      S3 ss, st;
+      Coeffs(medium, org + dir * t, &ss, &st);
+      const S3 sn = Sub(maj, st);
+      Acc(f.track, tr * sn, tr * sn);
+      Acc(f.nulls, tr * sn, tr * maj);
+      if (f.nulls.a[0][0] > LargeNumber && f.nulls.a[1][1] > LargeNumber && f.nulls.a[2][2] > LargeNumber) {
+        f.nulls = M33::Inf();
+        return;
+      }
+    }
+  }
+
+  // MisWeight (renderingalgorithms_pathtracing2.cxx:452-476).
+  std::pair<double, S3> MisWeight(bool has_pdf, double pdf, bool delta, double pdf_other, const M33& d,
+                                  const M33& d_other) const {
+    if (!has_pdf || delta || !(use_nee && use_emission)) return {1., RowMean(d)};
+    const S3 a = RowMeanScaledFixNan(d, pdf), b = RowMeanScaledFixNan(d_other, pdf_other);
+    return {pdf, a + b};
+  }
+
+  static S3 Div(S3 a, S3 b) { return {a[0] / b[0], a[1] / b[1], a[2] / b[2]}; }
+
+  struct State {
+    V3 org, dir;
+    MediumTracker mt;
+    M33 wt, wtn;
+    S3 path_weights;
+    bool has_last = false, last_delta = false;
+    double last_pdf = 0.;
+    double roughness = 0.;
+    int count = 0;
+  };
+
+  // AddDirectLighting (:479-560).  `vol_medium` >= 0 for a volume interaction at `pos`.
+  S3 DirectLighting(const State& ps, const Surf* si, V3 pos, int vol_medium) {
+    const int which = TowerSampling4(sc.type_probs, smp.Uniform01());
+    const int nlights = which == 0 ? 1 : (which == 1 ? (int)sc.area_lights.size() : (int)sc.points.size());
+    // TowerSamplingBisection over a uniform CMF: the first index whose (k + 1) / n exceeds r.
+    const double rr = smp.Uniform01();
+    int li = std::min(nlights - 1, std::max(0, (int)(rr * nlights)));
+    while (li > 0 && rr < (double)li / nlights) --li;
+    while (li < nlights - 1 && rr >= (double)(li + 1) / nlights) ++li;
+    const double prob = sc.type_probs[which] * (1. / nlights);
+    V3 org = si ? si->pos : pos, dir;
+    double len;
+    double pdf;
+    bool delta = false;
+    S3 light_weight;
+    if (which == 0) {
+      const DirSample e = EnvTakeDirectionSampleTotal(sc, smp, ctx.idx);
+      dir = -e.dir;
+      len = sc.long_distance;
+      if (si) org = org + AntiSelfIntersectionOffset(*si, dir);
+      pdf = e.pdf;
+      delta = e.delta;
+      light_weight = e.value / (e.pdf * prob);
+    } else {
+      V3 lpos, lng, lns;
+      S3 val;
+      double area_pdf;
+      if (which == 1) {
+        const int prim = sc.area_lights[li];
+        double r[2];
+        smp.UniformUnitSquare(r);
+        const V3 b = IsSphere(sc, prim) ? ToUniformSphere(r) * sc.sph_r[prim - sc.ntri] : ToTriangleBarycentricCoords(r);
+        const Surf ls = SurfaceFromBarycentric(sc, prim, b);
+        lpos = ls.pos;
+        lng = ls.geometry_normal;
+        lns = ls.shading_normal;
+        area_pdf = 1. / TriArea(sc, prim);
+      } else {
+        lpos = {sc.points[li].pos[0], sc.points[li].pos[1], sc.points[li].pos[2]};
+        area_pdf = 1.;
+        delta = true;
+      }
+      // Detail::SegmentToPoint (light.cxx:239-266): offset at the eye end only.
+      const V3 dd = lpos - org;
+      len = Length(dd);
+      if (len > 0.) dir = dd / len;
+      else { len = Eps; dir = si ? si->normal : V3{1., 0., 0.}; }
+      if (si) org = org + AntiSelfIntersectionOffset(*si, dir);
+      if (which == 1) {
+        const tt_material& lm = sc.materials[sc.mat_of_tri[sc.area_lights[li]]].m;
+        const double vis = Dot(lng, -dir) > 0. ? 1. : 0.;
+        val = Take(lm.emission, ctx.idx) * (vis / (2. * Pi)) * std::abs(Dot(lns, dir));
+        pdf = Sqr(len) / std::abs(Dot(dir, lng) + Eps) * area_pdf;
+      } else {
+        val = Take(sc.points[li].spectrum, ctx.idx) * (1. / (4. * Pi));
+        pdf = Sqr(len) / std::abs(0. + Eps) * area_pdf;
+      }
+      light_weight = val / (area_pdf * prob) / Sqr(len);
+    }
+    S3 pw = ps.path_weights;
+    MediumTracker mt = ps.mt;
+    double bsdf_pdf = 0.;
+    if (si) {
+      pw = pw * std::abs(Dot(si->shading_normal, dir));
+      const tt_material& m = sc.materials[sc.mat_of_tri[si->prim]].m;
+      pw = pw * EvaluateBSDF(m, -ps.dir, *si, dir, ctx.idx, &bsdf_pdf, ps.roughness);
+      if (Dot(dir, si->normal) < 0.) GoingThroughSurface(sc, mt, dir, Ff(si->geometry_normal), sc.mat_of_tri[si->prim]);
+    } else {
+      S3 ss, st;
+      pw = pw * MediumPhaseEvaluate(sc.media[vol_medium], pos, -ps.dir, dir, ctx.idx, &bsdf_pdf);
+      Coeffs(vol_medium, pos, &ss, &st);
+      pw = pw * Div(ss, st + S3(Eps));
+    }
+    // nullpath::Transmission (:384-420) on a stream seeded from the path's state here.
+    Sampler shadow;
+    SeedPath(shadow.g, smp.g.state, smp.g.inc);
+    Factors f;
+    const double slen = len * 0.9999;
+    double t, u, v;
+    if (Trace(sc, sc.surf, org, dir, 0., slen, true, &t, &u, &v) >= 0) {
+      f.track = M33::Inf();
+      f.nulls = M33::Inf();
+    } else {
+      std::vector<Crossing> hits;
+      AllHits(sc, sc.vol, org, dir, 0., slen, hits);
+      double snear = 0.;
+      size_t k = 0;
+      while (true) {
+        const double sfar = k < hits.size() ? hits[k].t : slen;
+        Factors seg;
+        TransmitSegment(mt.current, org + dir * snear, dir, sfar - snear, seg, shadow);
+        Acc(f.nulls, seg.nulls);
+        Acc(f.track, seg.track);
+        if (k >= hits.size()) break;
+        GoingThroughSurface(sc, mt, dir, hits[k].n, hits[k].material);
+        snear = sfar;
+        ++k;
+      }
+    }
+    Acc(f.track, ps.wt);
+    Acc(f.nulls, ps.wt);
+    const auto mw = MisWeight(true, pdf, delta, bsdf_pdf, f.nulls, f.track);
+    return Div(pw * light_weight * mw.first, mw.second);
+  }
+
+  void RenderPixel(int pixel, double rgb_out[3]) {
+    int main_idx = smp.UniformInt(0, 11);
+    int32_t idx[3] = {main_idx, main_idx + 12, main_idx + 24};
+    int rotation = smp.UniformInt(0, 2);
+    std::swap(idx[0], idx[rotation]);
+    for (int i = 0; i < 3; ++i) smp.Uniform01();
+    std::memcpy(ctx.idx, idx, sizeof(idx));
+    State ps;
+    ps.wt = M33::Ones();
+    ps.wtn = M33::Ones();
+    ps.path_weights = S3(12.);
+    ps.org = {sc.cam.pos.x, sc.cam.pos.y, sc.cam.pos.z};
+    const DirSample cs = CameraTakeDirectionSample(sc.cam, pixel, smp);
+    ps.path_weights = ps.path_weights * (cs.value / cs.pdf);
+    ps.dir = cs.dir;
+    InitializeMediumTracker(sc, ps.mt, ps.org);
+    ps.count = 2;
+    S3 total(0.);
+    if (ps.path_weights.IsZero()) { SpectralSelectionToRGB(total, ctx.idx, rgb_out); return; }
+    while (true) {
+      // nullpath::Tracking (:330-378): closest hit, then the segments in front of it.
+      double t = 0, u = 0, v = 0;
+      const int prim = Trace(sc, sc.surf, ps.org, ps.dir, 0., LargeNumber, false, &t, &u, &v);
+      const double tfar = prim >= 0 ? t : LargeNumber;
+      const double vend = tfar * 0.9999;
+      std::vector<Crossing> hits;
+      AllHits(sc, sc.vol, ps.org, ps.dir, 0., vend, hits);
+      Factors f;
+      bool volume = false;
+      int vmed = -1;
+      V3 vpos;
+      S3 vss;
+      double snear = 0.;
+      size_t k = 0;
+      while (true) {
+        const double sfar = k < hits.size() ? hits[k].t : vend;
+        const int medium = ps.mt.current;
+        Factors seg;
+        double tc;
+        S3 ss;
+        const bool hit_medium = TrackSegment(medium, ps.org + ps.dir * snear, ps.dir, sfar - snear, seg, &tc, &ss);
+        Acc(f.nulls, seg.nulls);
+        Acc(f.track, seg.track);
+        if (hit_medium) {
+          volume = true;
+          vmed = medium;
+          vpos = ps.org + ps.dir * (snear + tc);
+          vss = ss;
+          break;
+        }
+        if (k >= hits.size()) break;
+        GoingThroughSurface(sc, ps.mt, ps.dir, hits[k].n, hits[k].material);
+        snear = sfar;
+        ++k;
+      }
+      ps.wtn = ps.wt;
+      Acc(ps.wtn, f.nulls);
+      Acc(ps.wt, f.track);
+      if (!volume && prim < 0) {
+        // AddEnvEmission (:625-648).
+        if (use_emission && !sc.env.empty()) {
+          const S3 rad = EnvEvaluateTotal(sc, -ps.dir, ctx.idx);
+          const double pdf_env = EnvEvaluatePdfTotal(sc, -ps.dir) * sc.type_probs[0];
+          const auto mw = ps.has_last ? MisWeight(true, ps.last_pdf, ps.last_delta, pdf_env, ps.wt, ps.wtn)
+                                      : MisWeight(false, 0., false, 1., ps.wt, ps.wtn);
+          total = total + Div(rad * ps.path_weights * mw.first, mw.second);
+        }
+        break;
+      }
+      ScatterSample s;
+      Surf si;
+      if (!volume) {
+        si = SurfaceFromHit(sc, prim, u, v, ps.org, ps.dir, t);
+        const tt_material& m = sc.materials[sc.mat_of_tri[prim]].m;
+        // MaybeAddEmission (:592-622).
+        if (use_emission && m.emissive) {
+          const double vis = Dot(si.geometry_normal, -ps.dir) > 0. ? 1. : 0.;
+          const S3 rad = Take(m.emission, ctx.idx) * (vis / (2. * Pi));
+          std::pair<double, S3> mw;
+          if (ps.has_last) {
+            const double prob_select = sc.type_probs[1] * sc.in_class[1];
+            const double area_pdf = 1. / TriArea(sc, prim);
+            const double cvt = Sqr(Length(ps.org - si.pos)) / std::abs(Dot(ps.dir, si.normal) + Eps);
+            mw = MisWeight(true, ps.last_pdf, ps.last_delta, prob_select * area_pdf * cvt, ps.wt, ps.wtn);
+          } else {
+            mw = MisWeight(false, 0., false, 1., ps.wt, ps.wtn);
+          }
+          total = total + Div(rad * ps.path_weights * mw.first, mw.second);
+        }
+        if (use_nee) total = total + DirectLighting(ps, &si, si.pos, -1);
+        // SampleScatterer (:571-583): the query sees the roughness before this vertex.
+        s = SampleBSDF(m, -ps.dir, si, smp, ctx.idx, ps.roughness);
+        ps.roughness = std::max(MyRoughness(m), ps.roughness);
+      } else {
+        if (use_nee) total = total + DirectLighting(ps, nullptr, vpos, vmed);
+        s = MediumPhaseSample(sc.media[vmed], vpos, -ps.dir, smp, ctx.idx);
+        S3 ss, st;
+        Coeffs(vmed, vpos, &ss, &st);
+        s.value = s.value * Div(ss, st + S3(Eps));
+      }
+      ps.count++;
+      if (ps.count > max_node_count) break;
+      // PrepareStateForAfterScattering (:585-604).
+      if (!volume) {
+        ps.path_weights = ps.path_weights * s.value * (std::abs(Dot(si.shading_normal, s.dir)) / s.pdf);
+        ps.org = si.pos + AntiSelfIntersectionOffset(si, s.dir);
+        if (Dot(s.dir, si.normal) < 0.) GoingThroughSurface(sc, ps.mt, s.dir, Ff(si.geometry_normal), sc.mat_of_tri[prim]);
+      } else {
+        ps.path_weights = ps.path_weights * s.value / s.pdf;
+        ps.org = vpos;
+      }
+      ps.dir = s.dir;
+      ps.has_last = true;
+      ps.last_pdf = s.pdf;
+      ps.last_delta = s.delta;
+      // A path whose weights vanished adds nothing more (stopped here; the reference would
+      // continue it to the depth limit).
+      if (ps.path_weights.IsZero() || !(s.pdf > 0.)) break;
+    }
+    SpectralSelectionToRGB(total, ctx.idx, rgb_out);
+  }
+};
+
+// ---------------------------------------------------------------------------------------
 static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
   if (!d || !p) { g_err = "null argument"; return false; }
   s.params = *p;
@@ -2302,6 +2750,8 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
   std::vector<std::vector<Splat>> splats(nthreads);
   auto body = [&](int tid) {
     Worker w(sc);
+    Worker2 w2(sc);
+    const bool pt2 = sc.params.algo == TT_ALGO_PT2;
     std::vector<double> scratch;
     for (;;) {
       int p0 = next.fetch_add(CHUNK);
@@ -2310,9 +2760,14 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
       for (int p = p0; p < p1; ++p) {
         for (int sidx = 0; sidx < spp; ++sidx) {
           uint64_t sample = (uint64_t)sample_offset + sidx;
-          SeedPath(w.smp.g, seed, sample * (uint64_t)npix + (uint64_t)p);
           double rgb[3];
-          w.RenderPixel(p, rgb, &splats[tid]);
+          if (pt2) {
+            SeedPath(w2.smp.g, seed, sample * (uint64_t)npix + (uint64_t)p);
+            w2.RenderPixel(p, rgb);
+          } else {
+            SeedPath(w.smp.g, seed, sample * (uint64_t)npix + (uint64_t)p);
+            w.RenderPixel(p, rgb, &splats[tid]);
+          }
           for (int k = 0; k < 3; ++k) accum[3 * (size_t)p + k] += rgb[k];
         }
       }

@@ -60,3 +60,10 @@ def test_noalloc_limits(gpu_lib):
     st, acc, _ = noalloc_pass(g, 1, 1, 0, 65536)
     assert st == abi.TT_OK
     assert np.abs(acc).sum() > 0
+
+
+def test_noalloc_rejects_pt2(gpu_lib):
+    """The null-path tracer's per-path matrices have no room in the static array."""
+    g = GpuContext(scenes.cornell_box(8, 8), make_params(max_ray_depth=4, algo=abi.ALGO_PT2))
+    st, _, _ = noalloc_pass(g, 1, 1, 0, g.npix)
+    assert st == abi.TT_ERR_INVALID
