@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 4
+#define TT_ABI_VERSION 5
 
 typedef int32_t tt_status;
 enum {
@@ -185,6 +185,9 @@ typedef struct tt_params {
   int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default */
   int32_t device;               /* CUDA device ordinal */
   int32_t algo;                 /* TT_ALGO_* */
+  int32_t qmc;                  /* --qmc (RenderingParameters::qmc): Sobol points with per-pixel
+                                   rotations instead of pseudo-random numbers; used by pt2 only
+                                   (as in the reference), which then needs max_ray_depth <= 31 */
 } tt_params;
 
 typedef struct tt_ctx tt_ctx;

@@ -149,6 +149,7 @@ class Params(C.Structure):
         ("wave_paths", C.c_int32),
         ("device", C.c_int32),
         ("algo", C.c_int32),
+        ("qmc", C.c_int32),
     ]
 
 

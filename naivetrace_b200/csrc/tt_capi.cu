@@ -20,6 +20,7 @@
 #include "tt_guide.cuh"
 #include "tt_guide.h"
 #include "tt_internal.h"
+#include "tt_sobol_data.h"
 #include "tt_tables.h"
 
 using namespace tt;
@@ -161,6 +162,39 @@ static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
   return s;
 }
 
+// Generator matrices of the quasi-random sampler, 32 columns per dimension, each column
+// left-aligned to bit 31 (sampler.cxx:224-251).  Dimension 0 is the van der Corput
+// sequence.  Dimension d >= 1 takes (s, a, m_1..m_s) from the Joe-Kuo table and extends
+// the m's by the recurrence of the reference's generator (misc/
+// SobolSequenceGeneratorMatrices.ipynb, MakeTheMatrix): m_k = m_{k-s} ^ (m_{k-s} << s)
+// ^ the sum over i < s - 1 of bit (s - 2 - i) of a times m_{k-s+i+1} << (s - 1 - i).
+// (Joe and Kuo pair a's most significant bit with m_{k-1}; the reference pairs it with
+// m_{k-s+1}.  The two agree for s <= 2, and the matrices here follow the reference.)
+static void build_sobol_matrices(std::vector<uint32_t>* out) {
+  static_assert(TT_SOBOL_DIMS == kSobolDims && TT_ROTATION_BLOCK == kRotationBlock, "table sizes");
+  out->assign((size_t)kSobolDims * 32, 0u);
+  uint32_t* C = out->data();
+  for (int k = 0; k < 32; ++k) C[k] = 1u << (31 - k);
+  size_t pos = 0;
+  for (int d = 1; d < kSobolDims; ++d) {
+    const int s = tt_sobol_sam[pos], a = tt_sobol_sam[pos + 1];
+    const uint16_t* m = tt_sobol_sam + pos + 2;
+    pos += 2 + (size_t)s;
+    uint64_t mk[32];
+    for (int k = 0; k < 32; ++k) {
+      if (k < s) {
+        mk[k] = m[k];
+        continue;
+      }
+      uint64_t v = mk[k - s] ^ (mk[k - s] << s);
+      for (int i = 0; i < s - 1; ++i)
+        if ((a >> (s - 2 - i)) & 1) v ^= mk[k - s + i + 1] << (s - 1 - i);
+      mk[k] = v;
+    }
+    for (int k = 0; k < 32; ++k) C[32 * (size_t)d + k] = (uint32_t)(mk[k] << (31 - k));
+  }
+}
+
 #define TT_CUDA(ctx, call)                                                                   \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
@@ -233,6 +267,8 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   if (d->num_env_lights > (uint32_t)MAX_ENV_LIGHTS) return fail(nullptr, TT_ERR_CAPACITY, "too many env lights");
   if (p->pt_sample_mode < 0 || p->pt_sample_mode > 2) return fail(nullptr, TT_ERR_INVALID, "bad pt_sample_mode");
   if (p->algo != TT_ALGO_PT && p->algo != TT_ALGO_PT2) return fail(nullptr, TT_ERR_INVALID, "unknown algo");
+  if (p->algo == TT_ALGO_PT2 && p->qmc && (p->max_ray_depth <= 0 ? 25 : p->max_ray_depth) > 31)
+    return fail(nullptr, TT_ERR_INVALID, "qmc needs max_ray_depth <= 31 (64 sampler subsequences)");
   if (p->max_ray_depth > 1000) return fail(nullptr, TT_ERR_INVALID, "max_ray_depth above 1000");
   for (uint32_t t = 0; t < d->num_triangles; ++t) {
     for (int k = 0; k < 3; ++k)
@@ -670,6 +706,15 @@ tt_status tt_upload_scene(tt_ctx* c) {
   s.long_distance = (float)(10. * diag);
   s.max_path_nodes = c->params.max_ray_depth + 1;
   s.algo = c->params.algo;
+  // Quasi-random sampling: pt2 only, as in the reference (CameraRenderWorker's sampler).
+  s.sobol = nullptr;
+  s.rotations = nullptr;
+  std::vector<uint32_t> sobol;
+  if (c->params.qmc && c->params.algo == TT_ALGO_PT2) {
+    build_sobol_matrices(&sobol);
+    s.sobol = (const uint32_t*)upload(sobol.data(), sobol.size() * sizeof(uint32_t));
+    s.rotations = (const float*)upload(tt_rotation_offsets, sizeof(tt_rotation_offsets));
+  }
   s.sample_lights = c->params.pt_sample_mode != TT_SAMPLE_BSDF;
   s.sample_bsdf = c->params.pt_sample_mode != TT_SAMPLE_LIGHTS;
   if (tot == 0. && s.sample_lights) s.sample_lights = 0;  // no light to sample
@@ -752,6 +797,10 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
     if (c->dev.num_media > 0) {
       p.wt2 = (float*)m.alloc(n * 9 * sizeof(float));
       p.sh_wt = (float*)m.alloc(n * 9 * sizeof(float));
+    }
+    if (c->dev.sobol) {
+      p.qmc = (uint4*)m.alloc(n * sizeof(uint4));
+      if (c->dev.num_media > 0) p.sh_qmc = (uint4*)m.alloc(n * sizeof(uint4));
     }
   }
   if (guided) {

@@ -104,6 +104,51 @@ struct Rng {
 };
 
 // ----------------------------------------------------------------------------------------
+// QuasiRandomSequence (sampler.cxx:254-331) for pt2 with qmc, else the path's PCG32
+// stream.  The k-th one-dimensional draw of subsequence `id` is Sobol dimension
+// (id << 6) + 2 + k for k < 62 (later draws come from the PCG32 stream); two-dimensional
+// draws are dimensions (id << 6) and (id << 6) + 1.  The point index is the sample's index
+// in its pixel; every draw is shifted by the pixel's Cranley-Patterson rotation (x for 1D
+// draws, (x, y) for 2D draws) modulo 1, here in 32-bit fixed point.  Integer draws always
+// come from PCG32 (Sampler::UniformInt).  The subsequence is set per vertex as
+// PrepSamplerDimension does: (node count << 1) | 1 for next-event estimation, | 0 for
+// scattering; distance sampling continues the subsequence of the scatter before it.
+__device__ __forceinline__ uint32_t sobol_mult(uint32_t point, const uint32_t* m) {
+  uint32_t c = 0u;
+  for (int k = 0; k < 32 && point != 0u; ++k, point >>= 1)
+    if (point & 1u) c ^= __ldg(m + k);
+  return c;
+}
+__device__ __forceinline__ float fixed01(uint32_t u) { return (float)(u >> 8) * (1.f / 16777216.f); }
+
+struct Smp2 {
+  Rng rng;
+  const uint32_t* mats;  // null: pseudo-random
+  uint4 q;               // point, rotation x, rotation y, dimension offset | draw counter << 16
+  __device__ __forceinline__ void prep(uint32_t id) { q.w = id << 6; }
+  __device__ __forceinline__ float uniform() {
+    if (!mats) return rng.uniform();
+    const uint32_t base = q.w & 0xffffu, sub = q.w >> 16;
+    const uint32_t c = sub < 62u ? sobol_mult(q.x, mats + 32u * (base + 2u + sub)) : rng.next();
+    q.w = base | ((sub < 0xffffu ? sub + 1u : sub) << 16);
+    return fixed01(c + q.y);
+  }
+  __device__ __forceinline__ void square(float r[2]) {
+    if (!mats) {
+      rng.square(r);
+      return;
+    }
+    const uint32_t base = q.w & 0xffffu;
+    r[0] = fixed01(sobol_mult(q.x, mats + 32u * base) + q.y);
+    r[1] = fixed01(sobol_mult(q.x, mats + 32u * (base + 1u)) + q.z);
+  }
+  __device__ __forceinline__ int uniform_int(int a, int b_inclusive) { return rng.uniform_int(a, b_inclusive); }
+};
+
+// Rotation of a pixel in 32-bit fixed point.
+__device__ __forceinline__ uint32_t rotation_fixed(float r) { return (uint32_t)fminf(r * 4294967296.f, 4294967040.f); }
+
+// ----------------------------------------------------------------------------------------
 // Warps, sampler.cxx:6-124.
 __device__ __forceinline__ float3 to_uniform_sphere(const float r[2]) {
   float z = 1.f - 2.f * r[1];
@@ -393,7 +438,8 @@ __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, con
 // SampleBSDF: DiffuseShader (shader.cxx:300-318), SpecularReflectiveShader (:345-366),
 // SpecularTransmissiveDielectricShader::SampleBsdfRegular (:401-473), MicrofacetShader
 // (:692-707).  Draw order matches the reference: square, then single uniforms.
-__device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float3 wi, const Surf& s, Rng& rng,
+template <class R>
+__device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float3 wi, const Surf& s, R& rng,
                                                      Lambda l, float min_rough = 0.f) {
   ScatterSample out;
   out.delta = false;
@@ -607,7 +653,8 @@ struct DirSample {
   bool delta;
 };
 
-__device__ __forceinline__ DirSample env_sample_one(const DevEnvLight& L, Rng& rng, Lambda l) {
+template <class R>
+__device__ __forceinline__ DirSample env_sample_one(const DevEnvLight& L, R& rng, Lambda l) {
   DirSample s;
   s.delta = false;
   float r[2];
@@ -670,7 +717,8 @@ __device__ __forceinline__ float pixel_pdf_wrt_solid_angle(const DevCamera& c, f
   return 1.f / area * (l * l / fabsf(vz + kEps));
 }
 
-__device__ __forceinline__ DirSample camera_sample(const DevCamera& c, int unit, Rng& rng) {
+template <class R>
+__device__ __forceinline__ DirSample camera_sample(const DevCamera& c, int unit, R& rng) {
   DirSample s;
   const int py = unit / c.xres, px = unit - py * c.xres;
   float r[2];
@@ -745,7 +793,8 @@ __device__ __forceinline__ float phase_eval(int kind, float g, float3 wi, float3
 // Henyey-Greenstein uses its textbook inversion with a series for |g| <= 1e-3.
 // Directions are laid out as (sin(2 pi r1) rho, cos(2 pi r1) rho, mu) in the frame whose
 // z axis is the direction of travel.
-__device__ __forceinline__ float3 phase_sample(int kind, float g, float3 wi, Rng& rng, float* pdf) {
+template <class R>
+__device__ __forceinline__ float3 phase_sample(int kind, float g, float3 wi, R& rng, float* pdf) {
   float r[2];
   rng.square(r);
   if (kind == TT_PHASE_UNIFORM) {
@@ -1129,7 +1178,8 @@ __device__ __forceinline__ float3 medium_phase_eval(const DevMedium& m, float3 p
   return c.w0 * p0 + c.w1 * p1;
 }
 
-__device__ __forceinline__ float3 medium_phase_sample(const DevMedium& m, float3 pos, float3 wi, Rng& rng, Lambda l,
+template <class R>
+__device__ __forceinline__ float3 medium_phase_sample(const DevMedium& m, float3 pos, float3 wi, R& rng, Lambda l,
                                                       float3* value, float* pdf) {
   if (m.kind != TT_MEDIUM_ATMOSPHERE) {
     const float3 d = phase_sample(m.phase, m.g, wi, rng, pdf);

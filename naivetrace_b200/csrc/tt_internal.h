@@ -20,6 +20,8 @@ constexpr uint32_t ERR_CROSSINGS = 4u;  // a ray crossed more medium boundaries 
 constexpr int kMaxCrossings = 256;      // boundary crossings followed along one ray
 constexpr int kMaxMedia = 254;          // medium indices are stored in bytes (0xff = empty)
 constexpr int kCountersPerBounce = 4;  // ext, shadow, done, guided queue lengths
+constexpr int kSobolDims = 4096;       // quasi-random dimensions: subsequence ids < 64, 64 each
+constexpr int kRotationBlock = 128;    // per-pixel rotations repeat every 128 pixels in x and y
 
 // One training record of the learned guide: a guided surface vertex (position normalised to
 // the scene box, shading normal, outgoing direction), the sampled incident direction, the
@@ -133,6 +135,10 @@ struct DevScene {
   float box_lo[3];            // scene box, for the position encoding
   float box_inv[3];           // 1 / extent per axis
   int algo;                   // TT_ALGO_PT or TT_ALGO_PT2 (tt_pt2.cuh)
+  // Quasi-random sampling (pt2 with qmc): Sobol generator matrices, 32 words per dimension
+  // (TT_SOBOL_DIMS dimensions), and the per-pixel rotations [128 * 128][2]; null otherwise.
+  const uint32_t* sobol;
+  const float* rotations;
 };
 
 // Wavefront path state, structure of arrays, capacity `cap` paths.
@@ -176,6 +182,9 @@ struct PathState {
   float* rough;        // path roughness: largest microfacet alpha met so far
   float* wt2;          // media scenes: weights_track, 9 floats per path (row-major 3 x 3)
   float* sh_wt;        // media scenes: the path's weights_track at the shadow ray's vertex
+  uint4* qmc;          // quasi-random state: point index, rotations (32-bit fixed point),
+                       // subsequence (dimension offset | draw counter << 16)
+  uint4* sh_qmc;       // media scenes: the same at the shadow ray's connection
 };
 
 struct Framebuffer {

@@ -742,21 +742,26 @@ __device__ __forceinline__ void emit_shadow(const DevScene& sc, const PathState&
 // One camera sample: wavelength selection, next-event estimation at the camera vertex
 // (splatted to the pixel the light sample projects to, scaled by splat_scale), camera ray.
 // `slot` is the path's slot, `pixel` its index in the framebuffer, `unit` the pixel within
-// the camera; the random stream is (seed, path_id).
+// the camera, `sample` the sample's index in its pixel (the quasi-random point index); the
+// random stream is (seed, path_id).
 template <bool MEDIA>
 __device__ __forceinline__ void generate_one(const DevScene& sc, const PathState& p, int slot, int pixel, int unit,
                                              unsigned long long seed, unsigned long long path_id,
-                                             const DevCamera& cam, uint2 cam_track, float splat_scale,
-                                             int splat_base) {
+                                             unsigned long long sample, const DevCamera& cam, uint2 cam_track,
+                                             float splat_scale, int splat_base) {
   const int i = slot;
-  Rng rng;
+  Smp2 smp;
+  Rng& rng = smp.rng;
   rng.seed_path(seed, path_id);
+  smp.mats = sc.sobol;
   // LambdaSelectionStrategy::WithWeights (shader_util.hxx:83-91).
   const int main_idx = rng.uniform_int(0, 11);
   int idx[3] = {main_idx, main_idx + 12, main_idx + 24};
   const int rot = rng.uniform_int(0, 2);
   { const int t = idx[0]; idx[0] = idx[rot]; idx[rot] = t; }
-  rng.uniform(); rng.uniform(); rng.uniform();  // SampleWavelengthStrata
+  // SampleWavelengthStrata: its values are not used; quasi-random draws leave the PCG32
+  // stream untouched.
+  if (!smp.mats) { rng.uniform(); rng.uniform(); rng.uniform(); }
   const Lambda l{idx[0], idx[1], idx[2]};
   const float3 beta = f3(12.f, 12.f, 12.f);
   const float3 cam_pos = f3(cam.pos[0], cam.pos[1], cam.pos[2]);
@@ -787,8 +792,19 @@ __device__ __forceinline__ void generate_one(const DevScene& sc, const PathState
         emit_shadow<MEDIA>(sc, p, 0, i, c, L, beta, splat_scale, splat_base + c.unit, cam_mt, rng);
     }
   }
-  // Camera ray (TakeRandomWalkStep from the camera node).
-  DirSample s = camera_sample(cam, unit, rng);
+  // Camera ray (TakeRandomWalkStep from the camera node; pt2: subsequence 2, node count 1).
+  DirSample s;
+  if (smp.mats) {
+    const int py = unit / cam.xres, px = unit - py * cam.xres;
+    const int r = (px % kRotationBlock) + (py % kRotationBlock) * kRotationBlock;
+    smp.q = make_uint4((uint32_t)sample, rotation_fixed(__ldg(&sc.rotations[2 * r])),
+                       rotation_fixed(__ldg(&sc.rotations[2 * r + 1])), 0u);
+    smp.prep(2u);
+    s = camera_sample(cam, unit, smp);
+    p.qmc[i] = smp.q;
+  } else {
+    s = camera_sample(cam, unit, rng);
+  }
   const float3 bf = s.value * (1.f / s.pdf);
   // meta.z: node count; meta.w bit 0: last scatter was a delta (pt2: bit 1 = has one).
   p.meta[i] = make_uint4((unsigned)pixel, pack_lambda(l), pt2 ? 2u : 1u, pt2 ? 0u : (s.delta ? 1u : 0u));
@@ -816,7 +832,7 @@ __global__ void __launch_bounds__(256) k_generate(DevScene sc, PathState p, Fram
     const unsigned long long sample = w.sample_offset + (unsigned long long)(g / w.npix_range);
     const int pixel = w.pixel_begin + pix_local;
     generate_one<MEDIA>(sc, p, i, pixel, pixel, w.seed, sample * (unsigned long long)w.npix_total + (unsigned long long)pixel,
-                        sc.cam, sc.cam_track, 1.f / (float)w.npix_total, 0);
+                        sample, sc.cam, sc.cam_track, 1.f / (float)w.npix_total, 0);
   }
 }
 
@@ -850,7 +866,7 @@ __global__ void __launch_bounds__(256) k_generate_views(DevScene sc, PathState p
     const int pix = (int)(li % V.npix);
     const unsigned long long sample = (unsigned long long)(li / V.npix);
     generate_one<MEDIA>(sc, p, i, V.pix_begin + pix, pix, V.seed, sample * (unsigned long long)V.npix + (unsigned long long)pix,
-                        V.cam, V.cam_track, 1.f / (float)V.npix, V.pix_begin);
+                        sample, V.cam, V.cam_track, 1.f / (float)V.npix, V.pix_begin);
   }
 }
 

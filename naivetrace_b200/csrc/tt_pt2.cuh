@@ -90,8 +90,9 @@ __device__ __forceinline__ float3 exp_maj(float3 maj, float x) {
 
 // nullpath::Tracking on one segment: hero-wavelength delta tracking.  Returns true at a
 // real collision, at distance *t_out.  At most 10^4 steps (then no collision).
+template <class R>
 __device__ __forceinline__ bool track_segment2(const DevScene& sc, int medium, float3 org, float3 dir, float len,
-                                               M33f& ft, M33f& fn, Rng& rng, Lambda l, float* t_out) {
+                                               M33f& ft, M33f& fn, R& rng, Lambda l, float* t_out) {
   const float3 maj = majorant2(sc, medium, org, dir, len, l);
   const float mfp = 1.f / maj.x;
   float t = 0.f;
@@ -123,8 +124,9 @@ __device__ __forceinline__ bool track_segment2(const DevScene& sc, int medium, f
 
 // nullpath::Transmission on one segment: every collision is a null collision.  Stops once
 // every diagonal entry of the null matrix exceeds LargeNumber (the estimate is zero).
+template <class R>
 __device__ __forceinline__ void transmit_segment2(const DevScene& sc, int medium, float3 org, float3 dir, float len,
-                                                  M33f& ft, M33f& fn, Rng& rng, Lambda l) {
+                                                  M33f& ft, M33f& fn, R& rng, Lambda l) {
   const float3 maj = majorant2(sc, medium, org, dir, len, l);
   const float mfp = 1.f / maj.x;
   M33f st_, sn_;
@@ -173,7 +175,7 @@ __device__ __forceinline__ float3 mis2(const DevScene& sc, float3 x, bool has_pd
 // eye.  The light pdf returned for MIS is the light's own density (solid angle), without
 // the selection probability, as in the reference.  `s` is null at a volume vertex.
 template <bool MEDIA>
-__device__ __forceinline__ void nee2(const DevScene& sc, const PathState& p, int qbounce, int slot, Rng& rng, Lambda l,
+__device__ __forceinline__ void nee2(const DevScene& sc, const PathState& p, int qbounce, int slot, Smp2& rng, Lambda l,
                                      float3 beta, float3 wi, const Surf* s, float rough, int vmed, float3 vpos,
                                      const MTracker& mt, const M33f& wt) {
   const int which = tower_sampling4(sc.type_probs, rng.uniform());
@@ -278,9 +280,10 @@ __device__ __forceinline__ void nee2(const DevScene& sc, const PathState& p, int
   const bool mis_on = !delta && sc.sample_bsdf && sc.sample_lights;
   float3 contrib = pre;
   if (MEDIA) {
-    p.sh_med[slot] = make_float4(mis_on ? pdf : -1.f, bsdf_pdf, __uint_as_float((unsigned)(rng.state & 0xffffffffu)),
-                                 __uint_as_float((unsigned)(rng.state >> 32)));
+    p.sh_med[slot] = make_float4(mis_on ? pdf : -1.f, bsdf_pdf, __uint_as_float((unsigned)(rng.rng.state & 0xffffffffu)),
+                                 __uint_as_float((unsigned)(rng.rng.state >> 32)));
     p.sh_track[slot] = store_tracker(smt);
+    if (rng.mats) p.sh_qmc[slot] = rng.q;
 #pragma unroll
     for (int k = 0; k < 9; ++k) p.sh_wt[9 * (size_t)slot + k] = wt.a[k];
   } else {
@@ -313,7 +316,10 @@ __global__ void __launch_bounds__(256) k_shade2(DevScene sc, PathState p, int bo
     const bool has_last = (meta.w & 2u) != 0u, last_delta = (meta.w & 1u) != 0u;
     const float last_pdf = b4.w;
     float3 acc = xyz(p.accum[slot]);
-    Rng rng{p.rng_state[slot], p.rng_inc[slot]};
+    Smp2 rng;
+    rng.rng = Rng{p.rng_state[slot], p.rng_inc[slot]};
+    rng.mats = sc.sobol;
+    if (sc.sobol) rng.q = p.qmc[slot];
     const int tri = __float_as_int(h.w);
     bool done = false;
     M33f wt, wtn;
@@ -364,6 +370,8 @@ __global__ void __launch_bounds__(256) k_shade2(DevScene sc, PathState p, int bo
       m33_ones(wtn);
       rng.uniform();  // the vacuum segment's free-flight sample
     }
+    const int count0 = (int)meta.z;  // node count of this vertex
+    rng.prep(((unsigned)count0 << 1) | 1u);
     const float rough = p.rough[slot];
     Surf s;
     if (!done && !volume && tri < 0) {
@@ -401,8 +409,9 @@ __global__ void __launch_bounds__(256) k_shade2(DevScene sc, PathState p, int bo
     } else if (!done) {
       if (sc.sample_lights) nee2<MEDIA>(sc, p, bounce + 1, slot, rng, l, beta, wi, nullptr, rough, vmed, vpos, mt, wt);
     }
-    const int count = (int)meta.z + 1;
+    const int count = count0 + 1;
     if (!done && count > sc.max_path_nodes - 1) done = true;
+    rng.prep((unsigned)count0 << 1);
     if (!done) {
       float3 ndir, bf, norg;
       float pdf;
@@ -447,7 +456,8 @@ __global__ void __launch_bounds__(256) k_shade2(DevScene sc, PathState p, int bo
       }
     }
     p.accum[slot] = make_float4(acc.x, acc.y, acc.z, 0.f);
-    p.rng_state[slot] = rng.state;
+    p.rng_state[slot] = rng.rng.state;
+    if (sc.sobol) p.qmc[slot] = rng.q;
     if (done) {
       const int qd = warp_append(done_count(p, bounce + 1));
       p.done_q[qd] = slot;
@@ -473,8 +483,10 @@ __global__ void __launch_bounds__(256) k_shadow2(DevScene sc, PathState p, int b
     const Lambda l = unpack_lambda(p.meta[slot].y);
     MTracker mt = load_tracker(p.sh_track[slot]);
     const float4 med = p.sh_med[slot];
-    Rng srng;
-    srng.seed_path(((unsigned long long)__float_as_uint(med.w) << 32) | __float_as_uint(med.z), p.rng_inc[slot]);
+    Smp2 srng;
+    srng.rng.seed_path(((unsigned long long)__float_as_uint(med.w) << 32) | __float_as_uint(med.z), p.rng_inc[slot]);
+    srng.mats = sc.sobol;
+    if (sc.sobol) srng.q = p.sh_qmc[slot];
     M33f ft, fn;
     m33_ones(ft);
     m33_ones(fn);

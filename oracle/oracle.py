@@ -64,6 +64,9 @@ def load():
         "or_medium_phase_sample": ([vp, C.c_int, d, d, i32, C.c_int, C.c_uint64, d, d, d], C.c_int),
         "or_track": ([vp, d, d, i32, C.c_int, C.c_uint64, d], C.c_int),
         "or_phase_sample": ([C.c_int, C.c_double, d, C.c_int, C.c_uint64, d, d, d], C.c_int),
+        "or_sobol": ([C.c_int, C.c_int, P(C.c_uint32), d], C.c_int),
+        "or_sobol_matrix": ([C.c_int, C.c_int, P(C.c_uint16), P(C.c_uint32)], None),
+        "or_qmc_draws": ([C.c_int, C.c_int, C.c_uint32, C.c_int, i32, C.c_uint64, d], C.c_int),
     }
     for name, (a, r) in sig.items():
         fn = getattr(lib, name)

@@ -12,6 +12,7 @@
 // order.  The CUDA tracer uses the same streams, which makes per-path comparison possible.
 #include "tt_oracle.h"
 #include "../naivetrace_b200/csrc/tt_tables.h"
+#include "../naivetrace_b200/csrc/tt_sobol_data.h"
 
 #include <algorithm>
 #include <atomic>
@@ -20,6 +21,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -139,11 +141,40 @@ inline void SeedPath(Pcg32& g, uint64_t seed, uint64_t path) {
   g.Seed(s1, s2);
 }
 
+// SobolMatrixMult (sampler.cxx:224-234): the point index's bits select generator columns.
+inline double SobolMult(uint32_t point, const uint32_t* m) {
+  uint32_t c = 0;
+  for (int i = 0; i < 32; ++i, point >>= 1) c ^= (point & 1u) ? m[i] : 0u;
+  return (double)c / 4294967296.0;
+}
+
 // One stream per path; Uniform01 / UniformUnitSquare / UniformInt as Sampler and RandGen.
+// With `qmc` set it is QuasiRandomSequence (sampler.cxx:254-331): point index, per-pixel
+// rotation, subsequence (SetSubsequenceId: dimension offset id << 6, draw counter); the
+// k-th 1D draw is dimension offset + 2 + k for k < 62, then PCG32; 2D draws are dimensions
+// offset and offset + 1; every draw is rotated modulo 1.  UniformInt is always PCG32.
 struct Sampler {
   Pcg32 g;
-  double Uniform01() { return g.NextDouble(); }
-  void UniformUnitSquare(double r[2]) { r[0] = g.NextDouble(); r[1] = g.NextDouble(); }
+  const uint32_t* qmc = nullptr;  // generator matrices, 32 columns per dimension
+  uint32_t point = 0, offset = 0, sub = 0;
+  double rot[2] = {0., 0.};
+  void SetSubsequenceId(uint32_t id) { offset = id << 6; sub = 0; }
+  static double Wrap(double x) { return x >= 1. ? x - 1. : x; }
+  double Uniform01() {
+    if (!qmc) return g.NextDouble();
+    const double x = sub < 62 ? SobolMult(point, qmc + 32 * (size_t)(offset + 2 + sub)) : g.NextDouble();
+    ++sub;
+    return Wrap(x + rot[0]);
+  }
+  void UniformUnitSquare(double r[2]) {
+    if (!qmc) {
+      r[0] = g.NextDouble();
+      r[1] = g.NextDouble();
+      return;
+    }
+    r[0] = Wrap(SobolMult(point, qmc + 32 * (size_t)offset) + rot[0]);
+    r[1] = Wrap(SobolMult(point, qmc + 32 * (size_t)(offset + 1)) + rot[1]);
+  }
   int UniformInt(int a, int b_inclusive) {  // RandGen::UniformInt, sampler.cxx:384-391
     return a + (int)g.NextBounded((uint32_t)(b_inclusive + 1 - a));
   }
@@ -420,6 +451,7 @@ struct MediumDesc {
 };
 
 struct Scene {
+  std::vector<uint32_t> sobol;     // quasi-random generator matrices (pt2 with qmc), else empty
   // Primitives: triangles 0 .. ntri-1, then spheres (global id ntri + i).
   uint32_t ntri = 0;
   std::vector<V3> sph_c;           // sphere centres (from float)
@@ -2318,8 +2350,9 @@ struct Worker2 {
       Coeffs(vol_medium, pos, &ss, &st);
       pw = pw * Div(ss, st + S3(Eps));
     }
-    // nullpath::Transmission (:384-420) on a stream seeded from the path's state here.
-    Sampler shadow;
+    // nullpath::Transmission (:384-420) on a stream seeded from the path's state here; a
+    // quasi-random sampler continues the subsequence of the light sample.
+    Sampler shadow = smp;
     SeedPath(shadow.g, smp.g.state, smp.g.inc);
     Factors f;
     const double slen = len * 0.9999;
@@ -2357,6 +2390,7 @@ struct Worker2 {
     std::swap(idx[0], idx[rotation]);
     for (int i = 0; i < 3; ++i) smp.Uniform01();
     std::memcpy(ctx.idx, idx, sizeof(idx));
+    smp.SetSubsequenceId(2);  // PrepSamplerDimension at node count 1 (the camera direction)
     State ps;
     ps.wt = M33::Ones();
     ps.wtn = M33::Ones();
@@ -2424,6 +2458,7 @@ struct Worker2 {
       if (!volume) {
         si = SurfaceFromHit(sc, prim, u, v, ps.org, ps.dir, t);
         const tt_material& m = sc.materials[sc.mat_of_tri[prim]].m;
+        smp.SetSubsequenceId(((uint32_t)ps.count << 1) | 1u);  // PrepSamplerDimension(NEE_LIGHT)
         // MaybeAddEmission (:592-622).
         if (use_emission && m.emissive) {
           const double vis = Dot(si.geometry_normal, -ps.dir) > 0. ? 1. : 0.;
@@ -2440,11 +2475,14 @@ struct Worker2 {
           total = total + Div(rad * ps.path_weights * mw.first, mw.second);
         }
         if (use_nee) total = total + DirectLighting(ps, &si, si.pos, -1);
+        smp.SetSubsequenceId((uint32_t)ps.count << 1);  // PrepSamplerDimension(BSDF)
         // SampleScatterer (:571-583): the query sees the roughness before this vertex.
         s = SampleBSDF(m, -ps.dir, si, smp, ctx.idx, ps.roughness);
         ps.roughness = std::max(MyRoughness(m), ps.roughness);
       } else {
+        smp.SetSubsequenceId(((uint32_t)ps.count << 1) | 1u);
         if (use_nee) total = total + DirectLighting(ps, nullptr, vpos, vmed);
+        smp.SetSubsequenceId((uint32_t)ps.count << 1);
         s = MediumPhaseSample(sc.media[vmed], vpos, -ps.dir, smp, ctx.idx);
         S3 ss, st;
         Coeffs(vmed, vpos, &ss, &st);
@@ -2474,10 +2512,44 @@ struct Worker2 {
 };
 
 // ---------------------------------------------------------------------------------------
+// Generator matrix of one Sobol dimension as the reference's generator notebook builds it
+// (misc/SobolSequenceGeneratorMatrices.ipynb, MakeTheMatrix): the s initial direction
+// numbers, then for k >= s m_k = m_{k-s} ^ 2^s m_{k-s} ^ the terms 2^(s-1-i) m_{k-s+i+1}
+// for which bit (s - 2 - i) of a is set; finally column k is m_k shifted left by 31 - k.
+static void SobolMatrix(int s, int a, const uint16_t* m_init, uint32_t* C) {
+  uint64_t m[32];
+  for (int k = 0; k < 32; ++k) {
+    if (k < s) { m[k] = m_init[k]; continue; }
+    uint64_t pow2 = 1ull << s;
+    m[k] = m[k - s] ^ (pow2 * m[k - s]);
+    for (int i = 0; i < s - 1; ++i) {
+      pow2 >>= 1;
+      if (a & (1 << (s - 2 - i))) m[k] ^= pow2 * m[k - s + i + 1];
+    }
+  }
+  for (int k = 0; k < 32; ++k) C[k] = (uint32_t)(m[k] << (31 - k));
+}
+
+// All dimensions: 0 is MakeIdentityGenerator, d >= 1 the Joe-Kuo line d + 1.
+static void SobolMatrices(std::vector<uint32_t>& C) {
+  C.assign((size_t)TT_SOBOL_DIMS * 32, 0u);
+  for (int k = 0; k < 32; ++k) C[k] = 1u << (31 - k);
+  const uint16_t* q = tt_sobol_sam;
+  for (int d = 1; d < TT_SOBOL_DIMS; ++d) {
+    const int s = q[0], a = q[1];
+    SobolMatrix(s, a, q + 2, &C[32 * (size_t)d]);
+    q += 2 + s;
+  }
+}
+
 static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
   if (!d || !p) { g_err = "null argument"; return false; }
   s.params = *p;
   if (s.params.max_ray_depth <= 0) s.params.max_ray_depth = 25;
+  if (s.params.algo == TT_ALGO_PT2 && s.params.qmc) {
+    if (s.params.max_ray_depth > 31) { g_err = "qmc needs max_ray_depth <= 31"; return false; }
+    SobolMatrices(s.sobol);
+  }
   s.vert.resize(d->num_vertices);
   for (uint32_t i = 0; i < d->num_vertices; ++i)
     s.vert[i] = {d->vertices[3 * i], d->vertices[3 * i + 1], d->vertices[3 * i + 2]};
@@ -2763,6 +2835,17 @@ int or_render(or_scene* os, int spp, uint64_t seed, int sample_offset, int pixel
           double rgb[3];
           if (pt2) {
             SeedPath(w2.smp.g, seed, sample * (uint64_t)npix + (uint64_t)p);
+            if (!sc.sobol.empty()) {
+              // SetPixelIndex / SetPointNum (renderingalgorithms_pathtracing2.cxx:345-352).
+              const int px = p % sc.cam.xres, py = p / sc.cam.xres;
+              const int r = (px % TT_ROTATION_BLOCK) + (py % TT_ROTATION_BLOCK) * TT_ROTATION_BLOCK;
+              w2.smp.qmc = sc.sobol.data();
+              w2.smp.point = (uint32_t)sample;
+              w2.smp.rot[0] = tt_rotation_offsets[2 * r];
+              w2.smp.rot[1] = tt_rotation_offsets[2 * r + 1];
+              w2.smp.offset = 0;
+              w2.smp.sub = 0;
+            }
             w2.RenderPixel(p, rgb);
           } else {
             SeedPath(w.smp.g, seed, sample * (uint64_t)npix + (uint64_t)p);
@@ -3032,6 +3115,43 @@ int or_scene_info(or_scene* s, double* bbox6, int32_t* counts4) {
   counts4[1] = (int32_t)s->s.area_lights.size();
   counts4[2] = (int32_t)s->s.env.size();
   counts4[3] = (int32_t)s->s.surf.nodes.size();
+  return 0;
+}
+
+int or_sobol(int dim, int n, const uint32_t* points, double* out) {
+  static std::vector<uint32_t> mats;
+  static std::once_flag once;
+  std::call_once(once, [] { SobolMatrices(mats); });
+  if (dim < 0 || dim >= TT_SOBOL_DIMS) { g_err = "dimension out of range"; return 2; }
+  for (int i = 0; i < n; ++i) out[i] = SobolMult(points[i], &mats[32 * (size_t)dim]);
+  return 0;
+}
+
+void or_sobol_matrix(int s, int a, const uint16_t* m, uint32_t* out32) { SobolMatrix(s, a, m, out32); }
+
+int or_qmc_draws(int px, int py, uint32_t point, int n_ops, const int32_t* ops, uint64_t pcg_seed, double* out) {
+  static std::vector<uint32_t> mats;
+  static std::once_flag once;
+  std::call_once(once, [] { SobolMatrices(mats); });
+  Sampler smp;
+  SeedPath(smp.g, pcg_seed, 0);
+  const int r = (px % TT_ROTATION_BLOCK) + (py % TT_ROTATION_BLOCK) * TT_ROTATION_BLOCK;
+  smp.qmc = mats.data();
+  smp.point = point;
+  smp.rot[0] = tt_rotation_offsets[2 * r];
+  smp.rot[1] = tt_rotation_offsets[2 * r + 1];
+  int k = 0;
+  for (int i = 0; i < n_ops; ++i) {
+    if (ops[i] == 0) {
+      out[k++] = smp.Uniform01();
+    } else if (ops[i] == 1) {
+      smp.UniformUnitSquare(out + k);
+      k += 2;
+    } else {
+      if (ops[i] - 2 >= 64) { g_err = "subsequence id out of range"; return 2; }
+      smp.SetSubsequenceId((uint32_t)(ops[i] - 2));
+    }
+  }
   return 0;
 }
 

@@ -77,6 +77,13 @@ int or_medium_phase_sample(or_scene* s, int medium, const double* pos3, const do
                            uint64_t seed, double* dirs, double* value3, double* pdf);
 int or_phase_sample(int kind, double g, const double* wi3, int n, uint64_t seed, double* dirs, double* pdf,
                     double* value);
+/* Quasi-random sampler: SobolSequence(point, dim) for n points (dim < 4096); the generator
+ * matrix (32 columns) for given Joe-Kuo parameters; and the draws of QuasiRandomSequence
+ * for a pixel and point: `ops` holds per draw 0 = Uniform01, 1 = UniformUnitSquare,
+ * 2 + id = SetSubsequenceId(id) (no output). */
+int or_sobol(int dim, int n, const uint32_t* points, double* out);
+void or_sobol_matrix(int s, int a, const uint16_t* m, uint32_t* out32);
+int or_qmc_draws(int px, int py, uint32_t point, int n_ops, const int32_t* ops, uint64_t pcg_seed, double* out);
 
 #ifdef __cplusplus
 }

@@ -11,7 +11,8 @@
 2. Statistical parity: tile means of independent renders in a media scene (z-test).
 3. pt2 against pt on the GPU in BSDF-only mode (same vertices collect emission at depths
    D + 1 and D).
-4. The rest of the interface: multi-view batches, rejected combinations.
+4. Quasi-random sampling (qmc): per-path parity over two passes, lower error than PCG32.
+5. The rest of the interface: multi-view batches, rejected combinations.
 """
 import copy
 
@@ -106,9 +107,10 @@ def test_pt2_mis_matches_bsdf_with_one_light(gpu_lib):
     np.testing.assert_allclose(means[0], means[1], rtol=0.02)
 
 
-def test_pt2_views_match_single_passes(gpu_lib):
+@pytest.mark.parametrize("qmc", [False, True])
+def test_pt2_views_match_single_passes(gpu_lib, qmc):
     scene = scenes.cornell_box_medium(16, 16)
-    params = make_params(max_ray_depth=8, wave_paths=500, algo=abi.ALGO_PT2)
+    params = make_params(max_ray_depth=8, wave_paths=500, algo=abi.ALGO_PT2, qmc=qmc)
     c = scene.camera
     views = [(c, 3), (copy.copy(c), 2)]
     views[1][0].xres, views[1][0].yres = 20, 12
@@ -117,7 +119,7 @@ def test_pt2_views_match_single_passes(gpu_lib):
     for v, ((cam, spp), img) in enumerate(zip(views, imgs)):
         s = copy.copy(scene)
         s.camera = cam
-        one = GpuContext(s, make_params(max_ray_depth=8, algo=abi.ALGO_PT2))
+        one = GpuContext(s, make_params(max_ray_depth=8, algo=abi.ALGO_PT2, qmc=qmc))
         one.render(spp, 4 + v)
         ref = one.framebuffer().reshape(cam.yres, cam.xres, 3)
         np.testing.assert_allclose(img, ref, rtol=1e-4, atol=1e-5 * max(np.abs(ref).mean(), 1e-6))
@@ -140,3 +142,44 @@ def test_pt2_rendering_algo(gpu_lib):
     acc, light, spp, _ = algo.ctx.accumulators()
     assert np.all(spp == 4) and np.all(light == 0)
     assert algo.generate_image().shape == (16, 16, 3)
+
+
+@pytest.mark.parametrize("name", ["cornell_box_materials", "terrain_spheres_small", "cornell_box_media_mix"])
+def test_pt2_qmc_per_path_parity(gpu_lib, name):
+    """Quasi-random points (Sobol with per-pixel rotations) on both sides, over two passes so
+    that the second pass's point indices continue after the first's."""
+    scene = getattr(scenes, name)(32, 32) if name != "terrain_spheres_small" else scenes.terrain_spheres_small(48, 27)
+    p = make_params(max_ray_depth=10, algo=abi.ALGO_PT2, qmc=True)
+    g = GpuContext(scene, p)
+    g.render(2, 3)
+    g.render(2, 3)
+    ag = g.accumulators()[0].reshape(-1, 3)
+    o = OracleScene(scene, p)
+    a0, _, _ = o.render(2, seed=3, sample_offset=0)
+    a1, _, _ = o.render(2, seed=3, sample_offset=2)
+    ao = (a0 + a1).reshape(-1, 3)
+    assert g.stats()["error_flags"] == 0
+    scale = max(np.abs(ao).mean(), 1e-6)
+    close = np.all(np.abs(ag - ao) <= 1e-3 * np.abs(ao) + 1e-3 * scale, axis=1)
+    assert close.mean() >= 0.93, close.mean()
+    np.testing.assert_allclose(ag[close].sum(axis=0), ao[close].sum(axis=0), rtol=1e-3)
+
+
+def test_pt2_qmc_lowers_error(gpu_lib):
+    xres = yres = 32
+    scene = scenes.cornell_box(xres, yres)
+    ref = GpuContext(scene, make_params(max_ray_depth=3, algo=abi.ALGO_PT2))
+    ref.render(16384, seed=77)
+    R = ref.framebuffer().astype(np.float64)
+    errs = {}
+    for qmc in (False, True):
+        e = []
+        for k in range(3):
+            g = GpuContext(scene, make_params(max_ray_depth=3, algo=abi.ALGO_PT2, qmc=qmc))
+            g.render(64, seed=10 + k)
+            I = g.framebuffer().astype(np.float64)
+            e.append(np.mean((I - R) ** 2 / (R * R + 1e-2)))
+        errs[qmc] = np.mean(e)
+    assert errs[True] < 0.85 * errs[False], errs
+    with pytest.raises(abi.TTError):
+        GpuContext(scene, make_params(max_ray_depth=40, algo=abi.ALGO_PT2, qmc=True))
