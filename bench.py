@@ -295,6 +295,40 @@ def multiview_comparison(g, n_views=96, seed=4):
     }
 
 
+def pt2_comparison(scene, spp, depth, device):
+    """The null-path tracer (--algo pt2) on the bench workload, with pseudo-random and with
+    quasi-random (Sobol) sampling: one untimed 4-spp pass, then one timed frame each (CUDA
+    events around the render call)."""
+    import torch
+    from naivetrace_b200 import abi
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    out = {"workload": "the bench frame rendered by pt2 (no Russian roulette: every path runs to the depth cap "
+                       "unless it escapes or its weight vanishes)"}
+    paths = scene.camera.xres * scene.camera.yres * spp
+    for qmc in (False, True):
+        g = GpuContext(scene, make_params(max_ray_depth=depth, device=device, algo=abi.ALGO_PT2, qmc=qmc))
+        g.render(4, 1)
+        g.clear()
+        g.reset_stats()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        g.render(spp, 2)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        st = g.stats()
+        out["qmc" if qmc else "pcg"] = {
+            "ms": ms, "mpaths_per_s": paths / (ms * 1e-3) / 1e6,
+            "mrays_per_s": (st["extension_rays"] + st["shadow_rays"]) / (ms * 1e-3) / 1e6,
+            "rays_per_path": (st["extension_rays"] + st["shadow_rays"]) / paths,
+            "error_flags": st["error_flags"]}
+        g.close()
+    return out
+
+
 def run_reference_arm(args):
     from naivetrace_b200 import dist as nd
     r = nd.init_from_env()
@@ -457,6 +491,9 @@ def run_ours(args):
     multiview = None
     if rank == 0 and world == 1 and not args.no_multiview and not args.small:
         multiview = multiview_comparison(g)
+    pt2 = None
+    if rank == 0 and world == 1 and not args.no_pt2:
+        pt2 = pt2_comparison(scene, spp, depth, device)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -501,6 +538,7 @@ def run_ours(args):
                             "tt_read_framebuffer + tt_destroy"},
             "guiding": guiding,
             "multiview": multiview,
+            "pt2": pt2,
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": clk,
             "stats": {k: st[k] for k in ("extension_rays", "shadow_rays", "extend_launches", "extend_ms",
@@ -516,8 +554,10 @@ def run_ours(args):
 def profile_run(args):
     from naivetrace_b200.algo import GpuContext
     from naivetrace_b200.scene import make_params
+    from naivetrace_b200 import abi
     scene, spp, depth, name = workload(args)
-    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave))
+    algo = abi.ALGO_PT2 if args.algo == "pt2" else abi.ALGO_PT
+    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave, algo=algo))
     g.render(spp, 1)
     st = g.stats()
     q = g.queue_lengths(depth + 1)
@@ -526,6 +566,24 @@ def profile_run(args):
                       "last_wave_extension_rays_per_bounce": q[:, 0].tolist(),
                       "last_wave_shadow_rays_per_bounce": q[:, 1].tolist(),
                       "error_flags": st["error_flags"]}))
+    g.close()
+    return 0 if st["error_flags"] == 0 else 1
+
+
+def profile_views(args):
+    """No timing: 24 seeded views (sides 128-256, 4-16 spp) of the scaled-down terrain scene
+    in one batch (first wave eager, later waves replayed from the captured graph)."""
+    from naivetrace_b200 import scenes
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    args.small = True
+    scene, _, depth, _ = workload(args)
+    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=1 << 20))
+    views = scenes.terrain_views(24, seed=4, spp_range=(4, 16), resolutions=(128, 256))
+    imgs = g.render_views(views, seed=1)
+    st = g.stats()
+    print(json.dumps({"profile_views": len(views), "paths": sum(c.xres * c.yres * s for c, s in views),
+                      "finite": bool(all(np.isfinite(i).all() for i in imgs)), "error_flags": st["error_flags"]}))
     g.close()
     return 0 if st["error_flags"] == 0 else 1
 
@@ -563,6 +621,10 @@ def main(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")
     ap.add_argument("--no-multiview", action="store_true", help="skip the multi-view batch comparison")
+    ap.add_argument("--no-pt2", action="store_true", help="skip the null-path tracer (pt2) frames")
+    ap.add_argument("--algo", choices=["pt", "pt2"], default="pt", help="tracer of --profile-run")
+    ap.add_argument("--profile-views", action="store_true",
+                    help="no timing: a batch of 24 small views of the scaled-down scene (for ncu captures)")
     ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
     ap.add_argument("--profile-guiding", action="store_true",
                     help="no timing: training and frozen passes of the guiding workload (for ncu captures)")
@@ -573,6 +635,8 @@ def main(argv=None):
         return profile_run(args)
     if args.profile_guiding:
         return profile_guiding(args)
+    if args.profile_views:
+        return profile_views(args)
     if args.warmup < 3 and not args.small:
         args.warmup = 3
     if args.impl == "reference":
