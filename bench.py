@@ -165,7 +165,7 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
     passes that train the network after each pass, then freezes it and doubles like plain.
     Every sample, training passes included, stays in the image (each is unbiased).  Reports
     the time to reach relMSE `target` and the relMSE of both at equal time."""
-    from naivetrace_b200 import scenes
+    from naivetrace_b200 import abi, scenes
     from naivetrace_b200.algo import GpuContext
     from naivetrace_b200.scene import make_params
     scene = scenes.guiding_room(xres, yres)
@@ -192,24 +192,28 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
     w.render(1, 2)
     w.close()
 
-    def run(guided):
+    def run(guided, tree=False):
         g = GpuContext(scene, p)
+        # The tree guider (the reference's kd-tree cells with fitted vMF mixtures), batch EM.
+        kw = dict(learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+        if tree:
+            kw.update(method=abi.GUIDE_TREE, tree_subdivision=200, tree_em_iters=4)
         # One untimed pass at the largest wave size allocates the path state (with the
-        # guiding arrays for the guided run); the network is not trained by it.
+        # guiding arrays for the guided run); the guide is not trained by it.
         if guided:
-            g.set_guiding(True, 0, max_depth=guide_depth, seed=7)
+            g.set_guiding(True, 0, **kw)
         g.render(8, 3)
         g.clear()
         g.reset_stats()
         pts, el, spp_total, seed = [], 0.0, 0, 10
         if guided:
-            g.set_guiding(True, 1, learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+            g.set_guiding(True, 1, **kw)
             for k in range(train_passes):
                 el += timed(g, 1, seed)
                 seed += 1
                 spp_total += 1
                 pts.append((el, spp_total, relmse(g)))
-            g.set_guiding(True, 0, learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+            g.set_guiding(True, 0, **kw)
         spp = 1
         while el < budget_ms and spp_total < 1 << 14:
             el += timed(g, spp, seed)
@@ -240,6 +244,7 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
 
     plain, _ = run(False)
     guided, gst = run(True)
+    tree, tst = run(True, tree=True)
     t_eq = min(plain[-1][0], guided[-1][0])
     tp, tg = time_to(plain, target), time_to(guided, target)
     ep, eg = at_time(plain, t_eq), at_time(guided, t_eq)
@@ -255,6 +260,16 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
         "guided_bounces": guide_depth,
         "training": {"passes": train_passes, "adam_steps": int(gst["guide_steps"]), "learning_rate": lr,
                      "records": int(gst["guide_records"]), "train_kernel_ms": gst["guide_train_ms"]},
+        "tree_guider": {
+            "what": "kd-tree cells (200 records per initial cell) with 8-lobe vMF mixtures, batch EM (4 "
+                    "iterations per round), the same schedule of training passes",
+            "time_to_target_ms": time_to(tree, target),
+            "relmse_at_equal_time": at_time(tree, min(t_eq, tree[-1][0])),
+            "gain_equal_time": ep / at_time(tree, t_eq) if tree[-1][0] >= t_eq else None,
+            "rounds": int(tst["guide_steps"]), "records": int(tst["guide_records"]),
+            "round_ms_total": tst["guide_train_ms"],
+            "curve": [[round(t, 2), s, round(e, 6)] for t, s, e in tree],
+        },
         "curve_plain": [[round(t, 2), s, round(e, 6)] for t, s, e in plain],
         "curve_guided": [[round(t, 2), s, round(e, 6)] for t, s, e in guided],
     }

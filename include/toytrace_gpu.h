@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 5
+#define TT_ABI_VERSION 6
 
 typedef int32_t tt_status;
 enum {
@@ -355,7 +355,16 @@ typedef struct tt_guiding_params {
   int32_t max_depth;            /* guide the vertices of the first max_depth bounces only, BSDF
                                    sampling beyond (0: every bounce) */
   uint64_t seed;                /* weight initialisation */
+  int32_t method;               /* TT_GUIDE_LEARNED (the network) or TT_GUIDE_TREE (the
+                                   reference's kd-tree cells with vMF mixtures, below) */
+  int32_t tree_subdivision;     /* TT_GUIDE_TREE: records per cell of the initial tree
+                                   (--guide-subdiv-factor, scene.hxx:39; 0: 100) */
+  int32_t tree_em_iters;        /* TT_GUIDE_TREE: 0 = the reference's incremental EM (a
+                                   maximisation step every 10 x prior strength records, each
+                                   on that chunk alone); k > 0 = k EM iterations per round over
+                                   all of the round's records of the cell */
 } tt_guiding_params;
+enum { TT_GUIDE_LEARNED = 0, TT_GUIDE_TREE = 1 };
 
 /* Enables or disables guiding.  The network is created (He-uniform weights from `seed`) on
  * first use and keeps its trained weights while guiding is switched off and on again. */
@@ -381,6 +390,32 @@ tt_status tt_guide_read_records(tt_ctx* ctx, float* out, int32_t max_records, in
 /* Feature encoding of n points (position in [0,1]^3, normal, outgoing direction: 9 floats
  * each) into n x 96 features, as the renderer computes them. */
 tt_status tt_guide_features_batch(tt_ctx* ctx, const float* points, int32_t n, float* features);
+
+/* Tree guider (method TT_GUIDE_TREE): the guided tracer's spatial cells (PathGuiding,
+ * path_guiding.cxx:347-813) with per-cell 8-lobe vMF mixtures (MoVmfRadianceDistribution,
+ * path_guiding.hxx:63-190) fitted by incremental EM with a prior
+ * (distribution_mixture_models.cxx:279-388), sampled against the BSDF with probability 0.5
+ * (renderingalgorithms_pathtracing_guided.cxx:470).  After each training pass the pass's
+ * records are fitted into the cells on the GPU (one warp per cell); the first round builds
+ * the kd-tree from the records, later rounds split cells that received too many.
+ * Cell and node counts, fitted rounds and records: */
+tt_status tt_guide_tree_info(tt_ctx* ctx, int32_t* cells, int32_t* nodes, int32_t* rounds, int64_t* records);
+/* Mixtures of the first max_cells cells, 40 floats each: weights[8], means[8][3],
+ * concentrations[8]. */
+tt_status tt_guide_tree_mixtures(tt_ctx* ctx, float* out, int32_t max_cells);
+/* Cells of n normalised positions (3 floats each) in the current tree. */
+tt_status tt_guide_tree_lookup_batch(tt_ctx* ctx, const float* points, int32_t n, int32_t* cells);
+/* The fit of one cell on the device, for tests: n records of 4 floats (direction xyz,
+ * weight) in the order given, starting from mixture_in / fit_in (NULL: the prior mixture
+ * and an empty fit state of 36 floats: mean weight, its count, max record count, pending
+ * count, pending sums), incremental (batch_iters = 0) or batch EM; writes the 40-float
+ * mixture and the fit state. */
+tt_status tt_vmf_fit_batch(const float* records, int32_t n, const float* mixture_in, const float* fit_in,
+                           int32_t batch_iters, float* mixture_out, float* fit_out);
+/* The initial kd-tree build over n points (3 floats each, host only, no device use): writes
+ * each point's cell and *cells; min_points as --guide-subdiv-factor. */
+tt_status tt_kdtree_build_batch(const float* points, int32_t n, int32_t min_points, int32_t* cell_of_point,
+                                int32_t* cells);
 
 /* ---- Multi-view batches ------------------------------------------------------------
  * No counterpart in the reference (it renders one camera per RenderingAlgo).  A batch of

@@ -228,7 +228,15 @@ EXPORTED_SYMBOLS = [
     "tt_guide_features_batch",
     "tt_render_views",
     "tt_autotune_views",
+    "tt_guide_tree_info",
+    "tt_guide_tree_mixtures",
+    "tt_guide_tree_lookup_batch",
+    "tt_vmf_fit_batch",
+    "tt_kdtree_build_batch",
 ]
+
+GUIDE_LEARNED = 0
+GUIDE_TREE = 1
 
 
 class View(C.Structure):
@@ -260,6 +268,9 @@ class GuidingParams(C.Structure):
         ("steps_per_pass", C.c_int32),
         ("max_depth", C.c_int32),
         ("seed", C.c_uint64),
+        ("method", C.c_int32),
+        ("tree_subdivision", C.c_int32),
+        ("tree_em_iters", C.c_int32),
     ]
 
 
@@ -329,6 +340,12 @@ def load_library() -> C.CDLL:
         "tt_guide_features_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
         "tt_render_views": ([vp, P(View), C.c_int32, C.c_uint64, P(C.c_float)], C.c_int32),
         "tt_autotune_views": ([vp, P(View), C.c_int32, P(TuneResult)], C.c_int32),
+        "tt_guide_tree_info": ([vp, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int64)], C.c_int32),
+        "tt_guide_tree_mixtures": ([vp, P(C.c_float), C.c_int32], C.c_int32),
+        "tt_guide_tree_lookup_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_int32)], C.c_int32),
+        "tt_vmf_fit_batch": ([P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float),
+                              P(C.c_float)], C.c_int32),
+        "tt_kdtree_build_batch": ([P(C.c_float), C.c_int32, C.c_int32, P(C.c_int32), P(C.c_int32)], C.c_int32),
     }
     for name, (argtypes, restype) in sig.items():
         fn = getattr(lib, name)

@@ -150,14 +150,38 @@ class GpuContext:
     # Learned guiding ---------------------------------------------------------------
     def set_guiding(self, enabled: bool = True, train: int = 1, learning_rate: float = 1e-3,
                     record_pool: int = 1 << 16, batch: int = 8192, steps_per_pass: int = 16, max_depth: int = 2,
-                    seed: int = 1):
+                    seed: int = 1, method: int = abi.GUIDE_LEARNED, tree_subdivision: int = 100,
+                    tree_em_iters: int = 0):
         """train: 0 frozen, 1 collect records and train after every pass, 2 collect only;
         max_depth: guide the first max_depth bounces only (0: all).  Guiding the first two
         bounces measured the best relMSE per unit time on the gap-lit room (the network's cost
         grows with every guided vertex, its gain mostly comes from the first ones)."""
         gp = abi.GuidingParams(int(enabled), int(train), learning_rate, record_pool, batch, steps_per_pass, max_depth,
-                               seed)
+                               seed, int(method), int(tree_subdivision), int(tree_em_iters))
         self._check(self.lib.tt_set_guiding(self.h, C.byref(gp)), "tt_set_guiding")
+
+    def tree_info(self) -> dict:
+        """Cells, kd-tree nodes, fitted rounds and records of the tree guider."""
+        cells, nodes, rounds = C.c_int32(), C.c_int32(), C.c_int32()
+        recs = C.c_int64()
+        self._check(self.lib.tt_guide_tree_info(self.h, C.byref(cells), C.byref(nodes), C.byref(rounds),
+                                                C.byref(recs)), "tt_guide_tree_info")
+        return {"cells": cells.value, "nodes": nodes.value, "rounds": rounds.value, "records": recs.value}
+
+    def tree_mixtures(self) -> np.ndarray:
+        """(cells, 40): weights[8], means[8][3], concentrations[8] of every cell."""
+        n = self.tree_info()["cells"]
+        out = np.zeros((n, 40), np.float32)
+        self._check(self.lib.tt_guide_tree_mixtures(self.h, _fp(out), n), "tt_guide_tree_mixtures")
+        return out
+
+    def tree_lookup(self, points) -> np.ndarray:
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        out = np.zeros(len(pts), np.int32)
+        self._check(self.lib.tt_guide_tree_lookup_batch(self.h, _fp(pts), len(pts),
+                                                        out.ctypes.data_as(C.POINTER(C.c_int32))),
+                    "tt_guide_tree_lookup_batch")
+        return out
 
     def guide_params(self) -> np.ndarray:
         n = self.lib.tt_guide_num_params()
@@ -396,3 +420,31 @@ class GpuGuidedPathTracer(GpuPathTracer):
             if self._cb:
                 self._cb(True)
             self.schedule.update_for_next_pass()
+
+
+def vmf_fit_batch(records, mixture_in=None, fit_in=None, batch_iters: int = 0):
+    """The tree guider's fit of one cell on the device: records (n, 4) = direction xyz and
+    weight, in the order given; returns the 40-float mixture and the 36-float fit state."""
+    lib = abi.load_library()
+    r = np.ascontiguousarray(records, np.float32).reshape(-1, 4)
+    mi = None if mixture_in is None else np.ascontiguousarray(mixture_in, np.float32)
+    fi = None if fit_in is None else np.ascontiguousarray(fit_in, np.float32)
+    mo = np.zeros(40, np.float32)
+    fo = np.zeros(36, np.float32)
+    st = lib.tt_vmf_fit_batch(_fp(r), len(r), None if mi is None else _fp(mi), None if fi is None else _fp(fi),
+                              int(batch_iters), _fp(mo), _fp(fo))
+    abi.check(lib, None, st, "tt_vmf_fit_batch")
+    return mo, fo
+
+
+def kdtree_build_batch(points, min_points: int = 100):
+    """The tree guider's initial kd-tree over points (n, 3) (host code of the library, no
+    GPU needed): returns (cell of every point, number of cells)."""
+    lib = abi.load_library()
+    pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+    cells = np.zeros(len(pts), np.int32)
+    nc = C.c_int32()
+    st = lib.tt_kdtree_build_batch(_fp(pts), len(pts), int(min_points), cells.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   C.byref(nc))
+    abi.check(lib, None, st, "tt_kdtree_build_batch")
+    return cells, nc.value

@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -22,6 +23,7 @@
 #include "tt_internal.h"
 #include "tt_sobol_data.h"
 #include "tt_tables.h"
+#include "tt_tree.h"
 
 using namespace tt;
 
@@ -142,6 +144,7 @@ struct tt_ctx {
   uint32_t bvh_nodes = 0, bvh_depth = 0, bvh_node_bytes = 64;
   // Learned guiding.
   std::unique_ptr<GuideNet> gnet;
+  std::unique_ptr<TreeGuide> tree;   // tree guider (method TT_GUIDE_TREE)
   tt_guiding_params gparams{};
   GuideRecord* d_records = nullptr;   // record pool (ring)
   int* d_rec_count = nullptr;
@@ -845,6 +848,32 @@ static tt_status guide_train(tt_ctx* c, long long paths) {
     c->rec_seen = count;
   }
   const int pool = (int)std::min<long long>(count, c->rec_cap);
+  if (c->dev.guide_method == TT_GUIDE_TREE) {
+    // One round of the tree guider on this pass's records: the newest min(fresh, pool) of
+    // the ring, ending at index count % rec_cap.
+    const int n = (int)std::min<long long>(std::max(0ll, fresh), pool);
+    if (n <= 0) return TT_OK;
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<GuideRecord> recs(n);
+    const long long end = count % c->rec_cap;
+    const long long start = ((end - n) % c->rec_cap + c->rec_cap) % c->rec_cap;
+    const long long first = std::min<long long>(n, c->rec_cap - start);
+    TT_CUDA(c, cudaMemcpy(recs.data(), c->d_records + start, (size_t)first * sizeof(GuideRecord),
+                          cudaMemcpyDeviceToHost));
+    if (first < n)
+      TT_CUDA(c, cudaMemcpy(recs.data() + first, c->d_records, (size_t)(n - first) * sizeof(GuideRecord),
+                            cudaMemcpyDeviceToHost));
+    std::string gerr;
+    if (!c->tree->fit_round(recs.data(), n, c->gparams.seed, c->stream, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
+    c->dev.tree_nodes = c->tree->d_nodes;
+    c->dev.tree_root = c->tree->root_ref();
+    c->dev.tree_mix = c->tree->d_mix;
+    c->stats.guide_records += (uint64_t)n;
+    c->stats.guide_steps += 1;
+    c->stats.guide_train_ms +=
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return TT_OK;
+  }
   if (pool >= 256) {
     const int n = std::min(pool, c->gparams.batch > 0 ? c->gparams.batch : 8192);
     std::string gerr;
@@ -1335,6 +1364,7 @@ void tt_destroy(tt_ctx* c) {
   if (c->d_records) cudaFree(c->d_records);
   if (c->d_rec_count) cudaFree(c->d_rec_count);
   c->gnet.reset();
+  c->tree.reset();
   c->path_mem.free_all();
   c->scene_mem.free_all();
   if (c->stream) {
@@ -1358,10 +1388,20 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   }
   if (c->dev.algo != TT_ALGO_PT) return fail(c, TT_ERR_INVALID, "guiding needs algo pt");
   if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || gp->max_depth < 0 ||
-      !(gp->learning_rate >= 0.f) ||
-      gp->train < 0 || gp->train > 2)
+      !(gp->learning_rate >= 0.f) || gp->train < 0 || gp->train > 2 ||
+      (gp->method != TT_GUIDE_LEARNED && gp->method != TT_GUIDE_TREE) || gp->tree_subdivision < 0 ||
+      gp->tree_em_iters < 0)
     return fail(c, TT_ERR_INVALID, "bad guiding parameters");
   const int cap = gp->record_pool > 0 ? gp->record_pool : (1 << 16);
+  if (gp->method == TT_GUIDE_TREE && !c->tree) {
+    c->tree = std::make_unique<TreeGuide>();
+    std::string gerr;
+    if (!c->tree->init(gp->tree_subdivision, c->stream, &gerr)) {
+      c->tree.reset();
+      return fail(c, TT_ERR_CUDA, gerr);
+    }
+  }
+  if (c->tree) c->tree->em_iters = gp->tree_em_iters;
   if (!c->gnet) {
     c->gnet = std::make_unique<GuideNet>();
     std::string gerr;
@@ -1392,6 +1432,12 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   c->dev.guide_w16 = c->gnet->params16;
   c->dev.guide_w32 = c->gnet->params;
   c->dev.guide = 1;
+  c->dev.guide_method = gp->method;
+  if (gp->method == TT_GUIDE_TREE) {
+    c->dev.tree_nodes = c->tree->d_nodes;
+    c->dev.tree_root = c->tree->root_ref();
+    c->dev.tree_mix = c->tree->d_mix;
+  }
   c->dev.guide_record = gp->train ? 1 : 0;
   c->dev.guide_depth = gp->max_depth > 0 ? gp->max_depth : (1 << 30);
   return TT_OK;
@@ -1501,6 +1547,52 @@ tt_status tt_guide_read_records(tt_ctx* c, float* out, int32_t max_records, int3
   TT_CUDA(c, cudaMemset(c->d_rec_count, 0, sizeof(int)));
   c->rec_seen = 0;
   *n = cnt;
+  return TT_OK;
+}
+
+tt_status tt_guide_tree_info(tt_ctx* c, int32_t* cells, int32_t* nodes, int32_t* rounds, int64_t* records) {
+  if (!c) return TT_ERR_INVALID;
+  if (!c->tree) return fail(c, TT_ERR_NOT_READY, "the tree guider is not enabled");
+  if (cells) *cells = c->tree->ncells;
+  if (nodes) *nodes = (int32_t)c->tree->nodes.size();
+  if (rounds) *rounds = c->tree->round;
+  if (records) *records = c->tree->records_fitted;
+  return TT_OK;
+}
+
+tt_status tt_guide_tree_mixtures(tt_ctx* c, float* out, int32_t max_cells) {
+  if (!c || !out || max_cells < 0) return TT_ERR_INVALID;
+  if (!c->tree) return fail(c, TT_ERR_NOT_READY, "the tree guider is not enabled");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  TT_CUDA(c, cudaStreamSynchronize(c->stream));
+  const int n = std::min(max_cells, c->tree->ncells);
+  if (n > 0) TT_CUDA(c, cudaMemcpy(out, c->tree->d_mix, (size_t)n * kTreeMixFloats * sizeof(float), cudaMemcpyDeviceToHost));
+  return TT_OK;
+}
+
+tt_status tt_guide_tree_lookup_batch(tt_ctx* c, const float* points, int32_t n, int32_t* cells) {
+  if (!c || (n > 0 && (!points || !cells)) || n < 0) return TT_ERR_INVALID;
+  if (!c->tree) return fail(c, TT_ERR_NOT_READY, "the tree guider is not enabled");
+  for (int i = 0; i < n; ++i) cells[i] = c->tree->lookup(points[3 * i], points[3 * i + 1], points[3 * i + 2]);
+  return TT_OK;
+}
+
+tt_status tt_vmf_fit_batch(const float* records, int32_t n, const float* mixture_in, const float* fit_in,
+                           int32_t batch_iters, float* mixture_out, float* fit_out) {
+  if (!records || n <= 0 || !mixture_out || !fit_out || batch_iters < 0)
+    return fail(nullptr, TT_ERR_INVALID, "tt_vmf_fit_batch: bad arguments");
+  std::string err;
+  if (!vmf_fit_one(records, n, mixture_in, fit_in, batch_iters, mixture_out, fit_out, &err))
+    return fail(nullptr, TT_ERR_CUDA, err);
+  return TT_OK;
+}
+
+tt_status tt_kdtree_build_batch(const float* points, int32_t n, int32_t min_points, int32_t* cell_of_point,
+                                int32_t* cells) {
+  if (!points || n <= 0 || !cell_of_point || !cells || min_points < 0)
+    return fail(nullptr, TT_ERR_INVALID, "tt_kdtree_build_batch: bad arguments");
+  std::vector<TreeNodeHost> nodes;
+  *cells = kdtree_build(points, n, min_points > 0 ? min_points : 100, &nodes, cell_of_point);
   return TT_OK;
 }
 

@@ -135,6 +135,13 @@ struct DevScene {
   float box_lo[3];            // scene box, for the position encoding
   float box_inv[3];           // 1 / extent per axis
   int algo;                   // TT_ALGO_PT or TT_ALGO_PT2 (tt_pt2.cuh)
+  // Tree guider (tt_tree.cu), when guide_method == TT_GUIDE_TREE: kd-tree nodes (split,
+  // axis, child0, child1 as int bits; a child < 0 is ~cell), the root reference and the
+  // cells' mixtures (40 floats each: weights[8], means[8][3], concentrations[8]).
+  int guide_method;
+  const float4* tree_nodes;
+  int tree_root;
+  const float* tree_mix;
   // Quasi-random sampling (pt2 with qmc): Sobol generator matrices, 32 words per dimension
   // (TT_SOBOL_DIMS dimensions), and the per-pixel rotations [128 * 128][2]; null otherwise.
   const uint32_t* sobol;

@@ -1188,8 +1188,8 @@ __device__ __forceinline__ GuidePre guide_prefetch(const PathState& p, int slot)
 }
 
 template <bool MEDIA>
-__device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const PathState& p, int bounce,
-                                                  const GuidePre& pre, const float* gout) {
+__device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const PathState& p, int bounce,
+                                                  const GuidePre& pre, const GuideMixture& mix) {
   const int slot = pre.slot;
   const float4 h = pre.h;
   const float3 dir = xyz(pre.d4);
@@ -1205,7 +1205,6 @@ __device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const Path
   orient(s, dir);
   const DevMaterial& m = sc.materials[s.material];
   const float3 wi = -dir;
-  const GuideMixture mix = guide_decode(gout);
   float3 ndir, val;
   float pb = 0.f;
   if (rng.uniform() < mix.c) {
@@ -1276,6 +1275,47 @@ __device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const Path
     p.ext_q[(bounce + 1) & 1][qe] = slot;
   }
   p.rng_state[slot] = rng.state;
+}
+
+template <bool MEDIA>
+__device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const PathState& p, int bounce,
+                                                  const GuidePre& pre, const float* gout) {
+  guide_scatter_mix<MEDIA>(sc, p, bounce, pre, guide_decode(gout));
+}
+
+// Cell of a normalised position in the tree guider's kd-tree (kdtree::Tree::Lookup,
+// path_guiding_tree.hxx:129-150: left when the coordinate is below the split).
+__device__ __forceinline__ int tree_cell(const DevScene& sc, float x, float y, float z) {
+  int ref = sc.tree_root;
+  for (int d = 0; d < 64 && ref >= 0; ++d) {
+    const float4 nd = __ldg(&sc.tree_nodes[ref]);
+    const int axis = __float_as_int(nd.y);
+    const float c = axis == 0 ? x : (axis == 1 ? y : z);
+    ref = __float_as_int(c < nd.x ? nd.z : nd.w);
+  }
+  return ref < 0 ? ~ref : 0;
+}
+
+// Tree-guided scattering: the cell's fitted mixture against the BSDF by the same one-sample
+// MIS, the mixture chosen with probability 0.5 (PROB_BSDF, renderingalgorithms_pathtracing_
+// guided.cxx:470).
+template <bool MEDIA>
+__global__ void __launch_bounds__(256) k_guide_tree(DevScene sc, PathState p, int bounce) {
+  const int n = *guide_count(p, bounce);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const GuidePre pre = guide_prefetch(p, p.guide_q[i]);
+    const float4 a = p.ginp[3 * (size_t)i];
+    const float* cm = sc.tree_mix + 40 * (size_t)tree_cell(sc, a.x, a.y, a.z);
+    GuideMixture mix;
+#pragma unroll
+    for (int k = 0; k < kGLobes; ++k) {
+      mix.w[k] = __ldg(&cm[k]);
+      mix.mu[k] = f3(__ldg(&cm[8 + 3 * k]), __ldg(&cm[9 + 3 * k]), __ldg(&cm[10 + 3 * k]));
+      mix.kappa[k] = __ldg(&cm[32 + k]);
+    }
+    mix.c = 0.5f;
+    guide_scatter_mix<MEDIA>(sc, p, bounce, pre, mix);
+  }
 }
 
 // Guided scattering of the vertices k_shade queued this bounce: a persistent kernel whose
@@ -1715,6 +1755,19 @@ void prepare_guide_launch() {
 }
 
 void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st) {
+  if (s.guide_method == TT_GUIDE_TREE) {
+    static int tgrid = 0;
+    if (tgrid == 0) {
+      int dev = 0, sms = 0, per = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_guide_tree<true>, kBlock, 0);
+      tgrid = sms * (per > 0 ? per : 1);
+    }
+    if (s.num_media > 0) k_guide_tree<true><<<tgrid, kBlock, 0, st>>>(s, p, bounce);
+    else k_guide_tree<false><<<tgrid, kBlock, 0, st>>>(s, p, bounce);
+    return;
+  }
   prepare_guide_launch();
   const int grid = g_guide_grid;
   if (s.num_media > 0) k_guide<true><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
