@@ -46,3 +46,66 @@ def write_pfm(path, rgb_linear: np.ndarray, xres: int, yres: int) -> None:
     with open(path, "wb") as f:
         f.write(f"PF\n{xres} {yres}\n-1.0\n".encode())
         f.write(a.tobytes())
+
+
+def write_exr(path, rgb_linear: np.ndarray, xres: int, yres: int) -> None:
+    """OpenEXR, single-part scanline image, uncompressed, channels B, G, R as 32-bit floats
+    (the file layout of the OpenEXR specification: magic and version, header attributes,
+    one offset per scanline, then per line its y, byte count and the channels in name
+    order).  Input in unit order (row 0 at the bottom); EXR's first line is the top."""
+    a = np.asarray(rgb_linear, dtype="<f4").reshape(yres, xres, 3)[::-1]
+
+    def attr(name, typ, data):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(data)) + data
+
+    chlist = b"".join(c.encode() + b"\0" + struct.pack("<iB3xii", 2, 0, 1, 1) for c in "BGR") + b"\0"
+    box = struct.pack("<iiii", 0, 0, xres - 1, yres - 1)
+    header = (attr("channels", "chlist", chlist) + attr("compression", "compression", b"\0") +
+              attr("dataWindow", "box2i", box) + attr("displayWindow", "box2i", box) +
+              attr("lineOrder", "lineOrder", b"\0") + attr("pixelAspectRatio", "float", struct.pack("<f", 1.0)) +
+              attr("screenWindowCenter", "v2f", struct.pack("<ff", 0.0, 0.0)) +
+              attr("screenWindowWidth", "float", struct.pack("<f", 1.0)) + b"\0")
+    head = struct.pack("<ii", 20000630, 2) + header
+    line_bytes = 3 * 4 * xres
+    first = len(head) + 8 * yres
+    offsets = struct.pack(f"<{yres}Q", *[first + y * (8 + line_bytes) for y in range(yres)])
+    body = b"".join(struct.pack("<ii", y, line_bytes) + a[y, :, 2].tobytes() + a[y, :, 1].tobytes() +
+                    a[y, :, 0].tobytes() for y in range(yres))
+    Path(path).write_bytes(head + offsets + body)
+
+
+def read_exr(path) -> np.ndarray:
+    """Reads the uncompressed single-part FLOAT R, G, B images write_exr produces; returns
+    (height, width, 3) with row 0 at the top."""
+    data = Path(path).read_bytes()
+    magic, version = struct.unpack_from("<ii", data, 0)
+    if magic != 20000630:
+        raise ValueError("not an OpenEXR file")
+    pos = 8
+    attrs = {}
+    while data[pos] != 0:
+        end = data.index(b"\0", pos)
+        name = data[pos:end].decode()
+        tend = data.index(b"\0", end + 1)
+        size = struct.unpack_from("<i", data, tend + 1)[0]
+        attrs[name] = data[tend + 5:tend + 5 + size]
+        pos = tend + 5 + size
+    pos += 1
+    if attrs["compression"] != b"\0":
+        raise ValueError("only uncompressed EXR files are read here")
+    x0, y0, x1, y1 = struct.unpack("<iiii", attrs["dataWindow"])
+    w, h = x1 - x0 + 1, y1 - y0 + 1
+    names, p, cl = [], 0, attrs["channels"]
+    while cl[p] != 0:
+        e = cl.index(b"\0", p)
+        names.append(cl[p:e].decode())
+        p = e + 1 + 16
+    offsets = struct.unpack_from(f"<{h}Q", data, pos)
+    img = np.zeros((h, w, 3), np.float32)
+    for off in offsets:
+        y, size = struct.unpack_from("<ii", data, off)
+        row = np.frombuffer(data, "<f4", count=len(names) * w, offset=off + 8).reshape(len(names), w)
+        for c, name in enumerate(names):
+            if name in "RGB":
+                img[y - y0, :, "RGB".index(name)] = row[c]
+    return img

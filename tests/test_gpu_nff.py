@@ -1,0 +1,42 @@
+"""A scene read from NFF files (tests/golden/scenes/room.nff: media, glass, mirror,
+microfacet, spheres, area / point / sun / dome lights, an included file and an OBJ mesh)
+rendered on the GPU against the CPU oracle, per path (GPU); and its image written as
+OpenEXR."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from naivetrace_b200.algo import GpuContext
+from naivetrace_b200.image import read_exr, write_exr
+from naivetrace_b200.nff import parse_nff
+from naivetrace_b200.scene import make_params
+from test_gpu_render import render_both
+
+pytestmark = pytest.mark.gpu
+
+SCENES = Path(__file__).parent / "golden" / "scenes"
+
+
+def test_nff_room_per_path_parity(gpu_lib):
+    scene = parse_nff(SCENES / "room.nff", width=32, height=24)
+    (ag, lg, sg), (ao, lo, so), g, o = render_both(scene, 4, 8)
+    assert sg == so
+    assert g.stats()["error_flags"] == 0
+    ag, ao = ag.reshape(-1, 3), ao.reshape(-1, 3)
+    scale = max(np.abs(ao).mean(), 1e-6)
+    close = np.all(np.abs(ag - ao) <= 1e-3 * np.abs(ao) + 1e-3 * scale, axis=1)
+    assert close.mean() >= 0.9, close.mean()
+    np.testing.assert_allclose(ag[close].sum(axis=0), ao[close].sum(axis=0), rtol=2e-3)
+    assert ao.mean() > 0
+
+
+def test_nff_render_to_exr(gpu_lib, tmp_path):
+    scene = parse_nff(SCENES / "room.nff", width=24, height=16)
+    g = GpuContext(scene, make_params(max_ray_depth=8))
+    g.render(16, seed=2)
+    rgb = g.framebuffer()
+    write_exr(tmp_path / "room.exr", rgb, 24, 16)
+    img = read_exr(tmp_path / "room.exr")
+    np.testing.assert_array_equal(img[::-1].reshape(-1), rgb.astype(np.float32).reshape(-1))
+    assert np.isfinite(img).all() and img.mean() > 0

@@ -1,0 +1,109 @@
+"""The NFF reader (naivetrace_b200/nff.py, following parsenff.cxx:113-831) on scene files
+written for these tests (tests/golden/scenes/): camera, transforms and scopes, shaders,
+media with phase functions, invisible medium boundaries, area / point / sun / dome lights,
+included files, OBJ meshes with per-group shaders; errors name the file and line.  Also the
+float image writers (PFM, OpenEXR) round trip."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from naivetrace_b200 import abi
+from naivetrace_b200.image import read_exr, write_exr, write_pfm
+from naivetrace_b200.nff import NFFError, parse_nff, read_pfm
+from naivetrace_b200.spectral import rgb_to_spectrum
+
+SCENES = Path(__file__).parent / "golden" / "scenes"
+
+
+def _tris(scene):
+    v, n, t, m = scene.arrays()
+    return v, n, t, m
+
+
+def test_room_structure():
+    s = parse_nff(SCENES / "room.nff")
+    c = s.camera
+    assert (c.kind, c.xres, c.yres, c.fov_deg) == (abi.CAMERA_PINHOLE, 40, 30, 45.0)
+    np.testing.assert_allclose(c.pos, (0.5, 0.5, -1.5))
+    np.testing.assert_allclose(c.dir, (0.0, 0.0, 2.0))
+    v, n, t, mat = _tris(s)
+    # 3 walls x 2 + panel 1 + box 6 x 2 + light 2 + cube 6 x 2 = 33 triangles; 3 spheres.
+    assert len(t) == 33 and s.num_spheres == 3
+    kinds = [(m.shader, m.volume_boundary, m.emission is not None) for m in s.materials]
+    shaders = {k[0] for k in kinds}
+    assert {abi.SHADER_DIFFUSE, abi.SHADER_MICROFACET, abi.SHADER_SPECULAR_REFLECTIVE,
+            abi.SHADER_SPECULAR_DIELECTRIC} <= shaders
+    # Glossy: alpha 0.2, reflectance 1.0 x rgb.
+    gl = [m for m in s.materials if m.shader == abi.SHADER_MICROFACET][0]
+    assert gl.alpha == pytest.approx(0.2)
+    np.testing.assert_allclose(gl.reflectance, rgb_to_spectrum((0.9, 0.7, 0.4)), rtol=1e-12)
+    # Glass sphere with the fog medium inside; the fog is Henyey-Greenstein 0.6.
+    glass = [m for m in s.materials if m.shader == abi.SHADER_SPECULAR_DIELECTRIC][0]
+    assert glass.ior_ratio == 1.5 and glass.medium_inside == 0
+    fog, ink = s.media
+    assert fog.phase == abi.PHASE_HENYEY_GREENSTEIN and fog.phase_g == pytest.approx(0.6)
+    np.testing.assert_allclose(fog.sigma_s, np.maximum(rgb_to_spectrum((0.5,) * 3), 0))
+    assert (fog.priority, ink.priority) == (1, 2)
+    np.testing.assert_allclose(ink.sigma_a, np.maximum(rgb_to_spectrum((2, 1, 0.5)), 0))
+    box = [m for m in s.materials if m.volume_boundary]
+    assert len(box) == 1 and box[0].medium_inside == 1
+    # Area light: black shader, emission = power x spectrum of white.
+    light = [m for m in s.materials if m.emission is not None]
+    assert len(light) == 1
+    np.testing.assert_allclose(light[0].emission, 8 * rgb_to_spectrum((1, 1, 1)))
+    assert np.all(light[0].reflectance == 0)
+    # Point light (0.5 x colour), sun (default half angle 0.26 degrees) and dome.
+    assert len(s.point_lights) == 1
+    np.testing.assert_allclose(s.point_lights[0][0], rgb_to_spectrum((0.5, 0.45, 0.4)))
+    kinds = [e.kind for e in s.env_lights]
+    assert kinds == [abi.ENV_SUN, abi.ENV_DOME]
+    assert s.env_lights[0].scalar == 5 and s.env_lights[0].scalar2 == pytest.approx(0.26)
+    np.testing.assert_allclose(np.linalg.norm(s.env_lights[0].dir), 1.0)
+
+
+def test_transform_scope_and_obj():
+    s = parse_nff(SCENES / "room.nff")
+    v, n, t, mat = _tris(s)
+    # The glossy panel: heading pi/2 about y maps x to -z, then the translation.
+    gl_idx = [i for i, m in enumerate(s.materials) if m.shader == abi.SHADER_MICROFACET][0]
+    tri = t[mat == gl_idx][0]
+    np.testing.assert_allclose(v[tri], [[0.2, 0.05, 0.6], [0.2, 0.05, 0.3], [0.2, 0.35, 0.6]], atol=1e-6)
+    # Explicit normals are rotated too: (0, 1, 0) stays.
+    np.testing.assert_allclose(n[tri], [[0, 1, 0]] * 3, atol=1e-6)
+    # Spheres after the scope use the outer shaders (grey, then chrome), not the panel's.
+    sph, smat = s.sphere_arrays()
+    assert s.materials[int(smat[0])].shader == abi.SHADER_DIFFUSE
+    assert s.materials[int(smat[1])].shader == abi.SHADER_SPECULAR_REFLECTIVE
+    # The OBJ cube: three faces with usemtl grey, three with the active (black) shader.
+    cube = np.all(v[t][:, :, 0] >= 0.75 - 1e-6, axis=1) & np.all(v[t][:, :, 2] >= 0.7 - 1e-6, axis=1)
+    assert cube.sum() == 12
+    refl = np.array([s.materials[m].reflectance.max() for m in mat[cube]])
+    assert (refl > 0.5).sum() == 6 and (refl == 0).sum() == 6
+
+
+def test_resolution_override_and_text_input():
+    s = parse_nff(SCENES / "room.nff", width=16, height=12)
+    assert (s.camera.xres, s.camera.yres) == (16, 12)
+    s2 = parse_nff("vfisheye\nfrom 0 0 0\nat 0 1 0\nup 0 0 1\nresolution 8 8\ns 0 2 0 0.5\n")
+    assert s2.camera.kind == abi.CAMERA_FISHEYE and s2.num_spheres == 1
+
+
+@pytest.mark.parametrize("text,msg", [("v\nfrom 0 0 0\nat 0 0 1\nup 0 1 0\nresolution 4 4\nangle 30\nfoo 1\n", ":7"),
+                                      ("yaml{\n}yaml\n", "not supported"),
+                                      ("shader nothere\n", "unknown shader"),
+                                      ("larea a parallel 1 1 1 1\n", "uniform"),
+                                      ("p 2\n0 0 0\n1 0 0\n", "3 vertices")])
+def test_errors_name_the_line(text, msg):
+    with pytest.raises(NFFError, match=msg):
+        parse_nff(text + "\n")
+
+
+def test_float_image_writers(tmp_path):
+    a = np.random.default_rng(0).random(6 * 4 * 3).astype(np.float32)
+    write_exr(tmp_path / "a.exr", a, 6, 4)
+    np.testing.assert_array_equal(read_exr(tmp_path / "a.exr")[::-1].reshape(-1), a)
+    raw = (tmp_path / "a.exr").read_bytes()
+    assert raw[:4] == bytes([0x76, 0x2F, 0x31, 0x01]) and raw[4] == 2
+    write_pfm(tmp_path / "a.pfm", a, 6, 4)
+    np.testing.assert_array_equal(read_pfm(tmp_path / "a.pfm")[::-1].reshape(-1), a)
