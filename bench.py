@@ -198,11 +198,11 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
         kw = dict(learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
         if tree:
             kw.update(method=abi.GUIDE_TREE, tree_subdivision=200, tree_em_iters=4)
-        # One untimed pass at the largest wave size allocates the path state (with the
-        # guiding arrays for the guided run); the guide is not trained by it.
+        # One untimed pass at the largest wave size (2^26 paths) allocates the path state
+        # (with the guiding arrays for the guided run); the guide is not trained by it.
         if guided:
             g.set_guiding(True, 0, **kw)
-        g.render(8, 3)
+        g.render(-(-(1 << 26) // (xres * yres)), 3)
         g.clear()
         g.reset_stats()
         pts, el, spp_total, seed = [], 0.0, 0, 10
@@ -286,7 +286,7 @@ def multiview_comparison(g, n_views=96, seed=4):
     views = scenes.terrain_views(n_views, seed=seed)
     paths = sum(c.xres * c.yres * s for c, s in views)
     tune = g.autotune_views(views)
-    g.render_views(views[:4], seed=1)  # warm-up at the tuned configuration
+    g.render_views(views, seed=1)  # warm-up at the tuned configuration (allocates the path state)
 
     def timed(fn):
         torch.cuda.synchronize()
@@ -323,7 +323,7 @@ def pt2_comparison(scene, spp, depth, device):
     paths = scene.camera.xres * scene.camera.yres * spp
     for qmc in (False, True):
         g = GpuContext(scene, make_params(max_ray_depth=depth, device=device, algo=abi.ALGO_PT2, qmc=qmc))
-        g.render(4, 1)
+        g.render(spp, 1)  # allocates the path state of the timed frame
         g.clear()
         g.reset_stats()
         torch.cuda.synchronize()
@@ -631,7 +631,7 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--wave", type=int, default=0, help="paths per wavefront wave (0 = library default)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")

@@ -182,7 +182,8 @@ typedef struct tt_params {
   int32_t max_ray_depth;        /* --rd (reference default 25) */
   int32_t pt_sample_mode;       /* TT_SAMPLE_* */
   int32_t max_samples_per_pixel;/* --spp; <= 0 means unbounded (Run loops until stopped) */
-  int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default */
+  int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default (2^26, halved
+                                   while the device cannot hold it) */
   int32_t device;               /* CUDA device ordinal */
   int32_t algo;                 /* TT_ALGO_* */
   int32_t qmc;                  /* --qmc (RenderingParameters::qmc): Sobol points with per-pixel
@@ -445,7 +446,7 @@ typedef struct tt_tune_result {
   double candidate_ms[TT_TUNE_MAX];
 } tt_tune_result;
 
-/* Autotuner: times one-sample probes of the batch over queue capacities (2^20 .. 2^23 paths
+/* Autotuner: times one-sample probes of the batch over queue capacities (2^22, 2^24, 2^25, 2^26 paths
  * per wave) and launch widths (0.5, 1, 2 x the occupancy grid) and keeps the fastest for
  * this context's later passes.  The BVH layout stays binary: the 8-wide layout measured a
  * few percent slower on the mesh workloads (TT_BVH_WIDTH=8 selects it at upload). */

@@ -29,7 +29,12 @@ using namespace tt;
 
 namespace {
 
-constexpr int kDefaultWave = 1 << 22;
+// Paths resident per wave: 2^26 paths hold about 16 GB of path state (more with media or
+// guiding), a small share of the B200's HBM; a large wave keeps every launch of the bounce
+// loop full, so the latency-bound tail launches of the last bounces are paid once per 2^26
+// paths (the 1920x1080x64 frame: 2 waves instead of 32 at 2^22, 1.6x the throughput).
+// When the device cannot hold a wave, the wave is halved until it fits (down to 2^20).
+constexpr int kDefaultWave = 1 << 26;
 
 std::mutex g_err_mutex;
 std::string g_create_error;
@@ -828,6 +833,17 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
   return TT_OK;
 }
 
+// ensure_path_state for a wave of *cap paths, halving the wave while the allocation fails
+// (down to 2^20 paths); *cap is the capacity obtained.
+static tt_status ensure_path_state_fit(tt_ctx* c, int* cap) {
+  for (;;) {
+    const tt_status st = ensure_path_state(c, *cap);
+    if (st == TT_OK || *cap <= (1 << 20)) return st;
+    cudaGetLastError();
+    *cap = std::max(1 << 20, *cap / 2);
+  }
+}
+
 // After a pass: `steps_per_pass` Adam steps, each on a mini-batch drawn from the record
 // pool; also updates the pool's yield per path, from which the next pass's keep
 // probability follows.
@@ -915,13 +931,13 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
   const int npix_range = pe - pb;
   const long long total = (long long)spp * npix_range;
   const int wave_limit = c->params.wave_paths > 0 ? c->params.wave_paths : kDefaultWave;
-  const int cap = (int)std::min<long long>(total, wave_limit);
+  int cap = (int)std::min<long long>(total, wave_limit);
   if (c->dev.guide_record) {
     // Keep about 80 % of a pool's worth of this pass's records at most.
     const double expected = c->rec_rate * (double)total;
     c->dev.guide_keep = expected > 0.0 ? (float)std::min(1.0, 0.8 * c->rec_cap / expected) : 1.f;
   }
-  tt_status st = ensure_path_state(c, cap);
+  tt_status st = ensure_path_state_fit(c, &cap);
   if (st != TT_OK) return st;
   const bool counting = c->profiling >= 2;
   const bool timing = c->profiling >= 1;
@@ -1651,12 +1667,12 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
     paths += (long long)hv[v].npix * hv[v].spp;
     if (npix_total > (1ll << 30)) return fail(c, TT_ERR_CAPACITY, "views hold more than 2^30 pixels");
   }
-  const int cap = (int)std::min<long long>(paths, wave_limit);
+  int cap = (int)std::min<long long>(paths, wave_limit);
   if (c->dev.guide_record) {
     const double expected = c->rec_rate * (double)paths;
     c->dev.guide_keep = expected > 0.0 ? (float)std::min(1.0, 0.8 * c->rec_cap / expected) : 1.f;
   }
-  tt_status st = ensure_path_state(c, cap);
+  tt_status st = ensure_path_state_fit(c, &cap);
   if (st != TT_OK) return st;
   const int nwaves = (int)((paths + cap - 1) / cap);
   std::vector<ViewWave> hw((size_t)nwaves);
@@ -1798,7 +1814,7 @@ tt_status tt_autotune_views(tt_ctx* c, const tt_view* views, int32_t n, tt_tune_
   }
   if (npix <= 0 || npix > (1ll << 30)) return fail(c, TT_ERR_INVALID, "bad views");
   std::vector<float> rgb(3 * (size_t)npix);
-  const int waves[] = {1 << 20, 1 << 21, 1 << 22, 1 << 23};
+  const int waves[] = {1 << 22, 1 << 24, 1 << 25, 1 << 26};
   const int base_grid = c->grid;
   const int grids[] = {base_grid / 2 > 0 ? base_grid / 2 : base_grid, base_grid, 2 * base_grid};
   *out = tt_tune_result{};

@@ -77,7 +77,7 @@ def test_autotune_views(gpu_lib):
     g = GpuContext(scene, make_params(max_ray_depth=6))
     views = [(c, 2) for c, _ in scenes.terrain_views(8, seed=1, resolutions=(64, 128))]
     r = g.autotune_views(views)
-    assert r["wave_paths"] in (1 << 20, 1 << 21, 1 << 22, 1 << 23)
+    assert r["wave_paths"] in (1 << 22, 1 << 24, 1 << 25, 1 << 26)
     assert r["grid"] > 0 and r["ms"] > 0
     assert len(r["candidates"]) == 12
     assert r["ms"] == min(c["ms"] for c in r["candidates"])
