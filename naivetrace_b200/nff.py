@@ -73,13 +73,14 @@ class _Scope:
     shaders: Dict[str, Optional[_Shader]] = field(default_factory=dict)
     media: Dict[str, int] = field(default_factory=dict)          # name -> scene medium index (-1 vacuum)
     emitters: Dict[str, Optional[np.ndarray]] = field(default_factory=dict)
+    named: Dict[str, tuple] = field(default_factory=dict)          # material name -> (shader, medium, emitter)
     shader: str = "default"
     medium: str = "default"
     emitter: str = "none"
 
     def child(self) -> "_Scope":
         return replace(self, transform=self.transform.copy(), shaders=dict(self.shaders), media=dict(self.media),
-                       emitters=dict(self.emitters))
+                       emitters=dict(self.emitters), named=dict(self.named))
 
 
 def _default_scope() -> _Scope:
@@ -205,8 +206,18 @@ class _Parser:
                 continue
             if d == "}":
                 return i
-            if d == "yaml{" or d == "diffusetexture" or d == "exponenttexture":
-                raise NFFError(f"{where}: not supported by this reader")
+            if d == "yaml{":
+                block = []
+                while i < len(lines) and not lines[i].startswith("}yaml"):
+                    block.append(lines[i])
+                    i += 1
+                if i >= len(lines):
+                    raise NFFError(f"{where}: yaml section not terminated with }}yaml")
+                i += 1
+                self.yaml_section("\n".join(block), scope, where)
+                continue
+            if d == "diffusetexture" or d == "exponenttexture":
+                raise NFFError(f"{where}: textures are not supported by this reader")
             if d == "transform":
                 scope.transform = _transform(_floats(args, where))
             elif d in ("v", "vfisheye"):
@@ -367,6 +378,50 @@ class _Parser:
                 raise NFFError(f"{where}: unknown directive")
         return i
 
+    def yaml_section(self, text: str, scope: _Scope, where: str):
+        """NFFParser::ParseYamlNode (parsenff.cxx:868-970): transform (replaces the current
+        one; radians unless angle_in_degree), shader (speculartransmissivedielectric or glossy
+        with rgb and x; activated), material (names the active shader, medium and emitter)."""
+        import yaml
+        doc = yaml.safe_load(text) or {}
+        for key, node in doc.items():
+            if key == "transform":
+                f = math.pi / 180.0 if node.get("angle_in_degree") else 1.0
+                m = np.eye(4)
+                if "pos" in node:
+                    m[:3, 3] = [float(x) for x in node["pos"]]
+                if "hpb" in node:
+                    h, p, b = (float(x) * f for x in node["hpb"])
+                    m = m @ _rot(1, h) @ _rot(0, p) @ _rot(2, b)
+                if "rotaxis" in node:
+                    from .yaml_scene import _axis_angle
+                    r = np.array([float(x) for x in node["rotaxis"]]) * f
+                    n = np.linalg.norm(r)
+                    if n > 0:
+                        m = m @ _axis_angle(r / n, n)
+                if "scale" in node:
+                    m = m @ np.diag([float(x) for x in node["scale"]] + [1.0])
+                scope.transform = m
+            elif key == "shader":
+                cls, name = node["class"], node["name"]
+                if cls == "speculartransmissivedielectric":
+                    if "abbe_number" in node:
+                        raise NFFError(f"{where}: dispersion (abbe_number) is not supported")
+                    scope.shaders[name] = _Shader(abi.SHADER_SPECULAR_DIELECTRIC, np.zeros(NBINS),
+                                                  ior=float(node["ior_ratio"]))
+                elif cls == "glossy":
+                    rgb = [float(x) for x in node.get("rgb", [1.0, 1.0, 1.0])]
+                    k = float(node.get("x", 1.0))
+                    scope.shaders[name] = _Shader(abi.SHADER_MICROFACET, rgb_to_spectrum([k * x for x in rgb]),
+                                                  alpha=float(node["alpha"]))
+                else:
+                    raise NFFError(f"{where}: shader class {cls} is not supported by this tracer")
+                scope.shader = name
+            elif key == "material":
+                scope.named[node["name"]] = (scope.shader, scope.medium, scope.emitter)
+            else:
+                raise NFFError(f"{where}: yaml key {key} is not supported")
+
     @staticmethod
     def activate(table, name, where):
         if name not in table:
@@ -374,8 +429,13 @@ class _Parser:
 
     def mesh_material(self, scope: _Scope, name: Optional[str]) -> int:
         # GetMaterial (parsenff.cxx:41-66): a defined shader of that name, else the active material.
-        if name and name != "DefaultMaterial" and name in scope.shaders:
-            return self.material(scope, name)
+        if name and name != "DefaultMaterial":
+            if name in scope.named:
+                s = scope.child()
+                s.shader, s.medium, s.emitter = scope.named[name]
+                return self.material(s)
+            if name in scope.shaders:
+                return self.material(scope, name)
         return self.material(scope)
 
     def add_mesh(self, v, n, t, scope: _Scope, material: int):

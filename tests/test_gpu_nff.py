@@ -1,7 +1,8 @@
-"""A scene read from NFF files (tests/golden/scenes/room.nff: media, glass, mirror,
-microfacet, spheres, area / point / sun / dome lights, an included file and an OBJ mesh)
-rendered on the GPU against the CPU oracle, per path (GPU); and its image written as
-OpenEXR."""
+"""Scenes read from scene files rendered on the GPU against the CPU oracle, per path (GPU):
+tests/golden/scenes/room.nff (media, glass, mirror, microfacet, spheres, area / point / sun
+/ dome lights, an included file and an OBJ mesh) and tests/golden/scenes/room.yaml (the
+YAML schema: scopes with transforms, inline and named materials, an OBJ mesh with a
+material map); and an image written as OpenEXR."""
 from pathlib import Path
 
 import numpy as np
@@ -40,3 +41,16 @@ def test_nff_render_to_exr(gpu_lib, tmp_path):
     img = read_exr(tmp_path / "room.exr")
     np.testing.assert_array_equal(img[::-1].reshape(-1), rgb.astype(np.float32).reshape(-1))
     assert np.isfinite(img).all() and img.mean() > 0
+
+
+def test_yaml_room_per_path_parity(gpu_lib):
+    from naivetrace_b200.yaml_scene import parse_yaml_scene
+    scene = parse_yaml_scene(SCENES / "room.yaml", width=32, height=24)
+    (ag, lg, sg), (ao, lo, so), g, o = render_both(scene, 4, 8)
+    assert g.stats()["error_flags"] == 0
+    ag, ao = ag.reshape(-1, 3), ao.reshape(-1, 3)
+    scale = max(np.abs(ao).mean(), 1e-6)
+    close = np.all(np.abs(ag - ao) <= 1e-3 * np.abs(ao) + 1e-3 * scale, axis=1)
+    assert close.mean() >= 0.9, close.mean()
+    np.testing.assert_allclose(ag[close].sum(axis=0), ao[close].sum(axis=0), rtol=2e-3)
+    assert ao.mean() > 0

@@ -90,7 +90,7 @@ def test_resolution_override_and_text_input():
 
 
 @pytest.mark.parametrize("text,msg", [("v\nfrom 0 0 0\nat 0 0 1\nup 0 1 0\nresolution 4 4\nangle 30\nfoo 1\n", ":7"),
-                                      ("yaml{\n}yaml\n", "not supported"),
+                                      ("yaml{\nlight: 1\n}yaml\n", "not supported"),
                                       ("shader nothere\n", "unknown shader"),
                                       ("larea a parallel 1 1 1 1\n", "uniform"),
                                       ("p 2\n0 0 0\n1 0 0\n", "3 vertices")])
@@ -107,3 +107,40 @@ def test_float_image_writers(tmp_path):
     assert raw[:4] == bytes([0x76, 0x2F, 0x31, 0x01]) and raw[4] == 2
     write_pfm(tmp_path / "a.pfm", a, 6, 4)
     np.testing.assert_array_equal(read_pfm(tmp_path / "a.pfm")[::-1].reshape(-1), a)
+
+
+def test_yaml_scene_structure():
+    from naivetrace_b200.yaml_scene import parse_yaml_scene
+    s = parse_yaml_scene(SCENES / "room.yaml", width=32, height=24)
+    c = s.camera
+    assert (c.xres, c.yres, c.fov_deg) == (32, 24, 45.0)
+    sph, smat = s.sphere_arrays()
+    assert len(sph) == 3
+    # Scaled scope: radius x cube root of det(0.5^3) = 0.05; centre translated.
+    np.testing.assert_allclose(sph[1], [0.5, 0.98, 0.5, 0.05], atol=1e-6)
+    np.testing.assert_allclose(sph[2], [0.2, 0.2, 0.3, 0.12], atol=1e-6)
+    glass = s.materials[int(smat[0])]
+    assert glass.shader == abi.SHADER_SPECULAR_DIELECTRIC and glass.ior_ratio == pytest.approx(1.33)
+    assert glass.medium_inside == 0
+    water = s.media[0]
+    np.testing.assert_allclose(water.sigma_s, np.maximum(rgb_to_spectrum((1, 1, 1)), 0))
+    assert water.phase == abi.PHASE_HENYEY_GREENSTEIN and water.phase_g == 0.5
+    lamp = s.materials[int(smat[1])]
+    np.testing.assert_allclose(lamp.emission, rgb_to_spectrum((20, 20, 20)))
+    # The OBJ cube: faces of OBJ material `grey` map to `walls`, the others to `metal`.
+    v, n, t, mat = _tris(s)
+    kinds = sorted(s.materials[m].shader for m in mat)
+    assert kinds.count(abi.SHADER_DIFFUSE) == 6 and kinds.count(abi.SHADER_MICROFACET) == 6
+    assert [e.kind for e in s.env_lights] == [abi.ENV_SUN, abi.ENV_DOME]
+    d = np.array(s.env_lights[0].dir)
+    np.testing.assert_allclose(d, -np.array([0.2, 1, 0.1]) / np.linalg.norm([0.2, 1, 0.1]))
+    assert len(s.point_lights) == 1
+
+
+def test_nff_yaml_section():
+    text = ("yaml{\nshader:\n  class: glossy\n  name: shiny\n  alpha: 0.3\n  rgb: [1, 1, 1]\n  x: 0.5\n"
+            "material:\n  name: shinymat\n}yaml\ns 0 0 0 1\n")
+    s = parse_nff(text)
+    m = s.materials[int(s.sphere_arrays()[1][0])]
+    assert m.shader == abi.SHADER_MICROFACET and m.alpha == pytest.approx(0.3)
+    np.testing.assert_allclose(m.reflectance, rgb_to_spectrum((0.5, 0.5, 0.5)))
