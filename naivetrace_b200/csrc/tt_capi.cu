@@ -12,7 +12,9 @@
 #include <cstdlib>
 #include <memory>
 #include <mutex>
+#include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/toytrace_gpu.h"
@@ -160,6 +162,20 @@ struct tt_ctx {
   bool ps_guided = false;      // the path state carries the guiding arrays
   float bb_lo[3] = {0, 0, 0}, bb_hi[3] = {0, 0, 0};  // scene bounds (medium trackers of views)
 };
+
+// Runs f(lo, hi) over [0, n) split among up to 16 host threads (serially below 4096).
+template <class F>
+static void parallel_ranges(long long n, F&& f) {
+  const long long nt = std::min<long long>(16, std::max(1u, std::thread::hardware_concurrency()));
+  if (n < 4096 || nt <= 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const long long chunk = (n + nt - 1) / nt;
+  for (long long lo = 0; lo < n; lo += chunk) th.emplace_back([&f, lo, hi = std::min(n, lo + chunk)] { f(lo, hi); });
+  for (auto& t : th) t.join();
+}
 
 static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
   if (c) c->err = msg;
@@ -391,17 +407,40 @@ tt_status tt_upload_scene(tt_ctx* c) {
   c->path_mem.stream = c->stream;
   upload_constant_tables();
   TT_CUDA(c, cudaGetLastError());
+  // TT_UPLOAD_TIMING=1 prints the host time of the upload's phases to stderr.
+  const bool tm = std::getenv("TT_UPLOAD_TIMING") != nullptr;
+  auto t_last = std::chrono::steady_clock::now();
+  auto mark = [&](const char* what) {
+    if (!tm) return;
+    cudaStreamSynchronize(c->stream);
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "upload %-12s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - t_last).count());
+    t_last = now;
+  };
   const uint32_t ntri = (uint32_t)c->mats.size();
   // Surfaces and medium boundaries go into separate BVHs (Scene::BuildAccelStructure,
   // scene.cxx:116-141); both store global triangle ids in their slots.
   std::vector<uint32_t> sidx, smat, sid, vidx, vmat, vid;
-  for (uint32_t t = 0; t < ntri; ++t) {
-    const bool vol = c->materials[c->mats[t]].volume_boundary != 0;
-    std::vector<uint32_t>& ix = vol ? vidx : sidx;
-    ix.insert(ix.end(), &c->idx[3 * (size_t)t], &c->idx[3 * (size_t)t] + 3);
-    (vol ? vmat : smat).push_back(c->mats[t]);
-    (vol ? vid : sid).push_back(t);
+  bool any_vol = false;
+  for (const auto& m : c->materials) any_vol |= m.volume_boundary != 0;
+  if (!any_vol) {
+    sid.resize(ntri);
+    std::iota(sid.begin(), sid.end(), 0u);
+  } else {
+    for (uint32_t t = 0; t < ntri; ++t) (c->materials[c->mats[t]].volume_boundary ? vid : sid).push_back(t);
   }
+  // Index and material lists per BVH for the host builders (the device builder reads the
+  // mesh as uploaded, with the prim-id sets above).
+  auto host_split = [&]() {
+    for (uint32_t t : sid) {
+      sidx.insert(sidx.end(), &c->idx[3 * (size_t)t], &c->idx[3 * (size_t)t] + 3);
+      smat.push_back(c->mats[t]);
+    }
+    for (uint32_t t : vid) {
+      vidx.insert(vidx.end(), &c->idx[3 * (size_t)t], &c->idx[3 * (size_t)t] + 3);
+      vmat.push_back(c->mats[t]);
+    }
+  };
   std::vector<float> ssph, vsph;
   std::vector<uint32_t> ssmat, ssid, vsmat, vsid;
   const uint32_t nsph = (uint32_t)c->sphere_mats.size();
@@ -411,16 +450,20 @@ tt_status tt_upload_scene(tt_ctx* c) {
     (vol ? vsmat : ssmat).push_back(c->sphere_mats[i]);
     (vol ? vsid : ssid).push_back(ntri + i);
   }
-  BvhInput bi{c->verts.data(), sidx.data(), smat.data(), (uint32_t)sid.size(), sid.data()};
-  bi.num_spheres = (uint32_t)ssid.size();
-  bi.spheres = ssph.data();
-  bi.sphere_material_ids = ssmat.data();
-  bi.sphere_prim_ids = ssid.data();
-  BvhInput vbi{c->verts.data(), vidx.data(), vmat.data(), (uint32_t)vid.size(), vid.data()};
-  vbi.num_spheres = (uint32_t)vsid.size();
-  vbi.spheres = vsph.data();
-  vbi.sphere_material_ids = vsmat.data();
-  vbi.sphere_prim_ids = vsid.data();
+  mark("split");
+  auto host_inputs = [&](BvhInput* bi, BvhInput* vbi) {
+    host_split();
+    *bi = BvhInput{c->verts.data(), sidx.data(), smat.data(), (uint32_t)sid.size(), sid.data()};
+    bi->num_spheres = (uint32_t)ssid.size();
+    bi->spheres = ssph.data();
+    bi->sphere_material_ids = ssmat.data();
+    bi->sphere_prim_ids = ssid.data();
+    *vbi = BvhInput{c->verts.data(), vidx.data(), vmat.data(), (uint32_t)vid.size(), vid.data()};
+    vbi->num_spheres = (uint32_t)vsid.size();
+    vbi->spheres = vsph.data();
+    vbi->sphere_material_ids = vsmat.data();
+    vbi->sphere_prim_ids = vsid.data();
+  };
   auto upload = [&](const void* src, size_t bytes) -> void* {
     void* p = c->scene_mem.alloc(bytes);
     if (p && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
@@ -436,6 +479,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
   // host binned-SAH builder.
   const char* build_env = std::getenv("TT_BVH_BUILD");
   if (s.wide) {
+    BvhInput bi{}, vbi{};
+    host_inputs(&bi, &vbi);
     Bvh8Output bo, vbo;
     if (!build_bvh8(bi, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
     if (!build_bvh8(vbi, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
@@ -499,6 +544,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
     s.vnodes = vb.nodes;
     s.vtris = vb.tris;
   } else {
+    BvhInput bi{}, vbi{};
+    host_inputs(&bi, &vbi);
     BvhOutput bo, vbo;
     if (!build_bvh(bi, 4, &bo)) return fail(c, TT_ERR_INVALID, "BVH build failed");
     if (!build_bvh(vbi, 4, &vbo)) return fail(c, TT_ERR_INVALID, "medium-boundary BVH build failed");
@@ -516,13 +563,16 @@ tt_status tt_upload_scene(tt_ctx* c) {
   s.num_spheres = (int)nsph;
   // Per global primitive: vertex indices and material (spheres: material only).
   std::vector<uint32_t> ti(4 * ((size_t)ntri + nsph), 0u);
-  for (uint32_t t = 0; t < ntri; ++t) {
-    ti[4 * t] = c->idx[3 * t];
-    ti[4 * t + 1] = c->idx[3 * t + 1];
-    ti[4 * t + 2] = c->idx[3 * t + 2];
-    ti[4 * t + 3] = c->mats[t];
-  }
+  parallel_ranges(ntri, [&](long long lo, long long hi) {
+    for (long long t = lo; t < hi; ++t) {
+      ti[4 * t] = c->idx[3 * t];
+      ti[4 * t + 1] = c->idx[3 * t + 1];
+      ti[4 * t + 2] = c->idx[3 * t + 2];
+      ti[4 * t + 3] = c->mats[t];
+    }
+  });
   for (uint32_t i = 0; i < nsph; ++i) ti[4 * ((size_t)ntri + i) + 3] = c->sphere_mats[i];
+  mark("bvh");
   s.tri_idx = (const uint4*)upload(ti.data(), ti.size() * sizeof(uint32_t));
   s.normals = c->normals.empty() ? nullptr : (const float*)upload(c->normals.data(), c->normals.size() * sizeof(float));
   s.num_tris = (int)(sid.size() + ssid.size());
@@ -607,6 +657,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     const float rec[12] = {q[0], q[1], q[2], 1.f, q[3], 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     av.insert(av.end(), rec, rec + 12);
   }
+  mark("tables");
   s.area_lights = (const int*)upload(al.data(), al.size() * sizeof(int));
   s.area_verts = (const float4*)upload(av.data(), av.size() * sizeof(float));
   s.num_area_lights = (int)al.size();
@@ -656,20 +707,24 @@ tt_status tt_upload_scene(tt_ctx* c) {
       const int w = e.tex_width, h = e.tex_height;
       const std::vector<float>& tex = c->envs[i].tex;
       std::vector<float> rows(h), cols((size_t)w * h);
-      for (int y = 0; y < h; ++y) {
-        double row_weight = 0.;
-        for (int x = 0; x < w; ++x) {
-          const float* px = &tex[3 * ((size_t)y * w + x)];
-          const double mean = ((double)px[0] + px[1] + px[2]) / 3.;
+      std::atomic<bool> zero_row{false};
+      parallel_ranges(h, [&](long long y0, long long y1) {
+        for (long long y = y0; y < y1; ++y) {
           const float v = ((float)(h - 1 - y) + 0.5f) / h;
-          const float theta = v * (float)M_PI;
-          row_weight += std::sin(theta) * mean;
-          cols[(size_t)y * w + x] = (float)row_weight;
+          const double sin_theta = std::sin(v * (float)M_PI);
+          double row_weight = 0.;
+          for (int x = 0; x < w; ++x) {
+            const float* px = &tex[3 * ((size_t)y * w + x)];
+            const double mean = ((double)px[0] + px[1] + px[2]) / 3.;
+            row_weight += sin_theta * mean;
+            cols[(size_t)y * w + x] = (float)row_weight;
+          }
+          if (!(row_weight > 0.)) zero_row = true;
+          for (int x = 0; x < w; ++x) cols[(size_t)y * w + x] /= (float)row_weight;
+          rows[y] = (float)row_weight;
         }
-        if (!(row_weight > 0.)) return fail(c, TT_ERR_INVALID, "env map row with zero weight");
-        for (int x = 0; x < w; ++x) cols[(size_t)y * w + x] /= (float)row_weight;
-        rows[y] = (float)row_weight;
-      }
+      });
+      if (zero_row) return fail(c, TT_ERR_INVALID, "env map row with zero weight");
       for (int y = 1; y < h; ++y) rows[y] += rows[y - 1];
       const float inv = 1.f / rows[h - 1];
       for (int y = 0; y < h; ++y) rows[y] *= inv;
@@ -744,6 +799,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     TT_CUDA(c, cudaStreamSynchronize(c->stream));
     s.cam_track = h_track;
   }
+  mark("lights+env");
   // Framebuffers and counters.
   const size_t n3 = 3 * (size_t)c->npix;
   c->fb.accum = (float*)c->scene_mem.alloc(n3 * sizeof(float));
@@ -763,6 +819,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   c->grid = sms * kernel_blocks_per_sm();
   c->rounds = c->params.max_ray_depth;
   TT_CUDA(c, cudaDeviceSynchronize());
+  mark("framebuffer");
   c->uploaded = true;
   return TT_OK;
 }
