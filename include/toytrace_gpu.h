@@ -376,6 +376,9 @@ tt_status tt_guide_get_params(tt_ctx* ctx, float* out, int32_t n);
 tt_status tt_guide_set_params(tt_ctx* ctx, const float* in, int32_t n);
 /* Network outputs (n x 48) for n rows of 96 input features (host buffers). */
 tt_status tt_guide_forward_batch(tt_ctx* ctx, const float* features, int32_t n, float* out);
+/* The same forward pass on the tcgen05 tensor cores (128-row tiles, accumulators in tensor
+ * memory); TT_ERR_LOOP_CAP if a wait on the tensor cores timed out. */
+tt_status tt_guide_forward_batch_tc(tt_ctx* ctx, const float* features, int32_t n, float* out);
 /* Mean-loss gradient (tt_guide_num_params floats) and the loss for n training records of
  * 14 floats each: position in [0,1]^3, normal, outgoing direction, sampled direction,
  * BSDF pdf of the sampled direction, F/q (host buffers). */

@@ -228,6 +228,7 @@ EXPORTED_SYMBOLS = [
     "tt_guide_features_batch",
     "tt_render_views",
     "tt_autotune_views",
+    "tt_guide_forward_batch_tc",
     "tt_guide_tree_info",
     "tt_guide_tree_mixtures",
     "tt_guide_tree_lookup_batch",
@@ -340,6 +341,7 @@ def load_library() -> C.CDLL:
         "tt_guide_features_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
         "tt_render_views": ([vp, P(View), C.c_int32, C.c_uint64, P(C.c_float)], C.c_int32),
         "tt_autotune_views": ([vp, P(View), C.c_int32, P(TuneResult)], C.c_int32),
+        "tt_guide_forward_batch_tc": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
         "tt_guide_tree_info": ([vp, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int64)], C.c_int32),
         "tt_guide_tree_mixtures": ([vp, P(C.c_float), C.c_int32], C.c_int32),
         "tt_guide_tree_lookup_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_int32)], C.c_int32),

@@ -193,10 +193,13 @@ class GpuContext:
         p = np.ascontiguousarray(params, dtype=np.float32)
         self._check(self.lib.tt_guide_set_params(self.h, _fp(p), len(p)), "tt_guide_set_params")
 
-    def guide_forward(self, features: np.ndarray) -> np.ndarray:
+    def guide_forward(self, features: np.ndarray, tcgen05: bool = False) -> np.ndarray:
+        """Network outputs (n x 48) of feature rows (n x 96); `tcgen05` runs the tensor-core
+        kernel instead of the warp-level mma.sync one."""
         x = np.ascontiguousarray(features, dtype=np.float32).reshape(-1, 96)
         out = np.zeros((len(x), 48), np.float32)
-        self._check(self.lib.tt_guide_forward_batch(self.h, _fp(x), len(x), _fp(out)), "tt_guide_forward_batch")
+        name = "tt_guide_forward_batch_tc" if tcgen05 else "tt_guide_forward_batch"
+        self._check(getattr(self.lib, name)(self.h, _fp(x), len(x), _fp(out)), name)
         return out
 
     def guide_gradient(self, records: np.ndarray):

@@ -1550,7 +1550,7 @@ tt_status tt_guide_set_params(tt_ctx* c, const float* in, int32_t n) {
   return TT_OK;
 }
 
-tt_status tt_guide_forward_batch(tt_ctx* c, const float* features, int32_t n, float* out) {
+static tt_status guide_forward(tt_ctx* c, const float* features, int32_t n, float* out, bool tcgen05) {
   tt_status st = guide_prep(c);
   if (st != TT_OK) return st;
   if (!features || !out || n <= 0) return fail(c, TT_ERR_INVALID, "bad batch");
@@ -1559,11 +1559,24 @@ tt_status tt_guide_forward_batch(tt_ctx* c, const float* features, int32_t n, fl
   std::vector<__nv_bfloat16> x((size_t)n * kGIn);
   for (size_t i = 0; i < x.size(); ++i) x[i] = __float2bfloat16(features[i]);
   TT_CUDA(c, cudaMemcpy(c->gnet->x0, x.data(), x.size() * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice));
-  c->gnet->forward(c->gnet->x0, n, c->gnet->out, c->stream);
+  if (tcgen05) {
+    if (!c->gnet->forward_tc(c->gnet->x0, n, c->gnet->out, c->stream))
+      return fail(c, TT_ERR_LOOP_CAP, "tensor-core forward: a wait timed out");
+  } else {
+    c->gnet->forward(c->gnet->x0, n, c->gnet->out, c->stream);
+  }
   TT_CUDA(c, cudaStreamSynchronize(c->stream));
   TT_CUDA(c, cudaGetLastError());
   TT_CUDA(c, cudaMemcpy(out, c->gnet->out, (size_t)n * kGOut * sizeof(float), cudaMemcpyDeviceToHost));
   return TT_OK;
+}
+
+tt_status tt_guide_forward_batch(tt_ctx* c, const float* features, int32_t n, float* out) {
+  return guide_forward(c, features, n, out, false);
+}
+
+tt_status tt_guide_forward_batch_tc(tt_ctx* c, const float* features, int32_t n, float* out) {
+  return guide_forward(c, features, n, out, true);
 }
 
 // Copies n host records to a temporary device buffer, runs `steps` gradients (and Adam

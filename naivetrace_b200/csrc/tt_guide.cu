@@ -25,6 +25,7 @@
 
 #include "tt_guide.cuh"
 #include "tt_guide.h"
+#include "tt_guide_tc.cuh"
 #include "tt_internal.h"
 
 namespace tt {
@@ -350,6 +351,30 @@ __global__ void __launch_bounds__(kFwdWarps * 32) k_forward_x(const bf16* __rest
   }
 }
 
+// The same forward pass on the tcgen05 tensor cores: each CTA (persistent) runs kTcChains
+// independent chains of 128-row tiles over one shared copy of the weights.
+__global__ void __launch_bounds__(kTcThreads) k_forward_tc(const bf16* __restrict__ x, int n, const bf16* __restrict__ w16,
+                                                           const float* __restrict__ w32, float* __restrict__ out,
+                                                           unsigned* err) {
+  extern __shared__ __align__(128) unsigned char tsm[];
+  const TcChain c = tc_setup(tsm);
+  tc_load_weights(w16, w32, tsm);
+  __syncthreads();
+  uint32_t phase = 0;
+  bool ok = true;
+  const int tiles = (n + kTcRows - 1) / kTcRows;
+  const int g = threadIdx.x / kTcRows;
+  for (int t = blockIdx.x * kTcChains + g; t < tiles; t += gridDim.x * kTcChains) {
+    const long long r0 = (long long)t * kTcRows;
+    tc_load_x(x, r0, n, tsm, c);
+    ok = tc_mlp_tile(tsm, c, phase) && ok;
+    tc_store_out(tsm, r0, n, out, c);
+    tc_chain_sync(c);  // the buffer is read out before the next tile's features land there
+  }
+  if (!ok) atomicOr(err, kTcErrTimeout);
+  tc_teardown(tsm);
+}
+
 // Feature rows (BF16, kGIn) of n points given as 9 floats (p01, normal, wo): the input
 // fragments the kernels above build, stored.
 __global__ void __launch_bounds__(128) k_features(const float* __restrict__ pts, int n, bf16* __restrict__ x) {
@@ -426,6 +451,7 @@ void GuideNet::release() {
   scratch.clear();
   params = adam_m = adam_v = grad = loss = nullptr;
   params16 = nullptr;
+  tc_err = nullptr;
   cap = 0;
 }
 
@@ -525,6 +551,26 @@ void GuideNet::forward(const bf16* x, int n, float* out_rows, cudaStream_t st) {
   const int grid = persistent_grid((const void*)k_forward_x, kFwdWarps * 32, kFwdSmem,
                                    (n + kFwdWarps * 16 - 1) / (kFwdWarps * 16));
   k_forward_x<<<grid, kFwdWarps * 32, kFwdSmem, st>>>(x, n, params16, params, out_rows);
+}
+
+bool GuideNet::forward_tc(const bf16* x, int n, float* out_rows, cudaStream_t st) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    attr = true;
+  }
+  if (!tc_err) {
+    if (cudaMalloc(&tc_err, sizeof(unsigned)) != cudaSuccess) return false;
+    allocs.push_back(tc_err);
+  }
+  cudaMemsetAsync(tc_err, 0, sizeof(unsigned), st);
+  const int grid = persistent_grid((const void*)k_forward_tc, kTcThreads, kTcSmem,
+                                   (n + kTcThreads - 1) / kTcThreads);
+  k_forward_tc<<<grid, kTcThreads, kTcSmem, st>>>(x, n, params16, params, out_rows, tc_err);
+  unsigned e = 0;
+  cudaMemcpyAsync(&e, tc_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  return e == 0;
 }
 
 void GuideNet::features(const float* pts, int n, bf16* x, cudaStream_t st) {

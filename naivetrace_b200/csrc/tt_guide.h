@@ -40,6 +40,10 @@ struct GuideNet {
   bool ensure_capacity(int n, std::string* err);
   // Forward pass of n rows of BF16 features into FP32 outputs.
   void forward(const __nv_bfloat16* x, int n, float* out_rows, cudaStream_t st);
+  // The same on the tcgen05 tensor cores (tt_guide_tc.cuh); synchronous; false when a wait
+  // on the tensor cores timed out.
+  bool forward_tc(const __nv_bfloat16* x, int n, float* out_rows, cudaStream_t st);
+  unsigned* tc_err = nullptr;
   // Feature rows of n points (9 floats each: position in [0,1]^3, normal, outgoing direction).
   void features(const float* pts, int n, __nv_bfloat16* x, cudaStream_t st);
   // Mean-loss gradient over n records into `grad` and the loss into `loss`.

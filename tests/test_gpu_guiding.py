@@ -71,6 +71,24 @@ def test_forward_matches_oracle(gpu_lib):
     assert np.linalg.norm(og - of) / np.linalg.norm(of) < 3e-2
 
 
+@pytest.mark.parametrize("n", [3000, 100000])
+def test_forward_tcgen05_matches(gpu_lib, n):
+    """The tensor-core forward (128-row tiles, ragged last tile; 100000 rows give more tiles
+    than the resident chains) against the mma.sync forward and the oracle: both round the hidden
+    activations to bfloat16 and sum in FP32, so they agree to the summation order."""
+    g = _ctx()
+    p = _params()
+    g.guide_set_params(p)
+    x = G.record_features(G.random_records(n, seed=11))
+    ot = g.guide_forward(x, tcgen05=True)
+    om = g.guide_forward(x)
+    assert np.all(np.isfinite(ot))
+    assert np.linalg.norm(ot - om) / np.linalg.norm(om) < 2e-3
+    oo, _, _ = G.forward(p, x, True)
+    assert np.linalg.norm(ot - oo) / np.linalg.norm(oo) < 5e-3
+    assert g.stats()["error_flags"] == 0
+
+
 @pytest.mark.parametrize("n", [777, 9000])
 def test_gradient_matches_oracle(gpu_lib, n):
     """9000 records span 71 chunks of the split weight-gradient kernel, the last one ragged."""
