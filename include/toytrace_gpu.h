@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 6
+#define TT_ABI_VERSION 7
 
 typedef int32_t tt_status;
 enum {
@@ -364,8 +364,13 @@ typedef struct tt_guiding_params {
                                    maximisation step every 10 x prior strength records, each
                                    on that chunk alone); k > 0 = k EM iterations per round over
                                    all of the round's records of the cell */
+  int32_t network;              /* TT_GUIDE_LEARNED: the kernel that evaluates the network during
+                                   rendering, TT_GUIDE_NET_TCGEN05 (tensor-memory accumulators,
+                                   128-row tiles) or TT_GUIDE_NET_MMA (warp-level mma.sync,
+                                   16-row tiles); both give the same outputs */
 } tt_guiding_params;
 enum { TT_GUIDE_LEARNED = 0, TT_GUIDE_TREE = 1 };
+enum { TT_GUIDE_NET_TCGEN05 = 0, TT_GUIDE_NET_MMA = 1 };
 
 /* Enables or disables guiding.  The network is created (He-uniform weights from `seed`) on
  * first use and keeps its trained weights while guiding is switched off and on again. */

@@ -238,6 +238,8 @@ EXPORTED_SYMBOLS = [
 
 GUIDE_LEARNED = 0
 GUIDE_TREE = 1
+GUIDE_NET_TCGEN05 = 0
+GUIDE_NET_MMA = 1
 
 
 class View(C.Structure):
@@ -272,6 +274,7 @@ class GuidingParams(C.Structure):
         ("method", C.c_int32),
         ("tree_subdivision", C.c_int32),
         ("tree_em_iters", C.c_int32),
+        ("network", C.c_int32),
     ]
 
 

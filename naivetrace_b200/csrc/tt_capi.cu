@@ -1463,7 +1463,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || gp->max_depth < 0 ||
       !(gp->learning_rate >= 0.f) || gp->train < 0 || gp->train > 2 ||
       (gp->method != TT_GUIDE_LEARNED && gp->method != TT_GUIDE_TREE) || gp->tree_subdivision < 0 ||
-      gp->tree_em_iters < 0)
+      gp->tree_em_iters < 0 || (gp->network != TT_GUIDE_NET_TCGEN05 && gp->network != TT_GUIDE_NET_MMA))
     return fail(c, TT_ERR_INVALID, "bad guiding parameters");
   const int cap = gp->record_pool > 0 ? gp->record_pool : (1 << 16);
   if (gp->method == TT_GUIDE_TREE && !c->tree) {
@@ -1506,6 +1506,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   c->dev.guide_w32 = c->gnet->params;
   c->dev.guide = 1;
   c->dev.guide_method = gp->method;
+  c->dev.guide_net = gp->network;
   if (gp->method == TT_GUIDE_TREE) {
     c->dev.tree_nodes = c->tree->d_nodes;
     c->dev.tree_root = c->tree->root_ref();

@@ -17,6 +17,7 @@ constexpr int BVH8_STACK = 32;       // per-thread stack of node groups, 8-wide 
 constexpr uint32_t ERR_STACK = 1u;   // error-word bits written by kernels
 constexpr uint32_t ERR_QUEUE = 2u;
 constexpr uint32_t ERR_CROSSINGS = 4u;  // a ray crossed more medium boundaries than the cap
+constexpr uint32_t ERR_TENSOR = 8u;     // a wait on the tcgen05 tensor cores gave up
 constexpr int kMaxCrossings = 256;      // boundary crossings followed along one ray
 constexpr int kMaxMedia = 254;          // medium indices are stored in bytes (0xff = empty)
 constexpr int kCountersPerBounce = 4;  // ext, shadow, done, guided queue lengths
@@ -139,6 +140,7 @@ struct DevScene {
   // axis, child0, child1 as int bits; a child < 0 is ~cell), the root reference and the
   // cells' mixtures (40 floats each: weights[8], means[8][3], concentrations[8]).
   int guide_method;
+  int guide_net;  // TT_GUIDE_NET_TCGEN05 or TT_GUIDE_NET_MMA: the kernel that runs the network
   const float4* tree_nodes;
   int tree_root;
   const float* tree_mix;

@@ -22,6 +22,7 @@
 
 #include "tt_device.cuh"
 #include "tt_guide.cuh"
+#include "tt_guide_tc.cuh"
 #include "tt_internal.h"
 #include "tt_tables.h"
 
@@ -1362,6 +1363,53 @@ __global__ void __launch_bounds__(kGuideWarps * 32) k_guide(DevScene sc, PathSta
   }
 }
 
+// The same on the tcgen05 tensor cores (tt_guide_tc.cuh): each CTA runs kTcChains chains of
+// 128 queue entries; a thread encodes its entry's features into the chain's tile, the chain
+// runs the network with the accumulators in tensor memory, and each thread then decodes its
+// row's outputs and scatters its entry.
+template <bool MEDIA>
+__global__ void __launch_bounds__(kTcThreads) k_guide_tc(DevScene sc, PathState p, int bounce) {
+  extern __shared__ __align__(128) unsigned char tsm[];
+  const int n = *guide_count(p, bounce);
+  if ((long long)blockIdx.x * kTcThreads >= n) return;  // uniform over the CTA
+  const TcChain c = tc_setup(tsm);
+  tc_load_weights(sc.guide_w16, sc.guide_w32, tsm);
+  __syncthreads();
+  uint32_t phase = 0;
+  bool ok = true;
+  const int g = threadIdx.x / kTcRows;
+  for (int base = (blockIdx.x * kTcChains + g) * kTcRows; base < n; base += gridDim.x * kTcThreads) {
+    const int i = base + c.row;
+    GuidePre pre;
+    float q[kGInputs];
+    if (i < n) {
+      pre = guide_prefetch(p, p.guide_q[i]);
+      const float4* gi = p.ginp + 3 * (size_t)i;
+      const float4 a = gi[0], b = gi[1], d = gi[2];
+      q[0] = a.x; q[1] = a.y; q[2] = a.z; q[3] = a.w; q[4] = b.x; q[5] = b.y; q[6] = b.z; q[7] = b.w; q[8] = d.x;
+    } else {
+#pragma unroll
+      for (int k = 0; k < kGInputs; ++k) q[k] = 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < kGIn; k += 8)
+      *reinterpret_cast<uint4*>(tsm + c.xo + tc_off(c.row, k, kGIn)) =
+          make_uint4(guide_feature_pair(q, k), guide_feature_pair(q, k + 2), guide_feature_pair(q, k + 4),
+                     guide_feature_pair(q, k + 6));
+    ok = tc_mlp_tile(tsm, c, phase) && ok;
+    float o[kGOut];
+#pragma unroll
+    for (int k = 0; k < kGOut / 4; ++k) {
+      const float4 v = *tc_out_slot(tsm, c.xo, c.row, k);
+      o[4 * k] = v.x; o[4 * k + 1] = v.y; o[4 * k + 2] = v.z; o[4 * k + 3] = v.w;
+    }
+    tc_chain_sync(c);  // the outputs are read out before the next entries' features land there
+    if (i < n) guide_scatter_one<MEDIA>(sc, p, bounce, pre, o);
+  }
+  if (!ok) atomicOr(p.err, ERR_TENSOR);
+  tc_teardown(tsm);
+}
+
 // Occlusion test of the queued shadow rays.  Unoccluded rays add their contribution to
 // the path (or, for camera-vertex samples, splat it to the pixel they project to).  In
 // media scenes the contribution is multiplied by the transmittance through the media
@@ -1743,15 +1791,22 @@ void launch_resolve_views(const float* accum, const float* light, const DevView*
 
 static int g_guide_grid = 0;
 
+static int g_guide_tc_grid = 0;
+
 void prepare_guide_launch() {
   if (g_guide_grid != 0) return;
   cudaFuncSetAttribute(k_guide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
   cudaFuncSetAttribute(k_guide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
+  cudaFuncSetAttribute(k_guide_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+  cudaFuncSetAttribute(k_guide_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide<true>, kGuideWarps * 32, kGuideSmem);
   g_guide_grid = sms * (per_sm > 0 ? per_sm : 1);
+  per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_tc<true>, kTcThreads, kTcSmem);
+  g_guide_tc_grid = sms * (per_sm > 0 ? per_sm : 1);
 }
 
 void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st) {
@@ -1769,6 +1824,11 @@ void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_
     return;
   }
   prepare_guide_launch();
+  if (s.guide_net == TT_GUIDE_NET_TCGEN05) {
+    if (s.num_media > 0) k_guide_tc<true><<<g_guide_tc_grid, kTcThreads, kTcSmem, st>>>(s, p, bounce);
+    else k_guide_tc<false><<<g_guide_tc_grid, kTcThreads, kTcSmem, st>>>(s, p, bounce);
+    return;
+  }
   const int grid = g_guide_grid;
   if (s.num_media > 0) k_guide<true><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
   else k_guide<false><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);

@@ -15,7 +15,7 @@ rendering against plain rendering.
 import numpy as np
 import pytest
 
-from naivetrace_b200 import scenes
+from naivetrace_b200 import abi, scenes
 from naivetrace_b200.algo import GpuContext, GpuGuidedPathTracer
 from naivetrace_b200.scene import make_params
 from oracle import guiding as G
@@ -265,3 +265,23 @@ def test_guided_algo_schedule(gpu_lib):
     assert 0 < st["guide_steps"] <= 2 * (1 + 2 + 4) and st["guide_steps"] % 2 == 0
     img = algo.generate_image()
     assert img.shape == (32, 32, 3) and img.mean() > 5
+
+
+def test_guided_render_tcgen05_matches_mma(gpu_lib):
+    """Guided renders with the network on the tcgen05 kernel and on the mma.sync kernel,
+    same weights and seeds: the two kernels give the same network outputs, so the images
+    agree to the order of the floating-point accumulation."""
+    scene = scenes.guiding_room(96, 54)
+    g = GpuContext(scene, make_params(max_ray_depth=12))
+    g.set_guiding(True, 1, seed=3, network=abi.GUIDE_NET_MMA)
+    for k in range(3):
+        g.render(4, seed=50 + k)
+    imgs = []
+    for net in (abi.GUIDE_NET_MMA, abi.GUIDE_NET_TCGEN05):
+        g.set_guiding(True, 0, seed=3, network=net)
+        g.clear()
+        g.render(8, seed=77)
+        imgs.append(g.framebuffer().astype(np.float64))
+    assert g.stats()["error_flags"] == 0
+    a, b = imgs
+    assert np.abs(a - b).max() <= 1e-5 * max(np.abs(a).max(), 1e-6), np.abs(a - b).max()
