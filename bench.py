@@ -610,17 +610,39 @@ def profile_guiding(args):
     from naivetrace_b200 import scenes
     from naivetrace_b200.algo import GpuContext
     from naivetrace_b200.scene import make_params
+    from naivetrace_b200 import abi
+    net = abi.GUIDE_NET_MMA if args.guide_net == "mma" else abi.GUIDE_NET_TCGEN05
     g = GpuContext(scenes.guiding_room(640, 360), make_params(max_ray_depth=12))
-    g.set_guiding(True, 1, seed=7)
+    g.set_guiding(True, 1, seed=7, network=net)
     for k in range(4):
         g.render(1, seed=100 + k)
-    g.set_guiding(True, 0, seed=7)
+    g.set_guiding(True, 0, seed=7, network=net)
     g.render(4, seed=3)
     st = g.stats()
     print(json.dumps({"profile_guiding": "guiding_room 640x360", "guide_steps": st["guide_steps"],
                       "guide_records": st["guide_records"], "error_flags": st["error_flags"]}))
     g.close()
     return 0 if st["error_flags"] == 0 else 1
+
+
+def profile_network(args):
+    """No timing: the guiding network's forward pass on 2^20 feature rows, three times through
+    the tcgen05 kernel and three times through the mma.sync kernel (for ncu launch lists)."""
+    from naivetrace_b200 import scenes
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    g = GpuContext(scenes.guiding_room(16, 16), make_params(max_ray_depth=12))
+    g.set_guiding(True, 1, seed=7)
+    x = np.random.default_rng(1).uniform(-1.0, 1.0, (1 << 20, 96)).astype(np.float32)
+    outs = []
+    for _ in range(3):
+        outs.append(g.guide_forward(x, tcgen05=True))
+        outs.append(g.guide_forward(x))
+    same = all(np.array_equal(outs[0], o) for o in outs)
+    finite = all(np.isfinite(o).all() for o in outs)
+    print(json.dumps({"profile_network": "2^20 rows", "tcgen05_equals_mma": bool(same), "finite": bool(finite)}))
+    g.close()
+    return 0 if finite else 1
 
 
 def main(argv=None):
@@ -643,6 +665,10 @@ def main(argv=None):
     ap.add_argument("--small", action="store_true", help="scaled-down scene (for profiling captures)")
     ap.add_argument("--profile-guiding", action="store_true",
                     help="no timing: training and frozen passes of the guiding workload (for ncu captures)")
+    ap.add_argument("--guide-net", choices=["tcgen05", "mma"], default="tcgen05",
+                    help="network kernel of --profile-guiding")
+    ap.add_argument("--profile-network", action="store_true",
+                    help="no timing: the guiding network's forward pass through both kernels (for ncu launch lists)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing: upload the workload and render one pass of --spp samples (for ncu captures)")
     args = ap.parse_args(argv)
@@ -650,6 +676,8 @@ def main(argv=None):
         return profile_run(args)
     if args.profile_guiding:
         return profile_guiding(args)
+    if args.profile_network:
+        return profile_network(args)
     if args.profile_views:
         return profile_views(args)
     if args.warmup < 3 and not args.small:
