@@ -66,6 +66,21 @@ struct DeviceBuffers {
 std::mutex g_pool_mutex;
 cudaMemPool_t g_pools[64] = {nullptr};
 
+// Primitive ids 0 .. n - 1 (the surface set of a mesh without medium boundaries).
+__global__ void k_iota(uint32_t* out, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = i;
+}
+
+// Per global primitive: vertex indices and material (spheres after the triangles: material
+// only), from the mesh as uploaded for the device BVH build.
+__global__ void k_prim_table(const uint32_t* __restrict__ idx, const uint32_t* __restrict__ mats, uint32_t ntri,
+                             const uint32_t* __restrict__ sphere_mats, uint32_t nsph, uint4* __restrict__ out) {
+  const uint32_t n = ntri + nsph;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    out[i] = i < ntri ? make_uint4(idx[3 * (size_t)i], idx[3 * (size_t)i + 1], idx[3 * (size_t)i + 2], mats[i])
+                      : make_uint4(0u, 0u, 0u, sphere_mats[i - ntri]);
+}
+
 __global__ void k_tally(const int* counters, int rounds, unsigned long long* stats) {
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     unsigned long long e = 0, s = 0;
@@ -470,6 +485,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     return p;
   };
   DevScene& s = c->dev;
+  s.tri_idx = nullptr;  // set below, by the device build or from the host table
   // The binary BVH is the default layout; TT_BVH_WIDTH=8 selects the 8-wide compressed
   // BVH (80-byte nodes, about half the bytes per ray but more arithmetic per node, which
   // measured a few percent slower on the terrain workload).
@@ -502,9 +518,28 @@ tt_status tt_upload_scene(tt_ctx* c) {
       if (p && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
       return p;
     };
-    std::vector<uint32_t> sset(sid), vset(vid);
-    sset.insert(sset.end(), ssid.begin(), ssid.end());
-    vset.insert(vset.end(), vsid.begin(), vsid.end());
+    // Prim-id sets: the triangle ids, then the sphere ids (generated on the device when the
+    // surface set is every triangle).
+    const size_t ns = sid.size() + ssid.size(), nv = vid.size() + vsid.size();
+    uint32_t* d_sset = (uint32_t*)tmp.alloc(ns * sizeof(uint32_t));
+    uint32_t* d_vset = (uint32_t*)tmp.alloc(nv * sizeof(uint32_t));
+    if (d_sset) {
+      if (!any_vol) {
+        if (ntri) k_iota<<<std::min<uint32_t>(4096, (ntri + 255) / 256), 256, 0, c->stream>>>(d_sset, ntri);
+      } else if (!sid.empty()) {
+        cudaMemcpyAsync(d_sset, sid.data(), sid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+      }
+      if (!ssid.empty())
+        cudaMemcpyAsync(d_sset + sid.size(), ssid.data(), ssid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                        c->stream);
+    }
+    if (d_vset) {
+      if (!vid.empty())
+        cudaMemcpyAsync(d_vset, vid.data(), vid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
+      if (!vsid.empty())
+        cudaMemcpyAsync(d_vset + vid.size(), vsid.data(), vsid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                        c->stream);
+    }
     BuildInput in{};
     in.vertices = (const float*)up(c->verts.data(), c->verts.size() * sizeof(float));
     in.indices = (const uint32_t*)up(c->idx.data(), c->idx.size() * sizeof(uint32_t));
@@ -512,8 +547,6 @@ tt_status tt_upload_scene(tt_ctx* c) {
     in.num_triangles = ntri;
     in.spheres = (const float*)up(c->spheres.data(), c->spheres.size() * sizeof(float));
     in.sphere_material_ids = (const uint32_t*)up(c->sphere_mats.data(), c->sphere_mats.size() * sizeof(uint32_t));
-    const uint32_t* d_sset = (const uint32_t*)up(sset.data(), sset.size() * sizeof(uint32_t));
-    const uint32_t* d_vset = (const uint32_t*)up(vset.data(), vset.size() * sizeof(uint32_t));
     for (void* p : tmp.allocs)
       if (!p) {
         tmp.free_all();
@@ -522,14 +555,22 @@ tt_status tt_upload_scene(tt_ctx* c) {
     DeviceBvh sb{}, vb{};
     std::string berr;
     in.prim_ids = d_sset;
-    bool built = device_build_bvh2(in, d_sset, (uint32_t)sset.size(), &sb, c->stream, &berr);
+    bool built = device_build_bvh2(in, d_sset, (uint32_t)ns, &sb, c->stream, &berr);
     if (sb.nodes) c->scene_mem.allocs.push_back(sb.nodes);
     if (sb.tris) c->scene_mem.allocs.push_back(sb.tris);
     if (built) {
       in.prim_ids = d_vset;
-      built = device_build_bvh2(in, d_vset, (uint32_t)vset.size(), &vb, c->stream, &berr);
+      built = device_build_bvh2(in, d_vset, (uint32_t)nv, &vb, c->stream, &berr);
       if (vb.nodes) c->scene_mem.allocs.push_back(vb.nodes);
       if (vb.tris) c->scene_mem.allocs.push_back(vb.tris);
+    }
+    // The primitive table from the uploaded mesh, before the mesh's buffers go.
+    if (built) {
+      uint4* table = (uint4*)c->scene_mem.alloc(((size_t)ntri + nsph) * sizeof(uint4));
+      if (table && ntri + nsph > 0)
+        k_prim_table<<<std::min<uint32_t>(4096, (ntri + nsph + 255) / 256), 256, 0, c->stream>>>(
+            in.indices, in.material_ids, ntri, in.sphere_material_ids, nsph, table);
+      s.tri_idx = table;
     }
     cudaStreamSynchronize(c->stream);
     tmp.free_all();
@@ -561,19 +602,22 @@ tt_status tt_upload_scene(tt_ctx* c) {
   }
   s.num_vol_tris = (int)(vid.size() + vsid.size());
   s.num_spheres = (int)nsph;
-  // Per global primitive: vertex indices and material (spheres: material only).
-  std::vector<uint32_t> ti(4 * ((size_t)ntri + nsph), 0u);
-  parallel_ranges(ntri, [&](long long lo, long long hi) {
-    for (long long t = lo; t < hi; ++t) {
-      ti[4 * t] = c->idx[3 * t];
-      ti[4 * t + 1] = c->idx[3 * t + 1];
-      ti[4 * t + 2] = c->idx[3 * t + 2];
-      ti[4 * t + 3] = c->mats[t];
-    }
-  });
-  for (uint32_t i = 0; i < nsph; ++i) ti[4 * ((size_t)ntri + i) + 3] = c->sphere_mats[i];
+  // Per global primitive: vertex indices and material (spheres: material only); the device
+  // build made it on the device already.
+  if (!s.tri_idx) {
+    std::vector<uint32_t> ti(4 * ((size_t)ntri + nsph), 0u);
+    parallel_ranges(ntri, [&](long long lo, long long hi) {
+      for (long long t = lo; t < hi; ++t) {
+        ti[4 * t] = c->idx[3 * t];
+        ti[4 * t + 1] = c->idx[3 * t + 1];
+        ti[4 * t + 2] = c->idx[3 * t + 2];
+        ti[4 * t + 3] = c->mats[t];
+      }
+    });
+    for (uint32_t i = 0; i < nsph; ++i) ti[4 * ((size_t)ntri + i) + 3] = c->sphere_mats[i];
+    s.tri_idx = (const uint4*)upload(ti.data(), ti.size() * sizeof(uint32_t));
+  }
   mark("bvh");
-  s.tri_idx = (const uint4*)upload(ti.data(), ti.size() * sizeof(uint32_t));
   s.normals = c->normals.empty() ? nullptr : (const float*)upload(c->normals.data(), c->normals.size() * sizeof(float));
   s.num_tris = (int)(sid.size() + ssid.size());
   // Materials.
@@ -637,7 +681,9 @@ tt_status tt_upload_scene(tt_ctx* c) {
   // (Scene::UpdateEmissiveIndexOffset numbers emissive primitives consecutively).
   std::vector<int> al;
   std::vector<float> av;
-  for (uint32_t t = 0; t < ntri; ++t) {
+  bool any_emitter = false;
+  for (const auto& m : c->materials) any_emitter |= m.emissive && !m.volume_boundary;
+  for (uint32_t t = 0; any_emitter && t < ntri; ++t) {
     const tt_material& mt = c->materials[c->mats[t]];
     if (!mt.emissive || mt.volume_boundary) continue;
     al.push_back((int)t);
@@ -747,11 +793,20 @@ tt_status tt_upload_scene(tt_ctx* c) {
   s.type_probs[3] = 0.f;
   s.in_class_area = na > 0 ? (float)(1. / na) : 0.f;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (size_t v = 0; v < c->verts.size() / 3; ++v)
+  std::mutex box_mutex;
+  parallel_ranges((long long)(c->verts.size() / 3), [&](long long v0, long long v1) {
+    float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (long long v = v0; v < v1; ++v)
+      for (int k = 0; k < 3; ++k) {
+        l[k] = std::min(l[k], c->verts[3 * v + k]);
+        h[k] = std::max(h[k], c->verts[3 * v + k]);
+      }
+    std::lock_guard<std::mutex> g(box_mutex);
     for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], (double)c->verts[3 * v + k]);
-      hi[k] = std::max(hi[k], (double)c->verts[3 * v + k]);
+      lo[k] = std::min(lo[k], (double)l[k]);
+      hi[k] = std::max(hi[k], (double)h[k]);
     }
+  });
   for (uint32_t i = 0; i < nsph; ++i)
     for (int k = 0; k < 3; ++k) {
       lo[k] = std::min(lo[k], (double)c->spheres[4 * (size_t)i + k] - c->spheres[4 * (size_t)i + 3]);

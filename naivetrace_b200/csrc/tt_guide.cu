@@ -356,9 +356,9 @@ __global__ void __launch_bounds__(kFwdWarps * 32) k_forward_x(const bf16* __rest
 __global__ void __launch_bounds__(kTcThreads) k_forward_tc(const bf16* __restrict__ x, int n, const bf16* __restrict__ w16,
                                                            const float* __restrict__ w32, float* __restrict__ out,
                                                            unsigned* err) {
-  extern __shared__ __align__(128) unsigned char tsm[];
-  const TcChain c = tc_setup(tsm);
-  tc_load_weights(w16, w32, tsm);
+  extern __shared__ __align__(128) unsigned char csm[];
+  const TcChain c = tc_setup(csm);
+  tc_load_weights(w16, w32, csm);
   __syncthreads();
   uint32_t phase = 0;
   bool ok = true;
@@ -366,13 +366,13 @@ __global__ void __launch_bounds__(kTcThreads) k_forward_tc(const bf16* __restric
   const int g = threadIdx.x / kTcRows;
   for (int t = blockIdx.x * kTcChains + g; t < tiles; t += gridDim.x * kTcChains) {
     const long long r0 = (long long)t * kTcRows;
-    tc_load_x(x, r0, n, tsm, c);
-    ok = tc_mlp_tile(tsm, c, phase) && ok;
-    tc_store_out(tsm, r0, n, out, c);
+    tc_load_x(x, r0, n, csm, c);
+    ok = tc_mlp_tile(csm, c, phase) && ok;
+    tc_store_out(csm, r0, n, out, c);
     tc_chain_sync(c);  // the buffer is read out before the next tile's features land there
   }
   if (!ok) atomicOr(err, kTcErrTimeout);
-  tc_teardown(tsm);
+  tc_teardown(csm);
 }
 
 // Feature rows (BF16, kGIn) of n points given as 9 floats (p01, normal, wo): the input
