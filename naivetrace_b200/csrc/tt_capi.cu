@@ -41,9 +41,32 @@ constexpr int kDefaultWave = 1 << 26;
 std::mutex g_err_mutex;
 std::string g_create_error;
 
+// Allocator that leaves new elements uninitialised, so that the scene copies of tt_create
+// touch their pages once, from the threads that fill them.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+  template <class U>
+  struct rebind {
+    using other = NoInitAlloc<U>;
+  };
+  NoInitAlloc() = default;
+  template <class U>
+  NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  template <class U>
+  void construct(U* p) noexcept {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <class U, class... A>
+  void construct(U* p, A&&... a) {
+    ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+  }
+};
+template <class T>
+using HostArray = std::vector<T, NoInitAlloc<T>>;
+
 struct HostEnv {
   tt_env_light desc;
-  std::vector<float> tex;
+  HostArray<float> tex;
 };
 
 // Device buffers owned by a context, from the library's memory pool, ordered on `stream`.
@@ -126,8 +149,8 @@ void pool_free(void* p, cudaStream_t st) {
 
 struct tt_ctx {
   // Host copy of the scene.
-  std::vector<float> verts, normals;
-  std::vector<uint32_t> idx, mats;
+  HostArray<float> verts, normals;
+  HostArray<uint32_t> idx, mats;
   std::vector<tt_material> materials;
   std::vector<tt_medium> media;
   std::vector<std::vector<float>> media_tables;  // per medium: sigma_t, molecules, aerosols (rows x 36 each)
@@ -190,6 +213,15 @@ static void parallel_ranges(long long n, F&& f) {
   const long long chunk = (n + nt - 1) / nt;
   for (long long lo = 0; lo < n; lo += chunk) th.emplace_back([&f, lo, hi = std::min(n, lo + chunk)] { f(lo, hi); });
   for (auto& t : th) t.join();
+}
+
+// dst = src[0 .. n), copied by parallel_ranges' threads.
+template <class T>
+static void parallel_copy(HostArray<T>& dst, const T* src, size_t n) {
+  dst.resize(n);
+  parallel_ranges((long long)n, [&](long long lo, long long hi) {
+    std::memcpy(dst.data() + lo, src + lo, (size_t)(hi - lo) * sizeof(T));
+  });
 }
 
 static tt_status fail(tt_ctx* c, tt_status s, const std::string& msg) {
@@ -309,12 +341,28 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   if (p->algo == TT_ALGO_PT2 && p->qmc && (p->max_ray_depth <= 0 ? 25 : p->max_ray_depth) > 31)
     return fail(nullptr, TT_ERR_INVALID, "qmc needs max_ray_depth <= 31 (64 sampler subsequences)");
   if (p->max_ray_depth > 1000) return fail(nullptr, TT_ERR_INVALID, "max_ray_depth above 1000");
-  for (uint32_t t = 0; t < d->num_triangles; ++t) {
-    for (int k = 0; k < 3; ++k)
-      if (d->indices[3 * (size_t)t + k] >= d->num_vertices)
+  {
+    // The first triangle with an index out of range (threads keep the smallest they see).
+    std::atomic<long long> bad{(long long)d->num_triangles};
+    parallel_ranges(d->num_triangles, [&](long long lo, long long hi) {
+      for (long long t = lo; t < hi && t < bad.load(std::memory_order_relaxed); ++t) {
+        const uint32_t* v = d->indices + 3 * (size_t)t;
+        if (v[0] >= d->num_vertices || v[1] >= d->num_vertices || v[2] >= d->num_vertices ||
+            d->material_ids[t] >= d->num_materials) {
+          long long cur = bad.load();
+          while (t < cur && !bad.compare_exchange_weak(cur, t)) {
+          }
+          break;
+        }
+      }
+    });
+    const long long t = bad.load();
+    if (t < (long long)d->num_triangles) {
+      const uint32_t* v = d->indices + 3 * (size_t)t;
+      if (v[0] >= d->num_vertices || v[1] >= d->num_vertices || v[2] >= d->num_vertices)
         return fail(nullptr, TT_ERR_INVALID, "vertex index out of range in triangle " + std::to_string(t));
-    if (d->material_ids[t] >= d->num_materials)
       return fail(nullptr, TT_ERR_INVALID, "material index out of range in triangle " + std::to_string(t));
+    }
   }
   for (uint32_t i = 0; i < d->num_materials; ++i) {
     const tt_material& m = d->materials[i];
@@ -364,10 +412,10 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
         return fail(nullptr, TT_ERR_INVALID, "medium coefficients must be finite and non-negative");
   }
   auto* c = new tt_ctx;
-  c->verts.assign(d->vertices, d->vertices + 3 * (size_t)d->num_vertices);
-  if (d->normals) c->normals.assign(d->normals, d->normals + 3 * (size_t)d->num_vertices);
-  c->idx.assign(d->indices, d->indices + 3 * (size_t)d->num_triangles);
-  c->mats.assign(d->material_ids, d->material_ids + d->num_triangles);
+  parallel_copy(c->verts, d->vertices, 3 * (size_t)d->num_vertices);
+  if (d->normals) parallel_copy(c->normals, d->normals, 3 * (size_t)d->num_vertices);
+  parallel_copy(c->idx, d->indices, 3 * (size_t)d->num_triangles);
+  parallel_copy(c->mats, d->material_ids, (size_t)d->num_triangles);
   c->materials.assign(d->materials, d->materials + d->num_materials);
   if (d->num_media > 0) c->media.assign(d->media, d->media + d->num_media);
   for (auto& m : c->media) {
@@ -397,7 +445,7 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
         delete c;
         return fail(nullptr, TT_ERR_INVALID, "env map without texture");
       }
-      e.tex.assign(e.desc.tex_rgb, e.desc.tex_rgb + 3 * (size_t)e.desc.tex_width * e.desc.tex_height);
+      parallel_copy(e.tex, e.desc.tex_rgb, 3 * (size_t)e.desc.tex_width * e.desc.tex_height);
       e.desc.tex_rgb = nullptr;
     }
     c->envs.push_back(std::move(e));
@@ -751,7 +799,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
       const float Y[3] = {b, sign + up[1] * up[1] * a, -up[1]};
       for (int k = 0; k < 3; ++k) { L.X[k] = X[k]; L.Y[k] = Y[k]; L.Z[k] = up[k]; }
       const int w = e.tex_width, h = e.tex_height;
-      const std::vector<float>& tex = c->envs[i].tex;
+      const auto& tex = c->envs[i].tex;
       std::vector<float> rows(h), cols((size_t)w * h);
       std::atomic<bool> zero_row{false};
       parallel_ranges(h, [&](long long y0, long long y1) {

@@ -74,6 +74,18 @@ def test_create_validates_without_gpu(gpu_lib):
     st, h = _create(gpu_lib, scene, make_params())
     assert st == abi.TT_ERR_INVALID and not h.value
     assert "material index" in abi.last_error(gpu_lib, None)
+    # Large meshes are checked by several threads; the error names the first bad triangle.
+    big = scenes.terrain_spheres(xres=32, yres=18, terrain_n=256, sphere_level=2, num_spheres=2, env_w=16, env_h=8)
+    tris = big.arrays()[2]
+    assert len(tris) > 100_000
+    tris[100_000, 1] = 1 << 30
+    tris[70_000, 2] = 1 << 30
+    big.arrays()[3][60_000] = 99
+    st, h = _create(gpu_lib, big, make_params())
+    assert st == abi.TT_ERR_INVALID and "material index out of range in triangle 60000" in abi.last_error(gpu_lib, None)
+    big.arrays()[3][60_000] = 0
+    st, h = _create(gpu_lib, big, make_params())
+    assert st == abi.TT_ERR_INVALID and "vertex index out of range in triangle 70000" in abi.last_error(gpu_lib, None)
     # Bad sample mode.
     st, h = _create(gpu_lib, scenes.cornell_box(8, 8), make_params(pt_sample_mode=7))
     assert st == abi.TT_ERR_INVALID
