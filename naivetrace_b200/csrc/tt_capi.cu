@@ -595,6 +595,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     in.num_triangles = ntri;
     in.spheres = (const float*)up(c->spheres.data(), c->spheres.size() * sizeof(float));
     in.sphere_material_ids = (const uint32_t*)up(c->sphere_mats.data(), c->sphere_mats.size() * sizeof(uint32_t));
+    mark("mesh H2D");
     for (void* p : tmp.allocs)
       if (!p) {
         tmp.free_all();
@@ -602,6 +603,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
       }
     DeviceBvh sb{}, vb{};
     std::string berr;
+    mark("mesh check");
     in.prim_ids = d_sset;
     bool built = device_build_bvh2(in, d_sset, (uint32_t)ns, &sb, c->stream, &berr);
     if (sb.nodes) c->scene_mem.allocs.push_back(sb.nodes);
@@ -612,6 +614,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
       if (vb.nodes) c->scene_mem.allocs.push_back(vb.nodes);
       if (vb.tris) c->scene_mem.allocs.push_back(vb.tris);
     }
+    mark("device build");
     // The primitive table from the uploaded mesh, before the mesh's buffers go.
     if (built) {
       uint4* table = (uint4*)c->scene_mem.alloc(((size_t)ntri + nsph) * sizeof(uint4));
