@@ -37,6 +37,14 @@ constexpr int kTcBar = kTcBias + (4 * kGHid + kGOut) * 4;  // one mbarrier (8 by
 constexpr int kTcTmem = kTcBar + 8 * kTcChains;            // tensor-memory address
 constexpr int kTcSmem = kTcTmem + 8;
 constexpr unsigned kTcErrTimeout = 1u << 8;                // error bit: a wait gave up
+static_assert(kTcW1 % 16 == 0 && kTcW4 % 16 == 0 && kTcX % 16 == 0 && kTcXBytes % 16 == 0,
+              "UMMA operands start on 16-byte boundaries");
+static_assert(kTcRows * kGHid * 2 <= kTcXBytes && kTcRows * kGOut * 4 <= kTcXBytes,
+              "hidden activations and staged outputs fit in a tile buffer");
+static_assert(kTcBar % 8 == 0 && kTcSmem <= 227 * 1024, "mbarriers 8-byte aligned; shared memory within a CTA's limit");
+static_assert(kTcChains * kTcCols <= 512 && ((kTcChains * kTcCols) & (kTcChains * kTcCols - 1)) == 0,
+              "a tensor-memory allocation is a power of two of at most 512 columns");
+static_assert(kGIn % 16 == 0 && kGHid % 16 == 0 && kGOut % 16 == 0, "K and N in steps of 16");
 
 // What one chain (four warps, 128 threads) of the CTA owns.
 struct TcChain {
