@@ -1066,8 +1066,7 @@ static tt_status guide_train(tt_ctx* c, long long paths) {
     for (int k = 0; k < steps; ++k) {
       c->gnet->draw_batch(c->d_records, pool, n, c->gparams.seed * 0x9e3779b97f4a7c15ull + (++c->draw_seed),
                           c->stream);
-      c->gnet->gradient(c->gnet->batch, n, c->stream);
-      c->gnet->adam(lr, c->stream);
+      c->gnet->gradient(c->gnet->batch, n, c->stream, true, lr);
     }
     cudaEventRecord(b, c->stream);
     float loss = 0.f, ms = 0.f;
@@ -1696,8 +1695,7 @@ static tt_status guide_batch(tt_ctx* c, const float* records, int32_t n, int32_t
   TT_CUDA(c, cudaMalloc(&d, (size_t)n * sizeof(GuideRecord)));
   cudaError_t e = cudaMemcpy(d, records, (size_t)n * sizeof(GuideRecord), cudaMemcpyHostToDevice);
   for (int k = 0; k < steps && e == cudaSuccess; ++k) {
-    c->gnet->gradient(d, n, c->stream);
-    if (train) c->gnet->adam(lr, c->stream);
+    c->gnet->gradient(d, n, c->stream, train, lr);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e == cudaSuccess) e = cudaGetLastError();

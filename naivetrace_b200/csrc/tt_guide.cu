@@ -11,7 +11,7 @@
 //             weight image), storing each layer's output gradient;
 //   k_wgrad   dW_l = sum over records of dH_l^T X_l and the bias sums, split over chunks of
 //             128 records (mma.sync with ldmatrix.trans fragments of both operands);
-//   k_reduce  sum of the chunk partials;
+//   k_reduce  sum of the chunk partials (k_reduce_adam: with the Adam step fused in);
 //   k_adam    Adam on the FP32 master parameters, refreshing the BF16 copy.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -394,17 +394,34 @@ __global__ void __launch_bounds__(128) k_features(const float* __restrict__ pts,
 }
 
 // Adam (Kingma and Ba 2015) on the FP32 master parameters, refreshing the BF16 copy.
-__global__ void k_adam(float* p, float* m, float* v, const float* g, int n, float lr, float b1, float b2, float eps,
-                       float bc1, float bc2, bf16* w16) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const float gi = g[i];
-    const float mi = b1 * m[i] + (1.f - b1) * gi;
-    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    const float pi = p[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
-    p[i] = pi;
-    w16[i] = __float2bfloat16(pi);
+struct AdamArgs {
+  float* p;
+  float* m;
+  float* v;
+  bf16* w16;
+  float lr, b1, b2, eps, bc1, bc2;
+};
+__device__ __forceinline__ void adam_one(const AdamArgs& a, int i, float gi) {
+  const float mi = a.b1 * a.m[i] + (1.f - a.b1) * gi;
+  const float vi = a.b2 * a.v[i] + (1.f - a.b2) * gi * gi;
+  a.m[i] = mi;
+  a.v[i] = vi;
+  const float pi = a.p[i] - a.lr * (mi / a.bc1) / (sqrtf(vi / a.bc2) + a.eps);
+  a.p[i] = pi;
+  a.w16[i] = __float2bfloat16(pi);
+}
+
+__global__ void k_adam(AdamArgs a, const float* g, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) adam_one(a, i, g[i]);
+}
+
+// k_reduce and k_adam in one pass over the parameters (one launch less per training step).
+__global__ void k_reduce_adam(const float* __restrict__ part, int z, float* __restrict__ g, AdamArgs a) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGParams; i += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int k = 0; k < z; ++k) s += part[(size_t)k * kGParams + i];
+    g[i] = s;
+    adam_one(a, i, s);
   }
 }
 
@@ -577,7 +594,14 @@ void GuideNet::features(const float* pts, int n, bf16* x, cudaStream_t st) {
   k_features<<<std::max(1, std::min(4096, (n + 63) / 64)), 128, 0, st>>>(pts, n, x);
 }
 
-void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st) {
+static AdamArgs adam_args(GuideNet& g, float lr) {
+  ++g.step;
+  const float b1 = 0.9f, b2 = 0.999f;
+  return AdamArgs{g.params, g.adam_m, g.adam_v, g.params16, lr, b1, b2, 1e-8f,
+                  1.f - std::pow(b1, (float)g.step), 1.f - std::pow(b2, (float)g.step)};
+}
+
+void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool adam_step, float lr) {
   TrainBufs b{x0, {h[0], h[1], h[2], h[3]}, {dh[0], dh[1], dh[2], dh[3]}, dy, loss};
   cudaMemsetAsync(loss, 0, sizeof(float), st);
   const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
@@ -585,7 +609,10 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st) {
   k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b);
   const int z = (n + kWgChunk - 1) / kWgChunk;
   k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
-  k_reduce<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad);
+  if (adam_step)
+    k_reduce_adam<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad, adam_args(*this, lr));
+  else
+    k_reduce<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad);
 }
 
 void GuideNet::draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t seed, cudaStream_t st) {
@@ -593,11 +620,7 @@ void GuideNet::draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t s
 }
 
 void GuideNet::adam(float lr, cudaStream_t st) {
-  ++step;
-  const float b1 = 0.9f, b2 = 0.999f;
-  const float bc1 = 1.f - std::pow(b1, (float)step), bc2 = 1.f - std::pow(b2, (float)step);
-  k_adam<<<grid1(kGParams), 256, 0, st>>>(params, adam_m, adam_v, grad, kGParams, lr, b1, b2, 1e-8f, bc1, bc2,
-                                           params16);
+  k_adam<<<grid1(kGParams), 256, 0, st>>>(adam_args(*this, lr), grad, kGParams);
 }
 
 }  // namespace tt

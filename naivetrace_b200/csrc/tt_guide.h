@@ -46,8 +46,9 @@ struct GuideNet {
   unsigned* tc_err = nullptr;
   // Feature rows of n points (9 floats each: position in [0,1]^3, normal, outgoing direction).
   void features(const float* pts, int n, __nv_bfloat16* x, cudaStream_t st);
-  // Mean-loss gradient over n records into `grad` and the loss into `loss`.
-  void gradient(const GuideRecord* rec, int n, cudaStream_t st);
+  // Mean-loss gradient over n records into `grad` and the loss into `loss`; with adam_step
+  // also the Adam step of size lr (as adam(), fused into the gradient's last kernel).
+  void gradient(const GuideRecord* rec, int n, cudaStream_t st, bool adam_step = false, float lr = 0.f);
   // `batch` <- n records drawn uniformly (with replacement) from pool[0, pool_n); needs
   // ensure_capacity(n).
   void draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t seed, cudaStream_t st);
