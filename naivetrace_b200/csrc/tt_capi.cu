@@ -1064,9 +1064,8 @@ static tt_status guide_train(tt_ctx* c, long long paths) {
     const int steps = c->gparams.steps_per_pass > 0 ? c->gparams.steps_per_pass : 16;
     const float lr = c->gparams.learning_rate > 0.f ? c->gparams.learning_rate : 1e-3f;
     for (int k = 0; k < steps; ++k) {
-      c->gnet->draw_batch(c->d_records, pool, n, c->gparams.seed * 0x9e3779b97f4a7c15ull + (++c->draw_seed),
-                          c->stream);
-      c->gnet->gradient(c->gnet->batch, n, c->stream, true, lr);
+      c->gnet->gradient(c->d_records, n, c->stream, true, lr, pool,
+                        c->gparams.seed * 0x9e3779b97f4a7c15ull + (++c->draw_seed));
     }
     cudaEventRecord(b, c->stream);
     float loss = 0.f, ms = 0.f;

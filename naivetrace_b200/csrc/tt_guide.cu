@@ -172,9 +172,13 @@ constexpr int kTrainWarpBytes = kTrainRows * (kGInputs * 4 + kGOutStride * 4 + k
 constexpr int kTrainSmem = kGSmBytes + kTrainWarps * kTrainWarpBytes;
 static_assert(kTrainWarpBytes % 16 == 0, "per-warp regions stay 16-byte aligned");
 
+// Record i of the batch is rec[i], or with pool_n > 0 the i-th record of a mini-batch drawn
+// uniformly with replacement from the pool, rec[h(seed, i) mod pool_n] with h the SplitMix64
+// finalizer, read straight from the pool.
 __global__ void __launch_bounds__(kTrainWarps * 32) k_train(const GuideRecord* __restrict__ rec, int n,
                                                             const bf16* __restrict__ w16,
-                                                            const float* __restrict__ w32, TrainBufs b) {
+                                                            const float* __restrict__ w32, TrainBufs b, int pool_n,
+                                                            unsigned long long seed) {
   extern __shared__ __align__(16) unsigned char tsm[];
   bf16* sw = reinterpret_cast<bf16*>(tsm);
   float* sb = reinterpret_cast<float*>(tsm + kGSmW * 2);
@@ -193,7 +197,12 @@ __global__ void __launch_bounds__(kTrainWarps * 32) k_train(const GuideRecord* _
     const int i = base + lane;
     const bool mine = lane < kTrainRows && i < n;  // lanes 0..15 own the tile's records
     GuideRecord r{};
-    if (mine) r = rec[i];
+    if (mine) {
+      const int src =
+          pool_n > 0 ? (int)(Rng::splitmix64(seed ^ Rng::splitmix64((unsigned long long)i)) % (unsigned long long)pool_n)
+                     : i;
+      r = rec[src];
+    }
     if (lane < kTrainRows) {
       float* qr = q + lane * kGInputs;
       qr[0] = r.pos[0]; qr[1] = r.pos[1]; qr[2] = r.pos[2];
@@ -425,15 +434,6 @@ __global__ void k_reduce_adam(const float* __restrict__ part, int z, float* __re
   }
 }
 
-// batch[i] = pool[h(seed, i) mod pool_n], h the SplitMix64 finalizer.
-__global__ void k_draw(const GuideRecord* __restrict__ pool, int pool_n, GuideRecord* __restrict__ batch, int n,
-                       unsigned long long seed) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const unsigned long long h = Rng::splitmix64(seed ^ Rng::splitmix64((unsigned long long)i));
-    batch[i] = pool[(int)(h % (unsigned long long)pool_n)];
-  }
-}
-
 __global__ void k_to_bf16(const float* p, int n, bf16* w16) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) w16[i] = __float2bfloat16(p[i]);
 }
@@ -548,10 +548,9 @@ bool GuideNet::ensure_capacity(int n, std::string* err) {
   }
   out = (float*)al(rows * kGOut * sizeof(float));
   dy = (bf16*)al(rows * kGOut * sizeof(bf16));
-  batch = (GuideRecord*)al(rows * sizeof(GuideRecord));
   const int z = (n + kWgChunk - 1) / kWgChunk;
   partial = (float*)al((size_t)z * kGParams * sizeof(float));
-  bool ok = x0 && out && dy && partial && batch;
+  bool ok = x0 && out && dy && partial;
   for (int l = 0; l < 4; ++l) ok = ok && h[l] && dh[l];
   if (!ok) {
     for (void*& p : scratch) cudaFree(p);
@@ -601,12 +600,13 @@ static AdamArgs adam_args(GuideNet& g, float lr) {
                   1.f - std::pow(b1, (float)g.step), 1.f - std::pow(b2, (float)g.step)};
 }
 
-void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool adam_step, float lr) {
+void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool adam_step, float lr, int pool_n,
+                        uint64_t seed) {
   TrainBufs b{x0, {h[0], h[1], h[2], h[3]}, {dh[0], dh[1], dh[2], dh[3]}, dy, loss};
   cudaMemsetAsync(loss, 0, sizeof(float), st);
   const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
                                    (n + kTrainWarps * kTrainRows - 1) / (kTrainWarps * kTrainRows));
-  k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b);
+  k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b, pool_n, seed);
   const int z = (n + kWgChunk - 1) / kWgChunk;
   k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
   if (adam_step)
@@ -615,9 +615,6 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool ada
     k_reduce<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad);
 }
 
-void GuideNet::draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t seed, cudaStream_t st) {
-  k_draw<<<grid1(n), 256, 0, st>>>(pool, pool_n, batch, n, seed);
-}
 
 void GuideNet::adam(float lr, cudaStream_t st) {
   k_adam<<<grid1(kGParams), 256, 0, st>>>(adam_args(*this, lr), grad, kGParams);

@@ -31,7 +31,6 @@ struct GuideNet {
   float* out = nullptr;
   __nv_bfloat16* dy = nullptr;
   float* partial = nullptr;
-  GuideRecord* batch = nullptr;  // mini-batch drawn from the record pool
 
   ~GuideNet();
   void release();
@@ -47,11 +46,11 @@ struct GuideNet {
   // Feature rows of n points (9 floats each: position in [0,1]^3, normal, outgoing direction).
   void features(const float* pts, int n, __nv_bfloat16* x, cudaStream_t st);
   // Mean-loss gradient over n records into `grad` and the loss into `loss`; with adam_step
-  // also the Adam step of size lr (as adam(), fused into the gradient's last kernel).
-  void gradient(const GuideRecord* rec, int n, cudaStream_t st, bool adam_step = false, float lr = 0.f);
-  // `batch` <- n records drawn uniformly (with replacement) from pool[0, pool_n); needs
-  // ensure_capacity(n).
-  void draw_batch(const GuideRecord* pool, int pool_n, int n, uint64_t seed, cudaStream_t st);
+  // also the Adam step of size lr (as adam(), fused into the gradient's last kernel).  With
+  // pool_n > 0 the records are a mini-batch of n drawn uniformly (with replacement) from
+  // rec[0, pool_n) by `seed`, gathered from the pool by the gradient's first kernel.
+  void gradient(const GuideRecord* rec, int n, cudaStream_t st, bool adam_step = false, float lr = 0.f,
+                int pool_n = 0, uint64_t seed = 0);
   void adam(float lr, cudaStream_t st);
 };
 
