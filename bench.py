@@ -128,32 +128,86 @@ def hbm_peak():
 
 def cpu_reference(scene, spp, depth, budget_s=20.0, chunk_pixels=16384, seed=1):
     """Times the oracle (CPU restatement of the reference pt) on all host cores over a
-    bounded sample: consecutive pixel chunks of the frame at 1 sample each, until about
-    budget_s of CPU time.  Returns (Mpaths/s, cores, description)."""
+    bounded sample of the frame at 1 sample per pixel: chunks of consecutive pixels spread
+    uniformly over the frame (chunk k starts at chunk slot (k * 61) mod slots, so the first
+    `slots` chunks visit every part of the frame once; later rounds use the next sample
+    index), until about budget_s of CPU time.  Returns (Mpaths/s, cores, description)."""
     from oracle.oracle import OracleScene
     from naivetrace_b200.scene import make_params
     cores = os.cpu_count() or 1
     o = OracleScene(scene, make_params(max_ray_depth=depth))
     npix = o.npix
+    chunk_pixels = max(1, min(chunk_pixels, npix))
+    slots = max(1, npix // chunk_pixels)
+    stride = 61 if np.gcd(61, slots) == 1 else 1
     acc = np.zeros(3 * npix)
     light = np.zeros(3 * npix)
     done_paths = 0
-    start = npix // 2 - chunk_pixels * 4
     t0 = time.perf_counter()
     k = 0
     while True:
-        pb = (start + k * chunk_pixels) % (npix - chunk_pixels)
-        o.render(1, seed=seed, sample_offset=0, pixel_begin=pb, pixel_end=pb + chunk_pixels, nthreads=cores,
+        pb = ((k * stride) % slots) * chunk_pixels
+        pe = npix if (k * stride) % slots == slots - 1 else pb + chunk_pixels
+        o.render(1, seed=seed, sample_offset=k // slots, pixel_begin=pb, pixel_end=pe, nthreads=cores,
                  accum=acc, light_accum=light)
-        done_paths += chunk_pixels
+        done_paths += pe - pb
         k += 1
         el = time.perf_counter() - t0
         if el >= budget_s or k >= 100000:
             break
     mpaths = done_paths / el / 1e6
-    desc = (f"{k} chunks of {chunk_pixels} consecutive pixels from the frame centre at 1 sample each "
-            f"({done_paths} paths, {el:.1f} s, depth {depth}) on {cores} threads")
+    desc = (f"{k} chunks of {chunk_pixels} consecutive pixels spread uniformly over the "
+            f"{scene.camera.xres}x{scene.camera.yres} frame at 1 sample each ({done_paths} paths, "
+            f"{min(k, slots)} of {slots} chunk slots, {el:.1f} s, depth {depth}) on {cores} threads")
     return mpaths, cores, desc
+
+
+def config_figures(device, cpu_budget=5.0, frames=2):
+    """Throughput of the plain tracer on the other configurations of the workload family,
+    each with the CPU restatement timed beside it on a bounded sample:
+    cfg 0 the Cornell box 256x256 at 16 spp (depth 10), cfg 2A the Cornell box filled with a
+    homogeneous chromatic medium and cfg 2B the planet's atmosphere under a fisheye camera,
+    both 1024x1024 at 128 spp (depth 32).  One untimed frame (allocation, warm-up), then
+    `frames` frames timed with CUDA events on the library's stream."""
+    import torch
+
+    from naivetrace_b200 import scenes
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    cfgs = [("cfg0_cornell_box", scenes.cornell_box(256, 256), 16, 10),
+            ("cfg2a_cornell_box_medium", scenes.cornell_box_medium(1024, 1024), 128, 32),
+            ("cfg2b_planet_atmosphere", scenes.planet_atmosphere(1024, 1024), 128, 32)]
+    out = {}
+    for name, scene, spp, depth in cfgs:
+        g = GpuContext(scene, make_params(max_ray_depth=depth, device=device))
+        g.render(spp, 1)
+        g.clear()
+        g.reset_stats()
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for k in range(frames):
+            g.render(spp, 2 + k)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / frames
+        st = g.stats()
+        paths = scene.camera.xres * scene.camera.yres * spp
+        g.close()
+        v, cores, desc = cpu_reference(scene, spp, depth, budget_s=cpu_budget, chunk_pixels=4096)
+        out[name] = {
+            "workload": f"{scene.camera.xres}x{scene.camera.yres} at {spp} spp, max depth {depth}, "
+                        f"{scene.num_triangles} triangles, {len(scene.media)} media",
+            "ms_per_frame": ms,
+            "mpaths_per_s": paths / (ms * 1e-3) / 1e6,
+            "mrays_per_s": (st["extension_rays"] + st["shadow_rays"]) / frames / (ms * 1e-3) / 1e6,
+            "rays_per_path": (st["extension_rays"] + st["shadow_rays"]) / frames / paths,
+            "error_flags": st["error_flags"],
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": desc},
+            "gpu_over_cpu": (paths / (ms * 1e-3) / 1e6) / v if v > 0 else None,
+        }
+    return out
 
 
 def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth=12, train_passes=8,
@@ -509,6 +563,9 @@ def run_ours(args):
     pt2 = None
     if rank == 0 and world == 1 and not args.no_pt2:
         pt2 = pt2_comparison(scene, spp, depth, device)
+    configs = None
+    if rank == 0 and world == 1 and not args.no_configs and not args.small:
+        configs = config_figures(device, cpu_budget=min(5.0, args.cpu_budget))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -554,6 +611,7 @@ def run_ours(args):
             "guiding": guiding,
             "multiview": multiview,
             "pt2": pt2,
+            "configs": configs,
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": clk,
             "stats": {k: st[k] for k in ("extension_rays", "shadow_rays", "extend_launches", "extend_ms",
@@ -659,6 +717,8 @@ def main(argv=None):
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")
     ap.add_argument("--no-multiview", action="store_true", help="skip the multi-view batch comparison")
     ap.add_argument("--no-pt2", action="store_true", help="skip the null-path tracer (pt2) frames")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the Cornell box, medium and atmosphere configurations")
     ap.add_argument("--algo", choices=["pt", "pt2"], default="pt", help="tracer of --profile-run")
     ap.add_argument("--profile-views", action="store_true",
                     help="no timing: a batch of 24 small views of the scaled-down scene (for ncu captures)")

@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 7
+#define TT_ABI_VERSION 8
 
 typedef int32_t tt_status;
 enum {
@@ -46,7 +46,9 @@ enum {
   TT_SHADER_DIFFUSE = 0,             /* DiffuseShader            shader.cxx:251-318 */
   TT_SHADER_SPECULAR_REFLECTIVE = 1, /* SpecularReflectiveShader shader.cxx:322-366 */
   TT_SHADER_SPECULAR_DIELECTRIC = 2, /* SpecularTransmissiveDielectricShader shader.cxx:378-630 */
-  TT_SHADER_MICROFACET = 3           /* MicrofacetShader (Beckmann, VNDF) shader.cxx:634-707 */
+  TT_SHADER_MICROFACET = 3,          /* MicrofacetShader (Beckmann, VNDF) shader.cxx:634-707 */
+  TT_SHADER_GLOSSY_DIELECTRIC = 4    /* GlossyTransmissiveDielectricShader (rough Beckmann
+                                        interface, alpha and ior_ratio) shader.cxx:710-787 */
 };
 
 /* A material = shader + optional area emitter + optional media on either side
@@ -56,8 +58,8 @@ enum {
 typedef struct tt_material {
   int32_t shader;                  /* TT_SHADER_* (ignored for volume boundaries) */
   float reflectance[TT_NBINS];     /* kr_d / kr_s per bin (diffuse, mirror, microfacet) */
-  float alpha;                     /* Beckmann roughness (microfacet) */
-  float ior_ratio;                 /* inside / outside IOR (dielectric) */
+  float alpha;                     /* Beckmann roughness (microfacet, glossy dielectric) */
+  float ior_ratio;                 /* inside / outside IOR (dielectrics) */
   int32_t emissive;                /* nonzero: UniformAreaLight on every triangle */
   float emission[TT_NBINS];        /* UniformAreaLight spectrum (area power density;
                                       radiance = spectrum / 2pi, light.hxx:72-108) */
@@ -262,7 +264,11 @@ tt_status tt_render_pass_range(tt_ctx* ctx, int32_t spp, uint64_t seed,
  * static array: calls that overlap on the GPU race.  The call returns after the work has
  * finished on `stream` (a cudaStream_t; NULL = legacy default stream).  Its first call on
  * a device looks up the array's device address (cudaGetSymbolAddress) and must come before
- * any stream capture.  Requires tt_upload_scene (which allocates the scene) to have run. */
+ * any stream capture.  Requires tt_upload_scene (which allocates the scene) to have run.
+ * The pass always renders unguided, also in a context with guiding enabled (the guide's
+ * records and network inputs need buffers of their own), and algo pt only (TT_ERR_INVALID
+ * for pt2).  A stop requested before the call makes it return TT_ERR_INTERRUPTED without
+ * rendering; a stop requested while it runs does not cut it short. */
 tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t seed, int32_t pixel_begin,
                                  int32_t pixel_end, uint64_t sample_offset, float* d_accum,
                                  float* d_light_accum, void* stream);
@@ -320,6 +326,20 @@ tt_status tt_sample_bsdf_batch(tt_ctx* ctx, int32_t material, const float* wi,
 tt_status tt_eval_bsdf_batch(tt_ctx* ctx, int32_t material, const float* wi,
                              const int32_t* lambda_idx, const float* dirs, int32_t n,
                              float* out_value, float* out_pdf);
+
+/* Phase-function sampling/evaluation on the device for the sampling tests
+ * (PhaseFunctionTests, tests_sampling.cxx:1202-1259): the phase function of medium `medium`
+ * (index into tt_scene_desc.media) at a volume vertex at pos -- a homogeneous medium's own
+ * function, or the atmosphere's SimpleCombined Rayleigh + Henyey-Greenstein mixture weighted
+ * by the constituents' sigma_s at pos's altitude (phasefunctions.cxx:206-273).  wi: reverse
+ * incident direction (the direction of travel is -wi).  Sample i draws from the PCG32 stream
+ * (seed, i).  Outputs as the BSDF batch calls; value per selected wavelength, pdf. */
+tt_status tt_sample_phase_batch(tt_ctx* ctx, int32_t medium, const float* pos, const float* wi,
+                                const int32_t* lambda_idx, int32_t n, uint64_t seed,
+                                float* out_dir, float* out_value, float* out_pdf);
+tt_status tt_eval_phase_batch(tt_ctx* ctx, int32_t medium, const float* pos, const float* wi,
+                              const int32_t* lambda_idx, const float* dirs, int32_t n,
+                              float* out_value, float* out_pdf);
 
 /* Device-side copy of the raw accumulators into caller-owned device buffers (npix*3
  * doubles each), ordered on `stream` (a cudaStream_t; NULL = legacy default stream).

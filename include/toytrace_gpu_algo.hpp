@@ -3,8 +3,9 @@
 //
 // RenderingAlgo (src/renderingalgorithms_interface.hxx:13-30) is the plugin boundary every
 // ToyTrace renderer implements.  Inside the reference tree GpuPathTracer would derive from
-// ::RenderingAlgo directly; standalone, RenderingAlgoInterface below
-// declares the same members with the same contracts:
+// ::RenderingAlgo directly (its factory, RenderAlgorithmFactory in
+// src/renderingalgorithms.cxx:27-42, would construct it for a new algorithm name);
+// standalone, RenderingAlgoInterface below declares the same members with the same contracts:
 //  - the interrupt callback runs on the thread that called Run();
 //  - RequestInterrupt / RequestFullStop may come from any thread, also before Run();
 //  - GenerateImage may be called from inside the callback or after Run() returned.

@@ -33,6 +33,7 @@ SHADER_DIFFUSE = 0
 SHADER_SPECULAR_REFLECTIVE = 1
 SHADER_SPECULAR_DIELECTRIC = 2
 SHADER_MICROFACET = 3
+SHADER_GLOSSY_DIELECTRIC = 4
 
 ENV_DOME = 0
 ENV_SUN = 1
@@ -211,6 +212,8 @@ EXPORTED_SYMBOLS = [
     "tt_count_traversal",
     "tt_sample_bsdf_batch",
     "tt_eval_bsdf_batch",
+    "tt_sample_phase_batch",
+    "tt_eval_phase_batch",
     "tt_read_accumulators_device",
     "tt_set_profiling",
     "tt_get_stats",
@@ -327,6 +330,8 @@ def load_library() -> C.CDLL:
         "tt_count_traversal": ([vp, P(C.c_float), C.c_int32], C.c_int32),
         "tt_sample_bsdf_batch": ([vp, C.c_int32, P(C.c_float), P(C.c_int32), C.c_int32, C.c_uint64, P(C.c_float), P(C.c_float), P(C.c_float)], C.c_int32),
         "tt_eval_bsdf_batch": ([vp, C.c_int32, P(C.c_float), P(C.c_int32), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_sample_phase_batch": ([vp, C.c_int32, P(C.c_float), P(C.c_float), P(C.c_int32), C.c_int32, C.c_uint64, P(C.c_float), P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_eval_phase_batch": ([vp, C.c_int32, P(C.c_float), P(C.c_float), P(C.c_int32), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
         "tt_read_accumulators_device": ([vp, vp, vp, vp], C.c_int32),
         "tt_set_profiling": ([vp, C.c_int32], C.c_int32),
         "tt_get_stats": ([vp, P(Stats)], C.c_int32),

@@ -129,6 +129,33 @@ class GpuContext:
                                                 _fp(dirs), n, _fp(val), _fp(pdf)), "tt_eval_bsdf_batch")
         return val, pdf
 
+    def sample_phase(self, medium: int, pos, wi, lambda_idx, n: int, seed: int):
+        """(dirs, values per wavelength, pdf) of n phase-function samples of medium `medium`
+        at a volume vertex at pos; wi is the reverse incident direction."""
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        d = np.zeros((n, 3), np.float32)
+        val = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        self._check(self.lib.tt_sample_phase_batch(self.h, medium, _fp(pos), _fp(wi),
+                                                   li.ctypes.data_as(C.POINTER(C.c_int32)), n, seed, _fp(d),
+                                                   _fp(val), _fp(pdf)), "tt_sample_phase_batch")
+        return d, val, pdf
+
+    def eval_phase(self, medium: int, pos, wi, lambda_idx, dirs):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        wi = np.ascontiguousarray(wi, dtype=np.float32)
+        li = np.ascontiguousarray(lambda_idx, dtype=np.int32)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float32).reshape(-1, 3)
+        n = len(dirs)
+        val = np.zeros((n, 3), np.float32)
+        pdf = np.zeros(n, np.float32)
+        self._check(self.lib.tt_eval_phase_batch(self.h, medium, _fp(pos), _fp(wi),
+                                                 li.ctypes.data_as(C.POINTER(C.c_int32)), _fp(dirs), n, _fp(val),
+                                                 _fp(pdf)), "tt_eval_phase_batch")
+        return val, pdf
+
     def queue_lengths(self, bounces: int) -> np.ndarray:
         """(bounces, 3) extension / shadow / finished counts of the last wave."""
         out = np.zeros(3 * bounces, np.int32)

@@ -9,7 +9,7 @@
   reference's src/sampler_tables.cxx, written with the same decimal literals so that they
   round to the same floats.
 
-Usage: python make_sobol_data.py [reference_root]   (default /root/reference)
+Usage: python make_sobol_data.py REFERENCE_ROOT   (the root of the reference's source tree)
 """
 import re
 import sys
@@ -20,7 +20,10 @@ BLOCK = 128
 
 
 def main(argv):
-    ref = Path(argv[1] if len(argv) > 1 else "/root/reference")
+    if len(argv) != 2:
+        print(__doc__)
+        return 2
+    ref = Path(argv[1])
     lines = (ref / "misc" / "new-joe-kuo-5.21201").read_text().split("\n")
     sam = []
     for row in lines[1:NUM_DIMS]:
@@ -60,7 +63,8 @@ def main(argv):
     dst = Path(__file__).with_name("tt_sobol_data.h")
     dst.write_text("\n".join(out) + "\n")
     print(f"wrote {dst} ({len(flat)} direction-number entries, {len(pairs)} rotations)")
+    return 0
 
 
 if __name__ == "__main__":
-    main(sys.argv)
+    sys.exit(main(sys.argv))

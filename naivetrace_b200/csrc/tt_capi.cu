@@ -366,11 +366,11 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   }
   for (uint32_t i = 0; i < d->num_materials; ++i) {
     const tt_material& m = d->materials[i];
-    if (m.shader < TT_SHADER_DIFFUSE || m.shader > TT_SHADER_MICROFACET)
+    if (m.shader < TT_SHADER_DIFFUSE || m.shader > TT_SHADER_GLOSSY_DIELECTRIC)
       return fail(nullptr, TT_ERR_INVALID, "unknown shader kind in material " + std::to_string(i));
-    if (m.shader == TT_SHADER_MICROFACET && !(m.alpha > 0.f))
+    if ((m.shader == TT_SHADER_MICROFACET || m.shader == TT_SHADER_GLOSSY_DIELECTRIC) && !(m.alpha > 0.f))
       return fail(nullptr, TT_ERR_INVALID, "microfacet roughness must be positive");
-    if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && !(m.ior_ratio > 0.f))
+    if ((m.shader == TT_SHADER_SPECULAR_DIELECTRIC || m.shader == TT_SHADER_GLOSSY_DIELECTRIC) && !(m.ior_ratio > 0.f))
       return fail(nullptr, TT_ERR_INVALID, "dielectric ior_ratio must be positive");
     if (m.medium_inside < 0 || m.medium_inside > (int)d->num_media || m.medium_outside < 0 ||
         m.medium_outside > (int)d->num_media)
@@ -1444,6 +1444,58 @@ tt_status tt_eval_bsdf_batch(tt_ctx* c, int32_t material, const float* wi, const
   cudaMemcpy(di, dirs, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
   launch_eval_bsdf(c->dev, material, make_float3(wi[0], wi[1], wi[2]), make_int3(li[0], li[1], li[2]), di, n, dv, dp,
                    c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaMemcpy(out_val, dv, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_pdf, dp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(di); cudaFree(dv); cudaFree(dp);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+static tt_status phase_prep(tt_ctx* c, int32_t medium, const float* pos, const float* wi, const int32_t* li, int32_t n) {
+  if (!c || !pos || !wi || !li || n < 0) return TT_ERR_INVALID;
+  if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
+  if (medium < 0 || medium >= (int)c->media.size()) return fail(c, TT_ERR_INVALID, "bad medium index");
+  for (int k = 0; k < 3; ++k)
+    if (li[k] < 0 || li[k] >= NBINS) return fail(c, TT_ERR_INVALID, "bad wavelength bin");
+  TT_CUDA(c, cudaSetDevice(c->device));
+  return TT_OK;
+}
+
+tt_status tt_sample_phase_batch(tt_ctx* c, int32_t medium, const float* pos, const float* wi, const int32_t* li,
+                                int32_t n, uint64_t seed, float* out_dir, float* out_val, float* out_pdf) {
+  tt_status st = phase_prep(c, medium, pos, wi, li, n);
+  if (st != TT_OK || n == 0) return st;
+  if (!out_dir || !out_val || !out_pdf) return fail(c, TT_ERR_INVALID, "output buffer is NULL");
+  float *dd = nullptr, *dv = nullptr, *dp = nullptr;
+  TT_CUDA(c, cudaMalloc(&dd, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dv, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dp, (size_t)n * sizeof(float)));
+  launch_sample_phase(c->dev, medium, make_float3(pos[0], pos[1], pos[2]), make_float3(wi[0], wi[1], wi[2]),
+                      make_int3(li[0], li[1], li[2]), n, seed, dd, dv, dp, c->stream);
+  cudaStreamSynchronize(c->stream);
+  cudaError_t e = cudaGetLastError();
+  cudaMemcpy(out_dir, dd, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_val, dv, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaMemcpy(out_pdf, dp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  cudaFree(dd); cudaFree(dv); cudaFree(dp);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  return TT_OK;
+}
+
+tt_status tt_eval_phase_batch(tt_ctx* c, int32_t medium, const float* pos, const float* wi, const int32_t* li,
+                              const float* dirs, int32_t n, float* out_val, float* out_pdf) {
+  tt_status st = phase_prep(c, medium, pos, wi, li, n);
+  if (st != TT_OK || n == 0) return st;
+  if (!dirs || !out_val || !out_pdf) return fail(c, TT_ERR_INVALID, "buffer is NULL");
+  float *di = nullptr, *dv = nullptr, *dp = nullptr;
+  TT_CUDA(c, cudaMalloc(&di, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dv, 3 * (size_t)n * sizeof(float)));
+  TT_CUDA(c, cudaMalloc(&dp, (size_t)n * sizeof(float)));
+  cudaMemcpy(di, dirs, 3 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  launch_eval_phase(c->dev, medium, make_float3(pos[0], pos[1], pos[2]), make_float3(wi[0], wi[1], wi[2]),
+                    make_int3(li[0], li[1], li[2]), di, n, dv, dp, c->stream);
   cudaStreamSynchronize(c->stream);
   cudaError_t e = cudaGetLastError();
   cudaMemcpy(out_val, dv, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);

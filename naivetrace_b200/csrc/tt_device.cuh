@@ -290,6 +290,22 @@ __device__ __forceinline__ float g1_vcavity(float cos_v_m, float cos_v_n, float 
 __device__ __forceinline__ float g2_vcavity(float wh_in, float wh_out, float ns_in, float ns_out, float ns_wh) {
   return fminf(g1_vcavity(wh_in, ns_in, ns_wh), g1_vcavity(wh_out, ns_out, ns_wh));
 }
+// G2VCavityTransmissive (normaldistributionfunction.hxx:87-94).
+__device__ __forceinline__ float g2_vcavity_transmissive(float wh_in, float wh_out, float ns_in, float ns_out,
+                                                         float ns_wh) {
+  return fmaxf(g1_vcavity(wh_in, ns_in, ns_wh) + g1_vcavity(wh_out, ns_out, ns_wh) - 1.f, 0.f);
+}
+// FresnelReflectivity from the incident cosine alone (Walter et al. 2007; shader_physics.hxx:132-148).
+__device__ __forceinline__ float fresnel_reflectivity_walter(float cos_n_wi, float eta_i_over_t) {
+  const float c = fabsf(cos_n_wi);
+  const float tmp = 1.f / (eta_i_over_t * eta_i_over_t) - 1.f + c * c;
+  if (tmp < 0.f) return 1.f;
+  const float g = sqrtf(tmp);
+  if (g == 0.f && c == 0.f) return 1.f;
+  const float nom = c * (g + c) - 1.f, den = c * (g - c) + 1.f;
+  const float a = (g - c) / (g + c), b = nom / den;
+  return 0.5f * a * a * (1.f + b * b);
+}
 __device__ __forceinline__ float clamp_dot(float3 a, float3 b) { return fmaxf(0.f, dot3(a, b)); }
 constexpr float kWiBelowHorizonFix = 1.e-6f;
 __device__ __forceinline__ float vndf_pdf(float d, float3 wh, float3 wi) {
@@ -393,9 +409,94 @@ __device__ __forceinline__ float3 eval_dielectric_mollified(const DevMaterial& m
   return f3(total_val, total_val, total_val);
 }
 
-// Shader::MyRoughness (shader.cxx:244-247, 666-670): the microfacet's alpha, 0 otherwise.
+// Shader::MyRoughness (shader.cxx:244-247, 666-670, 728-731): the alpha of the microfacet
+// and of the glossy dielectric, 0 otherwise.
 __device__ __forceinline__ float my_roughness(const DevMaterial& m) {
-  return m.shader == TT_SHADER_MICROFACET ? m.alpha : 0.f;
+  return (m.shader == TT_SHADER_MICROFACET || m.shader == TT_SHADER_GLOSSY_DIELECTRIC) ? m.alpha : 0.f;
+}
+
+// GlossyTransmissiveDielectricShader (shader.cxx:710-787) with its wrapper
+// GlossyTransmissiveDielectricWrapper (shader.cxx:126-190) and the sampling density
+// TransmissiveMicrofacetDensity (normaldistributionfunction.hxx:149-197): a rough interface
+// with a Beckmann distribution of roughness alpha; reflection and refraction are chosen by
+// the Fresnel reflectivity at the sampled half vector, which is drawn from the Beckmann
+// distribution of the broadened roughness alpha (1.2 - 0.2 |cos wi|).  Local frame on the
+// oriented shading normal; eta_i_over_t from the winding normal's side of wi.
+struct GlossyDielectric {
+  Frame fr;
+  float3 wi;     // local
+  float3 ng;     // oriented geometry normal, local
+  float eta;     // eta_i / eta_t, i = the side of wi
+  float alpha, alpha_b;
+};
+__device__ __forceinline__ GlossyDielectric glossy_dielectric(const DevMaterial& m, float3 wi, const Surf& s,
+                                                              float min_rough) {
+  GlossyDielectric g;
+  g.fr = frame_z(s.ns);
+  g.wi = g.fr.to_local(wi);
+  g.ng = g.fr.to_local(s.n);
+  g.eta = dot3(s.ng, wi) < 0.f ? m.ior_ratio : 1.f / m.ior_ratio;
+  g.alpha = fmaxf(min_rough, m.alpha);
+  g.alpha_b = g.alpha * (1.2f - 0.2f * fabsf(g.wi.z));  // AlphaBroadeningFormula, shader.cxx:59-62
+  return g;
+}
+// HalfVector (shader_physics.hxx:37-46); a vanishing sum falls back to the frame's x axis.
+__device__ __forceinline__ float3 half_vector(float3 wi, float3 wo) {
+  const float3 h = wi + wo;
+  const float n = len3(h);
+  return n > 0.f ? h * (1.f / n) : frame_z(wi).X;
+}
+// HalfVectorRefracted (shader_physics.hxx:50-66), Walter et al. 2007 eq. 16.
+__device__ __forceinline__ bool half_vector_refracted(float3 wi, float3 wo, float eta, float3* out) {
+  float3 h = -(eta * wi + wo);
+  const float n = len3(h);
+  h = n > 0.f ? h * (1.f / n) : wi;
+  *out = h;
+  return dot3(h, wi) * dot3(h, wo) < 0.f;
+}
+// HalfVectorPdfToTransmittedPdf (shader_physics.hxx:80-88).
+__device__ __forceinline__ float half_pdf_to_transmitted(float pdf_wh, float eta, float wi_wh, float wo_wh) {
+  float den = eta * wi_wh + wo_wh;
+  if (den == 0.f) return pdf_wh;
+  return pdf_wh * fabsf(wo_wh) / (den * den);
+}
+// TransmissiveMicrofacetDensity::Pdf with the broadened distribution.
+__device__ __forceinline__ float glossy_dielectric_pdf(const GlossyDielectric& g, float3 wo) {
+  float pdf_t = 0.f;
+  float3 wht;
+  if (half_vector_refracted(g.wi, wo, g.eta, &wht)) {
+    const float fr = fresnel_reflectivity_walter(fabsf(dot3(wht, g.wi)), g.eta);
+    const float d = beckmann_d(g.alpha_b, fabsf(wht.z)) * fabsf(wht.z);
+    pdf_t = half_pdf_to_transmitted(d, g.eta, dot3(wht, g.wi), dot3(wht, wo)) * (1.f - fr);
+  }
+  const float3 whr = half_vector(g.wi, wo);
+  const float fr = fresnel_reflectivity_walter(fabsf(dot3(whr, g.wi)), g.eta);
+  const float d = beckmann_d(g.alpha_b, fabsf(whr.z)) * fabsf(whr.z);
+  const float pdf_r = d * 0.25f / (fabsf(dot3(whr, g.wi)) + kEps) * fr;
+  return pdf_r + pdf_t;
+}
+// GlossyTransmissiveDielectricWrapper::Evaluate: BRDF on the oriented geometry normal's
+// side, BTDF below; monochromatic.
+__device__ __forceinline__ float glossy_dielectric_eval(const GlossyDielectric& g, float3 wo, float* pdf) {
+  if (pdf) *pdf = glossy_dielectric_pdf(g, wo);
+  const float ns_out = wo.z, ns_in = g.wi.z;
+  if (dot3(g.ng, wo) >= 0.f) {
+    const float3 h = half_vector(g.wi, wo);
+    const float wh_out = dot3(wo, h), wh_in = dot3(g.wi, h);
+    const float fr = fresnel_reflectivity_walter(fabsf(wh_in), g.eta);
+    const float d = beckmann_d(g.alpha, fabsf(h.z));
+    const float gg = g2_vcavity(wh_in, wh_out, ns_in, ns_out, h.z);
+    return fr * gg * d * 0.25f / (fabsf(ns_in * ns_out) + kEps);
+  }
+  float3 h;
+  if (!half_vector_refracted(g.wi, wo, g.eta, &h)) return 0.f;
+  if (h.z < 0.f) h = -h;
+  const float wh_out = dot3(wo, h), wh_in = dot3(g.wi, h);
+  const float fr = fresnel_reflectivity_walter(fabsf(wh_in), g.eta);
+  const float d = beckmann_d(g.alpha, fabsf(h.z));
+  const float j = half_pdf_to_transmitted(1.f, g.eta, wh_in, wh_out);
+  const float gg = g2_vcavity_transmissive(wh_in, wh_out, ns_in, ns_out, h.z);
+  return (1.f - fr) * fabsf(wh_in) * gg * d * j / (fabsf(ns_in * ns_out) + kEps);
 }
 
 // EvaluateBSDF of DiffuseShader (shader.cxx:280-297), the delta shaders, and
@@ -410,6 +511,11 @@ __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, con
     if (dot3(s.n, wo) > 0.f) ret = take(m.reflectance, l) * (1.f / kPi);
     if (pdf) *pdf = fmaxf(0.f, dot3(s.ns, wo)) / kPi;
     return ret;
+  }
+  if (m.shader == TT_SHADER_GLOSSY_DIELECTRIC) {
+    const GlossyDielectric g = glossy_dielectric(m, wi, s, min_rough);
+    const float v = glossy_dielectric_eval(g, g.fr.to_local(wo), pdf);
+    return f3(v, v, v);
   }
   if (m.shader == TT_SHADER_MICROFACET) {
     const Frame fr = frame_z(s.ns);
@@ -471,6 +577,21 @@ __device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float
     value /= fabsf(dot3(out.dir, s.ns));
     if (dot3(out.dir, s.n) < 0.f) value *= eta * eta;
     out.value = f3(value, value, value);
+    return out;
+  }
+  if (m.shader == TT_SHADER_GLOSSY_DIELECTRIC) {
+    // TransmissiveMicrofacetDensity::Sample: half vector, then reflect or refract.
+    const GlossyDielectric g = glossy_dielectric(m, wi, s, min_rough);
+    float r[2];
+    rng.square(r);
+    const float3 wh = beckmann_sample_wh(g.alpha_b, r);
+    float fr = fresnel_reflectivity_walter(fabsf(dot3(wh, g.wi)), g.eta);
+    float3 wt;
+    if (!refracted(g.wi, wh, g.eta, &wt)) fr = 1.f;
+    const float3 wo = rng.uniform() < fr ? reflected(g.wi, wh) : wt;
+    const float v = glossy_dielectric_eval(g, wo, &out.pdf);
+    out.dir = g.fr.to_world(wo);
+    out.value = f3(v, v, v);
     return out;
   }
   if (m.shader == TT_SHADER_DIFFUSE) {

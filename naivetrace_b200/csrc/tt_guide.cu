@@ -376,11 +376,17 @@ __global__ void __launch_bounds__(kTcThreads) k_forward_tc(const bf16* __restric
   for (int t = blockIdx.x * kTcChains + g; t < tiles; t += gridDim.x * kTcChains) {
     const long long r0 = (long long)t * kTcRows;
     tc_load_x(x, r0, n, csm, c);
-    ok = tc_mlp_tile(csm, c, phase) && ok;
+    if (!tc_mlp_tile(csm, c, phase)) {  // the same on every thread of the chain
+      ok = false;
+      break;
+    }
     tc_store_out(csm, r0, n, out, c);
     tc_chain_sync(c);  // the buffer is read out before the next tile's features land there
   }
-  if (!ok) atomicOr(err, kTcErrTimeout);
+  if (!ok) {
+    atomicOr(err, kTcErrTimeout);
+    tc_drain(c, phase);
+  }
   tc_teardown(csm);
 }
 

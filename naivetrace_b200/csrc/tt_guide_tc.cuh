@@ -108,6 +108,16 @@ __device__ __forceinline__ void tc_fence_proxy() { asm volatile("fence.proxy.asy
 __device__ __forceinline__ void tc_chain_sync(const TcChain& c) {
   asm volatile("bar.sync %0, %1;" ::"r"(c.bar_id), "r"(kTcRows) : "memory");
 }
+// Barrier of the chain that also ANDs `v` over its threads: every thread gets the same answer.
+__device__ __forceinline__ bool tc_chain_all(const TcChain& c, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(c.bar_id), "r"(kTcRows)
+      : "memory");
+  return r != 0;
+}
 
 // 16 consecutive FP32 columns of this thread's lane (raw bits; complete after tc_ld_wait).
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
@@ -182,9 +192,11 @@ __device__ __forceinline__ void tc_store_out(unsigned char* sm, long long r0, in
 
 // Five layers on the 128 feature rows of the chain's buffer; the hidden activations
 // replace the features there once layer 0 has read them, and the 48 outputs of row t are
-// staged there at the end (tc_out_slot).  `phase` counts the chain's mbarrier phases.
-// Every thread of the chain takes the same barriers whatever happens; returns false on a
-// timeout.
+// staged there at the end (tc_out_slot).  `phase` counts the chain's mbarrier phases
+// (one per committed layer).  Returns false, the same on every thread of the chain, when a
+// wait on a layer's commit gave up on any thread; the chain then issues no further MMAs,
+// the caller stops using it and drains the outstanding commit with tc_drain before the
+// tensor memory is freed.
 __device__ __forceinline__ bool tc_mlp_tile(unsigned char* sm, const TcChain& c, uint32_t& phase) {
   const int offs[5] = {kTcW0, kTcW1, kTcW1 + kGHid * kGHid * 2, kTcW1 + 2 * kGHid * kGHid * 2, kTcW4};
   const float* bias = reinterpret_cast<const float*>(sm + kTcBias);
@@ -192,10 +204,11 @@ __device__ __forceinline__ bool tc_mlp_tile(unsigned char* sm, const TcChain& c,
   for (int l = 0; l < kGLayers; ++l) {
     const int K = guide_in(l), N = guide_out(l);
     // The A operand (written by every thread of the chain) is visible to the tensor cores,
-    // and the chain's previous reads of its accumulator are done.
+    // and the chain's previous reads of its accumulator are done; the vote carries the
+    // previous layer's wait.
     tc_fence_proxy();
     tc_fence_before();
-    tc_chain_sync(c);
+    if (!tc_chain_all(c, ok)) return false;
     tc_fence_after();
     if (c.issuer) {
       const uint32_t a0 = tc_smem(sm + c.xo), b0 = tc_smem(sm + offs[l]);
@@ -204,8 +217,10 @@ __device__ __forceinline__ bool tc_mlp_tile(unsigned char* sm, const TcChain& c,
         tc_mma(c.tmem, tc_desc(a0 + ks * 256, 128, K * 16), tc_desc(b0 + ks * 256, 128, K * 16), id, ks > 0 ? 1u : 0u);
       tc_commit(c.bar);
     }
-    ok = tc_wait(c.bar, phase & 1u) && ok;
+    // Warp-uniform, as tcgen05.ld is a warp-collective instruction.
+    ok = __all_sync(0xffffffffu, tc_wait(c.bar, phase & 1u));
     ++phase;
+    if (!ok) continue;  // nothing read from an accumulator that may still be written
     tc_fence_after();
     uint32_t v[kGHid];
     const uint32_t taddr = c.tmem + c.lanes;
@@ -236,8 +251,13 @@ __device__ __forceinline__ bool tc_mlp_tile(unsigned char* sm, const TcChain& c,
                         __uint_as_float(v[4 * q + 2]) + b[4 * q + 2], __uint_as_float(v[4 * q + 3]) + b[4 * q + 3]);
     }
   }
-  tc_chain_sync(c);  // the staged outputs are complete
-  return ok;
+  return tc_chain_all(c, ok);  // the staged outputs are complete
+}
+
+// After a failed tile: one more bounded wait for the chain's last commit, so that the
+// tensor memory is not freed under an MMA that is still writing it.
+__device__ __forceinline__ void tc_drain(const TcChain& c, uint32_t phase) {
+  if (phase > 0) tc_wait(c.bar, (phase - 1) & 1u);
 }
 
 // Tensor-memory allocation of kTcChains * kTcCols columns by warp 0, the address published

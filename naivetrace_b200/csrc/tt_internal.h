@@ -266,6 +266,10 @@ void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda,
                         float* dir, float* val, float* pdf, cudaStream_t st);
 void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, const float* dirs, int n, float* val,
                       float* pdf, cudaStream_t st);
+void launch_sample_phase(const DevScene& s, int medium, float3 pos, float3 wi, int3 lambda, int n,
+                         unsigned long long seed, float* dir, float* val, float* pdf, cudaStream_t st);
+void launch_eval_phase(const DevScene& s, int medium, float3 pos, float3 wi, int3 lambda, const float* dirs, int n,
+                       float* val, float* pdf, cudaStream_t st);
 // Blocks per SM that the shading kernel sustains (for grid sizing).
 int kernel_blocks_per_sm();
 // Framebuffer resolve: rgb = accum * inv_spp + splat_weight * light, per pixel.  inv_spp

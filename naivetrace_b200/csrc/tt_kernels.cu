@@ -1396,7 +1396,10 @@ __global__ void __launch_bounds__(kTcThreads) k_guide_tc(DevScene sc, PathState 
       *reinterpret_cast<uint4*>(tsm + c.xo + tc_off(c.row, k, kGIn)) =
           make_uint4(guide_feature_pair(q, k), guide_feature_pair(q, k + 2), guide_feature_pair(q, k + 4),
                      guide_feature_pair(q, k + 6));
-    ok = tc_mlp_tile(tsm, c, phase) && ok;
+    if (!tc_mlp_tile(tsm, c, phase)) {  // the same on every thread of the chain
+      ok = false;
+      break;
+    }
     float o[kGOut];
 #pragma unroll
     for (int k = 0; k < kGOut / 4; ++k) {
@@ -1406,7 +1409,10 @@ __global__ void __launch_bounds__(kTcThreads) k_guide_tc(DevScene sc, PathState 
     tc_chain_sync(c);  // the outputs are read out before the next entries' features land there
     if (i < n) guide_scatter_one<MEDIA>(sc, p, bounce, pre, o);
   }
-  if (!ok) atomicOr(p.err, ERR_TENSOR);
+  if (!ok) {
+    atomicOr(p.err, ERR_TENSOR);
+    tc_drain(c, phase);
+  }
   tc_teardown(tsm);
 }
 
@@ -1656,6 +1662,37 @@ __global__ void k_eval_bsdf(DevScene sc, int material, float3 wi, int3 li, const
   }
 }
 
+// Phase-function sampling and evaluation at a volume vertex at pos in medium `medium`
+// (the sampling-test hooks of the PhaseFunctionTests fixture, tests_sampling.cxx:1202-1259):
+// sample i draws from the PCG32 stream (seed, i), as the render kernels do per path.
+__global__ void k_sample_phase(DevScene sc, int medium, float3 pos, float3 wi, int3 li, int n, unsigned long long seed,
+                               float* dir, float* val, float* pdf) {
+  const Lambda l{li.x, li.y, li.z};
+  const DevMedium& m = sc.media[medium];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Rng rng;
+    rng.seed_path(seed, (unsigned long long)i);
+    float3 v;
+    float pp;
+    const float3 d = medium_phase_sample(m, pos, wi, rng, l, &v, &pp);
+    dir[3 * i] = d.x; dir[3 * i + 1] = d.y; dir[3 * i + 2] = d.z;
+    val[3 * i] = v.x; val[3 * i + 1] = v.y; val[3 * i + 2] = v.z;
+    pdf[i] = pp;
+  }
+}
+
+__global__ void k_eval_phase(DevScene sc, int medium, float3 pos, float3 wi, int3 li, const float* dirs, int n,
+                             float* val, float* pdf) {
+  const Lambda l{li.x, li.y, li.z};
+  const DevMedium& m = sc.media[medium];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float pp = 0.f;
+    const float3 v = medium_phase_eval(m, pos, wi, f3(dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]), l, &pp);
+    val[3 * i] = v.x; val[3 * i + 1] = v.y; val[3 * i + 2] = v.z;
+    pdf[i] = pp;
+  }
+}
+
 // ----------------------------------------------------------------------------------------
 // Host launchers.
 
@@ -1681,10 +1718,19 @@ static void with_bool(bool b, F&& f) {
   else f(std::false_type{});
 }
 
+// Launch grids depend on the device's SM count, so they are cached per device ordinal
+// (the current device of the calling thread).  Concurrent first calls compute the same value.
+constexpr int kGridCacheDevices = 64;
+static int current_device_slot() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev >= 0 && dev < kGridCacheDevices ? dev : kGridCacheDevices - 1;
+}
+
 // Traversal grid: every SM filled to the traversal kernels' occupancy limit (per layout).
 static int trace_grid(bool wide) {
-  static int g[2] = {0, 0};
-  int& gg = g[wide ? 1 : 0];
+  static int g[kGridCacheDevices][2] = {};
+  int& gg = g[current_device_slot()][wide ? 1 : 0];
   if (gg == 0) {
     int dev = 0, sms = 0, b0 = 0, b1 = 0;
     cudaGetDevice(&dev);
@@ -1789,12 +1835,12 @@ void launch_resolve_views(const float* accum, const float* light, const DevView*
   k_resolve_views<<<grid, 256, 0, st>>>(accum, light, views, nviews, npix, rgb);
 }
 
-static int g_guide_grid = 0;
-
-static int g_guide_tc_grid = 0;
+// Grids of the guided-scattering kernels, per device: [0] k_guide, [1] k_guide_tc, [2] k_guide_tree.
+static int g_guide_grids[kGridCacheDevices][3] = {};
 
 void prepare_guide_launch() {
-  if (g_guide_grid != 0) return;
+  int* grids = g_guide_grids[current_device_slot()];
+  if (grids[0] != 0) return;
   cudaFuncSetAttribute(k_guide<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
   cudaFuncSetAttribute(k_guide<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kGuideSmem);
   cudaFuncSetAttribute(k_guide_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
@@ -1802,34 +1848,30 @@ void prepare_guide_launch() {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide<true>, kGuideWarps * 32, kGuideSmem);
-  g_guide_grid = sms * (per_sm > 0 ? per_sm : 1);
-  per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_tc<true>, kTcThreads, kTcSmem);
-  g_guide_tc_grid = sms * (per_sm > 0 ? per_sm : 1);
+  grids[1] = sms * (per_sm > 0 ? per_sm : 1);
+  per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide_tree<true>, kBlock, 0);
+  grids[2] = sms * (per_sm > 0 ? per_sm : 1);
+  per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_guide<true>, kGuideWarps * 32, kGuideSmem);
+  grids[0] = sms * (per_sm > 0 ? per_sm : 1);  // last: marks the entry complete
 }
 
 void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st) {
-  if (s.guide_method == TT_GUIDE_TREE) {
-    static int tgrid = 0;
-    if (tgrid == 0) {
-      int dev = 0, sms = 0, per = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_guide_tree<true>, kBlock, 0);
-      tgrid = sms * (per > 0 ? per : 1);
-    }
-    if (s.num_media > 0) k_guide_tree<true><<<tgrid, kBlock, 0, st>>>(s, p, bounce);
-    else k_guide_tree<false><<<tgrid, kBlock, 0, st>>>(s, p, bounce);
-    return;
-  }
   prepare_guide_launch();
-  if (s.guide_net == TT_GUIDE_NET_TCGEN05) {
-    if (s.num_media > 0) k_guide_tc<true><<<g_guide_tc_grid, kTcThreads, kTcSmem, st>>>(s, p, bounce);
-    else k_guide_tc<false><<<g_guide_tc_grid, kTcThreads, kTcSmem, st>>>(s, p, bounce);
+  const int* grids = g_guide_grids[current_device_slot()];
+  if (s.guide_method == TT_GUIDE_TREE) {
+    if (s.num_media > 0) k_guide_tree<true><<<grids[2], kBlock, 0, st>>>(s, p, bounce);
+    else k_guide_tree<false><<<grids[2], kBlock, 0, st>>>(s, p, bounce);
     return;
   }
-  const int grid = g_guide_grid;
+  if (s.guide_net == TT_GUIDE_NET_TCGEN05) {
+    if (s.num_media > 0) k_guide_tc<true><<<grids[1], kTcThreads, kTcSmem, st>>>(s, p, bounce);
+    else k_guide_tc<false><<<grids[1], kTcThreads, kTcSmem, st>>>(s, p, bounce);
+    return;
+  }
+  const int grid = grids[0];
   if (s.num_media > 0) k_guide<true><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
   else k_guide<false><<<grid, kGuideWarps * 32, kGuideSmem, st>>>(s, p, bounce);
 }
@@ -1876,6 +1918,14 @@ void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda,
 void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, const float* dirs, int n, float* val,
                       float* pdf, cudaStream_t st) {
   if (n > 0) k_eval_bsdf<<<grid_for(n), kBlock, 0, st>>>(s, material, wi, lambda, dirs, n, val, pdf);
+}
+void launch_sample_phase(const DevScene& s, int medium, float3 pos, float3 wi, int3 lambda, int n,
+                         unsigned long long seed, float* dir, float* val, float* pdf, cudaStream_t st) {
+  if (n > 0) k_sample_phase<<<grid_for(n), kBlock, 0, st>>>(s, medium, pos, wi, lambda, n, seed, dir, val, pdf);
+}
+void launch_eval_phase(const DevScene& s, int medium, float3 pos, float3 wi, int3 lambda, const float* dirs, int n,
+                       float* val, float* pdf, cudaStream_t st) {
+  if (n > 0) k_eval_phase<<<grid_for(n), kBlock, 0, st>>>(s, medium, pos, wi, lambda, dirs, n, val, pdf);
 }
 __global__ void k_resolve(const double* accum, const double* light, const double* inv_spp_px, double inv_spp,
                           double splat_weight, int npix, float* rgb) {

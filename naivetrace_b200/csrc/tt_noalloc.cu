@@ -138,6 +138,9 @@ extern "C" tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t s
                                      " camera samples requested; at most 65536 (spp x pixels) per call");
   if (depth > kNoAllocMaxDepth)
     return fail(TT_ERR_CAPACITY, "tt_render_pass_noalloc: max_ray_depth above 1000");
+  // A pending stop request ends this pass before it starts, as it ends every later
+  // tt_render_pass.  Once launched, the pass (at most 65,536 samples) runs to completion.
+  if (tt_stop_requested(ctx)) return fail(TT_ERR_INTERRUPTED, "tt_render_pass_noalloc: stop requested");
   if (device < 0 || device >= kNoAllocMaxDevices) return fail(TT_ERR_INVALID, "device ordinal out of range");
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return fail(TT_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));

@@ -409,6 +409,11 @@ class _Parser:
                         raise NFFError(f"{where}: dispersion (abbe_number) is not supported")
                     scope.shaders[name] = _Shader(abi.SHADER_SPECULAR_DIELECTRIC, np.zeros(NBINS),
                                                   ior=float(node["ior_ratio"]))
+                elif cls == "glossytransmissivedielectric":
+                    if "alpha_texture" in node:
+                        raise NFFError(f"{where}: roughness textures are not supported")
+                    scope.shaders[name] = _Shader(abi.SHADER_GLOSSY_DIELECTRIC, np.zeros(NBINS),
+                                                  ior=float(node["ior_ratio"]), alpha=float(node["alpha"]))
                 elif cls == "glossy":
                     rgb = [float(x) for x in node.get("rgb", [1.0, 1.0, 1.0])]
                     k = float(node.get("x", 1.0))

@@ -132,6 +132,12 @@ def microfacet(reflectance, alpha: float) -> MaterialSpec:
     return MaterialSpec(shader=abi.SHADER_MICROFACET, reflectance=as_spectrum(reflectance), alpha=alpha)
 
 
+def glossy_glass(ior_ratio: float, alpha: float) -> MaterialSpec:
+    """GlossyTransmissiveDielectricShader (shader.cxx:710-787): a rough dielectric interface."""
+    return MaterialSpec(shader=abi.SHADER_GLOSSY_DIELECTRIC, reflectance=np.zeros(NBINS), ior_ratio=ior_ratio,
+                        alpha=alpha)
+
+
 def area_light(emission, reflectance=0.0) -> MaterialSpec:
     return MaterialSpec(shader=abi.SHADER_DIFFUSE, reflectance=as_spectrum(reflectance), emission=as_spectrum(emission))
 

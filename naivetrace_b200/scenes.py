@@ -16,7 +16,7 @@ import math
 import numpy as np
 
 from . import abi
-from .scene import (AtmosphereSpec, CameraSpec, MediumSpec, Scene, area_light, diffuse, env_map, glass,
+from .scene import (AtmosphereSpec, CameraSpec, MediumSpec, Scene, area_light, diffuse, env_map, glass, glossy_glass,
                     microfacet, mirror, sun_light, volume_boundary)
 from .spectral import band_spectrum, rgb_to_spectrum
 
@@ -101,7 +101,8 @@ def cornell_box(xres=256, yres=256, one_light_triangle=False) -> Scene:
 
 def cornell_box_materials(xres=64, yres=64) -> Scene:
     """The Cornell box with the tall box turned into glass and the small box into a
-    rough Beckmann metal plus a mirror back wall: exercises every shader."""
+    rough Beckmann metal, a mirror back wall and a rough-glass sphere above the small box:
+    exercises every shader."""
     s = Scene()
     s.name = "cornell_box_materials"
     white = s.add_material(diffuse(0.75))
@@ -121,6 +122,7 @@ def cornell_box_materials(xres=64, yres=64) -> Scene:
     s.add_mesh(*quad((0.5 - q, yl, 0.5 - q), (0.5 + q, yl, 0.5 - q), (0.5 + q, yl, 0.5 + q), (0.5 - q, yl, 0.5 + q)), light)
     s.add_mesh(*box_mesh((0.3, 0.3, 0.3), (0.65, 0.0, 0.35), 17.0), metal)
     s.add_mesh(*box_mesh((0.3, 0.6, 0.3), (0.3, 0.0, 0.65), -17.0), glass_m)
+    s.add_sphere((0.65, 0.45, 0.35), 0.12, s.add_material(glossy_glass(1.5, 0.15)))
     s.camera = CameraSpec(kind=abi.CAMERA_PINHOLE, pos=(0.5, 0.5, -1.4), dir=(0, 0, 1), up=(0, 1, 0),
                           fov_deg=40.0, xres=xres, yres=yres)
     return s

@@ -106,6 +106,13 @@ class _YamlReader(_Parser):
             if "abbe_number" in node:
                 raise NFFError("shader: dispersion (abbe_number) is not supported")
             sh = _Shader(abi.SHADER_SPECULAR_DIELECTRIC, np.zeros(NBINS), ior=ior)
+        elif cls == "glossytransmissivedielectric":
+            # parse_yaml_scene.cxx:443-450 (alpha_min only with a roughness texture)
+            ior = float(node.pop("ior_ratio"))
+            alpha = float(node.pop("alpha"))
+            if "alpha_texture" in node:
+                raise NFFError("shader: roughness textures are not supported")
+            sh = _Shader(abi.SHADER_GLOSSY_DIELECTRIC, np.zeros(NBINS), ior=ior, alpha=alpha)
         else:
             raise NFFError(f"shader class {cls} is not supported by this tracer")
         if node:

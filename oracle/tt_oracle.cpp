@@ -359,6 +359,18 @@ inline double G1VCavity(double cos_v_m, double cos_v_n, double cos_n_m) {
 inline double G2VCavity(double wh_dot_in, double wh_dot_out, double ns_dot_in, double ns_dot_out, double ns_dot_wh) {
   return std::min(G1VCavity(wh_dot_in, ns_dot_in, ns_dot_wh), G1VCavity(wh_dot_out, ns_dot_out, ns_dot_wh));
 }
+// G2VCavityTransmissive, normaldistributionfunction.hxx:87-94.
+inline double G2VCavityTransmissive(double wh_dot_in, double wh_dot_out, double ns_dot_in, double ns_dot_out,
+                                    double ns_dot_wh) {
+  return std::max(G1VCavity(wh_dot_in, ns_dot_in, ns_dot_wh) + G1VCavity(wh_dot_out, ns_dot_out, ns_dot_wh) - 1., 0.);
+}
+// HalfVectorPdfToTransmittedPdf, shader_physics.hxx:80-88.
+inline double HalfVectorPdfToTransmittedPdf(double pdf_wh, double eta, double dot_wi_wh, double dot_wo_wh) {
+  double denom = eta * dot_wi_wh + dot_wo_wh;
+  if (denom == 0.) return pdf_wh;
+  denom *= denom;
+  return pdf_wh * std::abs(dot_wo_wh) / denom;
+}
 inline double ClampDot(V3 a, V3 b) { return std::max(0., Dot(a, b)); }
 constexpr double WI_BELOW_HORIZON_FIX_FACTOR = 1.e-6;
 inline void VndfSample(V3& wh, V3 wi, double r) {
@@ -905,7 +917,72 @@ struct ScatterSample {
 // SpecularTransmissiveDielectricShader::SampleBsdfRegular, shader.cxx:401-473.
 // MicrofacetShader + MicrofacetShaderWrapper, shader.cxx:74-130, 676-707.
 // Shader::MyRoughness (shader.cxx:244-247, 666-670): the microfacet's alpha, 0 otherwise.
-inline double MyRoughness(const tt_material& m) { return m.shader == TT_SHADER_MICROFACET ? (double)m.alpha : 0.; }
+inline double MyRoughness(const tt_material& m) {
+  return (m.shader == TT_SHADER_MICROFACET || m.shader == TT_SHADER_GLOSSY_DIELECTRIC) ? (double)m.alpha : 0.;
+}
+
+// GlossyTransmissiveDielectricShader, shader.cxx:710-787: the wrapper
+// GlossyTransmissiveDielectricWrapper (shader.cxx:126-190) over the local frame of the
+// shading normal, sampled by TransmissiveMicrofacetDensity
+// (normaldistributionfunction.hxx:149-197) with the broadened roughness
+// AlphaBroadeningFormula (shader.cxx:59-62).
+struct GlossyDielectric {
+  Frame frame;
+  V3 wi, ng;  // local
+  double eta;  // eta_i / eta_t, i = the incident side
+  Beckman ndf, broadened;
+
+  GlossyDielectric(const tt_material& m, V3 wi_world, const Surf& si, double min_roughness)
+      : frame(OrthogonalSystemZAligned(si.shading_normal)), ndf{0.}, broadened{0.} {
+    wi = frame.ToLocal(wi_world);
+    ng = frame.ToLocal(si.normal);
+    eta = Dot(si.geometry_normal, wi_world) < 0. ? (double)m.ior_ratio : 1. / m.ior_ratio;
+    const double alpha = std::max(min_roughness, (double)m.alpha);
+    ndf = Beckman{alpha};
+    broadened = Beckman{alpha * (1.2 - 0.2 * std::abs(wi.z))};
+  }
+  double Pdf(V3 wo) const {  // TransmissiveMicrofacetDensity::Pdf
+    double pdf_wot = 0.;
+    V3 wht;
+    if (HalfVectorRefracted(wi, wo, eta, &wht)) {
+      const double fr_wht = FresnelReflectivityWalter(std::abs(Dot(wht, wi)), eta);
+      const double ndf_transm = broadened.EvalByHalfVector(std::abs(wht.z)) * std::abs(wht.z);
+      pdf_wot = HalfVectorPdfToTransmittedPdf(ndf_transm, eta, Dot(wht, wi), Dot(wht, wo)) * (1.0 - fr_wht);
+    }
+    const V3 whr = HalfVector(wi, wo);
+    const double fr_whr = FresnelReflectivityWalter(std::abs(Dot(whr, wi)), eta);
+    const double ndf_reflect = broadened.EvalByHalfVector(std::abs(whr.z)) * std::abs(whr.z);
+    return HalfVectorPdfToReflectedPdf(ndf_reflect, Dot(whr, wi)) * fr_whr + pdf_wot;
+  }
+  double Evaluate(V3 wo, double* pdf) const {
+    if (pdf) *pdf = Pdf(wo);
+    const double ns_dot_out = wo.z, ns_dot_in = wi.z;
+    if (Dot(ng, wo) >= 0) {
+      const V3 whr = HalfVector(wi, wo);
+      const double wh_dot_out = Dot(wo, whr), wh_dot_in = Dot(wi, whr);
+      const double fr_whr = FresnelReflectivityWalter(std::abs(wh_dot_in), eta);
+      const double D = ndf.EvalByHalfVector(std::abs(whr.z));
+      const double G = G2VCavity(wh_dot_in, wh_dot_out, ns_dot_in, ns_dot_out, whr.z);
+      return fr_whr * G * D * 0.25 / (std::abs(ns_dot_in * ns_dot_out) + Eps);
+    }
+    V3 wht;
+    if (!HalfVectorRefracted(wi, wo, eta, &wht)) return 0.;
+    if (wht.z < 0.) wht = -wht;
+    const double wh_dot_out = Dot(wo, wht), wh_dot_in = Dot(wi, wht);
+    const double fr_wht = FresnelReflectivityWalter(std::abs(wh_dot_in), eta);
+    const double D = ndf.EvalByHalfVector(std::abs(wht.z));
+    const double J = HalfVectorPdfToTransmittedPdf(1.0, eta, wh_dot_in, wh_dot_out);
+    const double G = G2VCavityTransmissive(wh_dot_in, wh_dot_out, ns_dot_in, ns_dot_out, wht.z);
+    return (1.0 - fr_wht) * std::abs(wh_dot_in) * G * D * J / (std::abs(ns_dot_in * ns_dot_out) + Eps);
+  }
+  V3 Sample(const double r1[2], double r2) const {  // TransmissiveMicrofacetDensity::Sample
+    const V3 wh = broadened.SampleHalfVector(r1);
+    double fr = FresnelReflectivityWalter(std::abs(Dot(wh, wi)), eta);
+    V3 wt;
+    if (!Refracted(wi, wh, eta, &wt)) fr = 1.0;
+    return r2 < fr ? Reflected(wi, wh) : wt;
+  }
+};
 
 // SpecularTransmissiveDielectricShader::Sample/EvaluateBsdfMollified (shader.cxx:482-605):
 // with a path roughness r > 0 (pt2's path regularisation) the specular lobes become
@@ -955,6 +1032,10 @@ static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const
     case TT_SHADER_SPECULAR_DIELECTRIC:
       if (pdf) *pdf = 0.;
       return S3(0.);
+    case TT_SHADER_GLOSSY_DIELECTRIC: {
+      const GlossyDielectric g(m, wi, si, min_roughness);
+      return S3(g.Evaluate(g.frame.ToLocal(wo), pdf));
+    }
     case TT_SHADER_MICROFACET: {
       const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
       const V3 ng = fr.ToLocal(si.normal);
@@ -1018,6 +1099,15 @@ static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sam
     return out;
   }
   switch (m.shader) {
+    case TT_SHADER_GLOSSY_DIELECTRIC: {
+      const GlossyDielectric g(m, wi, si, min_roughness);
+      double r[2];
+      smp.UniformUnitSquare(r);
+      const V3 wo = g.Sample(r, smp.Uniform01());
+      out.value = S3(g.Evaluate(wo, &out.pdf));
+      out.dir = g.frame.ToWorld(wo);
+      return out;
+    }
     case TT_SHADER_DIFFUSE: {
       const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
       double r[2];

@@ -44,7 +44,7 @@ int main() {
     t.join();
     algo.Run();
     auto img = algo.GenerateImage();
-    std::FILE* f = std::fopen("gpurun_out_algo_driver.ppm", "wb");
+    std::FILE* f = std::fopen("algo_driver_image.ppm", "wb");
     if (f) {
       std::fprintf(f, "P6\n%d %d\n255\n", img->width, img->height);
       std::fwrite(img->rgb.data(), 1, img->rgb.size(), f);

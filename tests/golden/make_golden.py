@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures of tests/golden/ from the reference source text.
 
-    python tests/golden/make_golden.py [REFERENCE_ROOT]
+    python tests/golden/make_golden.py REFERENCE_ROOT
 
 The reference cannot be compiled in this environment (its third-party dependencies are
 absent), so the only fixtures that can be taken from it are numbers written in its source:
@@ -71,4 +71,7 @@ def main(root: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        print("usage: python make_golden.py REFERENCE_ROOT")
+        sys.exit(2)
+    sys.exit(main(sys.argv[1]))

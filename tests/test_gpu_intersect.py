@@ -122,6 +122,31 @@ def test_terrain_ray_batch(gpu_lib):
     check_parity(g, o, rays)
 
 
+def test_full_terrain_ray_batch_device_built_bvh(gpu_lib):
+    """The benchmark's own acceleration structure: the full 2,748,418-triangle terrain with
+    its 32 spheres, BVH built on the device by PLOC (the default), 200k rays -- half from
+    above the terrain pointing down at it, half starting near random mesh vertices in random
+    directions -- against the oracle's own SAH tree."""
+    s = scenes.terrain_spheres()
+    g = GpuContext(s)
+    o = OracleScene(s, make_params())
+    rng = np.random.default_rng(11)
+    n = 100000
+    down = random_rays(n, -4.8, 4.8, rng)
+    down[:, 1] = rng.uniform(0.3, 2.0, size=n)
+    down[:, 5] = -np.abs(down[:, 5])
+    verts = s.arrays()[0]
+    near = random_rays(n, -0.6, 0.6, rng)
+    centres = verts[rng.integers(0, len(verts), size=n)]
+    near[:, :3] += centres
+    near[:, 1] = np.abs(near[:, 1]) + 0.05
+    rays = np.concatenate([down, near])
+    frac = check_parity(g, o, rays)
+    pg, _, _, _ = g.intersect(np.asarray(rays, np.float32).astype(np.float64))
+    assert (pg >= 0).mean() > 0.5  # the batch exercises the tree, not empty space
+    assert frac >= 0.9999
+
+
 def test_signed_zero_direction_components(gpu_lib):
     """Directions with a +0 or -0 component (mirror reflections off axis-aligned walls make
     them): the traversal must take the slab planes in the order the reciprocal's sign says."""
