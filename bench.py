@@ -210,100 +210,127 @@ def config_figures(device, cpu_budget=5.0, frames=2):
     return out
 
 
-def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth=12, train_passes=8,
-                       train_steps=16, lr=1e-3, guide_depth=2):
-    """Learned-guided against plain GPU tracing on the guiding workload (a room lit through a
-    0.3 x 0.3 gap, 1280x720, depth 12): relMSE against a 4096-spp plain render after every
-    pass, with the wall time of the render calls (training included) summed.  Plain passes
-    double their spp (1, 2, 4, ...); the guided run first renders `train_passes` one-sample
-    passes that train the network after each pass, then freezes it and doubles like plain.
-    Every sample, training passes included, stays in the image (each is unbiased).  Reports
-    the time to reach relMSE `target` and the relMSE of both at equal time."""
-    from naivetrace_b200 import abi, scenes
-    from naivetrace_b200.algo import GpuContext
-    from naivetrace_b200.scene import make_params
-    scene = scenes.guiding_room(xres, yres)
-    p = make_params(max_ray_depth=depth)
-    ref = GpuContext(scene, p)
-    for k in range(16):
-        ref.render(256, seed=1_000_000 + k)
-    R = ref.framebuffer().astype(np.float64)
-    ref.close()
+class GuidingWorkload:
+    """The guiding workload (a room lit through a 0.3 x 0.3 gap, 1280x720, depth 12) with its
+    converged reference: a 4096-spp plain render (16 passes of 256 spp)."""
 
-    def relmse(g):
+    def __init__(self, xres=1280, yres=720, depth=12):
+        from naivetrace_b200 import scenes
+        from naivetrace_b200.algo import GpuContext
+        from naivetrace_b200.scene import make_params
+        self.xres, self.yres, self.depth = xres, yres, depth
+        self.scene = scenes.guiding_room(xres, yres)
+        self.params = make_params(max_ray_depth=depth)
+        ref = GpuContext(self.scene, self.params)
+        for k in range(16):
+            ref.render(256, seed=1_000_000 + k)
+        self.R = ref.framebuffer().astype(np.float64)
+        ref.close()
+        # Warm-up context: kernels loaded, memory pool filled.
+        w = GpuContext(self.scene, self.params)
+        w.render(4, 1)
+        w.set_guiding(True, 1, seed=7)
+        w.render(1, 2)
+        w.close()
+
+    def relmse(self, g):
         I = g.framebuffer().astype(np.float64)
-        return float(np.mean((I - R) ** 2 / (R * R + 1e-2)))
+        return float(np.mean((I - self.R) ** 2 / (self.R * self.R + 1e-2)))
 
-    def timed(g, spp, seed):
-        t = time.perf_counter()
-        g.render(spp, seed)
-        return (time.perf_counter() - t) * 1e3
-
-    # Warm-up contexts: kernels loaded, memory pool filled.
-    w = GpuContext(scene, p)
-    w.render(4, 1)
-    w.set_guiding(True, 1, learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
-    w.render(1, 2)
-    w.close()
-
-    def run(guided, tree=False):
-        g = GpuContext(scene, p)
-        # The tree guider (the reference's kd-tree cells with fitted vMF mixtures), batch EM.
-        kw = dict(learning_rate=lr, steps_per_pass=train_steps, max_depth=guide_depth, seed=7)
+    def curve(self, guided=False, tree=False, train_passes=8, budget_ms=1000.0, discard_training=False,
+              **guide_kw):
+        """relMSE after every pass against the wall time of the render calls so far (training
+        included).  Plain runs double their spp per pass (1, 2, 4, ...); guided runs first
+        render `train_passes` one-sample passes that train the guide after each pass, then
+        freeze it and double.  With discard_training the training passes' samples are
+        dropped from the image when the guide freezes (as the reference's guided tracer
+        does), else every sample stays in the image (each is unbiased).  Returns the curve
+        [(ms, spp in the image, relMSE)] and the context's stats."""
+        from naivetrace_b200 import abi
+        from naivetrace_b200.algo import GpuContext
+        g = GpuContext(self.scene, self.params)
+        kw = dict(seed=7)
+        kw.update(guide_kw)
         if tree:
-            kw.update(method=abi.GUIDE_TREE, tree_subdivision=200, tree_em_iters=4)
+            kw.update(method=abi.GUIDE_TREE)
         # One untimed pass at the largest wave size (2^26 paths) allocates the path state
         # (with the guiding arrays for the guided run); the guide is not trained by it.
         if guided:
             g.set_guiding(True, 0, **kw)
-        g.render(-(-(1 << 26) // (xres * yres)), 3)
+        g.render(-(-(1 << 26) // (self.xres * self.yres)), 3)
         g.clear()
         g.reset_stats()
+
+        def timed(spp, seed):
+            t = time.perf_counter()
+            g.render(spp, seed)
+            return (time.perf_counter() - t) * 1e3
+
         pts, el, spp_total, seed = [], 0.0, 0, 10
-        if guided:
+        if guided and train_passes > 0:
             g.set_guiding(True, 1, **kw)
             for k in range(train_passes):
-                el += timed(g, 1, seed)
+                el += timed(1, seed)
                 seed += 1
                 spp_total += 1
-                pts.append((el, spp_total, relmse(g)))
+                if not discard_training:
+                    pts.append((el, spp_total, self.relmse(g)))
             g.set_guiding(True, 0, **kw)
+            if discard_training:
+                g.clear()
+                spp_total = 0
         spp = 1
         while el < budget_ms and spp_total < 1 << 14:
-            el += timed(g, spp, seed)
+            el += timed(spp, seed)
             seed += 1
             spp_total += spp
-            pts.append((el, spp_total, relmse(g)))
+            pts.append((el, spp_total, self.relmse(g)))
             spp *= 2
         st = g.stats()
         g.close()
         return pts, st
 
-    def time_to(pts, tgt):
-        prev = None
-        for t, s, e in pts:
-            if e <= tgt:
-                if prev is None or prev[2] <= e:
-                    return t
-                # log-log interpolation between the bracketing passes
-                a = (np.log(prev[2]) - np.log(tgt)) / (np.log(prev[2]) - np.log(e))
-                return float(np.exp(np.log(prev[0]) + a * (np.log(t) - np.log(prev[0]))))
-            prev = (t, s, e)
-        return None
 
-    def at_time(pts, t0):
-        ts = np.log([x[0] for x in pts])
-        es = np.log([x[2] for x in pts])
-        return float(np.exp(np.interp(np.log(t0), ts, es)))
+def time_to(pts, tgt):
+    """Time at which a relMSE curve first reaches tgt (log-log interpolation between passes)."""
+    prev = None
+    for t, s, e in pts:
+        if e <= tgt:
+            if prev is None or prev[2] <= e:
+                return t
+            a = (np.log(prev[2]) - np.log(tgt)) / (np.log(prev[2]) - np.log(e))
+            return float(np.exp(np.log(prev[0]) + a * (np.log(t) - np.log(prev[0]))))
+        prev = (t, s, e)
+    return None
 
-    plain, _ = run(False)
-    guided, gst = run(True)
-    tree, tst = run(True, tree=True)
+
+def at_time(pts, t0):
+    ts = np.log([x[0] for x in pts])
+    es = np.log([x[2] for x in pts])
+    return float(np.exp(np.interp(np.log(t0), ts, es)))
+
+
+GUIDE_SETTINGS = dict(train_passes=8, discard_training=False, learning_rate=1e-3, record_pool=1 << 16,
+                      batch=8192, steps_per_pass=16, max_depth=2, nee_records=False)
+
+
+def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
+    """Learned-guided against plain GPU tracing on the guiding workload: relMSE against a
+    4096-spp plain render after every pass, with the wall time of the render calls
+    (training included) summed.  Reports the time to reach relMSE `target`, their ratio and
+    the relMSE of both at equal time; the tree guider runs the same schedule."""
+    st_kw = dict(GUIDE_SETTINGS if settings is None else settings)
+    wl = GuidingWorkload()
+    plain, _ = wl.curve(False, budget_ms=budget_ms)
+    guided, gst = wl.curve(True, budget_ms=budget_ms, **st_kw)
+    tree_kw = dict(st_kw)
+    tree_kw.update(tree_subdivision=200, tree_em_iters=4, nee_records=False)
+    tree, tst = wl.curve(True, tree=True, budget_ms=budget_ms, **tree_kw)
     t_eq = min(plain[-1][0], guided[-1][0])
     tp, tg = time_to(plain, target), time_to(guided, target)
     ep, eg = at_time(plain, t_eq), at_time(guided, t_eq)
     return {
-        "workload": f"guiding_room: 4x3x4 room lit through a 0.3x0.3 gap, {xres}x{yres}, max depth {depth}, "
+        "workload": f"guiding_room: 4x3x4 room lit through a 0.3x0.3 gap, {wl.xres}x{wl.yres}, max depth {wl.depth}, "
                     f"relMSE = mean((I-R)^2/(R^2+1e-2)) against a 4096-spp plain render",
         "target_relmse": target,
         "time_to_target_ms": {"plain": tp, "guided": tg},
@@ -311,9 +338,9 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, xres=1280, yres=720, depth
         "equal_time_ms": t_eq,
         "relmse_at_equal_time": {"plain": ep, "guided": eg},
         "gain_equal_time": ep / eg if eg > 0 else None,
-        "guided_bounces": guide_depth,
-        "training": {"passes": train_passes, "adam_steps": int(gst["guide_steps"]), "learning_rate": lr,
-                     "records": int(gst["guide_records"]), "train_kernel_ms": gst["guide_train_ms"]},
+        "settings": st_kw,
+        "training": {"adam_steps": int(gst["guide_steps"]), "records": int(gst["guide_records"]),
+                     "train_kernel_ms": gst["guide_train_ms"]},
         "tree_guider": {
             "what": "kd-tree cells (200 records per initial cell) with 8-lobe vMF mixtures, batch EM (4 "
                     "iterations per round), the same schedule of training passes",

@@ -388,6 +388,12 @@ typedef struct tt_guiding_params {
                                    rendering, TT_GUIDE_NET_TCGEN05 (tensor-memory accumulators,
                                    128-row tiles) or TT_GUIDE_NET_MMA (warp-level mma.sync,
                                    16-row tiles); both give the same outputs */
+  int32_t nee_records;          /* TT_GUIDE_LEARNED: 1 = the next-event samples of guided vertices
+                                   that reach their light are training records too (direction to
+                                   the light, weight = MIS-weighted contribution over the light
+                                   sample's density), so that with the scattered directions' emission
+                                   hits the records cover all the incident radiance; 0 = scattered
+                                   directions only (no media: in media scenes this stays off) */
 } tt_guiding_params;
 enum { TT_GUIDE_LEARNED = 0, TT_GUIDE_TREE = 1 };
 enum { TT_GUIDE_NET_TCGEN05 = 0, TT_GUIDE_NET_MMA = 1 };

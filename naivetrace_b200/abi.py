@@ -278,6 +278,7 @@ class GuidingParams(C.Structure):
         ("tree_subdivision", C.c_int32),
         ("tree_em_iters", C.c_int32),
         ("network", C.c_int32),
+        ("nee_records", C.c_int32),
     ]
 
 

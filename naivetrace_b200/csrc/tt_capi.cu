@@ -1612,6 +1612,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   if (!gp->enabled) {
     c->dev.guide = 0;
     c->dev.guide_record = 0;
+    c->dev.guide_nee_records = 0;
     c->gparams = *gp;
     return TT_OK;
   }
@@ -1669,6 +1670,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     c->dev.tree_mix = c->tree->d_mix;
   }
   c->dev.guide_record = gp->train ? 1 : 0;
+  c->dev.guide_nee_records = (gp->method == TT_GUIDE_LEARNED && gp->nee_records && c->dev.num_media == 0) ? 1 : 0;
   c->dev.guide_depth = gp->max_depth > 0 ? gp->max_depth : (1 << 30);
   return TT_OK;
 }

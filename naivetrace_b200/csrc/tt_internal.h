@@ -131,6 +131,7 @@ struct DevScene {
   int guide_depth;            // guided vertices only at bounces < guide_depth
   float guide_keep;           // probability that a finished path keeps its record (a uniform
                               // subsample when a pass would yield more than the pool holds)
+  int guide_nee_records;      // 1: next-event samples at guided vertices are training records too
   const __nv_bfloat16* guide_w16;  // network weights (BF16, flat layout of tt_guide.cuh)
   const float* guide_w32;          // FP32 master copy (the biases are read from it)
   float box_lo[3];            // scene box, for the position encoding
@@ -180,8 +181,9 @@ struct PathState {
                        // shading normal xyz, outgoing direction xyz
   int* guide_q;        // guided-vertex queue (slots)
   float4* grec;        // pending training record per path: 6 float4 (tt_kernels.cu)
-  float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion,
-                       // BSDF pdf of the shadow direction, emitted flag
+  float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion (after
+                       // k_guide: the MIS-weighted contribution over the throughput, F / q of
+                       // the NEE training record), BSDF pdf of the shadow direction, emitted flag
   float* rr;           // Russian-roulette throughput factor: (throughput with BSDF densities at
                        // the guided vertices) / beta
   GuideRecord* records;  // training-record pool, a ring of rec_cap records
