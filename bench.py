@@ -311,7 +311,7 @@ def at_time(pts, t0):
 
 
 GUIDE_SETTINGS = dict(train_passes=8, discard_training=False, learning_rate=1e-3, record_pool=1 << 16,
-                      batch=8192, steps_per_pass=16, max_depth=2, nee_records=False)
+                      batch=8192, steps_per_pass=16, max_depth=2)
 
 
 def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
@@ -324,7 +324,7 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
     plain, _ = wl.curve(False, budget_ms=budget_ms)
     guided, gst = wl.curve(True, budget_ms=budget_ms, **st_kw)
     tree_kw = dict(st_kw)
-    tree_kw.update(tree_subdivision=200, tree_em_iters=4, nee_records=False)
+    tree_kw.update(tree_subdivision=200, tree_em_iters=4)
     tree, tst = wl.curve(True, tree=True, budget_ms=budget_ms, **tree_kw)
     t_eq = min(plain[-1][0], guided[-1][0])
     tp, tg = time_to(plain, target), time_to(guided, target)

@@ -67,7 +67,20 @@ typedef struct tt_material {
                                       0 = none (zero-initialised materials have no media) */
   int32_t medium_outside;          /* 1 + index of the medium the normal points into, 0 = none */
   int32_t volume_boundary;         /* nonzero: medium boundary only, no surface */
+  int32_t diffuse_texture;         /* TT_SHADER_DIFFUSE: 1 + index of the tt_texture that multiplies
+                                      the reflectance at the hit's texture coordinates
+                                      (MaybeMultiplyTextureLookup, shader.cxx:17-27); 0 = none */
 } tt_material;
+
+/* An RGB texture (Texture, texture.hxx:15-117): linear RGB floats, width * height * 3, row 0 =
+ * the TOP row of the image.  8-bit sRGB images are converted to linear by the caller
+ * (Color::SRGBToLinear), as Texture::GetPixel does.  Lookups take the texel under the
+ * coordinates wrapped to [0, 1) (UvToPixel, texture.hxx:37-55), no filtering. */
+typedef struct tt_texture {
+  int32_t width;
+  int32_t height;
+  const float* rgb;
+} tt_texture;
 
 /* Phase functions (src/phasefunctions.cxx). */
 enum { TT_PHASE_UNIFORM = 0, TT_PHASE_RAYLEIGH = 1, TT_PHASE_HENYEY_GREENSTEIN = 2 };
@@ -172,6 +185,13 @@ typedef struct tt_scene_desc {
   const float* spheres;                /* num_spheres * 4: centre x, y, z, radius */
   const uint32_t* sphere_material_ids; /* num_spheres */
   tt_camera camera;
+  const float* uvs;             /* num_vertices * 2 texture coordinates (Mesh::uvs), or NULL
+                                   (all zero); a triangle hit interpolates them with its
+                                   barycentrics; a sphere hit maps its normal to (phi / 2pi,
+                                   theta / pi), y up (EmbreeAccelerator, embreeaccelerator.cxx:
+                                   216-259) */
+  uint32_t num_textures;
+  const tt_texture* textures;
 } tt_scene_desc;
 
 enum { TT_SAMPLE_BOTH = 0, TT_SAMPLE_BSDF = 1, TT_SAMPLE_LIGHTS = 2 }; /* --pt-sample-mode */
@@ -388,12 +408,6 @@ typedef struct tt_guiding_params {
                                    rendering, TT_GUIDE_NET_TCGEN05 (tensor-memory accumulators,
                                    128-row tiles) or TT_GUIDE_NET_MMA (warp-level mma.sync,
                                    16-row tiles); both give the same outputs */
-  int32_t nee_records;          /* TT_GUIDE_LEARNED: 1 = the next-event samples of guided vertices
-                                   that reach their light are training records too (direction to
-                                   the light, weight = MIS-weighted contribution over the light
-                                   sample's density), so that with the scattered directions' emission
-                                   hits the records cover all the incident radiance; 0 = scattered
-                                   directions only (no media: in media scenes this stays off) */
 } tt_guiding_params;
 enum { TT_GUIDE_LEARNED = 0, TT_GUIDE_TREE = 1 };
 enum { TT_GUIDE_NET_TCGEN05 = 0, TT_GUIDE_NET_MMA = 1 };

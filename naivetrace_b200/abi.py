@@ -61,7 +61,12 @@ class Material(C.Structure):
         ("medium_inside", C.c_int32),
         ("medium_outside", C.c_int32),
         ("volume_boundary", C.c_int32),
+        ("diffuse_texture", C.c_int32),
     ]
+
+
+class Texture(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("rgb", C.POINTER(C.c_float))]
 
 
 PHASE_UNIFORM = 0
@@ -139,6 +144,9 @@ class SceneDesc(C.Structure):
         ("spheres", C.POINTER(C.c_float)),
         ("sphere_material_ids", C.POINTER(C.c_uint32)),
         ("camera", Camera),
+        ("uvs", C.POINTER(C.c_float)),
+        ("num_textures", C.c_uint32),
+        ("textures", C.POINTER(Texture)),
     ]
 
 
@@ -278,7 +286,6 @@ class GuidingParams(C.Structure):
         ("tree_subdivision", C.c_int32),
         ("tree_em_iters", C.c_int32),
         ("network", C.c_int32),
-        ("nee_records", C.c_int32),
     ]
 
 

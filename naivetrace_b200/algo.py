@@ -178,17 +178,15 @@ class GpuContext:
     def set_guiding(self, enabled: bool = True, train: int = 1, learning_rate: float = 1e-3,
                     record_pool: int = 1 << 16, batch: int = 8192, steps_per_pass: int = 16, max_depth: int = 2,
                     seed: int = 1, method: int = abi.GUIDE_LEARNED, tree_subdivision: int = 100,
-                    tree_em_iters: int = 0, network: int = abi.GUIDE_NET_TCGEN05, nee_records: bool = True):
+                    tree_em_iters: int = 0, network: int = abi.GUIDE_NET_TCGEN05):
         """train: 0 frozen, 1 collect records and train after every pass, 2 collect only;
         max_depth: guide the first max_depth bounces only (0: all).  Guiding the first two
         bounces measured the best relMSE per unit time on the gap-lit room (the network's cost
         grows with every guided vertex, its gain mostly comes from the first ones);
         network: the inference kernel of the learned guider (GUIDE_NET_TCGEN05 or
-        GUIDE_NET_MMA, same outputs); nee_records: the learned guider also trains on the
-        next-event samples of guided vertices."""
+        GUIDE_NET_MMA, same outputs)."""
         gp = abi.GuidingParams(int(enabled), int(train), learning_rate, record_pool, batch, steps_per_pass, max_depth,
-                               seed, int(method), int(tree_subdivision), int(tree_em_iters), int(network),
-                               int(nee_records))
+                               seed, int(method), int(tree_subdivision), int(tree_em_iters), int(network))
         self._check(self.lib.tt_set_guiding(self.h, C.byref(gp)), "tt_set_guiding")
 
     def tree_info(self) -> dict:

@@ -158,6 +158,9 @@ struct tt_ctx {
   std::vector<uint32_t> sphere_mats;
   std::vector<HostEnv> envs;
   std::vector<tt_point_light> points;
+  HostArray<float> uvs;                          // 2 per vertex, when given
+  std::vector<std::vector<float>> textures;      // linear RGB per texture
+  std::vector<int2> texture_sizes;               // width, height
   tt_camera camera{};
   tt_params params{};
   int npix = 0;
@@ -375,6 +378,10 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
     if (m.medium_inside < 0 || m.medium_inside > (int)d->num_media || m.medium_outside < 0 ||
         m.medium_outside > (int)d->num_media)
       return fail(nullptr, TT_ERR_INVALID, "medium index out of range in material " + std::to_string(i));
+    if (m.diffuse_texture < 0 || m.diffuse_texture > (int)d->num_textures)
+      return fail(nullptr, TT_ERR_INVALID, "texture index out of range in material " + std::to_string(i));
+    if (m.diffuse_texture > 0 && m.shader != TT_SHADER_DIFFUSE)
+      return fail(nullptr, TT_ERR_INVALID, "a texture needs the diffuse shader (material " + std::to_string(i) + ")");
   }
   if (d->num_media > 0 && !d->media) return fail(nullptr, TT_ERR_INVALID, "media missing");
   if (d->num_spheres > (1u << 26)) return fail(nullptr, TT_ERR_CAPACITY, "more than 2^26 spheres");
@@ -387,6 +394,15 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
     if (d->sphere_material_ids[i] >= d->num_materials)
       return fail(nullptr, TT_ERR_INVALID, "material index out of range in sphere " + std::to_string(i));
   }
+  if (d->num_textures > 0 && !d->textures) return fail(nullptr, TT_ERR_INVALID, "textures missing");
+  for (uint32_t i = 0; i < d->num_textures; ++i) {
+    const tt_texture& t = d->textures[i];
+    if (!t.rgb || t.width <= 0 || t.height <= 0 || (long long)t.width * t.height > (1ll << 28))
+      return fail(nullptr, TT_ERR_INVALID, "texture " + std::to_string(i) + " needs pixels and a positive size");
+  }
+  if (d->uvs)
+    for (size_t k = 0; k < 2 * (size_t)d->num_vertices; ++k)
+      if (!std::isfinite(d->uvs[k])) return fail(nullptr, TT_ERR_INVALID, "texture coordinates must be finite");
   if (d->num_media > (uint32_t)kMaxMedia) return fail(nullptr, TT_ERR_CAPACITY, "more than 254 media");
   for (uint32_t i = 0; i < d->num_media; ++i) {
     const tt_medium& m = d->media[i];
@@ -451,6 +467,12 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
     c->envs.push_back(std::move(e));
   }
   if (d->num_point_lights > 0) c->points.assign(d->point_lights, d->point_lights + d->num_point_lights);
+  if (d->uvs) parallel_copy(c->uvs, d->uvs, 2 * (size_t)d->num_vertices);
+  for (uint32_t i = 0; i < d->num_textures; ++i) {
+    const tt_texture& t = d->textures[i];
+    c->textures.emplace_back(t.rgb, t.rgb + 3 * (size_t)t.width * t.height);
+    c->texture_sizes.push_back(make_int2(t.width, t.height));
+  }
   c->camera = d->camera;
   c->params = *p;
   if (c->params.max_ray_depth <= 0) c->params.max_ray_depth = 25;
@@ -683,6 +705,22 @@ tt_status tt_upload_scene(tt_ctx* c) {
     dm[i].med_out = m.medium_outside - 1;
     std::memcpy(dm[i].reflectance, m.reflectance, sizeof(m.reflectance));
     std::memcpy(dm[i].emission, m.emission, sizeof(m.emission));
+    dm[i].tex = nullptr;
+    dm[i].tex_w = dm[i].tex_h = 0;
+  }
+  // Textures (one device array each) and the per-vertex texture coordinates.
+  {
+    std::vector<const float*> dtex(c->textures.size(), nullptr);
+    for (size_t k = 0; k < c->textures.size(); ++k)
+      dtex[k] = (const float*)upload(c->textures[k].data(), c->textures[k].size() * sizeof(float));
+    for (size_t i = 0; i < dm.size(); ++i) {
+      const int t = c->materials[i].diffuse_texture - 1;
+      if (t < 0) continue;
+      dm[i].tex = dtex[t];
+      dm[i].tex_w = c->texture_sizes[t].x;
+      dm[i].tex_h = c->texture_sizes[t].y;
+    }
+    s.uvs = c->uvs.empty() ? nullptr : (const float2*)upload(c->uvs.data(), c->uvs.size() * sizeof(float));
   }
   s.materials = (const DevMaterial*)upload(dm.data(), dm.size() * sizeof(DevMaterial));
   // Media.
@@ -1612,7 +1650,6 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   if (!gp->enabled) {
     c->dev.guide = 0;
     c->dev.guide_record = 0;
-    c->dev.guide_nee_records = 0;
     c->gparams = *gp;
     return TT_OK;
   }
@@ -1670,7 +1707,6 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
     c->dev.tree_mix = c->tree->d_mix;
   }
   c->dev.guide_record = gp->train ? 1 : 0;
-  c->dev.guide_nee_records = (gp->method == TT_GUIDE_LEARNED && gp->nee_records && c->dev.num_media == 0) ? 1 : 0;
   c->dev.guide_depth = gp->max_depth > 0 ? gp->max_depth : (1 << 30);
   return TT_OK;
 }

@@ -325,6 +325,7 @@ struct Surf {
   float3 n;         // oriented geometry normal
   float3 ns;        // oriented shading normal
   float3 bounds;    // pos_bounds
+  float2 uv;        // texture coordinates (SurfaceInteraction::tex_coord)
 };
 
 // util::Gamma<float>(7) (util.hxx:124-127) with the full float epsilon.
@@ -363,7 +364,48 @@ __device__ __forceinline__ Surf make_surface(const DevScene& sc, int slot, float
   s.bounds = (abs3(p0 * bw.x) + abs3(p1 * bw.y) + abs3(p2 * bw.z)) * gamma7();
   s.n = s.ng;
   s.ns = s.ns_raw;
+  // Texture coordinates interpolated like the position (rtcInterpolate1 of the uv vertex
+  // attribute, embreeaccelerator.cxx:226-228); only textured materials read them.
+  s.uv = make_float2(0.f, 0.f);
+  if (sc.uvs && sc.materials[s.material].tex) {
+    const uint4 ti = __ldg(&sc.tri_idx[s.prim]);
+    const float2 ua = __ldg(&sc.uvs[ti.x]), ub = __ldg(&sc.uvs[ti.y]), uc = __ldg(&sc.uvs[ti.z]);
+    s.uv = make_float2(ua.x * w0 + ub.x * w1 + uc.x * w2, ua.y * w0 + ub.y * w1 + uc.y * w2);
+  }
   return s;
+}
+
+// KartesianToSpherical (third component up, vec3f.hxx:298-321) then SphericalToUv
+// (vec3f.hxx:286-295) of a direction: a sphere hit's texture coordinates from its normal
+// (EmbreeAccelerator::FirstIntersectionSphere, embreeaccelerator.cxx:258).
+__device__ __forceinline__ float2 direction_uv(float3 d) {
+  const float x = d.x, z = d.y, y = d.z;
+  const float ax = fabsf(x), az = fabsf(z);
+  const float theta = acosf(fminf(1.f, fmaxf(-1.f, y / len3(d))));
+  float phi;
+  if (ax > az) {
+    phi = atan2f(z, ax);
+    phi = (x > 0.f) ? phi : kPi - phi;
+  } else {
+    phi = atan2f(x, az);
+    phi = (z > 0.f) ? (kPi / 2.f) - phi : (3.f / 2.f * kPi) + phi;
+  }
+  return make_float2(phi / (2.f * kPi), theta / kPi);
+}
+
+// UvToPixel (texture.hxx:37-55) and Texture::GetPixel (texture.hxx:94-117): the texel under
+// the coordinates wrapped to [0, 1), v up, row 0 at the top; linear RGB.
+__device__ __forceinline__ float3 texture_rgb(const DevMaterial& m, float2 uv) {
+  float dummy;
+  float u = modff(uv.x, &dummy), v = modff(uv.y, &dummy);
+  if (u < 0.f) u = 1.f + u;
+  if (v < 0.f) v = 1.f + v;
+  if (u > 1.f - kEpsF) u -= kEpsF;
+  if (v > 1.f - kEpsF) v -= kEpsF;
+  const int x = min(max((int)(u * m.tex_w), 0), m.tex_w - 1);
+  const int y = min(max(m.tex_h - (int)(v * m.tex_h) - 1, 0), m.tex_h - 1);
+  const float* p = m.tex + 3 * ((size_t)y * m.tex_w + x);
+  return f3(__ldg(p), __ldg(p + 1), __ldg(p + 2));
 }
 
 __device__ __forceinline__ void orient(Surf& s, float3 incident) {
@@ -407,6 +449,18 @@ __device__ __forceinline__ float3 eval_dielectric_mollified(const DevMaterial& m
   total_val /= fabsf(dot3(wo, s.ns));
   if (pdf) *pdf = total_pdf;
   return f3(total_val, total_val, total_val);
+}
+
+// DiffuseShader's reflectance at the hit: times the texture's RGB turned into the selected
+// wavelengths' values when the material has a texture (MaybeMultiplyTextureLookup,
+// shader.cxx:17-27).
+__device__ __forceinline__ float3 diffuse_kr(const DevMaterial& m, const Surf& s, Lambda l) {
+  float3 kr = take(m.reflectance, l);
+  if (m.tex) {
+    const float3 c = texture_rgb(m, s.uv);
+    kr = mul(kr, rgb_to_selection(c.x, c.y, c.z, l));
+  }
+  return kr;
 }
 
 // Shader::MyRoughness (shader.cxx:244-247, 666-670, 728-731): the alpha of the microfacet
@@ -508,7 +562,7 @@ __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, con
     return eval_dielectric_mollified(m, wi, s, wo, min_rough, pdf);
   if (m.shader == TT_SHADER_DIFFUSE) {
     float3 ret = f3(0.f, 0.f, 0.f);
-    if (dot3(s.n, wo) > 0.f) ret = take(m.reflectance, l) * (1.f / kPi);
+    if (dot3(s.n, wo) > 0.f) ret = diffuse_kr(m, s, l) * (1.f / kPi);
     if (pdf) *pdf = fmaxf(0.f, dot3(s.ns, wo)) / kPi;
     return ret;
   }
@@ -601,7 +655,7 @@ __device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float
     const float3 v = to_cos_hemisphere(r);
     out.pdf = v.z / kPi;
     out.dir = fr.to_world(v);
-    out.value = dot3(s.n, out.dir) > 0.f ? take(m.reflectance, l) * (1.f / kPi) : f3(0.f, 0.f, 0.f);
+    out.value = dot3(s.n, out.dir) > 0.f ? diffuse_kr(m, s, l) * (1.f / kPi) : f3(0.f, 0.f, 0.f);
     return out;
   }
   if (m.shader == TT_SHADER_SPECULAR_REFLECTIVE) {
@@ -1068,6 +1122,7 @@ __device__ __forceinline__ Surf sphere_surface(const float4* tris, int slot, dou
   s.bounds = abs3(s.pos) * gamma5();
   s.n = s.ng;
   s.ns = s.ns_raw;
+  s.uv = direction_uv(s.ng);
   return s;
 }
 

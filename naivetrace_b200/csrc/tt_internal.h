@@ -45,7 +45,8 @@ struct DevMaterial {
   float ior_ratio;
   int med_in;        // medium entered through the front side (winding normal), -1 none
   int med_out;       // medium on the front side, -1 none
-  int pad[2];
+  int tex_w, tex_h;  // diffuse texture size
+  const float* tex;  // diffuse texture (linear RGB, row 0 at the top), or nullptr
   float reflectance[NBINS];
   float emission[NBINS];
 };
@@ -99,6 +100,7 @@ struct DevScene {
   const float4* tris;         // 3 float4 per primitive slot of the active layout: v0 (w=prim), v1 (w=material), v2
   const uint4* tri_idx;       // per prim: vertex indices a, b, c and material
   const float* normals;       // per vertex xyz, or nullptr
+  const float2* uvs;          // per vertex texture coordinates, or nullptr
   const DevMaterial* materials;
   const int* area_lights;     // prim of each area light
   const float4* area_verts;   // 3 float4 (v0, v1, v2) per area light
@@ -131,7 +133,6 @@ struct DevScene {
   int guide_depth;            // guided vertices only at bounces < guide_depth
   float guide_keep;           // probability that a finished path keeps its record (a uniform
                               // subsample when a pass would yield more than the pool holds)
-  int guide_nee_records;      // 1: next-event samples at guided vertices are training records too
   const __nv_bfloat16* guide_w16;  // network weights (BF16, flat layout of tt_guide.cuh)
   const float* guide_w32;          // FP32 master copy (the biases are read from it)
   float box_lo[3];            // scene box, for the position encoding
@@ -181,9 +182,8 @@ struct PathState {
                        // shading normal xyz, outgoing direction xyz
   int* guide_q;        // guided-vertex queue (slots)
   float4* grec;        // pending training record per path: 6 float4 (tt_kernels.cu)
-  float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion (after
-                       // k_guide: the MIS-weighted contribution over the throughput, F / q of
-                       // the NEE training record), BSDF pdf of the shadow direction, emitted flag
+  float4* gnee;        // NEE at a guided vertex: light pdf (-1: no MIS), pdf conversion,
+                       // BSDF pdf of the shadow direction, emitted flag
   float* rr;           // Russian-roulette throughput factor: (throughput with BSDF densities at
                        // the guided vertices) / beta
   GuideRecord* records;  // training-record pool, a ring of rec_cap records

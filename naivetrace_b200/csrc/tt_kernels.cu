@@ -675,6 +675,8 @@ __device__ __forceinline__ LightNode pick_light(const DevScene& sc, Rng& rng, La
   L.type = LIGHT_NONE;
   L.delta = false;
   L.pdf = 0.f;
+  // A scene without lights has none to pick: no draw, no connection.
+  if (sc.num_env == 0 && sc.num_area_lights == 0 && sc.num_point_lights == 0) return L;
   const int which = tower_sampling4(sc.type_probs, rng.uniform());
   if (which == LIGHT_ENV) {
     const int i = rng.uniform_int(0, sc.num_env - 1);
@@ -1063,7 +1065,6 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
                           (sc.materials[s.material].shader == TT_SHADER_DIFFUSE ||
                            sc.materials[s.material].shader == TT_SHADER_MICROFACET);
       if (guided) p.gnee[slot].w = 0.f;
-      bool nee_emitted = false;
       if (sc.sample_lights) {
         LightNode L = pick_light(sc, rng, l);
         if (L.type != LIGHT_NONE) {
@@ -1088,7 +1089,6 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
               if (!is_volume && dot3(c.dir, s.n) < 0.f) going_through(sc, smt, c.dir, s.ng, s.material);
             }
             emit_shadow<MEDIA>(sc, p, bounce + 1, slot, c, L, beta, 1.f, -1, smt, rng, guided);
-            nee_emitted = true;
           }
         }
       }
@@ -1097,10 +1097,6 @@ __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bou
       if (guided) {
         const int qg = warp_append(guide_count(p, bounce));
         p.guide_q[qg] = slot;
-        // The shadow ray of this vertex (if any) knows its guide-queue entry, whose inputs
-        // (position, normal, outgoing direction) its NEE training record reuses.
-        if (!MEDIA && sc.guide_record && sc.guide_nee_records && nee_emitted)
-          p.sh_c[slot].w = __int_as_float(qg + 1);
         const float3 p01 = f3((s.pos.x - sc.box_lo[0]) * sc.box_inv[0], (s.pos.y - sc.box_lo[1]) * sc.box_inv[1],
                               (s.pos.z - sc.box_lo[2]) * sc.box_inv[2]);
         float4* gi = p.ginp + 3 * (size_t)qg;
@@ -1231,23 +1227,10 @@ __device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const Path
     const float pdf_due = ((1.f - mix.c) * nee.z + mix.c * guide_mixture_pdf(mix, sd)) * nee.y;
     if (MEDIA) {
       p.sh_med[slot].y = pdf_due;
-    } else {
-      const float w = nee.x > 0.f ? power_heuristic(nee.x, pdf_due) : 1.f;
+    } else if (nee.x > 0.f) {
+      const float w = power_heuristic(nee.x, pdf_due);
       const float4 c4 = p.sh_c[slot];
       p.sh_c[slot] = make_float4(c4.x * w, c4.y * w, c4.z * w, c4.w);
-      if (__float_as_int(c4.w) > 0) {
-        // F / q of the NEE training record: the MIS-weighted contribution over the
-        // throughput, averaged over the wavelengths that carry throughput.
-        float fq = 0.f;
-        int nz = 0;
-        const float cc[3] = {c4.x * w, c4.y * w, c4.z * w}, bb[3] = {beta.x, beta.y, beta.z};
-        for (int k = 0; k < 3; ++k)
-          if (bb[k] > 0.f) {
-            fq += fmaxf(cc[k], 0.f) / bb[k];
-            ++nz;
-          }
-        p.gnee[slot].y = nz > 0 ? fq / nz : 0.f;
-      }
     }
   }
   const float3 f = val * (bsdf_correction(s, ndir) * fabsf(dot3(s.ng, ndir)));
@@ -1488,26 +1471,6 @@ __global__ void __launch_bounds__(256) k_shadow(DevScene sc, PathState p, Frameb
       const float mis = med.x < 0.f ? 1.f : power_heuristic(med.x, med.y * ctr);
       c = mul(c, T) * mis;
     }
-    if (!MEDIA && target < 0 && __float_as_int(c4.w) > 0) {
-      // Next-event sample of a guided vertex: a training record for the light direction,
-      // weight F / q = its MIS-weighted contribution over the light sample's density, so
-      // that with the BSDF-side emission hits the records cover the incident radiance.
-      const float4 gn = p.gnee[slot];
-      Rng krng{p.rng_state[slot] ^ 0x9e3779b97f4a7c15ull, p.rng_inc[slot]};
-      if (gn.y > 0.f && isfinite(gn.y) && (sc.guide_keep >= 1.f || krng.uniform() < sc.guide_keep)) {
-        const float4* gi = p.ginp + 3 * (size_t)(__float_as_int(c4.w) - 1);
-        const float4 i0 = gi[0], i1 = gi[1], i2 = gi[2];
-        const unsigned idx = atomicAdd(reinterpret_cast<unsigned*>(p.rec_count), 1u) % (unsigned)p.rec_cap;
-        GuideRecord rec;
-        rec.pos[0] = i0.x; rec.pos[1] = i0.y; rec.pos[2] = i0.z;
-        rec.n[0] = i0.w; rec.n[1] = i1.x; rec.n[2] = i1.y;
-        rec.wo[0] = i1.z; rec.wo[1] = i1.w; rec.wo[2] = i2.x;
-        rec.wi[0] = d.x; rec.wi[1] = d.y; rec.wi[2] = d.z;
-        rec.p_bsdf = gn.z;
-        rec.f_over_q = gn.y;
-        p.records[idx] = rec;
-      }
-    }
     if (target < 0) {
       const float4 a = p.accum[slot];
       p.accum[slot] = make_float4(a.x + c.x, a.y + c.y, a.z + c.z, 0.f);
@@ -1671,6 +1634,7 @@ __device__ __forceinline__ Surf zup_surface(float3 wi) {
   s.ng = f3(0.f, 0.f, 1.f);
   s.ns_raw = s.ng;
   s.bounds = f3(0.f, 0.f, 0.f);
+  s.uv = make_float2(0.f, 0.f);
   orient(s, -wi);
   return s;
 }

@@ -178,6 +178,7 @@ template <bool MEDIA>
 __device__ __forceinline__ void nee2(const DevScene& sc, const PathState& p, int qbounce, int slot, Smp2& rng, Lambda l,
                                      float3 beta, float3 wi, const Surf* s, float rough, int vmed, float3 vpos,
                                      const MTracker& mt, const M33f& wt) {
+  if (sc.num_env == 0 && sc.num_area_lights == 0 && sc.num_point_lights == 0) return;  // no light to pick
   const int which = tower_sampling4(sc.type_probs, rng.uniform());
   const int nl = which == LIGHT_ENV ? 1 : (which == LIGHT_AREA ? sc.num_area_lights : sc.num_point_lights);
   // TowerSamplingBisection over the uniform CMF (k + 1) / nl.

@@ -11,10 +11,11 @@ definitions):
   s x y z r                                       sphere (centre transformed, radius not)
   p n + n vertex lines "x y z [nx ny nz [u v]]"   polygon, fan-triangulated; flat normals if
                                                   any vertex has none
-  m file                                          mesh file (Wavefront OBJ here)
+  m file                                          mesh file (Wavefront OBJ or COLLADA .dae)
   include file                                    another NFF file in the same scope
   shader name                                     activate a defined shader
-  diffuse name r g b k                            Lambert, reflectance k * rgb
+  diffuse name r g b k [+ "diffusetexture file"]  Lambert, reflectance k * rgb (times the
+                                                  texture's linear RGB at the hit)
   specularreflective name r g b k                 mirror
   speculartransmissivedielectric name ior         glass
   glossy name r g b k alpha                       Beckmann microfacet with alpha
@@ -24,8 +25,8 @@ definitions):
   vacuummedium name                               no medium
   simpleatmosphere name cx cy cz r                exponential atmosphere (tabulated here)
   tabulatedatmosphere name cx cy cz r file.json   atmosphere from the reference's table file
-  larea name uniform r g b power | larea name     uniform area emitter (or activate one;
-                                                  `larea none` deactivates)
+  larea name uniform|parallel r g b power        uniform or parallel area emitter, or
+  larea name                                      activate one (`larea none` deactivates)
   l x y z [r g b k]                               point light
   lsun dx dy dz power [half angle in degrees]     sun (default 0.26)
   lddirection dx dy dz r g b                      distant directional light
@@ -33,8 +34,8 @@ definitions):
   lenv ux uy uz file                              environment map (PFM, or any format Pillow reads)
 Geometry takes the material made of the active shader, medium (the medium inside the
 surface) and area emitter; the shader `invisible` makes the surface a pure medium boundary.
-Not supported here (an error names them): texture lines, `speculardensedielectric`,
-`parallel` area emitters and `yaml{ ... }yaml` sections; the tracer has no counterpart.
+Not supported here (an error names them): `speculardensedielectric` and the yaml keys the
+tracer has no counterpart for.
 """
 from __future__ import annotations
 
@@ -65,6 +66,7 @@ class _Shader:
     alpha: float = 0.0
     ior: float = 1.5
     invisible: bool = False
+    texture: int = -1  # scene texture multiplying the diffuse reflectance
 
 
 @dataclass
@@ -93,6 +95,17 @@ def _default_scope() -> _Scope:
     s.media = {"default": -1}
     s.emitters = {"none": None}
     return s
+
+
+def _axis_angle(axis, angle):
+    """Rotation by `angle` (radians) about the unit vector `axis`, as a 4x4 matrix."""
+    x, y, z = axis
+    c, s, t = math.cos(angle), math.sin(angle), 1 - math.cos(angle)
+    m = np.eye(4)
+    m[:3, :3] = [[t * x * x + c, t * x * y - s * z, t * x * z + s * y],
+                 [t * x * y + s * z, t * y * y + c, t * y * z - s * x],
+                 [t * x * z - s * y, t * y * z + s * x, t * z * z + c]]
+    return m
 
 
 def _rot(axis, a):
@@ -126,17 +139,28 @@ def _floats(tokens, what):
 
 
 def load_obj(path: Path):
-    """Wavefront OBJ: vertices, optional normals, polygons fan-triangulated (negative
-    indices allowed), `usemtl` names per triangle.  Returns (vertices, normals or None,
-    triangles, material name per triangle)."""
-    verts, norms, tris, tri_norms, names = [], [], [], [], []
+    """Wavefront OBJ: vertices, optional texture coordinates and normals, polygons
+    fan-triangulated (negative indices allowed), `usemtl` names per triangle.  When faces
+    carry normals or texture coordinates every triangle corner gets its own vertex (as the
+    reference's assimp import makes them).  Returns (vertices, normals or None, triangles,
+    material name per triangle, texture coordinates or None)."""
+    verts, uvs, norms, tris, names = [], [], [], [], []
     current = None
+
+    def ref(s, n):
+        if not s:
+            return -1
+        k = int(s)
+        return k - 1 if k > 0 else n + k
+
     for raw in Path(path).read_text().splitlines():
         t = raw.split()
         if not t or t[0].startswith("#"):
             continue
         if t[0] == "v":
             verts.append([float(x) for x in t[1:4]])
+        elif t[0] == "vt":
+            uvs.append([float(x) for x in t[1:3]] + [0.0] * max(0, 3 - len(t)))
         elif t[0] == "vn":
             norms.append([float(x) for x in t[1:4]])
         elif t[0] == "usemtl":
@@ -144,23 +168,165 @@ def load_obj(path: Path):
         elif t[0] == "f":
             idx = []
             for c in t[1:]:
-                parts = c.split("/")
-                vi = int(parts[0])
-                ni = int(parts[2]) if len(parts) > 2 and parts[2] else 0
-                idx.append((vi - 1 if vi > 0 else len(verts) + vi, (ni - 1 if ni > 0 else len(norms) + ni) if ni else -1))
+                parts = c.split("/") + ["", ""]
+                idx.append((ref(parts[0], len(verts)), ref(parts[1], len(uvs)), ref(parts[2], len(norms))))
             for k in range(1, len(idx) - 1):
-                tri = (idx[0], idx[k], idx[k + 1])
-                tris.append([p[0] for p in tri])
-                tri_norms.append([p[1] for p in tri])
+                tris.append((idx[0], idx[k], idx[k + 1]))
                 names.append(current)
     v = np.array(verts, np.float64).reshape(-1, 3)
-    t = np.array(tris, np.int64).reshape(-1, 3)
-    tn = np.array(tri_norms, np.int64).reshape(-1, 3)
-    if len(norms) and np.all(tn >= 0):
-        # Unshare vertices so that every corner carries its own normal.
-        n = np.array(norms, np.float64)
-        return v[t.reshape(-1)], n[tn.reshape(-1)], np.arange(3 * len(t)).reshape(-1, 3), names
-    return v, None, t, names
+    c = np.array(tris, np.int64).reshape(-1, 3, 3)  # triangle, corner, (v, vt, vn)
+    t = c[:, :, 0]
+    has_n = len(norms) > 0 and len(c) > 0 and bool(np.all(c[:, :, 2] >= 0))
+    has_uv = len(uvs) > 0 and len(c) > 0 and bool(np.all(c[:, :, 1] >= 0))
+    if not (has_n or has_uv):
+        return v, None, t, names, None
+    # Unshare vertices so that every corner carries its own normal and coordinates.
+    n = np.array(norms, np.float64)[c[:, :, 2].reshape(-1)] if has_n else None
+    uv = np.array(uvs, np.float64)[c[:, :, 1].reshape(-1)][:, :2] if has_uv else None
+    return v[t.reshape(-1)], n, np.arange(3 * len(t)).reshape(-1, 3), names, uv
+
+
+def _dae_floats(text):
+    return [float(x) for x in (text or "").split()]
+
+
+def _dae_node_matrix(node, ns):
+    """Local transform of a COLLADA <node>: its transform elements composed in document
+    order (translate, rotate axis+degrees, scale, matrix)."""
+    M = np.eye(4)
+    for el in node:
+        tag = el.tag[len(ns):]
+        v = _dae_floats(el.text)
+        if tag == "translate":
+            T = np.eye(4)
+            T[:3, 3] = v[:3]
+        elif tag == "rotate":
+            ax = np.array(v[:3], np.float64)
+            n = np.linalg.norm(ax)
+            T = np.eye(4)
+            if n > 0:
+                T[:3, :3] = _axis_angle(ax / n, math.radians(v[3]))[:3, :3]
+        elif tag == "scale":
+            T = np.diag(v[:3] + [1.0])
+        elif tag == "matrix":
+            T = np.array(v[:16], np.float64).reshape(4, 4)
+        else:
+            continue
+        M = M @ T
+    return M
+
+
+def load_dae(path: Path):
+    """COLLADA (.dae) triangle meshes, as the reference's assimp import delivers them for
+    the `m` directive (scenereader::assimp::Read, parse_common.cxx:106-239): every
+    <instance_geometry> of the visual scene's node tree with the node transforms composed
+    from the root, positions scaled by the asset's <unit meter>, <triangles> and <polylist>
+    (fan-triangulated) faces with one vertex per face corner, normals when the mesh has them,
+    faces of zero area dropped (CheckFace), and per face the name of the material bound to
+    its material symbol.  Only Y_UP assets are read.  Returns (vertices, normals or None,
+    triangles, material name per triangle, texture coordinates or None)."""
+    import xml.etree.ElementTree as ET
+    root = ET.parse(path).getroot()
+    ns = root.tag[: root.tag.index("}") + 1] if root.tag.startswith("{") else ""
+    q = lambda tag: ns + tag  # noqa: E731
+    unit = root.find(f"{q('asset')}/{q('unit')}")
+    scale = float(unit.get("meter", "1")) if unit is not None else 1.0
+    up = root.find(f"{q('asset')}/{q('up_axis')}")
+    if up is not None and (up.text or "").strip() not in ("Y_UP", ""):
+        raise ValueError(f"up axis {up.text.strip()} (only Y_UP is read)")
+    mat_names = {m.get("id"): m.get("name", m.get("id")) for m in root.iter(q("material"))}
+    geoms = {g.get("id"): g for g in root.iter(q("geometry"))}
+    verts, norms, uvs, names = [], [], [], []
+    has_normals = True
+    has_uvs = True
+
+    def mesh_faces(geom, M, binding):
+        nonlocal has_normals, has_uvs
+        mesh = geom.find(q("mesh"))
+        if mesh is None:
+            return
+        sources = {}
+        for src in mesh.findall(q("source")):
+            arr = src.find(q("float_array"))
+            acc = src.find(f"{q('technique_common')}/{q('accessor')}")
+            stride = int(acc.get("stride", "1")) if acc is not None else 1
+            vals = np.array(_dae_floats(arr.text if arr is not None else ""), np.float64)
+            sources["#" + src.get("id")] = vals.reshape(-1, stride)
+        vinput = mesh.find(q("vertices"))
+        vsrc = {i.get("semantic"): i.get("source") for i in vinput.findall(q("input"))} if vinput is not None else {}
+        N = np.linalg.inv(M[:3, :3]).T
+        for prim in list(mesh.findall(q("triangles"))) + list(mesh.findall(q("polylist"))):
+            inputs = prim.findall(q("input"))
+            stride = max(int(i.get("offset", "0")) for i in inputs) + 1
+            idx = np.array([int(x) for x in (prim.find(q("p")).text or "").split()], np.int64).reshape(-1, stride)
+            if prim.tag == q("polylist"):
+                counts = [int(x) for x in prim.find(q("vcount")).text.split()]
+            else:
+                counts = [3] * (len(idx) // 3)
+            pos = nrm = tc = None
+            for inp in inputs:
+                sem, off = inp.get("semantic"), int(inp.get("offset", "0"))
+                if sem == "VERTEX":
+                    pos = sources[vsrc["POSITION"]][idx[:, off]][:, :3]
+                    if "NORMAL" in vsrc:
+                        nrm = sources[vsrc["NORMAL"]][idx[:, off]][:, :3]
+                    if "TEXCOORD" in vsrc:
+                        tc = sources[vsrc["TEXCOORD"]][idx[:, off]][:, :2]
+                elif sem == "NORMAL":
+                    nrm = sources[inp.get("source")][idx[:, off]][:, :3]
+                elif sem == "TEXCOORD" and inp.get("set", "0") == "0" and tc is None:
+                    tc = sources[inp.get("source")][idx[:, off]][:, :2]
+            if pos is None:
+                raise ValueError("a face set without positions")
+            pw = np.c_[pos, np.ones(len(pos))] @ M.T
+            name = mat_names.get(binding.get(prim.get("material")), prim.get("material"))
+            start = 0
+            for cnt in counts:
+                for k in range(1, cnt - 1):
+                    c = [start, start + k, start + k + 1]
+                    tri = pw[c, :3] * scale
+                    if np.linalg.norm(np.cross(tri[1] - tri[0], tri[2] - tri[0])) > 0.0:
+                        verts.append(tri)
+                        if nrm is not None:
+                            nn = nrm[c] @ N.T
+                            norms.append(nn / np.maximum(np.linalg.norm(nn, axis=1, keepdims=True), 1e-30))
+                        else:
+                            has_normals = False
+                        if tc is not None and tc.shape[1] >= 2:
+                            uvs.append(tc[c, :2])
+                        else:
+                            has_uvs = False
+                        names.append(name)
+                start += cnt
+
+    def walk(node, parent):
+        M = parent @ _dae_node_matrix(node, ns)
+        for ig in node.findall(q("instance_geometry")):
+            binding = {im.get("symbol"): (im.get("target") or "").lstrip("#")
+                       for im in ig.iter(q("instance_material"))}
+            geom = geoms.get((ig.get("url") or "").lstrip("#"))
+            if geom is None:
+                raise ValueError(f"geometry {ig.get('url')} not found")
+            mesh_faces(geom, M, binding)
+        for child in node.findall(q("node")):
+            walk(child, M)
+
+    scene_ref = root.find(f"{q('scene')}/{q('instance_visual_scene')}")
+    vscenes = {v.get("id"): v for v in root.iter(q("visual_scene"))}
+    vs = vscenes.get((scene_ref.get("url") or "").lstrip("#")) if scene_ref is not None else None
+    if vs is None and vscenes:
+        vs = next(iter(vscenes.values()))
+    if vs is None:
+        raise ValueError("no visual scene")
+    for node in vs.findall(q("node")):
+        walk(node, np.eye(4))
+    if not verts:
+        raise ValueError("no triangles")
+    v = np.concatenate(verts)
+    t = np.arange(len(v)).reshape(-1, 3)
+    n = np.concatenate(norms) if has_normals and norms else None
+    uv = np.concatenate(uvs) if has_uvs and uvs else None
+    return v, n, t, names, uv
 
 
 class _Parser:
@@ -168,7 +334,8 @@ class _Parser:
         self.scene = scene
         self.width, self.height = width, height
         self.materials: Dict[tuple, int] = {}
-        self.meshes = []  # (vertices, normals or None, triangles, material), added at the end
+        self.meshes = []  # (vertices, normals or None, triangles, material, uvs or None), added at the end
+        self.textures: Dict[str, int] = {}  # image file -> scene texture index
 
     # The material of the active things (MakeMaterialFromActiveThings, parsenff.cxx:35-38).
     def material(self, scope: _Scope, shader_name: Optional[str] = None) -> int:
@@ -184,7 +351,7 @@ class _Parser:
                              volume_boundary=em is None)
         else:
             m = MaterialSpec(shader=sh.kind, reflectance=sh.reflectance.copy(), alpha=sh.alpha, ior_ratio=sh.ior,
-                             medium_inside=medium)
+                             medium_inside=medium, diffuse_texture=sh.texture)
         if em is not None:
             m.emission = em.copy()
         idx = self.scene.add_material(m)
@@ -217,7 +384,7 @@ class _Parser:
                 self.yaml_section("\n".join(block), scope, where)
                 continue
             if d == "diffusetexture" or d == "exponenttexture":
-                raise NFFError(f"{where}: textures are not supported by this reader")
+                raise NFFError(f"{where}: {d}: only a diffusetexture right after a diffuse shader is read")
             if d == "transform":
                 scope.transform = _transform(_floats(args, where))
             elif d in ("v", "vfisheye"):
@@ -245,7 +412,7 @@ class _Parser:
                 n = int(args[0])
                 if n < 3:
                     raise NFFError(f"{where}: a polygon needs at least 3 vertices")
-                vs, ns, flat = [], [], False
+                vs, ns, us, flat, no_uv = [], [], [], False, False
                 for _ in range(n):
                     if i >= len(lines):
                         raise NFFError(f"{where}: missing polygon vertices")
@@ -255,18 +422,27 @@ class _Parser:
                         raise NFFError(f"{where}: bad vertex")
                     vs.append(f[:3])
                     flat |= len(f) < 6
+                    no_uv |= len(f) < 8
                     ns.append(f[3:6] if len(f) >= 6 else [0.0, 0.0, 0.0])
+                    us.append(f[6:8] if len(f) >= 8 else [0.0, 0.0])
                 self.add_mesh(np.array(vs), None if flat else np.array(ns),
-                              np.array([[0, k, k + 1] for k in range(1, n - 1)]), scope, self.material(scope))
+                              np.array([[0, k, k + 1] for k in range(1, n - 1)]), scope, self.material(scope),
+                              None if no_uv else np.array(us))
             elif d == "m":
                 path = base.parent / args[0]
-                if path.suffix.lower() != ".obj":
-                    raise NFFError(f"{where}: only OBJ mesh files are read here ({path.name})")
-                v, nrm, t, names = load_obj(path)
+                if path.suffix.lower() == ".obj":
+                    v, nrm, t, names, uv = load_obj(path)
+                elif path.suffix.lower() == ".dae":
+                    try:
+                        v, nrm, t, names, uv = load_dae(path)
+                    except (ValueError, KeyError) as e:
+                        raise NFFError(f"{where}: {path.name}: {e}") from e
+                else:
+                    raise NFFError(f"{where}: mesh format {path.suffix} is not read here (OBJ and COLLADA are)")
                 mats = [self.mesh_material(scope, nm) for nm in names]
                 for mid in sorted(set(mats)):
                     sel = np.array([m == mid for m in mats])
-                    self.add_mesh(v, nrm, t[sel], scope, mid)
+                    self.add_mesh(v, nrm, t[sel], scope, mid, uv)
             elif d == "include":
                 path = base.parent / args[0]
                 self.parse(path.read_text().splitlines(), scope, path)
@@ -276,7 +452,16 @@ class _Parser:
                 scope.shader = args[0]
             elif d == "diffuse":
                 r, g, b, k = _floats(args[1:5], where)
-                scope.shaders[args[0]] = _Shader(abi.SHADER_DIFFUSE, rgb_to_spectrum((k * r, k * g, k * b)))
+                tex = -1
+                # MaybeReadTexture (parsenff.cxx:350-368): a `diffusetexture file` line right after.
+                if i < len(lines) and lines[i].strip().startswith("diffusetexture"):
+                    targs = lines[i].split()[1:]
+                    i += 1
+                    if len(targs) != 1:
+                        raise NFFError(f"{base}:{i}: diffusetexture needs a file name")
+                    tex = self.texture(base.parent / targs[0])
+                scope.shaders[args[0]] = _Shader(abi.SHADER_DIFFUSE, rgb_to_spectrum((k * r, k * g, k * b)),
+                                                 texture=tex)
                 scope.shader = args[0]
             elif d == "specularreflective":
                 r, g, b, k = _floats(args[1:5], where)
@@ -345,10 +530,15 @@ class _Parser:
                     self.activate(scope.emitters, args[0], where)
                     scope.emitter = args[0]
                     continue
-                if args[1] != "uniform":
-                    raise NFFError(f"{where}: only uniform area emitters are supported")
+                if args[1] not in ("uniform", "parallel"):
+                    raise NFFError(f"{where}: area emitter type {args[1]} is unknown")
                 r, g, b, power = _floats(args[2:6], where)
-                scope.emitters[args[0]] = power * rgb_to_spectrum((r, g, b))
+                # ParallelAreaLight (light.hxx:112-146) radiates only along the winding normal,
+                # a delta direction that a camera path's light sample or scattered ray never
+                # meets: under forward path tracing it is a light the picker selects (its
+                # triangles count as area lights) that contributes nothing.
+                scope.emitters[args[0]] = (power * rgb_to_spectrum((r, g, b)) if args[1] == "uniform"
+                                           else np.zeros(NBINS))
                 scope.emitter = args[0]
             elif d == "l":
                 v = _floats(args, where)
@@ -394,7 +584,6 @@ class _Parser:
                     h, p, b = (float(x) * f for x in node["hpb"])
                     m = m @ _rot(1, h) @ _rot(0, p) @ _rot(2, b)
                 if "rotaxis" in node:
-                    from .yaml_scene import _axis_angle
                     r = np.array([float(x) for x in node["rotaxis"]]) * f
                     n = np.linalg.norm(r)
                     if n > 0:
@@ -443,7 +632,7 @@ class _Parser:
                 return self.material(scope, name)
         return self.material(scope)
 
-    def add_mesh(self, v, n, t, scope: _Scope, material: int):
+    def add_mesh(self, v, n, t, scope: _Scope, material: int, uv=None):
         M = scope.transform
         vh = np.c_[v, np.ones(len(v))] @ M.T
         nn = None
@@ -454,32 +643,56 @@ class _Parser:
         used = np.unique(t)
         remap = -np.ones(len(v), np.int64)
         remap[used] = np.arange(len(used))
-        self.meshes.append((vh[used, :3], None if nn is None else nn[used], remap[t], material))
+        self.meshes.append((vh[used, :3], None if nn is None else nn[used], remap[t], material,
+                            None if uv is None else np.asarray(uv, np.float64)[used]))
+
+    def texture(self, path: Path) -> int:
+        """Scene texture index of an image file (read once per file)."""
+        key = str(Path(path).resolve())
+        if key not in self.textures:
+            self.textures[key] = self.scene.add_texture(read_texture(path))
+        return self.textures[key]
 
     def finish(self):
         # The Scene carries normals for all meshes or for none: meshes without get flat ones
         # (Mesh::MakeFlatNormals: every triangle its own vertices and geometric normal).
-        any_n = any(n is not None for _, n, _, _ in self.meshes)
-        for v, n, t, m in self.meshes:
+        any_n = any(n is not None for _, n, _, _, _ in self.meshes)
+        for v, n, t, m, uv in self.meshes:
             if any_n and n is None:
                 v = v[t.reshape(-1)]
+                if uv is not None:
+                    uv = uv[t.reshape(-1)]
                 t = np.arange(len(v)).reshape(-1, 3)
                 g = np.cross(v[t[:, 1]] - v[t[:, 0]], v[t[:, 2]] - v[t[:, 0]])
                 g /= np.maximum(np.linalg.norm(g, axis=1, keepdims=True), 1e-30)
                 n = np.repeat(g, 3, axis=0)
-            self.scene.add_mesh(v, t, m, n)
+            self.scene.add_mesh(v, t, m, n, uv)
+
+
+def srgb_to_linear(x):
+    """Color::SRGBToLinear (spectral.hxx:144-149)."""
+    x = np.asarray(x, np.float64)
+    return np.where(x <= 0.04045, x / 12.92, ((x + 0.055) / 1.055) ** 2.4)
 
 
 def read_image(path: Path) -> np.ndarray:
-    """Float RGB image, row 0 at the top: PFM read here, other formats through Pillow."""
+    """Linear float RGB image, row 0 at the top: PFM and OpenEXR as stored, 8-bit formats
+    through Pillow with the sRGB curve undone (Texture::GetPixel, texture.hxx:94-117)."""
     path = Path(path)
     if path.suffix.lower() == ".pfm":
         return read_pfm(path)
+    if path.suffix.lower() == ".exr":
+        from .image import read_exr
+        return read_exr(path)
     try:
         from PIL import Image
     except ImportError:
-        raise NFFError(f"cannot read {path.name}: only PFM is read without Pillow") from None
-    return np.asarray(Image.open(path).convert("RGB"), np.float32) / 255.0
+        raise NFFError(f"cannot read {path.name}: only PFM and EXR are read without Pillow") from None
+    return srgb_to_linear(np.asarray(Image.open(path).convert("RGB"), np.float64) / 255.0).astype(np.float32)
+
+
+def read_texture(path: Path) -> np.ndarray:
+    return np.ascontiguousarray(read_image(path), dtype=np.float32)
 
 
 def read_pfm(path: Path) -> np.ndarray:

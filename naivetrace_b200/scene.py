@@ -33,6 +33,7 @@ class MaterialSpec:
     medium_inside: int = -1
     medium_outside: int = -1
     volume_boundary: bool = False
+    diffuse_texture: int = -1  # index of the scene texture multiplying the diffuse reflectance
 
     def to_c(self) -> abi.Material:
         m = abi.Material()
@@ -46,6 +47,7 @@ class MaterialSpec:
         m.medium_inside = int(self.medium_inside) + 1  # C ABI: 0 = none, k = medium k-1
         m.medium_outside = int(self.medium_outside) + 1
         m.volume_boundary = int(bool(self.volume_boundary))
+        m.diffuse_texture = int(self.diffuse_texture) + 1  # C ABI: 0 = none, k = texture k-1
         return m
 
 
@@ -206,6 +208,8 @@ class Scene:
         self._norms: List[Optional[np.ndarray]] = []
         self._tris: List[np.ndarray] = []
         self._mats_of_tris: List[np.ndarray] = []
+        self._uvs: List[Optional[np.ndarray]] = []
+        self.textures: List[np.ndarray] = []  # linear RGB float32, (height, width, 3), row 0 at the top
         self._nverts = 0
         self.materials: List[MaterialSpec] = []
         self.env_lights: List[EnvLightSpec] = []
@@ -242,11 +246,22 @@ class Scene:
         a = np.array(self._spheres, dtype=np.float64)
         return np.ascontiguousarray(a[:, :4], dtype=np.float32), np.ascontiguousarray(a[:, 4], dtype=np.uint32)
 
-    def add_mesh(self, vertices, triangles, material: int, normals=None) -> None:
+    def add_texture(self, rgb) -> int:
+        """A diffuse texture (linear RGB, (height, width, 3), row 0 at the top); returns its index."""
+        t = np.ascontiguousarray(rgb, dtype=np.float32)
+        if t.ndim != 3 or t.shape[2] != 3 or t.shape[0] < 1 or t.shape[1] < 1:
+            raise ValueError("a texture is a (height, width, 3) array")
+        self.textures.append(t)
+        return len(self.textures) - 1
+
+    def add_mesh(self, vertices, triangles, material: int, normals=None, uvs=None) -> None:
         v = np.ascontiguousarray(vertices, dtype=np.float32).reshape(-1, 3)
         t = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1, 3)
         if t.size and int(t.max()) >= len(v):
             raise ValueError("triangle index out of range")
+        self._uvs.append(None if uvs is None else np.ascontiguousarray(uvs, dtype=np.float32).reshape(-1, 2))
+        if self._uvs[-1] is not None and len(self._uvs[-1]) != len(v):
+            raise ValueError("one texture coordinate pair per vertex")
         self._verts.append(v)
         self._norms.append(None if normals is None else np.ascontiguousarray(normals, dtype=np.float32).reshape(-1, 3))
         self._tris.append(t + np.uint32(self._nverts))
@@ -275,6 +290,14 @@ class Scene:
                 norms = None
             self._flat = (np.ascontiguousarray(verts), norms, np.ascontiguousarray(tris), np.ascontiguousarray(mats))
         return self._flat
+
+    def uv_array(self):
+        """Texture coordinates of all vertices (num_vertices, 2), zeros for meshes without;
+        None when no mesh has any."""
+        if all(u is None for u in self._uvs):
+            return None
+        return np.ascontiguousarray(np.concatenate(
+            [u if u is not None else np.zeros((len(v), 2), np.float32) for v, u in zip(self._verts, self._uvs)]))
 
     @property
     def num_triangles(self) -> int:
@@ -351,6 +374,19 @@ class Scene:
         d.camera.fov_deg = float(cam.fov_deg)
         d.camera.xres = int(cam.xres)
         d.camera.yres = int(cam.yres)
+        uv = self.uv_array()
+        keep.append(uv)
+        d.uvs = uv.ctypes.data_as(C.POINTER(C.c_float)) if uv is not None else None
+        texs = []
+        for t in self.textures:
+            tx = abi.Texture()
+            tx.height, tx.width = int(t.shape[0]), int(t.shape[1])
+            tx.rgb = t.ctypes.data_as(C.POINTER(C.c_float))
+            texs.append(tx)
+        tex_arr = (abi.Texture * max(1, len(texs)))(*texs)
+        keep.append(tex_arr)
+        d.num_textures = len(texs)
+        d.textures = C.cast(tex_arr, C.POINTER(abi.Texture))
         return d, keep
 
 

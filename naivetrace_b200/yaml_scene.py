@@ -5,26 +5,25 @@ A file is one scope: a mapping with any of
   transforms: [{pos: [x,y,z]} | {hpb: [h,p,b], rad: bool} | {rotaxis: [x,y,z], rad: bool} |
                {scale: [x,y,z]}, ...]   composed in order onto the scope's transform
                (degrees unless rad: true)
-  shaders:    [{name, class: diffuse | glossy | speculartransmissivedielectric, rgb, rgb_x,
-                alpha, ior_ratio}, ...]
+  shaders:    [{name, class: diffuse | glossy | speculartransmissivedielectric |
+                glossytransmissivedielectric, rgb, rgb_x, alpha, ior_ratio, texture}, ...]
   media:      [{name, class: homogeneous, absorb, absorb_x, scatter, scatter_x,
                 phasefunction: {class: rayleigh | henleygreenstein, g}}, ...]
-  arealights: [{name, class: uniform, rgb, rgb_x}, ...]
+  arealights: [{name, class: uniform | parallel, rgb, rgb_x}, ...]
   lights:     [{class: point, position, rgb, rgb_x} | {class: sun, direction, total_power,
                 opening_angle_deg} | {class: directional | dome, direction, rgb, rgb_x} |
                {class: env, direction, filename}, ...]
   materials:  [{name, shader, medium, outer_medium, arealight}, ...]  each a name or an
                inlined item
   models:     [{sphere, position, radius, defaultmaterial} |
-               {file: mesh.obj, defaultmaterial, materialmap: {obj material: material}}, ...]
+               {file: mesh.obj | mesh.dae, defaultmaterial, materialmap: {mesh material: material}}, ...]
   scopes:     [scope, ...]  nested, inheriting and then forgetting definitions and transform
   view:       {from, at, up, angle}  (resolution from the caller, default 640 x 480)
 Sections are read in the reference's order (transforms, shaders, media, arealights, lights,
 materials, models, scopes, view).  Colours are RGB (default 1) times the `_x` factor,
 converted to spectra.  A sphere's radius scales with the cube root of the transform's
-determinant.  Classes the tracer has no counterpart for (glossy transmissive and dense
-dielectrics, modulated-density media, parallel area lights, textures) and non-OBJ mesh
-files raise an error naming them.
+determinant.  Classes the tracer has no counterpart for (dense dielectrics,
+modulated-density media, roughness textures) raise an error naming them.
 """
 from __future__ import annotations
 
@@ -36,7 +35,7 @@ from typing import Optional
 import numpy as np
 
 from . import abi
-from .nff import NFFError, _Parser, _Scope, _Shader, _default_scope, load_obj, read_image
+from .nff import NFFError, _axis_angle, _Parser, _Scope, _Shader, _default_scope, load_dae, load_obj, read_image
 from .scene import CameraSpec, MediumSpec, Scene, directional_light, dome_light, env_map, sun_light
 from .spectral import rgb_to_spectrum
 
@@ -47,16 +46,6 @@ def _spectrum(node: dict, prefix: str) -> np.ndarray:
     rgb = node.pop(prefix, [1.0, 1.0, 1.0])
     k = float(node.pop(prefix + "_x", 1.0))
     return rgb_to_spectrum([k * float(x) for x in rgb])
-
-
-def _axis_angle(axis, angle):
-    x, y, z = axis
-    c, s, t = math.cos(angle), math.sin(angle), 1 - math.cos(angle)
-    m = np.eye(4)
-    m[:3, :3] = [[t * x * x + c, t * x * y - s * z, t * x * z + s * y],
-                 [t * x * y + s * z, t * y * y + c, t * y * z - s * x],
-                 [t * x * z - s * y, t * y * z + s * x, t * z * z + c]]
-    return m
 
 
 def parse_transform(items) -> np.ndarray:
@@ -97,7 +86,9 @@ class _YamlReader(_Parser):
         cls = node.pop("class")
         node.pop("prefer_path_tracing", None)
         if cls == "diffuse":
-            sh = _Shader(abi.SHADER_DIFFUSE, _spectrum(node, "rgb"))
+            tex = node.pop("texture", None)
+            sh = _Shader(abi.SHADER_DIFFUSE, _spectrum(node, "rgb"),
+                         texture=self.texture(self.base.parent / tex) if tex else -1)
         elif cls == "glossy":
             alpha = float(node.pop("alpha"))
             sh = _Shader(abi.SHADER_MICROFACET, _spectrum(node, "rgb"), alpha=alpha)
@@ -149,9 +140,12 @@ class _YamlReader(_Parser):
         node = dict(node)
         name = node.pop("name", None) or f"_inline{len(scope.emitters)}"
         cls = node.pop("class")
-        if cls != "uniform":
-            raise NFFError(f"area light class {cls} is not supported by this tracer")
-        scope.emitters[name] = _spectrum(node, "rgb")
+        if cls not in ("uniform", "parallel"):
+            raise NFFError(f"area light class {cls} is unknown")
+        spec = _spectrum(node, "rgb")
+        # A parallel area light (light.hxx:112-146) emits along the winding normal only: a
+        # selected light that contributes nothing to forward path tracing.
+        scope.emitters[name] = spec if cls == "uniform" else np.zeros(NBINS)
         if node:
             raise NFFError(f"area light {name}: unknown keys {sorted(node)}")
         return name
@@ -224,13 +218,16 @@ class _YamlReader(_Parser):
             self.scene.add_sphere(c[:3], r, self.material_index(scope, mats, default))
         elif "file" in node:
             path = self.base.parent / node.pop("file")
-            if path.suffix.lower() != ".obj":
-                raise NFFError(f"model {path.name}: only OBJ mesh files are read here")
-            v, nrm, t, names = load_obj(path)
+            if path.suffix.lower() == ".obj":
+                v, nrm, t, names, uv = load_obj(path)
+            elif path.suffix.lower() == ".dae":
+                v, nrm, t, names, uv = load_dae(path)
+            else:
+                raise NFFError(f"model {path.name}: mesh format {path.suffix} is not read here (OBJ and COLLADA are)")
             idx = [self.material_index(scope, mats, mmap.get(nm, default) if nm else default) for nm in names]
             for mid in sorted(set(idx)):
                 sel = np.array([i == mid for i in idx])
-                self.add_mesh(v, nrm, t[sel], scope, mid)
+                self.add_mesh(v, nrm, t[sel], scope, mid, uv)
         else:
             raise NFFError("model needs `sphere` or `file`")
         if node:

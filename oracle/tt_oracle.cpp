@@ -397,7 +397,52 @@ struct Surf {
   V3 normal;           // oriented toward where the incident ray came from
   V3 shading_normal;
   V3 pos_bounds;
+  float tex_u = 0.f, tex_v = 0.f;        // SurfaceInteraction::tex_coord
+  const struct Texture* tex = nullptr;   // the material's diffuse texture, if any
 };
+
+// Texture (texture.hxx:15-117): linear RGB, row 0 at the top; UvToPixel wraps the
+// coordinates to [0, 1) with v up, GetPixel returns the texel.
+struct Texture {
+  int w = 0, h = 0;
+  std::vector<float> rgb;
+  void Lookup(float u, float v, double out[3]) const {
+    float dummy;
+    u = std::modf(u, &dummy);
+    v = std::modf(v, &dummy);
+    if (u < 0.f) u = 1.f + u;
+    if (v < 0.f) v = 1.f + v;
+    if (u > 1.f - EpsF) u -= EpsF;
+    if (v > 1.f - EpsF) v -= EpsF;
+    const int x = std::min(std::max((int)(u * w), 0), w - 1);
+    const int y = std::min(std::max(h - (int)(v * h) - 1, 0), h - 1);
+    const float* p = &rgb[3 * ((size_t)y * w + x)];
+    out[0] = p[0];
+    out[1] = p[1];
+    out[2] = p[2];
+  }
+};
+
+// KartesianToSpherical (third component up, vec3f.hxx:298-321) and SphericalToUv
+// (vec3f.hxx:286-295) in float, as FirstIntersectionSphere maps a sphere hit's normal
+// (embreeaccelerator.cxx:258).
+inline void DirectionToUv(V3 d, float* u, float* v) {
+  const float x = (float)d.x, z = (float)d.y, y = (float)d.z;
+  const float ax = std::abs(x), az = std::abs(z);
+  const float r = std::sqrt(x * x + y * y + z * z);
+  const float theta = std::acos(std::min(1.f, std::max(-1.f, y / r)));
+  float phi;
+  const float pi = (float)Pi;
+  if (ax > az) {
+    phi = std::atan2(z, ax);
+    phi = (x > 0.f) ? phi : pi - phi;
+  } else {
+    phi = std::atan2(x, az);
+    phi = (z > 0.f) ? (pi / 2.f) - phi : (3.f / 2.f * pi) + phi;
+  }
+  *u = phi / (2.f * pi);
+  *v = theta / pi;
+}
 
 inline V3 AntiSelfIntersectionOffset(const Surf& s, V3 exitant_dir) {
   const V3 n = s.geometry_normal;
@@ -472,6 +517,8 @@ struct Scene {
   std::vector<F3> vert, nrm;
   std::vector<uint32_t> idx, mat_of_tri;  // mat_of_tri: per primitive (triangles, then spheres)
   bool has_normals = false;
+  std::vector<float> uv;           // 2 per vertex (Mesh::uvs), empty when none were given
+  std::vector<Texture> textures;
   std::vector<Material> materials;
   std::vector<EnvLight> env;
   std::vector<tt_point_light> points;
@@ -835,6 +882,11 @@ inline V3 SphereBounds(V3 pos) {
 // Sphere surface point with outward normal n (Spheres::GetLocalGeometry,
 // primitive.cxx:214-223, and FirstIntersectionSphere, embreeaccelerator.cxx:247-260: the
 // position is projected onto the sphere along the normal).
+inline const Texture* MaterialTexture(const Scene& s, int prim) {
+  const int t = s.materials[s.mat_of_tri[prim]].m.diffuse_texture - 1;
+  return t >= 0 ? &s.textures[t] : nullptr;
+}
+
 inline Surf SphereSurface(const Scene& s, int prim, V3 n) {
   Surf si;
   si.prim = prim;
@@ -843,6 +895,8 @@ inline Surf SphereSurface(const Scene& s, int prim, V3 n) {
   si.geometry_normal = n;
   si.smooth_normal = n;
   si.pos_bounds = SphereBounds(si.pos);
+  si.tex = MaterialTexture(s, prim);
+  if (si.tex) DirectionToUv(n, &si.tex_u, &si.tex_v);
   return si;
 }
 
@@ -865,6 +919,14 @@ inline Surf SurfaceFromHit(const Scene& s, int prim, double u, double v, V3 org,
   si.geometry_normal = GeometryNormal(s, prim);
   si.smooth_normal = SmoothNormal(s, prim, 1. - u - v, u, v, si.geometry_normal);
   si.pos_bounds = PosBounds(p0, p1, p2, si.barry);
+  si.tex = MaterialTexture(s, prim);
+  if (si.tex && !s.uv.empty()) {
+    // rtcInterpolate1 of the uv attribute (embreeaccelerator.cxx:226-228), in float.
+    const uint32_t a = s.idx[3 * prim], b = s.idx[3 * prim + 1], c = s.idx[3 * prim + 2];
+    const float fu = (float)u, fv = (float)v, fw = 1.f - fu - fv;
+    si.tex_u = s.uv[2 * a] * fw + s.uv[2 * b] * fu + s.uv[2 * c] * fv;
+    si.tex_v = s.uv[2 * a + 1] * fw + s.uv[2 * b + 1] * fu + s.uv[2 * c + 1] * fv;
+  }
   const double sign = -Sign(Dot(ray_dir, si.geometry_normal));
   si.normal = sign * si.geometry_normal;
   si.shading_normal = sign * si.smooth_normal;
@@ -1015,6 +1077,18 @@ static S3 EvaluateDielectricMollified(const tt_material& m, V3 wi, const Surf& s
   return S3(total_val);
 }
 
+// DiffuseShader's reflectance times MaybeMultiplyTextureLookup (shader.cxx:17-27): the
+// texel's RGB as the selected wavelengths' values.
+inline S3 DiffuseReflectance(const tt_material& m, const Surf& si, const int32_t idx[3]) {
+  S3 kr = Take(m.reflectance, idx);
+  if (si.tex) {
+    double rgb[3];
+    si.tex->Lookup(si.tex_u, si.tex_v, rgb);
+    kr = kr * RGBToSpectralSelection(rgb, idx);
+  }
+  return kr;
+}
+
 static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const int32_t idx[3], double* pdf,
                        double min_roughness = 0.) {
   if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && min_roughness > 0.)
@@ -1024,7 +1098,7 @@ static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const
       S3 ret(0.);
       double n_dot_out = Dot(si.normal, wo);
       double nsh_dot_out = Dot(si.shading_normal, wo);
-      if (n_dot_out > 0.) ret = Take(m.reflectance, idx) * (1. / Pi);
+      if (n_dot_out > 0.) ret = DiffuseReflectance(m, si, idx) * (1. / Pi);
       if (pdf) *pdf = std::max(0., nsh_dot_out) / Pi;
       return ret;
     }
@@ -1115,7 +1189,7 @@ static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sam
       V3 v = ToCosHemisphere(r);
       out.pdf = v.z / Pi;
       out.dir = fr.ToWorld(v);
-      out.value = Dot(si.normal, out.dir) > 0 ? Take(m.reflectance, idx) * (1. / Pi) : S3(0.);
+      out.value = Dot(si.normal, out.dir) > 0 ? DiffuseReflectance(m, si, idx) * (1. / Pi) : S3(0.);
       return out;
     }
     case TT_SHADER_SPECULAR_REFLECTIVE: {
@@ -1831,6 +1905,8 @@ struct Worker {
     max_path_node_count = s.params.max_ray_depth + 1;
     if (s.params.pt_sample_mode == TT_SAMPLE_BSDF) do_sample_lights = false;
     if (s.params.pt_sample_mode == TT_SAMPLE_LIGHTS) do_sample_brdf = false;
+    // A scene without lights has nothing to connect to (and no light to pick).
+    if (s.env.empty() && s.area_lights.empty() && s.points.empty()) do_sample_lights = false;
   }
 
   double DFactorOf(const Node& n, V3 dir) const {
@@ -2268,6 +2344,7 @@ struct Worker2 {
     max_node_count = s.params.max_ray_depth;
     if (s.params.pt_sample_mode == TT_SAMPLE_BSDF) use_nee = false;
     if (s.params.pt_sample_mode == TT_SAMPLE_LIGHTS) use_emission = false;
+    if (s.env.empty() && s.area_lights.empty() && s.points.empty()) use_nee = false;
   }
 
   // Medium::ComputeMajorante and EvaluateCoeffs; medium -1 is the vacuum.
@@ -2651,6 +2728,16 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
   }
   s.idx.assign(d->indices, d->indices + 3 * (size_t)d->num_triangles);
   s.mat_of_tri.assign(d->material_ids, d->material_ids + d->num_triangles);
+  if (d->uvs) s.uv.assign(d->uvs, d->uvs + 2 * (size_t)d->num_vertices);
+  for (uint32_t i = 0; i < d->num_textures; ++i) {
+    const tt_texture& t = d->textures[i];
+    if (!t.rgb || t.width <= 0 || t.height <= 0) { g_err = "bad texture"; return false; }
+    Texture tx;
+    tx.w = t.width;
+    tx.h = t.height;
+    tx.rgb.assign(t.rgb, t.rgb + 3 * (size_t)t.width * t.height);
+    s.textures.push_back(std::move(tx));
+  }
   for (uint32_t i = 0; i < d->num_media; ++i) {
     const tt_medium& m = d->media[i];
     MediumDesc md;
@@ -2699,6 +2786,10 @@ static bool BuildScene(Scene& s, const tt_scene_desc* d, const tt_params* p) {
     if (m.medium_inside < 0 || m.medium_inside > (int)d->num_media || m.medium_outside < 0 ||
         m.medium_outside > (int)d->num_media) {
       g_err = "medium index out of range";
+      return false;
+    }
+    if (m.diffuse_texture < 0 || m.diffuse_texture > (int)d->num_textures) {
+      g_err = "texture index out of range";
       return false;
     }
     s.materials.push_back(Material{m});

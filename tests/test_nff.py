@@ -92,7 +92,7 @@ def test_resolution_override_and_text_input():
 @pytest.mark.parametrize("text,msg", [("v\nfrom 0 0 0\nat 0 0 1\nup 0 1 0\nresolution 4 4\nangle 30\nfoo 1\n", ":7"),
                                       ("yaml{\nlight: 1\n}yaml\n", "not supported"),
                                       ("shader nothere\n", "unknown shader"),
-                                      ("larea a parallel 1 1 1 1\n", "uniform"),
+                                      ("larea a spot 1 1 1 1\n", "unknown"),
                                       ("p 2\n0 0 0\n1 0 0\n", "3 vertices")])
 def test_errors_name_the_line(text, msg):
     with pytest.raises(NFFError, match=msg):
@@ -144,3 +144,50 @@ def test_nff_yaml_section():
     m = s.materials[int(s.sphere_arrays()[1][0])]
     assert m.shader == abi.SHADER_MICROFACET and m.alpha == pytest.approx(0.3)
     np.testing.assert_allclose(m.reflectance, rgb_to_spectrum((0.5, 0.5, 0.5)))
+
+
+REFSCENES = Path(__file__).parent / "golden" / "refscenes"
+
+
+def test_collada_unit_cube():
+    """unitcube.dae: 12 triangles in centimetres (<unit meter="0.01">), scaled to a unit cube
+    centred at the origin; one normal per face corner, pointing outwards."""
+    from naivetrace_b200.nff import load_dae
+    v, n, t, names, uv = load_dae(REFSCENES / "unitcube.dae")
+    assert len(t) == 12 and n is not None and uv is not None
+    np.testing.assert_allclose(v.min(axis=0), [-0.5] * 3)
+    np.testing.assert_allclose(v.max(axis=0), [0.5] * 3)
+    tri = v[t]
+    centre = tri.mean(axis=1)
+    assert np.all(np.einsum("ij,ij->i", n[t[:, 0]], centre) > 0)
+
+
+def test_collada_cornell_box_materials():
+    """cornelbox.dae: the node translation, per face-set material symbols bound to the named
+    materials of <library_materials>."""
+    from naivetrace_b200.nff import load_dae
+    v, n, t, names, uv = load_dae(REFSCENES / "cornelbox.dae")
+    assert sorted(set(names)) == ["blue", "green", "red", "white"]
+    np.testing.assert_allclose(v.min(axis=0), [-0.5, 0.0, -1.2], atol=1e-9)
+    np.testing.assert_allclose(v.max(axis=0), [0.5, 1.0, 0.0], atol=1e-9)
+
+
+@pytest.mark.parametrize("path", sorted(REFSCENES.glob("*.nff")), ids=lambda p: p.stem)
+def test_reference_scenes_parse(path):
+    s = parse_nff(path, width=16, height=16)
+    assert s.num_triangles + s.num_spheres > 0
+    if path.stem in ("refractive_sphere_caustics", "refract_beam_at_cube"):
+        assert len(s.textures) == 1 and s.uv_array() is not None
+        tex = [m for m in s.materials if m.diffuse_texture >= 0]
+        assert tex and s.textures[0].shape[2] == 3 and s.textures[0].max() <= 1.0
+    if path.stem == "litcorner2":
+        em = [m for m in s.materials if m.emission is not None]
+        assert len(em) == 1 and not em[0].emission.any()  # parallel: an emitter that radiates nothing here
+
+
+def test_srgb_texture_is_linearised(tmp_path):
+    from PIL import Image
+    from naivetrace_b200.nff import read_texture
+    Image.fromarray(np.array([[[0, 128, 255]]], np.uint8)).save(tmp_path / "t.png")
+    t = read_texture(tmp_path / "t.png")
+    np.testing.assert_allclose(t[0, 0], [0.0, ((128 / 255 + 0.055) / 1.055) ** 2.4, 1.0], rtol=1e-6)
