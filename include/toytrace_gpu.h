@@ -413,7 +413,10 @@ enum { TT_GUIDE_LEARNED = 0, TT_GUIDE_TREE = 1 };
 enum { TT_GUIDE_NET_TCGEN05 = 0, TT_GUIDE_NET_MMA = 1 };
 
 /* Enables or disables guiding.  The network is created (He-uniform weights from `seed`) on
- * first use and keeps its trained weights while guiding is switched off and on again. */
+ * first use and keeps its trained weights while guiding is switched off and on again.  Until
+ * its first training step (or tt_guide_set_params) the network is not sampled: guided
+ * vertices draw from the BSDF alone, which keeps the first pass as good as unguided
+ * rendering while it collects the first training records. */
 tt_status tt_set_guiding(tt_ctx* ctx, const tt_guiding_params* params);
 /* Number of network parameters (FP32 layout: per layer W[out][in] then b[out]). */
 int32_t tt_guide_num_params(void);

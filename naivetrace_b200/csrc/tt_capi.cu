@@ -1136,6 +1136,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
     const double expected = c->rec_rate * (double)total;
     c->dev.guide_keep = expected > 0.0 ? (float)std::min(1.0, 0.8 * c->rec_cap / expected) : 1.f;
   }
+  c->dev.guide_cold = (c->dev.guide && c->dev.guide_method == TT_GUIDE_LEARNED && c->gnet && c->gnet->fresh) ? 1 : 0;
   tt_status st = ensure_path_state_fit(c, &cap);
   if (st != TT_OK) return st;
   const bool counting = c->profiling >= 2;
@@ -1936,6 +1937,7 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
     const double expected = c->rec_rate * (double)paths;
     c->dev.guide_keep = expected > 0.0 ? (float)std::min(1.0, 0.8 * c->rec_cap / expected) : 1.f;
   }
+  c->dev.guide_cold = (c->dev.guide && c->dev.guide_method == TT_GUIDE_LEARNED && c->gnet && c->gnet->fresh) ? 1 : 0;
   tt_status st = ensure_path_state_fit(c, &cap);
   if (st != TT_OK) return st;
   const int nwaves = (int)((paths + cap - 1) / cap);

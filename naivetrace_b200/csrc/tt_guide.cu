@@ -526,6 +526,7 @@ bool GuideNet::init(uint64_t seed, std::string* err) {
 }
 
 bool GuideNet::set_params(const float* host, std::string* err) {
+  fresh = false;
   cudaMemcpy(params, host, kGParams * sizeof(float), cudaMemcpyHostToDevice);
   k_to_bf16<<<grid1(kGParams), 256>>>(params, kGParams, params16);
   const cudaError_t e = cudaDeviceSynchronize();
@@ -601,6 +602,7 @@ void GuideNet::features(const float* pts, int n, bf16* x, cudaStream_t st) {
 
 static AdamArgs adam_args(GuideNet& g, float lr) {
   ++g.step;
+  g.fresh = false;
   const float b1 = 0.9f, b2 = 0.999f;
   return AdamArgs{g.params, g.adam_m, g.adam_v, g.params16, lr, b1, b2, 1e-8f,
                   1.f - std::pow(b1, (float)g.step), 1.f - std::pow(b2, (float)g.step)};

@@ -21,6 +21,7 @@ struct GuideNet {
   float* grad = nullptr;
   float* loss = nullptr;         // mean loss of the last gradient
   int step = 0;
+  bool fresh = true;             // still the random initial weights (no Adam step, no set_params)
   // Training scratch for up to `cap` records: features, hidden activations, their
   // gradients, output gradients, FP32 outputs (batch forward) and the weight-gradient
   // partials of the record chunks.

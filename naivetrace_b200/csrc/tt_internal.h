@@ -131,6 +131,8 @@ struct DevScene {
   int guide;                  // 1: guided scattering
   int guide_record;           // 1: collect training records
   int guide_depth;            // guided vertices only at bounces < guide_depth
+  int guide_cold;             // 1: the network still has its random initial weights: guided
+                              // vertices sample the BSDF only (records are still collected)
   float guide_keep;           // probability that a finished path keeps its record (a uniform
                               // subsample when a pass would yield more than the pool holds)
   const __nv_bfloat16* guide_w16;  // network weights (BF16, flat layout of tt_guide.cuh)

@@ -1210,7 +1210,10 @@ __device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const Path
   const float3 wi = -dir;
   float3 ndir, val;
   float pb = 0.f;
-  if (rng.uniform() < mix.c) {
+  // An untrained network is not sampled: selection probability 0 gives plain BSDF sampling
+  // with the BSDF density, while the records for the first training step are collected.
+  const float c = sc.guide_cold ? 0.f : mix.c;
+  if (rng.uniform() < c) {
     ndir = guide_mixture_sample(mix, rng);
     val = eval_bsdf(m, wi, s, ndir, l, &pb);
   } else {
@@ -1220,11 +1223,11 @@ __device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const Path
     pb = ss.pdf;
   }
   const float pg = guide_mixture_pdf(mix, ndir);
-  const float pdf = (1.f - mix.c) * pb + mix.c * pg;
+  const float pdf = (1.f - c) * pb + c * pg;
   const float4 nee = pre.nee;
   if (nee.w != 0.f) {
     const float3 sd = xyz(p.sh_d[slot]);
-    const float pdf_due = ((1.f - mix.c) * nee.z + mix.c * guide_mixture_pdf(mix, sd)) * nee.y;
+    const float pdf_due = ((1.f - c) * nee.z + c * guide_mixture_pdf(mix, sd)) * nee.y;
     if (MEDIA) {
       p.sh_med[slot].y = pdf_due;
     } else if (nee.x > 0.f) {
