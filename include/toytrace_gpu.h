@@ -47,8 +47,11 @@ enum {
   TT_SHADER_SPECULAR_REFLECTIVE = 1, /* SpecularReflectiveShader shader.cxx:322-366 */
   TT_SHADER_SPECULAR_DIELECTRIC = 2, /* SpecularTransmissiveDielectricShader shader.cxx:378-630 */
   TT_SHADER_MICROFACET = 3,          /* MicrofacetShader (Beckmann, VNDF) shader.cxx:634-707 */
-  TT_SHADER_GLOSSY_DIELECTRIC = 4    /* GlossyTransmissiveDielectricShader (rough Beckmann
+  TT_SHADER_GLOSSY_DIELECTRIC = 4,   /* GlossyTransmissiveDielectricShader (rough Beckmann
                                         interface, alpha and ior_ratio) shader.cxx:710-787 */
+  TT_SHADER_SPECULAR_DENSE_DIELECTRIC = 5 /* SpecularDenseDielectricShader: a smooth coating with
+                                        Schlick reflectivity specular_reflectivity over a Lambert
+                                        base of the reflectance (shader.cxx:977-1081) */
 };
 
 /* A material = shader + optional area emitter + optional media on either side
@@ -69,7 +72,10 @@ typedef struct tt_material {
   int32_t volume_boundary;         /* nonzero: medium boundary only, no surface */
   int32_t diffuse_texture;         /* TT_SHADER_DIFFUSE: 1 + index of the tt_texture that multiplies
                                       the reflectance at the hit's texture coordinates
-                                      (MaybeMultiplyTextureLookup, shader.cxx:17-27); 0 = none */
+                                      (MaybeMultiplyTextureLookup, shader.cxx:17-27); 0 = none
+                                      (also the dense dielectric's diffuse base) */
+  float specular_reflectivity;     /* TT_SHADER_SPECULAR_DENSE_DIELECTRIC: reflectivity at normal
+                                      incidence of the coating */
 } tt_material;
 
 /* An RGB texture (Texture, texture.hxx:15-117): linear RGB floats, width * height * 3, row 0 =

@@ -34,6 +34,7 @@ SHADER_SPECULAR_REFLECTIVE = 1
 SHADER_SPECULAR_DIELECTRIC = 2
 SHADER_MICROFACET = 3
 SHADER_GLOSSY_DIELECTRIC = 4
+SHADER_SPECULAR_DENSE_DIELECTRIC = 5
 
 ENV_DOME = 0
 ENV_SUN = 1
@@ -62,6 +63,7 @@ class Material(C.Structure):
         ("medium_outside", C.c_int32),
         ("volume_boundary", C.c_int32),
         ("diffuse_texture", C.c_int32),
+        ("specular_reflectivity", C.c_float),
     ]
 
 

@@ -369,7 +369,7 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   }
   for (uint32_t i = 0; i < d->num_materials; ++i) {
     const tt_material& m = d->materials[i];
-    if (m.shader < TT_SHADER_DIFFUSE || m.shader > TT_SHADER_GLOSSY_DIELECTRIC)
+    if (m.shader < TT_SHADER_DIFFUSE || m.shader > TT_SHADER_SPECULAR_DENSE_DIELECTRIC)
       return fail(nullptr, TT_ERR_INVALID, "unknown shader kind in material " + std::to_string(i));
     if ((m.shader == TT_SHADER_MICROFACET || m.shader == TT_SHADER_GLOSSY_DIELECTRIC) && !(m.alpha > 0.f))
       return fail(nullptr, TT_ERR_INVALID, "microfacet roughness must be positive");
@@ -380,8 +380,11 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
       return fail(nullptr, TT_ERR_INVALID, "medium index out of range in material " + std::to_string(i));
     if (m.diffuse_texture < 0 || m.diffuse_texture > (int)d->num_textures)
       return fail(nullptr, TT_ERR_INVALID, "texture index out of range in material " + std::to_string(i));
-    if (m.diffuse_texture > 0 && m.shader != TT_SHADER_DIFFUSE)
-      return fail(nullptr, TT_ERR_INVALID, "a texture needs the diffuse shader (material " + std::to_string(i) + ")");
+    if (m.diffuse_texture > 0 && m.shader != TT_SHADER_DIFFUSE && m.shader != TT_SHADER_SPECULAR_DENSE_DIELECTRIC)
+      return fail(nullptr, TT_ERR_INVALID, "a texture needs a diffuse base (material " + std::to_string(i) + ")");
+    if (m.shader == TT_SHADER_SPECULAR_DENSE_DIELECTRIC &&
+        !(m.specular_reflectivity >= 0.f && m.specular_reflectivity <= 1.f))
+      return fail(nullptr, TT_ERR_INVALID, "dense dielectric reflectivity must lie in [0, 1]");
   }
   if (d->num_media > 0 && !d->media) return fail(nullptr, TT_ERR_INVALID, "media missing");
   if (d->num_spheres > (1u << 26)) return fail(nullptr, TT_ERR_CAPACITY, "more than 2^26 spheres");
@@ -707,6 +710,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     std::memcpy(dm[i].emission, m.emission, sizeof(m.emission));
     dm[i].tex = nullptr;
     dm[i].tex_w = dm[i].tex_h = 0;
+    dm[i].spec = m.specular_reflectivity;
   }
   // Textures (one device array each) and the per-vertex texture coordinates.
   {

@@ -463,6 +463,20 @@ __device__ __forceinline__ float3 diffuse_kr(const DevMaterial& m, const Surf& s
   return kr;
 }
 
+// SpecularDenseDielectricShader (shader.cxx:977-1081): Schlick reflectivity of the coating
+// (SchlicksApproximation, shader_physics.hxx:95-101) and the diffuse attenuation
+// (1 - R(w_in)) (1 - R(w_out)) / (1 - average albedo) of Kelemen and Szirmay-Kalos 2001
+// (DiffuseAttenuationFactor), the average albedo k + (1 - k) 2 / 42
+// (AverageOfProjectedSchlicksApproximationOverHemisphere).
+__device__ __forceinline__ float schlick(float k, float cos_n) {
+  const float x = 1.f - cos_n;
+  return k + (1.f - k) * (x * x * x * x * x);
+}
+__device__ __forceinline__ float dense_attenuation(float k, float r_in, float r_out) {
+  const float avg = k + (1.f - k) * (2.f / 42.f);
+  return (1.f - r_in) * (1.f - r_out) / (1.f - avg);
+}
+
 // Shader::MyRoughness (shader.cxx:244-247, 666-670, 728-731): the alpha of the microfacet
 // and of the glossy dielectric, 0 otherwise.
 __device__ __forceinline__ float my_roughness(const DevMaterial& m) {
@@ -571,6 +585,17 @@ __device__ __forceinline__ float3 eval_bsdf(const DevMaterial& m, float3 wi, con
     const float v = glossy_dielectric_eval(g, g.fr.to_local(wo), pdf);
     return f3(v, v, v);
   }
+  if (m.shader == TT_SHADER_SPECULAR_DENSE_DIELECTRIC) {
+    // The diffuse part; the specular reflection is a delta lobe.
+    if (!(dot3(s.n, wo) > 0.f)) {
+      if (pdf) *pdf = 0.f;
+      return f3(0.f, 0.f, 0.f);
+    }
+    const float r_in = schlick(m.spec, fmaxf(0.f, dot3(s.ns, wi)));
+    const float r_out = schlick(m.spec, fmaxf(0.f, dot3(s.ns, wo)));
+    if (pdf) *pdf = fmaxf(0.f, dot3(s.ns, wo)) / kPi * (1.f - r_in);
+    return diffuse_kr(m, s, l) * ((1.f / kPi) * dense_attenuation(m.spec, r_in, r_out));
+  }
   if (m.shader == TT_SHADER_MICROFACET) {
     const Frame fr = frame_z(s.ns);
     const float3 ng = fr.to_local(s.n);
@@ -631,6 +656,31 @@ __device__ __forceinline__ ScatterSample sample_bsdf(const DevMaterial& m, float
     value /= fabsf(dot3(out.dir, s.ns));
     if (dot3(out.dir, s.n) < 0.f) value *= eta * eta;
     out.value = f3(value, value, value);
+    return out;
+  }
+  if (m.shader == TT_SHADER_SPECULAR_DENSE_DIELECTRIC) {
+    // Reflection off the coating with probability R(w_in), else the attenuated diffuse base.
+    const float cos_in = fmaxf(0.f, dot3(s.ns, wi));
+    const float r_in = schlick(m.spec, cos_in);
+    if (rng.uniform() < r_in) {
+      const float3 r = reflected(wi, s.ns);
+      out.dir = r;
+      out.pdf = r_in;
+      out.delta = true;
+      const float v = dot3(s.n, r) >= 0.f ? r_in / (cos_in + kEps) : 0.f;
+      out.value = f3(v, v, v);
+      return out;
+    }
+    const Frame fr = frame_z(s.ns);
+    float r[2];
+    rng.square(r);
+    const float3 v = to_cos_hemisphere(r);
+    out.dir = fr.to_world(v);
+    out.pdf = v.z / kPi * (1.f - r_in);
+    const float r_out = schlick(m.spec, fmaxf(0.f, dot3(s.ns, out.dir)));
+    out.value = dot3(s.n, out.dir) > 0.f
+                    ? diffuse_kr(m, s, l) * ((1.f / kPi) * dense_attenuation(m.spec, r_in, r_out))
+                    : f3(0.f, 0.f, 0.f);
     return out;
   }
   if (m.shader == TT_SHADER_GLOSSY_DIELECTRIC) {

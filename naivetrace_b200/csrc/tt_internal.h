@@ -47,6 +47,8 @@ struct DevMaterial {
   int med_out;       // medium on the front side, -1 none
   int tex_w, tex_h;  // diffuse texture size
   const float* tex;  // diffuse texture (linear RGB, row 0 at the top), or nullptr
+  float spec;        // dense dielectric: coating reflectivity at normal incidence
+  int pad;
   float reflectance[NBINS];
   float emission[NBINS];
 };

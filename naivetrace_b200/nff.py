@@ -17,6 +17,7 @@ definitions):
   diffuse name r g b k [+ "diffusetexture file"]  Lambert, reflectance k * rgb (times the
                                                   texture's linear RGB at the hit)
   specularreflective name r g b k                 mirror
+  speculardensedielectric name r g b k [+ texture] smooth coating (reflectivity k) over Lambert rgb
   speculartransmissivedielectric name ior         glass
   glossy name r g b k alpha                       Beckmann microfacet with alpha
   medium name [s a | sr sg sb ar ag ab] [+ "pf rayleigh" | "pf henleygreenstein g"]
@@ -34,8 +35,8 @@ definitions):
   lenv ux uy uz file                              environment map (PFM, or any format Pillow reads)
 Geometry takes the material made of the active shader, medium (the medium inside the
 surface) and area emitter; the shader `invisible` makes the surface a pure medium boundary.
-Not supported here (an error names them): `speculardensedielectric` and the yaml keys the
-tracer has no counterpart for.
+Not supported here (an error names them): roughness textures and the yaml keys the tracer
+has no counterpart for.
 """
 from __future__ import annotations
 
@@ -67,6 +68,7 @@ class _Shader:
     ior: float = 1.5
     invisible: bool = False
     texture: int = -1  # scene texture multiplying the diffuse reflectance
+    specular: float = 0.0  # dense dielectric coating reflectivity
 
 
 @dataclass
@@ -351,7 +353,7 @@ class _Parser:
                              volume_boundary=em is None)
         else:
             m = MaterialSpec(shader=sh.kind, reflectance=sh.reflectance.copy(), alpha=sh.alpha, ior_ratio=sh.ior,
-                             medium_inside=medium, diffuse_texture=sh.texture)
+                             medium_inside=medium, diffuse_texture=sh.texture, specular_reflectivity=sh.specular)
         if em is not None:
             m.emission = em.copy()
         idx = self.scene.add_material(m)
@@ -462,6 +464,19 @@ class _Parser:
                     tex = self.texture(base.parent / targs[0])
                 scope.shaders[args[0]] = _Shader(abi.SHADER_DIFFUSE, rgb_to_spectrum((k * r, k * g, k * b)),
                                                  texture=tex)
+                scope.shader = args[0]
+            elif d == "speculardensedielectric":
+                # parsenff.cxx:416-431: diffuse rgb (no factor), then the coating's reflectivity.
+                r, g, b, k = _floats(args[1:5], where)
+                tex = -1
+                if i < len(lines) and lines[i].strip().startswith("diffusetexture"):
+                    targs = lines[i].split()[1:]
+                    i += 1
+                    if len(targs) != 1:
+                        raise NFFError(f"{base}:{i}: diffusetexture needs a file name")
+                    tex = self.texture(base.parent / targs[0])
+                scope.shaders[args[0]] = _Shader(abi.SHADER_SPECULAR_DENSE_DIELECTRIC, rgb_to_spectrum((r, g, b)),
+                                                 texture=tex, specular=k)
                 scope.shader = args[0]
             elif d == "specularreflective":
                 r, g, b, k = _floats(args[1:5], where)

@@ -34,6 +34,7 @@ class MaterialSpec:
     medium_outside: int = -1
     volume_boundary: bool = False
     diffuse_texture: int = -1  # index of the scene texture multiplying the diffuse reflectance
+    specular_reflectivity: float = 0.0  # dense dielectric coating at normal incidence
 
     def to_c(self) -> abi.Material:
         m = abi.Material()
@@ -48,6 +49,7 @@ class MaterialSpec:
         m.medium_outside = int(self.medium_outside) + 1
         m.volume_boundary = int(bool(self.volume_boundary))
         m.diffuse_texture = int(self.diffuse_texture) + 1  # C ABI: 0 = none, k = texture k-1
+        m.specular_reflectivity = float(self.specular_reflectivity)
         return m
 
 
@@ -138,6 +140,12 @@ def glossy_glass(ior_ratio: float, alpha: float) -> MaterialSpec:
     """GlossyTransmissiveDielectricShader (shader.cxx:710-787): a rough dielectric interface."""
     return MaterialSpec(shader=abi.SHADER_GLOSSY_DIELECTRIC, reflectance=np.zeros(NBINS), ior_ratio=ior_ratio,
                         alpha=alpha)
+
+
+def dense_dielectric(specular_reflectivity: float, diffuse_reflectance) -> MaterialSpec:
+    """SpecularDenseDielectricShader (shader.cxx:977-1081): a smooth coating over a Lambert base."""
+    return MaterialSpec(shader=abi.SHADER_SPECULAR_DENSE_DIELECTRIC, reflectance=as_spectrum(diffuse_reflectance),
+                        specular_reflectivity=specular_reflectivity)
 
 
 def area_light(emission, reflectance=0.0) -> MaterialSpec:

@@ -16,8 +16,8 @@ import math
 import numpy as np
 
 from . import abi
-from .scene import (AtmosphereSpec, CameraSpec, MediumSpec, Scene, area_light, diffuse, env_map, glass, glossy_glass,
-                    microfacet, mirror, sun_light, volume_boundary)
+from .scene import (AtmosphereSpec, CameraSpec, MediumSpec, Scene, area_light, dense_dielectric, diffuse, env_map, glass,
+                    glossy_glass, microfacet, mirror, sun_light, volume_boundary)
 from .spectral import band_spectrum, rgb_to_spectrum
 
 
@@ -102,7 +102,8 @@ def cornell_box(xres=256, yres=256, one_light_triangle=False) -> Scene:
 def cornell_box_materials(xres=64, yres=64) -> Scene:
     """The Cornell box with the tall box turned into glass and the small box into a
     rough Beckmann metal, a mirror back wall and a rough-glass sphere above the small box:
-    exercises every shader."""
+    exercises every shader; the floor is a dense dielectric (a smooth coating over a Lambert
+    base)."""
     s = Scene()
     s.name = "cornell_box_materials"
     white = s.add_material(diffuse(0.75))
@@ -112,7 +113,8 @@ def cornell_box_materials(xres=64, yres=64) -> Scene:
     glass_m = s.add_material(glass(1.5))
     metal = s.add_material(microfacet(rgb_to_spectrum((0.9, 0.7, 0.4)), 0.2))
     mir = s.add_material(mirror(0.9))
-    s.add_mesh(*quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)), white)
+    coated = s.add_material(dense_dielectric(0.1, 0.7))
+    s.add_mesh(*quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0)), coated)
     s.add_mesh(*quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1)), white)
     s.add_mesh(*quad((0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1)), mir)
     s.add_mesh(*quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1)), red)

@@ -6,7 +6,8 @@ A file is one scope: a mapping with any of
                {scale: [x,y,z]}, ...]   composed in order onto the scope's transform
                (degrees unless rad: true)
   shaders:    [{name, class: diffuse | glossy | speculartransmissivedielectric |
-                glossytransmissivedielectric, rgb, rgb_x, alpha, ior_ratio, texture}, ...]
+                glossytransmissivedielectric | speculardensedielectric, rgb, rgb_x, alpha, ior_ratio,
+                specular, texture}, ...]
   media:      [{name, class: homogeneous, absorb, absorb_x, scatter, scatter_x,
                 phasefunction: {class: rayleigh | henleygreenstein, g}}, ...]
   arealights: [{name, class: uniform | parallel, rgb, rgb_x}, ...]
@@ -22,8 +23,8 @@ A file is one scope: a mapping with any of
 Sections are read in the reference's order (transforms, shaders, media, arealights, lights,
 materials, models, scopes, view).  Colours are RGB (default 1) times the `_x` factor,
 converted to spectra.  A sphere's radius scales with the cube root of the transform's
-determinant.  Classes the tracer has no counterpart for (dense dielectrics,
-modulated-density media, roughness textures) raise an error naming them.
+determinant.  Classes the tracer has no counterpart for (modulated-density media,
+roughness textures) raise an error naming them.
 """
 from __future__ import annotations
 
@@ -97,6 +98,12 @@ class _YamlReader(_Parser):
             if "abbe_number" in node:
                 raise NFFError("shader: dispersion (abbe_number) is not supported")
             sh = _Shader(abi.SHADER_SPECULAR_DIELECTRIC, np.zeros(NBINS), ior=ior)
+        elif cls == "speculardensedielectric":
+            # parse_yaml_scene.cxx:474-480
+            spec = float(node.pop("specular"))
+            tex = node.pop("texture", None)
+            sh = _Shader(abi.SHADER_SPECULAR_DENSE_DIELECTRIC, _spectrum(node, "rgb"),
+                         texture=self.texture(self.base.parent / tex) if tex else -1, specular=spec)
         elif cls == "glossytransmissivedielectric":
             # parse_yaml_scene.cxx:443-450 (alpha_min only with a roughness texture)
             ior = float(node.pop("ior_ratio"))

@@ -1089,6 +1089,15 @@ inline S3 DiffuseReflectance(const tt_material& m, const Surf& si, const int32_t
   return kr;
 }
 
+// SpecularDenseDielectricShader (shader.cxx:977-1081): SchlicksApproximation
+// (shader_physics.hxx:95-101) and DiffuseAttenuationFactor with the average albedo of
+// AverageOfProjectedSchlicksApproximationOverHemisphere.
+inline double Schlick(double k, double cos_n) { return k + (1. - k) * std::pow(1. - cos_n, 5.); }
+inline double DenseAttenuation(double k, double r_in, double r_out) {
+  const double avg = k + (1. - k) * 2. / 42.;
+  return (1. - r_in) * (1. - r_out) / (1. - avg);
+}
+
 static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const int32_t idx[3], double* pdf,
                        double min_roughness = 0.) {
   if (m.shader == TT_SHADER_SPECULAR_DIELECTRIC && min_roughness > 0.)
@@ -1109,6 +1118,17 @@ static S3 EvaluateBSDF(const tt_material& m, V3 wi, const Surf& si, V3 wo, const
     case TT_SHADER_GLOSSY_DIELECTRIC: {
       const GlossyDielectric g(m, wi, si, min_roughness);
       return S3(g.Evaluate(g.frame.ToLocal(wo), pdf));
+    }
+    case TT_SHADER_SPECULAR_DENSE_DIELECTRIC: {
+      if (!(Dot(si.normal, wo) > 0.)) {
+        if (pdf) *pdf = 0.;
+        return S3(0.);
+      }
+      const double k = m.specular_reflectivity;
+      const double r_in = Schlick(k, std::max(0., Dot(si.shading_normal, wi)));
+      const double r_out = Schlick(k, std::max(0., Dot(si.shading_normal, wo)));
+      if (pdf) *pdf = std::max(0., Dot(si.shading_normal, wo)) / Pi * (1. - r_in);
+      return DiffuseReflectance(m, si, idx) * (DenseAttenuation(k, r_in, r_out) / Pi);
     }
     case TT_SHADER_MICROFACET: {
       const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
@@ -1173,6 +1193,30 @@ static ScatterSample SampleBSDF(const tt_material& m, V3 wi, const Surf& si, Sam
     return out;
   }
   switch (m.shader) {
+    case TT_SHADER_SPECULAR_DENSE_DIELECTRIC: {
+      const double k = m.specular_reflectivity;
+      const double cos_in = std::max(0., Dot(si.shading_normal, wi));
+      const double r_in = Schlick(k, cos_in);
+      if (smp.Uniform01() < r_in) {
+        const V3 r = Reflected(wi, si.shading_normal);
+        out.dir = r;
+        out.pdf = r_in;
+        out.delta = true;
+        out.value = Dot(si.normal, r) >= 0. ? S3(r_in / (cos_in + Eps)) : S3(0.);
+        return out;
+      }
+      const Frame fr = OrthogonalSystemZAligned(si.shading_normal);
+      double r[2];
+      smp.UniformUnitSquare(r);
+      const V3 v = ToCosHemisphere(r);
+      out.dir = fr.ToWorld(v);
+      out.pdf = v.z / Pi * (1. - r_in);
+      const double r_out = Schlick(k, std::max(0., Dot(si.shading_normal, out.dir)));
+      out.value = Dot(si.normal, out.dir) > 0
+                      ? DiffuseReflectance(m, si, idx) * (DenseAttenuation(k, r_in, r_out) / Pi)
+                      : S3(0.);
+      return out;
+    }
     case TT_SHADER_GLOSSY_DIELECTRIC: {
       const GlossyDielectric g(m, wi, si, min_roughness);
       double r[2];

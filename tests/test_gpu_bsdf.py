@@ -19,8 +19,8 @@ from scipy import stats
 
 from naivetrace_b200 import abi
 from naivetrace_b200.algo import GpuContext
-from naivetrace_b200.scene import (CameraSpec, MaterialSpec, Scene, diffuse, glass, glossy_glass, make_params, microfacet,
-                                   mirror)
+from naivetrace_b200.scene import (CameraSpec, MaterialSpec, Scene, dense_dielectric, diffuse, glass, glossy_glass,
+                                   make_params, microfacet, mirror)
 from naivetrace_b200.spectral import rgb_to_spectrum
 from oracle.oracle import OracleScene
 
@@ -48,6 +48,7 @@ MATERIALS = {
     "beckmann_04": microfacet(0.3, 0.4),
     "beckmann_01": microfacet(rgb_to_spectrum((0.9, 0.6, 0.3)), 0.1),
     "glossy_glass": glossy_glass(1.3, 0.2),
+    "dense": dense_dielectric(0.3, rgb_to_spectrum((0.8, 0.5, 0.2))),
 }
 
 
@@ -86,7 +87,7 @@ def test_samples_match_oracle(contexts, mat, inc):
     np.testing.assert_allclose(vg[k], vo[k], rtol=2e-3, atol=1e-5)
 
 
-@pytest.mark.parametrize("mat", ["lambert", "beckmann_04", "beckmann_01", "glossy_glass"])
+@pytest.mark.parametrize("mat", ["lambert", "beckmann_04", "beckmann_01", "glossy_glass", "dense"])
 @pytest.mark.parametrize("inc", ["VERTICAL", "EXACT_45DEG", "MUCH_DEFLECTED"])
 def test_eval_matches_oracle(contexts, mat, inc):
     g, o, ids = contexts

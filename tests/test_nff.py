@@ -191,3 +191,10 @@ def test_srgb_texture_is_linearised(tmp_path):
     Image.fromarray(np.array([[[0, 128, 255]]], np.uint8)).save(tmp_path / "t.png")
     t = read_texture(tmp_path / "t.png")
     np.testing.assert_allclose(t[0, 0], [0.0, ((128 / 255 + 0.055) / 1.055) ** 2.4, 1.0], rtol=1e-6)
+
+
+def test_dense_dielectric_line():
+    s = parse_nff("speculardensedielectric coat 0.2 0.4 0.6 0.05\ns 0 0 1 0.5\n")
+    m = s.materials[int(s.sphere_arrays()[1][0])]
+    assert m.shader == abi.SHADER_SPECULAR_DENSE_DIELECTRIC and m.specular_reflectivity == pytest.approx(0.05)
+    np.testing.assert_allclose(m.reflectance, rgb_to_spectrum((0.2, 0.4, 0.6)))
