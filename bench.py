@@ -425,6 +425,32 @@ def pt2_comparison(scene, spp, depth, device):
     return out
 
 
+def sort_comparison(scene, spp, depth, device, frames=2):
+    """The bench frame with the hit queue shaded in traversal order and in material-sorted
+    order (tt_params.sort_shading): CUDA-event time per frame of each, after one untimed
+    frame that allocates the path state."""
+    import torch
+
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    out = {"workload": "the bench frame, shaded in traversal order and in material-sorted order"}
+    for key, sort in (("traversal_order", False), ("material_sorted", True)):
+        g = GpuContext(scene, make_params(max_ray_depth=depth, device=device, sort_shading=sort))
+        g.render(spp, 1)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        for k in range(frames):
+            g.render(spp, 2 + k)
+        b.record()
+        torch.cuda.synchronize()
+        out[key] = {"ms_per_frame": a.elapsed_time(b) / frames, "error_flags": g.stats()["error_flags"]}
+        g.close()
+    out["speedup_sorted"] = out["traversal_order"]["ms_per_frame"] / out["material_sorted"]["ms_per_frame"]
+    return out
+
+
 def run_reference_arm(args):
     from naivetrace_b200 import dist as nd
     r = nd.init_from_env()
@@ -590,6 +616,9 @@ def run_ours(args):
     pt2 = None
     if rank == 0 and world == 1 and not args.no_pt2:
         pt2 = pt2_comparison(scene, spp, depth, device)
+    sorted_shading = None
+    if rank == 0 and world == 1 and not args.no_sort:
+        sorted_shading = sort_comparison(scene, spp, depth, device)
     configs = None
     if rank == 0 and world == 1 and not args.no_configs and not args.small:
         configs = config_figures(device, cpu_budget=min(5.0, args.cpu_budget))
@@ -639,6 +668,7 @@ def run_ours(args):
             "multiview": multiview,
             "pt2": pt2,
             "configs": configs,
+            "sorted_shading": sorted_shading,
             "gpu_launches": int(st["kernel_launches"]),
             "clocks": clk,
             "stats": {k: st[k] for k in ("extension_rays", "shadow_rays", "extend_launches", "extend_ms",
@@ -657,7 +687,7 @@ def profile_run(args):
     from naivetrace_b200 import abi
     scene, spp, depth, name = workload(args)
     algo = abi.ALGO_PT2 if args.algo == "pt2" else abi.ALGO_PT
-    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave, algo=algo))
+    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave, algo=algo, sort_shading=args.sort))
     g.render(spp, 1)
     st = g.stats()
     q = g.queue_lengths(depth + 1)
@@ -744,6 +774,8 @@ def main(argv=None):
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")
     ap.add_argument("--no-multiview", action="store_true", help="skip the multi-view batch comparison")
     ap.add_argument("--no-pt2", action="store_true", help="skip the null-path tracer (pt2) frames")
+    ap.add_argument("--no-sort", action="store_true", help="skip the material-sorted shading frames")
+    ap.add_argument("--sort", action="store_true", help="--profile-run: shade in material-sorted order")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the Cornell box, medium and atmosphere configurations")
     ap.add_argument("--algo", choices=["pt", "pt2"], default="pt", help="tracer of --profile-run")

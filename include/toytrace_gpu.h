@@ -217,6 +217,10 @@ typedef struct tt_params {
   int32_t qmc;                  /* --qmc (RenderingParameters::qmc): Sobol points with per-pixel
                                    rotations instead of pseudo-random numbers; used by pt2 only
                                    (as in the reference), which then needs max_ray_depth <= 31 */
+  int32_t sort_shading;         /* algo pt: 1 = before each shading launch the bounce's hit queue is
+                                   partitioned by the hit's shading kind (escaped, volume, one key
+                                   per shader), so that a warp shades one material kind; 0 = the
+                                   queue in traversal order (the default) */
 } tt_params;
 
 typedef struct tt_ctx tt_ctx;

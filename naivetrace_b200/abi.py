@@ -161,6 +161,7 @@ class Params(C.Structure):
         ("device", C.c_int32),
         ("algo", C.c_int32),
         ("qmc", C.c_int32),
+        ("sort_shading", C.c_int32),
     ]
 
 

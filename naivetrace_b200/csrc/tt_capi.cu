@@ -917,6 +917,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   s.long_distance = (float)(10. * diag);
   s.max_path_nodes = c->params.max_ray_depth + 1;
   s.algo = c->params.algo;
+  s.sort_shading = (c->params.sort_shading && c->params.algo == TT_ALGO_PT) ? 1 : 0;
   // Quasi-random sampling: pt2 only, as in the reference (CameraRenderWorker's sampler).
   s.sobol = nullptr;
   s.rotations = nullptr;
@@ -999,6 +1000,10 @@ static tt_status ensure_path_state(tt_ctx* c, int cap) {
   p.sh_q = (int*)m.alloc(n * sizeof(int));
   p.done_q = (int*)m.alloc(n * sizeof(int));
   p.counters = (int*)m.alloc(kCountersPerBounce * (size_t)(c->rounds + 3) * sizeof(int));
+  if (c->dev.sort_shading && c->dev.algo == TT_ALGO_PT) {
+    p.sort_q = (int*)m.alloc(n * sizeof(int));
+    p.sort_key = (unsigned char*)m.alloc(n);
+  }
   if (c->dev.num_media > 0) {
     p.track = (uint2*)m.alloc(n * sizeof(uint2));
     p.vol = (float4*)m.alloc(n * sizeof(float4));
@@ -1197,7 +1202,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
         launch_guide(c->dev, c->ps, b, c->stream);
         launches++;
       }
-      launches += 4;
+      launches += 3 + shade_launches(c->dev, c->ps);
     }
     timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, rounds, counting, c->d_stats + 2, grid, c->stream); });
     launch_flush(c->dev, c->ps, c->fb, rounds, grid, c->stream);
@@ -2016,7 +2021,8 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
     k_tally<<<1, 32, 0, s>>>(ps.counters, rounds, c->d_stats);
     launch_wave_advance(d_idx, s);
   };
-  const int per_wave = 4 + rounds * (4 + (sc.num_media > 0)) + (sc.guide ? std::min(rounds, sc.guide_depth) : 0) + 2;
+  const int per_wave = 4 + rounds * (3 + shade_launches(sc, ps) + (sc.num_media > 0)) +
+                       (sc.guide ? std::min(rounds, sc.guide_depth) : 0) + 2;
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0, c->stream);

@@ -20,7 +20,10 @@ constexpr uint32_t ERR_CROSSINGS = 4u;  // a ray crossed more medium boundaries 
 constexpr uint32_t ERR_TENSOR = 8u;     // a wait on the tcgen05 tensor cores gave up
 constexpr int kMaxCrossings = 256;      // boundary crossings followed along one ray
 constexpr int kMaxMedia = 254;          // medium indices are stored in bytes (0xff = empty)
-constexpr int kCountersPerBounce = 4;  // ext, shadow, done, guided queue lengths
+// Shading keys of the material-sorted hit queue: escaped, volume vertex, then one per shader kind.
+constexpr int kShadeKeys = 8;
+// Per bounce: ext, shadow, done, guided queue lengths, then the shading-key counts and cursors.
+constexpr int kCountersPerBounce = 4 + 2 * kShadeKeys;
 constexpr int kSobolDims = 4096;       // quasi-random dimensions: subsequence ids < 64, 64 each
 constexpr int kRotationBlock = 128;    // per-pixel rotations repeat every 128 pixels in x and y
 
@@ -142,6 +145,7 @@ struct DevScene {
   float box_lo[3];            // scene box, for the position encoding
   float box_inv[3];           // 1 / extent per axis
   int algo;                   // TT_ALGO_PT or TT_ALGO_PT2 (tt_pt2.cuh)
+  int sort_shading;           // 1: shade the bounce's hits in material-sorted order (algo pt)
   // Tree guider (tt_tree.cu), when guide_method == TT_GUIDE_TREE: kd-tree nodes (split,
   // axis, child0, child1 as int bits; a child < 0 is ~cell), the root reference and the
   // cells' mixtures (40 floats each: weights[8], means[8][3], concentrations[8]).
@@ -174,6 +178,8 @@ struct PathState {
   int* sh_q;
   int* done_q;
   int* counters;       // kCountersPerBounce ints per bounce, (max bounces + 3) bounces
+  int* sort_q;         // material-sorted hit queue (sort_shading only, else null)
+  unsigned char* sort_key;  // shading key per entry of the bounce's hit queue
   unsigned int* err;
   // Media scenes only (null otherwise).
   uint2* track;        // medium tracker: x = 4 slot bytes (0xff empty), y = current medium (-1 vacuum)
@@ -248,6 +254,8 @@ void launch_resolve_views(const float* accum, const float* light, const DevView*
 void prepare_guide_launch();
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats,
                    int grid, cudaStream_t st);
+// Launches the shading stage (with the material sort when it is on); how many kernels that is.
+int shade_launches(const DevScene& s, const PathState& p);
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st);

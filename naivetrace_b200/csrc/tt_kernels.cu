@@ -45,6 +45,10 @@ __device__ __forceinline__ int* ext_count(const PathState& p, int b) { return &p
 __device__ __forceinline__ int* sh_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 1]; }
 __device__ __forceinline__ int* done_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 2]; }
 __device__ __forceinline__ int* guide_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 3]; }
+__device__ __forceinline__ int* key_count(const PathState& p, int b) { return &p.counters[kCountersPerBounce * b + 4]; }
+__device__ __forceinline__ int* key_cursor(const PathState& p, int b) {
+  return &p.counters[kCountersPerBounce * b + 4 + kShadeKeys];
+}
 
 // Pending training record of a guided path (PathState::grec, 6 float4 per slot):
 //   0: position normalised to the scene box (xyz), shading normal x
@@ -979,10 +983,67 @@ __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bou
   }
 }
 
+// Material-sorted shading.  The shading key of a hit: 0 escaped, 1 volume vertex, 2 + the
+// shader kind of the hit surface's material.  k_sort_count keys the bounce's hit queue and
+// counts the keys (warp-aggregated atomics, one per distinct key in a warp); k_sort_scatter
+// writes every entry into its key's range of sort_q (ranges in key order, entries of a key
+// in roughly their queue order), so that the warps of k_shade meet one material kind each.
+__device__ __forceinline__ int shade_key(const DevScene& sc, const PathState& p, int slot) {
+  const int tri = __float_as_int(p.hit[slot].w);
+  if (tri <= -2) return 1;
+  if (tri < 0) return 0;
+  const int mat = __float_as_int(__ldg(&sc.tris[3 * tri + 1]).w);
+  return 2 + min(sc.materials[mat].shader, kShadeKeys - 3);
+}
+
+// Adds 1 for this lane to counter[key]; lanes of a warp with the same key share one atomic.
+// Returns this lane's position among the appends to that counter.
+__device__ __forceinline__ int warp_append_key(int* counter, int key) {
+  const unsigned active = __activemask();
+  const unsigned peers = __match_any_sync(active, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&counter[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+__global__ void __launch_bounds__(256) k_sort_count(DevScene sc, PathState p, int bounce) {
+  const int n = *ext_count(p, bounce);
+  const int* q = p.ext_q[bounce & 1];
+  int* counts = key_count(p, bounce);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int key = shade_key(sc, p, q[i]);
+    p.sort_key[i] = (unsigned char)key;
+    warp_append_key(counts, key);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sort_scatter(PathState p, int bounce) {
+  __shared__ int base[kShadeKeys];
+  if (threadIdx.x == 0) {
+    const int* counts = key_count(p, bounce);
+    int acc = 0;
+    for (int k = 0; k < kShadeKeys; ++k) {
+      base[k] = acc;
+      acc += counts[k];
+    }
+  }
+  __syncthreads();
+  const int n = *ext_count(p, bounce);
+  const int* q = p.ext_q[bounce & 1];
+  int* cursor = key_cursor(p, bounce);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int key = p.sort_key[i];
+    p.sort_q[base[key] + warp_append_key(cursor, key)] = q[i];
+  }
+}
+
 template <bool MEDIA>
 __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
-  const int* q = p.ext_q[bounce & 1];
+  const int* q = (sc.sort_shading && p.sort_q) ? p.sort_q : p.ext_q[bounce & 1];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = q[i];
     const float4 h = p.hit[slot];
@@ -1770,7 +1831,14 @@ void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count
     });
   });
 }
+int shade_launches(const DevScene& s, const PathState& p) {
+  return (s.algo == TT_ALGO_PT && s.sort_shading && p.sort_q) ? 3 : 1;
+}
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
+  if (s.algo == TT_ALGO_PT && s.sort_shading && p.sort_q) {
+    k_sort_count<<<grid, kBlock, 0, st>>>(s, p, bounce);
+    k_sort_scatter<<<grid, kBlock, 0, st>>>(p, bounce);
+  }
   if (s.algo == TT_ALGO_PT2) {
     if (s.num_media == 0) {
       k_shade2<false, false, false><<<grid, kBlock, 0, st>>>(s, p, bounce);

@@ -399,8 +399,10 @@ class Scene:
 
 
 def make_params(max_ray_depth: int = 25, pt_sample_mode: int = abi.SAMPLE_BOTH, max_spp: int = -1,
-                wave_paths: int = 0, device: int = 0, algo: int = abi.ALGO_PT, qmc: bool = False) -> abi.Params:
+                wave_paths: int = 0, device: int = 0, algo: int = abi.ALGO_PT, qmc: bool = False,
+                sort_shading: bool = False) -> abi.Params:
     p = abi.Params()
+    p.sort_shading = int(bool(sort_shading))
     p.algo = algo
     p.qmc = int(bool(qmc))
     p.max_ray_depth = max_ray_depth
