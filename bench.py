@@ -359,9 +359,12 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
 def multiview_comparison(g, n_views=96, seed=4):
     """The multi-view workload on the already uploaded terrain scene: n seeded views, square
     sides from {128, 256, 512, 768, 1024}, 4-64 spp, max depth of the context.  The batch
-    runs as one wavefront after the autotuner picked the queue capacity and launch width;
-    the same views are then rendered one call per view.  Both timed on the device (CUDA
-    events around the calls, synchronised on both sides)."""
+    runs as one wavefront after the autotuner picked the queue capacity, launch width, block
+    size and BVH layout: plain, and with learned guiding on (the network trained first by
+    four one-sample passes of the batch, then frozen); the same views are then rendered one
+    call per view by the plain tracer.  Per-view completion times: for a batch the device
+    time at which the wave holding the view's last path ended (CUDA events), for one call per
+    view the time at which the view's call returned; p50 and p99 over the views."""
     import torch
     from naivetrace_b200 import scenes
     views = scenes.terrain_views(n_views, seed=seed)
@@ -376,18 +379,40 @@ def multiview_comparison(g, n_views=96, seed=4):
         torch.cuda.synchronize()
         return (time.perf_counter() - t0) * 1e3
 
+    def pct(x):
+        x = np.asarray(x, np.float64)
+        return {"p50_ms": float(np.percentile(x, 50)), "p99_ms": float(np.percentile(x, 99))}
+
     batch_ms = timed(lambda: g.render_views(views, seed=seed))
-    seq_ms = timed(lambda: [g.render_views([v], seed=seed + k) for k, v in enumerate(views)])
+    batch_done = g.views_completion_ms(len(views))
+    # Learned guiding on: train on the batch itself, then time a frozen guided batch.
+    probe = [(c, 1) for c, _ in views]
+    g.set_guiding(True, 1, seed=7)
+    for k in range(4):
+        g.render_views(probe, seed=100 + k)
+    g.set_guiding(True, 0, seed=7)
+    g.render_views(views, seed=2)  # allocates the guided path state
+    guided_ms = timed(lambda: g.render_views(views, seed=seed))
+    guided_done = g.views_completion_ms(len(views))
+    g.set_guiding(False)
+    seq_done, t = [], 0.0
+    for k, v in enumerate(views):
+        t += timed(lambda: g.render_views([v], seed=seed + k))
+        seq_done.append(t)
+    seq_ms = t
     return {
         "workload": f"terrain_views: {n_views} seeded views of the terrain_spheres scene, sides "
                     f"{{128..1024}}, 4-64 spp, {sum(c.xres * c.yres for c, _ in views)} pixels, {paths} paths",
         "paths": paths,
-        "batched": {"ms": batch_ms, "mpaths_per_s": paths / (batch_ms * 1e-3) / 1e6},
-        "one_call_per_view": {"ms": seq_ms, "mpaths_per_s": paths / (seq_ms * 1e-3) / 1e6},
+        "batched": {"ms": batch_ms, "mpaths_per_s": paths / (batch_ms * 1e-3) / 1e6, **pct(batch_done)},
+        "batched_guided": {"ms": guided_ms, "mpaths_per_s": paths / (guided_ms * 1e-3) / 1e6, **pct(guided_done),
+                           "what": "learned guiding on (2 guided bounces), network trained by 4 one-sample "
+                                   "passes of the batch and frozen"},
+        "one_call_per_view": {"ms": seq_ms, "mpaths_per_s": paths / (seq_ms * 1e-3) / 1e6, **pct(seq_done)},
         "speedup": seq_ms / batch_ms,
-        "autotune": {"wave_paths": tune["wave_paths"], "grid": tune["grid"], "probe_ms": tune["ms"],
-                     "candidates": tune["candidates"]},
-        "timing": "wall clock around synchronised calls (host-side view upload and image read-back included)",
+        "autotune": tune,
+        "timing": "wall clock around synchronised calls (host-side view upload and image read-back included); "
+                  "per-view completion from device events (batches) or call returns (one call per view)",
     }
 
 

@@ -496,6 +496,12 @@ typedef struct tt_view {
  * seed + v and sample numbers 0..spp-1.  The context's own framebuffer is not touched. */
 tt_status tt_render_views(tt_ctx* ctx, const tt_view* views, int32_t n, uint64_t seed, float* rgb);
 
+/* Completion time of every view of the last tt_render_views call, in ms after the batch
+ * started on the device (CUDA events): a view is complete when the wave that holds its last
+ * path has finished.  -1 for views a stop request left unfinished.  n must equal the last
+ * batch's view count. */
+tt_status tt_views_completion_ms(tt_ctx* ctx, float* out, int32_t n);
+
 #define TT_TUNE_MAX 16
 typedef struct tt_tune_result {
   int32_t wave_paths;           /* chosen paths per wave (queue capacity) */
@@ -505,12 +511,17 @@ typedef struct tt_tune_result {
   int32_t candidate_wave[TT_TUNE_MAX];
   int32_t candidate_grid[TT_TUNE_MAX];
   double candidate_ms[TT_TUNE_MAX];
+  int32_t block;                /* chosen threads per block of the wavefront launches */
+  int32_t bvh_width;            /* chosen BVH layout: 2 (binary) or 8 (8-wide compressed) */
+  int32_t candidate_block[TT_TUNE_MAX];
+  int32_t candidate_width[TT_TUNE_MAX];
 } tt_tune_result;
 
-/* Autotuner: times one-sample probes of the batch over queue capacities (2^22, 2^24, 2^25, 2^26 paths
- * per wave) and launch widths (0.5, 1, 2 x the occupancy grid) and keeps the fastest for
- * this context's later passes.  The BVH layout stays binary: the 8-wide layout measured a
- * few percent slower on the mesh workloads (TT_BVH_WIDTH=8 selects it at upload). */
+/* Autotuner: times one-sample probes of the batch over queue capacities (2^22, 2^24, 2^25,
+ * 2^26 paths per wave) and launch widths (0.5, 1, 2 x the occupancy grid) with 256-thread
+ * blocks on the binary BVH; then, at the best of those, 128-thread blocks (twice the grid)
+ * and the 8-wide compressed BVH (built on the host on first use, kept next to the binary
+ * one); and keeps the fastest configuration for this context's later passes. */
 tt_status tt_autotune_views(tt_ctx* ctx, const tt_view* views, int32_t n, tt_tune_result* out);
 
 void tt_destroy(tt_ctx* ctx);

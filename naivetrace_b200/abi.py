@@ -241,6 +241,7 @@ EXPORTED_SYMBOLS = [
     "tt_guide_read_records",
     "tt_guide_features_batch",
     "tt_render_views",
+    "tt_views_completion_ms",
     "tt_autotune_views",
     "tt_guide_forward_batch_tc",
     "tt_guide_tree_info",
@@ -272,6 +273,10 @@ class TuneResult(C.Structure):
         ("candidate_wave", C.c_int32 * TUNE_MAX),
         ("candidate_grid", C.c_int32 * TUNE_MAX),
         ("candidate_ms", C.c_double * TUNE_MAX),
+        ("block", C.c_int32),
+        ("bvh_width", C.c_int32),
+        ("candidate_block", C.c_int32 * TUNE_MAX),
+        ("candidate_width", C.c_int32 * TUNE_MAX),
     ]
 
 
@@ -359,6 +364,7 @@ def load_library() -> C.CDLL:
         "tt_guide_read_records": ([vp, P(C.c_float), C.c_int32, P(C.c_int32)], C.c_int32),
         "tt_guide_features_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
         "tt_render_views": ([vp, P(View), C.c_int32, C.c_uint64, P(C.c_float)], C.c_int32),
+        "tt_views_completion_ms": ([vp, P(C.c_float), C.c_int32], C.c_int32),
         "tt_autotune_views": ([vp, P(View), C.c_int32, P(TuneResult)], C.c_int32),
         "tt_guide_forward_batch_tc": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
         "tt_guide_tree_info": ([vp, P(C.c_int32), P(C.c_int32), P(C.c_int32), P(C.c_int64)], C.c_int32),

@@ -283,13 +283,20 @@ class GpuContext:
             o += n
         return out
 
+    def views_completion_ms(self, n: int) -> np.ndarray:
+        """Completion time (ms after the batch started) of each view of the last render_views."""
+        out = np.zeros(n, np.float32)
+        self._check(self.lib.tt_views_completion_ms(self.h, _fp(out), n), "tt_views_completion_ms")
+        return out
+
     def autotune_views(self, views) -> dict:
         arr, _ = self._views(views)
         r = abi.TuneResult()
         self._check(self.lib.tt_autotune_views(self.h, arr, len(views), C.byref(r)), "tt_autotune_views")
         k = min(r.candidates, abi.TUNE_MAX)
-        return {"wave_paths": r.wave_paths, "grid": r.grid, "ms": r.ms,
+        return {"wave_paths": r.wave_paths, "grid": r.grid, "block": r.block, "bvh_width": r.bvh_width, "ms": r.ms,
                 "candidates": [{"wave_paths": r.candidate_wave[i], "grid": r.candidate_grid[i],
+                                "block": r.candidate_block[i], "bvh_width": r.candidate_width[i],
                                 "ms": r.candidate_ms[i]} for i in range(k)]}
 
     def request_interrupt(self):

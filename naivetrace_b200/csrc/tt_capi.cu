@@ -159,6 +159,7 @@ struct tt_ctx {
   std::vector<HostEnv> envs;
   std::vector<tt_point_light> points;
   HostArray<float> uvs;                          // 2 per vertex, when given
+  std::vector<float> views_done_ms;              // per view of the last multi-view batch: completion time
   std::vector<std::vector<float>> textures;      // linear RGB per texture
   std::vector<int2> texture_sizes;               // width, height
   tt_camera camera{};
@@ -190,6 +191,18 @@ struct tt_ctx {
   tt_stats stats{};
   std::string err;
   uint32_t bvh_nodes = 0, bvh_depth = 0, bvh_node_bytes = 64;
+  // The two BVH layouts the autotuner can choose between: [0] binary, [1] 8-wide compressed
+  // (built on the host on the autotuner's first request).  Slot arrays belong to a layout.
+  struct Layout {
+    bool ready = false;
+    const float4* nodes = nullptr;
+    const uint4* nodes8 = nullptr;
+    const float4* tris = nullptr;
+    const float4* vnodes = nullptr;
+    const uint4* vnodes8 = nullptr;
+    const float4* vtris = nullptr;
+    uint32_t num_nodes = 0, depth = 0, node_bytes = 0;
+  } layouts[2];
   // Learned guiding.
   std::unique_ptr<GuideNet> gnet;
   std::unique_ptr<TreeGuide> tree;   // tree guider (method TT_GUIDE_TREE)
@@ -483,6 +496,101 @@ tt_status tt_create(const tt_scene_desc* d, const tt_params* p, tt_ctx** out) {
   c->device = p->device;
   c->spp_count.assign(c->npix, 0);
   *out = c;
+  return TT_OK;
+}
+
+// The scene split into surface and medium-boundary inputs for the host BVH builders
+// (Scene::BuildAccelStructure's two scenes, scene.cxx:116-141).
+struct HostSplit {
+  std::vector<uint32_t> sidx, smat, sid, vidx, vmat, vid, ssmat, ssid, vsmat, vsid;
+  std::vector<float> ssph, vsph;
+  void make(const tt_ctx* c) {
+    const uint32_t ntri = (uint32_t)c->mats.size();
+    for (uint32_t t = 0; t < ntri; ++t) {
+      const bool vol = c->materials[c->mats[t]].volume_boundary != 0;
+      (vol ? vid : sid).push_back(t);
+      (vol ? vidx : sidx).insert((vol ? vidx : sidx).end(), &c->idx[3 * (size_t)t], &c->idx[3 * (size_t)t] + 3);
+      (vol ? vmat : smat).push_back(c->mats[t]);
+    }
+    for (uint32_t i = 0; i < (uint32_t)c->sphere_mats.size(); ++i) {
+      const bool vol = c->materials[c->sphere_mats[i]].volume_boundary != 0;
+      (vol ? vsph : ssph).insert((vol ? vsph : ssph).end(), &c->spheres[4 * (size_t)i], &c->spheres[4 * (size_t)i] + 4);
+      (vol ? vsmat : ssmat).push_back(c->sphere_mats[i]);
+      (vol ? vsid : ssid).push_back(ntri + i);
+    }
+  }
+  BvhInput surface(const tt_ctx* c) const {
+    BvhInput b{c->verts.data(), sidx.data(), smat.data(), (uint32_t)sid.size(), sid.data()};
+    b.num_spheres = (uint32_t)ssid.size();
+    b.spheres = ssph.data();
+    b.sphere_material_ids = ssmat.data();
+    b.sphere_prim_ids = ssid.data();
+    return b;
+  }
+  BvhInput volume(const tt_ctx* c) const {
+    BvhInput b{c->verts.data(), vidx.data(), vmat.data(), (uint32_t)vid.size(), vid.data()};
+    b.num_spheres = (uint32_t)vsid.size();
+    b.spheres = vsph.data();
+    b.sphere_material_ids = vsmat.data();
+    b.sphere_prim_ids = vsid.data();
+    return b;
+  }
+};
+
+static void save_layout(tt_ctx* c) {
+  tt_ctx::Layout& L = c->layouts[c->dev.wide ? 1 : 0];
+  L.ready = true;
+  L.nodes = c->dev.nodes;
+  L.nodes8 = c->dev.nodes8;
+  L.tris = c->dev.tris;
+  L.vnodes = c->dev.vnodes;
+  L.vnodes8 = c->dev.vnodes8;
+  L.vtris = c->dev.vtris;
+  L.num_nodes = c->bvh_nodes;
+  L.depth = c->bvh_depth;
+  L.node_bytes = c->bvh_node_bytes;
+}
+
+// Makes `wide` the active BVH layout, building the 8-wide one on the host the first time.
+static tt_status use_layout(tt_ctx* c, bool wide) {
+  if ((c->dev.wide != 0) == wide) return TT_OK;
+  save_layout(c);
+  tt_ctx::Layout& L = c->layouts[wide ? 1 : 0];
+  if (!L.ready) {
+    if (!wide) return fail(c, TT_ERR_INVALID, "binary BVH layout missing");
+    HostSplit hs;
+    hs.make(c);
+    Bvh8Output bo, vbo;
+    if (!build_bvh8(hs.surface(c), &bo) || !build_bvh8(hs.volume(c), &vbo))
+      return fail(c, TT_ERR_INVALID, "8-wide BVH build failed");
+    if (bo.max_depth + 2 >= (uint32_t)BVH8_STACK || vbo.max_depth + 2 >= (uint32_t)BVH8_STACK)
+      return fail(c, TT_ERR_CAPACITY, "BVH deeper than the traversal stack");
+    auto up = [&](const void* src, size_t bytes) -> void* {
+      void* p = c->scene_mem.alloc(bytes);
+      if (p && bytes) cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream);
+      return p;
+    };
+    L.nodes8 = (const uint4*)up(bo.nodes.data(), bo.nodes.size() * sizeof(uint32_t));
+    L.tris = (const float4*)up(bo.tris.data(), bo.tris.size() * sizeof(float));
+    L.vnodes8 = (const uint4*)up(vbo.nodes.data(), vbo.nodes.size() * sizeof(uint32_t));
+    L.vtris = (const float4*)up(vbo.tris.data(), vbo.tris.size() * sizeof(float));
+    L.num_nodes = bo.num_nodes;
+    L.depth = bo.max_depth;
+    L.node_bytes = 80;
+    L.ready = true;
+    TT_CUDA(c, cudaStreamSynchronize(c->stream));
+    TT_CUDA(c, cudaGetLastError());
+  }
+  c->dev.wide = wide ? 1 : 0;
+  c->dev.nodes = L.nodes;
+  c->dev.nodes8 = L.nodes8;
+  c->dev.tris = L.tris;
+  c->dev.vnodes = L.vnodes;
+  c->dev.vnodes8 = L.vnodes8;
+  c->dev.vtris = L.vtris;
+  c->bvh_nodes = L.num_nodes;
+  c->bvh_depth = L.depth;
+  c->bvh_node_bytes = L.node_bytes;
   return TT_OK;
 }
 
@@ -1970,11 +2078,14 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> wave_end((size_t)nwaves, nullptr);  // recorded after each wave
   auto cleanup = [&]() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    for (cudaEvent_t& e : wave_end)
+      if (e) cudaEventDestroy(e);
     m.free_all();
   };
   auto check = [&](cudaError_t e) -> tt_status {
@@ -2028,7 +2139,10 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
   cudaEventRecord(ev0, c->stream);
   bool stopped = false;
   int done_waves = 0;
+  for (cudaEvent_t& e : wave_end)
+    if ((st = check(cudaEventCreate(&e))) != TT_OK) return st;
   wave(c->stream);  // eager first wave
+  cudaEventRecord(wave_end[0], c->stream);
   ++done_waves;
   if ((st = check(cudaGetLastError())) != TT_OK) return st;
   if (nwaves > 1) {
@@ -2040,6 +2154,7 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
     for (; done_waves < nwaves; ++done_waves) {
       if (c->stop.load()) { stopped = true; break; }
       if ((st = check(cudaGraphLaunch(exec, c->stream))) != TT_OK) return st;
+      cudaEventRecord(wave_end[done_waves], c->stream);
     }
   }
   launch_resolve_views(d_acc, d_light, d_views, n, (int)npix_total, d_rgb, c->stream);
@@ -2052,6 +2167,13 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
   float ms = 0.f;
   cudaEventElapsedTime(&ms, ev0, ev1);
   if (ms_out) *ms_out = ms;
+  // A view is complete when the wave holding its last path has finished.
+  c->views_done_ms.assign((size_t)n, -1.f);
+  for (int v = 0; v < n; ++v) {
+    const long long last = hv[v].path_begin + (long long)hv[v].npix * hv[v].spp - 1;
+    const int w = (int)(last / cap);
+    if (w < done_waves) cudaEventElapsedTime(&c->views_done_ms[v], ev0, wave_end[w]);
+  }
   c->stats.pass_ms += ms;
   c->stats.kernel_launches += (uint64_t)done_waves * per_wave + 1;
   c->stats.extend_launches += (uint64_t)done_waves * rounds;
@@ -2078,6 +2200,13 @@ tt_status tt_render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64_t s
   return render_views(c, views, n, seed, rgb, wave_limit, c->grid, nullptr);
 }
 
+tt_status tt_views_completion_ms(tt_ctx* c, float* out, int32_t n) {
+  if (!c || !out) return TT_ERR_INVALID;
+  if ((size_t)n != c->views_done_ms.size()) return fail(c, TT_ERR_INVALID, "view count differs from the last batch");
+  std::copy(c->views_done_ms.begin(), c->views_done_ms.end(), out);
+  return TT_OK;
+}
+
 tt_status tt_autotune_views(tt_ctx* c, const tt_view* views, int32_t n, tt_tune_result* out) {
   if (!c || !views || n <= 0 || !out) return TT_ERR_INVALID;
   if (!c->uploaded) return fail(c, TT_ERR_NOT_READY, "tt_upload_scene has not run");
@@ -2096,28 +2225,55 @@ tt_status tt_autotune_views(tt_ctx* c, const tt_view* views, int32_t n, tt_tune_
   *out = tt_tune_result{};
   double best = 1e300;
   int k = 0;
+  int best_block = 256;
+  bool best_wide = false;
+  auto probe_one = [&](int w, int g, int block, bool wide) -> tt_status {
+    float ms = 0.f;
+    c->dev.block = block;
+    tt_status st = render_views(c, probe.data(), n, 1, rgb.data(), w, g, &ms);
+    if (st != TT_OK) return st;
+    if (k < TT_TUNE_MAX) {
+      out->candidate_wave[k] = w;
+      out->candidate_grid[k] = g;
+      out->candidate_ms[k] = ms;
+      out->candidate_block[k] = block;
+      out->candidate_width[k] = wide ? 8 : 2;
+    }
+    ++k;
+    if (ms < best) {
+      best = ms;
+      out->wave_paths = w;
+      out->grid = g;
+      out->ms = ms;
+      best_block = block;
+      best_wide = wide;
+    }
+    return TT_OK;
+  };
+  const bool start_wide = c->dev.wide != 0;
+  tt_status st = use_layout(c, false);
+  if (st != TT_OK) return st;
   // One untimed call first (path state at the largest size, kernels loaded).
-  tt_status st = render_views(c, probe.data(), n, 1, rgb.data(), waves[3], base_grid, nullptr);
+  c->dev.block = 256;
+  st = render_views(c, probe.data(), n, 1, rgb.data(), waves[3], base_grid, nullptr);
   if (st != TT_OK) return st;
   for (int w : waves)
-    for (int g : grids) {
-      float ms = 0.f;
-      st = render_views(c, probe.data(), n, 1, rgb.data(), w, g, &ms);
-      if (st != TT_OK) return st;
-      if (k < TT_TUNE_MAX) {
-        out->candidate_wave[k] = w;
-        out->candidate_grid[k] = g;
-        out->candidate_ms[k] = ms;
-      }
-      ++k;
-      if (ms < best) {
-        best = ms;
-        out->wave_paths = w;
-        out->grid = g;
-        out->ms = ms;
-      }
-    }
+    for (int g : grids)
+      if ((st = probe_one(w, g, 256, false)) != TT_OK) return st;
+  // At the best queue capacity and launch width: half-size blocks, then the 8-wide BVH.
+  const int w0 = out->wave_paths, g0 = out->grid;
+  if ((st = probe_one(w0, 2 * g0, 128, false)) != TT_OK) return st;
+  const int g1 = best_block == 128 ? 2 * g0 : g0;
+  if ((st = use_layout(c, true)) != TT_OK) return st;
+  c->dev.block = best_block;
+  if ((st = render_views(c, probe.data(), n, 1, rgb.data(), w0, g1, nullptr)) != TT_OK) return st;  // warm-up
+  if ((st = probe_one(w0, g1, best_block, true)) != TT_OK) return st;
+  (void)start_wide;
   out->candidates = k;
+  out->block = best_block;
+  out->bvh_width = best_wide ? 8 : 2;
+  if ((st = use_layout(c, best_wide)) != TT_OK) return st;
+  c->dev.block = best_block;
   c->params.wave_paths = out->wave_paths;
   c->grid = out->grid;
   return TT_OK;

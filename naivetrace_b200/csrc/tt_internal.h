@@ -146,6 +146,7 @@ struct DevScene {
   float box_inv[3];           // 1 / extent per axis
   int algo;                   // TT_ALGO_PT or TT_ALGO_PT2 (tt_pt2.cuh)
   int sort_shading;           // 1: shade the bounce's hits in material-sorted order (algo pt)
+  int block;                  // threads per block of the wavefront launches (0: 256), host side only
   // Tree guider (tt_tree.cu), when guide_method == TT_GUIDE_TREE: kd-tree nodes (split,
   // axis, child0, child1 as int bits; a child < 0 is ~cell), the root reference and the
   // cells' mixtures (40 floats each: weights[8], means[8][3], concentrations[8]).

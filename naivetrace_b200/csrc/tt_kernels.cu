@@ -1794,6 +1794,10 @@ static int current_device_slot() {
   return dev >= 0 && dev < kGridCacheDevices ? dev : kGridCacheDevices - 1;
 }
 
+// Threads per block of the wavefront launches: the autotuner's choice (128 or 256), else
+// kBlock.  Every wavefront kernel loops grid-stride and takes any size up to kBlock.
+static int blk(const DevScene& s) { return (s.block > 0 && s.block <= kBlock && kBlock % s.block == 0) ? s.block : kBlock; }
+
 // Traversal grid: every SM filled to the traversal kernels' occupancy limit (per layout).
 static int trace_grid(bool wide) {
   static int g[kGridCacheDevices][2] = {};
@@ -1817,16 +1821,16 @@ static int trace_grid(bool wide) {
 
 void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
                      cudaStream_t st) {
-  if (s.num_media > 0) k_generate<true><<<grid, kBlock, 0, st>>>(s, p, fb, w);
-  else k_generate<false><<<grid, kBlock, 0, st>>>(s, p, fb, w);
+  if (s.num_media > 0) k_generate<true><<<grid, blk(s), 0, st>>>(s, p, fb, w);
+  else k_generate<false><<<grid, blk(s), 0, st>>>(s, p, fb, w);
 }
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
                    cudaStream_t st) {
-  grid = trace_grid(s.wide != 0);
+  grid = trace_grid(s.wide != 0) * (kBlock / blk(s));
   with_bool(count, [&](auto C) {
     with_bool(s.num_spheres > 0, [&](auto S) {
       with_bool(s.wide != 0, [&](auto W) {
-        k_extend<decltype(C)::value, decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce, stats);
+        k_extend<decltype(C)::value, decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce, stats);
       });
     });
   });
@@ -1836,31 +1840,31 @@ int shade_launches(const DevScene& s, const PathState& p) {
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
   if (s.algo == TT_ALGO_PT && s.sort_shading && p.sort_q) {
-    k_sort_count<<<grid, kBlock, 0, st>>>(s, p, bounce);
-    k_sort_scatter<<<grid, kBlock, 0, st>>>(p, bounce);
+    k_sort_count<<<grid, blk(s), 0, st>>>(s, p, bounce);
+    k_sort_scatter<<<grid, blk(s), 0, st>>>(p, bounce);
   }
   if (s.algo == TT_ALGO_PT2) {
     if (s.num_media == 0) {
-      k_shade2<false, false, false><<<grid, kBlock, 0, st>>>(s, p, bounce);
+      k_shade2<false, false, false><<<grid, blk(s), 0, st>>>(s, p, bounce);
       return;
     }
     with_bool(s.num_spheres > 0, [&](auto S) {
       with_bool(s.wide != 0, [&](auto W) {
-        k_shade2<true, decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);
+        k_shade2<true, decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce);
       });
     });
     return;
   }
-  if (s.num_media > 0) k_shade<true><<<grid, kBlock, 0, st>>>(s, p, bounce);
-  else k_shade<false><<<grid, kBlock, 0, st>>>(s, p, bounce);
+  if (s.num_media > 0) k_shade<true><<<grid, blk(s), 0, st>>>(s, p, bounce);
+  else k_shade<false><<<grid, blk(s), 0, st>>>(s, p, bounce);
 }
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
-  grid = trace_grid(s.wide != 0);
+  grid = trace_grid(s.wide != 0) * (kBlock / blk(s));
   if (s.algo == TT_ALGO_PT2 && s.num_media > 0) {
     with_bool(s.num_spheres > 0, [&](auto S) {
       with_bool(s.wide != 0, [&](auto W) {
-        k_shadow2<decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);
+        k_shadow2<decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce);
       });
     });
     return;
@@ -1872,7 +1876,7 @@ void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb,
       with_bool(s.num_spheres > 0, [&](auto S) {
         with_bool(s.wide != 0, [&](auto W) {
           k_shadow<decltype(M)::value, decltype(C)::value, decltype(S)::value, decltype(W)::value>
-              <<<grid, kBlock, 0, st>>>(s, p, fb, bounce, stats);
+              <<<grid, blk(s), 0, st>>>(s, p, fb, bounce, stats);
         });
       });
     });
@@ -1882,7 +1886,7 @@ void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, c
   if (s.algo == TT_ALGO_PT2) return;  // the null-path tracer tracks inside its shade stage
   with_bool(s.num_spheres > 0, [&](auto S) {
     with_bool(s.wide != 0, [&](auto W) {
-      k_track<decltype(S)::value, decltype(W)::value><<<grid, kBlock, 0, st>>>(s, p, bounce);
+      k_track<decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce);
     });
   });
 }
@@ -1892,13 +1896,13 @@ void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_
 }
 void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, int grid,
                   cudaStream_t st) {
-  k_flush<<<grid, kBlock, 0, st>>>(s, p, fb, bounce);
+  k_flush<<<grid, blk(s), 0, st>>>(s, p, fb, bounce);
 }
 
 void launch_generate_views(const DevScene& s, const PathState& p, const ViewWave* waves, const int* wave_idx,
                            const DevView* views, int nviews, int grid, cudaStream_t st) {
-  if (s.num_media > 0) k_generate_views<true><<<grid, kBlock, 0, st>>>(s, p, waves, wave_idx, views, nviews);
-  else k_generate_views<false><<<grid, kBlock, 0, st>>>(s, p, waves, wave_idx, views, nviews);
+  if (s.num_media > 0) k_generate_views<true><<<grid, blk(s), 0, st>>>(s, p, waves, wave_idx, views, nviews);
+  else k_generate_views<false><<<grid, blk(s), 0, st>>>(s, p, waves, wave_idx, views, nviews);
 }
 
 void launch_wave_advance(int* wave_idx, cudaStream_t st) { k_wave_advance<<<1, 32, 0, st>>>(wave_idx); }

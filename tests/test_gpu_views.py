@@ -79,10 +79,21 @@ def test_autotune_views(gpu_lib):
     r = g.autotune_views(views)
     assert r["wave_paths"] in (1 << 22, 1 << 24, 1 << 25, 1 << 26)
     assert r["grid"] > 0 and r["ms"] > 0
-    assert len(r["candidates"]) == 12
+    # 12 queue-capacity x launch-width probes, then half-size blocks and the 8-wide BVH.
+    assert len(r["candidates"]) == 14
+    assert {c["block"] for c in r["candidates"]} == {128, 256}
+    assert {c["bvh_width"] for c in r["candidates"]} == {2, 8}
+    assert r["block"] in (128, 256) and r["bvh_width"] in (2, 8)
     assert r["ms"] == min(c["ms"] for c in r["candidates"])
     imgs = g.render_views(views, seed=2)
     assert len(imgs) == 8 and all(np.isfinite(i).all() for i in imgs)
+    assert g.stats()["error_flags"] == 0
+    # Whichever configuration won, the images are those of single-camera passes.
+    for v in (0, 5):
+        cam, spp = views[v]
+        ref = _single(scene, cam, spp, 2 + v, make_params(max_ray_depth=6))
+        scale = max(np.abs(ref).mean(), 1e-6)
+        np.testing.assert_allclose(imgs[v].astype(np.float64), ref, rtol=1e-3, atol=1e-4 * scale)
 
 
 def test_views_reject_bad_input(gpu_lib):
@@ -93,3 +104,42 @@ def test_views_reject_bad_input(gpu_lib):
         g.render_views(bad)
     with pytest.raises(abi.TTError):
         g.render_views([(scene.camera, 0)])
+
+
+def test_views_per_path_against_oracle(gpu_lib):
+    """A three-view batch against the CPU oracle per path: view v of the batch draws the
+    streams of a single-camera pass with seed + v, which the oracle reproduces."""
+    from oracle.oracle import OracleScene, combine
+    scene = scenes.cornell_box_materials(16, 16)
+    views = _views(scene)[:3]
+    g = GpuContext(scene, make_params(max_ray_depth=8))
+    imgs = g.render_views(views, seed=21)
+    assert g.stats()["error_flags"] == 0
+    for v, ((cam, spp), img) in enumerate(zip(views, imgs)):
+        s = copy.copy(scene)
+        s.camera = cam
+        o = OracleScene(s, make_params(max_ray_depth=8))
+        acc, light, splat = o.render(spp, seed=21 + v)
+        ref = combine(acc, light, spp, splat, o.npix).reshape(cam.yres, cam.xres, 3)
+        a, b = img.reshape(-1, 3).astype(np.float64), ref.reshape(-1, 3)
+        scale = max(np.abs(b).mean(), 1e-6)
+        close = np.all(np.abs(a - b) <= 2e-3 * np.abs(b) + 2e-3 * scale, axis=1)
+        assert close.mean() >= 0.9, (v, close.mean())
+
+
+def test_views_completion_times_and_guiding(gpu_lib):
+    """Per-view completion times: within the batch's duration, ordered by the wave that
+    finishes each view; a guided batch (learned guiding on) renders finite images."""
+    scene = scenes.terrain_spheres_small(32, 18)
+    g = GpuContext(scene, make_params(max_ray_depth=6, wave_paths=4000))
+    views = [(c, 2) for c, _ in scenes.terrain_views(6, seed=2, resolutions=(32, 48))]
+    g.render_views(views, seed=3)
+    t = g.views_completion_ms(len(views))
+    assert np.all(t > 0) and np.all(np.diff(t) >= -1e-3)  # later views finish in later waves
+    g.set_guiding(True, 1, seed=7)
+    for k in range(2):
+        g.render_views([(c, 1) for c, _ in views], seed=10 + k)
+    g.set_guiding(True, 0, seed=7)
+    imgs = g.render_views(views, seed=4)
+    assert all(np.isfinite(i).all() for i in imgs)
+    assert g.stats()["guide_steps"] > 0 and g.stats()["error_flags"] == 0
