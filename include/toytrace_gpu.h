@@ -441,6 +441,12 @@ tt_status tt_guide_forward_batch_tc(tt_ctx* ctx, const float* features, int32_t 
  * 14 floats each: position in [0,1]^3, normal, outgoing direction, sampled direction,
  * BSDF pdf of the sampled direction, F/q (host buffers). */
 tt_status tt_guide_gradient_batch(tt_ctx* ctx, const float* records, int32_t n, float* grad, float* loss);
+/* The same mean-loss gradient over a mini-batch of n records drawn from a pool of pool_n
+ * records (host buffer) the way the renderer's training steps draw theirs: record i of the
+ * mini-batch is pool[h(seed ^ h(i)) mod pool_n], h the SplitMix64 finalizer, gathered on the
+ * device by the gradient kernel itself. */
+tt_status tt_guide_gradient_pool_batch(tt_ctx* ctx, const float* pool, int32_t pool_n, int32_t n, uint64_t seed,
+                                       float* grad, float* loss);
 /* `steps` Adam steps of size learning_rate on n training records (layout as above; host
  * buffer), the optimiser state carried over from earlier steps; *loss = the loss of the
  * last step's gradient (may be NULL). */

@@ -237,6 +237,7 @@ EXPORTED_SYMBOLS = [
     "tt_guide_set_params",
     "tt_guide_forward_batch",
     "tt_guide_gradient_batch",
+    "tt_guide_gradient_pool_batch",
     "tt_guide_train_batch",
     "tt_guide_read_records",
     "tt_guide_features_batch",
@@ -360,6 +361,7 @@ def load_library() -> C.CDLL:
         "tt_guide_set_params": ([vp, P(C.c_float), C.c_int32], C.c_int32),
         "tt_guide_forward_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),
         "tt_guide_gradient_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float)], C.c_int32),
+        "tt_guide_gradient_pool_batch": ([vp, P(C.c_float), C.c_int32, C.c_int32, C.c_uint64, P(C.c_float), P(C.c_float)], C.c_int32),
         "tt_guide_train_batch": ([vp, P(C.c_float), C.c_int32, C.c_int32, C.c_float, P(C.c_float)], C.c_int32),
         "tt_guide_read_records": ([vp, P(C.c_float), C.c_int32, P(C.c_int32)], C.c_int32),
         "tt_guide_features_batch": ([vp, P(C.c_float), C.c_int32, P(C.c_float)], C.c_int32),

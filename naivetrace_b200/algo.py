@@ -239,6 +239,15 @@ class GpuContext:
                     "tt_guide_gradient_batch")
         return float(loss.value), g
 
+    def guide_gradient_pool(self, pool: np.ndarray, n: int, seed: int):
+        """Gradient over a mini-batch of n records the device draws from `pool` by `seed`."""
+        r = np.ascontiguousarray(pool, dtype=np.float32).reshape(-1, 14)
+        g = np.zeros(self.lib.tt_guide_num_params(), np.float32)
+        loss = C.c_float(0.0)
+        self._check(self.lib.tt_guide_gradient_pool_batch(self.h, _fp(r), len(r), n, seed, _fp(g), C.byref(loss)),
+                    "tt_guide_gradient_pool_batch")
+        return float(loss.value), g
+
     def guide_train(self, records: np.ndarray, steps: int, learning_rate: float) -> float:
         r = np.ascontiguousarray(records, dtype=np.float32).reshape(-1, 14)
         loss = C.c_float(0.0)

@@ -1922,6 +1922,28 @@ tt_status tt_guide_gradient_batch(tt_ctx* c, const float* records, int32_t n, fl
   return TT_OK;
 }
 
+tt_status tt_guide_gradient_pool_batch(tt_ctx* c, const float* pool, int32_t pool_n, int32_t n, uint64_t seed,
+                                       float* grad, float* loss) {
+  tt_status st = guide_prep(c);
+  if (st != TT_OK) return st;
+  if (!pool || !grad || n <= 0 || pool_n <= 0) return fail(c, TT_ERR_INVALID, "bad batch");
+  std::string gerr;
+  if (!c->gnet->ensure_capacity(n, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
+  GuideRecord* d = nullptr;
+  TT_CUDA(c, cudaMalloc(&d, (size_t)pool_n * sizeof(GuideRecord)));
+  cudaError_t e = cudaMemcpy(d, pool, (size_t)pool_n * sizeof(GuideRecord), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    c->gnet->gradient(d, n, c->stream, false, 0.f, pool_n, seed);
+    e = cudaStreamSynchronize(c->stream);
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(c, TT_ERR_CUDA, cudaGetErrorString(e));
+  TT_CUDA(c, cudaMemcpy(grad, c->gnet->grad, kGParams * sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) TT_CUDA(c, cudaMemcpy(loss, c->gnet->loss, sizeof(float), cudaMemcpyDeviceToHost));
+  return TT_OK;
+}
+
 tt_status tt_guide_train_batch(tt_ctx* c, const float* records, int32_t n, int32_t steps, float lr, float* loss) {
   tt_status st = guide_prep(c);
   if (st != TT_OK) return st;

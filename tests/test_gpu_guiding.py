@@ -113,6 +113,30 @@ def test_gradient_matches_oracle(gpu_lib, n):
     assert cos_f > 0.99, cos_f
 
 
+def _splitmix64(z):
+    m = (1 << 64) - 1
+    z = (z + 0x9E3779B97F4A7C15) & m
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return z ^ (z >> 31)
+
+
+@pytest.mark.parametrize("n,pool_n", [(3000, 5000), (9000, 700)])
+def test_gradient_of_pool_minibatch(gpu_lib, n, pool_n):
+    """The training step draws its mini-batch inside the gradient kernel: record i of the
+    batch is pool[h(seed ^ h(i)) mod pool_n].  The same records gathered on the host with
+    that hash give the same gradient bit for bit (the loss sum uses float atomics)."""
+    g = _ctx()
+    g.guide_set_params(_params())
+    pool = G.random_records(pool_n, seed=pool_n)
+    seed = 0x1234ABCD5678 + n
+    loss_p, grad_p = g.guide_gradient_pool(pool, n, seed)
+    idx = [_splitmix64(seed ^ _splitmix64(i)) % pool_n for i in range(n)]
+    loss_h, grad_h = g.guide_gradient(pool[idx])
+    np.testing.assert_array_equal(grad_p, grad_h)
+    assert abs(loss_p - loss_h) <= 1e-5 * abs(loss_h)
+
+
 def test_adam_step_matches_oracle(gpu_lib):
     g = _ctx()
     p = _params(seed=8)
