@@ -710,7 +710,11 @@ def profile_run(args):
     from naivetrace_b200.algo import GpuContext
     from naivetrace_b200.scene import make_params
     from naivetrace_b200 import abi
-    scene, spp, depth, name = workload(args)
+    if args.profile_scene == "medium":
+        from naivetrace_b200 import scenes
+        scene, spp, depth, name = scenes.cornell_box_medium(1024, 1024), args.spp, 32, "cornell_box_medium"
+    else:
+        scene, spp, depth, name = workload(args)
     algo = abi.ALGO_PT2 if args.algo == "pt2" else abi.ALGO_PT
     g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave, algo=algo, sort_shading=args.sort))
     g.render(spp, 1)
@@ -801,6 +805,8 @@ def main(argv=None):
     ap.add_argument("--no-pt2", action="store_true", help="skip the null-path tracer (pt2) frames")
     ap.add_argument("--no-sort", action="store_true", help="skip the material-sorted shading frames")
     ap.add_argument("--sort", action="store_true", help="--profile-run: shade in material-sorted order")
+    ap.add_argument("--profile-scene", choices=["terrain", "medium"], default="terrain",
+                    help="--profile-run: the bench's terrain workload or the medium-filled Cornell box (1024^2)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the Cornell box, medium and atmosphere configurations")
     ap.add_argument("--algo", choices=["pt", "pt2"], default="pt", help="tracer of --profile-run")
