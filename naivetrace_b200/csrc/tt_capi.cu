@@ -1227,6 +1227,10 @@ static tt_status guide_train(tt_ctx* c, long long paths) {
     cudaMemcpyAsync(&loss, c->gnet->loss, sizeof(float), cudaMemcpyDeviceToHost, c->stream);
     TT_CUDA(c, cudaStreamSynchronize(c->stream));
     TT_CUDA(c, cudaGetLastError());
+    if (c->gnet->tensor_error(c->stream)) {
+      c->stats.error_flags |= ERR_TENSOR;
+      return fail(c, TT_ERR_LOOP_CAP, "a tensor-core wait of the training step timed out");
+    }
     cudaEventElapsedTime(&ms, a, b);
     cudaEventDestroy(a);
     cudaEventDestroy(b);
@@ -1814,6 +1818,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
       return fail(c, TT_ERR_CUDA, gerr);
   }
   c->gparams = *gp;
+  c->gnet->wgrad_tc = gp->network == TT_GUIDE_NET_TCGEN05;
   c->dev.guide_w16 = c->gnet->params16;
   c->dev.guide_w32 = c->gnet->params;
   c->dev.guide = 1;

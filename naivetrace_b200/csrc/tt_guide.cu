@@ -325,6 +325,115 @@ __global__ void __launch_bounds__(128) k_wgrad(int n, TrainBufs b, float* __rest
   if (tid < out) pw[guide_b_offset(l) + tid] = bsum;
 }
 
+// The same weight and bias gradients on the tcgen05 tensor cores.  A CTA of 128 threads
+// owns layer blockIdx.y over records [blockIdx.x * kWtChunk, +kWtChunk) and accumulates
+// D = A B^T in tensor memory, with A (M = 128 rows: the layer's inputs, then a row of ones
+// whose product is the bias gradient, then zeros) and B (N = the layer's outputs) both
+// K-major over records: A[m][k] = X[k][m], B[n][k] = G[k][n].  D[m][n] is dW[n][m] (and the
+// bias gradient of output n in row m = inputs).  Per tile of 128 records each thread stages
+// its record's X and G row transposed into the core-matrix layout of the UMMA descriptors
+// (tt_guide_tc.cuh), one thread issues the 8 MMAs of K = 16 and commits them to an
+// mbarrier; after the last tile every thread reads its lane (one input row) of D.
+constexpr int kWtRecs = 128;                        // records per staged tile (the K extent)
+constexpr int kWtTiles = 4;                         // tiles per CTA
+constexpr int kWtChunk = kWtRecs * kWtTiles;        // records per CTA
+constexpr int kWtA = 0;                             // 128 x 128 BF16
+constexpr int kWtB = kWtA + 128 * kWtRecs * 2;      // kGHid x 128 BF16
+constexpr int kWtBar = kWtB + kGHid * kWtRecs * 2;  // mbarrier
+constexpr int kWtTmem = kWtBar + 8;                 // tensor-memory address
+constexpr int kWtSmem = kWtTmem + 8;
+static_assert(kWtB % 16 == 0 && kWtBar % 8 == 0 && kWtSmem <= 227 * 1024, "tcgen05 weight-gradient layout");
+static_assert(kGIn + 1 <= 128 && kGHid + 1 <= 128, "the inputs and the ones row fit in M = 128");
+
+__global__ void __launch_bounds__(128) k_wgrad_tc(int n, TrainBufs b, float* __restrict__ partial, unsigned* err) {
+  extern __shared__ __align__(128) unsigned char wsm[];
+  const int l = blockIdx.y;
+  const int out = guide_out(l), in = guide_in(l);
+  const bf16* G = l == kGLayers - 1 ? b.dy : b.dh[l];
+  const bf16* X = l == 0 ? b.x : b.h[l - 1];
+  const int t = threadIdx.x;
+  const uint32_t bar = tc_smem(wsm + kWtBar);
+  if (t < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(wsm + kWtTmem)),
+                 "r"(64));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // Rows of A past the ones row stay zero for every tile.
+  for (int e = t; e < 128 * kWtRecs / 8; e += 128) reinterpret_cast<uint4*>(wsm + kWtA)[e] = make_uint4(0u, 0u, 0u, 0u);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(wsm + kWtTmem);
+  const uint32_t idesc = tc_idesc(128, out);
+  uint32_t phase = 0;
+  bool ok = true;
+  const bf16 one = __float2bfloat16(1.f), zero = __float2bfloat16(0.f);
+  for (int tile = 0; tile < kWtTiles && ok; ++tile) {
+    const long long r = (long long)blockIdx.x * kWtChunk + (long long)tile * kWtRecs + t;
+    const bool has = r < n;
+    // Stage record r as column t of A (inputs, ones row) and of B (outputs).
+    for (int c = 0; c < in; c += 8) {
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (has) v = *reinterpret_cast<const uint4*>(X + (size_t)r * in + c);
+      const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) *reinterpret_cast<bf16*>(wsm + kWtA + tc_off(c + j, t, kWtRecs)) = e[j];
+    }
+    *reinterpret_cast<bf16*>(wsm + kWtA + tc_off(in, t, kWtRecs)) = has ? one : zero;
+    for (int c = 0; c < out; c += 8) {
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (has) v = *reinterpret_cast<const uint4*>(G + (size_t)r * out + c);
+      const bf16* e = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) *reinterpret_cast<bf16*>(wsm + kWtB + tc_off(c + j, t, kWtRecs)) = e[j];
+    }
+    // The operands are visible to the tensor cores; the previous tile's MMAs are complete.
+    tc_fence_proxy();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (t == 0) {
+      const uint32_t a0 = tc_smem(wsm + kWtA), b0 = tc_smem(wsm + kWtB);
+      for (int ks = 0; ks < kWtRecs / 16; ++ks)
+        tc_mma(tmem, tc_desc(a0 + ks * 256, 128, kWtRecs * 16), tc_desc(b0 + ks * 256, 128, kWtRecs * 16), idesc,
+               (tile > 0 || ks > 0) ? 1u : 0u);
+      tc_commit(bar);
+    }
+    // Every thread waits before the buffers are overwritten or the accumulator is read.
+    ok = __syncthreads_and(tc_wait(bar, phase & 1u) ? 1 : 0) != 0;
+    ++phase;
+  }
+  if (ok) {
+    tc_fence_after();
+    // Lane t of the accumulator: dW[o][t] for the layer's outputs o, or the bias gradient
+    // when t is the ones row.
+    uint32_t v[kGHid];
+    const uint32_t taddr = tmem + ((uint32_t)((t >> 5) * 32) << 16);
+    tc_ld16(taddr, v);
+    tc_ld16(taddr + 16, v + 16);
+    tc_ld16(taddr + 32, v + 32);
+    tc_ld16(taddr + 48, v + 48);
+    tc_ld_wait();
+    float* pw = partial + (size_t)blockIdx.x * kGParams;
+    if (t < in) {
+      for (int o = 0; o < out; ++o) pw[guide_w_offset(l) + o * in + t] = __uint_as_float(v[o]);
+    } else if (t == in) {
+      for (int o = 0; o < out; ++o) pw[guide_b_offset(l) + o] = __uint_as_float(v[o]);
+    }
+  } else {
+    if (t == 0) atomicOr(err, kTcErrTimeout);
+    if (phase > 0) tc_wait(bar, (phase - 1) & 1u);  // the last commit, before the memory is freed
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (t < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+}
+
 __global__ void k_reduce(const float* __restrict__ part, int z, float* __restrict__ g) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGParams; i += gridDim.x * blockDim.x) {
     float s = 0.f;
@@ -615,14 +724,37 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool ada
   const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
                                    (n + kTrainWarps * kTrainRows - 1) / (kTrainWarps * kTrainRows));
   k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b, pool_n, seed);
-  const int z = (n + kWgChunk - 1) / kWgChunk;
-  k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
+  if (wgrad_tc && !tc_err) {
+    if (cudaMalloc(&tc_err, sizeof(unsigned)) == cudaSuccess) {
+      allocs.push_back(tc_err);
+      cudaMemsetAsync(tc_err, 0, sizeof(unsigned), st);
+    } else {
+      tc_err = nullptr;
+    }
+  }
+  int z;
+  if (wgrad_tc && tc_err) {
+    cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWtSmem);
+    z = (n + kWtChunk - 1) / kWtChunk;
+    k_wgrad_tc<<<dim3(z, kGLayers), 128, kWtSmem, st>>>(n, b, partial, tc_err);
+  } else {
+    z = (n + kWgChunk - 1) / kWgChunk;
+    k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
+  }
   if (adam_step)
     k_reduce_adam<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad, adam_args(*this, lr));
   else
     k_reduce<<<grid1(kGParams), 256, 0, st>>>(partial, z, grad);
 }
 
+
+unsigned GuideNet::tensor_error(cudaStream_t st) {
+  if (!tc_err) return 0u;
+  unsigned e = 0u;
+  cudaMemcpyAsync(&e, tc_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaStreamSynchronize(st);
+  return e;
+}
 
 void GuideNet::adam(float lr, cudaStream_t st) {
   k_adam<<<grid1(kGParams), 256, 0, st>>>(adam_args(*this, lr), grad, kGParams);

@@ -44,6 +44,11 @@ struct GuideNet {
   // on the tensor cores timed out.
   bool forward_tc(const __nv_bfloat16* x, int n, float* out_rows, cudaStream_t st);
   unsigned* tc_err = nullptr;
+  // Weight gradients on the tcgen05 tensor cores (k_wgrad_tc; a wait that gave up sets
+  // tc_err) or on warp-level mma.sync (k_wgrad).
+  bool wgrad_tc = true;
+  // Nonzero when a tcgen05 wait of the network kernels gave up (reads tc_err; synchronous).
+  unsigned tensor_error(cudaStream_t st);
   // Feature rows of n points (9 floats each: position in [0,1]^3, normal, outgoing direction).
   void features(const float* pts, int n, __nv_bfloat16* x, cudaStream_t st);
   // Mean-loss gradient over n records into `grad` and the loss into `loss`; with adam_step

@@ -91,7 +91,8 @@ def test_forward_tcgen05_matches(gpu_lib, n):
 
 @pytest.mark.parametrize("n", [777, 9000])
 def test_gradient_matches_oracle(gpu_lib, n):
-    """9000 records span 71 chunks of the split weight-gradient kernel, the last one ragged."""
+    """9000 records span 18 chunks of 512 records of the tcgen05 weight-gradient kernel, the
+    last one ragged."""
     g = _ctx()
     p = _params()
     g.guide_set_params(p)
@@ -111,6 +112,26 @@ def test_gradient_matches_oracle(gpu_lib, n):
     _, grad_f = G.gradient(p, rec, bf16_round=False)
     cos_f = grad_g @ grad_f / (np.linalg.norm(grad_g) * np.linalg.norm(grad_f))
     assert cos_f > 0.99, cos_f
+
+
+@pytest.mark.parametrize("n", [100, 5000, 70000])
+def test_weight_gradient_tcgen05_matches_mma(gpu_lib, n):
+    """The weight and bias gradients from the tcgen05 kernel (records staged transposed in
+    the UMMA core-matrix layout, accumulators in tensor memory, the bias gradient from a row
+    of ones) against the warp-level mma.sync kernel on the same records: the same BF16
+    products, summed in FP32 in another order."""
+    g = _ctx()
+    g.guide_set_params(_params())
+    rec = G.random_records(n, seed=n + 1)
+    loss_t, grad_t = g.guide_gradient(rec)
+    g.set_guiding(True, 0, network=abi.GUIDE_NET_MMA)
+    loss_m, grad_m = g.guide_gradient(rec)
+    assert abs(loss_t - loss_m) <= 1e-5 * abs(loss_m)
+    for l in range(G.N_LAYERS):
+        a, b = G.w_offset(l), G.b_offset(l) + G.layer_out(l)
+        e = np.linalg.norm(grad_t[a:b] - grad_m[a:b]) / np.linalg.norm(grad_m[a:b])
+        assert e < 2e-4, (l, e)
+    assert g.stats()["error_flags"] == 0
 
 
 def _splitmix64(z):
