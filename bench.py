@@ -310,8 +310,8 @@ def at_time(pts, t0):
     return float(np.exp(np.interp(np.log(t0), ts, es)))
 
 
-GUIDE_SETTINGS = dict(train_passes=4, discard_training=False, learning_rate=1e-3, record_pool=1 << 16,
-                      batch=8192, steps_per_pass=16, max_depth=1)
+GUIDE_SETTINGS = dict(train_passes=3, discard_training=False, learning_rate=1e-3, record_pool=1 << 16,
+                      batch=8192, steps_per_pass=32, max_depth=1)
 
 
 def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):

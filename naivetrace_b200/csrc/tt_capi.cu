@@ -1314,7 +1314,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
         launch_guide(c->dev, c->ps, b, c->stream);
         launches++;
       }
-      launches += 3 + shade_launches(c->dev, c->ps);
+      launches += 3 + shade_launches(c->dev, c->ps, b);
     }
     timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, rounds, counting, c->d_stats + 2, grid, c->stream); });
     launch_flush(c->dev, c->ps, c->fb, rounds, grid, c->stream);
@@ -2159,8 +2159,8 @@ static tt_status render_views(tt_ctx* c, const tt_view* views, int32_t n, uint64
     k_tally<<<1, 32, 0, s>>>(ps.counters, rounds, c->d_stats);
     launch_wave_advance(d_idx, s);
   };
-  const int per_wave = 4 + rounds * (3 + shade_launches(sc, ps) + (sc.num_media > 0)) +
-                       (sc.guide ? std::min(rounds, sc.guide_depth) : 0) + 2;
+  int per_wave = 4 + rounds * (3 + (sc.num_media > 0)) + (sc.guide ? std::min(rounds, sc.guide_depth) : 0) + 2;
+  for (int b = 0; b < rounds; ++b) per_wave += shade_launches(sc, ps, b);
   cudaEventCreate(&ev0);
   cudaEventCreate(&ev1);
   cudaEventRecord(ev0, c->stream);

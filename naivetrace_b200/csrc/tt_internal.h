@@ -256,7 +256,7 @@ void prepare_guide_launch();
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats,
                    int grid, cudaStream_t st);
 // Launches the shading stage (with the material sort when it is on); how many kernels that is.
-int shade_launches(const DevScene& s, const PathState& p);
+int shade_launches(const DevScene& s, const PathState& p, int bounce);
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st);
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st);

@@ -896,6 +896,38 @@ __global__ void k_resolve_views(const float* accum, const float* light, const De
   }
 }
 
+// Material-sorted shading.  The shading key of a hit: 0 escaped, 1 volume vertex, 2 + the
+// shader kind of the hit surface's material.  k_sort_count keys the bounce's hit queue and
+// counts the keys (warp-aggregated atomics, one per distinct key in a warp); k_sort_scatter
+// writes every entry into its key's range of sort_q (ranges in key order, entries of a key
+// in roughly their queue order), so that the warps of k_shade meet one material kind each.
+__device__ __forceinline__ int hit_key(const DevScene& sc, int tri) {
+  if (tri <= -2) return 1;
+  if (tri < 0) return 0;
+  const int mat = __float_as_int(__ldg(&sc.tris[3 * tri + 1]).w);
+  return 2 + min(sc.materials[mat].shader, kShadeKeys - 3);
+}
+__device__ __forceinline__ int shade_key(const DevScene& sc, const PathState& p, int slot) {
+  return hit_key(sc, __float_as_int(p.hit[slot].w));
+}
+// Bounce 0 (camera rays, whose hits are coherent in image order) is shaded unsorted.
+__host__ __device__ __forceinline__ bool sorted_bounce(const DevScene& sc, const PathState& p, int bounce) {
+  return sc.sort_shading && p.sort_q && bounce >= 1;
+}
+
+// Adds 1 for this lane to counter[key]; lanes of a warp with the same key share one atomic.
+// Returns this lane's position among the appends to that counter.
+__device__ __forceinline__ int warp_append_key(int* counter, int key) {
+  const unsigned active = __activemask();
+  const unsigned peers = __match_any_sync(active, key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(&counter[key], __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 // Closest hit of the queued extension rays, one ray per thread over a grid-stride loop
 // sized to the SM count times the kernel's resident blocks.  (A persistent variant that
 // refilled finished lanes after every traversal step measured 20 % slower.)
@@ -903,6 +935,7 @@ template <bool COUNT, bool SPH, bool WIDE>
 __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bounce, unsigned long long* counters) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
+  const bool keyed = sc.algo == TT_ALGO_PT && sc.num_media == 0 && sorted_bounce(sc, p, bounce);
   TraceCounters cnt{0u, 0u};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = q[i];
@@ -911,6 +944,12 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
     float t = 0.f, b1 = 0.f, b2 = 0.f;
     const int hit = trace<false, COUNT, SPH, WIDE>(sc, r, 0.f, d.w, &t, &b1, &b2, p.err, &cnt);
     p.hit[slot] = make_float4(t, b1, b2, __int_as_float(hit));
+    if (keyed) {
+      // Material sort, scenes without media: key and count the hit here.
+      const int key = hit_key(sc, hit);
+      p.sort_key[i] = (unsigned char)key;
+      warp_append_key(key_count(p, bounce), key);
+    }
   }
   if (COUNT) {
     atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
@@ -983,32 +1022,6 @@ __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bou
   }
 }
 
-// Material-sorted shading.  The shading key of a hit: 0 escaped, 1 volume vertex, 2 + the
-// shader kind of the hit surface's material.  k_sort_count keys the bounce's hit queue and
-// counts the keys (warp-aggregated atomics, one per distinct key in a warp); k_sort_scatter
-// writes every entry into its key's range of sort_q (ranges in key order, entries of a key
-// in roughly their queue order), so that the warps of k_shade meet one material kind each.
-__device__ __forceinline__ int shade_key(const DevScene& sc, const PathState& p, int slot) {
-  const int tri = __float_as_int(p.hit[slot].w);
-  if (tri <= -2) return 1;
-  if (tri < 0) return 0;
-  const int mat = __float_as_int(__ldg(&sc.tris[3 * tri + 1]).w);
-  return 2 + min(sc.materials[mat].shader, kShadeKeys - 3);
-}
-
-// Adds 1 for this lane to counter[key]; lanes of a warp with the same key share one atomic.
-// Returns this lane's position among the appends to that counter.
-__device__ __forceinline__ int warp_append_key(int* counter, int key) {
-  const unsigned active = __activemask();
-  const unsigned peers = __match_any_sync(active, key);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(peers) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(&counter[key], __popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  return base + __popc(peers & ((1u << lane) - 1u));
-}
-
 __global__ void __launch_bounds__(256) k_sort_count(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
@@ -1043,7 +1056,7 @@ __global__ void __launch_bounds__(256) k_sort_scatter(PathState p, int bounce) {
 template <bool MEDIA>
 __global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
-  const int* q = (sc.sort_shading && p.sort_q) ? p.sort_q : p.ext_q[bounce & 1];
+  const int* q = sorted_bounce(sc, p, bounce) ? p.sort_q : p.ext_q[bounce & 1];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = q[i];
     const float4 h = p.hit[slot];
@@ -1835,12 +1848,13 @@ void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count
     });
   });
 }
-int shade_launches(const DevScene& s, const PathState& p) {
-  return (s.algo == TT_ALGO_PT && s.sort_shading && p.sort_q) ? 3 : 1;
+int shade_launches(const DevScene& s, const PathState& p, int bounce) {
+  if (s.algo != TT_ALGO_PT || !sorted_bounce(s, p, bounce)) return 1;
+  return s.num_media > 0 ? 3 : 2;  // without media k_extend keys and counts the hits
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
-  if (s.algo == TT_ALGO_PT && s.sort_shading && p.sort_q) {
-    k_sort_count<<<grid, blk(s), 0, st>>>(s, p, bounce);
+  if (s.algo == TT_ALGO_PT && sorted_bounce(s, p, bounce)) {
+    if (s.num_media > 0) k_sort_count<<<grid, blk(s), 0, st>>>(s, p, bounce);
     k_sort_scatter<<<grid, blk(s), 0, st>>>(p, bounce);
   }
   if (s.algo == TT_ALGO_PT2) {
