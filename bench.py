@@ -769,6 +769,36 @@ def profile_guiding(args):
     return 0 if st["error_flags"] == 0 else 1
 
 
+def profile_training(args):
+    """No timing: four Adam steps of the guiding network on 2^18 synthetic training records
+    (the configuration's records per step), each step the training kernel, the tcgen05
+    weight-gradient kernel and the fused reduction and Adam step (for ncu captures)."""
+    from naivetrace_b200 import scenes
+    from naivetrace_b200.algo import GpuContext
+    from naivetrace_b200.scene import make_params
+    n = 1 << 18
+    rng = np.random.default_rng(5)
+
+    def unit(k):
+        v = rng.normal(size=(k, 3))
+        return v / np.linalg.norm(v, axis=1, keepdims=True)
+
+    rec = np.zeros((n, 14), np.float32)
+    rec[:, 0:3] = rng.random((n, 3))
+    rec[:, 3:6] = unit(n)
+    rec[:, 6:9] = unit(n)
+    rec[:, 9:12] = unit(n)
+    rec[:, 12] = 1.0 / (4.0 * np.pi)
+    rec[:, 13] = rng.exponential(1.0, n)
+    g = GpuContext(scenes.guiding_room(16, 16), make_params(max_ray_depth=12))
+    g.set_guiding(True, 1, seed=7, batch=n, record_pool=n)
+    loss = g.guide_train(rec, steps=4, learning_rate=1e-3)
+    st = g.stats()
+    print(json.dumps({"profile_training": "2^18 records, 4 Adam steps", "loss": loss, "error_flags": st["error_flags"]}))
+    g.close()
+    return 0 if (np.isfinite(loss) and st["error_flags"] == 0) else 1
+
+
 def profile_network(args):
     """No timing: the guiding network's forward pass on 2^20 feature rows, three times through
     the tcgen05 kernel and three times through the mma.sync kernel (for ncu launch lists)."""
@@ -819,6 +849,8 @@ def main(argv=None):
                     help="network kernel of --profile-guiding")
     ap.add_argument("--profile-network", action="store_true",
                     help="no timing: the guiding network's forward pass through both kernels (for ncu launch lists)")
+    ap.add_argument("--profile-training", action="store_true",
+                    help="no timing: Adam steps of the guiding network on 2^18 synthetic records (for ncu captures)")
     ap.add_argument("--profile-run", action="store_true",
                     help="no timing: upload the workload and render one pass of --spp samples (for ncu captures)")
     args = ap.parse_args(argv)
@@ -828,6 +860,8 @@ def main(argv=None):
         return profile_guiding(args)
     if args.profile_network:
         return profile_network(args)
+    if args.profile_training:
+        return profile_training(args)
     if args.profile_views:
         return profile_views(args)
     if args.warmup < 3 and not args.small:

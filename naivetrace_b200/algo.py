@@ -180,9 +180,9 @@ class GpuContext:
                     seed: int = 1, method: int = abi.GUIDE_LEARNED, tree_subdivision: int = 100,
                     tree_em_iters: int = 0, network: int = abi.GUIDE_NET_TCGEN05):
         """train: 0 frozen, 1 collect records and train after every pass, 2 collect only;
-        max_depth: guide the first max_depth bounces only (0: all).  Guiding the first two
-        bounces measured the best relMSE per unit time on the gap-lit room (the network's cost
-        grows with every guided vertex, its gain mostly comes from the first ones);
+        max_depth: guide the first max_depth bounces only (0: all).  Guiding the first bounce
+        only measured the best relMSE per unit time on the gap-lit room (the network's cost
+        grows with every guided vertex, its gain mostly comes from the first indirect one);
         network: the inference kernel of the learned guider (GUIDE_NET_TCGEN05 or
         GUIDE_NET_MMA, same outputs)."""
         gp = abi.GuidingParams(int(enabled), int(train), learning_rate, record_pool, batch, steps_per_pass, max_depth,
