@@ -168,7 +168,8 @@ def config_figures(device, cpu_budget=5.0, frames=2):
     cfg 0 the Cornell box 256x256 at 16 spp (depth 10), cfg 2A the Cornell box filled with a
     homogeneous chromatic medium and cfg 2B the planet's atmosphere under a fisheye camera,
     both 1024x1024 at 128 spp (depth 32).  One untimed frame (allocation, warm-up), then
-    `frames` frames timed with CUDA events on the library's stream."""
+    `frames` frames timed with CUDA events on the library's stream; the same again with the
+    hits shaded in traversal order instead of material-sorted order."""
     import torch
 
     from naivetrace_b200 import scenes
@@ -177,9 +178,8 @@ def config_figures(device, cpu_budget=5.0, frames=2):
     cfgs = [("cfg0_cornell_box", scenes.cornell_box(256, 256), 16, 10),
             ("cfg2a_cornell_box_medium", scenes.cornell_box_medium(1024, 1024), 128, 32),
             ("cfg2b_planet_atmosphere", scenes.planet_atmosphere(1024, 1024), 128, 32)]
-    out = {}
-    for name, scene, spp, depth in cfgs:
-        g = GpuContext(scene, make_params(max_ray_depth=depth, device=device))
+    def frame_ms(scene, spp, depth, sort):
+        g = GpuContext(scene, make_params(max_ray_depth=depth, device=device, sort_shading=sort))
         g.render(spp, 1)
         g.clear()
         g.reset_stats()
@@ -191,15 +191,21 @@ def config_figures(device, cpu_budget=5.0, frames=2):
             g.render(spp, 2 + k)
         b.record()
         torch.cuda.synchronize()
-        ms = a.elapsed_time(b) / frames
         st = g.stats()
-        paths = scene.camera.xres * scene.camera.yres * spp
         g.close()
+        return a.elapsed_time(b) / frames, st
+
+    out = {}
+    for name, scene, spp, depth in cfgs:
+        ms, st = frame_ms(scene, spp, depth, None)
+        ms_unsorted, _ = frame_ms(scene, spp, depth, False)
+        paths = scene.camera.xres * scene.camera.yres * spp
         v, cores, desc = cpu_reference(scene, spp, depth, budget_s=cpu_budget, chunk_pixels=4096)
         out[name] = {
             "workload": f"{scene.camera.xres}x{scene.camera.yres} at {spp} spp, max depth {depth}, "
                         f"{scene.num_triangles} triangles, {len(scene.media)} media",
             "ms_per_frame": ms,
+            "ms_per_frame_traversal_order": ms_unsorted,
             "mpaths_per_s": paths / (ms * 1e-3) / 1e6,
             "mrays_per_s": (st["extension_rays"] + st["shadow_rays"]) / frames / (ms * 1e-3) / 1e6,
             "rays_per_path": (st["extension_rays"] + st["shadow_rays"]) / frames / paths,
@@ -508,7 +514,7 @@ def run_reference_arm(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded procedural scene)",
-        "config": workload_config(scene, spp, depth, name),
+        "config": dict(workload_config(scene, spp, depth, name), parallelism=f"replicas{world}, framebuffer all-reduce"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": desc + "; the reference itself cannot be built here (Embree, Eigen, TBB, "
                                           "Boost, yaml-cpp, pcg32 are absent), so this is the CPU restatement"},
@@ -716,7 +722,8 @@ def profile_run(args):
     else:
         scene, spp, depth, name = workload(args)
     algo = abi.ALGO_PT2 if args.algo == "pt2" else abi.ALGO_PT
-    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave, algo=algo, sort_shading=args.sort))
+    g = GpuContext(scene, make_params(max_ray_depth=depth, wave_paths=args.wave, algo=algo,
+                                      sort_shading=True if args.sort else (False if args.unsorted else None)))
     g.render(spp, 1)
     st = g.stats()
     q = g.queue_lengths(depth + 1)
@@ -834,7 +841,8 @@ def main(argv=None):
     ap.add_argument("--no-multiview", action="store_true", help="skip the multi-view batch comparison")
     ap.add_argument("--no-pt2", action="store_true", help="skip the null-path tracer (pt2) frames")
     ap.add_argument("--no-sort", action="store_true", help="skip the material-sorted shading frames")
-    ap.add_argument("--sort", action="store_true", help="--profile-run: shade in material-sorted order")
+    ap.add_argument("--sort", action="store_true", help="--profile-run: shade in material-sorted order (the default)")
+    ap.add_argument("--unsorted", action="store_true", help="--profile-run: shade in traversal order")
     ap.add_argument("--profile-scene", choices=["terrain", "medium"], default="terrain",
                     help="--profile-run: the bench's terrain workload or the medium-filled Cornell box (1024^2)")
     ap.add_argument("--no-configs", action="store_true",

@@ -217,10 +217,13 @@ typedef struct tt_params {
   int32_t qmc;                  /* --qmc (RenderingParameters::qmc): Sobol points with per-pixel
                                    rotations instead of pseudo-random numbers; used by pt2 only
                                    (as in the reference), which then needs max_ray_depth <= 31 */
-  int32_t sort_shading;         /* algo pt: 1 = before each shading launch the bounce's hit queue is
-                                   partitioned by the hit's shading kind (escaped, volume, one key
-                                   per shader), so that a warp shades one material kind; 0 = the
-                                   queue in traversal order (the default) */
+  int32_t sort_shading;         /* algo pt: 1 = from the second bounce on, before each shading
+                                   launch the bounce's hit queue is partitioned by the hit's
+                                   shading kind (escaped, volume, one key per shader), so that a
+                                   warp shades one material kind; negative = the queue in
+                                   traversal order; 0 (the default) = sorted in scenes without
+                                   media whose surfaces use two or more shader kinds, else
+                                   traversal order */
 } tt_params;
 
 typedef struct tt_ctx tt_ctx;
@@ -296,8 +299,9 @@ tt_status tt_render_pass_range(tt_ctx* ctx, int32_t spp, uint64_t seed,
  * a device looks up the array's device address (cudaGetSymbolAddress) and must come before
  * any stream capture.  Requires tt_upload_scene (which allocates the scene) to have run.
  * The pass always renders unguided, also in a context with guiding enabled (the guide's
- * records and network inputs need buffers of their own), and algo pt only (TT_ERR_INVALID
- * for pt2).  A stop requested before the call makes it return TT_ERR_INTERRUPTED without
+ * records and network inputs need buffers of their own), shades in traversal order whatever
+ * sort_shading says (the sort needs buffers of its own too), and algo pt only
+ * (TT_ERR_INVALID for pt2).  A stop requested before the call makes it return TT_ERR_INTERRUPTED without
  * rendering; a stop requested while it runs does not cut it short. */
 tt_status tt_render_pass_noalloc(tt_ctx* ctx, int32_t spp, uint64_t seed, int32_t pixel_begin,
                                  int32_t pixel_end, uint64_t sample_offset, float* d_accum,

@@ -1025,7 +1025,26 @@ tt_status tt_upload_scene(tt_ctx* c) {
   s.long_distance = (float)(10. * diag);
   s.max_path_nodes = c->params.max_ray_depth + 1;
   s.algo = c->params.algo;
-  s.sort_shading = (c->params.sort_shading && c->params.algo == TT_ALGO_PT) ? 1 : 0;
+  // Material-sorted shading pays where the hits of a bounce mix shader kinds: by default
+  // (sort_shading = 0) it is on in scenes without media whose surfaces use two or more
+  // shader kinds.  (Measured: 1.08x on the terrain with Lambert, metal and glass; 1.04x
+  // slower on a Lambert-only box, whose sort buys nothing; 1.2x slower in a medium-filled
+  // box, where the extra counting launch and the scattered path-state reads of the sorted
+  // order outweigh it.)
+  bool sort = c->params.sort_shading > 0;
+  if (c->params.sort_shading == 0 && c->media.empty()) {
+    unsigned kinds = 0u;
+    std::mutex kinds_mutex;
+    parallel_ranges((long long)c->mats.size(), [&](long long t0, long long t1) {
+      unsigned k = 0u;
+      for (long long t = t0; t < t1; ++t) k |= 1u << (c->materials[c->mats[t]].shader & 31);
+      std::lock_guard<std::mutex> g(kinds_mutex);
+      kinds |= k;
+    });
+    for (uint32_t m : c->sphere_mats) kinds |= 1u << (c->materials[m].shader & 31);
+    sort = __builtin_popcount(kinds) >= 2;
+  }
+  s.sort_shading = (sort && c->params.algo == TT_ALGO_PT) ? 1 : 0;
   // Quasi-random sampling: pt2 only, as in the reference (CameraRenderWorker's sampler).
   s.sobol = nullptr;
   s.rotations = nullptr;

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 
 #include "tt_device.cuh"
@@ -273,6 +274,110 @@ __device__ __forceinline__ bool trace_step(const BvhRef& bvh, TraceState& s, int
   return false;
 }
 
+// No node: larger than any node index and not a leaf reference (leaf references are
+// negative, -1 included).
+constexpr int kNoNode = 0x7fffffff;
+
+// Both child boxes of binary node `node` against the ray, culled beyond best_t: returns
+// the child to visit next (kNoNode when neither is hit) and, when both are hit, the
+// farther one in *far_out (else kNoNode).
+__device__ __forceinline__ int visit_node2(const float4* __restrict__ nodes, const RayPre& r, int node, float tnear,
+                                           float best_t, int* far_out) {
+  const float4* np = nodes + 4 * (size_t)node;
+  const float4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+  const int4 n3 = __ldg(reinterpret_cast<const int4*>(np + 3));
+  const float lim = best_t * 1.0000004f;  // 1 + 2 gamma(3): conservative slabs
+  float tx0 = fmaf(n0.x, r.id.x, -r.ood.x), tx1 = fmaf(n0.y, r.id.x, -r.ood.x);
+  float ty0 = fmaf(n0.z, r.id.y, -r.ood.y), ty1 = fmaf(n0.w, r.id.y, -r.ood.y);
+  float tz0 = fmaf(n2.x, r.id.z, -r.ood.z), tz1 = fmaf(n2.y, r.id.z, -r.ood.z);
+  const float c0min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tnear));
+  const float c0max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+  tx0 = fmaf(n1.x, r.id.x, -r.ood.x); tx1 = fmaf(n1.y, r.id.x, -r.ood.x);
+  ty0 = fmaf(n1.z, r.id.y, -r.ood.y); ty1 = fmaf(n1.w, r.id.y, -r.ood.y);
+  tz0 = fmaf(n2.z, r.id.z, -r.ood.z); tz1 = fmaf(n2.w, r.id.z, -r.ood.z);
+  const float c1min = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), tnear));
+  const float c1max = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+  const bool h0 = c0min <= c0max, h1 = c1min <= c1max;
+  *far_out = kNoNode;
+  if (h0 && h1) {
+    const bool swap = c1min < c0min;
+    *far_out = swap ? n3.x : n3.y;
+    return swap ? n3.y : n3.x;
+  }
+  return h0 ? n3.x : (h1 ? n3.y : kNoNode);
+}
+
+// Binary-BVH traversal in the "speculative while-while" form of Aila and Laine (2009,
+// "Understanding the efficiency of ray traversal on GPUs"): a lane that reaches a leaf
+// postpones it and keeps descending inner nodes until every active lane of the warp holds
+// a leaf (or has finished); then the lanes test their leaves' primitives together, so inner
+// and leaf work run in separate loops instead of splitting the warp every step.  A
+// postponed leaf is tested after the inner nodes visited meanwhile (their culling used the
+// older best_t, which only adds work); the closest hit and its tie-break are unchanged.
+template <bool ANY, bool COUNT, bool SPH>
+__device__ __forceinline__ void trace_ww(const BvhRef& bvh, TraceState& s, int* stack, unsigned int* err,
+                                         TraceCounters* cnt) {
+  const RayPre& r = s.r;
+  int cur = 0;         // the root is always an inner node
+  int leaf = kNoNode;  // postponed leaf reference, or kNoNode
+  int sp = 0;
+  while (cur != kNoNode || leaf != kNoNode) {
+    // Inner nodes (0 <= cur < kNoNode).
+    while ((unsigned)cur < (unsigned)kNoNode) {
+      int far;
+      const int next = visit_node2(bvh.nodes, r, cur, s.tnear, s.best_t, &far);
+      if (COUNT) cnt->nodes++;
+      if (next == kNoNode) {
+        cur = sp > 0 ? stack[--sp] : kNoNode;
+      } else {
+        if (far != kNoNode) {
+          if (sp >= BVH_STACK) {
+            atomicOr(err, ERR_STACK);
+            s.best = -1;
+            return;
+          }
+          stack[sp++] = far;
+        }
+        cur = next;
+      }
+      // Postpone the first leaf met and carry on with the stack.
+      if (cur < 0 && leaf == kNoNode) {
+        leaf = cur;
+        cur = sp > 0 ? stack[--sp] : kNoNode;
+      }
+      if (!__any_sync(__activemask(), leaf == kNoNode)) break;
+    }
+    // Leaves: the postponed one, then cur while it is a leaf.
+    while (leaf != kNoNode) {
+      const unsigned v = ~(unsigned)leaf;
+      const int start = (int)(v >> 3), count = (int)(v & 7u) + 1;
+      for (int i = start; i < start + count; ++i) {
+        const float4 a = __ldg(&bvh.tris[3 * i]);
+        const float4 b = __ldg(&bvh.tris[3 * i + 1]);
+        const float4 c = __ldg(&bvh.tris[3 * i + 2]);
+        if (COUNT) cnt->tris++;
+        float t, b1 = 0.f, b2 = 0.f;
+        bool hit;
+        if (SPH && __float_as_int(c.w) != 0) hit = intersect_sphere(r, a, b, s.tnear, s.best_t, &t);
+        else hit = intersect_tri(r, xyz(a), xyz(b), xyz(c), s.tnear, s.best_t, &t, &b1, &b2);
+        if (hit && (ANY || closer(t, __float_as_int(a.w), s.best_t, s.best_prim))) {
+          s.best = i;
+          s.best_prim = __float_as_int(a.w);
+          s.best_t = t;
+          s.b1 = b1;
+          s.b2 = b2;
+          if (ANY) return;
+        }
+      }
+      leaf = kNoNode;
+      if (cur < 0) {
+        leaf = cur;
+        cur = sp > 0 ? stack[--sp] : kNoNode;
+      }
+    }
+  }
+}
+
 // Recomputes the distance of the closest hit from the plane equation in double precision
 // (float rounding of Ng.(v0 - o) is amplified by 1/|cos| at grazing incidence).
 __device__ __forceinline__ float refine_t(const float4* tris, const RayPre& r, int slot) {
@@ -457,7 +562,14 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
   s.best_prim = 0x7fffffff;
   s.cur = 0;
   s.sp = 0;
-  while (!trace_step<ANY, COUNT, SPH>(bvh, s, stack, err, cnt)) {
+  if (ANY) {
+    // Any hit: one node or leaf per step, so that a lane meets its first hit as early as
+    // the tree order allows (postponing leaves measured 3.5 % slower for shadow rays).
+    while (!trace_step<ANY, COUNT, SPH>(bvh, s, stack, err, cnt)) {
+    }
+  } else {
+    // Closest hit: while-while traversal (6.5 % less closest-hit time on the bench frame).
+    trace_ww<ANY, COUNT, SPH>(bvh, s, stack, err, cnt);
   }
   if (s.best >= 0) {
     *t_out = (ANY || (SPH && is_sphere_slot(sc.tris, s.best))) ? s.best_t : refine_t(sc.tris, r, s.best);
@@ -1054,7 +1166,7 @@ __global__ void __launch_bounds__(256) k_sort_scatter(PathState p, int bounce) {
 }
 
 template <bool MEDIA>
-__global__ void __launch_bounds__(256) k_shade(DevScene sc, PathState p, int bounce) {
+__global__ void __launch_bounds__(256, MEDIA ? 2 : 3) k_shade(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
   const int* q = sorted_bounce(sc, p, bounce) ? p.sort_q : p.ext_q[bounce & 1];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1811,39 +1923,70 @@ static int current_device_slot() {
 // kBlock.  Every wavefront kernel loops grid-stride and takes any size up to kBlock.
 static int blk(const DevScene& s) { return (s.block > 0 && s.block <= kBlock && kBlock % s.block == 0) ? s.block : kBlock; }
 
-// Traversal grid: every SM filled to the traversal kernels' occupancy limit (per layout).
-static int trace_grid(bool wide) {
-  static int g[kGridCacheDevices][2] = {};
-  int& gg = g[current_device_slot()][wide ? 1 : 0];
+// Blocks of `fn` that stay resident on one SM at `block` threads, cached per device,
+// kernel and block size (a short list under a mutex; the first launch of each kernel pays
+// one occupancy query).
+static int resident_blocks(const void* fn, int block) {
+  struct Entry {
+    const void* fn;
+    int dev, block, blocks;
+  };
+  static std::mutex mu;
+  static Entry cache[512];
+  static int used = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  for (int i = 0; i < used; ++i)
+    if (cache[i].fn == fn && cache[i].dev == dev && cache[i].block == block) return cache[i].blocks;
+  int b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, block, 0);
+  if (b < 1) b = 1;
+  if (used < 512) cache[used++] = Entry{fn, dev, block, b};
+  return b;
+}
+static int sm_count() {
+  static int g[kGridCacheDevices] = {};
+  int& gg = g[current_device_slot()];
   if (gg == 0) {
-    int dev = 0, sms = 0, b0 = 0, b1 = 0;
+    int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (wide) {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false, false, true>, kBlock, 0);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false, false, true>, kBlock, 0);
-    } else {
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, k_extend<false, false, false>, kBlock, 0);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_shadow<false, false, false, false>, kBlock, 0);
-    }
-    gg = sms * (b0 < b1 ? b0 : b1);
-    if (gg < 1) gg = 1;
+    gg = sms > 0 ? sms : 1;
   }
   return gg;
+}
+// Grid of a grid-stride wavefront launch: every SM filled to the launched kernel's own
+// occupancy limit (traversal kernels).  A kernel whose variants differ in registers (the
+// sphere and media instantiations) would otherwise get a grid sized for another variant
+// and run a last partial round of blocks on a third of the SMs' slots.
+template <class K>
+static int full_grid(K* kernel, int block) {
+  return sm_count() * resident_blocks(reinterpret_cast<const void*>(kernel), block);
+}
+// A requested grid (the context's default or the autotuner's choice) cut down to whole
+// rounds of resident blocks of this kernel: no partial last round.
+template <class K>
+static int fit_grid(K* kernel, int grid, int block) {
+  const int cap = full_grid(kernel, block);
+  return grid > cap ? grid / cap * cap : grid;
 }
 
 void launch_generate(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
                      cudaStream_t st) {
-  if (s.num_media > 0) k_generate<true><<<grid, blk(s), 0, st>>>(s, p, fb, w);
-  else k_generate<false><<<grid, blk(s), 0, st>>>(s, p, fb, w);
+  const int b = blk(s);
+  if (s.num_media > 0) k_generate<true><<<fit_grid(k_generate<true>, grid, b), b, 0, st>>>(s, p, fb, w);
+  else k_generate<false><<<fit_grid(k_generate<false>, grid, b), b, 0, st>>>(s, p, fb, w);
 }
 void launch_extend(const DevScene& s, const PathState& p, int bounce, bool count, unsigned long long* stats, int grid,
                    cudaStream_t st) {
-  grid = trace_grid(s.wide != 0) * (kBlock / blk(s));
+  (void)grid;
+  const int b = blk(s);
   with_bool(count, [&](auto C) {
     with_bool(s.num_spheres > 0, [&](auto S) {
       with_bool(s.wide != 0, [&](auto W) {
-        k_extend<decltype(C)::value, decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce, stats);
+        auto* k = k_extend<decltype(C)::value, decltype(S)::value, decltype(W)::value>;
+        k<<<full_grid(k, b), b, 0, st>>>(s, p, bounce, stats);
       });
     });
   });
@@ -1853,32 +1996,37 @@ int shade_launches(const DevScene& s, const PathState& p, int bounce) {
   return s.num_media > 0 ? 3 : 2;  // without media k_extend keys and counts the hits
 }
 void launch_shade(const DevScene& s, const PathState& p, int bounce, int grid, cudaStream_t st) {
+  const int b = blk(s);
   if (s.algo == TT_ALGO_PT && sorted_bounce(s, p, bounce)) {
-    if (s.num_media > 0) k_sort_count<<<grid, blk(s), 0, st>>>(s, p, bounce);
-    k_sort_scatter<<<grid, blk(s), 0, st>>>(p, bounce);
+    if (s.num_media > 0) k_sort_count<<<fit_grid(k_sort_count, grid, b), b, 0, st>>>(s, p, bounce);
+    k_sort_scatter<<<fit_grid(k_sort_scatter, grid, b), b, 0, st>>>(p, bounce);
   }
   if (s.algo == TT_ALGO_PT2) {
     if (s.num_media == 0) {
-      k_shade2<false, false, false><<<grid, blk(s), 0, st>>>(s, p, bounce);
+      auto* k = k_shade2<false, false, false>;
+      k<<<fit_grid(k, grid, b), b, 0, st>>>(s, p, bounce);
       return;
     }
     with_bool(s.num_spheres > 0, [&](auto S) {
       with_bool(s.wide != 0, [&](auto W) {
-        k_shade2<true, decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce);
+        auto* k = k_shade2<true, decltype(S)::value, decltype(W)::value>;
+        k<<<fit_grid(k, grid, b), b, 0, st>>>(s, p, bounce);
       });
     });
     return;
   }
-  if (s.num_media > 0) k_shade<true><<<grid, blk(s), 0, st>>>(s, p, bounce);
-  else k_shade<false><<<grid, blk(s), 0, st>>>(s, p, bounce);
+  if (s.num_media > 0) k_shade<true><<<fit_grid(k_shade<true>, grid, b), b, 0, st>>>(s, p, bounce);
+  else k_shade<false><<<fit_grid(k_shade<false>, grid, b), b, 0, st>>>(s, p, bounce);
 }
 void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, bool count,
                    unsigned long long* stats, int grid, cudaStream_t st) {
-  grid = trace_grid(s.wide != 0) * (kBlock / blk(s));
+  (void)grid;
+  const int b = blk(s);
   if (s.algo == TT_ALGO_PT2 && s.num_media > 0) {
     with_bool(s.num_spheres > 0, [&](auto S) {
       with_bool(s.wide != 0, [&](auto W) {
-        k_shadow2<decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce);
+        auto* k = k_shadow2<decltype(S)::value, decltype(W)::value>;
+        k<<<full_grid(k, b), b, 0, st>>>(s, p, bounce);
       });
     });
     return;
@@ -1889,8 +2037,8 @@ void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb,
     with_bool(count, [&](auto C) {
       with_bool(s.num_spheres > 0, [&](auto S) {
         with_bool(s.wide != 0, [&](auto W) {
-          k_shadow<decltype(M)::value, decltype(C)::value, decltype(S)::value, decltype(W)::value>
-              <<<grid, blk(s), 0, st>>>(s, p, fb, bounce, stats);
+          auto* k = k_shadow<decltype(M)::value, decltype(C)::value, decltype(S)::value, decltype(W)::value>;
+          k<<<full_grid(k, b), b, 0, st>>>(s, p, fb, bounce, stats);
         });
       });
     });
@@ -1900,7 +2048,8 @@ void launch_track(const DevScene& s, const PathState& p, int bounce, int grid, c
   if (s.algo == TT_ALGO_PT2) return;  // the null-path tracer tracks inside its shade stage
   with_bool(s.num_spheres > 0, [&](auto S) {
     with_bool(s.wide != 0, [&](auto W) {
-      k_track<decltype(S)::value, decltype(W)::value><<<grid, blk(s), 0, st>>>(s, p, bounce);
+      auto* k = k_track<decltype(S)::value, decltype(W)::value>;
+      k<<<fit_grid(k, grid, blk(s)), blk(s), 0, st>>>(s, p, bounce);
     });
   });
 }
@@ -1910,13 +2059,16 @@ void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_
 }
 void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, int grid,
                   cudaStream_t st) {
-  k_flush<<<grid, blk(s), 0, st>>>(s, p, fb, bounce);
+  k_flush<<<fit_grid(k_flush, grid, blk(s)), blk(s), 0, st>>>(s, p, fb, bounce);
 }
 
 void launch_generate_views(const DevScene& s, const PathState& p, const ViewWave* waves, const int* wave_idx,
                            const DevView* views, int nviews, int grid, cudaStream_t st) {
-  if (s.num_media > 0) k_generate_views<true><<<grid, blk(s), 0, st>>>(s, p, waves, wave_idx, views, nviews);
-  else k_generate_views<false><<<grid, blk(s), 0, st>>>(s, p, waves, wave_idx, views, nviews);
+  const int b = blk(s);
+  if (s.num_media > 0)
+    k_generate_views<true><<<fit_grid(k_generate_views<true>, grid, b), b, 0, st>>>(s, p, waves, wave_idx, views, nviews);
+  else
+    k_generate_views<false><<<fit_grid(k_generate_views<false>, grid, b), b, 0, st>>>(s, p, waves, wave_idx, views, nviews);
 }
 
 void launch_wave_advance(int* wave_idx, cudaStream_t st) { k_wave_advance<<<1, 32, 0, st>>>(wave_idx); }

@@ -400,9 +400,12 @@ class Scene:
 
 def make_params(max_ray_depth: int = 25, pt_sample_mode: int = abi.SAMPLE_BOTH, max_spp: int = -1,
                 wave_paths: int = 0, device: int = 0, algo: int = abi.ALGO_PT, qmc: bool = False,
-                sort_shading: bool = False) -> abi.Params:
+                sort_shading: bool | None = None) -> abi.Params:
+    """sort_shading: None = the library default (material-sorted shading from the second
+    bounce on in scenes without media whose surfaces use two or more shader kinds),
+    True = always sorted, False = traversal order."""
     p = abi.Params()
-    p.sort_shading = int(bool(sort_shading))
+    p.sort_shading = 0 if sort_shading is None else (1 if sort_shading else -1)
     p.algo = algo
     p.qmc = int(bool(qmc))
     p.max_ray_depth = max_ray_depth

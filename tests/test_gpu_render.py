@@ -196,7 +196,7 @@ def test_material_sorted_shading(gpu_lib, name):
     pass up to the order of the float atomics, and per-path parity with the oracle."""
     scene = getattr(scenes, name)(48, 32) if name != "terrain_spheres_small" else scenes.terrain_spheres_small(48, 27)
     depth = 12
-    g0 = GpuContext(scene, make_params(max_ray_depth=depth))
+    g0 = GpuContext(scene, make_params(max_ray_depth=depth, sort_shading=False))
     g0.render(4, seed=3)
     a0, l0, _, _ = g0.accumulators()
     g1 = GpuContext(scene, make_params(max_ray_depth=depth, sort_shading=True))

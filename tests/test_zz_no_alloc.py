@@ -35,7 +35,8 @@ def noalloc_pass(g, spp, seed, pixel_begin, pixel_end, sample_offset=0):
                                             ("cornell_box_media_mix", 4, 10)])
 def test_noalloc_matches_render_pass(gpu_lib, name, spp, depth):
     scene = scenes.terrain_spheres_small(64, 36) if name == "terrain_spheres_small" else getattr(scenes, name)(32, 32)
-    params = make_params(max_ray_depth=depth)
+    # The allocation-free pass shades in traversal order (it has no sort buffers).
+    params = make_params(max_ray_depth=depth, sort_shading=False)
     ref = GpuContext(scene, params)
     ref.render(spp, seed=7)
     acc_ref, light_ref, _, _ = ref.accumulators()
