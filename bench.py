@@ -719,6 +719,9 @@ def profile_run(args):
     if args.profile_scene == "medium":
         from naivetrace_b200 import scenes
         scene, spp, depth, name = scenes.cornell_box_medium(1024, 1024), args.spp, 32, "cornell_box_medium"
+    elif args.profile_scene == "room":
+        from naivetrace_b200 import scenes
+        scene, spp, depth, name = scenes.guiding_room(1280, 720), args.spp, 12, "guiding_room"
     else:
         scene, spp, depth, name = workload(args)
     algo = abi.ALGO_PT2 if args.algo == "pt2" else abi.ALGO_PT
@@ -843,8 +846,9 @@ def main(argv=None):
     ap.add_argument("--no-sort", action="store_true", help="skip the material-sorted shading frames")
     ap.add_argument("--sort", action="store_true", help="--profile-run: shade in material-sorted order (the default)")
     ap.add_argument("--unsorted", action="store_true", help="--profile-run: shade in traversal order")
-    ap.add_argument("--profile-scene", choices=["terrain", "medium"], default="terrain",
-                    help="--profile-run: the bench's terrain workload or the medium-filled Cornell box (1024^2)")
+    ap.add_argument("--profile-scene", choices=["terrain", "medium", "room"], default="terrain",
+                    help="--profile-run: the bench's terrain workload, the medium-filled Cornell box (1024^2) "
+                         "or the gap-lit room of the guiding workload (1280x720)")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the Cornell box, medium and atmosphere configurations")
     ap.add_argument("--algo", choices=["pt", "pt2"], default="pt", help="tracer of --profile-run")

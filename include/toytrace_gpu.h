@@ -222,7 +222,7 @@ typedef struct tt_params {
                                    shading kind (escaped, volume, one key per shader), so that a
                                    warp shades one material kind; negative = the queue in
                                    traversal order; 0 (the default) = sorted in scenes without
-                                   media whose surfaces use two or more shader kinds, else
+                                   media whose surfaces use three or more shader kinds, else
                                    traversal order */
 } tt_params;
 

@@ -204,10 +204,10 @@ __global__ void k_merge(const int* clusters, int c, const int* nn, const int* cr
 }
 
 // Bottom-up over one creation range: subtree sizes and SAH costs (traversal step 1,
-// primitive test 1 per primitive), and whether a subtree of at most kMaxLeaf primitives
-// is cheaper as one leaf.
+// primitive test 1 per primitive), whether a subtree of at most kMaxLeaf primitives is
+// cheaper as one leaf, and the number of inner nodes the subtree emits.
 __global__ void k_costs(int first, int count, uint32_t n, const Aabb* node_box, const int* left, const int* right,
-                        int* size, float* cost, unsigned char* collapse) {
+                        int* size, float* cost, unsigned char* collapse, int* inner) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
     const int k = first + t;
     const int l = left[k], r = right[k];
@@ -222,15 +222,18 @@ __global__ void k_costs(int first, int count, uint32_t n, const Aabb* node_box, 
     size[k] = s;
     cost[k] = as_leaf ? leaf : split;
     collapse[k] = as_leaf ? 1 : 0;
+    inner[k] = as_leaf ? 0 : 1 + (l < (int)n ? 0 : inner[l]) + (r < (int)n ? 0 : inner[r]);
   }
 }
 
-// Top-down over one creation range: primitive offsets (depth-first order) and whether the
-// node is emitted as an inner node, lies inside a leaf, or is a leaf itself.
-// state: bit 0 = inside a leaf (set by an ancestor that became a leaf).
+// Top-down over one creation range: primitive offsets and node indices (both in depth-first
+// order: an inner node's first child follows it in memory, its second child follows the
+// first child's subtree) and whether the node is emitted as an inner node, lies inside a
+// leaf, or is a leaf itself.  state: bit 0 = inside a leaf (set by an ancestor that
+// became a leaf).
 __global__ void k_topdown(int first, int count, uint32_t n, const int* left, const int* right, const int* size,
-                          const unsigned char* collapse, int* offset, unsigned char* state, int* depth,
-                          unsigned char* emit, unsigned* max_depth) {
+                          const unsigned char* collapse, const int* inner, int* offset, int* index,
+                          unsigned char* state, int* depth, unsigned char* emit, unsigned* max_depth) {
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
     const int k = first + t;
     const bool inside = state[k] & 1u;
@@ -245,6 +248,8 @@ __global__ void k_topdown(int first, int count, uint32_t n, const int* left, con
     if (!leafnode) {
       depth[l] = depth[k] + 1;
       depth[r] = depth[k] + 1;
+      index[l] = index[k] + 1;
+      index[r] = index[k] + 1 + (l < (int)n ? 0 : inner[l]);
       atomicMax(max_depth, (unsigned)(depth[k] + 1));
     }
   }
@@ -298,16 +303,6 @@ __global__ void k_write_nodes(int first, int count, uint32_t n, const Aabb* node
     d[3] = make_float4(__int_as_float(child_ref(l, n, size, offset, emit, index)),
                        __int_as_float(child_ref(r, n, size, offset, emit, index)), 0.f, 0.f);
   }
-}
-
-// index[k] = number of emitted nodes with a larger id (so the root, the last node, is 0).
-__global__ void k_reverse_flags(const unsigned char* emit, int total, int* rev) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
-    rev[i] = emit[total - 1 - i];
-}
-__global__ void k_reverse_index(const int* rev_off, int total, int* index) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
-    index[total - 1 - i] = rev_off[i];
 }
 
 // Root handling for trees whose root is a leaf: one node with the leaf as child 0 and an
@@ -470,42 +465,33 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   unsigned char* state = sc.alloc<unsigned char>(total);
   int* depth = sc.alloc<int>(total);
   unsigned char* emit = sc.alloc<unsigned char>(total);
-  int* rev = sc.alloc<int>(total);
-  int* rev_off = sc.alloc<int>(total);
+  int* inner = sc.alloc<int>(total);
   int* index = sc.alloc<int>(total);
   unsigned* max_depth = sc.alloc<unsigned>(1);
-  if (!size || !cost || !collapse || !offset || !state || !depth || !emit || !rev || !rev_off || !index || !max_depth)
+  if (!size || !cost || !collapse || !offset || !state || !depth || !emit || !inner || !index || !max_depth)
     return fail("out of device memory");
   cudaMemsetAsync(collapse, 1, n, st);  // primitive leaves
   cudaMemsetAsync(emit, 0, total, st);
   cudaMemsetAsync(max_depth, 0, sizeof(unsigned), st);
   for (const auto& r : ranges)
-    k_costs<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, cost, collapse);
+    k_costs<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, cost, collapse,
+                                                      inner);
   const int zero = 0;
   const unsigned char none = 0;
   cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(index + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(state + root, &none, 1, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(depth + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
   for (auto it = ranges.rbegin(); it != ranges.rend(); ++it)
-    k_topdown<<<grid_for(it->second), kThreads, 0, st>>>(it->first, it->second, n, left, right, size, collapse, offset,
-                                                          state, depth, emit, max_depth);
-  // Node indices: emitted nodes numbered from the root down.
-  k_reverse_flags<<<grid_for(total), kThreads, 0, st>>>(emit, (int)total, rev);
-  size_t tb = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, tb, rev, rev_off, (int)total, st);
-  void* temp2 = sc.alloc<unsigned char>(tb);
-  if (!temp2) return fail("out of device memory");
-  cub::DeviceScan::ExclusiveSum(temp2, tb, rev, rev_off, (int)total, st);
-  k_reverse_index<<<grid_for(total), kThreads, 0, st>>>(rev_off, (int)total, index);
-  int emitted_tail[2] = {0, 0};
+    k_topdown<<<grid_for(it->second), kThreads, 0, st>>>(it->first, it->second, n, left, right, size, collapse, inner,
+                                                          offset, index, state, depth, emit, max_depth);
+  int emitted = 0;
   unsigned depth_host = 0;
   unsigned char root_emit = 0;
-  cudaMemcpyAsync(&emitted_tail[0], rev_off + total - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&emitted_tail[1], rev + total - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (root >= (int)n) cudaMemcpyAsync(&emitted, inner + root, sizeof(int), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(&depth_host, max_depth, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(&root_emit, emit + root, 1, cudaMemcpyDeviceToHost, st);
   if (!ok(cudaStreamSynchronize(st), "emission")) return false;
-  const int emitted = emitted_tail[0] + emitted_tail[1];
   const int num_nodes = root_emit ? emitted : 1;
   if (!ok(pool_malloc((void**)&out->nodes, 4 * sizeof(float4) * (size_t)num_nodes, st), "allocation") ||
       !ok(pool_malloc((void**)&out->tris, 3 * sizeof(float4) * (size_t)n, st), "allocation"))

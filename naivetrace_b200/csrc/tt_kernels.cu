@@ -1009,10 +1009,15 @@ __global__ void k_resolve_views(const float* accum, const float* light, const De
 }
 
 // Material-sorted shading.  The shading key of a hit: 0 escaped, 1 volume vertex, 2 + the
-// shader kind of the hit surface's material.  k_sort_count keys the bounce's hit queue and
-// counts the keys (warp-aggregated atomics, one per distinct key in a warp); k_sort_scatter
-// writes every entry into its key's range of sort_q (ranges in key order, entries of a key
-// in roughly their queue order), so that the warps of k_shade meet one material kind each.
+// shader kind of the hit surface's material.  k_sort_count (or k_extend itself) keys the
+// bounce's hit queue and counts the keys (a shared-memory histogram per block);
+// k_sort_scatter writes every entry into its key's range of sort_q (ranges in key order,
+// entries of a key in queue order within each block's share), so that the warps of k_shade
+// meet one material kind each.  The sorted order interleaves the path slots of different
+// keys: in a scene of two shader kinds k_shade fetched 1.8x the DRAM bytes sorted, and a
+// partition within windows of 1,024 queue entries (which keeps the slots a block touches)
+// did not recover the loss, so the library sorts by default only where the divergence it
+// removes is larger (three or more shader kinds).
 __device__ __forceinline__ int hit_key(const DevScene& sc, int tri) {
   if (tri <= -2) return 1;
   if (tri < 0) return 0;
@@ -1027,18 +1032,24 @@ __host__ __device__ __forceinline__ bool sorted_bounce(const DevScene& sc, const
   return sc.sort_shading && p.sort_q && bounce >= 1;
 }
 
-// Adds 1 for this lane to counter[key]; lanes of a warp with the same key share one atomic.
-// Returns this lane's position among the appends to that counter.
-__device__ __forceinline__ int warp_append_key(int* counter, int key) {
-  const unsigned active = __activemask();
-  const unsigned peers = __match_any_sync(active, key);
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(peers) - 1;
-  int base = 0;
-  if (lane == leader) base = atomicAdd(&counter[key], __popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  return base + __popc(peers & ((1u << lane) - 1u));
-}
+// Per-block key histogram in shared memory: lanes with the same key share one shared
+// atomic per warp, and the block adds its counts to the bounce's global counters once at
+// the end (one global atomic per key and block; one per key and warp serialised on the few
+// counter addresses).
+struct KeyHistogram {
+  int* h;  // kShadeKeys shared ints
+  __device__ void clear() {
+    if (threadIdx.x < kShadeKeys) h[threadIdx.x] = 0;
+  }
+  __device__ void add(int key) {
+    const unsigned peers = __match_any_sync(__activemask(), key);
+    if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[key], __popc(peers));
+  }
+  // After a __syncthreads that follows every add.
+  __device__ void flush(int* global) {
+    if (threadIdx.x < kShadeKeys && h[threadIdx.x] != 0) atomicAdd(&global[threadIdx.x], h[threadIdx.x]);
+  }
+};
 
 // Closest hit of the queued extension rays, one ray per thread over a grid-stride loop
 // sized to the SM count times the kernel's resident blocks.  (A persistent variant that
@@ -1048,6 +1059,12 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
   const bool keyed = sc.algo == TT_ALGO_PT && sc.num_media == 0 && sorted_bounce(sc, p, bounce);
+  __shared__ int hist_mem[kShadeKeys];
+  KeyHistogram hist{hist_mem};
+  if (keyed) {
+    hist.clear();
+    __syncthreads();
+  }
   TraceCounters cnt{0u, 0u};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int slot = q[i];
@@ -1060,8 +1077,12 @@ __global__ void __launch_bounds__(256) k_extend(DevScene sc, PathState p, int bo
       // Material sort, scenes without media: key and count the hit here.
       const int key = hit_key(sc, hit);
       p.sort_key[i] = (unsigned char)key;
-      warp_append_key(key_count(p, bounce), key);
+      hist.add(key);
     }
+  }
+  if (keyed) {  // uniform over the grid
+    __syncthreads();
+    hist.flush(key_count(p, bounce));
   }
   if (COUNT) {
     atomicAdd(&counters[0], (unsigned long long)cnt.nodes);
@@ -1137,16 +1158,28 @@ __global__ void __launch_bounds__(256) k_track(DevScene sc, PathState p, int bou
 __global__ void __launch_bounds__(256) k_sort_count(DevScene sc, PathState p, int bounce) {
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
-  int* counts = key_count(p, bounce);
+  __shared__ int hist_mem[kShadeKeys];
+  KeyHistogram hist{hist_mem};
+  hist.clear();
+  __syncthreads();
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int key = shade_key(sc, p, q[i]);
     p.sort_key[i] = (unsigned char)key;
-    warp_append_key(counts, key);
+    hist.add(key);
   }
+  __syncthreads();
+  hist.flush(key_count(p, bounce));
 }
 
 __global__ void __launch_bounds__(256) k_sort_scatter(PathState p, int bounce) {
+  // Per block and iteration of blockDim queue entries: each warp ranks its lanes per key
+  // (match_any), the block adds up the warps' counts per key in shared memory and reserves
+  // its range of every key's segment with one global atomic per key, and every entry is
+  // written at segment start + block range + warp offset + lane rank.
+  constexpr int kWarps = 256 / 32;
   __shared__ int base[kShadeKeys];
+  __shared__ int wcount[kWarps][kShadeKeys];
+  __shared__ int block_off[kShadeKeys];
   if (threadIdx.x == 0) {
     const int* counts = key_count(p, bounce);
     int acc = 0;
@@ -1155,13 +1188,33 @@ __global__ void __launch_bounds__(256) k_sort_scatter(PathState p, int bounce) {
       acc += counts[k];
     }
   }
-  __syncthreads();
   const int n = *ext_count(p, bounce);
   const int* q = p.ext_q[bounce & 1];
   int* cursor = key_cursor(p, bounce);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const int key = p.sort_key[i];
-    p.sort_q[base[key] + warp_append_key(cursor, key)] = q[i];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nwarps = blockDim.x >> 5;
+  for (int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+    const int i = i0 + threadIdx.x;
+    const int key = i < n ? (int)p.sort_key[i] : -1;
+    for (int k = threadIdx.x; k < kWarps * kShadeKeys; k += blockDim.x) (&wcount[0][0])[k] = 0;
+    __syncthreads();
+    const unsigned peers = __match_any_sync(0xffffffffu, key);
+    const int rank = __popc(peers & ((1u << lane) - 1u));
+    if (key >= 0 && lane == __ffs(peers) - 1) wcount[warp][key] = __popc(peers);
+    __syncthreads();
+    if (threadIdx.x < kShadeKeys) {
+      const int k = threadIdx.x;
+      int acc = 0;
+      for (int w = 0; w < nwarps; ++w) {
+        const int c = wcount[w][k];
+        wcount[w][k] = acc;
+        acc += c;
+      }
+      block_off[k] = acc > 0 ? atomicAdd(&cursor[k], acc) : 0;
+    }
+    __syncthreads();
+    if (key >= 0) p.sort_q[base[key] + block_off[key] + wcount[warp][key] + rank] = q[i];
+    __syncthreads();
   }
 }
 

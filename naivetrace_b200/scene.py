@@ -402,7 +402,7 @@ def make_params(max_ray_depth: int = 25, pt_sample_mode: int = abi.SAMPLE_BOTH, 
                 wave_paths: int = 0, device: int = 0, algo: int = abi.ALGO_PT, qmc: bool = False,
                 sort_shading: bool | None = None) -> abi.Params:
     """sort_shading: None = the library default (material-sorted shading from the second
-    bounce on in scenes without media whose surfaces use two or more shader kinds),
+    bounce on in scenes without media whose surfaces use three or more shader kinds),
     True = always sorted, False = traversal order."""
     p = abi.Params()
     p.sort_shading = 0 if sort_shading is None else (1 if sort_shading else -1)
