@@ -332,6 +332,9 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
     tree_kw = dict(st_kw)
     tree_kw.update(tree_subdivision=200, tree_em_iters=4)
     tree, tst = wl.curve(True, tree=True, budget_ms=budget_ms, **tree_kw)
+    quad_kw = dict(st_kw)
+    quad_kw.update(tree_subdivision=200, tree_distribution=1)
+    quad, qst = wl.curve(True, tree=True, budget_ms=budget_ms, **quad_kw)
     t_eq = min(plain[-1][0], guided[-1][0])
     tp, tg = time_to(plain, target), time_to(guided, target)
     ep, eg = at_time(plain, t_eq), at_time(guided, t_eq)
@@ -356,6 +359,16 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
             "rounds": int(tst["guide_steps"]), "records": int(tst["guide_records"]),
             "round_ms_total": tst["guide_train_ms"],
             "curve": [[round(t, 2), s, round(e, 6)] for t, s, e in tree],
+        },
+        "tree_guider_quadtree": {
+            "what": "kd-tree cells (200 records per initial cell) with the reference's quadtree radiance "
+                    "distributions and the stochastic record filter, the same schedule of training passes",
+            "time_to_target_ms": time_to(quad, target),
+            "relmse_at_equal_time": at_time(quad, min(t_eq, quad[-1][0])),
+            "gain_equal_time": ep / at_time(quad, t_eq) if quad[-1][0] >= t_eq else None,
+            "rounds": int(qst["guide_steps"]), "records": int(qst["guide_records"]),
+            "round_ms_total": qst["guide_train_ms"],
+            "curve": [[round(t, 2), s, round(e, 6)] for t, s, e in quad],
         },
         "curve_plain": [[round(t, 2), s, round(e, 6)] for t, s, e in plain],
         "curve_guided": [[round(t, 2), s, round(e, 6)] for t, s, e in guided],

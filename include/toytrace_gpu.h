@@ -28,7 +28,7 @@ extern "C" {
 #endif
 
 #define TT_NBINS 36
-#define TT_ABI_VERSION 8
+#define TT_ABI_VERSION 9
 
 typedef int32_t tt_status;
 enum {
@@ -422,9 +422,15 @@ typedef struct tt_guiding_params {
                                    rendering, TT_GUIDE_NET_TCGEN05 (tensor-memory accumulators,
                                    128-row tiles) or TT_GUIDE_NET_MMA (warp-level mma.sync,
                                    16-row tiles); both give the same outputs */
+  int32_t tree_distribution;    /* TT_GUIDE_TREE: the directional distribution of a cell,
+                                   TT_TREE_VMF (8-lobe vMF mixture, the reference's MoVmf
+                                   distribution) or TT_TREE_QUADTREE (the reference's active
+                                   quadtree radiance distribution, fitted with the stochastic
+                                   record filter) */
 } tt_guiding_params;
 enum { TT_GUIDE_LEARNED = 0, TT_GUIDE_TREE = 1 };
 enum { TT_GUIDE_NET_TCGEN05 = 0, TT_GUIDE_NET_MMA = 1 };
+enum { TT_TREE_VMF = 0, TT_TREE_QUADTREE = 1 };
 
 /* Enables or disables guiding.  The network is created (He-uniform weights from `seed`) on
  * first use and keeps its trained weights while guiding is switched off and on again.  Until
@@ -488,6 +494,28 @@ tt_status tt_vmf_fit_batch(const float* records, int32_t n, const float* mixture
  * each point's cell and *cells; min_points as --guide-subdiv-factor. */
 tt_status tt_kdtree_build_batch(const float* points, int32_t n, int32_t min_points, int32_t* cell_of_point,
                                 int32_t* cells);
+/* Quadtree radiance distribution (tree_distribution = TT_TREE_QUADTREE; path_guiding.cxx:
+ * 108-310, path_guiding_quadtree.cxx).  Directions map to the unit square by
+ * u = atan2(y, x) / (2 pi) + 1/2, v = (z + 1) / 2; a node's children are the quadrants
+ * 0 = (u < c, v < c), 1 = (u >= c, v < c), 2 = (u < c, v >= c), 3 = (u >= c, v >= c) of its
+ * square; every parent precedes its children.  Sampling weights: leaves as fitted, inner
+ * nodes the sums of their children.
+ * A cell's current distribution: children (4 per node, -1 for a leaf) and sampling weights
+ * of up to cap nodes, *num_nodes = its node count (TT_ERR_CAPACITY if above cap). */
+tt_status tt_guide_tree_quadtree(tt_ctx* ctx, int32_t cell, int32_t cap, int32_t* children, float* weights,
+                                 int32_t* num_nodes);
+/* The quadtree fit on the host, for tests (no device use): InitialFit + Bake on the na
+ * records A (unit directions, 3 floats each, and weights); with stage >= 1 then
+ * IncrementalFit of the nb records B; with stage >= 2 then IterationUpdateAndBake.  Writes
+ * children, sampling weights and the prior of up to cap nodes and *num_nodes. */
+tt_status tt_quadtree_fit_batch(const float* dirs_a, const float* weights_a, int32_t na, const float* dirs_b,
+                                const float* weights_b, int32_t nb, int32_t stage, int32_t cap, int32_t* children,
+                                float* weights, float* prior, int32_t* num_nodes);
+/* The device sampler of the tree-guided kernel on a given quadtree, for tests: n directions
+ * drawn with the uniforms u[2i], u[2i+1] (hierarchical warping), their densities per unit
+ * solid angle, and the density the guided kernel evaluates at the returned direction. */
+tt_status tt_quadtree_sample_batch(const int32_t* children, const float* weights, int32_t num_nodes, const float* u,
+                                   int32_t n, float* out_dir, float* out_pdf, float* out_pdf_eval);
 
 /* ---- Multi-view batches ------------------------------------------------------------
  * No counterpart in the reference (it renders one camera per RenderingAlgo).  A batch of

@@ -250,12 +250,17 @@ EXPORTED_SYMBOLS = [
     "tt_guide_tree_lookup_batch",
     "tt_vmf_fit_batch",
     "tt_kdtree_build_batch",
+    "tt_guide_tree_quadtree",
+    "tt_quadtree_fit_batch",
+    "tt_quadtree_sample_batch",
 ]
 
 GUIDE_LEARNED = 0
 GUIDE_TREE = 1
 GUIDE_NET_TCGEN05 = 0
 GUIDE_NET_MMA = 1
+TREE_VMF = 0
+TREE_QUADTREE = 1
 
 
 class View(C.Structure):
@@ -295,6 +300,7 @@ class GuidingParams(C.Structure):
         ("tree_subdivision", C.c_int32),
         ("tree_em_iters", C.c_int32),
         ("network", C.c_int32),
+        ("tree_distribution", C.c_int32),
     ]
 
 
@@ -375,6 +381,12 @@ def load_library() -> C.CDLL:
         "tt_vmf_fit_batch": ([P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float),
                               P(C.c_float)], C.c_int32),
         "tt_kdtree_build_batch": ([P(C.c_float), C.c_int32, C.c_int32, P(C.c_int32), P(C.c_int32)], C.c_int32),
+        "tt_guide_tree_quadtree": ([vp, C.c_int32, C.c_int32, P(C.c_int32), P(C.c_float), P(C.c_int32)], C.c_int32),
+        "tt_quadtree_fit_batch": ([P(C.c_float), P(C.c_float), C.c_int32, P(C.c_float), P(C.c_float), C.c_int32,
+                                   C.c_int32, C.c_int32, P(C.c_int32), P(C.c_float), P(C.c_float), P(C.c_int32)],
+                                  C.c_int32),
+        "tt_quadtree_sample_batch": ([P(C.c_int32), P(C.c_float), C.c_int32, P(C.c_float), C.c_int32, P(C.c_float),
+                                      P(C.c_float), P(C.c_float)], C.c_int32),
     }
     for name, (argtypes, restype) in sig.items():
         fn = getattr(lib, name)

@@ -28,6 +28,10 @@ def _fp(a):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+def _ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int32))
+
+
 class GpuContext:
     """One tt_ctx: a scene uploaded to one GPU plus its accumulators."""
 
@@ -178,15 +182,18 @@ class GpuContext:
     def set_guiding(self, enabled: bool = True, train: int = 1, learning_rate: float = 1e-3,
                     record_pool: int = 1 << 16, batch: int = 8192, steps_per_pass: int = 16, max_depth: int = 2,
                     seed: int = 1, method: int = abi.GUIDE_LEARNED, tree_subdivision: int = 100,
-                    tree_em_iters: int = 0, network: int = abi.GUIDE_NET_TCGEN05):
+                    tree_em_iters: int = 0, network: int = abi.GUIDE_NET_TCGEN05,
+                    tree_distribution: int = abi.TREE_VMF):
         """train: 0 frozen, 1 collect records and train after every pass, 2 collect only;
         max_depth: guide the first max_depth bounces only (0: all).  Guiding the first bounce
         only measured the best relMSE per unit time on the gap-lit room (the network's cost
         grows with every guided vertex, its gain mostly comes from the first indirect one);
         network: the inference kernel of the learned guider (GUIDE_NET_TCGEN05 or
-        GUIDE_NET_MMA, same outputs)."""
+        GUIDE_NET_MMA, same outputs); tree_distribution: the tree guider's per-cell
+        distribution (TREE_VMF mixtures or TREE_QUADTREE, the reference's quadtrees)."""
         gp = abi.GuidingParams(int(enabled), int(train), learning_rate, record_pool, batch, steps_per_pass, max_depth,
-                               seed, int(method), int(tree_subdivision), int(tree_em_iters), int(network))
+                               seed, int(method), int(tree_subdivision), int(tree_em_iters), int(network),
+                               int(tree_distribution))
         self._check(self.lib.tt_set_guiding(self.h, C.byref(gp)), "tt_set_guiding")
 
     def tree_info(self) -> dict:
@@ -203,6 +210,15 @@ class GpuContext:
         out = np.zeros((n, 40), np.float32)
         self._check(self.lib.tt_guide_tree_mixtures(self.h, _fp(out), n), "tt_guide_tree_mixtures")
         return out
+
+    def tree_quadtree(self, cell: int, cap: int = 1 << 16):
+        """A cell's quadtree: children (nodes, 4; -1 for a leaf) and sampling weights."""
+        ch = np.zeros((cap, 4), np.int32)
+        w = np.zeros(cap, np.float32)
+        nn = C.c_int32(0)
+        self._check(self.lib.tt_guide_tree_quadtree(self.h, int(cell), cap, _ip(ch), _fp(w), C.byref(nn)),
+                    "tt_guide_tree_quadtree")
+        return ch[: nn.value].copy(), w[: nn.value].copy()
 
     def tree_lookup(self, points) -> np.ndarray:
         pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
@@ -496,3 +512,40 @@ def kdtree_build_batch(points, min_points: int = 100):
                                    C.byref(nc))
     abi.check(lib, None, st, "tt_kdtree_build_batch")
     return cells, nc.value
+
+
+def quadtree_fit_batch(dirs_a, weights_a, dirs_b=None, weights_b=None, stage: int = 0, cap: int = 1 << 16):
+    """The tree guider's quadtree fit (host code of the library, no GPU needed): InitialFit +
+    Bake on records A (unit directions (n, 3), weights), then with stage >= 1 IncrementalFit
+    of records B, with stage >= 2 IterationUpdateAndBake.  Returns (children (nodes, 4),
+    sampling weights, prior)."""
+    lib = abi.load_library()
+    da = np.ascontiguousarray(dirs_a, np.float32).reshape(-1, 3)
+    wa = np.ascontiguousarray(weights_a, np.float32).reshape(-1)
+    db = np.ascontiguousarray(dirs_b if dirs_b is not None else np.zeros((0, 3)), np.float32).reshape(-1, 3)
+    wb = np.ascontiguousarray(weights_b if weights_b is not None else np.zeros(0), np.float32).reshape(-1)
+    ch = np.zeros((cap, 4), np.int32)
+    w = np.zeros(cap, np.float32)
+    pr = np.zeros(cap, np.float32)
+    nn = C.c_int32(0)
+    st = lib.tt_quadtree_fit_batch(_fp(da), _fp(wa), len(da), _fp(db), _fp(wb), len(db), int(stage), cap, _ip(ch),
+                                   _fp(w), _fp(pr), C.byref(nn))
+    abi.check(lib, None, st, "tt_quadtree_fit_batch")
+    n = nn.value
+    return ch[:n].copy(), w[:n].copy(), pr[:n].copy()
+
+
+def quadtree_sample_batch(children, weights, u):
+    """The tree-guided kernel's quadtree sampler on the device with given uniforms u (n, 2):
+    returns directions (n, 3), their densities and the densities evaluated at them."""
+    lib = abi.load_library()
+    ch = np.ascontiguousarray(children, np.int32).reshape(-1, 4)
+    w = np.ascontiguousarray(weights, np.float32).reshape(-1)
+    uu = np.ascontiguousarray(u, np.float32).reshape(-1, 2)
+    n = len(uu)
+    d = np.zeros((n, 3), np.float32)
+    p = np.zeros(n, np.float32)
+    e = np.zeros(n, np.float32)
+    st = lib.tt_quadtree_sample_batch(_ip(ch), _fp(w), len(ch), _fp(uu), n, _fp(d), _fp(p), _fp(e))
+    abi.check(lib, None, st, "tt_quadtree_sample_batch")
+    return d, p, e

@@ -19,8 +19,9 @@ CSRC = PKG / "csrc"
 OUT_DIR = PKG / "_build"
 LIB = OUT_DIR / "libtoytrace_gpu.so"
 
-SOURCES = ["tt_kernels.cu", "tt_capi.cu", "tt_noalloc.cu", "tt_build.cu", "tt_guide.cu", "tt_tree.cu", "tt_bvh.cpp"]
-HEADERS = ["tt_internal.h", "tt_device.cuh", "tt_bvh.h", "tt_build.h", "tt_guide.h", "tt_guide.cuh", "tt_tables.h", "tt_pt2.cuh", "tt_sobol_data.h", "tt_tree.h", "tt_guide_tc.cuh"]
+SOURCES = ["tt_kernels.cu", "tt_capi.cu", "tt_noalloc.cu", "tt_build.cu", "tt_guide.cu", "tt_tree.cu", "tt_bvh.cpp",
+           "tt_quadtree.cpp"]
+HEADERS = ["tt_internal.h", "tt_device.cuh", "tt_bvh.h", "tt_build.h", "tt_guide.h", "tt_guide.cuh", "tt_tables.h", "tt_pt2.cuh", "tt_sobol_data.h", "tt_tree.h", "tt_guide_tc.cuh", "tt_quadtree.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

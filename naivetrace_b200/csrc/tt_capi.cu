@@ -25,6 +25,7 @@
 #include "tt_internal.h"
 #include "tt_sobol_data.h"
 #include "tt_tables.h"
+#include "tt_quadtree.h"
 #include "tt_tree.h"
 
 using namespace tt;
@@ -1181,6 +1182,17 @@ static tt_status ensure_path_state_fit(tt_ctx* c, int* cap) {
   }
 }
 
+// The tree guider's device arrays into the scene the kernels see.
+static void tree_to_dev(tt_ctx* c) {
+  c->dev.tree_nodes = c->tree->d_nodes;
+  c->dev.tree_root = c->tree->root_ref();
+  c->dev.tree_mix = c->tree->d_mix;
+  c->dev.tree_quad = c->tree->distribution == TT_TREE_QUADTREE ? 1 : 0;
+  c->dev.tree_qchild = c->tree->d_qchild;
+  c->dev.tree_qprob = c->tree->d_qprob;
+  c->dev.tree_qroot = c->tree->d_qroot;
+}
+
 // After a pass: `steps_per_pass` Adam steps, each on a mini-batch drawn from the record
 // pool; also updates the pool's yield per path, from which the next pass's keep
 // probability follows.
@@ -1218,9 +1230,7 @@ static tt_status guide_train(tt_ctx* c, long long paths) {
                             cudaMemcpyDeviceToHost));
     std::string gerr;
     if (!c->tree->fit_round(recs.data(), n, c->gparams.seed, c->stream, &gerr)) return fail(c, TT_ERR_CUDA, gerr);
-    c->dev.tree_nodes = c->tree->d_nodes;
-    c->dev.tree_root = c->tree->root_ref();
-    c->dev.tree_mix = c->tree->d_mix;
+    tree_to_dev(c);
     c->stats.guide_records += (uint64_t)n;
     c->stats.guide_steps += 1;
     c->stats.guide_train_ms +=
@@ -1798,12 +1808,16 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   if (gp->record_pool < 0 || gp->batch < 0 || gp->steps_per_pass < 0 || gp->max_depth < 0 ||
       !(gp->learning_rate >= 0.f) || gp->train < 0 || gp->train > 2 ||
       (gp->method != TT_GUIDE_LEARNED && gp->method != TT_GUIDE_TREE) || gp->tree_subdivision < 0 ||
-      gp->tree_em_iters < 0 || (gp->network != TT_GUIDE_NET_TCGEN05 && gp->network != TT_GUIDE_NET_MMA))
+      gp->tree_em_iters < 0 || (gp->network != TT_GUIDE_NET_TCGEN05 && gp->network != TT_GUIDE_NET_MMA) ||
+      (gp->tree_distribution != TT_TREE_VMF && gp->tree_distribution != TT_TREE_QUADTREE))
     return fail(c, TT_ERR_INVALID, "bad guiding parameters");
   const int cap = gp->record_pool > 0 ? gp->record_pool : (1 << 16);
+  // A tree fitted with the other directional distribution starts over.
+  if (c->tree && c->tree->distribution != gp->tree_distribution) c->tree.reset();
   if (gp->method == TT_GUIDE_TREE && !c->tree) {
     c->tree = std::make_unique<TreeGuide>();
     std::string gerr;
+    c->tree->distribution = gp->tree_distribution;
     if (!c->tree->init(gp->tree_subdivision, c->stream, &gerr)) {
       c->tree.reset();
       return fail(c, TT_ERR_CUDA, gerr);
@@ -1843,11 +1857,7 @@ tt_status tt_set_guiding(tt_ctx* c, const tt_guiding_params* gp) {
   c->dev.guide = 1;
   c->dev.guide_method = gp->method;
   c->dev.guide_net = gp->network;
-  if (gp->method == TT_GUIDE_TREE) {
-    c->dev.tree_nodes = c->tree->d_nodes;
-    c->dev.tree_root = c->tree->root_ref();
-    c->dev.tree_mix = c->tree->d_mix;
-  }
+  if (gp->method == TT_GUIDE_TREE) tree_to_dev(c);
   c->dev.guide_record = gp->train ? 1 : 0;
   c->dev.guide_depth = gp->max_depth > 0 ? gp->max_depth : (1 << 30);
   return TT_OK;
@@ -2037,6 +2047,90 @@ tt_status tt_kdtree_build_batch(const float* points, int32_t n, int32_t min_poin
     return fail(nullptr, TT_ERR_INVALID, "tt_kdtree_build_batch: bad arguments");
   std::vector<TreeNodeHost> nodes;
   *cells = kdtree_build(points, n, min_points > 0 ? min_points : 100, &nodes, cell_of_point);
+  return TT_OK;
+}
+
+// Children (-1 for a leaf) and weights of a quadtree into caller buffers.
+static tt_status write_quad(const QuadDist& q, int32_t cap, int32_t* children, float* weights, float* prior,
+                            int32_t* num_nodes) {
+  *num_nodes = q.num_nodes();
+  if (q.num_nodes() > cap) return fail(nullptr, TT_ERR_CAPACITY, "quadtree larger than the buffers");
+  for (int j = 0; j < q.num_nodes(); ++j) {
+    for (int k = 0; k < 4; ++k) children[4 * j + k] = q.child[j][k];
+    if (weights) weights[j] = q.probs[j];
+    if (prior) prior[j] = q.prior[j];
+  }
+  return TT_OK;
+}
+
+tt_status tt_guide_tree_quadtree(tt_ctx* c, int32_t cell, int32_t cap, int32_t* children, float* weights,
+                                 int32_t* num_nodes) {
+  if (!c || !children || !weights || !num_nodes || cap < 0) return TT_ERR_INVALID;
+  if (!c->tree || c->tree->distribution != TT_TREE_QUADTREE)
+    return fail(c, TT_ERR_NOT_READY, "the tree guider with quadtrees is not enabled");
+  if (cell < 0 || cell >= c->tree->ncells) return fail(c, TT_ERR_INVALID, "no such cell");
+  return write_quad(c->tree->quads[cell], cap, children, weights, nullptr, num_nodes);
+}
+
+tt_status tt_quadtree_fit_batch(const float* dirs_a, const float* weights_a, int32_t na, const float* dirs_b,
+                                const float* weights_b, int32_t nb, int32_t stage, int32_t cap, int32_t* children,
+                                float* weights, float* prior, int32_t* num_nodes) {
+  if (na < 0 || nb < 0 || (na > 0 && (!dirs_a || !weights_a)) || (nb > 0 && (!dirs_b || !weights_b)) || stage < 0 ||
+      stage > 2 || cap < 0 || !children || !weights || !prior || !num_nodes)
+    return fail(nullptr, TT_ERR_INVALID, "tt_quadtree_fit_batch: bad arguments");
+  auto to_square = [](const float* d, int n) {
+    std::vector<float> uv(2 * (size_t)n);
+    for (int i = 0; i < n; ++i) dir_to_square(d + 3 * (size_t)i, &uv[2 * (size_t)i]);
+    return uv;
+  };
+  QuadDist q;
+  const std::vector<float> ua = to_square(dirs_a, na);
+  q.initial_fit(ua.data(), weights_a, na);
+  q.bake();
+  if (stage >= 1) {
+    const std::vector<float> ub = to_square(dirs_b, nb);
+    q.incremental_fit(ub.data(), weights_b, nb, 1);
+  }
+  if (stage >= 2) q.update_and_bake();
+  return write_quad(q, cap, children, weights, prior, num_nodes);
+}
+
+tt_status tt_quadtree_sample_batch(const int32_t* children, const float* weights, int32_t num_nodes, const float* u,
+                                   int32_t n, float* out_dir, float* out_pdf, float* out_pdf_eval) {
+  if (!children || !weights || num_nodes <= 0 || n < 0 || (n > 0 && (!u || !out_dir || !out_pdf || !out_pdf_eval)))
+    return fail(nullptr, TT_ERR_INVALID, "tt_quadtree_sample_batch: bad arguments");
+  // Every child index must name a node after its parent (no cycles, all in range), so that
+  // the device walk ends at a leaf.
+  for (int j = 0; j < num_nodes; ++j) {
+    const int32_t* k = children + 4 * (size_t)j;
+    const bool leaf = k[0] < 0;
+    for (int q = 0; q < 4; ++q)
+      if (leaf ? k[q] >= 0 : (k[q] <= j || k[q] >= num_nodes))
+        return fail(nullptr, TT_ERR_INVALID, "tt_quadtree_sample_batch: bad tree");
+  }
+  if (n == 0) return TT_OK;
+  int4* dc = nullptr;
+  float *dw = nullptr, *du = nullptr, *dd = nullptr, *dp = nullptr, *de = nullptr;
+  cudaError_t e = cudaMalloc(&dc, (size_t)num_nodes * sizeof(int4));
+  if (e == cudaSuccess) e = cudaMalloc(&dw, (size_t)num_nodes * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&du, 2 * (size_t)n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dd, 3 * (size_t)n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&dp, (size_t)n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc(&de, (size_t)n * sizeof(float));
+  if (e == cudaSuccess) e = cudaMemcpy(dc, children, (size_t)num_nodes * sizeof(int4), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dw, weights, (size_t)num_nodes * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(du, u, 2 * (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    launch_quadtree_sample(dc, dw, du, n, dd, dp, de, 0);
+    e = cudaDeviceSynchronize();
+  }
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(out_dir, dd, 3 * (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(out_pdf, dp, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(out_pdf_eval, de, (size_t)n * sizeof(float), cudaMemcpyDeviceToHost);
+  for (void* p : {(void*)dc, (void*)dw, (void*)du, (void*)dd, (void*)dp, (void*)de})
+    if (p) cudaFree(p);
+  if (e != cudaSuccess) return fail(nullptr, TT_ERR_CUDA, cudaGetErrorString(e));
   return TT_OK;
 }
 

@@ -155,6 +155,10 @@ struct DevScene {
   const float4* tree_nodes;
   int tree_root;
   const float* tree_mix;
+  int tree_quad;             // the cells' directional distributions are quadtrees
+  const int4* tree_qchild;   // their nodes (absolute child indices, -1: leaf)
+  const float* tree_qprob;   // sampling weights per node
+  const int* tree_qroot;     // root node per cell
   // Quasi-random sampling (pt2 with qmc): Sobol generator matrices, 32 words per dimension
   // (TT_SOBOL_DIMS dimensions), and the per-pixel rotations [128 * 128][2]; null otherwise.
   const uint32_t* sobol;
@@ -281,6 +285,8 @@ void launch_sample_bsdf(const DevScene& s, int material, float3 wi, int3 lambda,
                         float* dir, float* val, float* pdf, cudaStream_t st);
 void launch_eval_bsdf(const DevScene& s, int material, float3 wi, int3 lambda, const float* dirs, int n, float* val,
                       float* pdf, cudaStream_t st);
+void launch_quadtree_sample(const int4* child, const float* prob, const float* u, int n, float* dir, float* pdf,
+                            float* pdf_eval, cudaStream_t st);
 void launch_sample_phase(const DevScene& s, int medium, float3 pos, float3 wi, int3 lambda, int n,
                          unsigned long long seed, float* dir, float* val, float* pdf, cudaStream_t st);
 void launch_eval_phase(const DevScene& s, int medium, float3 pos, float3 wi, int3 lambda, const float* dirs, int n,

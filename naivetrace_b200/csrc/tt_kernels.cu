@@ -1429,9 +1429,11 @@ __device__ __forceinline__ GuidePre guide_prefetch(const PathState& p, int slot)
   return g;
 }
 
-template <bool MEDIA>
-__device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const PathState& p, int bounce,
-                                                  const GuidePre& pre, const GuideMixture& mix) {
+// One-sample MIS between the BSDF and a guiding distribution `dist` (sample(rng), pdf(x),
+// and c, the probability of sampling it) at a queued guided vertex.
+template <bool MEDIA, class Dist>
+__device__ __forceinline__ void guide_scatter_dist(const DevScene& sc, const PathState& p, int bounce,
+                                                   const GuidePre& pre, const Dist& dist) {
   const int slot = pre.slot;
   const float4 h = pre.h;
   const float3 dir = xyz(pre.d4);
@@ -1451,9 +1453,9 @@ __device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const Path
   float pb = 0.f;
   // An untrained network is not sampled: selection probability 0 gives plain BSDF sampling
   // with the BSDF density, while the records for the first training step are collected.
-  const float c = sc.guide_cold ? 0.f : mix.c;
+  const float c = sc.guide_cold ? 0.f : dist.c;
   if (rng.uniform() < c) {
-    ndir = guide_mixture_sample(mix, rng);
+    ndir = dist.sample(rng);
     val = eval_bsdf(m, wi, s, ndir, l, &pb);
   } else {
     const ScatterSample ss = sample_bsdf(m, wi, s, rng, l);
@@ -1461,12 +1463,12 @@ __device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const Path
     val = ss.value;
     pb = ss.pdf;
   }
-  const float pg = guide_mixture_pdf(mix, ndir);
+  const float pg = dist.pdf(ndir);
   const float pdf = (1.f - c) * pb + c * pg;
   const float4 nee = pre.nee;
   if (nee.w != 0.f) {
     const float3 sd = xyz(p.sh_d[slot]);
-    const float pdf_due = ((1.f - c) * nee.z + c * guide_mixture_pdf(mix, sd)) * nee.y;
+    const float pdf_due = ((1.f - c) * nee.z + c * dist.pdf(sd)) * nee.y;
     if (MEDIA) {
       p.sh_med[slot].y = pdf_due;
     } else if (nee.x > 0.f) {
@@ -1522,6 +1524,19 @@ __device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const Path
   p.rng_state[slot] = rng.state;
 }
 
+// The learned or fitted vMF mixture as a guiding distribution.
+struct MixDist {
+  const GuideMixture& m;
+  float c;
+  __device__ __forceinline__ float3 sample(Rng& rng) const { return guide_mixture_sample(m, rng); }
+  __device__ __forceinline__ float pdf(float3 x) const { return guide_mixture_pdf(m, x); }
+};
+template <bool MEDIA>
+__device__ __forceinline__ void guide_scatter_mix(const DevScene& sc, const PathState& p, int bounce,
+                                                  const GuidePre& pre, const GuideMixture& mix) {
+  guide_scatter_dist<MEDIA>(sc, p, bounce, pre, MixDist{mix, mix.c});
+}
+
 template <bool MEDIA>
 __device__ __forceinline__ void guide_scatter_one(const DevScene& sc, const PathState& p, int bounce,
                                                   const GuidePre& pre, const float* gout) {
@@ -1541,16 +1556,103 @@ __device__ __forceinline__ int tree_cell(const DevScene& sc, float x, float y, f
   return ref < 0 ? ~ref : 0;
 }
 
-// Tree-guided scattering: the cell's fitted mixture against the BSDF by the same one-sample
-// MIS, the mixture chosen with probability 0.5 (PROB_BSDF, renderingalgorithms_pathtracing_
-// guided.cxx:470).
+// Quadtree distribution of a cell (layout in tt_quadtree.h): hierarchical warping of two
+// uniforms down the tree (quadtree::Sample, path_guiding_quadtree.cxx:178-244, after
+// Clarberg et al. 2005, section 5.1: at every node the column is chosen by the first
+// uniform against the left and right sums of the children's weights and the row by the
+// second against the chosen column's bottom and top weights, each uniform rescaled to the
+// chosen part), then a point uniform in the leaf's square, mapped to the sphere with
+// u = phi / 2 pi + 1/2, v = (z + 1) / 2.  Density per solid angle: leaf weight / (root
+// weight x leaf area) / 4 pi.  At most kQuadMaxDepth levels; the loop stops at 16.
+__device__ __forceinline__ float3 quad_square_to_dir(float u, float v) {
+  const float z = 2.f * v - 1.f;
+  const float rho = sqrtf(fmaxf(0.f, 1.f - z * z));
+  float sn, cs;
+  sincospif(2.f * u - 1.f, &sn, &cs);
+  return f3(rho * cs, rho * sn, z);
+}
+__device__ __forceinline__ float3 quad_sample(const int4* __restrict__ child, const float* __restrict__ prob, int root,
+                                              float u0, float u1, float* pdf) {
+  constexpr float kLt1 = 0.99999994f;  // the largest float below 1
+  constexpr float kEpsF = 1.1920929e-07f;
+  u0 = fminf(u0, kLt1);
+  u1 = fminf(u1, kLt1);
+  float lo0 = 0.f, lo1 = 0.f, hi0 = 1.f, hi1 = 1.f;
+  int node = root;
+  for (int d = 0; d < 16; ++d) {
+    const int4 c = __ldg(&child[node]);
+    if (c.x < 0) break;
+    const float w0 = __ldg(&prob[c.x]), w1 = __ldg(&prob[c.y]), w2 = __ldg(&prob[c.z]), w3 = __ldg(&prob[c.w]);
+    const float wl = w0 + w2, wr = w1 + w3;
+    const float s0 = u0 * (wl + wr);
+    int q = s0 < wl ? 0 : 1;
+    u0 = s0 < wl ? s0 / (wl + kEpsF) : (s0 - wl) / (wr + kEpsF);
+    const float wb = q ? w1 : w0, wt = q ? w3 : w2;
+    const float s1 = u1 * (wb + wt);
+    q |= s1 < wb ? 0 : 2;
+    u1 = s1 < wb ? s1 / (wb + kEpsF) : (s1 - wb) / (wt + kEpsF);
+    u0 = fminf(u0, kLt1);
+    u1 = fminf(u1, kLt1);
+    const float c0 = 0.5f * (lo0 + hi0), c1 = 0.5f * (lo1 + hi1);
+    if (q & 1) lo0 = c0; else hi0 = c0;
+    if (q & 2) lo1 = c1; else hi1 = c1;
+    node = q == 0 ? c.x : (q == 1 ? c.y : (q == 2 ? c.z : c.w));
+  }
+  const float a0 = hi0 - lo0, a1 = hi1 - lo1;
+  *pdf = __ldg(&prob[node]) / (__ldg(&prob[root]) * a0 * a1) * (1.f / (4.f * kPi));
+  const float pu = fmaxf(fminf(a0 * u0 + lo0, hi0 * kLt1), lo0);
+  const float pv = fmaxf(fminf(a1 * u1 + lo1, hi1 * kLt1), lo1);
+  return quad_square_to_dir(pu, pv);
+}
+__device__ __forceinline__ float quad_pdf(const int4* __restrict__ child, const float* __restrict__ prob, int root,
+                                          float3 x) {
+  const float u = (atan2f(x.y, x.x) * (1.f / kPi) + 1.f) * 0.5f, v = (x.z + 1.f) * 0.5f;
+  float lo0 = 0.f, lo1 = 0.f, hi0 = 1.f, hi1 = 1.f;
+  int node = root;
+  for (int d = 0; d < 16; ++d) {
+    const int4 c = __ldg(&child[node]);
+    if (c.x < 0) break;
+    const float c0 = 0.5f * (lo0 + hi0), c1 = 0.5f * (lo1 + hi1);
+    const int q = (u < c0 ? 0 : 1) | (v < c1 ? 0 : 2);
+    if (q & 1) lo0 = c0; else hi0 = c0;
+    if (q & 2) lo1 = c1; else hi1 = c1;
+    node = q == 0 ? c.x : (q == 1 ? c.y : (q == 2 ? c.z : c.w));
+  }
+  return __ldg(&prob[node]) / (__ldg(&prob[root]) * (hi0 - lo0) * (hi1 - lo1)) * (1.f / (4.f * kPi));
+}
+// A cell's quadtree as a guiding distribution (c = 0: not sampled, when the tree carries no
+// weight).
+struct QuadGuide {
+  const int4* child;
+  const float* prob;
+  int root;
+  float c;
+  __device__ __forceinline__ float3 sample(Rng& rng) const {
+    const float u0 = rng.uniform(), u1 = rng.uniform();
+    float pdf;
+    return quad_sample(child, prob, root, u0, u1, &pdf);
+  }
+  __device__ __forceinline__ float pdf(float3 x) const { return quad_pdf(child, prob, root, x); }
+};
+
+// Tree-guided scattering: the cell's fitted distribution (vMF mixture or quadtree) against
+// the BSDF by the same one-sample MIS, the distribution chosen with probability 0.5
+// (PROB_BSDF, renderingalgorithms_pathtracing_guided.cxx:470).
 template <bool MEDIA>
 __global__ void __launch_bounds__(256) k_guide_tree(DevScene sc, PathState p, int bounce) {
   const int n = *guide_count(p, bounce);
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const GuidePre pre = guide_prefetch(p, p.guide_q[i]);
     const float4 a = p.ginp[3 * (size_t)i];
-    const float* cm = sc.tree_mix + 40 * (size_t)tree_cell(sc, a.x, a.y, a.z);
+    const int cell = tree_cell(sc, a.x, a.y, a.z);
+    if (sc.tree_quad) {
+      const int root = __ldg(&sc.tree_qroot[cell]);
+      const float w = __ldg(&sc.tree_qprob[root]);
+      guide_scatter_dist<MEDIA>(sc, p, bounce, pre,
+                                QuadGuide{sc.tree_qchild, sc.tree_qprob, root, (w > 0.f && isfinite(w)) ? 0.5f : 0.f});
+      continue;
+    }
+    const float* cm = sc.tree_mix + 40 * (size_t)cell;
     GuideMixture mix;
 #pragma unroll
     for (int k = 0; k < kGLobes; ++k) {
@@ -2230,6 +2332,23 @@ __global__ void k_resolve(const double* accum, const double* light, const double
     const double inv = inv_spp_px ? inv_spp_px[i / 3] : inv_spp;
     rgb[i] = (float)(accum[i] * inv + splat_weight * light[i]);
   }
+}
+// The tree guider's quadtree sampler on given uniforms (test hook).
+__global__ void k_quadtree_sample(const int4* child, const float* prob, const float* u, int n, float* dir, float* pdf,
+                                  float* pdf_eval) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float pd;
+    const float3 d = quad_sample(child, prob, 0, u[2 * i], u[2 * i + 1], &pd);
+    dir[3 * i] = d.x;
+    dir[3 * i + 1] = d.y;
+    dir[3 * i + 2] = d.z;
+    pdf[i] = pd;
+    pdf_eval[i] = quad_pdf(child, prob, 0, d);
+  }
+}
+void launch_quadtree_sample(const int4* child, const float* prob, const float* u, int n, float* dir, float* pdf,
+                            float* pdf_eval, cudaStream_t st) {
+  if (n > 0) k_quadtree_sample<<<grid_for(n), kBlock, 0, st>>>(child, prob, u, n, dir, pdf, pdf_eval);
 }
 void launch_resolve(const double* accum, const double* light, const double* inv_spp_px, double inv_spp,
                     double splat_weight, int npix, float* rgb, cudaStream_t st) {

@@ -31,6 +31,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "tt_device.cuh"
@@ -320,13 +321,18 @@ int kdtree_build(const float* pts, int n, int min_points, std::vector<TreeNodeHo
 TreeGuide::~TreeGuide() { release(); }
 
 void TreeGuide::release() {
-  for (void* p : {(void*)d_nodes, (void*)d_mix, (void*)d_fit, (void*)d_recs, (void*)d_offsets, (void*)d_copy})
+  for (void* p : {(void*)d_nodes, (void*)d_mix, (void*)d_fit, (void*)d_recs, (void*)d_offsets, (void*)d_copy,
+                  (void*)d_qchild, (void*)d_qprob, (void*)d_qroot})
     if (p) cudaFree(p);
   d_nodes = nullptr;
   d_mix = d_fit = nullptr;
   d_recs = nullptr;
   d_offsets = d_copy = nullptr;
+  d_qchild = nullptr;
+  d_qprob = nullptr;
+  d_qroot = nullptr;
   node_cap = mix_cap = fit_cap = rec_cap = off_cap = copy_cap = 0;
+  qchild_cap = qprob_cap = qroot_cap = 0;
 }
 
 bool TreeGuide::ensure(int cells, int nodes_n, int recs, cudaStream_t st, std::string* err) {
@@ -349,11 +355,14 @@ bool TreeGuide::init(int subdivision_factor, cudaStream_t st, std::string* err) 
   prev_max_samples = subdivision;
   prev_total_samples = 0;
   records_fitted = 0;
+  // Before the first round the single cell's quadtree is one leaf: uniform over the sphere.
+  quads.assign(1, QuadDist{});
+  frames.assign(1, std::array<double, 9>{1, 0, 0, 0, 1, 0, 0, 0, 1});
   if (upload_prior() != cudaSuccess) {
     *err = "tree guider: constant upload failed";
     return false;
   }
-  if (!ensure(1, 1, 1, st, err)) return false;
+  if (!ensure(1, 1, 1, st, err) || !upload_quads(st, err)) return false;
   std::vector<float> mix(kTreeMixFloats), fit(kTreeFitFloats, 0.f);
   tree_prior_mixture(mix.data());
   cudaMemcpyAsync(d_mix, mix.data(), mix.size() * sizeof(float), cudaMemcpyHostToDevice, st);
@@ -418,15 +427,21 @@ bool TreeGuide::fit_round(const GuideRecord* recs, int n, uint64_t seed, cudaStr
     sorted[i] = make_float4(r.wi[0], r.wi[1], r.wi[2], r.f_over_q);
   }
   if (!ensure(ncells, (int)nodes.size(), n, st, err)) return false;
-  if (initial) {
+  const bool quad = distribution == TT_TREE_QUADTREE;
+  if (quad) fit_quads(recs, cell_of, initial, seed);
+  if (quad) {
+    // The vMF state is not used.
+  } else if (initial) {
     std::vector<float> mix((size_t)ncells * kTreeMixFloats), fit((size_t)ncells * kTreeFitFloats, 0.f);
     for (int c = 0; c < ncells; ++c) tree_prior_mixture(&mix[(size_t)c * kTreeMixFloats]);
     cudaMemcpyAsync(d_mix, mix.data(), mix.size() * sizeof(float), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(d_fit, fit.data(), fit.size() * sizeof(float), cudaMemcpyHostToDevice, st);
   }
-  cudaMemcpyAsync(d_recs, sorted.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(d_offsets, offsets.data(), offsets.size() * sizeof(int), cudaMemcpyHostToDevice, st);
-  launch_tree_fit(d_recs, d_offsets, d_mix, d_fit, ncells, em_iters, st);
+  if (!quad) {
+    cudaMemcpyAsync(d_recs, sorted.data(), (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_offsets, offsets.data(), offsets.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    launch_tree_fit(d_recs, d_offsets, d_mix, d_fit, ncells, em_iters, st);
+  }
   if (!initial) {
     // AdaptIncremental: split cells that received too many records this round.
     const double max_per_cell = std::sqrt((double)n) * prev_max_samples / std::sqrt(std::max(1.0, prev_total_samples));
@@ -459,10 +474,15 @@ bool TreeGuide::fit_round(const GuideRecord* recs, int n, uint64_t seed, cudaStr
       cell_depth.push_back(cell_depth[c]);
       pairs.push_back(nc);
       pairs.push_back(c);
+      if (quad) {
+        // Both halves start from the cell's distribution (AdaptIncremental's CopyCell).
+        quads.push_back(quads[c]);
+        frames.push_back(frames[c]);
+      }
     }
     prev_max_samples = max_per_cell;
     prev_total_samples = n;
-    if (!pairs.empty()) {
+    if (!pairs.empty() && !quad) {
       if (!ensure(ncells, (int)nodes.size(), n, st, err)) return false;
       cudaMemcpyAsync(d_copy, pairs.data(), pairs.size() * sizeof(int), cudaMemcpyHostToDevice, st);
       k_tree_copy<<<(int)pairs.size() / 2, 64, 0, st>>>(d_copy, (int)pairs.size() / 2, d_mix, d_fit);
@@ -476,7 +496,9 @@ bool TreeGuide::fit_round(const GuideRecord* recs, int n, uint64_t seed, cudaStr
   };
   for (size_t i = 0; i < nodes.size(); ++i)
     dn[i] = make_float4(nodes[i].split, bits(nodes[i].axis), bits(nodes[i].child[0]), bits(nodes[i].child[1]));
+  if (!grow(&d_nodes, &node_cap, (int)dn.size(), st, false, err)) return false;
   cudaMemcpyAsync(d_nodes, dn.data(), dn.size() * sizeof(float4), cudaMemcpyHostToDevice, st);
+  if (quad && !upload_quads(st, err)) return false;
   // The host vectors above are pageable: wait for the copies before they go out of scope.
   const cudaError_t e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
@@ -485,6 +507,134 @@ bool TreeGuide::fit_round(const GuideRecord* recs, int n, uint64_t seed, cudaStr
   }
   ++round;
   records_fitted += n;
+  return true;
+}
+
+// The quadtree distributions of one round.  First round (AdaptInitial, path_guiding.cxx:
+// 623-674): every cell's tree from its records (InitialFit + Bake) and the stochastic
+// filter's frame from their positions.  Later rounds: FitTheSamples (:433-475) with the
+// stochastic filter, whose copies of the records (jittered by the cells' current frames
+// and trees, looked up again) are the ones the quadtrees fit (IncrementalFit skips the
+// originals); then, as AdaptIncremental (:676-790) does per cell, IterationUpdateAndBake
+// and a new frame from the round's positions when the cell received at least 10 records.
+// Deviation: the reference adapts after each sweep of passes; here every round adapts.
+// Runs f(begin, end) over [0, n) in contiguous chunks on the host's threads.
+template <class F>
+static void host_parallel(int n, F&& f) {
+  const int nt = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), (n + 255) / 256));
+  if (nt <= 1) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; ++t) {
+    const int b = (int)((long long)n * t / nt), e = (int)((long long)n * (t + 1) / nt);
+    th.emplace_back([&f, b, e] { f(b, e); });
+  }
+  for (auto& x : th) x.join();
+}
+
+void TreeGuide::fit_quads(const GuideRecord* recs, const std::vector<int>& cell_of, bool initial, uint64_t seed) {
+  const int n = (int)cell_of.size();
+  if (initial) {
+    quads.assign(ncells, QuadDist{});
+    frames.assign(ncells, std::array<double, 9>{1, 0, 0, 0, 1, 0, 0, 0, 1});
+  }
+  // The records the quadtrees fit: the originals in the first round, the stochastic
+  // filter's copies (moved to the cell of their jittered position) later.  The filter's
+  // uniforms are drawn in record order, so the result does not depend on the threading.
+  std::vector<float> uv(2 * (size_t)n);
+  std::vector<int> fit_cell(n);
+  if (initial) {
+    host_parallel(n, [&](int b, int e) {
+      for (int i = b; i < e; ++i) {
+        dir_to_square(recs[i].wi, &uv[2 * (size_t)i]);
+        fit_cell[i] = cell_of[i];
+      }
+    });
+  } else {
+    std::mt19937_64 rng(seed * 0x9e3779b97f4a7c15ull + 0xd1b54a32d192ed03ull * (uint64_t)(round + 1));
+    std::uniform_real_distribution<double> uni(0.0, 1.0);
+    std::vector<double> rr(5 * (size_t)n);
+    for (double& x : rr) x = uni(rng);
+    host_parallel(n, [&](int b, int e) {
+      for (int i = b; i < e; ++i) {
+        const int c = cell_of[i];
+        float p2[3], d2[3];
+        filter_record(quads[c], frames[c].data(), &rr[5 * (size_t)i], recs[i].pos, recs[i].wi, p2, d2);
+        fit_cell[i] = lookup(p2[0], p2[1], p2[2]);
+        dir_to_square(d2, &uv[2 * (size_t)i]);
+      }
+    });
+  }
+  // Records of every cell, in record order.
+  std::vector<int> off(ncells + 1, 0);
+  for (int c : fit_cell) off[c + 1]++;
+  for (int c = 0; c < ncells; ++c) off[c + 1] += off[c];
+  std::vector<int> fill(off.begin(), off.end() - 1), idx(n);
+  for (int i = 0; i < n; ++i) idx[fill[fit_cell[i]]++] = i;
+  std::vector<int> pos_off(ncells + 1, 0);
+  for (int c : cell_of) pos_off[c + 1]++;
+  for (int c = 0; c < ncells; ++c) pos_off[c + 1] += pos_off[c];
+  std::vector<int> pfill(pos_off.begin(), pos_off.end() - 1), pidx(n);
+  for (int i = 0; i < n; ++i) pidx[pfill[cell_of[i]]++] = i;
+  host_parallel(ncells, [&](int c0, int c1) {
+    std::vector<float> cu, cw;
+    for (int c = c0; c < c1; ++c) {
+      cu.clear();
+      cw.clear();
+      for (int k = off[c]; k < off[c + 1]; ++k) {
+        const int i = idx[k];
+        cu.push_back(uv[2 * (size_t)i]);
+        cu.push_back(uv[2 * (size_t)i + 1]);
+        cw.push_back(recs[i].f_over_q);
+      }
+      PointCov ps;
+      for (int k = pos_off[c]; k < pos_off[c + 1]; ++k) ps.add(recs[pidx[k]].pos);
+      const int m = (int)cw.size();
+      if (initial) {
+        quads[c].initial_fit(cu.data(), cw.data(), m);
+        quads[c].bake();
+        ps.frame(frames[c].data());
+      } else {
+        quads[c].incremental_fit(cu.data(), cw.data(), m, 1);
+        quads[c].update_and_bake();
+        if (ps.n >= 10.0) ps.frame(frames[c].data());
+      }
+    }
+  });
+}
+
+bool TreeGuide::upload_quads(cudaStream_t st, std::string* err) {
+  std::vector<int> roots(std::max(1, ncells));
+  int total = 0;
+  for (int c = 0; c < ncells; ++c) {
+    roots[c] = total;
+    total += quads[c].num_nodes();
+  }
+  std::vector<int4> ch(std::max(1, total));
+  std::vector<float> pr(std::max(1, total));
+  for (int c = 0; c < ncells; ++c) {
+    const QuadDist& q = quads[c];
+    for (int j = 0; j < q.num_nodes(); ++j) {
+      const auto& k = q.child[j];
+      ch[roots[c] + j] = k[0] < 0 ? make_int4(-1, -1, -1, -1)
+                                  : make_int4(roots[c] + k[0], roots[c] + k[1], roots[c] + k[2], roots[c] + k[3]);
+      pr[roots[c] + j] = q.probs[j];
+    }
+  }
+  if (!grow(&d_qchild, &qchild_cap, (int)ch.size(), st, false, err) ||
+      !grow(&d_qprob, &qprob_cap, (int)pr.size(), st, false, err) ||
+      !grow(&d_qroot, &qroot_cap, (int)roots.size(), st, false, err))
+    return false;
+  cudaMemcpyAsync(d_qchild, ch.data(), ch.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_qprob, pr.data(), pr.size() * sizeof(float), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(d_qroot, roots.data(), roots.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+  const cudaError_t e = cudaStreamSynchronize(st);  // the host vectors are local
+  if (e != cudaSuccess) {
+    *err = std::string("tree guider: ") + cudaGetErrorString(e);
+    return false;
+  }
   return true;
 }
 

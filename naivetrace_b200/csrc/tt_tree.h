@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "tt_internal.h"
+#include "tt_quadtree.h"
 
 namespace tt {
 
@@ -33,6 +34,7 @@ class TreeGuide {
  public:
   int subdivision = 100;   // guiding_tree_subdivision_factor (scene.hxx:39)
   int em_iters = 0;        // 0: the reference's incremental EM; k > 0: k batch EM iterations per round
+  int distribution = 0;    // TT_TREE_VMF or TT_TREE_QUADTREE
   int round = 0;           // fitted rounds
   int ncells = 1;
   std::vector<TreeNodeHost> nodes;        // empty: the root is leaf cell 0
@@ -41,8 +43,17 @@ class TreeGuide {
   std::vector<int> cell_side{0};
   double prev_max_samples = 100.0, prev_total_samples = 0.0;
   long long records_fitted = 0;
+  // Quadtree distribution: per cell its quadtree (learned statistics and sampling weights),
+  // the positions of the round's records and the stochastic filter's frame.
+  std::vector<QuadDist> quads;
+  std::vector<PointCov> pstats;
+  std::vector<std::array<double, 9>> frames;
   // Device state.
   float4* d_nodes = nullptr;   // split, axis, child0, child1 (int bits)
+  int4* d_qchild = nullptr;    // quadtree nodes of all cells (absolute child indices, -1: leaf)
+  float* d_qprob = nullptr;    // their sampling weights
+  int* d_qroot = nullptr;      // root node of every cell
+  int qchild_cap = 0, qprob_cap = 0, qroot_cap = 0;
   float* d_mix = nullptr;      // ncells x kTreeMixFloats
   float* d_fit = nullptr;      // ncells x kTreeFitFloats
   float4* d_recs = nullptr;    // records of a round sorted by cell: direction xyz, weight
@@ -62,6 +73,8 @@ class TreeGuide {
 
  private:
   bool ensure(int cells, int nodes_n, int recs, cudaStream_t st, std::string* err);
+  bool upload_quads(cudaStream_t st, std::string* err);
+  void fit_quads(const GuideRecord* recs, const std::vector<int>& cell_of, bool initial, uint64_t seed);
   int build(std::vector<int>& idx, int lo, int hi, int depth, const GuideRecord* recs, std::vector<int>& cell_of,
             int parent, int side);
 };

@@ -50,7 +50,7 @@ def test_struct_layout_matches_header(tmp_path):
 
 
 def test_abi_version(gpu_lib):
-    assert gpu_lib.tt_abi_version() == 8
+    assert gpu_lib.tt_abi_version() == 9
 
 
 def _create(lib, scene, params):

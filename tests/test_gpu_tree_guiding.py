@@ -19,7 +19,7 @@ from naivetrace_b200.scene import make_params
 from oracle import guiding as G
 from oracle import tree_guiding as T
 from oracle.oracle import combine
-from test_gpu_guiding import tile_means
+from test_gpu_guiding import assert_tiles_agree, tile_means
 
 pytestmark = pytest.mark.gpu
 
@@ -93,8 +93,8 @@ def _batches(ctx, K, spp, seed0, xres, yres, tile):
 @pytest.mark.parametrize("name,train_during,em_iters", [("cornell_box", True, 4), ("cornell_box_medium", False, 4),
                                                         ("guiding_room", True, 0), ("guiding_room", False, 4)])
 def test_tree_guided_render_unbiased(gpu_lib, name, train_during, em_iters):
-    """Tile means of tree-guided and plain renders: at least 93 % of the tile-channels within
-    3 sigma and all within 4.5 sigma (as for the learned guider)."""
+    """Tile means of tree-guided and plain renders agree within the Bonferroni bound of
+    assert_tiles_agree (as for the learned guider)."""
     xres, yres, tile = (64, 64, 16) if name != "guiding_room" else (96, 54, 18)
     scene = getattr(scenes, name)(xres, yres)
     p = make_params(max_ray_depth=10 if name != "guiding_room" else 12)
@@ -108,15 +108,12 @@ def test_tree_guided_render_unbiased(gpu_lib, name, train_during, em_iters):
     assert rounds_before == 6
     if not train_during:
         guided.set_guiding(True, 0, **kw)
-    K = 16
+    K = 32  # batches per side: the room's batch means are skewed, and 16 left the t tails too light
     spp = 16 if name != "guiding_room" else 64
     tp = _batches(plain, K, spp, 100, xres, yres, tile)
     tg = _batches(guided, K, spp, 300, xres, yres, tile)
     assert (guided.tree_info()["rounds"] > rounds_before) == train_during
-    se = np.sqrt(tp.var(0, ddof=1) / K + tg.var(0, ddof=1) / K)
-    z = np.abs(tg.mean(0) - tp.mean(0)) / np.maximum(se, 1e-12)
-    assert (z < 3.0).mean() >= 0.93, ((z < 3.0).mean(), z.max())
-    assert np.all(z < 4.5), z.max()
+    assert_tiles_agree(tp, tg)
     assert guided.stats()["error_flags"] == 0
 
 
@@ -154,3 +151,107 @@ def test_tree_guiding_gain(gpu_lib):
         e_tree.append(relmse(g))
     gain = np.mean(e_plain) / np.mean(e_tree)
     assert gain > 1.25, (e_plain, e_tree)
+
+
+# ---- Quadtree distribution (tree_distribution = TREE_QUADTREE) -------------------------
+
+def _quad_fixture(seed=21, n=4000):
+    rng = np.random.default_rng(seed)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    m = n // 2
+    d[:m] = d[:m] * 0.1 + np.array([0.5, 0.5, 0.7])
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    w = rng.exponential(1.0, n).astype(np.float32)
+    from naivetrace_b200.algo import quadtree_fit_batch
+    ch, wt, _ = quadtree_fit_batch(d.astype(np.float32), w, d[::3].astype(np.float32), w[::3], stage=2)
+    return ch, wt
+
+
+def test_quadtree_device_sampler_matches_oracle(gpu_lib):
+    """The tree-guided kernel's quadtree sampler (hierarchical warping in float32) against
+    the oracle's on the same uniforms: the same leaf and point, directions within float
+    rounding, densities equal; the density evaluated at the returned direction equals the
+    sampled one except where the direction sits on a leaf boundary."""
+    from naivetrace_b200.algo import quadtree_sample_batch
+    ch, wt = _quad_fixture()
+    rng = np.random.default_rng(5)
+    u = rng.random((20000, 2)).astype(np.float32)
+    d, pdf, pdf_eval = quadtree_sample_batch(ch, wt, u)
+    pts, pdo = [], []
+    for u0, u1 in u:
+        (pu, pv), pd, _ = T.quad_sample(ch.tolist(), wt, u0, u1)
+        pts.append((pu, pv))
+        pdo.append(float(pd) / (4 * np.pi))
+    do = T.square_to_dir(np.array(pts, np.float32))
+    np.testing.assert_allclose(d, do, atol=2e-6)
+    np.testing.assert_allclose(pdf, pdo, rtol=2e-6)
+    assert np.mean(np.isclose(pdf_eval, pdf, rtol=1e-5)) >= 0.999
+    np.testing.assert_allclose(pdf, T.quad_pdf(ch.tolist(), wt, d), rtol=1e-4)
+
+
+def test_quadtree_device_chi_square(gpu_lib):
+    """2^20 device samples binned by the leaves of the tree: chi-square against the leaf
+    weights, p >= 0.01 (the quadtree sampling check of the reference's sampling tests)."""
+    from scipy import stats
+    from naivetrace_b200.algo import quadtree_sample_batch
+    ch, wt = _quad_fixture(seed=31)
+    n = 1 << 20
+    u = np.random.default_rng(6).random((n, 2)).astype(np.float32)
+    d, _, _ = quadtree_sample_batch(ch, wt, u)
+    child = ch.tolist()
+    leaves = [k for k in range(len(child)) if child[k][0] < 0]
+    index = {k: i for i, k in enumerate(leaves)}
+    uv = T.dir_to_square(d)
+    counts = np.zeros(len(leaves))
+    for p in uv:
+        counts[index[T.quad_leaf(child, p)[0]]] += 1
+    exp = wt[leaves].astype(np.float64) / float(wt[0]) * n
+    keep = exp > 5
+    e = exp[keep] * counts[keep].sum() / exp[keep].sum()
+    assert stats.chisquare(counts[keep], e).pvalue >= 0.01
+
+
+def test_quadtree_rounds_and_cells(gpu_lib):
+    """Training rounds with quadtrees: cells multiply, every cell's tree is well formed
+    (children after parents, inner weights the sums of their children, positive root)."""
+    scene = scenes.guiding_room(96, 54)
+    g = GpuContext(scene, make_params(max_ray_depth=12))
+    g.set_guiding(True, 1, method=abi.GUIDE_TREE, tree_subdivision=100, seed=3,
+                  tree_distribution=abi.TREE_QUADTREE)
+    for k in range(4):
+        g.render(8, seed=1 + k)
+    info = g.tree_info()
+    assert info["rounds"] == 4 and info["cells"] > 1
+    for c in range(info["cells"]):
+        ch, w = g.tree_quadtree(c)
+        assert len(ch) >= 1 and w[0] > 0 and np.all(np.isfinite(w))
+        for k in range(len(ch)):
+            if ch[k, 0] >= 0:
+                assert np.all(ch[k] > k) and np.all(ch[k] < len(ch))
+                assert w[k] == pytest.approx(float(w[ch[k]].astype(np.float64).sum()), rel=1e-5)
+    assert g.stats()["error_flags"] == 0
+
+
+@pytest.mark.parametrize("name,train_during", [("cornell_box", True), ("guiding_room", False),
+                                               ("cornell_box_medium", False)])
+def test_quadtree_guided_render_unbiased(gpu_lib, name, train_during):
+    """Quadtree-guided against plain renders: tile means within the Bonferroni bound of
+    assert_tiles_agree, with the trees trained between the passes or frozen."""
+    xres, yres, tile = (64, 64, 16) if name != "guiding_room" else (96, 54, 18)
+    scene = getattr(scenes, name)(xres, yres)
+    p = make_params(max_ray_depth=10 if name != "guiding_room" else 12)
+    plain = GpuContext(scene, p)
+    guided = GpuContext(scene, p)
+    kw = dict(method=abi.GUIDE_TREE, tree_subdivision=100, seed=5, tree_distribution=abi.TREE_QUADTREE)
+    guided.set_guiding(True, 1, **kw)
+    for k in range(6):
+        guided.render(4, seed=900 + k)
+    if not train_during:
+        guided.set_guiding(True, 0, **kw)
+    K = 32  # batches per side: the room's batch means are skewed, and 16 left the t tails too light
+    spp = 16 if name != "guiding_room" else 64
+    tp = _batches(plain, K, spp, 100, xres, yres, tile)
+    tg = _batches(guided, K, spp, 300, xres, yres, tile)
+    assert_tiles_agree(tp, tg)
+    assert guided.stats()["error_flags"] == 0
