@@ -264,7 +264,11 @@ tt_status tt_last_wave_queue_lengths(tt_ctx* ctx, int32_t* out, int32_t n);
 int32_t tt_abi_version(void);
 
 /* RenderAlgorithmFactory + constructor (renderingalgorithms.cxx:27-42): validates and deep
- * copies the scene description; allocates nothing on the GPU yet. */
+ * copies the scene description; allocates nothing on the GPU yet.  The large arrays of the
+ * copy (vertices, normals, indices, materials per triangle, texture coordinates, environment
+ * maps) live in page-locked host memory from a process-wide pool (blocks of 1 MiB and more;
+ * reused by later contexts after tt_destroy, up to 4 GiB kept; ordinary memory when the
+ * CUDA runtime cannot pin), so that tt_upload_scene copies them by DMA. */
 tt_status tt_create(const tt_scene_desc* scene, const tt_params* params, tt_ctx** out_ctx);
 
 /* RenderingAlgo::InitializeScene + Scene::BuildAccelStructure (scene.cxx:116-141): builds

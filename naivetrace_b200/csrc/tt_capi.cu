@@ -6,15 +6,18 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
-#include <cstdio>
-#include <cstring>
 #include <cstddef>
+#include <cstdio>
 #include <cstdlib>
+#include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <new>
 #include <numeric>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/toytrace_gpu.h"
@@ -42,8 +45,82 @@ constexpr int kDefaultWave = 1 << 26;
 std::mutex g_err_mutex;
 std::string g_create_error;
 
-// Allocator that leaves new elements uninitialised, so that the scene copies of tt_create
-// touch their pages once, from the threads that fill them.
+// Page-locked host memory for the contexts' scene copies, kept for reuse by later
+// contexts (as the device memory pool keeps device buffers): the copies of tt_create then
+// write into memory that is already mapped, and tt_upload_scene's host-to-device copies run
+// as DMA from it instead of through pageable staging.  Blocks of 1 MiB and more are pinned
+// (cudaHostAlloc, portable to every device), in multiples of 1 MiB; a freed block is kept
+// while the pool holds at most kHostPoolKeep bytes, else released.  Smaller blocks, and all
+// blocks once a pinned allocation has failed (no GPU, no driver), come from malloc.  The pool
+// is never destroyed: blocks still cached at exit go with the process.
+class HostPool {
+ public:
+  static HostPool& get() {
+    static HostPool* pool = new HostPool;
+    return *pool;
+  }
+  void* alloc(size_t bytes) {
+    constexpr size_t kMiB = 1 << 20;
+    if (bytes >= kMiB) {
+      const size_t rounded = (bytes + kMiB - 1) / kMiB * kMiB;
+      std::lock_guard<std::mutex> g(mu_);
+      auto it = free_.lower_bound(rounded);
+      if (it != free_.end() && it->first <= 2 * rounded) {
+        void* p = it->second;
+        kept_ -= it->first;
+        live_[p] = Block{it->first, true};
+        free_.erase(it);
+        return p;
+      }
+      if (pinned_ok_) {
+        void* p = nullptr;
+        if (cudaHostAlloc(&p, rounded, cudaHostAllocPortable) == cudaSuccess && p) {
+          live_[p] = Block{rounded, true};
+          return p;
+        }
+        cudaGetLastError();  // clear the failed call's error
+        pinned_ok_ = false;
+      }
+    }
+    void* p = std::malloc(bytes > 0 ? bytes : 1);
+    if (!p) throw std::bad_alloc();
+    std::lock_guard<std::mutex> g(mu_);
+    live_[p] = Block{bytes, false};
+    return p;
+  }
+  void release(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = live_.find(p);
+    if (it == live_.end()) return;
+    const Block b = it->second;
+    live_.erase(it);
+    if (!b.pinned) {
+      std::free(p);
+    } else if (kept_ + b.bytes <= kHostPoolKeep) {
+      free_.emplace(b.bytes, p);
+      kept_ += b.bytes;
+    } else {
+      cudaFreeHost(p);
+    }
+  }
+
+ private:
+  static constexpr size_t kHostPoolKeep = size_t(4) << 30;
+  struct Block {
+    size_t bytes;
+    bool pinned;
+  };
+  std::mutex mu_;
+  std::multimap<size_t, void*> free_;
+  std::unordered_map<void*, Block> live_;
+  size_t kept_ = 0;
+  bool pinned_ok_ = true;
+};
+
+// Allocator of the scene copies: memory from the host pool, new elements left
+// uninitialised, so that the copies of tt_create touch their pages once, from the threads
+// that fill them.
 template <class T>
 struct NoInitAlloc : std::allocator<T> {
   template <class U>
@@ -53,6 +130,8 @@ struct NoInitAlloc : std::allocator<T> {
   NoInitAlloc() = default;
   template <class U>
   NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+  T* allocate(size_t n) { return static_cast<T*>(HostPool::get().alloc(n * sizeof(T))); }
+  void deallocate(T* p, size_t) noexcept { HostPool::get().release(p); }
   template <class U>
   void construct(U* p) noexcept {
     ::new (static_cast<void*>(p)) U;
@@ -62,6 +141,14 @@ struct NoInitAlloc : std::allocator<T> {
     ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
   }
 };
+template <class T, class U>
+bool operator==(const NoInitAlloc<T>&, const NoInitAlloc<U>&) noexcept {
+  return true;
+}
+template <class T, class U>
+bool operator!=(const NoInitAlloc<T>&, const NoInitAlloc<U>&) noexcept {
+  return false;
+}
 template <class T>
 using HostArray = std::vector<T, NoInitAlloc<T>>;
 
