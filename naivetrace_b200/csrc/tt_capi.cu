@@ -155,6 +155,7 @@ using HostArray = std::vector<T, NoInitAlloc<T>>;
 struct HostEnv {
   tt_env_light desc;
   HostArray<float> tex;
+  HostArray<float> cmf_rows, cmf_cols;  // made at upload; kept until tt_destroy (DMA sources)
 };
 
 // Device buffers owned by a context, from the library's memory pool, ordered on `stream`.
@@ -307,9 +308,9 @@ struct tt_ctx {
 
 // Runs f(lo, hi) over [0, n) split among up to 16 host threads (serially below 4096).
 template <class F>
-static void parallel_ranges(long long n, F&& f) {
+static void parallel_ranges(long long n, F&& f, long long serial_below = 4096) {
   const long long nt = std::min<long long>(16, std::max(1u, std::thread::hardware_concurrency()));
-  if (n < 4096 || nt <= 1) {
+  if (n < serial_below || nt <= 1) {
     f(0, n);
     return;
   }
@@ -707,15 +708,18 @@ tt_status tt_upload_scene(tt_ctx* c) {
   std::vector<uint32_t> sidx, smat, sid, vidx, vmat, vid;
   bool any_vol = false;
   for (const auto& m : c->materials) any_vol |= m.volume_boundary != 0;
-  if (!any_vol) {
-    sid.resize(ntri);
-    std::iota(sid.begin(), sid.end(), 0u);
-  } else {
+  // Without medium boundaries every triangle is a surface and the surface ids are the
+  // identity: the device build writes them itself, the host builders get them listed.
+  if (any_vol)
     for (uint32_t t = 0; t < ntri; ++t) (c->materials[c->mats[t]].volume_boundary ? vid : sid).push_back(t);
-  }
+  const size_t nsurf = any_vol ? sid.size() : ntri;
   // Index and material lists per BVH for the host builders (the device builder reads the
   // mesh as uploaded, with the prim-id sets above).
   auto host_split = [&]() {
+    if (!any_vol) {
+      sid.resize(ntri);
+      std::iota(sid.begin(), sid.end(), 0u);
+    }
     for (uint32_t t : sid) {
       sidx.insert(sidx.end(), &c->idx[3 * (size_t)t], &c->idx[3 * (size_t)t] + 3);
       smat.push_back(c->mats[t]);
@@ -789,7 +793,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     };
     // Prim-id sets: the triangle ids, then the sphere ids (generated on the device when the
     // surface set is every triangle).
-    const size_t ns = sid.size() + ssid.size(), nv = vid.size() + vsid.size();
+    const size_t ns = nsurf + ssid.size(), nv = vid.size() + vsid.size();
     uint32_t* d_sset = (uint32_t*)tmp.alloc(ns * sizeof(uint32_t));
     uint32_t* d_vset = (uint32_t*)tmp.alloc(nv * sizeof(uint32_t));
     if (d_sset) {
@@ -799,7 +803,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
         cudaMemcpyAsync(d_sset, sid.data(), sid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream);
       }
       if (!ssid.empty())
-        cudaMemcpyAsync(d_sset + sid.size(), ssid.data(), ssid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+        cudaMemcpyAsync(d_sset + nsurf, ssid.data(), ssid.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
                         c->stream);
     }
     if (d_vset) {
@@ -891,7 +895,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
   }
   mark("bvh");
   s.normals = c->normals.empty() ? nullptr : (const float*)upload(c->normals.data(), c->normals.size() * sizeof(float));
-  s.num_tris = (int)(sid.size() + ssid.size());
+  s.num_tris = (int)(nsurf + ssid.size());
   // Materials.
   std::vector<DevMaterial> dm(c->materials.size());
   for (size_t i = 0; i < dm.size(); ++i) {
@@ -1041,7 +1045,10 @@ tt_status tt_upload_scene(tt_ctx* c) {
       for (int k = 0; k < 3; ++k) { L.X[k] = X[k]; L.Y[k] = Y[k]; L.Z[k] = up[k]; }
       const int w = e.tex_width, h = e.tex_height;
       const auto& tex = c->envs[i].tex;
-      std::vector<float> rows(h), cols((size_t)w * h);
+      HostArray<float>& rows = c->envs[i].cmf_rows;
+      HostArray<float>& cols = c->envs[i].cmf_cols;
+      rows.resize(h);
+      cols.resize((size_t)w * h);
       std::atomic<bool> zero_row{false};
       parallel_ranges(h, [&](long long y0, long long y1) {
         for (long long y = y0; y < y1; ++y) {
@@ -1058,7 +1065,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
           for (int x = 0; x < w; ++x) cols[(size_t)y * w + x] /= (float)row_weight;
           rows[y] = (float)row_weight;
         }
-      });
+      }, /*serial_below=*/64);  // rows of a few thousand texels each
       if (zero_row) return fail(c, TT_ERR_INVALID, "env map row with zero weight");
       for (int y = 1; y < h; ++y) rows[y] += rows[y - 1];
       const float inv = 1.f / rows[h - 1];
@@ -1070,6 +1077,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
       L.cmf_cols = (const float*)upload(cols.data(), cols.size() * sizeof(float));
     }
   }
+  mark("env maps");
   // Camera (camera.hxx:38-108, 159-175), computed in double.
   s.cam = make_dev_camera(c->camera);
   // Light picker (TrivialLightPicker, lightpicker_trivial.cxx:11-31) and scene bounds.
@@ -1110,6 +1118,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     s.box_lo[k] = (float)lo[k];
     s.box_inv[k] = hi[k] > lo[k] ? (float)(1.0 / (hi[k] - lo[k])) : 1.f;
   }
+  mark("bounds");
   s.long_distance = (float)(10. * diag);
   s.max_path_nodes = c->params.max_ray_depth + 1;
   s.algo = c->params.algo;
@@ -1133,6 +1142,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
     sort = __builtin_popcount(kinds) >= 3;
   }
   s.sort_shading = (sort && c->params.algo == TT_ALGO_PT) ? 1 : 0;
+  mark("sort keys");
   // Quasi-random sampling: pt2 only, as in the reference (CameraRenderWorker's sampler).
   s.sobol = nullptr;
   s.rotations = nullptr;
