@@ -554,15 +554,17 @@ typedef struct tt_tune_result {
   int32_t candidate_grid[TT_TUNE_MAX];
   double candidate_ms[TT_TUNE_MAX];
   int32_t block;                /* chosen threads per block of the wavefront launches */
-  int32_t bvh_width;            /* chosen BVH layout: 2 (binary) or 8 (8-wide compressed) */
+  int32_t bvh_width;            /* chosen BVH layout: 4 (the device-built tree with four children
+                                   per node, the default), 2 (binary: host-built trees) or 8
+                                   (8-wide compressed) */
   int32_t candidate_block[TT_TUNE_MAX];
   int32_t candidate_width[TT_TUNE_MAX];
 } tt_tune_result;
 
 /* Autotuner: times one-sample probes of the batch over queue capacities (2^22, 2^24, 2^25,
  * 2^26 paths per wave) and launch widths (0.5, 1, 2 x the occupancy grid) with 256-thread
- * blocks on the binary BVH; then, at the best of those, 128-thread blocks (twice the grid)
- * and the 8-wide compressed BVH (built on the host on first use, kept next to the binary
+ * blocks on the default BVH layout; then, at the best of those, 128-thread blocks (twice the grid)
+ * and the 8-wide compressed BVH (built on the host on first use, kept next to the default
  * one); and keeps the fastest configuration for this context's later passes. */
 tt_status tt_autotune_views(tt_ctx* ctx, const tt_view* views, int32_t n, tt_tune_result* out);
 

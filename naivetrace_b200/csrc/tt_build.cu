@@ -305,6 +305,70 @@ __global__ void k_write_nodes(int first, int count, uint32_t n, const Aabb* node
   }
 }
 
+// 4-wide layout: a node for every emitted binary node at even depth (root depth 0), its
+// slots the children of its binary children that are inner nodes and those binary children
+// that are leaves; numbered in depth-first order by a scan over the binary depth-first
+// numbering.
+__global__ void k_flag4(int total, uint32_t n, const unsigned char* emit, const int* depth, const int* index,
+                        int* flag_dfs) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
+    if (k >= (int)n && emit[k]) flag_dfs[index[k]] = (depth[k] & 1) == 0 ? 1 : 0;
+}
+__global__ void k_write_nodes4(int first, int count, uint32_t n, const Aabb* node_box, const int* left,
+                               const int* right, const int* size, const int* offset, const unsigned char* emit,
+                               const int* depth, const int* index, const int* index4, float4* nodes4) {
+  constexpr int kEmpty = 0x7fffffff;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
+    const int k = first + t;
+    if (!emit[k] || (depth[k] & 1)) continue;
+    Aabb box[4];
+    int ref[4];
+    int m = 0;
+    const int kids[2] = {left[k], right[k]};
+    for (int s = 0; s < 2; ++s) {
+      const int c = kids[s];
+      if (c >= (int)n && emit[c]) {
+        const int g[2] = {left[c], right[c]};
+        for (int u = 0; u < 2; ++u) {
+          box[m] = node_box[g[u]];
+          ref[m++] = (g[u] >= (int)n && emit[g[u]]) ? index4[index[g[u]]] : child_ref(g[u], n, size, offset, emit, index);
+        }
+      } else {
+        box[m] = node_box[c];
+        ref[m++] = child_ref(c, n, size, offset, emit, index);
+      }
+    }
+    for (; m < 4; ++m) {
+      box[m] = Aabb{make_float3(INFINITY, INFINITY, INFINITY), make_float3(-INFINITY, -INFINITY, -INFINITY)};
+      ref[m] = kEmpty;
+    }
+    float4* d = nodes4 + 8 * (size_t)index4[index[k]];
+    d[0] = make_float4(box[0].lo.x, box[1].lo.x, box[2].lo.x, box[3].lo.x);
+    d[1] = make_float4(box[0].hi.x, box[1].hi.x, box[2].hi.x, box[3].hi.x);
+    d[2] = make_float4(box[0].lo.y, box[1].lo.y, box[2].lo.y, box[3].lo.y);
+    d[3] = make_float4(box[0].hi.y, box[1].hi.y, box[2].hi.y, box[3].hi.y);
+    d[4] = make_float4(box[0].lo.z, box[1].lo.z, box[2].lo.z, box[3].lo.z);
+    d[5] = make_float4(box[0].hi.z, box[1].hi.z, box[2].hi.z, box[3].hi.z);
+    d[6] = make_float4(__int_as_float(ref[0]), __int_as_float(ref[1]), __int_as_float(ref[2]), __int_as_float(ref[3]));
+    d[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+// 4-wide root of a tree whose root is a leaf: one slot with the leaf.
+__global__ void k_leaf_root4(const Aabb* node_box, int root, int count, float4* nodes4) {
+  const Aabb a = node_box[root];
+  const float inf = INFINITY;
+  nodes4[0] = make_float4(a.lo.x, inf, inf, inf);
+  nodes4[1] = make_float4(a.hi.x, -inf, -inf, -inf);
+  nodes4[2] = make_float4(a.lo.y, inf, inf, inf);
+  nodes4[3] = make_float4(a.hi.y, -inf, -inf, -inf);
+  nodes4[4] = make_float4(a.lo.z, inf, inf, inf);
+  nodes4[5] = make_float4(a.hi.z, -inf, -inf, -inf);
+  const int e = 0x7fffffff;
+  nodes4[6] = make_float4(__int_as_float(~(int)(unsigned)(count - 1)), __int_as_float(e), __int_as_float(e),
+                          __int_as_float(e));
+  nodes4[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
 // Root handling for trees whose root is a leaf: one node with the leaf as child 0 and an
 // empty child 1 (inverted box, reference to slot 0 with count 1).
 __global__ void k_leaf_root(const Aabb* node_box, int root, int count, float4* nodes) {
@@ -355,6 +419,8 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   out->max_depth = 0;
   out->nodes = nullptr;
   out->tris = nullptr;
+  out->nodes4 = nullptr;  // none for an empty tree: traversal uses the binary layout
+  out->num_nodes4 = 0;
   if (n == 0) {
     // No primitives: a root with two empty children and one degenerate slot (prim -1).
     float host_node[16];
@@ -493,21 +559,46 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   cudaMemcpyAsync(&root_emit, emit + root, 1, cudaMemcpyDeviceToHost, st);
   if (!ok(cudaStreamSynchronize(st), "emission")) return false;
   const int num_nodes = root_emit ? emitted : 1;
+  // 4-wide numbering: the emitted nodes at even depth, in binary depth-first order.
+  int num4 = 1;
+  int* index4 = nullptr;
+  if (root_emit) {
+    int* flag_dfs = sc.alloc<int>(std::max(1, emitted));
+    index4 = sc.alloc<int>(std::max(1, emitted));
+    if (!flag_dfs || !index4) return fail("out of device memory");
+    k_flag4<<<grid_for(total), kThreads, 0, st>>>((int)total, n, emit, depth, index, flag_dfs);
+    size_t tb4 = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb4, flag_dfs, index4, emitted, st);
+    void* temp4 = sc.alloc<unsigned char>(tb4);
+    if (!temp4) return fail("out of device memory");
+    cub::DeviceScan::ExclusiveSum(temp4, tb4, flag_dfs, index4, emitted, st);
+    int last[2] = {0, 0};
+    cudaMemcpyAsync(&last[0], index4 + emitted - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(&last[1], flag_dfs + emitted - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (!ok(cudaStreamSynchronize(st), "4-wide numbering")) return false;
+    num4 = last[0] + last[1];
+  }
   if (!ok(pool_malloc((void**)&out->nodes, 4 * sizeof(float4) * (size_t)num_nodes, st), "allocation") ||
-      !ok(pool_malloc((void**)&out->tris, 3 * sizeof(float4) * (size_t)n, st), "allocation"))
+      !ok(pool_malloc((void**)&out->tris, 3 * sizeof(float4) * (size_t)n, st), "allocation") ||
+      !ok(pool_malloc((void**)&out->nodes4, 8 * sizeof(float4) * (size_t)num4, st), "allocation"))
     return false;
   // The root is a leaf when the whole tree collapses (or n == 1): its subtree starts at 0.
   if (!root_emit) {
     cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
     k_leaf_root<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes);
+    k_leaf_root4<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes4);
   } else {
-    for (const auto& r : ranges)
+    for (const auto& r : ranges) {
       k_write_nodes<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, offset,
                                                               emit, index, out->nodes);
+      k_write_nodes4<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size,
+                                                               offset, emit, depth, index, index4, out->nodes4);
+    }
   }
   k_write_slots<<<grid_for(n), kThreads, 0, st>>>(in, set, left, offset, n, out->tris);
   if (!ok(cudaStreamSynchronize(st), "emission") || !ok(cudaGetLastError(), "kernels")) return false;
   out->num_nodes = (uint32_t)num_nodes;
+  out->num_nodes4 = (uint32_t)num4;
   out->max_depth = root_emit ? depth_host : 0;
   if (verbose) {
     float root_cost = 0.f;

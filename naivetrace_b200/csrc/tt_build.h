@@ -26,6 +26,12 @@ struct DeviceBvh {
   float4* tris;         // primitive slots, from the memory pool (caller frees)
   uint32_t num_nodes;
   uint32_t max_depth;
+  // The same tree with four children per node (the binary tree's nodes at even depth, each
+  // with its children's children; 8 float4: lo.x[4], hi.x[4], lo.y[4], hi.y[4], lo.z[4],
+  // hi.z[4], int4 references (inner node, leaf reference as in the binary layout, or
+  // 0x7fffffff for an empty slot with an empty box), padding), from the memory pool.
+  float4* nodes4;
+  uint32_t num_nodes4;
 };
 
 // Builds the binary BVH of the `n` primitives whose global ids are in `set` (device array).

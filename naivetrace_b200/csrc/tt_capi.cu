@@ -280,11 +280,13 @@ struct tt_ctx {
   tt_stats stats{};
   std::string err;
   uint32_t bvh_nodes = 0, bvh_depth = 0, bvh_node_bytes = 64;
-  // The two BVH layouts the autotuner can choose between: [0] binary, [1] 8-wide compressed
-  // (built on the host on the autotuner's first request).  Slot arrays belong to a layout.
+  // The two BVH layouts the autotuner can choose between: [0] the device-built tree (binary,
+  // with its 4-wide collapse when built), [1] 8-wide compressed (built on the host on the
+  // autotuner's first request).  Slot arrays belong to a layout.
   struct Layout {
     bool ready = false;
     const float4* nodes = nullptr;
+    const float4* nodes4 = nullptr;
     const uint4* nodes8 = nullptr;
     const float4* tris = nullptr;
     const float4* vnodes = nullptr;
@@ -630,6 +632,7 @@ static void save_layout(tt_ctx* c) {
   tt_ctx::Layout& L = c->layouts[c->dev.wide ? 1 : 0];
   L.ready = true;
   L.nodes = c->dev.nodes;
+  L.nodes4 = c->dev.nodes4;
   L.nodes8 = c->dev.nodes8;
   L.tris = c->dev.tris;
   L.vnodes = c->dev.vnodes;
@@ -672,6 +675,7 @@ static tt_status use_layout(tt_ctx* c, bool wide) {
   }
   c->dev.wide = wide ? 1 : 0;
   c->dev.nodes = L.nodes;
+  c->dev.nodes4 = L.nodes4;
   c->dev.nodes8 = L.nodes8;
   c->dev.tris = L.tris;
   c->dev.vnodes = L.vnodes;
@@ -759,11 +763,16 @@ tt_status tt_upload_scene(tt_ctx* c) {
   };
   DevScene& s = c->dev;
   s.tri_idx = nullptr;  // set below, by the device build or from the host table
-  // The binary BVH is the default layout; TT_BVH_WIDTH=8 selects the 8-wide compressed
-  // BVH (80-byte nodes, about half the bytes per ray but more arithmetic per node, which
-  // measured a few percent slower on the terrain workload).
+  // The default layout is the device-built tree with four children per node (the binary
+  // tree collapsed pairwise on the device; its traversal fetches half as many nodes per ray:
+  // 6 % less closest-hit time than the binary tree on the terrain workload);
+  // TT_BVH_WIDTH=2 keeps the binary layout, TT_BVH_WIDTH=8 selects the 8-wide compressed BVH
+  // (80-byte nodes, about half the bytes per ray but more arithmetic per node, which
+  // measured slower on the terrain workload).
   const char* width_env = std::getenv("TT_BVH_WIDTH");
   s.wide = width_env && std::atoi(width_env) == 8;
+  const bool binary_only = width_env && std::atoi(width_env) == 2;
+  s.nodes4 = nullptr;
   // The binary BVH is built on the device (PLOC) unless TT_BVH_BUILD=host asks for the
   // host binned-SAH builder.
   const char* build_env = std::getenv("TT_BVH_BUILD");
@@ -851,6 +860,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
     cudaStreamSynchronize(c->stream);
     tmp.free_all();
     if (!built) return fail(c, TT_ERR_CUDA, berr);
+    if (sb.nodes4) c->scene_mem.allocs.push_back(sb.nodes4);
+    if (vb.nodes4) c->scene_mem.allocs.push_back(vb.nodes4);
     c->bvh_nodes = sb.num_nodes;
     c->bvh_depth = sb.max_depth;
     c->bvh_node_bytes = 64;
@@ -860,6 +871,13 @@ tt_status tt_upload_scene(tt_ctx* c) {
     s.tris = sb.tris;
     s.vnodes = vb.nodes;
     s.vtris = vb.tris;
+    if (sb.nodes4 && !binary_only) {
+      // Closest hit runs on the 4-wide nodes; a counted node visit reads 112 bytes (the
+      // eighth float4 of a node is padding).
+      s.nodes4 = sb.nodes4;
+      c->bvh_nodes = sb.num_nodes4;
+      c->bvh_node_bytes = 112;
+    }
   } else {
     BvhInput bi{}, vbi{};
     host_inputs(&bi, &vbi);
@@ -2474,7 +2492,7 @@ tt_status tt_autotune_views(tt_ctx* c, const tt_view* views, int32_t n, tt_tune_
       out->candidate_grid[k] = g;
       out->candidate_ms[k] = ms;
       out->candidate_block[k] = block;
-      out->candidate_width[k] = wide ? 8 : 2;
+      out->candidate_width[k] = wide ? 8 : (c->dev.nodes4 ? 4 : 2);
     }
     ++k;
     if (ms < best) {
@@ -2508,7 +2526,7 @@ tt_status tt_autotune_views(tt_ctx* c, const tt_view* views, int32_t n, tt_tune_
   (void)start_wide;
   out->candidates = k;
   out->block = best_block;
-  out->bvh_width = best_wide ? 8 : 2;
+  out->bvh_width = best_wide ? 8 : (c->layouts[0].nodes4 || (!c->dev.wide && c->dev.nodes4) ? 4 : 2);
   if ((st = use_layout(c, best_wide)) != TT_OK) return st;
   c->dev.block = best_block;
   c->params.wave_paths = out->wave_paths;

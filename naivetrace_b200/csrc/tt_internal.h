@@ -98,6 +98,8 @@ struct DevCamera {
 
 // Everything a kernel needs to know about the scene; passed by value (constant bank).
 struct DevScene {
+  const float4* nodes4;       // the surface BVH with four children per node (tt_build.h), when
+                              // built: the binary layout's traversal then uses it
   int wide;                   // 1: the 8-wide BVH (nodes8 / vnodes8) is the active layout
   const uint4* nodes8;        // 8-wide BVH, 5 uint4 per node (tt_bvh.h)
   const uint4* vnodes8;

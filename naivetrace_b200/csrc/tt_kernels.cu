@@ -378,6 +378,108 @@ __device__ __forceinline__ void trace_ww(const BvhRef& bvh, TraceState& s, int* 
   }
 }
 
+// Traversal of the 4-wide layout (nodes at even depth of the binary tree, each with up to
+// four children: tt_build.h).  A node's four boxes are tested together (structure of arrays),
+// the hit children sorted by entry distance: the nearest is visited next, the others pushed
+// farthest first.  Closest hit postpones leaves as trace_ww does (speculative while-while);
+// any hit tests a leaf as soon as it reaches it.  Half the binary tree's depth means half
+// the chain of dependent node fetches that bounds the traversal.  (Used for closest hit;
+// the ANY form, leaves tested as soon as reached, measured slower than the binary per-step
+// traversal for shadow rays.)
+__device__ __forceinline__ void sort2(float& da, int& ra, float& db, int& rb) {
+  if (db < da) {
+    const float t = da;
+    da = db;
+    db = t;
+    const int u = ra;
+    ra = rb;
+    rb = u;
+  }
+}
+template <bool ANY, bool COUNT, bool SPH>
+__device__ __forceinline__ void trace4(const float4* __restrict__ nodes4, const float4* __restrict__ tris,
+                                       TraceState& s, int* stack, unsigned int* err, TraceCounters* cnt) {
+  const RayPre& r = s.r;
+  int cur = 0;
+  int leaf = kNoNode;
+  int sp = 0;
+  while (cur != kNoNode || leaf != kNoNode) {
+    while ((unsigned)cur < (unsigned)kNoNode) {
+      const float4* np = nodes4 + 8 * (size_t)cur;
+      const float4 lx = __ldg(np), hx = __ldg(np + 1), ly = __ldg(np + 2), hy = __ldg(np + 3);
+      const float4 lz = __ldg(np + 4), hz = __ldg(np + 5);
+      const int4 rf = __ldg(reinterpret_cast<const int4*>(np + 6));
+      if (COUNT) cnt->nodes++;
+      const float lim = s.best_t * 1.0000004f;  // 1 + 2 gamma(3): conservative slabs
+      const float lxs[4] = {lx.x, lx.y, lx.z, lx.w}, hxs[4] = {hx.x, hx.y, hx.z, hx.w};
+      const float lys[4] = {ly.x, ly.y, ly.z, ly.w}, hys[4] = {hy.x, hy.y, hy.z, hy.w};
+      const float lzs[4] = {lz.x, lz.y, lz.z, lz.w}, hzs[4] = {hz.x, hz.y, hz.z, hz.w};
+      float d[4];
+      int c[4] = {rf.x, rf.y, rf.z, rf.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float tx0 = fmaf(lxs[j], r.id.x, -r.ood.x), tx1 = fmaf(hxs[j], r.id.x, -r.ood.x);
+        const float ty0 = fmaf(lys[j], r.id.y, -r.ood.y), ty1 = fmaf(hys[j], r.id.y, -r.ood.y);
+        const float tz0 = fmaf(lzs[j], r.id.z, -r.ood.z), tz1 = fmaf(hzs[j], r.id.z, -r.ood.z);
+        const float tmin = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), s.tnear));
+        const float tmax = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), lim));
+        d[j] = (tmin <= tmax && c[j] != kNoNode) ? tmin : INFINITY;  // empty slots never hit
+      }
+      sort2(d[0], c[0], d[1], c[1]);
+      sort2(d[2], c[2], d[3], c[3]);
+      sort2(d[0], c[0], d[2], c[2]);
+      sort2(d[1], c[1], d[3], c[3]);
+      sort2(d[1], c[1], d[2], c[2]);
+      if (d[0] == INFINITY) {
+        cur = sp > 0 ? stack[--sp] : kNoNode;
+      } else {
+        if (sp + 3 > BVH_STACK) {
+          atomicOr(err, ERR_STACK);
+          s.best = -1;
+          return;
+        }
+        if (d[3] != INFINITY) stack[sp++] = c[3];
+        if (d[2] != INFINITY) stack[sp++] = c[2];
+        if (d[1] != INFINITY) stack[sp++] = c[1];
+        cur = c[0];
+      }
+      if (cur < 0 && leaf == kNoNode) {
+        leaf = cur;
+        cur = sp > 0 ? stack[--sp] : kNoNode;
+        if (ANY) break;
+      }
+      if (!ANY && !__any_sync(__activemask(), leaf == kNoNode)) break;
+    }
+    while (leaf != kNoNode) {
+      const unsigned v = ~(unsigned)leaf;
+      const int start = (int)(v >> 3), count = (int)(v & 7u) + 1;
+      for (int i = start; i < start + count; ++i) {
+        const float4 a = __ldg(&tris[3 * i]);
+        const float4 b = __ldg(&tris[3 * i + 1]);
+        const float4 cc = __ldg(&tris[3 * i + 2]);
+        if (COUNT) cnt->tris++;
+        float t, b1 = 0.f, b2 = 0.f;
+        bool hit;
+        if (SPH && __float_as_int(cc.w) != 0) hit = intersect_sphere(r, a, b, s.tnear, s.best_t, &t);
+        else hit = intersect_tri(r, xyz(a), xyz(b), xyz(cc), s.tnear, s.best_t, &t, &b1, &b2);
+        if (hit && (ANY || closer(t, __float_as_int(a.w), s.best_t, s.best_prim))) {
+          s.best = i;
+          s.best_prim = __float_as_int(a.w);
+          s.best_t = t;
+          s.b1 = b1;
+          s.b2 = b2;
+          if (ANY) return;
+        }
+      }
+      leaf = kNoNode;
+      if (cur < 0) {
+        leaf = cur;
+        cur = sp > 0 ? stack[--sp] : kNoNode;
+      }
+    }
+  }
+}
+
 // Recomputes the distance of the closest hit from the plane equation in double precision
 // (float rounding of Ng.(v0 - o) is amplified by 1/|cos| at grazing incidence).
 __device__ __forceinline__ float refine_t(const float4* tris, const RayPre& r, int slot) {
@@ -562,9 +664,14 @@ __device__ __forceinline__ int trace(const DevScene& sc, const RayPre& r, float 
   s.best_prim = 0x7fffffff;
   s.cur = 0;
   s.sp = 0;
-  if (ANY) {
-    // Any hit: one node or leaf per step, so that a lane meets its first hit as early as
-    // the tree order allows (postponing leaves measured 3.5 % slower for shadow rays).
+  if (!ANY && sc.nodes4) {
+    // Closest hit on the 4-wide nodes (6 % less closest-hit time than the binary while-while
+    // traversal on the terrain workload).
+    trace4<ANY, COUNT, SPH>(sc.nodes4, sc.tris, s, stack, err, cnt);
+  } else if (ANY) {
+    // Any hit: one binary node or leaf per step, so that a lane meets its first hit as early
+    // as the tree order allows (postponing leaves measured 3.5 % slower for shadow rays, the
+    // 4-wide nodes 7 % slower).
     while (!trace_step<ANY, COUNT, SPH>(bvh, s, stack, err, cnt)) {
     }
   } else {

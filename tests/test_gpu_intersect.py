@@ -186,19 +186,21 @@ def test_traversal_counts(gpu_lib):
     st = g.stats()
     assert st["counted_rays"] == 10000
     assert st["node_visits"] > 10000 and st["tri_tests"] > 0
-    assert st["bvh_nodes"] > 0 and st["bvh_node_bytes"] in (64, 80) and st["tri_bytes"] == 48
+    assert st["bvh_nodes"] > 0 and st["bvh_node_bytes"] in (64, 80, 112) and st["tri_bytes"] == 48
 
 
-@pytest.fixture
-def wide_bvh(monkeypatch):
-    """Selects the 8-wide compressed BVH for contexts created in the test."""
-    monkeypatch.setenv("TT_BVH_WIDTH", "8")
+@pytest.fixture(params=[2, 8])
+def wide_bvh(monkeypatch, request):
+    """Selects the binary layout or the 8-wide compressed BVH (instead of the default 4-wide
+    collapse of the device-built tree) for contexts created in the test."""
+    monkeypatch.setenv("TT_BVH_WIDTH", str(request.param))
+    return request.param
 
 
 def test_wide_bvh_matches_oracle(gpu_lib, wide_bvh):
     s = scenes.terrain_spheres_small()
     g = GpuContext(s)
-    assert g.stats()["bvh_node_bytes"] == 80
+    assert g.stats()["bvh_node_bytes"] == {2: 64, 8: 80}[wide_bvh]
     o = OracleScene(s, make_params())
     rng = np.random.default_rng(12)
     rays = random_rays(200000, -4.5, 4.5, rng)

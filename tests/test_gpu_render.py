@@ -175,13 +175,15 @@ def test_no_device_errors(gpu_lib):
     assert np.all(np.isfinite(rgb))
 
 
+@pytest.mark.parametrize("width", [2, 8])
 @pytest.mark.parametrize("name", ["cornell_box_materials", "terrain_spheres_small"])
-def test_per_path_parity_wide_bvh(gpu_lib, monkeypatch, name):
-    """The same per-path parity with the 8-wide compressed BVH as the traversal layout."""
-    monkeypatch.setenv("TT_BVH_WIDTH", "8")
+def test_per_path_parity_wide_bvh(gpu_lib, monkeypatch, name, width):
+    """The same per-path parity with the binary layout or the 8-wide compressed BVH as the
+    traversal layout (the default is the 4-wide collapse of the device-built tree)."""
+    monkeypatch.setenv("TT_BVH_WIDTH", str(width))
     scene = scenes.cornell_box_materials(32, 32) if name != "terrain_spheres_small" else scenes.terrain_spheres_small(48, 27)
     (ag, lg, sg), (ao, lo, so), g, o = render_both(scene, 4, 10)
-    assert g.stats()["bvh_node_bytes"] == 80
+    assert g.stats()["bvh_node_bytes"] == {2: 64, 8: 80}[width]
     ag = ag.reshape(-1, 3)
     ao = ao.reshape(-1, 3)
     scale = max(np.abs(ao).mean(), 1e-6)

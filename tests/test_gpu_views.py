@@ -82,8 +82,8 @@ def test_autotune_views(gpu_lib):
     # 12 queue-capacity x launch-width probes, then half-size blocks and the 8-wide BVH.
     assert len(r["candidates"]) == 14
     assert {c["block"] for c in r["candidates"]} == {128, 256}
-    assert {c["bvh_width"] for c in r["candidates"]} == {2, 8}
-    assert r["block"] in (128, 256) and r["bvh_width"] in (2, 8)
+    assert {c["bvh_width"] for c in r["candidates"]} == {4, 8}  # the device-built default, then 8-wide
+    assert r["block"] in (128, 256) and r["bvh_width"] in (4, 8)
     assert r["ms"] == min(c["ms"] for c in r["candidates"])
     imgs = g.render_views(views, seed=2)
     assert len(imgs) == 8 and all(np.isfinite(i).all() for i in imgs)
