@@ -305,44 +305,56 @@ __global__ void k_write_nodes(int first, int count, uint32_t n, const Aabb* node
   }
 }
 
-// 4-wide layout: a node for every emitted binary node at even depth (root depth 0), its
-// slots the children of its binary children that are inner nodes and those binary children
-// that are leaves; numbered in depth-first order by a scan over the binary depth-first
-// numbering.
-__global__ void k_flag4(int total, uint32_t n, const unsigned char* emit, const int* depth, const int* index,
-                        int* flag_dfs) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
-    if (k >= (int)n && emit[k]) flag_dfs[index[k]] = (depth[k] & 1) == 0 ? 1 : 0;
-}
-__global__ void k_write_nodes4(int first, int count, uint32_t n, const Aabb* node_box, const int* left,
-                               const int* right, const int* size, const int* offset, const unsigned char* emit,
-                               const int* depth, const int* index, const int* index4, float4* nodes4) {
+// 4-wide layout, built top down one level at a time: a 4-wide node starts from a binary
+// inner node's two children and, while it has fewer than four, replaces the inner child of
+// the largest surface area by that child's two children (the usual collapse of a binary
+// tree into a wide one); its remaining inner children become the next level's 4-wide
+// nodes, numbered by an atomic counter.  frontier: (binary node, 4-wide index) pairs.
+__global__ void k_collapse4(const int2* frontier, int nfront, uint32_t n, const Aabb* node_box, const int* left,
+                            const int* right, const int* size, const int* offset, const unsigned char* emit,
+                            const int* index, int* counter, int2* next, int* nnext, float4* nodes4) {
   constexpr int kEmpty = 0x7fffffff;
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < count; t += gridDim.x * blockDim.x) {
-    const int k = first + t;
-    if (!emit[k] || (depth[k] & 1)) continue;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nfront; t += gridDim.x * blockDim.x) {
+    const int k = frontier[t].x, i4 = frontier[t].y;
+    int slot[4] = {left[k], right[k], -1, -1};
+    int m = 2;
+    while (m < 4) {
+      int best = -1;
+      float best_area = -1.f;
+      for (int j = 0; j < m; ++j) {
+        const int c = slot[j];
+        if (c >= (int)n && emit[c]) {
+          const float a = half_area(node_box[c]);
+          if (a > best_area) {
+            best_area = a;
+            best = j;
+          }
+        }
+      }
+      if (best < 0) break;
+      const int c = slot[best];
+      slot[best] = left[c];
+      slot[m++] = right[c];
+    }
     Aabb box[4];
     int ref[4];
-    int m = 0;
-    const int kids[2] = {left[k], right[k]};
-    for (int s = 0; s < 2; ++s) {
-      const int c = kids[s];
+    for (int j = 0; j < 4; ++j) {
+      if (j >= m) {
+        box[j] = Aabb{make_float3(INFINITY, INFINITY, INFINITY), make_float3(-INFINITY, -INFINITY, -INFINITY)};
+        ref[j] = kEmpty;
+        continue;
+      }
+      const int c = slot[j];
+      box[j] = node_box[c];
       if (c >= (int)n && emit[c]) {
-        const int g[2] = {left[c], right[c]};
-        for (int u = 0; u < 2; ++u) {
-          box[m] = node_box[g[u]];
-          ref[m++] = (g[u] >= (int)n && emit[g[u]]) ? index4[index[g[u]]] : child_ref(g[u], n, size, offset, emit, index);
-        }
+        const int j4 = atomicAdd(counter, 1);
+        next[atomicAdd(nnext, 1)] = make_int2(c, j4);
+        ref[j] = j4;
       } else {
-        box[m] = node_box[c];
-        ref[m++] = child_ref(c, n, size, offset, emit, index);
+        ref[j] = child_ref(c, n, size, offset, emit, index);
       }
     }
-    for (; m < 4; ++m) {
-      box[m] = Aabb{make_float3(INFINITY, INFINITY, INFINITY), make_float3(-INFINITY, -INFINITY, -INFINITY)};
-      ref[m] = kEmpty;
-    }
-    float4* d = nodes4 + 8 * (size_t)index4[index[k]];
+    float4* d = nodes4 + 8 * (size_t)i4;
     d[0] = make_float4(box[0].lo.x, box[1].lo.x, box[2].lo.x, box[3].lo.x);
     d[1] = make_float4(box[0].hi.x, box[1].hi.x, box[2].hi.x, box[3].hi.x);
     d[2] = make_float4(box[0].lo.y, box[1].lo.y, box[2].lo.y, box[3].lo.y);
@@ -559,41 +571,49 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   cudaMemcpyAsync(&root_emit, emit + root, 1, cudaMemcpyDeviceToHost, st);
   if (!ok(cudaStreamSynchronize(st), "emission")) return false;
   const int num_nodes = root_emit ? emitted : 1;
-  // 4-wide numbering: the emitted nodes at even depth, in binary depth-first order.
-  int num4 = 1;
-  int* index4 = nullptr;
-  if (root_emit) {
-    int* flag_dfs = sc.alloc<int>(std::max(1, emitted));
-    index4 = sc.alloc<int>(std::max(1, emitted));
-    if (!flag_dfs || !index4) return fail("out of device memory");
-    k_flag4<<<grid_for(total), kThreads, 0, st>>>((int)total, n, emit, depth, index, flag_dfs);
-    size_t tb4 = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, tb4, flag_dfs, index4, emitted, st);
-    void* temp4 = sc.alloc<unsigned char>(tb4);
-    if (!temp4) return fail("out of device memory");
-    cub::DeviceScan::ExclusiveSum(temp4, tb4, flag_dfs, index4, emitted, st);
-    int last[2] = {0, 0};
-    cudaMemcpyAsync(&last[0], index4 + emitted - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(&last[1], flag_dfs + emitted - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (!ok(cudaStreamSynchronize(st), "4-wide numbering")) return false;
-    num4 = last[0] + last[1];
-  }
+  // The 4-wide nodes are at most the emitted binary nodes (each 4-wide node replaces at
+  // least one); the actual count comes from the collapse.
+  const int cap4 = root_emit ? std::max(1, emitted) : 1;
   if (!ok(pool_malloc((void**)&out->nodes, 4 * sizeof(float4) * (size_t)num_nodes, st), "allocation") ||
       !ok(pool_malloc((void**)&out->tris, 3 * sizeof(float4) * (size_t)n, st), "allocation") ||
-      !ok(pool_malloc((void**)&out->nodes4, 8 * sizeof(float4) * (size_t)num4, st), "allocation"))
+      !ok(pool_malloc((void**)&out->nodes4, 8 * sizeof(float4) * (size_t)cap4, st), "allocation"))
     return false;
+  int num4 = 1;
   // The root is a leaf when the whole tree collapses (or n == 1): its subtree starts at 0.
   if (!root_emit) {
     cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
     k_leaf_root<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes);
     k_leaf_root4<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes4);
   } else {
-    for (const auto& r : ranges) {
+    for (const auto& r : ranges)
       k_write_nodes<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, offset,
                                                               emit, index, out->nodes);
-      k_write_nodes4<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size,
-                                                               offset, emit, depth, index, index4, out->nodes4);
+    int2* front[2] = {sc.alloc<int2>(cap4), sc.alloc<int2>(cap4)};
+    int* counts = sc.alloc<int>(2);  // [0] 4-wide nodes numbered, [1] next level's size
+    if (!front[0] || !front[1] || !counts) return fail("out of device memory");
+    const int2 root4 = make_int2(root, 0);
+    const int init[2] = {1, 0};
+    cudaMemcpyAsync(front[0], &root4, sizeof(int2), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(counts, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    int nfront = 1;
+    for (int level = 0; nfront > 0 && level < 64; ++level) {
+      cudaMemsetAsync(counts + 1, 0, sizeof(int), st);
+      k_collapse4<<<grid_for(nfront), kThreads, 0, st>>>(front[level & 1], nfront, n, node_box, left, right, size,
+                                                          offset, emit, index, counts, front[(level + 1) & 1],
+                                                          counts + 1, out->nodes4);
+      int c2[2] = {0, 0};
+      cudaMemcpyAsync(c2, counts, sizeof(c2), cudaMemcpyDeviceToHost, st);
+      if (!ok(cudaStreamSynchronize(st), "4-wide collapse")) return false;
+      nfront = c2[1];
+      num4 = c2[0];
     }
+    if (nfront > 0) return fail("4-wide collapse deeper than 64 levels");
+    // Keep the nodes in a buffer of their exact size (the collapse wrote into an upper bound).
+    float4* exact = nullptr;
+    if (!ok(pool_malloc((void**)&exact, 8 * sizeof(float4) * (size_t)num4, st), "allocation")) return false;
+    cudaMemcpyAsync(exact, out->nodes4, 8 * sizeof(float4) * (size_t)num4, cudaMemcpyDeviceToDevice, st);
+    pool_free(out->nodes4, st);
+    out->nodes4 = exact;
   }
   k_write_slots<<<grid_for(n), kThreads, 0, st>>>(in, set, left, offset, n, out->tris);
   if (!ok(cudaStreamSynchronize(st), "emission") || !ok(cudaGetLastError(), "kernels")) return false;

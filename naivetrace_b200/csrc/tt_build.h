@@ -26,10 +26,11 @@ struct DeviceBvh {
   float4* tris;         // primitive slots, from the memory pool (caller frees)
   uint32_t num_nodes;
   uint32_t max_depth;
-  // The same tree with four children per node (the binary tree's nodes at even depth, each
-  // with its children's children; 8 float4: lo.x[4], hi.x[4], lo.y[4], hi.y[4], lo.z[4],
-  // hi.z[4], int4 references (inner node, leaf reference as in the binary layout, or
-  // 0x7fffffff for an empty slot with an empty box), padding), from the memory pool.
+  // The same tree with up to four children per node (a binary node's children, the inner
+  // child of the largest surface area replaced by its children until there are four; 8
+  // float4: lo.x[4], hi.x[4], lo.y[4], hi.y[4], lo.z[4], hi.z[4], int4 references (inner
+  // node, leaf reference as in the binary layout, or 0x7fffffff for an empty slot with an
+  // empty box), padding; the root is node 0), from the memory pool.
   float4* nodes4;
   uint32_t num_nodes4;
 };

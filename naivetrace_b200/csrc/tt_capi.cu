@@ -764,8 +764,8 @@ tt_status tt_upload_scene(tt_ctx* c) {
   DevScene& s = c->dev;
   s.tri_idx = nullptr;  // set below, by the device build or from the host table
   // The default layout is the device-built tree with four children per node (the binary
-  // tree collapsed pairwise on the device; its traversal fetches half as many nodes per ray:
-  // 6 % less closest-hit time than the binary tree on the terrain workload);
+  // tree collapsed on the device; its traversal fetches half as many nodes per ray: 6 % less
+  // closest-hit time than the binary tree on the terrain workload);
   // TT_BVH_WIDTH=2 keeps the binary layout, TT_BVH_WIDTH=8 selects the 8-wide compressed BVH
   // (80-byte nodes, about half the bytes per ray but more arithmetic per node, which
   // measured slower on the terrain workload).

@@ -378,8 +378,8 @@ __device__ __forceinline__ void trace_ww(const BvhRef& bvh, TraceState& s, int* 
   }
 }
 
-// Traversal of the 4-wide layout (nodes at even depth of the binary tree, each with up to
-// four children: tt_build.h).  A node's four boxes are tested together (structure of arrays),
+// Traversal of the 4-wide layout (the binary tree collapsed to nodes of up to four
+// children: tt_build.h).  A node's four boxes are tested together (structure of arrays),
 // the hit children sorted by entry distance: the nearest is visited next, the others pushed
 // farthest first.  Closest hit postpones leaves as trace_ww does (speculative while-while);
 // any hit tests a leaf as soon as it reaches it.  Half the binary tree's depth means half
