@@ -638,15 +638,23 @@ def run_ours(args):
     d2h = 3 * npix * 4
     h2d = scene_bytes(scene)
     rgb = np.zeros(3 * npix, np.float32)
+    e2e_phases = []
     for k in range(1 + args.e2e_steps):  # the first call is an untimed warm-up
         nd.barrier(r)
         t0 = time.perf_counter()
-        ge = GpuContext(scene, params)
+        ge = GpuContext(scene, params, upload=False)
+        t1 = time.perf_counter()
+        ge.upload()
+        t2 = time.perf_counter()
         ge.render(spp, seed)
+        t3 = time.perf_counter()
         ge.lib.tt_read_framebuffer(ge.h, rgb.ctypes.data_as(C.POINTER(C.c_float)), None)
+        t4 = time.perf_counter()
         ge.close()
+        t5 = time.perf_counter()
         if k > 0:
-            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            e2e_ms.append((t5 - t0) * 1e3)
+            e2e_phases.append([round((b - a) * 1e3, 1) for a, b in ((t0, t1), (t1, t2), (t2, t3), (t3, t4), (t4, t5))])
     e2e_step = float(np.median(e2e_ms)) if e2e_ms else float("nan")
     e2e_step = nd.max_over_ranks(e2e_step, r)
     e2e_value = nd.weak_scaling_value(paths_per_step, world, e2e_step)
@@ -706,6 +714,8 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": e2e_step, "ms_each": [round(x, 1) for x in e2e_ms],
+                    "phases_ms_each": {"order": ["create", "upload", "render", "read", "destroy"],
+                                       "calls": e2e_phases},
                     "what": "tt_create + tt_upload_scene (scene H2D, device BVH build) + tt_render_pass + "
                             "tt_read_framebuffer + tt_destroy"},
             "guiding": guiding,

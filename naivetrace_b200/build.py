@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -44,8 +45,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     deps = [CSRC / s for s in SOURCES] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "toytrace_gpu.h", Path(__file__)]
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", str(ROOT / "include")]
+    cmds, objs = [], []
     for src in SOURCES:
         obj = OUT_DIR / (Path(src).stem + ".o")
         cmd = [nvcc(), *ARCH, "-lineinfo", *common, "-c", str(CSRC / src), "-o", str(obj)]
@@ -53,8 +54,12 @@ def build(force: bool = False, verbose: bool = False) -> Path:
             cmd += ["-Xptxas", "-v"] if verbose else []
         else:
             cmd += ["-x", "c++"]
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # The translation units are independent: compile them side by side.
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.run, c, check=True) for c in cmds]:
+            f.result()
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs, "-lcudart"], check=True)
     os.replace(tmp, LIB)
