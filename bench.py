@@ -804,8 +804,8 @@ def profile_guiding(args):
 
 def profile_training(args):
     """No timing: four Adam steps of the guiding network on 2^18 synthetic training records
-    (the configuration's records per step), each step the training kernel, the tcgen05
-    weight-gradient kernel and the fused reduction and Adam step (for ncu captures)."""
+    (the configuration's records per step), each step the tcgen05 gradient kernel and the
+    fused reduction and Adam step (for ncu captures)."""
     from naivetrace_b200 import scenes
     from naivetrace_b200.algo import GpuContext
     from naivetrace_b200.scene import make_params

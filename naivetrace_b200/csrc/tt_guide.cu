@@ -3,16 +3,22 @@
 // sampled with density q at direction wi with target value F, minimise -(F / q) log p(wi)
 // with p = (1 - c) p_bsdf + c p_vmf, which also learns the selection probability c.
 //
-// One training step is four launches:
+// One training step is two launches with the default (tcgen05) network kernels:
+//   k_step_tc      persistent over tiles of 128 records: features, the five layers, the loss
+//                  gradient per record, the backward pass and the weight and bias gradients,
+//                  the tile's activations in shared memory and the CTA's weight gradients in
+//                  tensor memory, written once per CTA as a partial sum;
+//   k_reduce_adam  sum of the CTAs' partials with the Adam step fused in (k_reduce and k_adam
+//                  separately when the gradient alone is asked for).
+// With the warp-level mma.sync kernels it is three:
 //   k_train   persistent; per warp 16 records: features in registers, the five layers
-//             (guide_mlp_tile, activations kept in global memory for the weight gradients),
-//             the loss gradient per record, and the backward pass through the layers on the
-//             same tensor-core tiles (B fragments of W^T by ldmatrix.trans from the forward
-//             weight image), storing each layer's output gradient;
+//             (activations kept in global memory for the weight gradients), the loss gradient
+//             per record, and the backward pass through the layers on the same tensor-core
+//             tiles (B fragments of W^T by ldmatrix.trans from the forward weight image),
+//             storing each layer's output gradient;
 //   k_wgrad   dW_l = sum over records of dH_l^T X_l and the bias sums, split over chunks of
-//             128 records (mma.sync with ldmatrix.trans fragments of both operands);
-//   k_reduce  sum of the chunk partials (k_reduce_adam: with the Adam step fused in);
-//   k_adam    Adam on the FP32 master parameters, refreshing the BF16 copy.
+//             128 records (ldmatrix.trans fragments of both operands);
+//   k_reduce_adam  as above.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -325,113 +331,279 @@ __global__ void __launch_bounds__(128) k_wgrad(int n, TrainBufs b, float* __rest
   if (tid < out) pw[guide_b_offset(l) + tid] = bsum;
 }
 
-// The same weight and bias gradients on the tcgen05 tensor cores.  A CTA of 128 threads
-// owns layer blockIdx.y over records [blockIdx.x * kWtChunk, +kWtChunk) and accumulates
-// D = A B^T in tensor memory, with A (M = 128 rows: the layer's inputs, then a row of ones
-// whose product is the bias gradient, then zeros) and B (N = the layer's outputs) both
-// K-major over records: A[m][k] = X[k][m], B[n][k] = G[k][n].  D[m][n] is dW[n][m] (and the
-// bias gradient of output n in row m = inputs).  Per tile of 128 records each thread stages
-// its record's X and G row transposed into the core-matrix layout of the UMMA descriptors
-// (tt_guide_tc.cuh), one thread issues the 8 MMAs of K = 16 and commits them to an
-// mbarrier; after the last tile every thread reads its lane (one input row) of D.
-constexpr int kWtRecs = 128;                        // records per staged tile (the K extent)
-constexpr int kWtTiles = 4;                         // tiles per CTA
-constexpr int kWtChunk = kWtRecs * kWtTiles;        // records per CTA
-constexpr int kWtA = 0;                             // 128 x 128 BF16
-constexpr int kWtB = kWtA + 128 * kWtRecs * 2;      // kGHid x 128 BF16
-constexpr int kWtBar = kWtB + kGHid * kWtRecs * 2;  // mbarrier
-constexpr int kWtTmem = kWtBar + 8;                 // tensor-memory address
-constexpr int kWtSmem = kWtTmem + 8;
-static_assert(kWtB % 16 == 0 && kWtBar % 8 == 0 && kWtSmem <= 227 * 1024, "tcgen05 weight-gradient layout");
-static_assert(kGIn + 1 <= 128 && kGHid + 1 <= 128, "the inputs and the ones row fit in M = 128");
+// The gradient of a training step in one kernel on the tcgen05 tensor cores.  A CTA of 128
+// threads (four warps) walks the mini-batch in tiles of 128 records, thread t owning record
+// t of the tile, and keeps the whole tile on chip: the features and the four hidden
+// activations in shared memory, the ReLU masks in registers, the per-layer accumulator and
+// the CTA's weight gradients of all five layers in tensor memory (64 + 304 of 512 columns).
+// Every GEMM has M = 128 and BF16 operands in the core-matrix layout of tt_guide_tc.cuh:
+//   forward   H_l = ReLU(H_{l-1} W_l^T + b_l): A = the input tile (K-major over features),
+//             B = W_l as stored ([out][in], K-major);
+//   backward  dH_{l-1} = (dH_l W_l) masked by H_{l-1} > 0: A = the gradient tile (K-major
+//             over the layer's outputs), B = W_l^T (a transposed copy made when the CTA
+//             loads the weights);
+//   weights   dW_l += H_{l-1}^T dH_l over the tile's 128 records, D[m = input][n = output]:
+//             A = the input tile read MN-major (the same bytes: 8 consecutive features of a
+//             record form a 16-byte core-matrix row, 8 records its 8 rows), B = the gradient
+//             tile read MN-major.  The hidden tiles carry a column of ones after the 64
+//             activations, so row 64 of D is the bias gradient; layer 0's inputs hold the
+//             network's constant feature (column kGOneFeature), whose row is its bias gradient.
+//             Rows of D past a layer's inputs (M = 128 reads on into the next core-matrix
+//             rows of the tile) are not used.
+// The loss and its output gradient per record are guide_loss_row's, rounded to BF16 after the
+// division by n as in k_train; hidden gradients are rounded to BF16 as there.  At the end the
+// CTA writes its weight and bias gradients to partial[blockIdx.x] (k_reduce_adam sums them).
+constexpr int kFhK = kGHid + 8;                                   // hidden tile row: 64 + ones + 7 zeros
+constexpr int kGOneFeature = 6 * kGFreq + kGInputs;              // the constant-1 input feature
+static_assert(kGOneFeature < kGIn, "the constant feature is one of layer 0's inputs");
+constexpr int kFwBytes = kGHid * kGIn * 2 + 3 * kGHid * kGHid * 2 + kGOut * kGHid * 2;
+constexpr int kFwtBytes = 3 * kGHid * kGHid * 2 + kGHid * kGOut * 2;
+constexpr int kFX = 0;                                            // 128 x 96 features
+constexpr int kFHBytes = kTcRows * kFhK * 2;
+constexpr int kFH = kFX + kTcRows * kGIn * 2;                     // 4 tiles of 128 x 72
+constexpr int kFD = kFH + 4 * kFHBytes;                           // 128 x (48 or 64) gradients
+constexpr int kFW = kFD + kTcRows * kGHid * 2;                    // forward weights
+constexpr int kFWt = kFW + kFwBytes;                              // W_l^T, l = 1..4
+constexpr int kFBias = kFWt + kFwtBytes;
+constexpr int kFBar = kFBias + (4 * kGHid + kGOut) * 4;
+constexpr int kFTmem = kFBar + 8;
+constexpr int kFSmem = kFTmem + 8;
+constexpr int kFCols = 512;                                       // tensor-memory columns of the CTA
+static_assert(kFH % 16 == 0 && kFHBytes % 16 == 0 && kFD % 16 == 0 && kFW % 16 == 0 && kFWt % 16 == 0 &&
+                  kFBar % 8 == 0 && kFSmem <= 227 * 1024,
+              "fused training layout: operands 16-byte aligned, mbarrier 8-byte aligned, within a CTA's limit");
+// An MN-major read with M = 128 reaches up to 16 core-matrix rows (2 KB) past a tile's last
+// record group; the buffers after each tile cover that.
+static_assert(kFH + 4 * kFHBytes + 16 * 128 <= kFW, "MN-major reads stay inside the CTA's buffers");
+static_assert(64 + 4 * kGHid + kGOut <= kFCols, "accumulator and weight gradients fit the tensor-memory allocation");
 
-__global__ void __launch_bounds__(128) k_wgrad_tc(int n, TrainBufs b, float* __restrict__ partial, unsigned* err) {
-  extern __shared__ __align__(128) unsigned char wsm[];
-  const int l = blockIdx.y;
-  const int out = guide_out(l), in = guide_in(l);
-  const bf16* G = l == kGLayers - 1 ? b.dy : b.dh[l];
-  const bf16* X = l == 0 ? b.x : b.h[l - 1];
+__device__ __forceinline__ int f_w(int l) { return kFW + (l == 0 ? 0 : kGHid * kGIn * 2 + (l - 1) * kGHid * kGHid * 2); }
+__device__ __forceinline__ int f_wt(int l) { return kFWt + (l - 1) * kGHid * kGHid * 2; }  // l = 1..4
+__device__ __forceinline__ int f_act(int l) { return l == 0 ? kFX : kFH + (l - 1) * kFHBytes; }  // layer l's input
+__device__ __forceinline__ int f_act_k(int l) { return l == 0 ? kGIn : kFhK; }                   // its row length
+__device__ __forceinline__ uint32_t f_dw_col(int l) { return 64u + 64u * (uint32_t)l; }
+
+// Instruction descriptor of kind::f16 with both operands MN-major.
+__host__ __device__ constexpr uint32_t tc_idesc_mn(int M, int N) { return tc_idesc(M, N) | (1u << 15) | (1u << 16); }
+
+__global__ void __launch_bounds__(kTcRows, 1) k_step_tc(const GuideRecord* __restrict__ rec, int n,
+                                                        const bf16* __restrict__ w16, const float* __restrict__ w32,
+                                                        float* __restrict__ loss, float* __restrict__ partial,
+                                                        int pool_n, unsigned long long seed, unsigned* err) {
+  extern __shared__ __align__(128) unsigned char sm[];
   const int t = threadIdx.x;
-  const uint32_t bar = tc_smem(wsm + kWtBar);
+  const uint32_t bar = tc_smem(sm + kFBar);
   if (t < 32) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(wsm + kWtTmem)),
-                 "r"(64));
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(sm + kFTmem)),
+                 "r"(kFCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (t == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  // Rows of A past the ones row stay zero for every tile.
-  for (int e = t; e < 128 * kWtRecs / 8; e += 128) reinterpret_cast<uint4*>(wsm + kWtA)[e] = make_uint4(0u, 0u, 0u, 0u);
+  // Weights in the forward layout and, for layers 1..4, transposed; biases in FP32.
+  for (int l = 0; l < kGLayers; ++l) {
+    const int K = guide_in(l), N = guide_out(l);
+    const uint4* w = reinterpret_cast<const uint4*>(w16 + guide_w_offset(l));
+    const int per_row = K / 8;
+    for (int e = t; e < N * per_row; e += kTcRows) {
+      const int o = e / per_row, i = (e - o * per_row) * 8;
+      const uint4 v = __ldg(w + e);
+      *reinterpret_cast<uint4*>(sm + f_w(l) + tc_off(o, i, K)) = v;
+      if (l > 0) {
+        const bf16* el = reinterpret_cast<const bf16*>(&v);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) *reinterpret_cast<bf16*>(sm + f_wt(l) + tc_off(i + j, o, N)) = el[j];
+      }
+    }
+  }
+  float* bias = reinterpret_cast<float*>(sm + kFBias);
+  for (int l = 0; l < kGLayers; ++l)
+    for (int c = t; c < guide_out(l); c += kTcRows) bias[l * kGHid + c] = w32[guide_b_offset(l) + c];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(wsm + kWtTmem);
-  const uint32_t idesc = tc_idesc(128, out);
+  const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + kFTmem);
+  const uint32_t lanes = (uint32_t)((t >> 5) * 32) << 16;
+  const float inv_n = 1.f / (float)n;
+  const int ntiles = (n + kTcRows - 1) / kTcRows;
   uint32_t phase = 0;
-  bool ok = true;
-  const bf16 one = __float2bfloat16(1.f), zero = __float2bfloat16(0.f);
-  for (int tile = 0; tile < kWtTiles && ok; ++tile) {
-    const long long r = (long long)blockIdx.x * kWtChunk + (long long)tile * kWtRecs + t;
-    const bool has = r < n;
-    // Stage record r as column t of A (inputs, ones row) and of B (outputs).
-    for (int c = 0; c < in; c += 8) {
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (has) v = *reinterpret_cast<const uint4*>(X + (size_t)r * in + c);
-      const bf16* e = reinterpret_cast<const bf16*>(&v);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) *reinterpret_cast<bf16*>(wsm + kWtA + tc_off(c + j, t, kWtRecs)) = e[j];
-    }
-    *reinterpret_cast<bf16*>(wsm + kWtA + tc_off(in, t, kWtRecs)) = has ? one : zero;
-    for (int c = 0; c < out; c += 8) {
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (has) v = *reinterpret_cast<const uint4*>(G + (size_t)r * out + c);
-      const bf16* e = reinterpret_cast<const bf16*>(&v);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) *reinterpret_cast<bf16*>(wsm + kWtB + tc_off(c + j, t, kWtRecs)) = e[j];
-    }
-    // The operands are visible to the tensor cores; the previous tile's MMAs are complete.
+  bool ok = true, first = true;
+  float lsum = 0.f;
+
+  // Makes every thread's shared-memory writes visible to the tensor cores and ends every
+  // thread's reads of the accumulator; thread 0 then issues `issue` and commits it.  Waits
+  // (bounded) for the commit; false, the same on every thread, when the wait gave up.
+  auto run = [&](auto issue) {
     tc_fence_proxy();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (t == 0) {
-      const uint32_t a0 = tc_smem(wsm + kWtA), b0 = tc_smem(wsm + kWtB);
-      for (int ks = 0; ks < kWtRecs / 16; ++ks)
-        tc_mma(tmem, tc_desc(a0 + ks * 256, 128, kWtRecs * 16), tc_desc(b0 + ks * 256, 128, kWtRecs * 16), idesc,
-               (tile > 0 || ks > 0) ? 1u : 0u);
+      issue();
       tc_commit(bar);
     }
-    // Every thread waits before the buffers are overwritten or the accumulator is read.
-    ok = __syncthreads_and(tc_wait(bar, phase & 1u) ? 1 : 0) != 0;
+    const bool done = __syncthreads_and(tc_wait(bar, phase & 1u) ? 1 : 0) != 0;
     ++phase;
+    if (done) tc_fence_after();
+    return done;
+  };
+  // K-major GEMM into the layer accumulator: A at a_off (row length ak), B at b_off (N rows
+  // of K columns).
+  auto mma_k = [&](int a_off, int ak, int b_off, int K, int N) {
+    const uint32_t a0 = tc_smem(sm + a_off), b0 = tc_smem(sm + b_off);
+    for (int ks = 0; ks < K / 16; ++ks)
+      tc_mma(tmem, tc_desc(a0 + ks * 256, 128, ak * 16), tc_desc(b0 + ks * 256, 128, K * 16), tc_idesc(kTcRows, N),
+             ks > 0 ? 1u : 0u);
+  };
+  // Weight gradient of layer l over the tile: A = its input tile, B = the gradient tile (row
+  // length N = the layer's outputs), both MN-major (core matrices adjacent in M or N 128
+  // bytes apart, adjacent in K one 8-record group apart), K = 128 records in steps of 16.
+  auto mma_dw = [&](int l, bool init) {
+    const int ak = f_act_k(l), N = guide_out(l);
+    const uint32_t a0 = tc_smem(sm + f_act(l)), b0 = tc_smem(sm + kFD);
+    for (int ks = 0; ks < kTcRows / 16; ++ks)
+      tc_mma(tmem + f_dw_col(l), tc_desc(a0 + ks * 2 * (ak * 16), ak * 16, 128),
+             tc_desc(b0 + ks * 2 * (N * 16), N * 16, 128), tc_idesc_mn(kTcRows, N), (init && ks == 0) ? 0u : 1u);
+  };
+
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const long long i = (long long)tile * kTcRows + t;
+    const bool has = i < n;
+    GuideRecord r{};
+    if (has) {
+      const long long src =
+          pool_n > 0 ? (long long)(Rng::splitmix64(seed ^ Rng::splitmix64((unsigned long long)i)) % (unsigned long long)pool_n)
+                     : i;
+      r = rec[src];
+    }
+    {
+      const float q[kGInputs] = {r.pos[0], r.pos[1], r.pos[2], r.n[0], r.n[1], r.n[2], r.wo[0], r.wo[1], r.wo[2]};
+#pragma unroll
+      for (int k = 0; k < kGIn; k += 8) {
+        const uint4 v = has ? make_uint4(guide_feature_pair(q, k), guide_feature_pair(q, k + 2),
+                                         guide_feature_pair(q, k + 4), guide_feature_pair(q, k + 6))
+                            : make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(sm + kFX + tc_off(t, k, kGIn)) = v;
+      }
+    }
+    uint32_t mask[4][2];
+    float o[kGOut];
+    for (int l = 0; l < kGLayers; ++l) {
+      const int N = guide_out(l);
+      if (!(ok = run([&] { mma_k(f_act(l), f_act_k(l), f_w(l), guide_in(l), N); }))) break;
+      uint32_t v[kGHid];
+      const uint32_t taddr = tmem + lanes;
+      tc_ld16(taddr, v);
+      tc_ld16(taddr + 16, v + 16);
+      tc_ld16(taddr + 32, v + 32);
+      if (N > 48) tc_ld16(taddr + 48, v + 48);
+      tc_ld_wait();
+      const float* bl = bias + l * kGHid;
+      if (l < kGLayers - 1) {
+        unsigned char* hrow = sm + f_act(l + 1);
+        mask[l][0] = mask[l][1] = 0u;
+#pragma unroll
+        for (int k = 0; k < kGHid; k += 8) {
+          uint32_t pw[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const int c = k + 2 * j;
+            pw[j] = pack_bf16x2(fmaxf(__uint_as_float(v[c]) + bl[c], 0.f),
+                                fmaxf(__uint_as_float(v[c + 1]) + bl[c + 1], 0.f));
+            // ReLU mask of the rounded activations, as the backward pass reads them.
+            const uint32_t bits = (lo_bf16(pw[j]) > 0.f ? 1u : 0u) | (hi_bf16(pw[j]) > 0.f ? 2u : 0u);
+            mask[l][c >> 5] |= bits << (c & 31);
+          }
+          *reinterpret_cast<uint4*>(hrow + tc_off(t, k, kFhK)) = make_uint4(pw[0], pw[1], pw[2], pw[3]);
+        }
+        // The ones column (bias gradients) of a record of the batch, zeros after it.
+        *reinterpret_cast<uint4*>(hrow + tc_off(t, kGHid, kFhK)) =
+            make_uint4(has ? pack_bf16x2(1.f, 0.f) : 0u, 0u, 0u, 0u);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kGOut; ++k) o[k] = __uint_as_float(v[k]) + bl[k];
+      }
+    }
+    if (!ok) break;
+    {
+      // Loss and output gradient of this record, divided by n and rounded to BF16.
+      float d[kGOut];
+      if (has) {
+        lsum += guide_loss_row(r, o, d);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kGOut; ++k) d[k] = 0.f;
+      }
+#pragma unroll
+      for (int k = 0; k < kGOut; k += 8)
+        *reinterpret_cast<uint4*>(sm + kFD + tc_off(t, k, kGOut)) =
+            make_uint4(pack_bf16x2(d[k] * inv_n, d[k + 1] * inv_n), pack_bf16x2(d[k + 2] * inv_n, d[k + 3] * inv_n),
+                       pack_bf16x2(d[k + 4] * inv_n, d[k + 5] * inv_n), pack_bf16x2(d[k + 6] * inv_n, d[k + 7] * inv_n));
+    }
+    for (int l = kGLayers - 1; l >= 1; --l) {
+      // dH_{l-1} into the accumulator and dW_l into its columns, both from the gradient tile.
+      if (!(ok = run([&] {
+              mma_k(kFD, guide_out(l), f_wt(l), guide_out(l), kGHid);
+              mma_dw(l, first);
+            })))
+        break;
+      uint32_t v[kGHid];
+      const uint32_t taddr = tmem + lanes;
+      tc_ld16(taddr, v);
+      tc_ld16(taddr + 16, v + 16);
+      tc_ld16(taddr + 32, v + 32);
+      tc_ld16(taddr + 48, v + 48);
+      tc_ld_wait();
+#pragma unroll
+      for (int k = 0; k < kGHid; k += 8) {
+        uint32_t pw[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int c = k + 2 * j;
+          const uint32_t m = mask[l - 1][c >> 5] >> (c & 31);
+          pw[j] = pack_bf16x2((m & 1u) ? __uint_as_float(v[c]) : 0.f, (m & 2u) ? __uint_as_float(v[c + 1]) : 0.f);
+        }
+        *reinterpret_cast<uint4*>(sm + kFD + tc_off(t, k, kGHid)) = make_uint4(pw[0], pw[1], pw[2], pw[3]);
+      }
+    }
+    if (!ok) break;
+    if (!(ok = run([&] { mma_dw(0, first); }))) break;
+    first = false;
   }
-  if (ok) {
-    tc_fence_after();
-    // Lane t of the accumulator: dW[o][t] for the layer's outputs o, or the bias gradient
-    // when t is the ones row.
-    uint32_t v[kGHid];
-    const uint32_t taddr = tmem + ((uint32_t)((t >> 5) * 32) << 16);
-    tc_ld16(taddr, v);
-    tc_ld16(taddr + 16, v + 16);
-    tc_ld16(taddr + 32, v + 32);
-    tc_ld16(taddr + 48, v + 48);
-    tc_ld_wait();
-    float* pw = partial + (size_t)blockIdx.x * kGParams;
-    if (t < in) {
-      for (int o = 0; o < out; ++o) pw[guide_w_offset(l) + o * in + t] = __uint_as_float(v[o]);
-    } else if (t == in) {
-      for (int o = 0; o < out; ++o) pw[guide_b_offset(l) + o] = __uint_as_float(v[o]);
+  for (int s = 16; s > 0; s >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, s);
+  if ((t & 31) == 0 && lsum != 0.f) atomicAdd(loss, lsum * inv_n);
+  float* pw = partial + (size_t)blockIdx.x * kGParams;
+  if (ok && !first) {
+    // Lane t of each weight-gradient accumulator: dW_l[o][t] for the layer's inputs t, and
+    // the bias gradient in the ones row (layer 0: the constant feature's row).
+    for (int l = 0; l < kGLayers; ++l) {
+      const int in = guide_in(l), out = guide_out(l);
+      uint32_t v[kGHid];
+      const uint32_t taddr = tmem + lanes + f_dw_col(l);
+      tc_ld16(taddr, v);
+      tc_ld16(taddr + 16, v + 16);
+      tc_ld16(taddr + 32, v + 32);
+      if (out > 48) tc_ld16(taddr + 48, v + 48);
+      tc_ld_wait();
+      if (t < in)
+        for (int c = 0; c < out; ++c) pw[guide_w_offset(l) + c * in + t] = __uint_as_float(v[c]);
+      if (t == (l == 0 ? kGOneFeature : kGHid))
+        for (int c = 0; c < out; ++c) pw[guide_b_offset(l) + c] = __uint_as_float(v[c]);
     }
   } else {
-    if (t == 0) atomicOr(err, kTcErrTimeout);
-    if (phase > 0) tc_wait(bar, (phase - 1) & 1u);  // the last commit, before the memory is freed
+    // No tile, or a wait gave up: this CTA adds nothing to the step.
+    for (int e = t; e < kGParams; e += kTcRows) pw[e] = 0.f;
+    if (!ok) {
+      if (t == 0) atomicOr(err, kTcErrTimeout);
+      if (phase > 0) tc_wait(bar, (phase - 1) & 1u);  // the last commit, before the memory is freed
+    }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (t < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(64));
+  if (t < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kFCols));
 }
 
 __global__ void k_reduce(const float* __restrict__ part, int z, float* __restrict__ g) {
@@ -721,9 +893,6 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool ada
                         uint64_t seed) {
   TrainBufs b{x0, {h[0], h[1], h[2], h[3]}, {dh[0], dh[1], dh[2], dh[3]}, dy, loss};
   cudaMemsetAsync(loss, 0, sizeof(float), st);
-  const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
-                                   (n + kTrainWarps * kTrainRows - 1) / (kTrainWarps * kTrainRows));
-  k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b, pool_n, seed);
   if (wgrad_tc && !tc_err) {
     if (cudaMalloc(&tc_err, sizeof(unsigned)) == cudaSuccess) {
       allocs.push_back(tc_err);
@@ -734,10 +903,13 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool ada
   }
   int z;
   if (wgrad_tc && tc_err) {
-    cudaFuncSetAttribute(k_wgrad_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kWtSmem);
-    z = (n + kWtChunk - 1) / kWtChunk;
-    k_wgrad_tc<<<dim3(z, kGLayers), 128, kWtSmem, st>>>(n, b, partial, tc_err);
+    cudaFuncSetAttribute(k_step_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem);
+    z = persistent_grid((const void*)k_step_tc, kTcRows, kFSmem, (n + kTcRows - 1) / kTcRows);
+    k_step_tc<<<z, kTcRows, kFSmem, st>>>(rec, n, params16, params, loss, partial, pool_n, seed, tc_err);
   } else {
+    const int grid = persistent_grid((const void*)k_train, kTrainWarps * 32, kTrainSmem,
+                                     (n + kTrainWarps * kTrainRows - 1) / (kTrainWarps * kTrainRows));
+    k_train<<<grid, kTrainWarps * 32, kTrainSmem, st>>>(rec, n, params16, params, b, pool_n, seed);
     z = (n + kWgChunk - 1) / kWgChunk;
     k_wgrad<<<dim3(z, kGLayers), 128, 0, st>>>(n, b, partial);
   }

@@ -44,8 +44,9 @@ struct GuideNet {
   // on the tensor cores timed out.
   bool forward_tc(const __nv_bfloat16* x, int n, float* out_rows, cudaStream_t st);
   unsigned* tc_err = nullptr;
-  // Weight gradients on the tcgen05 tensor cores (k_wgrad_tc; a wait that gave up sets
-  // tc_err) or on warp-level mma.sync (k_wgrad).
+  // Training step on the tcgen05 tensor cores (k_step_tc: forward, backward and weight
+  // gradients in one kernel; a wait that gave up sets tc_err) or on warp-level mma.sync
+  // (k_train + k_wgrad).
   bool wgrad_tc = true;
   // Nonzero when a tcgen05 wait of the network kernels gave up (reads tc_err; synchronous).
   unsigned tensor_error(cudaStream_t st);

@@ -91,8 +91,8 @@ def test_forward_tcgen05_matches(gpu_lib, n):
 
 @pytest.mark.parametrize("n", [777, 9000])
 def test_gradient_matches_oracle(gpu_lib, n):
-    """9000 records span 18 chunks of 512 records of the tcgen05 weight-gradient kernel, the
-    last one ragged."""
+    """9000 records span 71 tiles of 128 records of the tcgen05 training kernel, the last
+    one ragged."""
     g = _ctx()
     p = _params()
     g.guide_set_params(p)
@@ -116,10 +116,12 @@ def test_gradient_matches_oracle(gpu_lib, n):
 
 @pytest.mark.parametrize("n", [100, 5000, 70000])
 def test_weight_gradient_tcgen05_matches_mma(gpu_lib, n):
-    """The weight and bias gradients from the tcgen05 kernel (records staged transposed in
-    the UMMA core-matrix layout, accumulators in tensor memory, the bias gradient from a row
-    of ones) against the warp-level mma.sync kernel on the same records: the same BF16
-    products, summed in FP32 in another order."""
+    """The training step on the tcgen05 tensor cores (one kernel: forward, backward and the
+    weight and bias gradients accumulated in tensor memory, the bias gradient from a column
+    of ones) against the warp-level mma.sync kernels on the same records: the same BF16
+    products, summed in FP32 in another order.  Where the two sums of a hidden gradient round
+    to neighbouring BF16 values (one step is 2^-8 relative) the difference travels back
+    through the layers, so the bound is 2e-3 relative per layer."""
     g = _ctx()
     g.guide_set_params(_params())
     rec = G.random_records(n, seed=n + 1)
@@ -130,7 +132,7 @@ def test_weight_gradient_tcgen05_matches_mma(gpu_lib, n):
     for l in range(G.N_LAYERS):
         a, b = G.w_offset(l), G.b_offset(l) + G.layer_out(l)
         e = np.linalg.norm(grad_t[a:b] - grad_m[a:b]) / np.linalg.norm(grad_m[a:b])
-        assert e < 2e-4, (l, e)
+        assert e < 2e-3, (l, e)
     assert g.stats()["error_flags"] == 0
 
 
