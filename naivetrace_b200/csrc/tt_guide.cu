@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -730,18 +731,36 @@ int grid1(long long n) {
   return (int)(g < 1 ? 1 : (g > 8192 ? 8192 : g));
 }
 
+// Resident-block capacity of a kernel on the current device (SMs x blocks per SM), with its
+// dynamic shared-memory limit raised to `smem`; looked up once per kernel, launch shape and
+// device, as a training step launches its kernels many times per pass.
 int persistent_grid(const void* fn, int threads, int smem, long long work_blocks) {
-  static int sms = 0;
-  if (sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  struct Entry {
+    const void* fn;
+    int dev, threads, smem;
+    long long cap;
+  };
+  static std::mutex mu;
+  static std::vector<Entry> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  long long cap = 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : cache)
+      if (e.fn == fn && e.dev == dev && e.threads == threads && e.smem == smem) cap = e.cap;
+    if (cap == 0) {
+      int sms = 0, per_sm = 0;
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
+      cap = (long long)std::max(1, sms) * (per_sm > 0 ? per_sm : 1);
+      cache.push_back(Entry{fn, dev, threads, smem, cap});
+    }
   }
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem);
-  const long long cap = (long long)sms * (per_sm > 0 ? per_sm : 1);
   return (int)std::max(1LL, std::min(cap, work_blocks));
 }
+
 
 }  // namespace
 
@@ -903,7 +922,6 @@ void GuideNet::gradient(const GuideRecord* rec, int n, cudaStream_t st, bool ada
   }
   int z;
   if (wgrad_tc && tc_err) {
-    cudaFuncSetAttribute(k_step_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kFSmem);
     z = persistent_grid((const void*)k_step_tc, kTcRows, kFSmem, (n + kTcRows - 1) / kTcRows);
     k_step_tc<<<z, kTcRows, kFSmem, st>>>(rec, n, params16, params, loss, partial, pool_n, seed, tc_err);
   } else {
