@@ -316,8 +316,10 @@ def at_time(pts, t0):
     return float(np.exp(np.interp(np.log(t0), ts, es)))
 
 
-GUIDE_SETTINGS = dict(train_passes=3, discard_training=False, learning_rate=1e-3, record_pool=1 << 16,
-                      batch=8192, steps_per_pass=32, max_depth=1)
+GUIDE_SETTINGS = dict(train_passes=2, discard_training=False, learning_rate=1e-3, record_pool=1 << 16,
+                      batch=8192, steps_per_pass=64, max_depth=2)
+# The guided configuration's own training settings: 2^18 records per step at lr 1e-2.
+CONFIG_GUIDE_SETTINGS = dict(GUIDE_SETTINGS, batch=1 << 18, record_pool=1 << 18, learning_rate=1e-2)
 
 
 def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
@@ -329,6 +331,7 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
     wl = GuidingWorkload()
     plain, _ = wl.curve(False, budget_ms=budget_ms)
     guided, gst = wl.curve(True, budget_ms=budget_ms, **st_kw)
+    cfg_guided, cst = wl.curve(True, budget_ms=budget_ms, **CONFIG_GUIDE_SETTINGS)
     tree_kw = dict(st_kw)
     tree_kw.update(tree_subdivision=200, tree_em_iters=4)
     tree, tst = wl.curve(True, tree=True, budget_ms=budget_ms, **tree_kw)
@@ -350,6 +353,17 @@ def guiding_comparison(target=0.01, budget_ms=1000.0, settings=None):
         "settings": st_kw,
         "training": {"adam_steps": int(gst["guide_steps"]), "records": int(gst["guide_records"]),
                      "train_kernel_ms": gst["guide_train_ms"]},
+        "config_training_settings": {
+            "what": "the learned guider with the configuration's training settings (2^18 records per Adam "
+                    "step, lr 1e-2) on the same schedule",
+            "settings": CONFIG_GUIDE_SETTINGS,
+            "time_to_target_ms": time_to(cfg_guided, target),
+            "time_ratio_guided_over_plain": (time_to(cfg_guided, target) / tp) if (tp and time_to(cfg_guided, target))
+            else None,
+            "relmse_at_equal_time": at_time(cfg_guided, min(t_eq, cfg_guided[-1][0])),
+            "training": {"adam_steps": int(cst["guide_steps"]), "records": int(cst["guide_records"]),
+                         "train_kernel_ms": cst["guide_train_ms"]},
+        },
         "tree_guider": {
             "what": "kd-tree cells (200 records per initial cell) with 8-lobe vMF mixtures, batch EM (4 "
                     "iterations per round), the same schedule of training passes",
@@ -860,7 +874,7 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--spp", type=int, default=64)
     ap.add_argument("--wave", type=int, default=0, help="paths per wavefront wave (0 = library default)")
-    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--e2e-steps", type=int, default=7)
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU work for the CPU baseline")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-guiding", action="store_true", help="skip the learned-guided vs plain comparison")

@@ -422,10 +422,12 @@ typedef struct tt_guiding_params {
                                    maximisation step every 10 x prior strength records, each
                                    on that chunk alone); k > 0 = k EM iterations per round over
                                    all of the round's records of the cell */
-  int32_t network;              /* TT_GUIDE_LEARNED: the kernel that evaluates the network during
-                                   rendering, TT_GUIDE_NET_TCGEN05 (tensor-memory accumulators,
-                                   128-row tiles) or TT_GUIDE_NET_MMA (warp-level mma.sync,
-                                   16-row tiles); both give the same outputs */
+  int32_t network;              /* TT_GUIDE_LEARNED: the kernels that evaluate and train the
+                                   network, TT_GUIDE_NET_TCGEN05 (tensor-memory accumulators,
+                                   128-row tiles; a training step is one kernel) or
+                                   TT_GUIDE_NET_MMA (warp-level mma.sync, 16-row tiles); both
+                                   give the same network outputs, and gradients equal up to the
+                                   rounding of BF16 hidden gradients */
   int32_t tree_distribution;    /* TT_GUIDE_TREE: the directional distribution of a cell,
                                    TT_TREE_VMF (8-lobe vMF mixture, the reference's MoVmf
                                    distribution) or TT_TREE_QUADTREE (the reference's active

@@ -185,9 +185,10 @@ class GpuContext:
                     tree_em_iters: int = 0, network: int = abi.GUIDE_NET_TCGEN05,
                     tree_distribution: int = abi.TREE_VMF):
         """train: 0 frozen, 1 collect records and train after every pass, 2 collect only;
-        max_depth: guide the first max_depth bounces only (0: all).  Guiding the first bounce
-        only measured the best relMSE per unit time on the gap-lit room (the network's cost
-        grows with every guided vertex, its gain mostly comes from the first indirect one);
+        max_depth: guide the first max_depth bounces only (0: all).  Guiding the first two
+        bounces measured the best time to a given relMSE on the gap-lit room (the network's
+        cost grows with every guided vertex, its gain mostly comes from the first indirect
+        ones);
         network: the inference kernel of the learned guider (GUIDE_NET_TCGEN05 or
         GUIDE_NET_MMA, same outputs); tree_distribution: the tree guider's per-cell
         distribution (TREE_VMF mixtures or TREE_QUADTREE, the reference's quadtrees)."""
