@@ -156,7 +156,19 @@ struct HostEnv {
   tt_env_light desc;
   HostArray<float> tex;
   HostArray<float> cmf_rows, cmf_cols;  // made at upload; kept until tt_destroy (DMA sources)
+  HostArray<int> guide_rows, guide_cols;
 };
+
+// Guide table of a CMF (see kEnvGuide): guide[g] = the first index i with cmf[i] > g / kEnvGuide
+// (n when there is none), for g = 0 .. kEnvGuide, by one merged sweep.
+static void cmf_guide(const float* cmf, int n, int* guide) {
+  int i = 0;
+  for (int g = 0; g <= kEnvGuide; ++g) {
+    const float u = (float)g / (float)kEnvGuide;
+    while (i < n && !(cmf[i] > u)) ++i;
+    guide[g] = i;
+  }
+}
 
 // Device buffers owned by a context, from the library's memory pool, ordered on `stream`.
 struct DeviceBuffers {
@@ -1065,8 +1077,12 @@ tt_status tt_upload_scene(tt_ctx* c) {
       const auto& tex = c->envs[i].tex;
       HostArray<float>& rows = c->envs[i].cmf_rows;
       HostArray<float>& cols = c->envs[i].cmf_cols;
+      HostArray<int>& grows = c->envs[i].guide_rows;
+      HostArray<int>& gcols = c->envs[i].guide_cols;
       rows.resize(h);
       cols.resize((size_t)w * h);
+      grows.resize(kEnvGuide + 1);
+      gcols.resize((size_t)h * (kEnvGuide + 1));
       std::atomic<bool> zero_row{false};
       parallel_ranges(h, [&](long long y0, long long y1) {
         for (long long y = y0; y < y1; ++y) {
@@ -1081,6 +1097,7 @@ tt_status tt_upload_scene(tt_ctx* c) {
           }
           if (!(row_weight > 0.)) zero_row = true;
           for (int x = 0; x < w; ++x) cols[(size_t)y * w + x] /= (float)row_weight;
+          cmf_guide(&cols[(size_t)y * w], w, &gcols[(size_t)y * (kEnvGuide + 1)]);
           rows[y] = (float)row_weight;
         }
       }, /*serial_below=*/64);  // rows of a few thousand texels each
@@ -1088,11 +1105,14 @@ tt_status tt_upload_scene(tt_ctx* c) {
       for (int y = 1; y < h; ++y) rows[y] += rows[y - 1];
       const float inv = 1.f / rows[h - 1];
       for (int y = 0; y < h; ++y) rows[y] *= inv;
+      cmf_guide(rows.data(), h, grows.data());
       L.w = w;
       L.h = h;
       L.tex = (const float*)upload(tex.data(), tex.size() * sizeof(float));
       L.cmf_rows = (const float*)upload(rows.data(), rows.size() * sizeof(float));
       L.cmf_cols = (const float*)upload(cols.data(), cols.size() * sizeof(float));
+      L.guide_rows = (const int*)upload(grows.data(), grows.size() * sizeof(int));
+      L.guide_cols = (const int*)upload(gcols.data(), gcols.size() * sizeof(int));
     }
   }
   mark("env maps");

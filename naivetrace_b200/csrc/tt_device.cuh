@@ -211,6 +211,20 @@ __device__ __forceinline__ int tower_bisection(const float* cmf, int size, float
   }
   return upper >= size ? size - 1 : upper;
 }
+// tower_bisection's index (the first i with cmf[i] > r, at most size - 1) for r in [0, 1],
+// searched only between the guide entries that bracket r: the index is non-decreasing in r,
+// so it lies in [guide[g], guide[g + 1]] for g = floor(r kEnvGuide).
+__device__ __forceinline__ int guided_bisection(const float* __restrict__ cmf, const int* __restrict__ guide, int size,
+                                                float r) {
+  const int g = min((int)(r * (float)kEnvGuide), kEnvGuide - 1);
+  int lo = __ldg(&guide[g]), hi = __ldg(&guide[g + 1]);
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&cmf[mid]) > r) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo >= size ? size - 1 : lo;
+}
 __device__ __forceinline__ float prob_from_cmf(const float* cmf, int idx) {
   return cmf[idx] - (idx > 0 ? cmf[idx - 1] : 0.f);
 }
@@ -904,10 +918,10 @@ __device__ __forceinline__ DirSample env_sample_one(const DevEnvLight& L, R& rng
       return s;
     default: {  // TT_ENV_MAP
       rng.square(r);
-      const int y = tower_bisection(L.cmf_rows, L.h, r[1]);
+      const int y = guided_bisection(L.cmf_rows, L.guide_rows, L.h, r[1]);
       const float proby = prob_from_cmf(L.cmf_rows, y);
       const float* row = L.cmf_cols + (size_t)y * L.w;
-      const int x = tower_bisection(row, L.w, r[0]);
+      const int x = guided_bisection(row, L.guide_cols + (size_t)y * (kEnvGuide + 1), L.w, r[0]);
       const float probx = prob_from_cmf(row, x);
       float phi0, z0, phi1, z1;
       envmap_pixel_angles(L, x, y, &phi0, &z0, &phi1, &z1);

@@ -87,7 +87,14 @@ struct DevEnvLight {
   const float* tex;                      // env map RGB, row 0 = top
   const float* cmf_rows;                 // h
   const float* cmf_cols;                 // w * h
+  const int* guide_rows;                 // kEnvGuide + 1: search range of cmf_rows per 1/kEnvGuide of [0, 1]
+  const int* guide_cols;                 // h * (kEnvGuide + 1): the same per row of cmf_cols
 };
+// Entries of the env map's CMF guide tables: guide[g] = the index that inverting the CMF
+// gives for r = g / kEnvGuide (the first entry above r), so that a sample r needs only a
+// bisection between guide[g] and guide[g + 1], g = floor(r kEnvGuide).  A power of two, so
+// that g / kEnvGuide and r kEnvGuide are exact in float.
+constexpr int kEnvGuide = 256;
 
 struct DevCamera {
   int kind;
