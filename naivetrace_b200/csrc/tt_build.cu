@@ -458,6 +458,12 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     return true;
   }
   Scratch sc(st);
+  // Small values read back (or sent) during the build go through page-locked host memory:
+  // a copy into a pageable stack variable would make every one of them a synchronous round
+  // trip, four per clustering iteration.  One 256-byte area per host thread that builds,
+  // kept for the thread's lifetime.
+  thread_local int* hb = nullptr;
+  if (!hb && !ok(cudaHostAlloc((void**)&hb, 256, cudaHostAllocPortable), "page-locked read-back area")) return false;
   const uint32_t total = 2 * n - 1;
   // TT_BUILD_VERBOSE=1 prints the phase times and the iteration count to stderr.
   const bool verbose = std::getenv("TT_BUILD_VERBOSE") != nullptr;
@@ -515,7 +521,7 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     cub::DeviceScan::ExclusiveSum(temp, tb, create, create_off, c, st);
     tb = std::max(sort_bytes, scan_bytes);
     cub::DeviceScan::ExclusiveSum(temp, tb, keep, keep_off, c, st);
-    int tail[4];
+    int* tail = hb;
     cudaMemcpyAsync(&tail[0], create_off + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&tail[1], create + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaMemcpyAsync(&tail[2], keep_off + c - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -531,10 +537,10 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     std::swap(cur, nxt);
   }
   const double t_clustered = verbose ? ms_since(t_start) : 0.0;
-  int root = 0;
-  if (!ok(cudaMemcpyAsync(&root, cur, sizeof(int), cudaMemcpyDeviceToHost, st), "copy") ||
+  if (!ok(cudaMemcpyAsync(&hb[4], cur, sizeof(int), cudaMemcpyDeviceToHost, st), "copy") ||
       !ok(cudaStreamSynchronize(st), "sync"))
     return false;
+  const int root = hb[4];
   // Bottom-up costs, top-down offsets and emission.
   int* size = sc.alloc<int>(total);
   float* cost = sc.alloc<float>(total);
@@ -554,22 +560,23 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   for (const auto& r : ranges)
     k_costs<<<grid_for(r.second), kThreads, 0, st>>>(r.first, r.second, n, node_box, left, right, size, cost, collapse,
                                                       inner);
-  const int zero = 0;
-  const unsigned char none = 0;
-  cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(index + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(state + root, &none, 1, cudaMemcpyHostToDevice, st);
-  cudaMemcpyAsync(depth + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(offset + root, 0, sizeof(int), st);
+  cudaMemsetAsync(index + root, 0, sizeof(int), st);
+  cudaMemsetAsync(state + root, 0, 1, st);  // no state
+  cudaMemsetAsync(depth + root, 0, sizeof(int), st);
   for (auto it = ranges.rbegin(); it != ranges.rend(); ++it)
     k_topdown<<<grid_for(it->second), kThreads, 0, st>>>(it->first, it->second, n, left, right, size, collapse, inner,
                                                           offset, index, state, depth, emit, max_depth);
-  int emitted = 0;
-  unsigned depth_host = 0;
-  unsigned char root_emit = 0;
-  if (root >= (int)n) cudaMemcpyAsync(&emitted, inner + root, sizeof(int), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&depth_host, max_depth, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(&root_emit, emit + root, 1, cudaMemcpyDeviceToHost, st);
+  hb[5] = 0;
+  hb[6] = 0;
+  hb[7] = 0;
+  if (root >= (int)n) cudaMemcpyAsync(&hb[5], inner + root, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&hb[6], max_depth, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&hb[7], emit + root, 1, cudaMemcpyDeviceToHost, st);
   if (!ok(cudaStreamSynchronize(st), "emission")) return false;
+  const int emitted = hb[5];
+  const unsigned depth_host = (unsigned)hb[6];
+  const unsigned char root_emit = (unsigned char)(hb[7] & 0xff);
   const int num_nodes = root_emit ? emitted : 1;
   // The 4-wide nodes are at most the emitted binary nodes (each 4-wide node replaces at
   // least one); the actual count comes from the collapse.
@@ -581,7 +588,7 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
   int num4 = 1;
   // The root is a leaf when the whole tree collapses (or n == 1): its subtree starts at 0.
   if (!root_emit) {
-    cudaMemcpyAsync(offset + root, &zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(offset + root, 0, sizeof(int), st);
     k_leaf_root<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes);
     k_leaf_root4<<<1, 1, 0, st>>>(node_box, root, (int)n, out->nodes4);
   } else {
@@ -591,18 +598,20 @@ bool device_build_bvh2(const BuildInput& in, const uint32_t* set, uint32_t n, De
     int2* front[2] = {sc.alloc<int2>(cap4), sc.alloc<int2>(cap4)};
     int* counts = sc.alloc<int>(2);  // [0] 4-wide nodes numbered, [1] next level's size
     if (!front[0] || !front[1] || !counts) return fail("out of device memory");
-    const int2 root4 = make_int2(root, 0);
-    const int init[2] = {1, 0};
-    cudaMemcpyAsync(front[0], &root4, sizeof(int2), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(counts, init, sizeof(init), cudaMemcpyHostToDevice, st);
+    hb[8] = root;  // the first front: (root, 0); counts: {1, 0}
+    hb[9] = 0;
+    hb[10] = 1;
+    hb[11] = 0;
+    cudaMemcpyAsync(front[0], &hb[8], sizeof(int2), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(counts, &hb[10], 2 * sizeof(int), cudaMemcpyHostToDevice, st);
     int nfront = 1;
     for (int level = 0; nfront > 0 && level < 64; ++level) {
       cudaMemsetAsync(counts + 1, 0, sizeof(int), st);
       k_collapse4<<<grid_for(nfront), kThreads, 0, st>>>(front[level & 1], nfront, n, node_box, left, right, size,
                                                           offset, emit, index, counts, front[(level + 1) & 1],
                                                           counts + 1, out->nodes4);
-      int c2[2] = {0, 0};
-      cudaMemcpyAsync(c2, counts, sizeof(c2), cudaMemcpyDeviceToHost, st);
+      int* c2 = &hb[12];
+      cudaMemcpyAsync(c2, counts, 2 * sizeof(int), cudaMemcpyDeviceToHost, st);
       if (!ok(cudaStreamSynchronize(st), "4-wide collapse")) return false;
       nfront = c2[1];
       num4 = c2[0];

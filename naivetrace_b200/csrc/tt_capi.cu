@@ -703,21 +703,27 @@ tt_status tt_upload_scene(tt_ctx* c) {
   if (!c) return TT_ERR_INVALID;
   TT_CUDA(c, cudaSetDevice(c->device));
   if (c->uploaded) return TT_OK;
+  const auto t_enter = std::chrono::steady_clock::now();
   TT_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   c->scene_mem.stream = c->stream;
   c->path_mem.stream = c->stream;
   upload_constant_tables();
   TT_CUDA(c, cudaGetLastError());
-  // TT_UPLOAD_TIMING=1 prints the host time of the upload's phases to stderr.
-  const bool tm = std::getenv("TT_UPLOAD_TIMING") != nullptr;
-  auto t_last = std::chrono::steady_clock::now();
+  // TT_UPLOAD_TIMING=1 prints the time of the upload's phases to stderr, each phase ended
+  // by a stream synchronisation; TT_UPLOAD_TIMING=2 prints the host time of each phase
+  // without synchronising (queued device work then counts where the host waits for it).
+  const char* tm_env = std::getenv("TT_UPLOAD_TIMING");
+  const bool tm = tm_env != nullptr;
+  const bool tm_sync = tm && std::atoi(tm_env) != 2;
+  auto t_last = t_enter;
   auto mark = [&](const char* what) {
     if (!tm) return;
-    cudaStreamSynchronize(c->stream);
+    if (tm_sync) cudaStreamSynchronize(c->stream);
     const auto now = std::chrono::steady_clock::now();
     std::fprintf(stderr, "upload %-12s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(now - t_last).count());
     t_last = now;
   };
+  mark("stream+consts");
   const uint32_t ntri = (uint32_t)c->mats.size();
   // Surfaces and medium boundaries go into separate BVHs (Scene::BuildAccelStructure,
   // scene.cxx:116-141); both store global triangle ids in their slots.
