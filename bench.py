@@ -55,7 +55,7 @@ def workload_config(scene, spp, depth, name):
         "spp": spp,
         "max_depth": depth,
         "paths_per_step": cam.xres * cam.yres * spp,
-        "l2_policy": "inputs larger than L2: BVH + triangles ~0.3 GB and ~13 GB of path state per wave of 2^26 paths",
+        "l2_policy": "inputs larger than L2: BVH + triangles ~0.3 GB and ~30 GB of path state per wave of 2^27 paths",
     }
 
 
@@ -259,11 +259,11 @@ class GuidingWorkload:
         kw.update(guide_kw)
         if tree:
             kw.update(method=abi.GUIDE_TREE)
-        # One untimed pass at the largest wave size (2^26 paths) allocates the path state
+        # One untimed pass at the largest wave size (2^27 paths) allocates the path state
         # (with the guiding arrays for the guided run); the guide is not trained by it.
         if guided:
             g.set_guiding(True, 0, **kw)
-        g.render(-(-(1 << 26) // (self.xres * self.yres)), 3)
+        g.render(-(-(1 << 27) // (self.xres * self.yres)), 3)
         g.clear()
         g.reset_stats()
 

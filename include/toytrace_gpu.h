@@ -210,7 +210,7 @@ typedef struct tt_params {
   int32_t max_ray_depth;        /* --rd (reference default 25) */
   int32_t pt_sample_mode;       /* TT_SAMPLE_* */
   int32_t max_samples_per_pixel;/* --spp; <= 0 means unbounded (Run loops until stopped) */
-  int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default (2^26, halved
+  int32_t wave_paths;           /* paths resident per wavefront wave; 0 = default (2^27, halved
                                    while the device cannot hold it) */
   int32_t device;               /* CUDA device ordinal */
   int32_t algo;                 /* TT_ALGO_* */

@@ -35,12 +35,13 @@ using namespace tt;
 
 namespace {
 
-// Paths resident per wave: 2^26 paths hold about 16 GB of path state (more with media or
-// guiding), a small share of the B200's HBM; a large wave keeps every launch of the bounce
-// loop full, so the latency-bound tail launches of the last bounces are paid once per 2^26
-// paths (the 1920x1080x64 frame: 2 waves instead of 32 at 2^22, 1.6x the throughput).
+// Paths resident per wave: 2^27 paths hold about 30 GB of path state (more with media or
+// guiding), a sixth of the B200's HBM; a large wave keeps every launch of the bounce loop
+// full, so the latency-bound tail launches of the last bounces are paid once per 2^27 paths
+// (the 1920x1080x64 frame: one wave, against 2 at 2^26 (2.6 % slower) and 32 at 2^22
+// (1.6x slower)).  Path-slot indices stay below 2^31 in every array for waves up to 2^27.
 // When the device cannot hold a wave, the wave is halved until it fits (down to 2^20).
-constexpr int kDefaultWave = 1 << 26;
+constexpr int kDefaultWave = 1 << 27;
 
 std::mutex g_err_mutex;
 std::string g_create_error;
@@ -1473,7 +1474,7 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
     launches++;
     for (int b = 0; b < rounds; ++b) {
       timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, b, counting, c->d_stats + 2, grid, c->stream); });
-      launch_flush(c->dev, c->ps, c->fb, b, grid, c->stream);
+      if (c->dev.guide_record) launch_flush(c->dev, c->ps, c->fb, b, grid, c->stream);
       timed(0, [&] { launch_extend(c->dev, c->ps, b, counting, c->d_stats, grid, c->stream); });
       if (c->dev.num_media > 0) {
         launch_track(c->dev, c->ps, b, grid, c->stream);
@@ -1484,10 +1485,13 @@ static tt_status render_range(tt_ctx* c, int32_t spp, uint64_t seed, int32_t pb,
         launch_guide(c->dev, c->ps, b, c->stream);
         launches++;
       }
-      launches += 3 + shade_launches(c->dev, c->ps, b);
+      launches += (c->dev.guide_record ? 3 : 2) + shade_launches(c->dev, c->ps, b);
     }
     timed(1, [&] { launch_shadow(c->dev, c->ps, c->fb, rounds, counting, c->d_stats + 2, grid, c->stream); });
-    launch_flush(c->dev, c->ps, c->fb, rounds, grid, c->stream);
+    // Finished paths into the pass framebuffer: with guiding records, k_flush after every
+    // bounce (it also commits the records); without, one gather at the end of the wave.
+    if (c->dev.guide_record) launch_flush(c->dev, c->ps, c->fb, rounds, grid, c->stream);
+    else launch_gather(c->dev, c->ps, c->fb, w, grid, c->stream);
     k_tally<<<1, 32, 0, c->stream>>>(c->ps.counters, rounds, c->d_stats);
     launches += 3;
     cudaEventRecord(wave_ev[wave_index & 1], c->stream);

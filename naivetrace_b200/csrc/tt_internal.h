@@ -275,6 +275,11 @@ void launch_shadow(const DevScene& s, const PathState& p, const Framebuffer& fb,
                    unsigned long long* stats, int grid, cudaStream_t st);
 void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, int grid,
                   cudaStream_t st);
+// End of a wave without guiding records: every path's accumulator is final, so each pixel
+// of the pass range sums the RGB of its paths in the wave (its slots npix_range apart, in
+// sample order) into the pass framebuffer; this replaces the wave's k_flush launches.
+void launch_gather(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
+                   cudaStream_t st);
 // Guided scenes: network evaluation and one-sample MIS scattering of the queued guided
 // vertices (persistent kernel, as many CTAs as fit on the SMs).
 void launch_guide(const DevScene& s, const PathState& p, int bounce, cudaStream_t st);

@@ -2025,6 +2025,22 @@ __global__ void __launch_bounds__(256) k_flush(DevScene sc, PathState p, Framebu
   }
 }
 
+__global__ void __launch_bounds__(256) k_gather(PathState p, Framebuffer fb, WaveArgs w) {
+  const int off = (int)(w.wave_start % w.npix_range);
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < w.npix_range; j += gridDim.x * blockDim.x) {
+    // Slot i holds pixel (wave_start + i) mod npix_range.
+    int i = j - off;
+    if (i < 0) i += w.npix_range;
+    float3 sum = f3(0.f, 0.f, 0.f);
+    for (; i < w.wave_paths; i += w.npix_range)
+      sum = sum + selection_to_rgb(xyz(p.accum[i]), unpack_lambda(p.meta[i].y));
+    float* a = fb.accum + 3 * (size_t)(w.pixel_begin + j);
+    a[0] += sum.x;
+    a[1] += sum.y;
+    a[2] += sum.z;
+  }
+}
+
 __global__ void k_accumulate(Framebuffer fb, double* acc, double* light, int n3) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += gridDim.x * blockDim.x) {
     acc[i] += (double)fb.accum[i];
@@ -2322,6 +2338,11 @@ void launch_init_tracker(const DevScene& s, float3 pos, float3 bb_lo, float3 bb_
 void launch_flush(const DevScene& s, const PathState& p, const Framebuffer& fb, int bounce, int grid,
                   cudaStream_t st) {
   k_flush<<<fit_grid(k_flush, grid, blk(s)), blk(s), 0, st>>>(s, p, fb, bounce);
+}
+
+void launch_gather(const DevScene& s, const PathState& p, const Framebuffer& fb, const WaveArgs& w, int grid,
+                   cudaStream_t st) {
+  k_gather<<<fit_grid(k_gather, grid, 256), 256, 0, st>>>(p, fb, w);
 }
 
 void launch_generate_views(const DevScene& s, const PathState& p, const ViewWave* waves, const int* wave_idx,
